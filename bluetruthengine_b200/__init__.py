@@ -1,0 +1,402 @@
+"""bluetruthengine_b200 -- B200-native wavefront path tracer behind Blue Truth
+Engine's renderer API.
+
+Python host mirror of the reference's include/render_kernel.h over the C-ABI
+library libbte_b200.so (include/bte/render_api.h).  Function names follow the
+reference (init_scene <- cudaInitScene, render <- cudaRender, ...).  Errors
+raise BteError with the library's message; the reference exits the process
+instead (src/host/cuda_check.h:14-32).  There is no CPU fallback: without the
+library or without a CUDA device, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+__all__ = ["BteError", "Renderer", "Scene", "load_scene", "library_path", "load_library", "RenderConfig",
+           "ENV_CDF", "ENV_ALIAS", "TRIANGLE_DTYPE", "BSDF_DTYPE", "EMITTER_DTYPE", "SPOT_DTYPE", "CAMERA_DTYPE"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ENV_CDF = 0
+ENV_ALIAS = 1
+
+
+class BteError(RuntimeError):
+    pass
+
+
+# ---- POD layouts, byte-identical to render_kernel.h:9-94 ----
+TRIANGLE_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("n0", "<f4", 3), ("n1", "<f4", 3),
+                           ("n2", "<f4", 3), ("uv0", "<f4", 2), ("uv1", "<f4", 2), ("uv2", "<f4", 2)])
+BSDF_DTYPE = np.dtype([("type", "<i4"), ("p0", "<f4", 4), ("p1", "<f4", 4), ("p2", "<f4", 4), ("p3", "<f4", 4)])
+EMITTER_DTYPE = np.dtype([("triIndexOffset", "<i4"), ("triCount", "<i4"), ("cdfOffset", "<i4"), ("radiance", "<f4", 3),
+                          ("areaSum", "<f4"), ("powerWeight", "<f4")])
+SPOT_DTYPE = np.dtype([("position", "<f4", 3), ("direction", "<f4", 3), ("radiance", "<f4", 3), ("intensity", "<f4"),
+                       ("innerConeCosine", "<f4"), ("outerConeCosine", "<f4")])
+CAMERA_DTYPE = np.dtype([("origin", "<f4", 3), ("forward", "<f4", 3), ("right", "<f4", 3), ("up", "<f4", 3),
+                         ("fovYRadians", "<f4"), ("aspect", "<f4")])
+assert TRIANGLE_DTYPE.itemsize == 96 and BSDF_DTYPE.itemsize == 68 and CAMERA_DTYPE.itemsize == 56
+
+
+class RenderConfig(C.Structure):
+    _fields_ = [("samplesPerFrame", C.c_int), ("maxDepth", C.c_int), ("rrStart", C.c_int), ("envSampling", C.c_int),
+                ("blockSize", C.c_int), ("useGraph", C.c_int)]
+
+
+class FrameStats(C.Structure):
+    _fields_ = [("samples", C.c_int64), ("extends", C.c_int64), ("shadowRays", C.c_int64),
+                ("maxBounceReached", C.c_int), ("msTotal", C.c_float), ("msGenerate", C.c_float),
+                ("msExtend", C.c_float), ("msShade", C.c_float), ("msConnect", C.c_float), ("msPresent", C.c_float)]
+
+
+class _SceneArrays(C.Structure):
+    _fields_ = [("triangles", C.c_void_p), ("triangleCount", C.c_int), ("materials", C.c_void_p),
+                ("materialCount", C.c_int), ("triangleMaterialIds", C.c_void_p), ("triangleBsdfIds", C.c_void_p),
+                ("bsdfs", C.c_void_p), ("bsdfCount", C.c_int), ("triangleEmission", C.c_void_p),
+                ("triangleEmitterFlags", C.c_void_p), ("emitters", C.c_void_p), ("emitterCount", C.c_int),
+                ("emitterTriIndices", C.c_void_p), ("emitterTriIndexCount", C.c_int), ("emitterTriCdf", C.c_void_p),
+                ("emitterTriCdfCount", C.c_int), ("sceneEmitterCdf", C.c_void_p), ("spotlights", C.c_void_p),
+                ("spotlightCount", C.c_int), ("envRGBA", C.c_void_p), ("envWidth", C.c_int), ("envHeight", C.c_int),
+                ("envIntensity", C.c_float), ("envRotationDeg", C.c_float), ("camera", C.c_ubyte * 56),
+                ("width", C.c_int), ("height", C.c_int)]
+
+
+def library_path() -> str:
+    return os.path.join(HERE, "libbte_b200.so")
+
+
+_LIB: Optional[C.CDLL] = None
+
+
+def load_library(build_if_missing: bool = True) -> C.CDLL:
+    """Load libbte_b200.so (building it with nvcc when absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if build_if_missing:
+        from . import build as _build
+        _build.build()
+    if not os.path.exists(path):
+        raise BteError(f"libbte_b200.so not found at {path}; run bluetruthengine_b200/build.py")
+    lib = C.CDLL(path)
+    lib.bte_last_error.restype = C.c_char_p
+    lib.bte_get_render_mode.restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc: int):
+    if rc < 0:
+        raise BteError(load_library(False).bte_last_error().decode("utf-8", "replace"))
+    return rc
+
+
+def _view(ptr: int, dtype, count: int) -> np.ndarray:
+    if count <= 0 or not ptr:
+        return np.zeros(0, dtype=dtype)
+    dt = np.dtype(dtype)
+    buf = (C.c_char * (dt.itemsize * count)).from_address(ptr)
+    return np.frombuffer(buf, dtype=dt, count=count).copy()
+
+
+@dataclass
+class Scene:
+    """Flattened scene: the arrays src/main.cpp:600-930 passes to the cudaInit* calls."""
+    triangles: np.ndarray           # TRIANGLE_DTYPE [T]
+    materials: np.ndarray           # float32 [M,3]
+    triangle_material_ids: np.ndarray
+    triangle_bsdf_ids: np.ndarray
+    bsdfs: np.ndarray               # BSDF_DTYPE [B]
+    triangle_emission: np.ndarray   # float32 [T,3]
+    triangle_emitter_flags: np.ndarray  # uint8 [T]
+    emitters: np.ndarray            # EMITTER_DTYPE [E]
+    emitter_tri_indices: np.ndarray
+    emitter_tri_cdf: np.ndarray
+    scene_emitter_cdf: np.ndarray   # float32 [E+1]
+    spotlights: np.ndarray          # SPOT_DTYPE [S]
+    env_rgba: Optional[np.ndarray]  # float32 [H,W,4]
+    env_intensity: float
+    env_rotation_deg: float
+    camera: np.ndarray              # CAMERA_DTYPE scalar
+    width: int
+    height: int
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.triangles.shape[0])
+
+
+def load_scene(path: str) -> Scene:
+    """Parse scene.xml + OBJ (+ .hdr) with the library's loader (no GPU needed)."""
+    lib = load_library()
+    h = C.c_void_p()
+    _check(lib.bte_scene_load(path.encode(), C.byref(h)))
+    try:
+        a = _SceneArrays()
+        _check(lib.bte_scene_arrays(h, C.byref(a)))
+        T = a.triangleCount
+        env = None
+        if a.envRGBA and a.envWidth > 0:
+            env = _view(a.envRGBA, np.float32, a.envWidth * a.envHeight * 4).reshape(a.envHeight, a.envWidth, 4)
+        cam = np.frombuffer(bytes(a.camera), dtype=CAMERA_DTYPE, count=1)[0].copy()
+        E = a.emitterCount
+        return Scene(
+            triangles=_view(a.triangles, TRIANGLE_DTYPE, T),
+            materials=_view(a.materials, np.float32, 3 * a.materialCount).reshape(-1, 3),
+            triangle_material_ids=_view(a.triangleMaterialIds, np.int32, T),
+            triangle_bsdf_ids=_view(a.triangleBsdfIds, np.int32, T),
+            bsdfs=_view(a.bsdfs, BSDF_DTYPE, a.bsdfCount),
+            triangle_emission=_view(a.triangleEmission, np.float32, 3 * T).reshape(-1, 3),
+            triangle_emitter_flags=_view(a.triangleEmitterFlags, np.uint8, T),
+            emitters=_view(a.emitters, EMITTER_DTYPE, E),
+            emitter_tri_indices=_view(a.emitterTriIndices, np.int32, a.emitterTriIndexCount),
+            emitter_tri_cdf=_view(a.emitterTriCdf, np.float32, a.emitterTriCdfCount),
+            scene_emitter_cdf=_view(a.sceneEmitterCdf, np.float32, E + 1 if E > 0 else 1),
+            spotlights=_view(a.spotlights, SPOT_DTYPE, a.spotlightCount),
+            env_rgba=env, env_intensity=float(a.envIntensity), env_rotation_deg=float(a.envRotationDeg),
+            camera=cam, width=int(a.width), height=int(a.height))
+    finally:
+        lib.bte_scene_free(h)
+
+
+class Renderer:
+    """The reference's renderer API (render_kernel.h:100-211) over libbte_b200.
+
+    One renderer state per process, like the reference's globals.
+    """
+
+    def __init__(self):
+        self.lib = load_library()
+        self._keep = []
+
+    # ---- uploads ----
+    def init_scene(self, triangles, materials, triangle_material_ids, width, height):
+        t = np.ascontiguousarray(triangles, dtype=TRIANGLE_DTYPE)
+        m = np.ascontiguousarray(materials, dtype=np.float32)
+        ids = None if triangle_material_ids is None else np.ascontiguousarray(triangle_material_ids, dtype=np.int32)
+        _check(self.lib.bte_init_scene(_ptr(t), len(t), _ptr(m), len(m), _ptr(ids), int(width), int(height)))
+
+    def init_accel(self):
+        _check(self.lib.bte_init_accel())
+
+    init_optix = init_accel   # the reference name (cudaInitOptix) builds the acceleration structure
+
+    def init_camera(self, camera):
+        c = np.ascontiguousarray(np.asarray(camera, dtype=CAMERA_DTYPE).reshape(1))
+        _check(self.lib.bte_init_camera(_ptr(c)))
+
+    def init_triangle_emission(self, emission):
+        e = None if emission is None else np.ascontiguousarray(emission, dtype=np.float32)
+        _check(self.lib.bte_init_triangle_emission(_ptr(e), 0 if e is None else len(e)))
+
+    def init_triangle_emitter_flags(self, flags):
+        f = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+        _check(self.lib.bte_init_triangle_emitter_flags(_ptr(f), 0 if f is None else len(f)))
+
+    def init_emitter_table(self, emitters, tri_indices, tri_cdf, scene_cdf):
+        if emitters is None or len(emitters) == 0:
+            _check(self.lib.bte_init_emitter_table(None, 0, None, 0, None, 0, None))
+            return
+        e = np.ascontiguousarray(emitters, dtype=EMITTER_DTYPE)
+        ti = np.ascontiguousarray(tri_indices, dtype=np.int32)
+        tc = np.ascontiguousarray(tri_cdf, dtype=np.float32)
+        sc = np.ascontiguousarray(scene_cdf, dtype=np.float32)
+        _check(self.lib.bte_init_emitter_table(_ptr(e), len(e), _ptr(ti), len(ti), _ptr(tc), len(tc), _ptr(sc)))
+
+    def init_bsdfs(self, bsdfs, triangle_bsdf_ids):
+        b = np.ascontiguousarray(bsdfs, dtype=BSDF_DTYPE)
+        ids = np.ascontiguousarray(triangle_bsdf_ids, dtype=np.int32)
+        _check(self.lib.bte_init_bsdfs(_ptr(b), len(b), _ptr(ids), len(ids)))
+
+    def init_spotlights(self, spots):
+        if spots is None or len(spots) == 0:
+            _check(self.lib.bte_init_spotlights(None, 0))
+            return
+        s = np.ascontiguousarray(spots, dtype=SPOT_DTYPE)
+        _check(self.lib.bte_init_spotlights(_ptr(s), len(s)))
+
+    def init_env_map(self, rgba, intensity=1.0, rotation_deg=0.0):
+        if rgba is None:
+            _check(self.lib.bte_init_env_map(None, 0, 0, C.c_float(0.0), C.c_float(0.0)))
+            return
+        e = np.ascontiguousarray(rgba, dtype=np.float32)
+        h, w = e.shape[0], e.shape[1]
+        _check(self.lib.bte_init_env_map(_ptr(e), w, h, C.c_float(intensity), C.c_float(rotation_deg)))
+
+    def init_textures(self, images):
+        self._init_tex(self.lib.bte_init_textures, images)
+
+    def init_mr_textures(self, images):
+        self._init_tex(self.lib.bte_init_mr_textures, images)
+
+    def _init_tex(self, fn, images):
+        if not images:
+            _check(fn(None, None, None, 0))
+            return
+        arrs = [None if im is None else np.ascontiguousarray(im, dtype=np.uint8) for im in images]
+        ptrs = (C.c_void_p * len(arrs))(*[None if a is None else a.ctypes.data for a in arrs])
+        ws = np.array([0 if a is None else a.shape[1] for a in arrs], dtype=np.int32)
+        hs = np.array([0 if a is None else a.shape[0] for a in arrs], dtype=np.int32)
+        _check(fn(ptrs, _ptr(ws), _ptr(hs), len(arrs)))
+
+    def upload(self, scene: Scene):
+        """All uploads in the order of src/main.cpp:819-930."""
+        self.init_camera(scene.camera)
+        self.init_textures(None)
+        self.init_mr_textures(None)
+        self.init_scene(scene.triangles, scene.materials, scene.triangle_material_ids, scene.width, scene.height)
+        self.init_accel()
+        self.init_triangle_emission(scene.triangle_emission)
+        self.init_triangle_emitter_flags(scene.triangle_emitter_flags)
+        self.init_emitter_table(scene.emitters, scene.emitter_tri_indices, scene.emitter_tri_cdf,
+                                scene.scene_emitter_cdf)
+        self.init_bsdfs(scene.bsdfs, scene.triangle_bsdf_ids)
+        self.init_spotlights(scene.spotlights)
+        self.init_env_map(scene.env_rgba, scene.env_intensity, scene.env_rotation_deg)
+
+    # ---- frame API ----
+    def set_config(self, samples_per_frame=1, max_depth=200, rr_start=3, env_sampling=ENV_CDF, block_size=0,
+                   use_graph=0):
+        cfg = RenderConfig(samples_per_frame, max_depth, rr_start, env_sampling, block_size, use_graph)
+        _check(self.lib.bte_set_render_config(C.byref(cfg)))
+
+    def reset_accumulation(self, width, height):
+        _check(self.lib.bte_reset_accumulation(int(width), int(height)))
+
+    def render(self, width, height):
+        _check(self.lib.bte_render(int(width), int(height)))
+
+    def set_output_buffer(self, device_ptr: int):
+        _check(self.lib.bte_set_output_buffer(C.c_void_p(device_ptr)))
+
+    def set_render_mode(self, mode: int):
+        _check(self.lib.bte_set_render_mode(int(mode)))
+
+    def get_render_mode(self) -> int:
+        return int(self.lib.bte_get_render_mode())
+
+    def toggle_denoiser(self) -> bool:
+        return bool(_check(self.lib.bte_toggle_denoiser()))
+
+    def cleanup(self):
+        _check(self.lib.bte_cleanup())
+
+    def stats(self) -> FrameStats:
+        s = FrameStats()
+        _check(self.lib.bte_get_frame_stats(C.byref(s)))
+        return s
+
+    def set_stage_timing(self, on: bool):
+        _check(self.lib.bte_set_stage_timing(1 if on else 0))
+
+    def set_hit_log(self, on: bool):
+        _check(self.lib.bte_set_hit_log(1 if on else 0))
+
+    def frame_index(self) -> int:
+        v = C.c_uint32()
+        _check(self.lib.bte_get_frame_index(C.byref(v)))
+        return int(v.value)
+
+    def set_frame_index(self, i: int):
+        _check(self.lib.bte_set_frame_index(C.c_uint32(i)))
+
+    def read_framebuffer(self, width, height) -> np.ndarray:
+        out = np.empty(width * height, dtype=np.uint32)
+        _check(self.lib.bte_read_framebuffer(_ptr(out)))
+        return out
+
+    def read_accum(self, width, height) -> np.ndarray:
+        out = np.empty((width * height, 3), dtype=np.float32)
+        _check(self.lib.bte_read_accum(_ptr(out)))
+        return out
+
+    def read_accum_f64(self, width, height) -> np.ndarray:
+        out = np.empty((width * height, 3), dtype=np.float64)
+        _check(self.lib.bte_read_accum_f64(_ptr(out)))
+        return out
+
+    def read_sample_radiance(self, count: int) -> np.ndarray:
+        out = np.empty((count, 3), dtype=np.float32)
+        _check(self.lib.bte_read_sample_radiance(_ptr(out), int(count)))
+        return out
+
+    def read_hit_log(self, count: int) -> np.ndarray:
+        out = np.empty(count, dtype=np.int32)
+        _check(self.lib.bte_read_hit_log(_ptr(out), int(count)))
+        return out
+
+    # ---- parity probes ----
+    def trace_closest(self, rays: np.ndarray):
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = len(r)
+        tri = np.empty(n, dtype=np.int32)
+        tuv = np.empty((n, 3), dtype=np.float32)
+        _check(self.lib.bte_trace_closest(_ptr(r), n, _ptr(tri), _ptr(tuv)))
+        return tri, tuv
+
+    def trace_occluded(self, rays: np.ndarray, tmax: np.ndarray):
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        t = np.ascontiguousarray(tmax, dtype=np.float32)
+        out = np.empty(len(r), dtype=np.uint8)
+        _check(self.lib.bte_trace_occluded(_ptr(r), len(r), _ptr(t), _ptr(out)))
+        return out
+
+    def env_query(self, op: int, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n = len(x)
+        width = {0: 3, 1: 1, 2: 7}[op]
+        out = np.empty((n, width), dtype=np.float32)
+        _check(self.lib.bte_env_query(int(op), _ptr(x), n, _ptr(out)))
+        return out
+
+    def env_tables(self, w, h):
+        marg = np.empty(h + 1, dtype=np.float32)
+        cond = np.empty(h * (w + 1), dtype=np.float32)
+        tp = C.c_float()
+        _check(self.lib.bte_env_tables(_ptr(marg), _ptr(cond), C.byref(tp)))
+        return marg, cond, float(tp.value)
+
+    def env_alias_tables(self, w, h):
+        rp = np.empty(h, dtype=np.float32)
+        ri = np.empty(h, dtype=np.int32)
+        cp = np.empty(h * w, dtype=np.float32)
+        ci = np.empty(h * w, dtype=np.int32)
+        pp = np.empty(h * w, dtype=np.float32)
+        _check(self.lib.bte_env_alias_tables(_ptr(rp), _ptr(ri), _ptr(cp), _ptr(ci), _ptr(pp)))
+        return rp, ri, cp, ci, pp
+
+    def math_eval(self, fn: int, a: np.ndarray, b: Optional[np.ndarray] = None) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        bb = None if b is None else np.ascontiguousarray(b, dtype=np.float32)
+        out = np.empty_like(a)
+        _check(self.lib.bte_math_eval(int(fn), _ptr(a), _ptr(bb), _ptr(out), len(a)))
+        return out
+
+    def bsdf_query(self, bsdf, op: int, wi: np.ndarray, x: np.ndarray) -> np.ndarray:
+        b = np.ascontiguousarray(np.asarray(bsdf, dtype=BSDF_DTYPE).reshape(1))
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n = len(wi)
+        width = {0: 3, 1: 1, 2: 8}[op]
+        out = np.empty((n, width), dtype=np.float32)
+        _check(self.lib.bte_bsdf_query(_ptr(b), int(op), _ptr(wi), _ptr(x), n, _ptr(out)))
+        return out
+
+    def tex_hw_vs_sw(self, texels: np.ndarray, wrap_v: bool, uv: np.ndarray):
+        t = np.ascontiguousarray(texels, dtype=np.float32)
+        h, w = t.shape[0], t.shape[1]
+        uv = np.ascontiguousarray(uv, dtype=np.float32)
+        n = len(uv)
+        hw = np.empty((n, 4), dtype=np.float32)
+        sw = np.empty((n, 4), dtype=np.float32)
+        _check(self.lib.bte_tex_hw_vs_sw(_ptr(t), w, h, 1 if wrap_v else 0, _ptr(uv), n, _ptr(hw), _ptr(sw)))
+        return hw, sw

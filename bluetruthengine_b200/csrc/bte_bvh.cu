@@ -1,0 +1,381 @@
+// bte_bvh.cu -- LBVH construction on the GPU (replaces the OptiX GAS build,
+// src/host/optix_setup.cu:215-292).
+//
+//   1. per-triangle bounds and centroids; scene centroid bounds (order-free
+//      min/max reduction through monotone integer encodings)
+//   2. 63-bit Morton codes (21 bits per axis)
+//   3. stable LSD radix sort of (code, triangle) pairs, 4-bit digits
+//      (16 passes); ties keep ascending triangle order
+//   4. hierarchy from the sorted codes (T. Karras, "Maximizing Parallelism in
+//      the Construction of BVHs, Octrees, and k-d Trees", HPG 2012), equal
+//      codes separated by their index
+//   5. bottom-up refit with one atomic arrival counter per node
+//   6. output: 64-byte BVH2 nodes holding both child boxes, and the triangles
+//      in leaf order as three float4 each (v0|original index, v1, v2)
+// All integer steps are deterministic; the result does not depend on thread
+// scheduling.
+#include "bte_kernels.h"
+
+#include <cfloat>
+#include <vector>
+
+namespace bte {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kDigits = 16;
+
+__device__ __forceinline__ unsigned int floatToOrdered(float f)
+{
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float orderedToFloat(unsigned int u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void kTriPrep(const TriangleData* __restrict__ tris, int n, float4* cen, unsigned int* bounds)
+{
+    __shared__ unsigned int sLo[3], sHi[3];
+    if (threadIdx.x < 3) { sLo[threadIdx.x] = 0xffffffffu; sHi[threadIdx.x] = 0u; }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const TriangleData t = tris[i];
+        const float lx = fminf(t.v0.x, fminf(t.v1.x, t.v2.x)), hx = fmaxf(t.v0.x, fmaxf(t.v1.x, t.v2.x));
+        const float ly = fminf(t.v0.y, fminf(t.v1.y, t.v2.y)), hy = fmaxf(t.v0.y, fmaxf(t.v1.y, t.v2.y));
+        const float lz = fminf(t.v0.z, fminf(t.v1.z, t.v2.z)), hz = fmaxf(t.v0.z, fmaxf(t.v1.z, t.v2.z));
+        const float cx = 0.5f * (lx + hx), cy = 0.5f * (ly + hy), cz = 0.5f * (lz + hz);
+        cen[i] = make_float4(cx, cy, cz, 0.0f);
+        atomicMin(&sLo[0], floatToOrdered(cx)); atomicMax(&sHi[0], floatToOrdered(cx));
+        atomicMin(&sLo[1], floatToOrdered(cy)); atomicMax(&sHi[1], floatToOrdered(cy));
+        atomicMin(&sLo[2], floatToOrdered(cz)); atomicMax(&sHi[2], floatToOrdered(cz));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        atomicMin(&bounds[threadIdx.x], sLo[threadIdx.x]);
+        atomicMax(&bounds[3 + threadIdx.x], sHi[threadIdx.x]);
+    }
+}
+
+__device__ __forceinline__ unsigned long long spread21(unsigned int v)
+{
+    unsigned long long x = v & 0x1fffffu;
+    x = (x | (x << 32)) & 0x1f00000000ffffULL;
+    x = (x | (x << 16)) & 0x1f0000ff0000ffULL;
+    x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
+    x = (x | (x << 2)) & 0x1249249249249249ULL;
+    return x;
+}
+
+__global__ void kMorton(const float4* __restrict__ cen, int n, const unsigned int* bounds, unsigned long long* keys,
+                        int* vals)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float lo[3] = {orderedToFloat(bounds[0]), orderedToFloat(bounds[1]), orderedToFloat(bounds[2])};
+    const float hi[3] = {orderedToFloat(bounds[3]), orderedToFloat(bounds[4]), orderedToFloat(bounds[5])};
+    const float4 c = cen[i];
+    const float cc[3] = {c.x, c.y, c.z};
+    unsigned int q[3];
+    for (int k = 0; k < 3; ++k) {
+        const float ext = hi[k] - lo[k];
+        float f = (ext > 0.0f) ? (cc[k] - lo[k]) / ext : 0.0f;
+        f = fminf(fmaxf(f, 0.0f), 1.0f);
+        q[k] = min(static_cast<unsigned int>(f * 2097152.0f), 2097151u);
+    }
+    keys[i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+    vals[i] = i;
+}
+
+__global__ void kRadixHist(const unsigned long long* __restrict__ keys, int n, int shift, int numTiles, int* hist)
+{
+    __shared__ int cnt[kDigits];
+    if (threadIdx.x < kDigits) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+    for (int j = 0; j < kSortItems; ++j) {
+        const int i = base + j * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&cnt[static_cast<int>((keys[i] >> shift) & 0xf)], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kDigits) hist[threadIdx.x * numTiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// exclusive scan of hist[0..m) by one block
+__global__ void kScanSingle(int* data, int m)
+{
+    __shared__ int carry;
+    __shared__ int warpSums[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < m; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = (i < m) ? data[i] : 0;
+        int x = v;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = (lane < static_cast<int>(blockDim.x >> 5)) ? warpSums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warpSums[lane] = w;
+        }
+        __syncthreads();
+        const int warpPrefix = (warp > 0) ? warpSums[warp - 1] : 0;
+        const int incl = x + warpPrefix;
+        if (i < m) data[i] = carry + incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += incl;
+        __syncthreads();
+    }
+}
+
+// Stable scatter: element order within a tile is thread-major (thread t owns
+// items t*kSortItems .. +kSortItems-1 of the tile).
+__global__ void kRadixScatter(const unsigned long long* __restrict__ keysIn, const int* __restrict__ valsIn,
+                              unsigned long long* keysOut, int* valsOut, int n, int shift, int numTiles,
+                              const int* __restrict__ histScan)
+{
+    __shared__ int cnt[kDigits][kSortThreads + 1];
+    __shared__ int gbase[kDigits];
+    const int t = threadIdx.x;
+    const int tileBase = blockIdx.x * kSortTile + t * kSortItems;
+    unsigned long long k[kSortItems];
+    int v[kSortItems];
+    int dg[kSortItems];
+    for (int d = 0; d < kDigits; ++d) cnt[d][t] = 0;
+    for (int j = 0; j < kSortItems; ++j) {
+        const int i = tileBase + j;
+        if (i < n) {
+            k[j] = keysIn[i];
+            v[j] = valsIn[i];
+            dg[j] = static_cast<int>((k[j] >> shift) & 0xf);
+        } else {
+            dg[j] = -1;
+        }
+    }
+    for (int j = 0; j < kSortItems; ++j) if (dg[j] >= 0) cnt[dg[j]][t] += 1;
+    if (t < kDigits) gbase[t] = histScan[t * numTiles + blockIdx.x];
+    __syncthreads();
+    if (t < kDigits) {   // exclusive scan over threads for digit t
+        int run = 0;
+        for (int u = 0; u < kSortThreads; ++u) {
+            const int c = cnt[t][u];
+            cnt[t][u] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int j = 0; j < kSortItems; ++j) {
+        if (dg[j] < 0) continue;
+        int rank = 0;
+        for (int jj = 0; jj < j; ++jj) rank += (dg[jj] == dg[j]) ? 1 : 0;
+        const int pos = gbase[dg[j]] + cnt[dg[j]][t] + rank;
+        keysOut[pos] = k[j];
+        valsOut[pos] = v[j];
+    }
+}
+
+__device__ __forceinline__ int delta(const unsigned long long* keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    const unsigned long long a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz(static_cast<unsigned int>(i) ^ static_cast<unsigned int>(j));
+    return __clzll(a ^ b);
+}
+
+// internal node i in [0, n-2]; children encoded >= 0 internal, < 0 leaf ~k
+__global__ void kKarras(const unsigned long long* __restrict__ keys, int n, int2* children, int* parentInner,
+                        int* parentLeaf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int div = 2;
+    int t;
+    do {
+        t = (l + div - 1) / div;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        div *= 2;
+    } while (t > 1);
+    const int gamma = i + s * d + min(d, 0);
+    const int lo = min(i, j), hi = max(i, j);
+    int left, right;
+    if (lo == gamma) { left = ~gamma; parentLeaf[gamma] = i; }
+    else { left = gamma; parentInner[gamma] = i; }
+    if (hi == gamma + 1) { right = ~(gamma + 1); parentLeaf[gamma + 1] = i; }
+    else { right = gamma + 1; parentInner[gamma + 1] = i; }
+    children[i] = make_int2(left, right);
+    if (i == 0) parentInner[0] = -1;
+}
+
+struct Box { float lx, ly, lz, hx, hy, hz; };
+
+__device__ __forceinline__ Box triBox(const TriangleData& t)
+{
+    Box b;
+    b.lx = fminf(t.v0.x, fminf(t.v1.x, t.v2.x)); b.hx = fmaxf(t.v0.x, fmaxf(t.v1.x, t.v2.x));
+    b.ly = fminf(t.v0.y, fminf(t.v1.y, t.v2.y)); b.hy = fmaxf(t.v0.y, fmaxf(t.v1.y, t.v2.y));
+    b.lz = fminf(t.v0.z, fminf(t.v1.z, t.v2.z)); b.hz = fmaxf(t.v0.z, fmaxf(t.v1.z, t.v2.z));
+    return b;
+}
+
+// leaf k (sorted position) -> leaf triangle data + its box; walks up and
+// fills the inner nodes' boxes (second arrival computes the union).
+__global__ void kRefit(const TriangleData* __restrict__ tris, const int* __restrict__ sortedTri, int n,
+                       const int2* __restrict__ children, const int* __restrict__ parentInner,
+                       const int* __restrict__ parentLeaf, float4* leafTris, float* innerBox /*[n-1][6]*/,
+                       float* leafBox /*[n][6]*/, int* arrivals)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int ti = sortedTri[k];
+    const TriangleData t = tris[ti];
+    leafTris[3 * k] = make_float4(t.v0.x, t.v0.y, t.v0.z, __int_as_float(ti));
+    leafTris[3 * k + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
+    leafTris[3 * k + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
+    const Box b = triBox(t);
+    float* lb = leafBox + 6 * static_cast<size_t>(k);
+    lb[0] = b.lx; lb[1] = b.ly; lb[2] = b.lz; lb[3] = b.hx; lb[4] = b.hy; lb[5] = b.hz;
+    if (n < 2) return;
+    __threadfence();
+    int node = parentLeaf[k];
+    while (node >= 0) {
+        if (atomicAdd(&arrivals[node], 1) == 0) return;   // first arrival: sibling not ready
+        __threadfence();
+        const int2 c = children[node];
+        float a[6], bb[6];
+        const float* pa = (c.x >= 0) ? innerBox + 6 * static_cast<size_t>(c.x) : leafBox + 6 * static_cast<size_t>(~c.x);
+        const float* pb = (c.y >= 0) ? innerBox + 6 * static_cast<size_t>(c.y) : leafBox + 6 * static_cast<size_t>(~c.y);
+        for (int q = 0; q < 6; ++q) { a[q] = __ldcg(pa + q); bb[q] = __ldcg(pb + q); }
+        float* out = innerBox + 6 * static_cast<size_t>(node);
+        out[0] = fminf(a[0], bb[0]); out[1] = fminf(a[1], bb[1]); out[2] = fminf(a[2], bb[2]);
+        out[3] = fmaxf(a[3], bb[3]); out[4] = fmaxf(a[4], bb[4]); out[5] = fmaxf(a[5], bb[5]);
+        __threadfence();
+        node = parentInner[node];
+    }
+}
+
+__global__ void kEmitNodes(const int2* __restrict__ children, const float* __restrict__ innerBox,
+                           const float* __restrict__ leafBox, int n, BvhNode* nodes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int2 c = children[i];
+    const float* a = (c.x >= 0) ? innerBox + 6 * static_cast<size_t>(c.x) : leafBox + 6 * static_cast<size_t>(~c.x);
+    const float* b = (c.y >= 0) ? innerBox + 6 * static_cast<size_t>(c.y) : leafBox + 6 * static_cast<size_t>(~c.y);
+    BvhNode nd;
+    nd.lxy = make_float4(a[0], a[3], a[1], a[4]);
+    nd.rxy = make_float4(b[0], b[3], b[1], b[4]);
+    nd.z = make_float4(a[2], a[5], b[2], b[5]);
+    // leaf children hold one triangle: ~(start | (1-1) << 25) == ~start
+    nd.child = make_int4(c.x, c.y, 0, 0);
+    nodes[i] = nd;
+}
+
+}  // namespace
+
+#define BVH_CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { err = std::string("LBVH build: ") + cudaGetErrorString(e_); goto fail; } } while (0)
+
+int buildLbvh(const TriangleData* dTris, int n, BvhBuildResult& out, cudaStream_t st, std::string& err)
+{
+    out = BvhBuildResult{};
+    if (n <= 0) return 0;
+    if (n > kLeafStartMask) { err = "LBVH build: too many triangles for the leaf encoding"; return -1; }
+    float4* cen = nullptr;
+    unsigned int* bounds = nullptr;
+    unsigned long long *keysA = nullptr, *keysB = nullptr;
+    int *valsA = nullptr, *valsB = nullptr, *hist = nullptr;
+    int2* children = nullptr;
+    int *parentInner = nullptr, *parentLeaf = nullptr, *arrivals = nullptr;
+    float *innerBox = nullptr, *leafBox = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const int numTiles = (n + kSortTile - 1) / kSortTile;
+    const int inner = n > 1 ? n - 1 : 1;
+    {
+        BVH_CK(cudaEventCreate(&e0));
+        BVH_CK(cudaEventCreate(&e1));
+        BVH_CK(cudaEventRecord(e0, st));
+        BVH_CK(cudaMalloc(&cen, sizeof(float4) * n));
+        BVH_CK(cudaMalloc(&bounds, sizeof(unsigned int) * 6));
+        BVH_CK(cudaMalloc(&keysA, sizeof(unsigned long long) * n));
+        BVH_CK(cudaMalloc(&keysB, sizeof(unsigned long long) * n));
+        BVH_CK(cudaMalloc(&valsA, sizeof(int) * n));
+        BVH_CK(cudaMalloc(&valsB, sizeof(int) * n));
+        BVH_CK(cudaMalloc(&hist, sizeof(int) * kDigits * numTiles));
+        BVH_CK(cudaMalloc(&children, sizeof(int2) * inner));
+        BVH_CK(cudaMalloc(&parentInner, sizeof(int) * inner));
+        BVH_CK(cudaMalloc(&parentLeaf, sizeof(int) * n));
+        BVH_CK(cudaMalloc(&arrivals, sizeof(int) * inner));
+        BVH_CK(cudaMalloc(&innerBox, sizeof(float) * 6 * inner));
+        BVH_CK(cudaMalloc(&leafBox, sizeof(float) * 6 * n));
+        BVH_CK(cudaMalloc(&out.leafTris, sizeof(float4) * 3 * static_cast<size_t>(n)));
+        BVH_CK(cudaMalloc(&out.nodes, sizeof(BvhNode) * inner));
+        {
+            const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+            BVH_CK(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st));
+        }
+        BVH_CK(cudaMemsetAsync(arrivals, 0, sizeof(int) * inner, st));
+        const int B = 256, G = (n + B - 1) / B;
+        kTriPrep<<<G, B, 0, st>>>(dTris, n, cen, bounds);
+        kMorton<<<G, B, 0, st>>>(cen, n, bounds, keysA, valsA);
+        unsigned long long *kin = keysA, *kout = keysB;
+        int *vin = valsA, *vout = valsB;
+        for (int shift = 0; shift < 64; shift += 4) {
+            kRadixHist<<<numTiles, kSortThreads, 0, st>>>(kin, n, shift, numTiles, hist);
+            kScanSingle<<<1, 1024, 0, st>>>(hist, kDigits * numTiles);
+            kRadixScatter<<<numTiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, numTiles, hist);
+            unsigned long long* tk = kin; kin = kout; kout = tk;
+            int* tv = vin; vin = vout; vout = tv;
+        }
+        if (n > 1) {
+            kKarras<<<(n - 1 + B - 1) / B, B, 0, st>>>(kin, n, children, parentInner, parentLeaf);
+        }
+        kRefit<<<G, B, 0, st>>>(dTris, vin, n, children, parentInner, parentLeaf, out.leafTris, innerBox, leafBox, arrivals);
+        if (n > 1) kEmitNodes<<<(n - 1 + B - 1) / B, B, 0, st>>>(children, innerBox, leafBox, n, out.nodes);
+        BVH_CK(cudaGetLastError());
+        BVH_CK(cudaEventRecord(e1, st));
+        BVH_CK(cudaEventSynchronize(e1));
+        BVH_CK(cudaEventElapsedTime(&out.msBuild, e0, e1));
+        out.nodeCount = n > 1 ? n - 1 : 0;
+        out.rootIsLeaf = n == 1 ? 1 : 0;
+    }
+    cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
+    cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
+    cudaFree(leafBox);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    return 0;
+fail:
+    cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
+    cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
+    cudaFree(leafBox);
+    cudaFree(out.leafTris); cudaFree(out.nodes);
+    out = BvhBuildResult{};
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return -1;
+}
+
+}  // namespace bte

@@ -1,0 +1,423 @@
+// bte_kernels.cu -- wavefront stage kernels (sm_100a).
+//
+//   generate -> [extend -> shade -> connect] x maxDepth -> present
+//
+// One frame is a fixed launch sequence with no host round trip: every stage
+// reads its work count from a per-bounce device counter, so the sequence can
+// be replayed as a CUDA graph.  This replaces the reference's host-driven
+// loop (src/host/wavefront_host.cu:155-236), which copies counters to the
+// host and synchronises several times per bounce.
+//
+// Path state is structure-of-arrays with 16-byte records (one 128-bit load or
+// store per field) instead of the reference's 12-byte Float3 arrays
+// (include/wavefront/wavefront_buffers.h:40-90).  Queue appends are
+// warp-aggregated (one atomic per coalesced group).  NEE shadow rays live in
+// fixed per-path slots (area, spotlights, env); connect clears the visibility
+// bit of occluded slots and the next shade (or present) adds the surviving
+// contributions in the reference's megakernel order, which makes the result
+// deterministic where the reference races float atomicAdds
+// (src/wavefront/ray_connect.cu:67-69).
+#include "bte_kernels.h"
+#include "bte_shade.cuh"
+#include "bte_trace.cuh"
+
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+namespace bte {
+
+namespace {
+
+BTE_DI int appendCoalesced(int* counter)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, static_cast<int>(g.size()));
+    base = g.shfl(base, 0);
+    return base + static_cast<int>(g.thread_rank());
+}
+
+BTE_DI V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
+
+// Adds the contributions of the visible NEE slots in slot order and clears the mask.
+BTE_DI V3 resolveShadows(const DevPaths& P, int idx, V3 L)
+{
+    const uint32_t mask = P.shMask[idx];
+    if (mask != 0u) {
+        for (int s = 0; s < P.slots; ++s) {
+            if (mask & (1u << s)) {
+                const float4 c = P.shContrib[static_cast<size_t>(idx) * P.slots + s];
+                L = add3(L, v3(c.x, c.y, c.z));
+            }
+        }
+        P.shMask[idx] = 0u;
+    }
+    return L;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- generate
+// src/wavefront/ray_generate.cu:42-80.  Path i covers pixel i % (W*H) and
+// sample frameIndex + i / (W*H).
+__global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) P.rayCount[0] = P.count;
+    if (i >= P.count) return;
+    const int wh = f.width * f.height;
+    const int pix = i % wh;
+    const int s = i / wh;
+    const int px = pix % f.width, py = pix / f.width;
+    uint32_t rng = rngSeed(static_cast<uint32_t>(pix), f.frameIndex + static_cast<uint32_t>(s));
+    const float jx = rngNext(rng) - 0.5f;
+    const float jy = rngNext(rng) - 0.5f;
+    V3 o, d;
+    primaryRay(px, py, f.width, f.height, f.cam, f.tanHalf, jx, jy, o, d);
+    P.o[i] = make_float4(o.x, o.y, o.z, __uint_as_float(rng));
+    P.d[i] = make_float4(d.x, d.y, d.z, 1.0f);
+    P.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    P.L[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(1u << 16));
+    P.queue[0][i] = i;
+    P.shMask[i] = 0u;
+}
+
+// ---------------------------------------------------------------- extend
+// src/wavefront/ray_extend.cu:49-72 with src/optix_programs.cu:110-148 moved
+// to shade (the hit record is t, u, v, triangle).
+__global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounce)
+{
+    const int count = P.rayCount[bounce];
+    const int* __restrict__ q = P.queue[bounce & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += stride) {
+        const int idx = q[slot];
+        const float4 o = P.o[idx];
+        const float4 d = P.d[idx];
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z);
+        float t = 0.0f, u = 0.0f, v = 0.0f;
+        const int tri = traceClosest(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
+        P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
+        if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
+    }
+}
+
+// ---------------------------------------------------------------- shade
+// src/wavefront/ray_shade.cu:103-183 (rt_optix_shading.cuh:412-447 order).
+__global__ void __launch_bounds__(256) kShade(DevScene s, DevPaths P, FrameParams f, int bounce)
+{
+    const int count = P.rayCount[bounce];
+    const int* __restrict__ q = P.queue[bounce & 1];
+    int* qn = P.queue[(bounce + 1) & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += stride) {
+        const int idx = q[slot];
+        const float4 o4 = P.o[idx], d4 = P.d[idx], tp4 = P.tp[idx], L4 = P.L[idx];
+        uint32_t rng = __float_as_uint(o4.w);
+        PathReg p;
+        p.o = xyz(o4); p.d = xyz(d4); p.tp = xyz(tp4); p.L = xyz(L4);
+        p.eta = d4.w;
+        p.brdfPdf = tp4.w;
+        const uint32_t bits = __float_as_uint(L4.w);
+        p.bounce = static_cast<int>(bits & 0xffffu);
+        p.specular = ((bits >> 16) & 1u) != 0u;
+
+        p.L = resolveShadows(P, idx, p.L);
+
+        const float4 hv = P.hit[idx];
+        const int tri = __float_as_int(hv.w);
+        if (tri < 0) {
+            accumulateEnvHit(s, p);
+            P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z, L4.w);
+            continue;
+        }
+        // closest-hit attributes, src/optix_programs.cu:121-140
+        HitReg h;
+        h.tri = tri;
+        {
+            const float t = hv.x, u = hv.y, v = hv.z;
+            const float w0 = 1.0f - u - v;
+            const TriangleData& T = s.tris[tri];
+            h.p = v3(p.o.x + t * p.d.x, p.o.y + t * p.d.y, p.o.z + t * p.d.z);
+            h.n = normalize3(v3(w0 * T.n0.x + u * T.n1.x + v * T.n2.x, w0 * T.n0.y + u * T.n1.y + v * T.n2.y,
+                                w0 * T.n0.z + u * T.n1.z + v * T.n2.z));
+            h.u = w0 * T.uv0.x + u * T.uv1.x + v * T.uv2.x;
+            h.v = w0 * T.uv0.y + u * T.uv1.y + v * T.uv2.y;
+        }
+        const Bsdf b = loadBsdf(s, tri, h.u, h.v);
+        if (s.emitterFlags[tri] != 0) accumulateEmitterHit(s, p, h);
+
+        const Frame fr = makeFrame(h.n);
+        const V3 wiLocal = toLocal(fr, mul3(p.d, -1.0f));
+        if (bsdfIsDiffuseClass(b.type)) {
+            p.specular = false;
+            uint32_t newMask = 0u;
+            ShadowRec sr;
+            const size_t base = static_cast<size_t>(idx) * P.slots;
+            if (prepareArea(s, p, rng, h, b, wiLocal, fr, sr)) {
+                P.shDir[base] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
+                P.shContrib[base] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
+                newMask |= 1u;
+                P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base);
+            }
+            for (int si = 0; si < s.spotCount; ++si) {
+                if (prepareSpot(s, p, h, b, si, wiLocal, fr, sr)) {
+                    P.shDir[base + 1 + si] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
+                    P.shContrib[base + 1 + si] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
+                    newMask |= 1u << (1 + si);
+                    P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base + 1 + si);
+                }
+            }
+            if (prepareEnv(s, p, rng, h, b, wiLocal, fr, sr)) {
+                const int es = P.slots - 1;
+                P.shDir[base + es] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
+                P.shContrib[base + es] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
+                newMask |= 1u << es;
+                P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base + es);
+            }
+            if (newMask != 0u) {
+                P.shOrigin[idx] = make_float4(h.p.x, h.p.y, h.p.z, 0.0f);
+                P.shMask[idx] = newMask;
+            }
+        } else {
+            p.specular = true;
+        }
+        scatter(p, rng, h, b, wiLocal, fr);
+        const bool alive = roulette(p, rng, f.rrStart);
+        if (alive) p.bounce++;
+        P.o[idx] = make_float4(p.o.x, p.o.y, p.o.z, __uint_as_float(rng));
+        P.d[idx] = make_float4(p.d.x, p.d.y, p.d.z, p.eta);
+        P.tp[idx] = make_float4(p.tp.x, p.tp.y, p.tp.z, p.brdfPdf);
+        P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z,
+                               __uint_as_float(static_cast<uint32_t>(p.bounce) | (p.specular ? (1u << 16) : 0u)));
+        if (alive && bounce + 1 < P.maxDepth) qn[appendCoalesced(P.rayCount + bounce + 1)] = idx;
+    }
+}
+
+// ---------------------------------------------------------------- connect
+// src/wavefront/ray_connect.cu:52-72: occlusion in (1e-4, tMax); an occluded
+// slot loses its visibility bit.
+__global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int bounce)
+{
+    const int count = P.shadowCount[bounce];
+    const int stride = gridDim.x * blockDim.x;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += stride) {
+        const int e = P.shadowQueue[k];
+        const int path = e / P.slots;
+        const int slot = e - path * P.slots;
+        const float4 o = P.shOrigin[path];
+        const float4 d = P.shDir[e];
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z);
+        if (traceOccluded(s, r, kEps, d.w, P.errorFlags)) atomicAnd(P.shMask + path, ~(1u << slot));
+    }
+}
+
+// ---------------------------------------------------------------- present
+// src/wavefront/ray_present.cu:43-62 for spp consecutive samples per pixel:
+// FP32 Welford mean (rt_path_integrator.cuh:72-87) in sample order, an FP64
+// running sum, and the gamma-2.2 RGBA8 pack (:93-105).
+__global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float* accum, double* accumD,
+                                                uint32_t* framebuffer, uint32_t* extFramebuffer)
+{
+    const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int wh = f.width * f.height;
+    if (pix >= wh) return;
+    float ax = accum[3 * pix], ay = accum[3 * pix + 1], az = accum[3 * pix + 2];
+    double sx = accumD[3 * pix], sy = accumD[3 * pix + 1], sz = accumD[3 * pix + 2];
+    for (int s = 0; s < f.spp; ++s) {
+        const int idx = s * wh + pix;
+        const float4 L4 = P.L[idx];
+        V3 L = resolveShadows(P, idx, v3(L4.x, L4.y, L4.z));
+        P.L[idx] = make_float4(L.x, L.y, L.z, L4.w);
+        const float n = static_cast<float>(f.frameIndex + static_cast<uint32_t>(s) + 1u);
+        ax = ax + (L.x - ax) / n;
+        ay = ay + (L.y - ay) / n;
+        az = az + (L.z - az) / n;
+        sx += static_cast<double>(L.x);
+        sy += static_cast<double>(L.y);
+        sz += static_cast<double>(L.z);
+    }
+    accum[3 * pix] = ax; accum[3 * pix + 1] = ay; accum[3 * pix + 2] = az;
+    accumD[3 * pix] = sx; accumD[3 * pix + 1] = sy; accumD[3 * pix + 2] = sz;
+    const uint32_t px = packGamma(ax, ay, az);
+    framebuffer[pix] = px;
+    if (extFramebuffer) extFramebuffer[pix] = px;
+}
+
+// ---------------------------------------------------------------- debug / parity kernels
+__global__ void kTraceClosestRays(DevScene s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* r6 = rays + 6 * static_cast<size_t>(i);
+    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5]);
+    float t = 0.0f, u = 0.0f, v = 0.0f;
+    const int tri = traceClosest(s, r, kEps, 1e30f, t, u, v, err);
+    outTri[i] = tri;
+    outTuv[3 * i] = t; outTuv[3 * i + 1] = u; outTuv[3 * i + 2] = v;
+}
+
+__global__ void kTraceOccludedRays(DevScene s, const float* rays, const float* tmax, int n, uint8_t* out, unsigned int* err)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* r6 = rays + 6 * static_cast<size_t>(i);
+    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5]);
+    out[i] = traceOccluded(s, r, kEps, tmax[i], err) ? 1 : 0;
+}
+
+__global__ void kEnvQuery(DevScene s, int op, const float* in, int n, float* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (op == 0) {
+        const V3 r = envEval(s.env, v3(in[3 * i], in[3 * i + 1], in[3 * i + 2]));
+        out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
+    } else if (op == 1) {
+        out[i] = envPdf(s.env, v3(in[3 * i], in[3 * i + 1], in[3 * i + 2]));
+    } else {
+        const EnvSample e = envSample(s.env, in[2 * i], in[2 * i + 1]);
+        float* o = out + 7 * static_cast<size_t>(i);
+        o[0] = e.dir.x; o[1] = e.dir.y; o[2] = e.dir.z; o[3] = e.pdf; o[4] = e.rad.x; o[5] = e.rad.y; o[6] = e.rad.z;
+    }
+}
+
+__global__ void kMathEval(int fn, const float* a, const float* b, float* out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float r;
+    switch (fn) {
+    case 0: r = m::sinf_(a[i]); break;
+    case 1: r = m::cosf_(a[i]); break;
+    case 2: r = m::tanf_(a[i]); break;
+    case 3: r = m::expf_(a[i]); break;
+    case 4: r = m::logf_(a[i]); break;
+    case 5: r = m::powf_(a[i], b[i]); break;
+    case 6: r = m::atan2f_(a[i], b[i]); break;
+    case 7: r = m::acosf_(a[i]); break;
+    // CUDA's own functions, for the accuracy comparison of the deterministic set
+    case 100: r = sinf(a[i]); break;
+    case 101: r = cosf(a[i]); break;
+    case 102: r = tanf(a[i]); break;
+    case 103: r = expf(a[i]); break;
+    case 104: r = logf(a[i]); break;
+    case 105: r = powf(a[i], b[i]); break;
+    case 106: r = atan2f(a[i], b[i]); break;
+    case 107: r = acosf(a[i]); break;
+    default: r = NAN; break;
+    }
+    out[i] = r;
+}
+
+// op 0: eval(wi, wo) -> 3; op 1: pdf(wi, wo) -> 1; op 2: sample(wi, u[3]) -> wo 3, weight 3, pdf 1, eta 1
+__global__ void kBsdfQuery(BsdfData g, int op, const float* wi, const float* x, int n, float* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Bsdf b;
+    b.type = g.type;
+    b.p0 = make_float4(g.p0.x, g.p0.y, g.p0.z, g.p0.w);
+    b.p1 = make_float4(g.p1.x, g.p1.y, g.p1.z, g.p1.w);
+    b.p2 = make_float4(g.p2.x, g.p2.y, g.p2.z, g.p2.w);
+    b.p3 = make_float4(g.p3.x, g.p3.y, g.p3.z, g.p3.w);
+    BRec r = brec0();
+    r.wi = v3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+    if (op == 0 || op == 1) {
+        r.wo = v3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+        r.measure = kSolid;
+        if (op == 0) {
+            const V3 v = bsdfEval(b, r);
+            out[3 * i] = v.x; out[3 * i + 1] = v.y; out[3 * i + 2] = v.z;
+        } else {
+            out[i] = bsdfPdf(b, r);
+        }
+    } else {
+        r.rndExtra = x[3 * i];
+        const V3 w = bsdfSample(b, r, x[3 * i + 1], x[3 * i + 2]);
+        float* o = out + 8 * static_cast<size_t>(i);
+        o[0] = r.wo.x; o[1] = r.wo.y; o[2] = r.wo.z;
+        o[3] = w.x; o[4] = w.y; o[5] = w.z;
+        o[6] = bsdfPdf(b, r);
+        o[7] = r.eta;
+    }
+}
+
+__global__ void kTexCompare(cudaTextureObject_t tex, const float4* texels, int w, int h, int wrapV, const float* uv, int n,
+                            float* outHw, float* outSw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float u = uv[2 * i], v = uv[2 * i + 1];
+    const float4 a = tex2D<float4>(tex, u, v);
+    const float4 b = texFloat4(texels, w, h, wrapV != 0, u, v);
+    outHw[4 * i] = a.x; outHw[4 * i + 1] = a.y; outHw[4 * i + 2] = a.z; outHw[4 * i + 3] = a.w;
+    outSw[4 * i] = b.x; outSw[4 * i + 1] = b.y; outSw[4 * i + 2] = b.z; outSw[4 * i + 3] = b.w;
+}
+
+// ---------------------------------------------------------------- launchers
+void launchGenerate(const DevPaths& P, const FrameParams& f, cudaStream_t st)
+{
+    const int blocks = (P.count + 255) / 256;
+    kGenerate<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, f);
+}
+void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
+{
+    kExtend<<<grid, block, 0, st>>>(s, P, bounce);
+}
+void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block, cudaStream_t st)
+{
+    kShade<<<grid, block, 0, st>>>(s, P, f, bounce);
+}
+void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
+{
+    kConnect<<<grid, block, 0, st>>>(s, P, bounce);
+}
+void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
+                   cudaStream_t st)
+{
+    const int wh = f.width * f.height;
+    kPresent<<<(wh + 255) / 256, 256, 0, st>>>(P, f, accum, accumD, fb, extFb);
+}
+void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
+                            cudaStream_t st)
+{
+    kTraceClosestRays<<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
+}
+void launchTraceOccludedRays(const DevScene& s, const float* rays, const float* tmax, int n, uint8_t* out, unsigned int* err,
+                             cudaStream_t st)
+{
+    kTraceOccludedRays<<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
+}
+void launchEnvQuery(const DevScene& s, int op, const float* in, int n, float* out, cudaStream_t st)
+{
+    kEnvQuery<<<(n + 127) / 128, 128, 0, st>>>(s, op, in, n, out);
+}
+void launchMathEval(int fn, const float* a, const float* b, float* out, int n, cudaStream_t st)
+{
+    kMathEval<<<(n + 255) / 256, 256, 0, st>>>(fn, a, b, out, n);
+}
+void launchBsdfQuery(const BsdfData& g, int op, const float* wi, const float* x, int n, float* out, cudaStream_t st)
+{
+    kBsdfQuery<<<(n + 127) / 128, 128, 0, st>>>(g, op, wi, x, n, out);
+}
+void launchTexCompare(cudaTextureObject_t tex, const float4* texels, int w, int h, int wrapV, const float* uv, int n,
+                      float* outHw, float* outSw, cudaStream_t st)
+{
+    kTexCompare<<<(n + 127) / 128, 128, 0, st>>>(tex, texels, w, h, wrapV, uv, n, outHw, outSw);
+}
+
+int occupancyGrid(int which, int block)
+{
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = which == 0 ? reinterpret_cast<const void*>(kExtend)
+                   : which == 1 ? reinterpret_cast<const void*>(kShade)
+                                : reinterpret_cast<const void*>(kConnect);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0) != cudaSuccess || per < 1) per = 1;
+    return sms * per;
+}
+
+}  // namespace bte

@@ -1,0 +1,45 @@
+// bte_kernels.h -- host-side launchers of the device code (bte_kernels.cu,
+// bte_bvh.cu, bte_env.cu).
+#pragma once
+
+#include "bte_types.cuh"
+
+#include <string>
+
+namespace bte {
+
+void launchGenerate(const DevPaths& P, const FrameParams& f, cudaStream_t st);
+void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
+void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block, cudaStream_t st);
+void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
+void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
+                   cudaStream_t st);
+void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
+                            cudaStream_t st);
+void launchTraceOccludedRays(const DevScene& s, const float* rays, const float* tmax, int n, uint8_t* out,
+                             unsigned int* err, cudaStream_t st);
+void launchEnvQuery(const DevScene& s, int op, const float* in, int n, float* out, cudaStream_t st);
+void launchMathEval(int fn, const float* a, const float* b, float* out, int n, cudaStream_t st);
+void launchBsdfQuery(const BsdfData& g, int op, const float* wi, const float* x, int n, float* out, cudaStream_t st);
+void launchTexCompare(cudaTextureObject_t tex, const float4* texels, int w, int h, int wrapV, const float* uv, int n,
+                      float* outHw, float* outSw, cudaStream_t st);
+int occupancyGrid(int which, int block);
+
+// LBVH build over device triangles (bte_bvh.cu).  Allocates `nodes` and
+// `leafTris`; the caller frees them.  Returns 0 or a CUDA error code.
+struct BvhBuildResult {
+    BvhNode* nodes = nullptr;
+    float4* leafTris = nullptr;
+    int nodeCount = 0;
+    int rootIsLeaf = 0;
+    float msBuild = 0.0f;
+};
+int buildLbvh(const TriangleData* dTris, int triCount, BvhBuildResult& out, cudaStream_t st, std::string& err);
+
+// Env-map tables (bte_env.cu).
+int buildEnvCdf(const float4* dTexels, int w, int h, const float* hSinTheta, float* dMarginal, float* dConditional,
+                cudaStream_t st, std::string& err);
+int buildEnvAlias(const float4* dTexels, int w, int h, float* dRowProb, int* dRowAlias, float* dColProb, int* dColAlias,
+                  float* dPixelPdf, double* hTotal, cudaStream_t st, std::string& err);
+
+}  // namespace bte

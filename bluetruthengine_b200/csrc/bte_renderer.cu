@@ -1,0 +1,910 @@
+// bte_renderer.cu -- renderer state and the C-ABI entry points.
+//
+// Host orchestration of the reference (src/render_kernel.cu,
+// src/host/scene_upload.cu, src/host/wavefront_host.cu,
+// src/host/renderer_state.*) restated for one B200: one process-wide renderer
+// state (the reference's s_* globals), one stream, device-resident uploads,
+// an LBVH instead of the OptiX GAS, and a frame that is a fixed,
+// host-synchronisation-free launch sequence.  Every entry point returns a
+// status and records a message for bte_last_error() instead of exiting.
+#include "bte_internal.h"
+#include "bte_kernels.h"
+#include "bte_math.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace bte {
+
+namespace {
+
+thread_local std::string g_lastError;
+
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct CudaError {
+    std::string msg;
+};
+
+inline void ck(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw CudaError{std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+void upload(DeviceBuffer& b, const void* src, size_t bytes, cudaStream_t st)
+{
+    b.release();
+    if (!src || bytes == 0) return;
+    ck(cudaMalloc(&b.p, bytes), "cudaMalloc");
+    b.bytes = bytes;
+    ck(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync H2D");
+}
+
+void ensure(DeviceBuffer& b, size_t bytes)
+{
+    if (b.p && b.bytes >= bytes) return;
+    b.release();
+    if (bytes == 0) return;
+    ck(cudaMalloc(&b.p, bytes), "cudaMalloc");
+    b.bytes = bytes;
+}
+
+struct Renderer {
+    bool init = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t stageEv[8] = {};
+
+    // scene (src/host/renderer_state.h:30-169)
+    DeviceBuffer tris, materials, triMatIds, emission, emitterFlags, triEmitter, emitters, emitterTriIndices,
+        emitterTriCdf, sceneEmitterCdf, bsdfs, triBsdfIds, spots;
+    int triCount = 0, materialCount = 0, emitterCount = 0, bsdfCount = 0, spotCount = 0;
+    bool hasEmission = false, hasFlags = false;
+    std::vector<int> hostEmitterTriIndices;
+    std::vector<EmitterData> hostEmitters;
+    // textures
+    std::vector<DeviceBuffer> tex, texMr;
+    DeviceBuffer texTable, texTableMr;
+    int textureCount = 0;
+    bool hasMr = false;
+    // env map
+    DeviceBuffer envTexels, envMarginal, envConditional, envRowProb, envRowAlias, envColProb, envColAlias, envPixelPdf;
+    int envW = 0, envH = 0;
+    float envIntensity = 0.0f, envRotation = 0.0f, envTotalPowerF = 0.0f;
+    double envTotalPowerD = 0.0;
+    bool hasEnv = false;
+    // acceleration structure
+    DeviceBuffer bvhNodes, leafTris;
+    int rootIsLeaf = 0;
+    bool accelReady = false;
+    float msBvh = 0.0f;
+    // camera / frame
+    CameraData camera{};
+    BteRenderConfig cfg{1, 200, 3, BTE_ENV_SAMPLING_CDF, 256, 0};
+    int renderMode = BTE_RENDER_WAVEFRONT;
+    bool denoiser = false;
+    uint32_t frameIndex = 0;
+    int accumW = 0, accumH = 0;
+    DeviceBuffer accum, accumD, framebuffer;
+    uint32_t* extFramebuffer = nullptr;
+    // wavefront buffers
+    DeviceBuffer pO, pD, pTp, pL, pHit, q0, q1, rayCount, shadowCount, shadowQueue, shOrigin, shDir, shContrib, shMask,
+        hitLog, errorFlags;
+    int pathCap = 0, slotCap = 0, depthCap = 0;
+    bool hitLogEnabled = false;
+    bool stageTiming = false;
+    int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
+    BteFrameStats stats{};
+    int gridExtend = 0, gridShade = 0, gridConnect = 0, gridBlock = 0;
+};
+
+Renderer g;
+std::mutex g_mutex;
+
+void ensureInit()
+{
+    if (g.init) return;
+    int n = 0;
+    ck(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+    if (n <= 0) throw CudaError{"no CUDA device"};
+    ck(cudaGetDevice(&g.device), "cudaGetDevice");
+    ck(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreate(&g.ev0), "cudaEventCreate");
+    ck(cudaEventCreate(&g.ev1), "cudaEventCreate");
+    for (auto& e : g.stageEv) ck(cudaEventCreate(&e), "cudaEventCreate");
+    g.init = true;
+}
+
+DevScene makeDevScene()
+{
+    DevScene s{};
+    s.tris = g.tris.as<TriangleData>();
+    s.triCount = g.accelReady ? g.triCount : 0;
+    s.leafTris = g.leafTris.as<float4>();
+    s.nodes = g.bvhNodes.as<BvhNode>();
+    s.rootIsLeaf = g.rootIsLeaf;
+    s.bsdfs = g.bsdfs.as<BsdfData>();
+    s.triBsdfIds = g.triBsdfIds.as<int>();
+    s.triMaterialIds = g.triMatIds.as<int>();
+    s.texTable = g.textureCount > 0 ? g.texTable.as<TexRef>() : nullptr;
+    s.texTableMr = (g.textureCount > 0 && g.hasMr) ? g.texTableMr.as<TexRef>() : nullptr;
+    s.textureCount = g.textureCount;
+    s.emitterFlags = g.emitterFlags.as<uint8_t>();
+    s.emission = g.emission.as<Float3>();
+    s.triEmitter = g.triEmitter.as<int>();
+    s.emitters = g.emitters.as<EmitterData>();
+    s.emitterCount = g.emitterCount;
+    s.emitterTriIndices = g.emitterTriIndices.as<int>();
+    s.emitterTriCdf = g.emitterTriCdf.as<float>();
+    s.sceneEmitterCdf = g.sceneEmitterCdf.as<float>();
+    s.spots = g.spots.as<SpotlightData>();
+    s.spotCount = g.spotCount;
+    s.hasEnv = g.hasEnv ? 1 : 0;
+    DevEnv& e = s.env;
+    e.texels = g.envTexels.as<float4>();
+    e.w = g.envW; e.h = g.envH;
+    e.intensity = g.envIntensity;
+    e.rotation = g.envRotation;
+    e.sampling = g.cfg.envSampling;
+    e.totalPower = (g.cfg.envSampling == BTE_ENV_SAMPLING_ALIAS) ? static_cast<float>(g.envTotalPowerD) : g.envTotalPowerF;
+    e.marginal = g.envMarginal.as<float>();
+    e.conditional = g.envConditional.as<float>();
+    e.rowProb = g.envRowProb.as<float>();
+    e.rowAlias = g.envRowAlias.as<int>();
+    e.colProb = g.envColProb.as<float>();
+    e.colAlias = g.envColAlias.as<int>();
+    e.pixelPdf = g.envPixelPdf.as<float>();
+    return s;
+}
+
+// The tri -> emitter side table: for each triangle the first emitter (in
+// emitter order) whose list holds it, as findEmitterIndexForTriangle
+// (include/rt_emitter_sampling.cuh:132-148) returns.
+void rebuildTriEmitter()
+{
+    g.triEmitter.release();
+    if (g.triCount <= 0 || g.emitterCount <= 0) return;
+    std::vector<int> t(static_cast<size_t>(g.triCount), -1);
+    for (int e = g.emitterCount - 1; e >= 0; --e) {
+        const EmitterData& E = g.hostEmitters[static_cast<size_t>(e)];
+        for (int j = 0; j < E.triCount; ++j) {
+            const size_t k = static_cast<size_t>(E.triIndexOffset) + static_cast<size_t>(j);
+            if (k >= g.hostEmitterTriIndices.size()) continue;
+            const int ti = g.hostEmitterTriIndices[k];
+            if (ti >= 0 && ti < g.triCount) t[static_cast<size_t>(ti)] = e;
+        }
+    }
+    upload(g.triEmitter, t.data(), t.size() * sizeof(int), g.stream);
+}
+
+void releaseWavefront()
+{
+    for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.shadowQueue,
+                            &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
+        b->release();
+    g.pathCap = g.slotCap = g.depthCap = 0;
+}
+
+void ensureWavefront(int paths, int slots, int depth)
+{
+    const bool grow = paths > g.pathCap || slots > g.slotCap || depth > g.depthCap;
+    if (!grow && (!g.hitLogEnabled || g.hitLog.p)) return;
+    if (grow) {
+        releaseWavefront();
+        const size_t P = static_cast<size_t>(paths), S = static_cast<size_t>(slots);
+        ensure(g.pO, P * 16); ensure(g.pD, P * 16); ensure(g.pTp, P * 16); ensure(g.pL, P * 16); ensure(g.pHit, P * 16);
+        ensure(g.q0, P * 4); ensure(g.q1, P * 4);
+        ensure(g.rayCount, sizeof(int) * (depth + 1));
+        ensure(g.shadowCount, sizeof(int) * (depth + 1));
+        ensure(g.shadowQueue, P * S * 4);
+        ensure(g.shOrigin, P * 16);
+        ensure(g.shDir, P * S * 16);
+        ensure(g.shContrib, P * S * 16);
+        ensure(g.shMask, P * 4);
+        ensure(g.errorFlags, 4);
+        g.pathCap = paths; g.slotCap = slots; g.depthCap = depth;
+    }
+    if (g.hitLogEnabled) ensure(g.hitLog, static_cast<size_t>(g.pathCap) * g.depthCap * 4);
+}
+
+void ensureAccum(int w, int h)
+{
+    const size_t n = static_cast<size_t>(w) * h;
+    if (g.accumW != w || g.accumH != h || !g.accum.p) {
+        g.accum.release(); g.accumD.release(); g.framebuffer.release();
+        ensure(g.accum, n * 12);
+        ensure(g.accumD, n * 24);
+        ensure(g.framebuffer, n * 4);
+        g.accumW = w; g.accumH = h;
+    }
+    ck(cudaMemsetAsync(g.accum.p, 0, n * 12, g.stream), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.accumD.p, 0, n * 24, g.stream), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.framebuffer.p, 0, n * 4, g.stream), "cudaMemsetAsync");
+    ck(cudaStreamSynchronize(g.stream), "cudaStreamSynchronize");
+    g.frameIndex = 0;
+}
+
+int slotsFor() { return 1 + g.spotCount + 1; }
+
+void renderFrame(int w, int h)
+{
+    if (w <= 0 || h <= 0) throw CudaError{"bte_render: image size must be positive"};
+    if (!g.tris.p || g.triCount <= 0) throw CudaError{"bte_render: no scene uploaded (bte_init_scene)"};
+    if (!g.accelReady) throw CudaError{"bte_render: acceleration structure missing (call bte_init_accel after bte_init_scene)"};
+    if (!g.bsdfs.p || !g.triBsdfIds.p) throw CudaError{"bte_render: no BSDFs uploaded (bte_init_bsdfs)"};
+    if (!g.emitterFlags.p) throw CudaError{"bte_render: emitter flags missing (bte_init_triangle_emitter_flags)"};
+    if (!g.accum.p || g.accumW != w || g.accumH != h) ensureAccum(w, h);   // render_kernel.cu:62-64
+    const int spp = g.cfg.samplesPerFrame > 0 ? g.cfg.samplesPerFrame : 1;
+    const int depth = g.cfg.maxDepth > 0 ? g.cfg.maxDepth : 1;
+    const long long paths64 = static_cast<long long>(w) * h * spp;
+    if (paths64 > (1LL << 30)) throw CudaError{"bte_render: too many paths per frame (W*H*spp > 2^30)"};
+    const int paths = static_cast<int>(paths64);
+    const int slots = slotsFor();
+    if (slots > 32) throw CudaError{"bte_render: at most 30 spotlights are supported"};
+    ensureWavefront(paths, slots, depth);
+    const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 256;
+    if (g.gridBlock != block) {
+        g.gridExtend = occupancyGrid(0, block);
+        g.gridShade = occupancyGrid(1, block);
+        g.gridConnect = occupancyGrid(2, block);
+        g.gridBlock = block;
+    }
+    DevPaths P{};
+    P.o = g.pO.as<float4>(); P.d = g.pD.as<float4>(); P.tp = g.pTp.as<float4>(); P.L = g.pL.as<float4>();
+    P.hit = g.pHit.as<float4>();
+    P.queue[0] = g.q0.as<int>(); P.queue[1] = g.q1.as<int>();
+    P.rayCount = g.rayCount.as<int>();
+    P.shadowCount = g.shadowCount.as<int>();
+    P.shadowQueue = g.shadowQueue.as<int>();
+    P.shOrigin = g.shOrigin.as<float4>();
+    P.shDir = g.shDir.as<float4>();
+    P.shContrib = g.shContrib.as<float4>();
+    P.shMask = g.shMask.as<uint32_t>();
+    P.hitLog = g.hitLogEnabled ? g.hitLog.as<int>() : nullptr;
+    P.slots = slots;
+    P.maxDepth = depth;
+    P.count = paths;
+    P.errorFlags = g.errorFlags.as<unsigned int>();
+    FrameParams f{};
+    f.width = w; f.height = h; f.spp = spp;
+    f.frameIndex = g.frameIndex;
+    f.rrStart = g.cfg.rrStart;
+    f.tanHalf = m::tanf_(0.5f * g.camera.fovYRadians);
+    f.cam = g.camera;
+    const DevScene s = makeDevScene();
+    cudaStream_t st = g.stream;
+    ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+    if (g.hitLogEnabled) ck(cudaMemsetAsync(g.hitLog.p, 0xfe, static_cast<size_t>(paths) * depth * 4, st), "cudaMemsetAsync");
+    float stage[5] = {0, 0, 0, 0, 0};
+    ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+    if (!g.stageTiming) {
+        launchGenerate(P, f, st);
+        for (int b = 0; b < depth; ++b) {
+            launchExtend(s, P, b, g.gridExtend, block, st);
+            launchShade(s, P, f, b, g.gridShade, block, st);
+            launchConnect(s, P, b, g.gridConnect, block, st);
+        }
+        launchPresent(P, f, g.accum.as<float>(), g.accumD.as<double>(), g.framebuffer.as<uint32_t>(), g.extFramebuffer, st);
+    } else {
+        // per-stage device time, summed over bounces (adds a sync per stage)
+        auto timed = [&](int k, auto&& fn) {
+            ck(cudaEventRecord(g.stageEv[0], st), "cudaEventRecord");
+            fn();
+            ck(cudaEventRecord(g.stageEv[1], st), "cudaEventRecord");
+            ck(cudaEventSynchronize(g.stageEv[1]), "cudaEventSynchronize");
+            float ms = 0.0f;
+            ck(cudaEventElapsedTime(&ms, g.stageEv[0], g.stageEv[1]), "cudaEventElapsedTime");
+            stage[k] += ms;
+        };
+        timed(0, [&] { launchGenerate(P, f, st); });
+        for (int b = 0; b < depth; ++b) {
+            timed(1, [&] { launchExtend(s, P, b, g.gridExtend, block, st); });
+            timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, st); });
+            timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
+        }
+        timed(4, [&] {
+            launchPresent(P, f, g.accum.as<float>(), g.accumD.as<double>(), g.framebuffer.as<uint32_t>(), g.extFramebuffer, st);
+        });
+    }
+    ck(cudaGetLastError(), "kernel launch");
+    ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
+    std::vector<int> rc(static_cast<size_t>(depth + 1)), sc(static_cast<size_t>(depth + 1));
+    unsigned int errFlags = 0;
+    ck(cudaMemcpyAsync(rc.data(), g.rayCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    ck(cudaMemcpyAsync(sc.data(), g.shadowCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    ck(cudaMemcpyAsync(&errFlags, g.errorFlags.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    ck(cudaStreamSynchronize(st), "frame");
+    BteFrameStats& S = g.stats;
+    S = BteFrameStats{};
+    S.samples = paths;
+    for (int b = 0; b < depth; ++b) {
+        S.extends += rc[static_cast<size_t>(b)];
+        S.shadowRays += sc[static_cast<size_t>(b)];
+        if (rc[static_cast<size_t>(b)] > 0) S.maxBounceReached = b;
+    }
+    ck(cudaEventElapsedTime(&S.msTotal, g.ev0, g.ev1), "cudaEventElapsedTime");
+    S.msGenerate = stage[0]; S.msExtend = stage[1]; S.msShade = stage[2]; S.msConnect = stage[3]; S.msPresent = stage[4];
+    g.frameIndex += static_cast<uint32_t>(spp);
+    g.lastPaths = paths; g.lastDepth = depth; g.lastSpp = spp; g.lastW = w; g.lastH = h; g.lastSlots = slots;
+    if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
+}
+
+template <typename F>
+int guarded(F&& fn)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    try {
+        ensureInit();
+        return fn();
+    } catch (const CudaError& e) {
+        g_lastError = e.msg;
+        return -1;
+    } catch (const std::exception& e) {
+        g_lastError = e.what();
+        return -1;
+    }
+}
+
+}  // namespace
+
+void setError(const std::string& msg) { g_lastError = msg; }
+
+}  // namespace bte
+
+using namespace bte;
+
+extern "C" {
+
+const char* bte_last_error(void) { return g_lastError.c_str(); }
+int bte_version(void) { return 1; }
+
+// src/host/scene_upload.cu:18-63
+int bte_init_scene(const TriangleData* triangles, int triangleCount, const Float3* materials, int materialCount,
+                   const int* triangleMaterialIds, int imageWidth, int imageHeight)
+{
+    (void)imageWidth; (void)imageHeight;
+    return guarded([&] {
+        g.tris.release(); g.materials.release(); g.triMatIds.release();
+        g.bvhNodes.release(); g.leafTris.release(); g.accelReady = false;
+        g.triCount = triangleCount > 0 ? triangleCount : 0;
+        g.materialCount = materialCount > 0 ? materialCount : 0;
+        if (triangleCount > 0) upload(g.tris, triangles, sizeof(TriangleData) * triangleCount, g.stream);
+        if (materialCount > 0) upload(g.materials, materials, sizeof(Float3) * materialCount, g.stream);
+        if (triangleMaterialIds && triangleCount > 0)
+            upload(g.triMatIds, triangleMaterialIds, sizeof(int) * triangleCount, g.stream);
+        rebuildTriEmitter();
+        ck(cudaStreamSynchronize(g.stream), "bte_init_scene");
+        return 0;
+    });
+}
+
+int bte_init(const TriangleData* tri, const Float3* color, int imageWidth, int imageHeight)
+{
+    return bte_init_scene(tri, 1, color, 1, nullptr, imageWidth, imageHeight);
+}
+
+// src/host/optix_setup.cu:298-302 (GAS build) -> LBVH
+int bte_init_accel(void)
+{
+    return guarded([&] {
+        g.bvhNodes.release(); g.leafTris.release(); g.accelReady = false;
+        if (!g.tris.p || g.triCount <= 0) throw CudaError{"bte_init_accel: call bte_init_scene first"};
+        BvhBuildResult r;
+        std::string err;
+        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, r, g.stream, err) != 0) throw CudaError{err};
+        g.bvhNodes.p = r.nodes; g.bvhNodes.bytes = sizeof(BvhNode) * (r.nodeCount > 0 ? r.nodeCount : 1);
+        g.leafTris.p = r.leafTris; g.leafTris.bytes = sizeof(float4) * 3 * static_cast<size_t>(g.triCount);
+        g.rootIsLeaf = r.rootIsLeaf;
+        g.msBvh = r.msBuild;
+        g.accelReady = true;
+        return 0;
+    });
+}
+
+int bte_init_camera(const CameraData* camera)
+{
+    return guarded([&] {
+        if (!camera) throw CudaError{"bte_init_camera: null camera"};
+        g.camera = *camera;
+        return 0;
+    });
+}
+
+int bte_init_triangle_emission(const Float3* emission, int triangleCount)
+{
+    return guarded([&] {
+        g.emission.release();
+        if (emission && triangleCount > 0) upload(g.emission, emission, sizeof(Float3) * triangleCount, g.stream);
+        ck(cudaStreamSynchronize(g.stream), "bte_init_triangle_emission");
+        return 0;
+    });
+}
+
+int bte_init_triangle_emitter_flags(const uint8_t* flags, int triangleCount)
+{
+    return guarded([&] {
+        g.emitterFlags.release();
+        if (flags && triangleCount > 0) upload(g.emitterFlags, flags, triangleCount, g.stream);
+        ck(cudaStreamSynchronize(g.stream), "bte_init_triangle_emitter_flags");
+        return 0;
+    });
+}
+
+// src/host/scene_upload.cu:111-157
+int bte_init_emitter_table(const EmitterData* emitters, int emitterCount, const int* emitterTriIndices,
+                           int emitterTriIndexCount, const float* emitterTriCdf, int emitterTriCdfCount,
+                           const float* sceneEmitterCdf)
+{
+    return guarded([&] {
+        g.emitters.release(); g.emitterTriIndices.release(); g.emitterTriCdf.release(); g.sceneEmitterCdf.release();
+        g.emitterCount = 0;
+        g.hostEmitters.clear(); g.hostEmitterTriIndices.clear();
+        if (emitters && emitterCount > 0 && emitterTriIndices && emitterTriIndexCount > 0 && emitterTriCdf &&
+            emitterTriCdfCount > 0 && sceneEmitterCdf) {
+            g.emitterCount = emitterCount;
+            upload(g.emitters, emitters, sizeof(EmitterData) * emitterCount, g.stream);
+            upload(g.emitterTriIndices, emitterTriIndices, sizeof(int) * emitterTriIndexCount, g.stream);
+            upload(g.emitterTriCdf, emitterTriCdf, sizeof(float) * emitterTriCdfCount, g.stream);
+            upload(g.sceneEmitterCdf, sceneEmitterCdf, sizeof(float) * (emitterCount + 1), g.stream);
+            g.hostEmitters.assign(emitters, emitters + emitterCount);
+            g.hostEmitterTriIndices.assign(emitterTriIndices, emitterTriIndices + emitterTriIndexCount);
+        }
+        rebuildTriEmitter();
+        ck(cudaStreamSynchronize(g.stream), "bte_init_emitter_table");
+        return 0;
+    });
+}
+
+// src/host/scene_upload.cu:159-178
+int bte_init_bsdfs(const BsdfData* bsdfs, int bsdfCount, const int* triangleBsdfIds, int triangleCount)
+{
+    return guarded([&] {
+        g.bsdfs.release(); g.triBsdfIds.release();
+        g.bsdfCount = 0;
+        if (bsdfs && bsdfCount > 0 && triangleBsdfIds && triangleCount > 0) {
+            for (int i = 0; i < triangleCount; ++i)
+                if (triangleBsdfIds[i] < 0 || triangleBsdfIds[i] >= bsdfCount)
+                    throw CudaError{"bte_init_bsdfs: triangle " + std::to_string(i) + " has BSDF id " +
+                                    std::to_string(triangleBsdfIds[i]) + " outside [0, " + std::to_string(bsdfCount) + ")"};
+            g.bsdfCount = bsdfCount;
+            upload(g.bsdfs, bsdfs, sizeof(BsdfData) * bsdfCount, g.stream);
+            upload(g.triBsdfIds, triangleBsdfIds, sizeof(int) * triangleCount, g.stream);
+        }
+        ck(cudaStreamSynchronize(g.stream), "bte_init_bsdfs");
+        return 0;
+    });
+}
+
+int bte_init_spotlights(const SpotlightData* spotlights, int spotlightCount)
+{
+    return guarded([&] {
+        g.spots.release();
+        g.spotCount = 0;
+        if (spotlights && spotlightCount > 0) {
+            if (spotlightCount > 30) throw CudaError{"bte_init_spotlights: at most 30 spotlights are supported"};
+            g.spotCount = spotlightCount;
+            upload(g.spots, spotlights, sizeof(SpotlightData) * spotlightCount, g.stream);
+        }
+        ck(cudaStreamSynchronize(g.stream), "bte_init_spotlights");
+        return 0;
+    });
+}
+
+static int initTextureSet(const uint8_t* const* pixels, const int* widths, const int* heights, int count,
+                          std::vector<DeviceBuffer>& set, DeviceBuffer& table, bool isMr)
+{
+    return guarded([&] {
+        for (auto& b : set) b.release();
+        set.clear();
+        table.release();
+        if (!isMr) g.textureCount = 0;
+        else g.hasMr = false;
+        if (!pixels || count <= 0) return 0;
+        set.resize(static_cast<size_t>(count));
+        std::vector<TexRef> refs(static_cast<size_t>(count), TexRef{nullptr, 0, 0});
+        for (int i = 0; i < count; ++i) {
+            if (!pixels[i]) continue;
+            if (widths[i] <= 0 || heights[i] <= 0) throw CudaError{"texture with non-positive size"};
+            upload(set[static_cast<size_t>(i)], pixels[i], static_cast<size_t>(widths[i]) * heights[i] * 4, g.stream);
+            refs[static_cast<size_t>(i)] = TexRef{set[static_cast<size_t>(i)].as<uchar4>(), widths[i], heights[i]};
+        }
+        upload(table, refs.data(), refs.size() * sizeof(TexRef), g.stream);
+        ck(cudaStreamSynchronize(g.stream), "texture upload");
+        if (!isMr) g.textureCount = count;
+        else g.hasMr = true;
+        return 0;
+    });
+}
+
+// src/host/scene_upload.cu:213-293
+int bte_init_textures(const uint8_t* const* pixels, const int* widths, const int* heights, int count)
+{
+    return initTextureSet(pixels, widths, heights, count, g.tex, g.texTable, false);
+}
+int bte_init_mr_textures(const uint8_t* const* pixels, const int* widths, const int* heights, int count)
+{
+    return initTextureSet(pixels, widths, heights, count, g.texMr, g.texTableMr, true);
+}
+
+// src/host/scene_upload.cu:390-484
+int bte_init_env_map(const float* rgba, int width, int height, float intensity, float rotationDeg)
+{
+    return guarded([&] {
+        for (DeviceBuffer* b : {&g.envTexels, &g.envMarginal, &g.envConditional, &g.envRowProb, &g.envRowAlias,
+                                &g.envColProb, &g.envColAlias, &g.envPixelPdf})
+            b->release();
+        g.hasEnv = false;
+        g.envW = g.envH = 0;
+        g.envTotalPowerF = 0.0f;
+        g.envTotalPowerD = 0.0;
+        if (!rgba || width <= 0 || height <= 0) return 0;
+        const size_t n = static_cast<size_t>(width) * height;
+        upload(g.envTexels, rgba, n * 16, g.stream);
+        ensure(g.envMarginal, sizeof(float) * (height + 1));
+        ensure(g.envConditional, sizeof(float) * static_cast<size_t>(height) * (width + 1));
+        ensure(g.envRowProb, sizeof(float) * height);
+        ensure(g.envRowAlias, sizeof(int) * height);
+        ensure(g.envColProb, sizeof(float) * n);
+        ensure(g.envColAlias, sizeof(int) * n);
+        ensure(g.envPixelPdf, sizeof(float) * n);
+        // theta at each row centre and its sine, evaluated as the reference's host loop does
+        const float PI = 3.14159265358979323846f;
+        std::vector<float> sinT(static_cast<size_t>(height));
+        for (int iy = 0; iy < height; ++iy) {
+            const float theta = PI * (static_cast<float>(iy) + 0.5f) / static_cast<float>(height);
+            sinT[static_cast<size_t>(iy)] = std::sin(theta);
+        }
+        std::string err;
+        if (buildEnvCdf(g.envTexels.as<float4>(), width, height, sinT.data(), g.envMarginal.as<float>(),
+                        g.envConditional.as<float>(), g.stream, err) != 0)
+            throw CudaError{err};
+        if (buildEnvAlias(g.envTexels.as<float4>(), width, height, g.envRowProb.as<float>(), g.envRowAlias.as<int>(),
+                          g.envColProb.as<float>(), g.envColAlias.as<int>(), g.envPixelPdf.as<float>(), &g.envTotalPowerD,
+                          g.stream, err) != 0)
+            throw CudaError{err};
+        ck(cudaMemcpy(&g.envTotalPowerF, g.envMarginal.as<float>() + height, sizeof(float), cudaMemcpyDeviceToHost),
+           "cudaMemcpy");
+        g.envW = width; g.envH = height;
+        g.envIntensity = intensity;
+        g.envRotation = rotationDeg * (PI / 180.0f);
+        g.hasEnv = true;
+        return 0;
+    });
+}
+
+int bte_set_output_buffer(uint32_t* deviceRGBA8)
+{
+    return guarded([&] { g.extFramebuffer = deviceRGBA8; return 0; });
+}
+
+// src/render_kernel.cu:40-56
+int bte_reset_accumulation(int imageWidth, int imageHeight)
+{
+    return guarded([&] {
+        if (imageWidth <= 0 || imageHeight <= 0) throw CudaError{"bte_reset_accumulation: size must be positive"};
+        ensureAccum(imageWidth, imageHeight);
+        return 0;
+    });
+}
+
+// src/render_kernel.cu:58-144
+int bte_render(int imageWidth, int imageHeight)
+{
+    return guarded([&] {
+        renderFrame(imageWidth, imageHeight);
+        return 0;
+    });
+}
+
+int bte_toggle_denoiser(void)
+{
+    return guarded([&]() -> int {
+        throw CudaError{"bte_toggle_denoiser: the learned denoiser is not part of this build; plain accumulation only"};
+    });
+}
+
+// src/render_kernel.cu:171-183
+int bte_set_render_mode(int mode)
+{
+    return guarded([&] {
+        if (mode != BTE_RENDER_MEGAKERNEL && mode != BTE_RENDER_WAVEFRONT) throw CudaError{"bte_set_render_mode: bad mode"};
+        if (mode != g.renderMode) {
+            g.renderMode = mode;
+            if (g.accumW > 0) ensureAccum(g.accumW, g.accumH);
+        }
+        return 0;
+    });
+}
+int bte_get_render_mode(void) { return g.renderMode; }
+
+// src/render_kernel.cu:146-168
+int bte_cleanup(void)
+{
+    return guarded([&] {
+        for (DeviceBuffer* b : {&g.tris, &g.materials, &g.triMatIds, &g.emission, &g.emitterFlags, &g.triEmitter,
+                                &g.emitters, &g.emitterTriIndices, &g.emitterTriCdf, &g.sceneEmitterCdf, &g.bsdfs,
+                                &g.triBsdfIds, &g.spots, &g.texTable, &g.texTableMr, &g.envTexels, &g.envMarginal,
+                                &g.envConditional, &g.envRowProb, &g.envRowAlias, &g.envColProb, &g.envColAlias,
+                                &g.envPixelPdf, &g.bvhNodes, &g.leafTris, &g.accum, &g.accumD, &g.framebuffer})
+            b->release();
+        for (auto& b : g.tex) b.release();
+        for (auto& b : g.texMr) b.release();
+        g.tex.clear(); g.texMr.clear();
+        releaseWavefront();
+        g.triCount = g.materialCount = g.emitterCount = g.bsdfCount = g.spotCount = g.textureCount = 0;
+        g.hasEnv = false; g.hasMr = false; g.accelReady = false;
+        g.accumW = g.accumH = 0; g.frameIndex = 0; g.extFramebuffer = nullptr;
+        g.hostEmitters.clear(); g.hostEmitterTriIndices.clear();
+        return 0;
+    });
+}
+
+int bte_set_render_config(const BteRenderConfig* cfg)
+{
+    return guarded([&] {
+        if (!cfg) throw CudaError{"bte_set_render_config: null config"};
+        if (cfg->samplesPerFrame < 1 || cfg->maxDepth < 1 || cfg->maxDepth > 1024)
+            throw CudaError{"bte_set_render_config: samplesPerFrame >= 1 and 1 <= maxDepth <= 1024 required"};
+        if (cfg->envSampling != BTE_ENV_SAMPLING_CDF && cfg->envSampling != BTE_ENV_SAMPLING_ALIAS)
+            throw CudaError{"bte_set_render_config: bad envSampling"};
+        if (cfg->blockSize != 0 && (cfg->blockSize < 32 || cfg->blockSize > 256 || cfg->blockSize % 32 != 0))
+            throw CudaError{"bte_set_render_config: blockSize must be 0 or a multiple of 32 in [32, 256]"};
+        g.cfg = *cfg;
+        return 0;
+    });
+}
+int bte_get_render_config(BteRenderConfig* cfg)
+{
+    return guarded([&] { if (cfg) *cfg = g.cfg; return 0; });
+}
+int bte_get_frame_stats(BteFrameStats* out)
+{
+    return guarded([&] { if (out) *out = g.stats; return 0; });
+}
+int bte_set_stage_timing(int enabled)
+{
+    return guarded([&] { g.stageTiming = enabled != 0; return 0; });
+}
+int bte_get_frame_index(uint32_t* out)
+{
+    return guarded([&] { if (out) *out = g.frameIndex; return 0; });
+}
+int bte_set_frame_index(uint32_t frameIndex)
+{
+    return guarded([&] { g.frameIndex = frameIndex; return 0; });
+}
+int bte_set_hit_log(int enabled)
+{
+    return guarded([&] { g.hitLogEnabled = enabled != 0; if (!g.hitLogEnabled) g.hitLog.release(); return 0; });
+}
+
+int bte_read_framebuffer(uint32_t* host)
+{
+    return guarded([&] {
+        if (!g.framebuffer.p) throw CudaError{"bte_read_framebuffer: nothing rendered"};
+        ck(cudaMemcpy(host, g.framebuffer.p, static_cast<size_t>(g.accumW) * g.accumH * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+int bte_read_accum(float* host)
+{
+    return guarded([&] {
+        if (!g.accum.p) throw CudaError{"bte_read_accum: nothing rendered"};
+        ck(cudaMemcpy(host, g.accum.p, static_cast<size_t>(g.accumW) * g.accumH * 12, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+int bte_read_accum_f64(double* host)
+{
+    return guarded([&] {
+        if (!g.accumD.p) throw CudaError{"bte_read_accum_f64: nothing rendered"};
+        ck(cudaMemcpy(host, g.accumD.p, static_cast<size_t>(g.accumW) * g.accumH * 24, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+int bte_read_sample_radiance(float* host, int count)
+{
+    return guarded([&] {
+        if (count < 0 || count > g.lastPaths) throw CudaError{"bte_read_sample_radiance: count out of range"};
+        std::vector<float4> tmp(static_cast<size_t>(count));
+        ck(cudaMemcpy(tmp.data(), g.pL.p, sizeof(float4) * count, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        for (int i = 0; i < count; ++i) {
+            host[3 * i] = tmp[static_cast<size_t>(i)].x;
+            host[3 * i + 1] = tmp[static_cast<size_t>(i)].y;
+            host[3 * i + 2] = tmp[static_cast<size_t>(i)].z;
+        }
+        return 0;
+    });
+}
+int bte_read_hit_log(int* host, int count)
+{
+    return guarded([&] {
+        if (!g.hitLog.p) throw CudaError{"bte_read_hit_log: enable with bte_set_hit_log before rendering"};
+        if (count < 0 || static_cast<long long>(count) > static_cast<long long>(g.lastPaths) * g.lastDepth)
+            throw CudaError{"bte_read_hit_log: count out of range"};
+        ck(cudaMemcpy(host, g.hitLog.p, sizeof(int) * count, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+}  // extern "C"
+
+// ---- debug / parity entry points ----
+namespace {
+template <typename T>
+struct Tmp {
+    T* p = nullptr;
+    explicit Tmp(size_t n) { ck(cudaMalloc(&p, sizeof(T) * (n > 0 ? n : 1)), "cudaMalloc"); }
+    ~Tmp() { cudaFree(p); }
+};
+}  // namespace
+
+extern "C" {
+
+int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv)
+{
+    return guarded([&] {
+        if (n <= 0) return 0;
+        if (!g.accelReady) throw CudaError{"bte_trace_closest: no acceleration structure"};
+        Tmp<float> dr(6 * static_cast<size_t>(n)), dt(3 * static_cast<size_t>(n));
+        Tmp<int> di(n);
+        Tmp<unsigned int> de(1);
+        ck(cudaMemcpy(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemset(de.p, 0, 4), "cudaMemset");
+        launchTraceClosestRays(makeDevScene(), dr.p, n, di.p, dt.p, de.p, g.stream);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(g.stream), "trace");
+        ck(cudaMemcpy(outTri, di.p, sizeof(int) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpy(outTuv, dt.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* outOccluded)
+{
+    return guarded([&] {
+        if (n <= 0) return 0;
+        if (!g.accelReady) throw CudaError{"bte_trace_occluded: no acceleration structure"};
+        Tmp<float> dr(6 * static_cast<size_t>(n)), dm(n);
+        Tmp<uint8_t> dout(n);
+        Tmp<unsigned int> de(1);
+        ck(cudaMemcpy(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemcpy(dm.p, tmax, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemset(de.p, 0, 4), "cudaMemset");
+        launchTraceOccludedRays(makeDevScene(), dr.p, dm.p, n, dout.p, de.p, g.stream);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(g.stream), "trace");
+        ck(cudaMemcpy(outOccluded, dout.p, n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+int bte_env_query(int op, const float* in, int n, float* out)
+{
+    return guarded([&] {
+        if (n <= 0) return 0;
+        if (!g.hasEnv) throw CudaError{"bte_env_query: no environment map"};
+        const size_t inN = (op == 2 ? 2 : 3) * static_cast<size_t>(n);
+        const size_t outN = (op == 0 ? 3 : (op == 1 ? 1 : 7)) * static_cast<size_t>(n);
+        Tmp<float> di(inN), dout(outN);
+        ck(cudaMemcpy(di.p, in, sizeof(float) * inN, cudaMemcpyHostToDevice), "cudaMemcpy");
+        launchEnvQuery(makeDevScene(), op, di.p, n, dout.p, g.stream);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(g.stream), "env query");
+        ck(cudaMemcpy(out, dout.p, sizeof(float) * outN, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+int bte_env_tables(float* marginal, float* conditional, float* totalPower)
+{
+    return guarded([&] {
+        if (!g.hasEnv) throw CudaError{"bte_env_tables: no environment map"};
+        if (marginal) ck(cudaMemcpy(marginal, g.envMarginal.p, sizeof(float) * (g.envH + 1), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (conditional)
+            ck(cudaMemcpy(conditional, g.envConditional.p, sizeof(float) * static_cast<size_t>(g.envH) * (g.envW + 1),
+                          cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (totalPower) *totalPower = g.envTotalPowerF;
+        return 0;
+    });
+}
+
+int bte_env_alias_tables(float* rowProb, int* rowIdx, float* colProb, int* colIdx, float* pixelPdf)
+{
+    return guarded([&] {
+        if (!g.hasEnv) throw CudaError{"bte_env_alias_tables: no environment map"};
+        const size_t n = static_cast<size_t>(g.envW) * g.envH;
+        if (rowProb) ck(cudaMemcpy(rowProb, g.envRowProb.p, sizeof(float) * g.envH, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (rowIdx) ck(cudaMemcpy(rowIdx, g.envRowAlias.p, sizeof(int) * g.envH, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (colProb) ck(cudaMemcpy(colProb, g.envColProb.p, sizeof(float) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (colIdx) ck(cudaMemcpy(colIdx, g.envColAlias.p, sizeof(int) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (pixelPdf) ck(cudaMemcpy(pixelPdf, g.envPixelPdf.p, sizeof(float) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+int bte_math_eval(int fn, const float* a, const float* b, float* out, int n)
+{
+    return guarded([&] {
+        if (n <= 0) return 0;
+        Tmp<float> da(n), db(n), dout(n);
+        ck(cudaMemcpy(da.p, a, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        if (b) ck(cudaMemcpy(db.p, b, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        else ck(cudaMemset(db.p, 0, sizeof(float) * n), "cudaMemset");
+        launchMathEval(fn, da.p, db.p, dout.p, n, g.stream);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(g.stream), "math");
+        ck(cudaMemcpy(out, dout.p, sizeof(float) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+int bte_bsdf_query(const BsdfData* bsdf, int op, const float* wi, const float* woOrU, int n, float* out)
+{
+    return guarded([&] {
+        if (n <= 0) return 0;
+        if (!bsdf || op < 0 || op > 2) throw CudaError{"bte_bsdf_query: bad arguments"};
+        const size_t outN = (op == 0 ? 3 : (op == 1 ? 1 : 8)) * static_cast<size_t>(n);
+        Tmp<float> dwi(3 * static_cast<size_t>(n)), dx(3 * static_cast<size_t>(n)), dout(outN);
+        ck(cudaMemcpy(dwi.p, wi, sizeof(float) * 3 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemcpy(dx.p, woOrU, sizeof(float) * 3 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        launchBsdfQuery(*bsdf, op, dwi.p, dx.p, n, dout.p, g.stream);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(g.stream), "bsdf");
+        ck(cudaMemcpy(out, dout.p, sizeof(float) * outN, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+// Hardware tex2D with the reference's env-map texture settings
+// (src/host/scene_upload.cu:406-420) against the library's software filter.
+int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* uv, int n, float* outHw, float* outSw)
+{
+    return guarded([&] {
+        if (n <= 0 || w <= 0 || h <= 0) return 0;
+        cudaArray_t arr = nullptr;
+        cudaTextureObject_t tex = 0;
+        const cudaChannelFormatDesc desc = cudaCreateChannelDesc<float4>();
+        ck(cudaMallocArray(&arr, &desc, w, h), "cudaMallocArray");
+        struct Guard {
+            cudaArray_t a; cudaTextureObject_t* t;
+            ~Guard() { if (*t) cudaDestroyTextureObject(*t); cudaFreeArray(a); }
+        } guard{arr, &tex};
+        ck(cudaMemcpy2DToArray(arr, 0, 0, texels, static_cast<size_t>(w) * 16, static_cast<size_t>(w) * 16, h,
+                               cudaMemcpyHostToDevice), "cudaMemcpy2DToArray");
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = cudaAddressModeWrap;
+        td.addressMode[1] = wrapV ? cudaAddressModeWrap : cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 1;
+        ck(cudaCreateTextureObject(&tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+        Tmp<float4> dt(static_cast<size_t>(w) * h);
+        Tmp<float> duv(2 * static_cast<size_t>(n)), dhw(4 * static_cast<size_t>(n)), dsw(4 * static_cast<size_t>(n));
+        ck(cudaMemcpy(dt.p, texels, sizeof(float4) * w * h, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemcpy(duv.p, uv, sizeof(float) * 2 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        launchTexCompare(tex, dt.p, w, h, wrapV, duv.p, n, dhw.p, dsw.p, g.stream);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(g.stream), "tex compare");
+        ck(cudaMemcpy(outHw, dhw.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpy(outSw, dsw.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        return 0;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+/*
+ * bte/render_api.h -- C-ABI of the B200 wavefront path tracer (libbte_b200.so).
+ *
+ * Drop-in boundary for Blue Truth Engine's renderer API.  Every entry point
+ * replaces one free function of the reference's include/render_kernel.h (cited
+ * per function, paths relative to the reference project root) with an
+ * extern "C" twin that takes plain pointers and sizes and returns a status
+ * (0 = success, negative = error; bte_last_error() describes the last error
+ * of the calling thread).  The reference aborts the process on any error
+ * (src/host/cuda_check.h:14-32); the reference-named C++ wrappers in
+ * bte/render_kernel.h keep that behaviour for drop-in callers.
+ *
+ * POD types are byte-identical to render_kernel.h:9-94.  Inputs are
+ * caller-owned host arrays copied synchronously during the call; the library
+ * owns the device copies; re-calling replaces; NULL/0 clears (as
+ * src/host/scene_upload.cu:18-198).  Not re-entrant: one renderer state per
+ * process, driven from one thread, like the reference's globals.
+ */
+#ifndef BTE_RENDER_API_H
+#define BTE_RENDER_API_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- POD types: render_kernel.h:9-94 ---- */
+typedef struct { float x, y; } Float2;
+typedef struct { float x, y, z; } Float3;
+typedef struct { float x, y, z, w; } Float4;
+typedef struct { Float3 v0, v1, v2; Float3 n0, n1, n2; Float2 uv0, uv1, uv2; } TriangleData;      /* 96 B */
+typedef struct { Float3 origin, forward, right, up; float fovYRadians, aspect; } CameraData;       /* 56 B */
+typedef struct { int triIndexOffset, triCount, cdfOffset; Float3 radiance; float areaSum, powerWeight; } EmitterData;
+typedef struct { Float3 position, direction, radiance; float intensity, innerConeCosine, outerConeCosine; } SpotlightData;
+typedef struct { int type; Float4 p0, p1, p2, p3; } BsdfData;                                      /* 68 B */
+enum { BSDF_Diffuse = 1, BSDF_Dielectric = 2, BSDF_Mirror = 3, BSDF_Microfacet = 4, BSDF_Disney = 5 };
+
+/* render_kernel.h:199-202 (only Wavefront is implemented; Megakernel is accepted and runs the wavefront path) */
+enum { BTE_RENDER_MEGAKERNEL = 0, BTE_RENDER_WAVEFRONT = 1 };
+
+/* env-map importance sampling: the reference's marginal/conditional CDF
+ * (rt_env_map.cuh:82-199, bit-exact) or FP64-built two-level alias tables. */
+enum { BTE_ENV_SAMPLING_CDF = 0, BTE_ENV_SAMPLING_ALIAS = 1 };
+
+/* Runtime knobs that are compile-time constants in the reference
+ * (include/rt_constants.cuh:11-19, rt_path_integrator.cuh:56). */
+typedef struct {
+    int samplesPerFrame;   /* paths per pixel per bte_render call (reference wavefront: 1) */
+    int maxDepth;          /* extend+shade steps per path (reference: MAX_BOUNCES = 200) */
+    int rrStart;           /* roulette when bounceCount > rrStart (reference: 3) */
+    int envSampling;       /* BTE_ENV_SAMPLING_* */
+    int blockSize;         /* threads per block of the stage kernels (0 = default) */
+    int useGraph;          /* capture the frame's launch sequence in a CUDA graph */
+} BteRenderConfig;
+
+typedef struct {
+    int64_t samples;       /* camera paths traced by the last bte_render */
+    int64_t extends;       /* closest-hit rays (path segments) */
+    int64_t shadowRays;    /* NEE shadow rays */
+    int maxBounceReached;  /* deepest bounce with a non-empty queue */
+    float msTotal;         /* device time of the last frame (CUDA events) */
+    float msGenerate, msExtend, msShade, msConnect, msPresent;  /* per stage (only with timing enabled) */
+} BteFrameStats;
+
+const char* bte_last_error(void);
+int bte_version(void);
+
+/* ---- scene uploads: render_kernel.h:100-174 ---- */
+int bte_init_scene(const TriangleData* triangles, int triangleCount, const Float3* materials, int materialCount,
+                   const int* triangleMaterialIds, int imageWidth, int imageHeight);       /* cudaInitScene :111 */
+int bte_init(const TriangleData* tri, const Float3* color, int imageWidth, int imageHeight); /* cudaInit :117 */
+int bte_init_accel(void);                                   /* cudaInitOptix :103 -> LBVH build */
+int bte_init_camera(const CameraData* camera);              /* cudaInitCamera :121 */
+int bte_init_triangle_emission(const Float3* emission, int triangleCount);      /* :125 */
+int bte_init_triangle_emitter_flags(const uint8_t* flags, int triangleCount);   /* :129 */
+int bte_init_emitter_table(const EmitterData* emitters, int emitterCount, const int* emitterTriIndices,
+                           int emitterTriIndexCount, const float* emitterTriCdf, int emitterTriCdfCount,
+                           const float* sceneEmitterCdf);                        /* :137 */
+int bte_init_bsdfs(const BsdfData* bsdfs, int bsdfCount, const int* triangleBsdfIds, int triangleCount); /* :143 */
+int bte_init_spotlights(const SpotlightData* spotlights, int spotlightCount);  /* :148 */
+int bte_init_textures(const uint8_t* const* pixels, const int* widths, const int* heights, int count);    /* :155 */
+int bte_init_mr_textures(const uint8_t* const* pixels, const int* widths, const int* heights, int count); /* :163 */
+int bte_init_env_map(const float* rgba, int width, int height, float intensity, float rotationDeg);      /* :173 */
+
+/* ---- frame API: render_kernel.h:177-211 ---- */
+int bte_set_output_buffer(uint32_t* deviceRGBA8);   /* replaces cudaRegisterPBO :177 (no GL on the box) */
+int bte_reset_accumulation(int imageWidth, int imageHeight);                    /* :183 */
+int bte_render(int imageWidth, int imageHeight);                                /* :187 */
+int bte_toggle_denoiser(void);                      /* :192; returns new state (0/1) or <0 */
+int bte_set_render_mode(int mode);                                              /* :205 */
+int bte_get_render_mode(void);                                                  /* :208 */
+int bte_cleanup(void);                                                          /* :211 */
+
+/* ---- additions (no reference counterpart; headless replacements of the PBO path) ---- */
+int bte_set_render_config(const BteRenderConfig* cfg);
+int bte_get_render_config(BteRenderConfig* cfg);
+int bte_get_frame_stats(BteFrameStats* out);
+int bte_set_stage_timing(int enabled);
+int bte_get_frame_index(uint32_t* out);              /* samples accumulated so far */
+int bte_set_frame_index(uint32_t frameIndex);        /* resume an accumulation at a sample index */
+int bte_read_framebuffer(uint32_t* hostRGBA8);       /* W*H packed ABGR, rt_path_integrator.cuh:93-105 */
+int bte_read_accum(float* hostRGB);                  /* FP32 Welford mean, W*H*3 */
+int bte_read_accum_f64(double* hostRGBSum);          /* FP64 running sum of samples, W*H*3 */
+int bte_read_sample_radiance(float* hostRGB, int count);  /* per-path radiance of the last frame [W*H*spp*3] */
+int bte_read_hit_log(int* hostTri, int count);       /* per-bounce closest-hit triangle of the last frame */
+int bte_set_hit_log(int enabled);                    /* record [path][bounce] hit triangles (debug/parity) */
+
+/* ---- debug/parity entry points over device-resident state ---- */
+/* closest hit for n rays [origin, dir] (host arrays): triangle index (-1 miss) and t, u, v */
+int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv);
+int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* outOccluded);
+/* env-map queries through the device tables */
+int bte_env_query(int op, const float* in, int n, float* out);   /* op 0 eval, 1 pdf, 2 sample */
+int bte_env_tables(float* marginal, float* conditional, float* totalPower);      /* CDF mode tables */
+int bte_env_alias_tables(float* rowProb, int* rowIdx, float* colProb, int* colIdx, float* pixelPdf);
+/* deterministic elementary functions as evaluated on the device */
+int bte_math_eval(int fn, const float* a, const float* b, float* out, int n);
+/* BSDF queries evaluated on the device */
+int bte_bsdf_query(const BsdfData* bsdf, int op, const float* wi, const float* woOrU, int n, float* out);
+/* hardware texture fetch vs the library's software filter, for the texture-filter pin */
+int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* uv, int n, float* outHw, float* outSw);
+
+/* ---- scene.xml / OBJ loader (src/scene.cpp:83-523, src/main.cpp:267-930) ---- */
+typedef struct BteScene BteScene;
+typedef struct {
+    const TriangleData* triangles; int triangleCount;
+    const Float3* materials; int materialCount;
+    const int* triangleMaterialIds;
+    const int* triangleBsdfIds;
+    const BsdfData* bsdfs; int bsdfCount;
+    const Float3* triangleEmission;
+    const uint8_t* triangleEmitterFlags;
+    const EmitterData* emitters; int emitterCount;
+    const int* emitterTriIndices; int emitterTriIndexCount;
+    const float* emitterTriCdf; int emitterTriCdfCount;
+    const float* sceneEmitterCdf;
+    const SpotlightData* spotlights; int spotlightCount;
+    const float* envRGBA; int envWidth, envHeight; float envIntensity, envRotationDeg;
+    CameraData camera;
+    int width, height;
+} BteSceneArrays;
+int bte_scene_load(const char* scenePath, BteScene** out);
+int bte_scene_arrays(const BteScene* scene, BteSceneArrays* out);
+void bte_scene_free(BteScene* scene);
+int bte_scene_upload(const BteScene* scene);   /* all bte_init_* calls of src/main.cpp:819-930 in order */
+
+#ifdef __cplusplus
+}
+#endif
+#endif
