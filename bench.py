@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Benchmark: Msamples/s of the wavefront path tracer at 1920x1080.
+
+Workload (the Disney/env-map configuration): ~1.0M triangles (64 seed-placed
+icospheres of subdivision 3-6 on a 200x200 tessellated ground), per-object
+Disney BSDFs, a 2048x1024 procedural HDR sky with a 0.5-degree sun of radiance
+1e4 sampled through the alias tables, 1920x1080, max depth 16, seeded
+synthetic data.  One step = one frame of `--spp` paths per pixel through the
+whole hot path (generate, extend, shade, connect, present).
+
+value  samples/s over K steps, device time (CUDA events around each frame,
+       inputs resident), max over ranks.
+e2e    samples/s through the C-ABI (bte_render + bte_read_framebuffer into a
+       host buffer every step), wall clock.
+Ranks (torchrun, N>1) render disjoint sample-index ranges of the same view:
+weak scaling, no collective on the data path.
+`--impl reference` times the reference's own integrator (its shading headers
+compiled on the host, oracle/_ref) on all host cores over a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes per unit of work, fixed by the reference's SoA record sizes
+# (include/wavefront/wavefront_buffers.h:40-90): path state 69 B, hit 36 B,
+# queue entry 4 B, shadow record 44 B.
+BYTES_PER_SAMPLE_FIXED = 113      # generate 69+4, present 12+4+24
+BYTES_PER_SEGMENT = 251           # extend 64 + shade 182 + 5 scene gathers
+BYTES_PER_SHADOW = 112            # 44 W + 44 R + 24 radiance RMW
+BYTES_PER_EXTEND_RAY = 64         # extend stage alone: queue 4 + ray 24 + hit 36
+BYTES_PER_SHADE_SEGMENT = 182
+BYTES_PER_CONNECT_RAY = 68        # 44 R + 24 RMW
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spp", type=int, default=2, help="paths per pixel per step")
+    ap.add_argument("--depth", type=int, default=16)
+    ap.add_argument("--env", default="alias", choices=["alias", "cdf"])
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def scene_path(args):
+    from bluetruthengine_b200 import scenes
+    return scenes.disney_spheres(seed=2, width=args.width, height=args.height)
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_r%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                for k, name in enumerate(names):
+                    if f[5 + k].lower().startswith("active"):
+                        reasons.add(name)
+        except Exception:
+            return None
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(scene, args, seconds: float, fast: bool = True):
+    """The reference's integrator (its headers compiled on the host) on all host cores, bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref = O.Ref(fast=fast)
+    view = O.SceneView(scene, env_mode=0, oracle=O.Oracle(libm=True), build_accel=True)
+    W, H = scene.width, scene.height
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+    # calibrate on a small random pixel sample, then size the timed sample to ~`seconds`
+    n = 4096
+    pix = rng.integers(0, W * H, size=n).astype(np.uint32)
+    t0 = time.perf_counter()
+    O.render_samples(ref.lib, view, scene.camera, W, H, args.depth, pix, np.zeros(n, np.uint32), prefix="ref_",
+                     threads=cores)
+    rate = n / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(max(rate * seconds, 4096), W * H * 4))
+    pix = rng.integers(0, W * H, size=n).astype(np.uint32)
+    t0 = time.perf_counter()
+    _, _, (ext, sh) = O.render_samples(ref.lib, view, scene.camera, W, H, args.depth, pix, np.zeros(n, np.uint32),
+                                       prefix="ref_", threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt / 1e6, "unit": "Msamples/s", "cores": cores, "kind": "reference",
+            "sample": "%d random pixels x 1 spp of the same 1920x1080 view, depth %d, CDF env sampling "
+                      "(the reference's own), %.1f s" % (n, args.depth, dt),
+            "extends_per_sample": ext / n, "shadow_rays_per_sample": sh / n}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import bluetruthengine_b200 as bte
+    scene = bte.load_scene(scene_path(args))
+    per_step = []
+    for _ in range(args.warmup):
+        pass
+    budget = max(3.0, 60.0 / max(args.steps, 1))
+    for _ in range(args.steps):
+        r = cpu_baseline(scene, args, seconds=budget)
+        per_step.append(r["value"])
+    val = statistics.median(per_step)
+    out = {"metric": "Msamples/s @1080p", "value": val, "unit": "Msamples/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "disney_spheres_1080p", "width": args.width, "height": args.height,
+                      "max_depth": args.depth, "triangles": int(scene.triangle_count)},
+           "cpu_baseline": {"value": val, "unit": "Msamples/s", "cores": r["cores"], "kind": "reference",
+                            "sample": r["sample"]},
+           "e2e": {"value": val, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    import bluetruthengine_b200 as bte
+    scene = bte.load_scene(scene_path(args))
+    W, H = scene.width, scene.height
+    r = bte.Renderer()
+    r.upload(scene)
+    env_mode = bte.ENV_ALIAS if args.env == "alias" else bte.ENV_CDF
+    r.set_config(samples_per_frame=args.spp, max_depth=args.depth, rr_start=3, env_sampling=env_mode)
+    r.reset_accumulation(W, H)
+    # disjoint sample ranges per rank
+    r.set_frame_index(rank * (args.steps + args.warmup + 8) * args.spp)
+    host_fb = torch.empty(W * H, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+
+    def step_e2e():
+        r.render(W, H)
+        r.lib.bte_read_framebuffer(host_fb.ctypes.data_as(__import__("ctypes").c_void_p))
+
+    for _ in range(args.warmup):
+        r.render(W, H)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # --- device-timed region (value) ---
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    ms = []
+    ext = shd = 0
+    for _ in range(args.steps):
+        r.render(W, H)
+        st = r.stats()
+        ms.append(st.msTotal)
+        ext += st.extends
+        shd += st.shadowRays
+    barrier()
+    clk = clocks.stop()
+    t_dev = sum(ms) / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([t_dev], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = float(t.item())
+    samples_per_rank = W * H * args.spp * args.steps
+    value = samples_per_rank * world / t_dev / 1e6
+
+    # --- end-to-end through the C-ABI with host buffers ---
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = samples_per_rank * world / t_e2e / 1e6
+
+    # --- per-stage split (separate, untimed pass) for the roofline of the dominant kernel ---
+    r.set_stage_timing(True)
+    r.render(W, H)
+    st = r.stats()
+    r.set_stage_timing(False)
+    stages = {"generate": st.msGenerate, "extend": st.msExtend, "shade": st.msShade, "connect": st.msConnect,
+              "present": st.msPresent}
+    dom = max(stages, key=stages.get)
+    launches_per_frame = 2 + 3 * args.depth
+    ext_f, sh_f = st.extends, st.shadowRays
+    bytes_dom = {"extend": ext_f * BYTES_PER_EXTEND_RAY, "shade": ext_f * BYTES_PER_SHADE_SEGMENT,
+                 "connect": sh_f * BYTES_PER_CONNECT_RAY,
+                 "generate": W * H * args.spp * 73, "present": W * H * args.spp * 40}[dom]
+    launches_dom = 1 if dom in ("generate", "present") else args.depth
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_dom / (stages[dom] / 1e3) / 1e9      # GB/s over the stage's launches in the frame
+    spp_samples = W * H * args.spp
+    s_mean = ext / (samples_per_rank)
+    r_mean = shd / (samples_per_rank)
+    b_sample = BYTES_PER_SAMPLE_FIXED + BYTES_PER_SEGMENT * s_mean + BYTES_PER_SHADOW * r_mean
+    out = {"metric": "Msamples/s @1080p", "value": value, "unit": "Msamples/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded procedural scene, no dataset)",
+           "config": {"workload": "disney_spheres_1080p", "width": W, "height": H, "spp_per_step": args.spp,
+                      "max_depth": args.depth, "triangles": int(scene.triangle_count), "env_sampling": args.env,
+                      "l2": "inputs larger than L2 (path state %d MB per step)" % (spp_samples * 150 // (1 << 20)),
+                      "parallelism": "replicas over sample ranges x%d" % world},
+           "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": 56,
+                   "d2h_bytes_per_step": W * H * 4 + (3 * (args.depth + 1) * 4)},
+           "gpu_launches": launches_per_frame * args.steps,
+           "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                        "algorithmic_bytes_per_launch": bytes_dom / launches_dom,
+                        "stage_ms": stages},
+           "path_stats": {"extends_per_sample": s_mean, "shadow_rays_per_sample": r_mean,
+                          "bytes_per_sample": b_sample,
+                          "whole_frame_hbm_frac": (value * 1e6 / world) * b_sample / (peak * 1e9)}}
+    if clk is not None:
+        out["clocks"] = clk
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(scene, args, seconds=args.cpu_seconds)
+        except Exception as e:  # the baseline is reported, never the product
+            out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

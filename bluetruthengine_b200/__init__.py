@@ -347,7 +347,7 @@ class Renderer:
         r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
         t = np.ascontiguousarray(tmax, dtype=np.float32)
         out = np.empty(len(r), dtype=np.uint8)
-        _check(self.lib.bte_trace_occluded(_ptr(r), len(r), _ptr(t), _ptr(out)))
+        _check(self.lib.bte_trace_occluded(_ptr(r), _ptr(t), len(r), _ptr(out)))
         return out
 
     def env_query(self, op: int, x: np.ndarray) -> np.ndarray:

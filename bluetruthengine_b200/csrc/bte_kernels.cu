@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
         const int idx = q[slot];
         const float4 o = P.o[idx];
         const float4 d = P.d[idx];
-        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z);
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
         float t = 0.0f, u = 0.0f, v = 0.0f;
         const int tri = traceClosest(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
         P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int boun
         const int slot = e - path * P.slots;
         const float4 o = P.shOrigin[path];
         const float4 d = P.shDir[e];
-        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z);
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
         if (traceOccluded(s, r, kEps, d.w, P.errorFlags)) atomicAnd(P.shMask + path, ~(1u << slot));
     }
 }
@@ -251,7 +251,7 @@ __global__ void kTraceClosestRays(DevScene s, const float* rays, int n, int* out
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* r6 = rays + 6 * static_cast<size_t>(i);
-    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5]);
+    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5], s.sceneMaxAbs);
     float t = 0.0f, u = 0.0f, v = 0.0f;
     const int tri = traceClosest(s, r, kEps, 1e30f, t, u, v, err);
     outTri[i] = tri;
@@ -263,7 +263,7 @@ __global__ void kTraceOccludedRays(DevScene s, const float* rays, const float* t
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* r6 = rays + 6 * static_cast<size_t>(i);
-    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5]);
+    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5], s.sceneMaxAbs);
     out[i] = traceOccluded(s, r, kEps, tmax[i], err) ? 1 : 0;
 }
 

@@ -69,6 +69,7 @@ struct Renderer {
     DeviceBuffer tris, materials, triMatIds, emission, emitterFlags, triEmitter, emitters, emitterTriIndices,
         emitterTriCdf, sceneEmitterCdf, bsdfs, triBsdfIds, spots;
     int triCount = 0, materialCount = 0, emitterCount = 0, bsdfCount = 0, spotCount = 0;
+    float sceneMaxAbs = 0.0f;
     bool hasEmission = false, hasFlags = false;
     std::vector<int> hostEmitterTriIndices;
     std::vector<EmitterData> hostEmitters;
@@ -133,6 +134,7 @@ DevScene makeDevScene()
     s.leafTris = g.leafTris.as<float4>();
     s.nodes = g.bvhNodes.as<BvhNode>();
     s.rootIsLeaf = g.rootIsLeaf;
+    s.sceneMaxAbs = g.sceneMaxAbs;
     s.bsdfs = g.bsdfs.as<BsdfData>();
     s.triBsdfIds = g.triBsdfIds.as<int>();
     s.triMaterialIds = g.triMatIds.as<int>();
@@ -381,6 +383,13 @@ int bte_init_scene(const TriangleData* triangles, int triangleCount, const Float
         g.triCount = triangleCount > 0 ? triangleCount : 0;
         g.materialCount = materialCount > 0 ? materialCount : 0;
         if (triangleCount > 0) upload(g.tris, triangles, sizeof(TriangleData) * triangleCount, g.stream);
+        float mx = 0.0f;
+        for (int i = 0; i < triangleCount; ++i) {
+            const TriangleData& t = triangles[i];
+            const float c[9] = {t.v0.x, t.v0.y, t.v0.z, t.v1.x, t.v1.y, t.v1.z, t.v2.x, t.v2.y, t.v2.z};
+            for (float x : c) mx = std::fmax(mx, std::fabs(x));
+        }
+        g.sceneMaxAbs = mx;
         if (materialCount > 0) upload(g.materials, materials, sizeof(Float3) * materialCount, g.stream);
         if (triangleMaterialIds && triangleCount > 0)
             upload(g.triMatIds, triangleMaterialIds, sizeof(int) * triangleCount, g.stream);
@@ -574,8 +583,9 @@ int bte_init_env_map(const float* rgba, int width, int height, float intensity, 
                           g.envColProb.as<float>(), g.envColAlias.as<int>(), g.envPixelPdf.as<float>(), &g.envTotalPowerD,
                           g.stream, err) != 0)
             throw CudaError{err};
-        ck(cudaMemcpy(&g.envTotalPowerF, g.envMarginal.as<float>() + height, sizeof(float), cudaMemcpyDeviceToHost),
-           "cudaMemcpy");
+        ck(cudaMemcpyAsync(&g.envTotalPowerF, g.envMarginal.as<float>() + height, sizeof(float), cudaMemcpyDeviceToHost,
+                           g.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(g.stream), "sync");
         g.envW = width; g.envH = height;
         g.envIntensity = intensity;
         g.envRotation = rotationDeg * (PI / 180.0f);
@@ -694,7 +704,7 @@ int bte_read_framebuffer(uint32_t* host)
 {
     return guarded([&] {
         if (!g.framebuffer.p) throw CudaError{"bte_read_framebuffer: nothing rendered"};
-        ck(cudaMemcpy(host, g.framebuffer.p, static_cast<size_t>(g.accumW) * g.accumH * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(host, g.framebuffer.p, static_cast<size_t>(g.accumW) * g.accumH * 4, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -702,7 +712,7 @@ int bte_read_accum(float* host)
 {
     return guarded([&] {
         if (!g.accum.p) throw CudaError{"bte_read_accum: nothing rendered"};
-        ck(cudaMemcpy(host, g.accum.p, static_cast<size_t>(g.accumW) * g.accumH * 12, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(host, g.accum.p, static_cast<size_t>(g.accumW) * g.accumH * 12, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -710,7 +720,7 @@ int bte_read_accum_f64(double* host)
 {
     return guarded([&] {
         if (!g.accumD.p) throw CudaError{"bte_read_accum_f64: nothing rendered"};
-        ck(cudaMemcpy(host, g.accumD.p, static_cast<size_t>(g.accumW) * g.accumH * 24, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(host, g.accumD.p, static_cast<size_t>(g.accumW) * g.accumH * 24, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -719,7 +729,8 @@ int bte_read_sample_radiance(float* host, int count)
     return guarded([&] {
         if (count < 0 || count > g.lastPaths) throw CudaError{"bte_read_sample_radiance: count out of range"};
         std::vector<float4> tmp(static_cast<size_t>(count));
-        ck(cudaMemcpy(tmp.data(), g.pL.p, sizeof(float4) * count, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(tmp.data(), g.pL.p, sizeof(float4) * count, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(g.stream), "sync");
         for (int i = 0; i < count; ++i) {
             host[3 * i] = tmp[static_cast<size_t>(i)].x;
             host[3 * i + 1] = tmp[static_cast<size_t>(i)].y;
@@ -734,7 +745,7 @@ int bte_read_hit_log(int* host, int count)
         if (!g.hitLog.p) throw CudaError{"bte_read_hit_log: enable with bte_set_hit_log before rendering"};
         if (count < 0 || static_cast<long long>(count) > static_cast<long long>(g.lastPaths) * g.lastDepth)
             throw CudaError{"bte_read_hit_log: count out of range"};
-        ck(cudaMemcpy(host, g.hitLog.p, sizeof(int) * count, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(host, g.hitLog.p, sizeof(int) * count, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -761,13 +772,13 @@ int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv)
         Tmp<float> dr(6 * static_cast<size_t>(n)), dt(3 * static_cast<size_t>(n));
         Tmp<int> di(n);
         Tmp<unsigned int> de(1);
-        ck(cudaMemcpy(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-        ck(cudaMemset(de.p, 0, 4), "cudaMemset");
+        ck(cudaMemcpyAsync(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        ck(cudaMemsetAsync(de.p, 0, 4, g.stream), "cudaMemsetAsync");
         launchTraceClosestRays(makeDevScene(), dr.p, n, di.p, dt.p, de.p, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "trace");
-        ck(cudaMemcpy(outTri, di.p, sizeof(int) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
-        ck(cudaMemcpy(outTuv, dt.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(outTri, di.p, sizeof(int) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        ck(cudaMemcpyAsync(outTuv, dt.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -780,13 +791,13 @@ int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* out
         Tmp<float> dr(6 * static_cast<size_t>(n)), dm(n);
         Tmp<uint8_t> dout(n);
         Tmp<unsigned int> de(1);
-        ck(cudaMemcpy(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-        ck(cudaMemcpy(dm.p, tmax, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-        ck(cudaMemset(de.p, 0, 4), "cudaMemset");
+        ck(cudaMemcpyAsync(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        ck(cudaMemcpyAsync(dm.p, tmax, sizeof(float) * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        ck(cudaMemsetAsync(de.p, 0, 4, g.stream), "cudaMemsetAsync");
         launchTraceOccludedRays(makeDevScene(), dr.p, dm.p, n, dout.p, de.p, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "trace");
-        ck(cudaMemcpy(outOccluded, dout.p, n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(outOccluded, dout.p, n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -799,11 +810,11 @@ int bte_env_query(int op, const float* in, int n, float* out)
         const size_t inN = (op == 2 ? 2 : 3) * static_cast<size_t>(n);
         const size_t outN = (op == 0 ? 3 : (op == 1 ? 1 : 7)) * static_cast<size_t>(n);
         Tmp<float> di(inN), dout(outN);
-        ck(cudaMemcpy(di.p, in, sizeof(float) * inN, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemcpyAsync(di.p, in, sizeof(float) * inN, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
         launchEnvQuery(makeDevScene(), op, di.p, n, dout.p, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "env query");
-        ck(cudaMemcpy(out, dout.p, sizeof(float) * outN, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(out, dout.p, sizeof(float) * outN, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -812,10 +823,11 @@ int bte_env_tables(float* marginal, float* conditional, float* totalPower)
 {
     return guarded([&] {
         if (!g.hasEnv) throw CudaError{"bte_env_tables: no environment map"};
-        if (marginal) ck(cudaMemcpy(marginal, g.envMarginal.p, sizeof(float) * (g.envH + 1), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (marginal) ck(cudaMemcpyAsync(marginal, g.envMarginal.p, sizeof(float) * (g.envH + 1), cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         if (conditional)
-            ck(cudaMemcpy(conditional, g.envConditional.p, sizeof(float) * static_cast<size_t>(g.envH) * (g.envW + 1),
-                          cudaMemcpyDeviceToHost), "cudaMemcpy");
+            ck(cudaMemcpyAsync(conditional, g.envConditional.p, sizeof(float) * static_cast<size_t>(g.envH) * (g.envW + 1),
+                               cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(g.stream), "sync");
         if (totalPower) *totalPower = g.envTotalPowerF;
         return 0;
     });
@@ -826,11 +838,11 @@ int bte_env_alias_tables(float* rowProb, int* rowIdx, float* colProb, int* colId
     return guarded([&] {
         if (!g.hasEnv) throw CudaError{"bte_env_alias_tables: no environment map"};
         const size_t n = static_cast<size_t>(g.envW) * g.envH;
-        if (rowProb) ck(cudaMemcpy(rowProb, g.envRowProb.p, sizeof(float) * g.envH, cudaMemcpyDeviceToHost), "cudaMemcpy");
-        if (rowIdx) ck(cudaMemcpy(rowIdx, g.envRowAlias.p, sizeof(int) * g.envH, cudaMemcpyDeviceToHost), "cudaMemcpy");
-        if (colProb) ck(cudaMemcpy(colProb, g.envColProb.p, sizeof(float) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
-        if (colIdx) ck(cudaMemcpy(colIdx, g.envColAlias.p, sizeof(int) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
-        if (pixelPdf) ck(cudaMemcpy(pixelPdf, g.envPixelPdf.p, sizeof(float) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (rowProb) ck(cudaMemcpyAsync(rowProb, g.envRowProb.p, sizeof(float) * g.envH, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        if (rowIdx) ck(cudaMemcpyAsync(rowIdx, g.envRowAlias.p, sizeof(int) * g.envH, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        if (colProb) ck(cudaMemcpyAsync(colProb, g.envColProb.p, sizeof(float) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        if (colIdx) ck(cudaMemcpyAsync(colIdx, g.envColAlias.p, sizeof(int) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        if (pixelPdf) ck(cudaMemcpyAsync(pixelPdf, g.envPixelPdf.p, sizeof(float) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -840,13 +852,13 @@ int bte_math_eval(int fn, const float* a, const float* b, float* out, int n)
     return guarded([&] {
         if (n <= 0) return 0;
         Tmp<float> da(n), db(n), dout(n);
-        ck(cudaMemcpy(da.p, a, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-        if (b) ck(cudaMemcpy(db.p, b, sizeof(float) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-        else ck(cudaMemset(db.p, 0, sizeof(float) * n), "cudaMemset");
+        ck(cudaMemcpyAsync(da.p, a, sizeof(float) * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        if (b) ck(cudaMemcpyAsync(db.p, b, sizeof(float) * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        else ck(cudaMemsetAsync(db.p, 0, sizeof(float) * n, g.stream), "cudaMemsetAsync");
         launchMathEval(fn, da.p, db.p, dout.p, n, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "math");
-        ck(cudaMemcpy(out, dout.p, sizeof(float) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(out, dout.p, sizeof(float) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -858,12 +870,12 @@ int bte_bsdf_query(const BsdfData* bsdf, int op, const float* wi, const float* w
         if (!bsdf || op < 0 || op > 2) throw CudaError{"bte_bsdf_query: bad arguments"};
         const size_t outN = (op == 0 ? 3 : (op == 1 ? 1 : 8)) * static_cast<size_t>(n);
         Tmp<float> dwi(3 * static_cast<size_t>(n)), dx(3 * static_cast<size_t>(n)), dout(outN);
-        ck(cudaMemcpy(dwi.p, wi, sizeof(float) * 3 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
-        ck(cudaMemcpy(dx.p, woOrU, sizeof(float) * 3 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemcpyAsync(dwi.p, wi, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        ck(cudaMemcpyAsync(dx.p, woOrU, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
         launchBsdfQuery(*bsdf, op, dwi.p, dx.p, n, dout.p, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "bsdf");
-        ck(cudaMemcpy(out, dout.p, sizeof(float) * outN, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(out, dout.p, sizeof(float) * outN, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }
@@ -882,8 +894,8 @@ int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* 
             cudaArray_t a; cudaTextureObject_t* t;
             ~Guard() { if (*t) cudaDestroyTextureObject(*t); cudaFreeArray(a); }
         } guard{arr, &tex};
-        ck(cudaMemcpy2DToArray(arr, 0, 0, texels, static_cast<size_t>(w) * 16, static_cast<size_t>(w) * 16, h,
-                               cudaMemcpyHostToDevice), "cudaMemcpy2DToArray");
+        ck(cudaMemcpy2DToArrayAsync(arr, 0, 0, texels, static_cast<size_t>(w) * 16, static_cast<size_t>(w) * 16, h,
+                                    cudaMemcpyHostToDevice, g.stream), "cudaMemcpy2DToArrayAsync");
         cudaResourceDesc rd{};
         rd.resType = cudaResourceTypeArray;
         rd.res.array.array = arr;
@@ -896,13 +908,13 @@ int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* 
         ck(cudaCreateTextureObject(&tex, &rd, &td, nullptr), "cudaCreateTextureObject");
         Tmp<float4> dt(static_cast<size_t>(w) * h);
         Tmp<float> duv(2 * static_cast<size_t>(n)), dhw(4 * static_cast<size_t>(n)), dsw(4 * static_cast<size_t>(n));
-        ck(cudaMemcpy(dt.p, texels, sizeof(float4) * w * h, cudaMemcpyHostToDevice), "cudaMemcpy");
-        ck(cudaMemcpy(duv.p, uv, sizeof(float) * 2 * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        ck(cudaMemcpyAsync(dt.p, texels, sizeof(float4) * w * h, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
+        ck(cudaMemcpyAsync(duv.p, uv, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
         launchTexCompare(tex, dt.p, w, h, wrapV, duv.p, n, dhw.p, dsw.p, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "tex compare");
-        ck(cudaMemcpy(outHw, dhw.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
-        ck(cudaMemcpy(outSw, dsw.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        ck(cudaMemcpyAsync(outHw, dhw.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        ck(cudaMemcpyAsync(outSw, dsw.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }

@@ -911,7 +911,7 @@ BTE_DI float areaToSolid(float pA, const EQ& q)
 // :60-99 (emitter lookup through the tri -> emitter side table)
 BTE_DI void accumulateEmitterHit(const DevScene& s, PathReg& p, const HitReg& h)
 {
-    const Float3 r0 = s.emission[h.tri];
+    const Float3 r0 = s.emission ? s.emission[h.tri] : Float3{0.0f, 0.0f, 0.0f};
     EQ q = eq0();
     q.origin = p.o; q.hitPoint = h.p; q.hitNormal = h.n; q.dirToLight = p.d;
     float w = 1.0f;

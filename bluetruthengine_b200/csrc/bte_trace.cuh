@@ -8,8 +8,12 @@
 // not depend on the tree or on traversal order.  The box test is the robust
 // slab test (tmax scaled by 1 + 2*gamma_3, Ize 2013) and nodes are culled only
 // when their entry distance exceeds the current best by a relative margin, so
-// culling never changes which triangle wins.  Barycentrics follow the OptiX
-// convention: u weights v1, v weights v2.
+// culling never changes which triangle wins.  Because the watertight test's t
+// carries an absolute error that grows with the coordinates' magnitude
+// (cancellation between vertex and origin coordinates), every slab is widened
+// by kTriErrK * 2^-24 * (max|origin| + max|scene coordinate|): a node is
+// culled only if no triangle inside could report a t the test would accept.
+// Barycentrics follow the OptiX convention: u weights v1, v weights v2.
 #pragma once
 
 #include "bte_types.cuh"
@@ -23,12 +27,15 @@ struct RayPre {
     int kx, ky, kz;
     float Sx, Sy, Sz;
     float ix, iy, iz;     // reciprocal direction for the slab test (zeros replaced by +-1e-30)
+    float px, py, pz;     // per-slab widening in t units
     bool valid;
 };
 
+constexpr float kTriErrK = 64.0f;
+
 BTE_DI float comp3(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
 
-BTE_DI RayPre rayPre(float ox, float oy, float oz, float dx, float dy, float dz)
+BTE_DI RayPre rayPre(float ox, float oy, float oz, float dx, float dy, float dz, float sceneMaxAbs)
 {
     RayPre r;
     r.ox = ox; r.oy = oy; r.oz = oz;
@@ -48,6 +55,10 @@ BTE_DI RayPre rayPre(float ox, float oy, float oz, float dx, float dy, float dz)
     r.ix = 1.0f / (fabsf(dx) > 1e-30f ? dx : copysignf(1e-30f, dx));
     r.iy = 1.0f / (fabsf(dy) > 1e-30f ? dy : copysignf(1e-30f, dy));
     r.iz = 1.0f / (fabsf(dz) > 1e-30f ? dz : copysignf(1e-30f, dz));
+    const float pad = kTriErrK * 5.9604645e-8f * (fmaxf(fabsf(ox), fmaxf(fabsf(oy), fabsf(oz))) + sceneMaxAbs);
+    r.px = pad * fabsf(r.ix);
+    r.py = pad * fabsf(r.iy);
+    r.pz = pad * fabsf(r.iz);
     return r;
 }
 
@@ -96,8 +107,8 @@ BTE_DI bool boxHit(const RayPre& r, float lx, float hx, float ly, float hy, floa
     const float tx0 = (lx - r.ox) * r.ix, tx1 = (hx - r.ox) * r.ix;
     const float ty0 = (ly - r.oy) * r.iy, ty1 = (hy - r.oy) * r.iy;
     const float tz0 = (lz - r.oz) * r.iz, tz1 = (hz - r.oz) * r.iz;
-    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
-    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax)) * kBoxGrow;
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1) - r.px, fminf(ty0, ty1) - r.py), fmaxf(fminf(tz0, tz1) - r.pz, tmin));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1) + r.px, fmaxf(ty0, ty1) + r.py), fminf(fmaxf(tz0, tz1) + r.pz, tmax)) * kBoxGrow;
     tEnter = tn;
     return tn <= tf;
 }

@@ -50,6 +50,7 @@ struct DevScene {
     const float4* leafTris;           // [triCount*3] v0.xyz|origIndex, v1.xyz, v2.xyz in leaf order
     const BvhNode* nodes;             // root = node 0 (triCount >= 2) or a single-leaf root
     int rootIsLeaf;                   // triCount == 1
+    float sceneMaxAbs;                // max |coordinate| over all vertices (traversal error bound)
     // materials
     const BsdfData* bsdfs;
     const int* triBsdfIds;

@@ -26,7 +26,7 @@ import struct
 
 import numpy as np
 
-GENERATOR_VERSION = 3
+GENERATOR_VERSION = 4
 CACHE_ROOT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), ".scene_cache")
 
 
@@ -270,7 +270,12 @@ def disney_spheres(seed: int = 2, width: int = 1920, height: int = 1080, n_spher
              'roughness="0.6" metallic="0" specular="0.5" clearcoat="0" />',
              '    <material name="groundM" bsdf="groundB" />',
              '    <mesh filename="ground.obj" material="groundM" />']
-    levels = rng.choice([3, 4, 5, 6], size=n_spheres, p=[0.35, 0.35, 0.2, 0.1])
+    # subdivision levels: a fixed mix (32 x L3, 15 x L4, 9 x L5, 8 x L6 for 64 spheres) that puts the
+    # scene at ~1.04M triangles with the ground, assigned to spheres in seeded order
+    mix = np.array([3] * 32 + [4] * 15 + [5] * 9 + [6] * 8)
+    if n_spheres != 64:
+        mix = np.resize(mix, n_spheres)
+    levels = rng.permutation(mix)
     for i in range(n_spheres):
         r = rng.uniform(0.2, 2.0)
         x, z = rng.uniform(-20.0, 20.0, size=2)

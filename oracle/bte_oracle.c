@@ -1484,7 +1484,7 @@ static int o_isectTri(const ORayPre* r, const OTri* T, float tmin, float tmax, f
 
 /* ---- CPU BVH (binary, object-median split on the longest centroid axis) ---- */
 typedef struct { float lo[3], hi[3]; int left, right; int first, count; } OBvhNode;
-typedef struct { OBvhNode* nodes; int nodeCount; int* idx; double slack; } OAccel;
+typedef struct { OBvhNode* nodes; int nodeCount; int* idx; double maxAbs; } OAccel;
 
 static void o_triBounds(const OTri* t, float lo[3], float hi[3])
 {
@@ -1553,7 +1553,7 @@ int or_build_accel(OScene* s)
             ext = fmax(ext, fmax(fabs((double)lo[k]), fabs((double)hi[k])));
         }
     }
-    A->slack = ext * 1e-6 + 1e-6;
+    A->maxAbs = ext;
     o_buildRec(A, s->triangles, cen, 0, T);
     free(cen);
     s->accel = A;
@@ -1568,13 +1568,16 @@ void or_free_accel(OScene* s)
     s->accel = NULL;
 }
 
-/* Conservative slab test in double with boxes padded by A->slack. */
+/* Conservative slab test in double, each slab widened by the bound on the
+ * watertight test's t error (128 * 2^-24 * (max|origin| + max|scene coordinate|)). */
 static inline int o_boxHit(const OAccel* A, const OBvhNode* n, const double o[3], const double inv[3],
                            double tmin, double tmax)
 {
     double t0 = tmin, t1 = tmax;
+    const double pad = 128.0 * 5.9604644775390625e-8 * (fmax(fabs(o[0]), fmax(fabs(o[1]), fabs(o[2]))) + A->maxAbs);
+    (void)A;
     for (int k = 0; k < 3; ++k) {
-        const double lo = (double)n->lo[k] - A->slack, hi = (double)n->hi[k] + A->slack;
+        const double lo = (double)n->lo[k] - pad, hi = (double)n->hi[k] + pad;
         double a = (lo - o[k]) * inv[k], b = (hi - o[k]) * inv[k];
         if (a != a) a = -INFINITY;   /* 0 * inf when the origin lies on the slab plane */
         if (b != b) b = INFINITY;
@@ -1694,7 +1697,7 @@ static void o_fillHit(const OScene* s, OF3 o, OF3 d, int tri, float t, float u, 
 /* megakernel's per-path order (src/optix_programs.cu:54-108).         */
 /* ------------------------------------------------------------------ */
 static OF3 o_renderSample(const OScene* s, const OCamera* cam, const OConfig* cfg, uint32_t pixel, uint32_t sampleIndex,
-                          int* hitLog, OStats* st)
+                          int* hitLog, OStats* st, float* rayLog)
 {
     const int px = (int)(pixel % (uint32_t)cfg->width);
     const int py = (int)(pixel / (uint32_t)cfg->width);
@@ -1713,6 +1716,10 @@ static OF3 o_renderSample(const OScene* s, const OCamera* cam, const OConfig* cf
 
     for (int bounce = 0; bounce < cfg->maxDepth; ++bounce) {
         float t, u, v;
+        if (rayLog) {
+            float* r6 = rayLog + 6 * bounce;
+            r6[0] = p.o.x; r6[1] = p.o.y; r6[2] = p.o.z; r6[3] = p.d.x; r6[4] = p.d.y; r6[5] = p.d.z;
+        }
         const int tri = o_traceClosest(s, p.o, p.d, O_RT_EPSILON, 1e30f, &t, &u, &v);
         if (st) st->extends++;
         if (hitLog) hitLog[bounce] = tri;
@@ -1763,12 +1770,20 @@ void or_render_samples(const OScene* s, const OCamera* cam, const OConfig* cfg, 
     for (int i = 0; i < n; ++i) {
         OStats local = {0, 0};
         OF3 L = o_renderSample(s, cam, cfg, pixels[i], sampleIndices[i], hitLog ? hitLog + (size_t)i * cfg->maxDepth : NULL,
-                               &local);
+                               &local, NULL);
         outRadiance[3 * i] = L.x; outRadiance[3 * i + 1] = L.y; outRadiance[3 * i + 2] = L.z;
         ext += local.extends; sh += local.shadowRays;
     }
     (void)threads;
     if (stats) { stats->extends += ext; stats->shadowRays += sh; }
+}
+
+/* per-bounce rays of one sample (diagnostics): rays [maxDepth*6], hits [maxDepth] */
+void or_path_rays(const OScene* s, const OCamera* cam, const OConfig* cfg, uint32_t pixel, uint32_t sampleIndex,
+                  float* rays, int* hits)
+{
+    for (int i = 0; i < 6 * cfg->maxDepth; ++i) rays[i] = NAN;
+    (void)o_renderSample(s, cam, cfg, pixel, sampleIndex, hits, NULL, rays);
 }
 
 /* ------------------------------------------------------------------ */

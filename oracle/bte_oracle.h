@@ -124,6 +124,9 @@ void or_render_samples(const OScene* s, const OCamera* cam, const OConfig* cfg,
                        const uint32_t* pixels, const uint32_t* sampleIndices, int n,
                        float* outRadiance, int* hitLog, OStats* stats, int threads);
 
+void or_path_rays(const OScene* s, const OCamera* cam, const OConfig* cfg, uint32_t pixel, uint32_t sampleIndex,
+                  float* rays, int* hits);
+
 /* Welford running mean (FP32, rt_path_integrator.cuh:72-87) and gamma pack (:93-105). */
 void or_present(float* accum, const float* radiance, int count, uint32_t frameIndex, uint32_t* outRGBA8);
 uint32_t or_pack_gamma(float r, float g, float b);
