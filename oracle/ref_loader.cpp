@@ -1,0 +1,177 @@
+/*
+ * oracle/ref_loader.cpp -- ORACLE (test infrastructure only).
+ *
+ * Loader pin: the reference's own scene.xml parser (src/scene.cpp, compiled
+ * where it lies), its vendored OBJ parser (external/tinyobjloader) and its
+ * transforms (include/mesh_transform.h), glued as src/main.cpp:267-401 and
+ * :629-758 flatten a scene (that glue is restated here because main.cpp also
+ * pulls in the window/GL stack).  Produces the flattened triangle, BSDF and
+ * emitter arrays for comparison with the product's loader.
+ * Built by oracle/Makefile into oracle/_ref/libbteref_loader.so.
+ */
+#include "scene.h"
+#include "mesh_transform.h"
+#define TINYOBJLOADER_IMPLEMENTATION
+#include "tiny_obj_loader.h"
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#define REF_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+std::vector<TriangleData> g_tris;
+std::vector<BsdfData> g_bsdfs;
+std::vector<int> g_triBsdf, g_triMat, g_emTri;
+std::vector<float> g_emCdf, g_sceneCdf, g_cam;
+std::vector<uint8_t> g_flags;
+
+std::string resolve(const std::string& scenePath, const std::string& p)
+{
+    if (p.empty() || p[0] == '/') return p;
+    const size_t s = scenePath.find_last_of('/');
+    return (s == std::string::npos ? std::string() : scenePath.substr(0, s + 1)) + p;
+}
+
+// src/main.cpp:267-401 restated over tinyobjloader and mesh_transform.h
+void loadObj(const std::string& path, const TransformDesc& xf, std::vector<TriangleData>& tris)
+{
+    tinyobj::attrib_t attrib;
+    std::vector<tinyobj::shape_t> shapes;
+    std::vector<tinyobj::material_t> materials;
+    std::string warn, err;
+    tinyobj::LoadObj(&attrib, &shapes, &materials, &warn, &err, path.c_str());
+    auto V = [&](int i) -> Float3 { return {attrib.vertices[3 * i], attrib.vertices[3 * i + 1], attrib.vertices[3 * i + 2]}; };
+    auto N = [&](int i) -> Float3 {
+        if (i < 0 || attrib.normals.empty()) return {0, 0, 0};
+        return {attrib.normals[3 * i], attrib.normals[3 * i + 1], attrib.normals[3 * i + 2]};
+    };
+    auto UV = [&](int i) -> Float2 {
+        if (i < 0 || attrib.texcoords.empty()) return {0, 0};
+        return {attrib.texcoords[2 * i], attrib.texcoords[2 * i + 1]};
+    };
+    const bool realUV = attrib.texcoords.size() > 2;
+    auto planar = [](const Float3& p, const Float3& n) -> Float2 {
+        const float ax = std::fabs(n.x), ay = std::fabs(n.y), az = std::fabs(n.z);
+        if (ay >= ax && ay >= az) return {p.x, p.z};
+        if (ax >= ay && ax >= az) return {p.y, p.z};
+        return {p.x, p.y};
+    };
+    for (const auto& sh : shapes) {
+        const auto& idx = sh.mesh.indices;
+        for (size_t i = 0; i + 2 < idx.size(); i += 3) {
+            const auto a = idx[i], b = idx[i + 1], c = idx[i + 2];
+            TriangleData t{};
+            t.v0 = transformPoint(V(a.vertex_index), xf);
+            t.v1 = transformPoint(V(b.vertex_index), xf);
+            t.v2 = transformPoint(V(c.vertex_index), xf);
+            const bool hasN = a.normal_index >= 0 && b.normal_index >= 0 && c.normal_index >= 0 && !attrib.normals.empty();
+            if (hasN) {
+                t.n0 = transformNormal(N(a.normal_index), xf);
+                t.n1 = transformNormal(N(b.normal_index), xf);
+                t.n2 = transformNormal(N(c.normal_index), xf);
+            } else {
+                const Float3 e1 = {t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z};
+                const Float3 e2 = {t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z};
+                Float3 g = {e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x};
+                const float len = std::sqrt(g.x * g.x + g.y * g.y + g.z * g.z);
+                if (len > 1e-8f) { g.x /= len; g.y /= len; g.z /= len; }
+                t.n0 = t.n1 = t.n2 = g;
+            }
+            if (realUV) { t.uv0 = UV(a.texcoord_index); t.uv1 = UV(b.texcoord_index); t.uv2 = UV(c.texcoord_index); }
+            else { t.uv0 = planar(t.v0, t.n0); t.uv1 = planar(t.v1, t.n0); t.uv2 = planar(t.v2, t.n0); }
+            tris.push_back(t);
+        }
+    }
+}
+
+float area(const TriangleData& t)
+{
+    const float ax = t.v1.x - t.v0.x, ay = t.v1.y - t.v0.y, az = t.v1.z - t.v0.z;
+    const float bx = t.v2.x - t.v0.x, by = t.v2.y - t.v0.y, bz = t.v2.z - t.v0.z;
+    const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    return 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
+}
+}  // namespace
+
+REF_API int refl_load(const char* scenePath)
+{
+    g_tris.clear(); g_bsdfs.clear(); g_triBsdf.clear(); g_triMat.clear(); g_emTri.clear(); g_emCdf.clear();
+    g_sceneCdf.clear(); g_flags.clear(); g_cam.clear();
+    const SceneDescription d = loadSceneDescription(scenePath);   // src/scene.cpp:83
+    for (const auto& b : d.bsdfs) {   // src/main.cpp:629-665
+        BsdfData x{};
+        if (b.type == "diffuse") { x.type = BSDF_Diffuse; x.p0 = {b.albedoR, b.albedoG, b.albedoB, 0.0f}; }
+        else if (b.type == "dielectric") { x.type = BSDF_Dielectric; x.p1 = {b.intIOR, b.extIOR, 0.0f, 0.0f}; }
+        else if (b.type == "mirror") {
+            x.type = BSDF_Mirror;
+            x.p0 = {b.albedoR > 0.0f ? b.albedoR : 1.0f, b.albedoG > 0.0f ? b.albedoG : 1.0f, b.albedoB > 0.0f ? b.albedoB : 1.0f, 0.0f};
+        } else if (b.type == "microfacet") {
+            x.type = BSDF_Microfacet;
+            const float ks = 1.0f - std::fmax(b.albedoR, std::fmax(b.albedoG, b.albedoB));
+            x.p0 = {b.albedoR, b.albedoG, b.albedoB, 0.0f};
+            x.p1 = {b.alpha, b.intIOR, b.extIOR, ks};
+        } else {
+            x.type = BSDF_Disney;
+            x.p0 = {b.baseColorR, b.baseColorG, b.baseColorB, b.roughness};
+            x.p1 = {b.metallic, b.specular, b.specularTransmission, b.specularTint};
+            x.p2 = {b.sheen, b.sheenTint, b.subsurface, b.anisotropic};
+            x.p3 = {b.clearcoat, b.clearcoatGloss, b.eta, 0.0f};
+        }
+        g_bsdfs.push_back(x);
+    }
+    g_sceneCdf.push_back(0.0f);
+    float wsum = 0.0f;
+    for (const auto& m : d.meshes) {   // src/main.cpp:704-758
+        int matId = -1, bsdfId = -1;
+        for (size_t i = 0; i < d.materials.size(); ++i) if (d.materials[i].name == m.materialName) matId = (int)i;
+        for (size_t i = 0; i < d.bsdfs.size(); ++i) if (d.bsdfs[i].name == d.materials[(size_t)matId].bsdfName) bsdfId = (int)i;
+        std::vector<TriangleData> mt;
+        loadObj(resolve(scenePath, m.filename), m.transform, mt);
+        if (m.isEmitter) g_emCdf.push_back(0.0f);
+        float a = 0.0f;
+        for (const auto& t : mt) {
+            g_tris.push_back(t);
+            g_triMat.push_back(matId);
+            g_triBsdf.push_back(bsdfId);
+            g_flags.push_back(m.isEmitter ? 1 : 0);
+            if (m.isEmitter) {
+                a += area(t);
+                g_emTri.push_back((int)g_tris.size() - 1);
+                g_emCdf.push_back(a);
+            }
+        }
+        if (m.isEmitter) {
+            const float lum = 0.2126f * m.radianceR + 0.7152f * m.radianceG + 0.0722f * m.radianceB;
+            wsum += a * lum;
+            g_sceneCdf.push_back(wsum);
+        }
+    }
+    const CameraDesc& c = d.camera;
+    g_cam = {c.eyeX, c.eyeY, c.eyeZ, c.lookAtX, c.lookAtY, c.lookAtZ, c.upX, c.upY, c.upZ, c.fovYDegrees,
+             (float)d.windowWidth, (float)d.windowHeight, d.envMapIntensity, d.envMapRotation, (float)d.spotlights.size()};
+    return (int)g_tris.size();
+}
+
+REF_API int refl_counts(int* out)
+{
+    out[0] = (int)g_tris.size(); out[1] = (int)g_bsdfs.size(); out[2] = (int)g_emTri.size();
+    out[3] = (int)g_emCdf.size(); out[4] = (int)g_sceneCdf.size(); out[5] = (int)g_cam.size();
+    return 0;
+}
+
+REF_API void refl_copy(TriangleData* tris, BsdfData* bsdfs, int* triBsdf, int* triMat, uint8_t* flags, int* emTri,
+                       float* emCdf, float* sceneCdf, float* cam)
+{
+    std::memcpy(tris, g_tris.data(), g_tris.size() * sizeof(TriangleData));
+    std::memcpy(bsdfs, g_bsdfs.data(), g_bsdfs.size() * sizeof(BsdfData));
+    std::memcpy(triBsdf, g_triBsdf.data(), g_triBsdf.size() * sizeof(int));
+    std::memcpy(triMat, g_triMat.data(), g_triMat.size() * sizeof(int));
+    std::memcpy(flags, g_flags.data(), g_flags.size());
+    std::memcpy(emTri, g_emTri.data(), g_emTri.size() * sizeof(int));
+    std::memcpy(emCdf, g_emCdf.data(), g_emCdf.size() * sizeof(float));
+    std::memcpy(sceneCdf, g_sceneCdf.data(), g_sceneCdf.size() * sizeof(float));
+    std::memcpy(cam, g_cam.data(), g_cam.size() * sizeof(float));
+}
