@@ -38,3 +38,30 @@ def test_pod_layouts_match_reference(bte):
     assert bte.EMITTER_DTYPE.itemsize == 32      # render_kernel.h:44-51
     assert bte.SPOT_DTYPE.itemsize == 48         # render_kernel.h:56-63
     assert np.dtype(bte.RenderConfig).itemsize if hasattr(np, "dtype") else True
+
+
+REFERENCE_NAMES = ["cudaInitOptix", "cudaInitScene", "cudaInit", "cudaInitCamera", "cudaInitTriangleEmission",
+                   "cudaInitTriangleEmitterFlags", "cudaInitEmitterTable", "cudaInitBsdfs", "cudaInitSpotlights",
+                   "cudaInitTextures", "cudaInitMrTextures", "cudaInitEnvMap", "cudaRegisterPBO",
+                   "cudaResetAccumulation", "cudaRender", "cudaToggleDenoiser", "cudaSetRenderMode",
+                   "cudaGetRenderMode", "cudaCleanup"]
+
+
+def test_reference_named_cpp_api_links(bte, tmp_path):
+    """A caller written against the reference's render_kernel.h (include/render_kernel.h:100-211)
+    compiles against bte/render_kernel.h and links with libbte_b200.so."""
+    src = tmp_path / "caller.cpp"
+    src.write_text('#include "bte/render_kernel.h"\n'
+                   'int main(int argc, char**) {\n'
+                   '  if (argc > 5) {\n'
+                   '    CameraData c{}; cudaInitCamera(c); cudaInitScene(nullptr, 0, nullptr, 0, nullptr, 8, 8);\n'
+                   '    cudaInitOptix(); cudaInitEnvMap(nullptr, 0, 0, 0.f, 0.f); cudaSetRenderMode(RenderMode::Wavefront);\n'
+                   '    cudaResetAccumulation(8, 8); cudaRender(8, 8); (void)cudaGetRenderMode(); cudaCleanup();\n'
+                   '  }\n  return 0;\n}\n')
+    lib = bte.library_path()
+    r = subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(tmp_path / "a.out"),
+                        lib, "-Wl,-rpath," + os.path.dirname(lib)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
+    for name in REFERENCE_NAMES:
+        assert name + "(" in out, name
