@@ -11,8 +11,13 @@
 // linear-time construction, IEEE TSE 17(9) 1991), plus the per-pixel discrete
 // probability used for MIS.  Sampling is then O(1) per NEE instead of two
 // binary searches.
+#include "bte_internal.h"
 #include "bte_kernels.h"
 #include "bte_math.cuh"
+
+#include <cstdint>
+#include <mutex>
+#include <string>
 
 namespace bte {
 
@@ -167,3 +172,117 @@ done:
 }
 
 }  // namespace bte
+
+// ---------------------------------------------------------------- no-allocation variant
+//
+// bte_env_build_alias_noalloc builds the same FP64 alias tables as the
+// allocating path above, but never calls cudaMalloc/cudaFree (or anything that
+// allocates).  It exists for callers that cannot allocate device memory at the
+// moment they need new tables: a render loop that swaps environment maps
+// between frames (cudaMalloc and cudaFree synchronise the whole device and
+// would stall the frames already queued), and host applications that reserve
+// all device memory for their own pool up front, leaving nothing for a
+// library to allocate from.  The caller owns the input texels and every output
+// table; the intermediate FP64 weights, row sums and Vose work lists live in
+// one file-scope device array of fixed size, so maps are limited to
+// kNoAllocMaxTexels texels and kNoAllocMaxRows rows.
+//
+// The array is shared by every call in the process: two calls whose kernels
+// overlap on the GPU (different streams, or different host threads on one
+// device) race on it and produce garbage; serialise them.  Nothing in it has
+// to start at zero -- every scratch word is written before it is read -- and
+// it keeps whatever the last call left there.  Each device that loads the
+// library holds the array until the process exits.
+namespace bte {
+namespace {
+
+constexpr int kNoAllocMaxTexels = 512 * 256;
+constexpr int kNoAllocMaxRows = 4096;
+constexpr size_t kAlign = 256;
+constexpr size_t alignUp(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+// layout: weights [texels] double | row sums [rows] double | work ints [2*texels] | work doubles [texels]
+constexpr size_t kOffWeights = 0;
+constexpr size_t kOffRowSum = alignUp(kOffWeights + sizeof(double) * kNoAllocMaxTexels);
+constexpr size_t kOffWorkI = alignUp(kOffRowSum + sizeof(double) * kNoAllocMaxRows);
+constexpr size_t kOffWorkD = alignUp(kOffWorkI + sizeof(int) * 2 * kNoAllocMaxTexels);
+constexpr size_t kNoAllocScratchBytes = alignUp(kOffWorkD + sizeof(double) * kNoAllocMaxTexels);
+
+static __device__ __align__(256) unsigned char g_envAliasScratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_scratchAddr[kMaxDevices] = {};
+std::mutex g_scratchMutex;
+
+// Device address of g_envAliasScratch on the current device, looked up once per
+// device (the host-side symbol is a stand-in, not a device address).
+int scratchForCurrentDevice(unsigned char** out, std::string& err)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { err = std::string("cudaGetDevice: ") + cudaGetErrorString(e); return -1; }
+    if (dev < 0 || dev >= kMaxDevices) { err = "device ordinal out of range"; return -1; }
+    std::lock_guard<std::mutex> lk(g_scratchMutex);
+    if (!g_scratchAddr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_envAliasScratch);
+        if (e != cudaSuccess || !p) {
+            err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+            return -1;
+        }
+        g_scratchAddr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_scratchAddr[dev];
+    return 0;
+}
+
+}  // namespace
+
+}  // namespace bte
+
+extern "C" int bte_env_build_alias_noalloc(const float* dTexelsRGBA, int width, int height, float* dRowProb,
+                                           int* dRowAlias, float* dColProb, int* dColAlias, float* dPixelPdf,
+                                           double* dTotalPower, void* stream)
+{
+    using namespace bte;
+    if (!dTexelsRGBA || !dRowProb || !dRowAlias || !dColProb || !dColAlias || !dPixelPdf || !dTotalPower) {
+        setError("bte_env_build_alias_noalloc: null pointer argument");
+        return -1;
+    }
+    if (width <= 0 || height <= 0) {
+        setError("bte_env_build_alias_noalloc: width and height must be positive");
+        return -1;
+    }
+    if (static_cast<long long>(width) * height > kNoAllocMaxTexels || height > kNoAllocMaxRows) {
+        setError("bte_env_build_alias_noalloc: " + std::to_string(width) + "x" + std::to_string(height) +
+                 " exceeds the fixed scratch of this entry point (at most " + std::to_string(kNoAllocMaxTexels) +
+                 " texels and " + std::to_string(kNoAllocMaxRows) + " rows); use bte_init_env_map for larger maps");
+        return -1;
+    }
+    if (reinterpret_cast<uintptr_t>(dTexelsRGBA) % 16 != 0) {
+        setError("bte_env_build_alias_noalloc: texels must be 16-byte aligned (float4 per texel)");
+        return -1;
+    }
+    unsigned char* base = nullptr;
+    std::string err;
+    if (scratchForCurrentDevice(&base, err) != 0) {
+        setError("bte_env_build_alias_noalloc: " + err);
+        return -1;
+    }
+    double* wt = reinterpret_cast<double*>(base + kOffWeights);
+    double* rowSum = reinterpret_cast<double*>(base + kOffRowSum);
+    int* workI = reinterpret_cast<int*>(base + kOffWorkI);
+    double* workD = reinterpret_cast<double*>(base + kOffWorkD);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float4* tex = reinterpret_cast<const float4*>(dTexelsRGBA);
+    kEnvWeights<<<(height + 127) / 128, 128, 0, st>>>(tex, width, height, wt, rowSum);
+    kEnvTotal<<<1, 1, 0, st>>>(rowSum, height, dTotalPower);
+    kEnvAliasRows<<<(height + 127) / 128, 128, 0, st>>>(wt, rowSum, width, height, dTotalPower, dColProb, dColAlias,
+                                                        dPixelPdf, workI, workD);
+    kEnvAliasMarginal<<<1, 1, 0, st>>>(rowSum, height, dTotalPower, dRowProb, dRowAlias, workI, workD);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        setError(std::string("bte_env_build_alias_noalloc: ") + cudaGetErrorString(e));
+        return -1;
+    }
+    return 0;
+}

@@ -121,6 +121,23 @@ int bte_bsdf_query(const BsdfData* bsdf, int op, const float* wi, const float* w
 /* hardware texture fetch vs the library's software filter, for the texture-filter pin */
 int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* uv, int n, float* outHw, float* outSw);
 
+/* ---- env-map alias tables without allocation ----
+ * No counterpart in the reference.  Builds the same FP64 alias tables and
+ * per-pixel pdf that bte_init_env_map builds, for a caller that cannot
+ * allocate device memory at that point (cudaMalloc/cudaFree synchronise the
+ * whole device; some hosts reserve all device memory for their own pool).
+ * Inputs and outputs are the caller's device buffers: dTexelsRGBA is
+ * width*height float4 texels (16-byte aligned), outputs are rowProb/rowAlias
+ * [height], colProb/colAlias/pixelPdf [width*height] and the FP64 total
+ * weight [1].  Work is queued on `stream` (0 = default stream) and nothing is
+ * allocated: the intermediates live in one fixed device array, so maps are
+ * limited to 131072 texels (e.g. 512x256) and 4096 rows; larger sizes return
+ * an error.  The first call on a device looks up that array's address (make it
+ * before any stream capture).  All calls share the array: calls whose kernels
+ * overlap on the GPU race and must be serialised by the caller. */
+int bte_env_build_alias_noalloc(const float* dTexelsRGBA, int width, int height, float* dRowProb, int* dRowAlias,
+                                float* dColProb, int* dColAlias, float* dPixelPdf, double* dTotalPower, void* stream);
+
 /* ---- scene.xml / OBJ loader (src/scene.cpp:83-523, src/main.cpp:267-930) ---- */
 typedef struct BteScene BteScene;
 typedef struct {
