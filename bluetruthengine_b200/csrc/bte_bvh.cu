@@ -9,7 +9,9 @@
 //   4. hierarchy from the sorted codes (T. Karras, "Maximizing Parallelism in
 //      the Construction of BVHs, Octrees, and k-d Trees", HPG 2012), equal
 //      codes separated by their index
-//   5. bottom-up refit with one atomic arrival counter per node
+//   5. bottom-up refit with one atomic arrival counter per node, with a
+//      surface-area cost decision collapsing small subtrees (contiguous
+//      ranges of the sorted triangles) into multi-triangle leaves
 //   6. output: 64-byte BVH2 nodes holding both child boxes, and the triangles
 //      in leaf order as three float4 each (v0|original index, v1, v2)
 // All integer steps are deterministic; the result does not depend on thread
@@ -199,7 +201,7 @@ __device__ __forceinline__ int delta(const unsigned long long* keys, int n, int 
 
 // internal node i in [0, n-2]; children encoded >= 0 internal, < 0 leaf ~k
 __global__ void kKarras(const unsigned long long* __restrict__ keys, int n, int2* children, int* parentInner,
-                        int* parentLeaf)
+                        int* parentLeaf, int2* range)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -228,6 +230,7 @@ __global__ void kKarras(const unsigned long long* __restrict__ keys, int n, int2
     if (hi == gamma + 1) { right = ~(gamma + 1); parentLeaf[gamma + 1] = i; }
     else { right = gamma + 1; parentInner[gamma + 1] = i; }
     children[i] = make_int2(left, right);
+    range[i] = make_int2(lo, hi);
     if (i == 0) parentInner[0] = -1;
 }
 
@@ -244,10 +247,23 @@ __device__ __forceinline__ Box triBox(const TriangleData& t)
 
 // leaf k (sorted position) -> leaf triangle data + its box; walks up and
 // fills the inner nodes' boxes (second arrival computes the union).
+// Surface-area cost model for collapsing subtrees into leaves: a node becomes
+// a leaf of its whole (contiguous) triangle range when that is no costlier
+// than keeping the split (kCostTrav per node visit, kCostIsect per triangle).
+constexpr float kCostTrav = 1.2f;
+constexpr float kCostIsect = 1.0f;
+
+__device__ __forceinline__ float halfArea(const float* b)
+{
+    const float dx = fmaxf(b[3] - b[0], 0.0f), dy = fmaxf(b[4] - b[1], 0.0f), dz = fmaxf(b[5] - b[2], 0.0f);
+    return dx * dy + dy * dz + dz * dx;
+}
+
 __global__ void kRefit(const TriangleData* __restrict__ tris, const int* __restrict__ sortedTri, int n,
                        const int2* __restrict__ children, const int* __restrict__ parentInner,
-                       const int* __restrict__ parentLeaf, float4* leafTris, float* innerBox /*[n-1][6]*/,
-                       float* leafBox /*[n][6]*/, int* arrivals)
+                       const int* __restrict__ parentLeaf, const int2* __restrict__ range, float4* leafTris,
+                       float* innerBox /*[n-1][6]*/, float* leafBox /*[n][6]*/, int* arrivals, float* cost,
+                       int* collapsed, int maxLeaf)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -271,15 +287,30 @@ __global__ void kRefit(const TriangleData* __restrict__ tris, const int* __restr
         const float* pb = (c.y >= 0) ? innerBox + 6 * static_cast<size_t>(c.y) : leafBox + 6 * static_cast<size_t>(~c.y);
         for (int q = 0; q < 6; ++q) { a[q] = __ldcg(pa + q); bb[q] = __ldcg(pb + q); }
         float* out = innerBox + 6 * static_cast<size_t>(node);
-        out[0] = fminf(a[0], bb[0]); out[1] = fminf(a[1], bb[1]); out[2] = fminf(a[2], bb[2]);
-        out[3] = fmaxf(a[3], bb[3]); out[4] = fmaxf(a[4], bb[4]); out[5] = fmaxf(a[5], bb[5]);
+        float u[6];
+        u[0] = fminf(a[0], bb[0]); u[1] = fminf(a[1], bb[1]); u[2] = fminf(a[2], bb[2]);
+        u[3] = fmaxf(a[3], bb[3]); u[4] = fmaxf(a[4], bb[4]); u[5] = fmaxf(a[5], bb[5]);
+        for (int q = 0; q < 6; ++q) out[q] = u[q];
+        const float cl = (c.x >= 0) ? __ldcg(cost + c.x) : kCostIsect;
+        const float cr = (c.y >= 0) ? __ldcg(cost + c.y) : kCostIsect;
+        const float A = halfArea(u);
+        const float split = (A > 0.0f) ? kCostTrav + (halfArea(a) * cl + halfArea(bb) * cr) / A : kCostTrav + cl + cr;
+        const int2 rg = range[node];
+        const int cnt = rg.y - rg.x + 1;
+        const float leafCost = kCostIsect * static_cast<float>(cnt);
+        const bool col = cnt <= maxLeaf && leafCost <= split;
+        cost[node] = col ? leafCost : split;
+        collapsed[node] = col ? 1 : 0;
         __threadfence();
         node = parentInner[node];
     }
 }
 
+__device__ __forceinline__ int leafCode(int start, int count) { return ~(start | ((count - 1) << kLeafCountShift)); }
+
 __global__ void kEmitNodes(const int2* __restrict__ children, const float* __restrict__ innerBox,
-                           const float* __restrict__ leafBox, int n, BvhNode* nodes)
+                           const float* __restrict__ leafBox, const int2* __restrict__ range,
+                           const int* __restrict__ collapsed, int n, BvhNode* nodes)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -290,8 +321,10 @@ __global__ void kEmitNodes(const int2* __restrict__ children, const float* __res
     nd.lxy = make_float4(a[0], a[3], a[1], a[4]);
     nd.rxy = make_float4(b[0], b[3], b[1], b[4]);
     nd.z = make_float4(a[2], a[5], b[2], b[5]);
-    // leaf children hold one triangle: ~(start | (1-1) << 25) == ~start
-    nd.child = make_int4(c.x, c.y, 0, 0);
+    int e0 = c.x, e1 = c.y;   // ~k is already the leaf code of a single triangle
+    if (c.x >= 0 && collapsed[c.x]) e0 = leafCode(range[c.x].x, range[c.x].y - range[c.x].x + 1);
+    if (c.y >= 0 && collapsed[c.y]) e1 = leafCode(range[c.y].x, range[c.y].y - range[c.y].x + 1);
+    nd.child = make_int4(e0, e1, 0, 0);
     nodes[i] = nd;
 }
 
@@ -299,18 +332,21 @@ __global__ void kEmitNodes(const int2* __restrict__ children, const float* __res
 
 #define BVH_CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { err = std::string("LBVH build: ") + cudaGetErrorString(e_); goto fail; } } while (0)
 
-int buildLbvh(const TriangleData* dTris, int n, BvhBuildResult& out, cudaStream_t st, std::string& err)
+int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, BvhBuildResult& out, cudaStream_t st, std::string& err)
 {
     out = BvhBuildResult{};
     if (n <= 0) return 0;
     if (n > kLeafStartMask) { err = "LBVH build: too many triangles for the leaf encoding"; return -1; }
+    if (maxLeaf < 1) maxLeaf = 1;
+    if (maxLeaf > kMaxLeafTris) maxLeaf = kMaxLeafTris;
     float4* cen = nullptr;
     unsigned int* bounds = nullptr;
     unsigned long long *keysA = nullptr, *keysB = nullptr;
     int *valsA = nullptr, *valsB = nullptr, *hist = nullptr;
     int2* children = nullptr;
-    int *parentInner = nullptr, *parentLeaf = nullptr, *arrivals = nullptr;
-    float *innerBox = nullptr, *leafBox = nullptr;
+    int *parentInner = nullptr, *parentLeaf = nullptr, *arrivals = nullptr, *collapsed = nullptr;
+    float *innerBox = nullptr, *leafBox = nullptr, *cost = nullptr;
+    int2* range = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     const int numTiles = (n + kSortTile - 1) / kSortTile;
     const int inner = n > 1 ? n - 1 : 1;
@@ -329,6 +365,9 @@ int buildLbvh(const TriangleData* dTris, int n, BvhBuildResult& out, cudaStream_
         BVH_CK(cudaMalloc(&parentInner, sizeof(int) * inner));
         BVH_CK(cudaMalloc(&parentLeaf, sizeof(int) * n));
         BVH_CK(cudaMalloc(&arrivals, sizeof(int) * inner));
+        BVH_CK(cudaMalloc(&collapsed, sizeof(int) * inner));
+        BVH_CK(cudaMalloc(&cost, sizeof(float) * inner));
+        BVH_CK(cudaMalloc(&range, sizeof(int2) * inner));
         BVH_CK(cudaMalloc(&innerBox, sizeof(float) * 6 * inner));
         BVH_CK(cudaMalloc(&leafBox, sizeof(float) * 6 * n));
         BVH_CK(cudaMalloc(&out.leafTris, sizeof(float4) * 3 * static_cast<size_t>(n)));
@@ -351,26 +390,34 @@ int buildLbvh(const TriangleData* dTris, int n, BvhBuildResult& out, cudaStream_
             int* tv = vin; vin = vout; vout = tv;
         }
         if (n > 1) {
-            kKarras<<<(n - 1 + B - 1) / B, B, 0, st>>>(kin, n, children, parentInner, parentLeaf);
+            kKarras<<<(n - 1 + B - 1) / B, B, 0, st>>>(kin, n, children, parentInner, parentLeaf, range);
         }
-        kRefit<<<G, B, 0, st>>>(dTris, vin, n, children, parentInner, parentLeaf, out.leafTris, innerBox, leafBox, arrivals);
-        if (n > 1) kEmitNodes<<<(n - 1 + B - 1) / B, B, 0, st>>>(children, innerBox, leafBox, n, out.nodes);
+        kRefit<<<G, B, 0, st>>>(dTris, vin, n, children, parentInner, parentLeaf, range, out.leafTris, innerBox, leafBox,
+                                arrivals, cost, collapsed, maxLeaf);
+        if (n > 1) kEmitNodes<<<(n - 1 + B - 1) / B, B, 0, st>>>(children, innerBox, leafBox, range, collapsed, n, out.nodes);
         BVH_CK(cudaGetLastError());
         BVH_CK(cudaEventRecord(e1, st));
         BVH_CK(cudaEventSynchronize(e1));
         BVH_CK(cudaEventElapsedTime(&out.msBuild, e0, e1));
         out.nodeCount = n > 1 ? n - 1 : 0;
         out.rootIsLeaf = n == 1 ? 1 : 0;
+        out.rootCode = ~0;
+        if (n > 1) {   // a scene small enough to be one leaf
+            int rootCollapsed = 0;
+            BVH_CK(cudaMemcpyAsync(&rootCollapsed, collapsed, sizeof(int), cudaMemcpyDeviceToHost, st));
+            BVH_CK(cudaStreamSynchronize(st));
+            if (rootCollapsed) { out.rootIsLeaf = 1; out.rootCode = ~((n - 1) << kLeafCountShift); }
+        }
     }
     cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
     cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
-    cudaFree(leafBox);
+    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range);
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     return 0;
 fail:
     cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
     cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
-    cudaFree(leafBox);
+    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range);
     cudaFree(out.leafTris); cudaFree(out.nodes);
     out = BvhBuildResult{};
     if (e0) cudaEventDestroy(e0);

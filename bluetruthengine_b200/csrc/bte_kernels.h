@@ -32,9 +32,11 @@ struct BvhBuildResult {
     float4* leafTris = nullptr;
     int nodeCount = 0;
     int rootIsLeaf = 0;
+    int rootCode = ~0;      // leaf code of the root when rootIsLeaf
     float msBuild = 0.0f;
 };
-int buildLbvh(const TriangleData* dTris, int triCount, BvhBuildResult& out, cudaStream_t st, std::string& err);
+int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, BvhBuildResult& out, cudaStream_t st,
+              std::string& err);
 
 // Env-map tables (bte_env.cu).
 int buildEnvCdf(const float4* dTexels, int w, int h, const float* hSinTheta, float* dMarginal, float* dConditional,

@@ -278,6 +278,40 @@ BTE_HD float powf_(float x, float y)
     if (l < -104.0) return sign * 0.0f;
     return sign * static_cast<float>(expD(l));
 }
+// x^5 and x^2 for the reference's powf(x, 5) / powf(x, 2) call sites: the
+// double products (x*x exact, then two rounded products) carry relative error
+// < 3e-16, so the single rounding to float gives the correctly rounded power
+// except in vanishingly rare near-halfway cases; special values follow C99
+// pow for odd/even integer exponents.
+BTE_HD float pow5f_(float x)
+{
+    const double d = static_cast<double>(x);
+    const double d2 = d * d;
+    const double d4 = d2 * d2;
+    return static_cast<float>(d4 * d);
+}
+BTE_HD float pow2f_(float x)
+{
+    const double d = static_cast<double>(x);
+    return static_cast<float>(d * d);
+}
+// sin and cos of one argument with a single reduction; bit-identical to
+// sinf_(x) and cosf_(x).
+BTE_HD void sincosf_(float x, float& s, float& c)
+{
+    if (isnanf_(x)) { s = x + x * 0.0f; c = x; return; }
+    if (isinff_(x)) { s = NAN; c = NAN; return; }
+    if (x == 0.0f) { s = x + x * 0.0f; c = static_cast<float>(cosD(static_cast<double>(x))); return; }
+    int q;
+    const double r = reducePio2(static_cast<double>(x), q);
+    const double sp = sinPoly(r), cp = cosPoly(r);
+    switch (q) {
+    case 0: s = static_cast<float>(sp); c = static_cast<float>(cp); break;
+    case 1: s = static_cast<float>(cp); c = static_cast<float>(-sp); break;
+    case 2: s = static_cast<float>(-sp); c = static_cast<float>(-cp); break;
+    default: s = static_cast<float>(-cp); c = static_cast<float>(sp); break;
+    }
+}
 BTE_HD float atan2f_(float y, float x)
 {
     if (isnanf_(x) || isnanf_(y)) return NAN;

@@ -86,7 +86,8 @@ struct Renderer {
     bool hasEnv = false;
     // acceleration structure
     DeviceBuffer bvhNodes, leafTris;
-    int rootIsLeaf = 0;
+    int rootIsLeaf = 0, rootCode = ~0;
+    int maxLeaf = 8;
     bool accelReady = false;
     float msBvh = 0.0f;
     // camera / frame
@@ -134,6 +135,7 @@ DevScene makeDevScene()
     s.leafTris = g.leafTris.as<float4>();
     s.nodes = g.bvhNodes.as<BvhNode>();
     s.rootIsLeaf = g.rootIsLeaf;
+    s.rootCode = g.rootCode;
     s.sceneMaxAbs = g.sceneMaxAbs;
     s.bsdfs = g.bsdfs.as<BsdfData>();
     s.triBsdfIds = g.triBsdfIds.as<int>();
@@ -412,10 +414,11 @@ int bte_init_accel(void)
         if (!g.tris.p || g.triCount <= 0) throw CudaError{"bte_init_accel: call bte_init_scene first"};
         BvhBuildResult r;
         std::string err;
-        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, r, g.stream, err) != 0) throw CudaError{err};
+        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, r, g.stream, err) != 0) throw CudaError{err};
         g.bvhNodes.p = r.nodes; g.bvhNodes.bytes = sizeof(BvhNode) * (r.nodeCount > 0 ? r.nodeCount : 1);
         g.leafTris.p = r.leafTris; g.leafTris.bytes = sizeof(float4) * 3 * static_cast<size_t>(g.triCount);
         g.rootIsLeaf = r.rootIsLeaf;
+        g.rootCode = r.rootCode;
         g.msBvh = r.msBuild;
         g.accelReady = true;
         return 0;

@@ -164,7 +164,9 @@ BTE_DI V3 sqCosHemi(float u1, float u2)
 {
     const float r = sqrtf(fmaxf(u1, 0.0f));
     const float phi = 2.0f * kPiF * u2;
-    return v3(r * m::cosf_(phi), r * m::sinf_(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
+    float sp, cp;
+    m::sincosf_(phi, sp, cp);
+    return v3(r * cp, r * sp, sqrtf(fmaxf(0.0f, 1.0f - u1)));
 }
 // rt_bsdf_diffuse.cuh:27-62
 BTE_DI V3 evalDiffuse(const Bsdf& b, const BRec& r)
@@ -244,7 +246,9 @@ BTE_DI V3 sqBeckmann(float u1, float u2, float alpha)
     const float tan2 = -alpha * alpha * m::logf_(fmaxf(1.0e-6f, 1.0f - u1));
     const float c = 1.0f / sqrtf(1.0f + tan2);
     const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
-    return v3(s * m::cosf_(phi), s * m::sinf_(phi), c);
+    float sp, cp;
+    m::sincosf_(phi, sp, cp);
+    return v3(s * cp, s * sp, c);
 }
 BTE_DI float sqBeckmannPdf(V3 mm, float alpha)
 {
@@ -313,7 +317,7 @@ BTE_DI V3 sampleMicrofacet(const Bsdf& b, BRec& r, float u1, float u2)
 // ---- Disney: rt_bsdf_disney.cuh:16-892 ----
 BTE_DI V3 dBase(const Bsdf& b) { return v3(b.p0.x, b.p0.y, b.p0.z); }
 BTE_DI V3 dSqrt3(V3 c) { return v3(sqrtf(fmaxf(0.0f, c.x)), sqrtf(fmaxf(0.0f, c.y)), sqrtf(fmaxf(0.0f, c.z))); }
-BTE_DI float dDiffF(float c, float f90) { return 1.0f + ((f90 - 1.0f) * m::powf_(1.0f - c, 5)); }
+BTE_DI float dDiffF(float c, float f90) { return 1.0f + ((f90 - 1.0f) * m::pow5f_(1.0f - c)); }
 BTE_DI V3 evalDiffuseLobe(const Bsdf& b, const BRec& r)            // :59-104
 {
     const float ci = r.wi.z, co = r.wo.z;
@@ -344,13 +348,13 @@ BTE_DI V3 fresnelMetal(const Bsdf& b, float hDotWo)                // :157-184
     const V3 sp = v3((1.0f - st) + (st * tint.x), (1.0f - st) + (st * tint.y), (1.0f - st) + (st * tint.z));
     const float coef = b.p1.y * schlickF0(b.p3.z) * (1.0f - b.p1.x);
     const V3 clr = v3((coef * sp.x) + (bc.x * b.p1.x), (coef * sp.y) + (bc.y * b.p1.x), (coef * sp.z) + (bc.z * b.p1.x));
-    const float sch = m::powf_(1.0f - hDotWo, 5);
+    const float sch = m::pow5f_(1.0f - hDotWo);
     return v3(clr.x + ((1.0f - clr.x) * sch), clr.y + ((1.0f - clr.y) * sch), clr.z + ((1.0f - clr.z) * sch));
 }
 BTE_DI float ggxD(V3 wh, float ax, float ay)                        // :186-192
 {
     const float den = kPiF * ax * ay *
-                      m::powf_(((wh.x * wh.x) / (ax * ax)) + ((wh.y * wh.y) / (ay * ay)) + (wh.z * wh.z), 2);
+                      m::pow2f_(((wh.x * wh.x) / (ax * ax)) + ((wh.y * wh.y) / (ay * ay)) + (wh.z * wh.z));
     return 1.0f / den;
 }
 BTE_DI float lambdaG(V3 w, float ax, float ay)                      // :194-204
@@ -399,8 +403,10 @@ BTE_DI V3 vndf(V3 w, float ax, float ay, float u1, float u2)        // :293-317 
     const V3 o2 = cross3(vh, o1);
     const float radius = sqrtf(u1);
     const float phi = 2.0f * kPiF * u2;
-    const float t1 = radius * m::cosf_(phi);
-    float t2 = radius * m::sinf_(phi);
+    float sphi, cphi;
+    m::sincosf_(phi, sphi, cphi);
+    const float t1 = radius * cphi;
+    float t2 = radius * sphi;
     const float skew = 0.5f * (1.0f + vh.z);
     t2 = (1.0f - skew) * sqrtf(1.0f - (t1 * t1)) + (skew * t2);
     const V3 ph = add3(add3(mul3(o1, t1), mul3(o2, t2)), mul3(vh, sqrtf(fmaxf(0.0f, 1 - (t1 * t1) - (t2 * t2)))));
@@ -433,7 +439,7 @@ BTE_DI V3 evalClearLobe(const Bsdf& b, const BRec& r)               // :370-394
     const V3 wh = normalize3(add3(r.wi, r.wo));
     const float hDotWo = fabsf(dot3(wh, r.wo));
     const float rr = static_cast<float>(0.04);
-    const float fc = rr + ((1.0f - rr) * m::powf_(1.0f - hDotWo, 5));
+    const float fc = rr + ((1.0f - rr) * m::pow5f_(1.0f - hDotWo));
     const float dc = clearD(b, wh);
     const float gc = lambdaG(r.wi, 0.25f, 0.25f) * lambdaG(r.wo, 0.25f, 0.25f);
     const float den = 4.0f * ci;
@@ -459,8 +465,10 @@ BTE_DI V3 sampleClearLobe(const Bsdf& b, BRec& r, float u1, float u2)   // :417-
     const float ce2 = (1.0f - m::powf_(ir2, 1.0f - u2)) / (1.0f - ir2);
     const float se = sqrtf(1.0f - ce2);
     const float hz = sqrtf(ce2);
-    const float hy = se * m::sinf_(az);
-    const float hx = se * m::cosf_(az);
+    float saz, caz;
+    m::sincosf_(az, saz, caz);
+    const float hy = se * saz;
+    const float hx = se * caz;
     const V3 wh = normalize3(v3(hx, hy, hz));
     r.wo = sub3(mul3(wh, 2.0f * dot3(r.wi, wh)), r.wi);
     r.eta = 1.0f;
@@ -501,7 +509,7 @@ BTE_DI V3 evalGlassLobe(const Bsdf& b, const BRec& r)               // :475-532
         return div3(num, den);
     }
     const V3 num = mul3(dSqrt3(dBase(b)), (1.0f - fg) * dg * gg * fabsf(hDotWi * hDotWo));
-    const float den = fabsf(ci) * fmaxf(m::powf_(hDotWi + eho, 2), 1e-4f);
+    const float den = fabsf(ci) * fmaxf(m::pow2f_(hDotWi + eho), 1e-4f);
     return div3(num, den);
 }
 BTE_DI float pdfGlassLobe(const Bsdf& b, const BRec& r)             // :535-588
@@ -518,7 +526,7 @@ BTE_DI float pdfGlassLobe(const Bsdf& b, const BRec& r)             // :535-588
     const float gg = lambdaG(r.wi, ax, ay);
     const float common = (dg * gg * fabsf(hDotWi)) / fabsf(ci);
     if (inNout > 0.0f) return (common * fg) / (4.0f * fabsf(hDotWo));
-    const float jac = (eta * eta * fabsf(hDotWo)) / fmaxf(m::powf_(hDotWi + (eta * hDotWo), 2), 1e-4f);
+    const float jac = (eta * eta * fabsf(hDotWo)) / fmaxf(m::pow2f_(hDotWi + (eta * hDotWo)), 1e-4f);
     return (1.0f - fg) * common * jac;
 }
 BTE_DI V3 sampleGlassLobe(const Bsdf& b, BRec& r, float u1, float u2)   // :591-674
@@ -559,7 +567,7 @@ BTE_DI V3 evalSheenLobe(const Bsdf& b, const BRec& r)               // :679-709
     if (lumi > 0) tint = div3(bc, lumi);
     const float st = b.p2.y;
     const V3 sh = v3((1.0f - st) + (st * tint.x), (1.0f - st) + (st * tint.y), (1.0f - st) + (st * tint.z));
-    return mul3(sh, m::powf_(1.0f - hDotWo, 5) * co);
+    return mul3(sh, m::pow5f_(1.0f - hDotWo) * co);
 }
 BTE_DI V3 evalDisney(const Bsdf& b, const BRec& r)                  // :758-787
 {
@@ -630,7 +638,7 @@ BTE_DI V3 sampleDisney(const Bsdf& b, BRec& r, float u1, float u2)  // :823-892
 }
 
 // dispatch, rt_bsdf.cuh:42-84
-BTE_DI V3 bsdfEval(const Bsdf& b, const BRec& r)
+__device__ __noinline__ V3 bsdfEval(const Bsdf& b, const BRec& r)
 {
     switch (b.type) {
     case BSDF_Diffuse: return evalDiffuse(b, r);
@@ -639,7 +647,7 @@ BTE_DI V3 bsdfEval(const Bsdf& b, const BRec& r)
     default: return v3(0, 0, 0);
     }
 }
-BTE_DI float bsdfPdf(const Bsdf& b, const BRec& r)
+__device__ __noinline__ float bsdfPdf(const Bsdf& b, const BRec& r)
 {
     switch (b.type) {
     case BSDF_Diffuse: return pdfDiffuse(r);
@@ -648,7 +656,7 @@ BTE_DI float bsdfPdf(const Bsdf& b, const BRec& r)
     default: return 0.0f;
     }
 }
-BTE_DI V3 bsdfSample(const Bsdf& b, BRec& r, float u1, float u2)
+__device__ __noinline__ V3 bsdfSample(const Bsdf& b, BRec& r, float u1, float u2)
 {
     switch (b.type) {
     case BSDF_Diffuse: return sampleDiffuse(b, r, u1, u2);
@@ -708,8 +716,10 @@ BTE_DI V3 equirectToDir(float u, float v, float rot)
 {
     const float phi = u * 2.0f * kMPI - kMPI - rot;
     const float theta = v * kMPI;
-    const float st = m::sinf_(theta);
-    return normalize3(v3(st * m::cosf_(phi), m::cosf_(theta), st * m::sinf_(phi)));
+    float st, ct, sp, cp;
+    m::sincosf_(theta, st, ct);
+    m::sincosf_(phi, sp, cp);
+    return normalize3(v3(st * cp, ct, st * sp));
 }
 BTE_DI V3 envTex(const DevEnv& e, float u, float v)
 {

@@ -28,6 +28,7 @@ struct RayPre {
     float Sx, Sy, Sz;
     float ix, iy, iz;     // reciprocal direction for the slab test (zeros replaced by +-1e-30)
     float px, py, pz;     // per-slab widening in t units
+    float nx, ny, nz;     // -origin * reciprocal direction (slab test in fused form)
     bool valid;
 };
 
@@ -59,6 +60,9 @@ BTE_DI RayPre rayPre(float ox, float oy, float oz, float dx, float dy, float dz,
     r.px = pad * fabsf(r.ix);
     r.py = pad * fabsf(r.iy);
     r.pz = pad * fabsf(r.iz);
+    r.nx = -ox * r.ix;
+    r.ny = -oy * r.iy;
+    r.nz = -oz * r.iz;
     return r;
 }
 
@@ -104,9 +108,9 @@ constexpr float kCullMargin = 1.0001f;
 BTE_DI bool boxHit(const RayPre& r, float lx, float hx, float ly, float hy, float lz, float hz, float tmin, float tmax,
                    float& tEnter)
 {
-    const float tx0 = (lx - r.ox) * r.ix, tx1 = (hx - r.ox) * r.ix;
-    const float ty0 = (ly - r.oy) * r.iy, ty1 = (hy - r.oy) * r.iy;
-    const float tz0 = (lz - r.oz) * r.iz, tz1 = (hz - r.oz) * r.iz;
+    const float tx0 = __fmaf_rn(lx, r.ix, r.nx), tx1 = __fmaf_rn(hx, r.ix, r.nx);
+    const float ty0 = __fmaf_rn(ly, r.iy, r.ny), ty1 = __fmaf_rn(hy, r.iy, r.ny);
+    const float tz0 = __fmaf_rn(lz, r.iz, r.nz), tz1 = __fmaf_rn(hz, r.iz, r.nz);
     const float tn = fmaxf(fmaxf(fminf(tx0, tx1) - r.px, fminf(ty0, ty1) - r.py), fmaxf(fminf(tz0, tz1) - r.pz, tmin));
     const float tf = fminf(fminf(fmaxf(tx0, tx1) + r.px, fmaxf(ty0, ty1) + r.py), fminf(fmaxf(tz0, tz1) + r.pz, tmax)) * kBoxGrow;
     tEnter = tn;
@@ -125,7 +129,7 @@ BTE_DI int traceClosest(const DevScene& s, const RayPre& r, float tmin, float tm
     float bt = tmax, bu = 0.0f, bv = 0.0f;
     int stack[kTraversalStack];
     int sp = 0;
-    int node = s.rootIsLeaf ? ~0 : 0;
+    int node = s.rootIsLeaf ? s.rootCode : 0;
     while (true) {
         if (node >= 0) {
             const BvhNode* n = s.nodes + node;
@@ -171,7 +175,7 @@ BTE_DI bool traceOccluded(const DevScene& s, const RayPre& r, float tmin, float 
     if (!r.valid || s.triCount <= 0) return false;
     int stack[kTraversalStack];
     int sp = 0;
-    int node = s.rootIsLeaf ? ~0 : 0;
+    int node = s.rootIsLeaf ? s.rootCode : 0;
     const float cull = tmax * kCullMargin;
     while (true) {
         if (node >= 0) {

@@ -49,7 +49,8 @@ struct DevScene {
     int triCount;
     const float4* leafTris;           // [triCount*3] v0.xyz|origIndex, v1.xyz, v2.xyz in leaf order
     const BvhNode* nodes;             // root = node 0 (triCount >= 2) or a single-leaf root
-    int rootIsLeaf;                   // triCount == 1
+    int rootIsLeaf;                   // the whole scene is one leaf
+    int rootCode;                     // its leaf code
     float sceneMaxAbs;                // max |coordinate| over all vertices (traversal error bound)
     // materials
     const BsdfData* bsdfs;

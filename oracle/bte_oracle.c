@@ -46,6 +46,8 @@
 #define O_POWF powf
 #define O_ATAN2F atan2f
 #define O_ACOSF acosf
+#define O_POW5(x) powf((x), 5)
+#define O_POW2(x) powf((x), 2)
 #else
 #define O_SINF om_sinf
 #define O_COSF om_cosf
@@ -55,6 +57,8 @@
 #define O_POWF om_powf
 #define O_ATAN2F om_atan2f
 #define O_ACOSF om_acosf
+#define O_POW5(x) om_pow5f(x)
+#define O_POW2(x) om_pow2f(x)
 #endif
 
 int or_math_mode(void)
@@ -442,9 +446,9 @@ static inline OF3 o_dsqrt3(OF3 c) { return f3(sqrtf(fmaxf(0.0f, c.x)), sqrtf(fma
 
 /* :42-56 */
 static inline float o_diffF90(const OBsdf* b, float h) { return 0.5f + (2.0f * DROUGH(b) * h * h); }
-static inline float o_diffF(float c, float f90) { return 1.0f + ((f90 - 1.0f) * O_POWF(1.0f - c, 5)); }
+static inline float o_diffF(float c, float f90) { return 1.0f + ((f90 - 1.0f) * O_POW5(1.0f - c)); }
 static inline float o_ssF90(const OBsdf* b, float h) { return DROUGH(b) * h * h; }
-static inline float o_ssF(float c, float f90) { return 1.0f + ((f90 - 1.0f) * O_POWF(1.0f - c, 5)); }
+static inline float o_ssF(float c, float f90) { return 1.0f + ((f90 - 1.0f) * O_POW5(1.0f - c)); }
 
 /* :59-104 */
 static OF3 o_evalDiffuseLobe(const OBsdf* b, const OBRec* r)
@@ -494,14 +498,14 @@ static OF3 o_fresnelMetal(const OBsdf* b, float hDotWo)
     float coef = DSPEC(b) * o_schlickFresnel(DETA(b)) * (1.0f - DMETAL(b));
     OF3 clr = f3((coef * spec.x) + (bc.x * DMETAL(b)), (coef * spec.y) + (bc.y * DMETAL(b)),
                  (coef * spec.z) + (bc.z * DMETAL(b)));
-    float sch = O_POWF(1.0f - hDotWo, 5);
+    float sch = O_POW5(1.0f - hDotWo);
     return f3(clr.x + ((1.0f - clr.x) * sch), clr.y + ((1.0f - clr.y) * sch), clr.z + ((1.0f - clr.z) * sch));
 }
 /* :186-210 */
 static inline float o_ggxD(OF3 wh, float ax, float ay)
 {
     float den = O_PI * ax * ay *
-                O_POWF(((wh.x * wh.x) / (ax * ax)) + ((wh.y * wh.y) / (ay * ay)) + (wh.z * wh.z), 2);
+                O_POW2(((wh.x * wh.x) / (ax * ax)) + ((wh.y * wh.y) / (ay * ay)) + (wh.z * wh.z));
     return 1.0f / den;
 }
 static inline float o_lambda(OF3 w, float ax, float ay)
@@ -582,7 +586,7 @@ static OF3 o_sampleMetalLobe(const OBsdf* b, OBRec* r, float u1, float u2)
 static inline float o_fresnelClear(float hDotWo)
 {
     float rr = (float)0.04;
-    return rr + ((1.0f - rr) * O_POWF(1.0f - hDotWo, 5));
+    return rr + ((1.0f - rr) * O_POW5(1.0f - hDotWo));
 }
 static inline float o_clearD(const OBsdf* b, OF3 wh)
 {
@@ -673,7 +677,7 @@ static OF3 o_evalGlassLobe(const OBsdf* b, const OBRec* r)
         return div3(num, den);
     } else {
         OF3 num = mul3s(o_dsqrt3(DBASE(b)), (1.0f - fg) * dg * gg * fabsf(hDotWi * hDotWo));
-        float den = fabsf(ci) * fmaxf(O_POWF(hDotWi + eho, 2), 1e-4f);
+        float den = fabsf(ci) * fmaxf(O_POW2(hDotWi + eho), 1e-4f);
         return div3(num, den);
     }
 }
@@ -692,7 +696,7 @@ static float o_pdfGlassLobe(const OBsdf* b, const OBRec* r)
     float gg = o_lambda(r->wi, ax, ay);
     float common = (dg * gg * fabsf(hDotWi)) / fabsf(ci);
     if (inNout > 0.0f) return (common * fg) / (4.0f * fabsf(hDotWo));
-    float jac = (eta * eta * fabsf(hDotWo)) / fmaxf(O_POWF(hDotWi + (eta * hDotWo), 2), 1e-4f);
+    float jac = (eta * eta * fabsf(hDotWo)) / fmaxf(O_POW2(hDotWi + (eta * hDotWo)), 1e-4f);
     return (1.0f - fg) * common * jac;
 }
 /* :591-674 */
@@ -735,7 +739,7 @@ static OF3 o_evalSheenLobe(const OBsdf* b, const OBRec* r)
     if (lumi > 0) tint = div3(bc, lumi);
     float st = DSHEENTINT(b);
     OF3 sh = f3((1.0f - st) + (st * tint.x), (1.0f - st) + (st * tint.y), (1.0f - st) + (st * tint.z));
-    return mul3s(sh, O_POWF(1.0f - hDotWo, 5) * co);
+    return mul3s(sh, O_POW5(1.0f - hDotWo) * co);
 }
 /* :758-787 */
 static OF3 o_evalDisney(const OBsdf* b, const OBRec* r)

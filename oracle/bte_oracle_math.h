@@ -253,6 +253,22 @@ static inline float om_powf(float x, float y)
     return sign * (float)om_exp_d(l);
 }
 
+/* x^5 and x^2 (the reference's powf(x, 5) / powf(x, 2) call sites): double
+ * products rounded once to float -- correctly rounded except in vanishingly
+ * rare near-halfway cases; C99 pow special values for odd/even exponents. */
+static inline float om_pow5f(float x)
+{
+    const double d = (double)x;
+    const double d2 = d * d;
+    const double d4 = d2 * d2;
+    return (float)(d4 * d);
+}
+static inline float om_pow2f(float x)
+{
+    const double d = (double)x;
+    return (float)(d * d);
+}
+
 /* ---- atan2 / acos ---- */
 /* atan of z in [0, 1] (double) */
 static inline double om_atan01_d(double z)
