@@ -298,6 +298,9 @@ class Renderer:
     def set_stage_timing(self, on: bool):
         _check(self.lib.bte_set_stage_timing(1 if on else 0))
 
+    def set_tuning(self, max_leaf: int = 8, shade_min_blocks: int = 2):
+        _check(self.lib.bte_set_tuning(int(max_leaf), int(shade_min_blocks)))
+
     def set_hit_log(self, on: bool):
         _check(self.lib.bte_set_hit_log(1 if on else 0))
 

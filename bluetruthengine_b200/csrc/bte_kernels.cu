@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
 
 // ---------------------------------------------------------------- shade
 // src/wavefront/ray_shade.cu:103-183 (rt_optix_shading.cuh:412-447 order).
-__global__ void __launch_bounds__(256) kShade(DevScene s, DevPaths P, FrameParams f, int bounce)
+template <int MinBlocks>
+__global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P, FrameParams f, int bounce)
 {
     const int count = P.rayCount[bounce];
     const int* __restrict__ q = P.queue[bounce & 1];
@@ -366,9 +367,11 @@ void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, in
 {
     kExtend<<<grid, block, 0, st>>>(s, P, bounce);
 }
-void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block, cudaStream_t st)
+void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block,
+                 int minBlocks, cudaStream_t st)
 {
-    kShade<<<grid, block, 0, st>>>(s, P, f, bounce);
+    if (minBlocks == 3) kShade<3><<<grid, block, 0, st>>>(s, P, f, bounce);
+    else kShade<2><<<grid, block, 0, st>>>(s, P, f, bounce);
 }
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
 {
@@ -414,7 +417,8 @@ int occupancyGrid(int which, int block)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const void* fn = which == 0 ? reinterpret_cast<const void*>(kExtend)
-                   : which == 1 ? reinterpret_cast<const void*>(kShade)
+                   : which == 1 ? reinterpret_cast<const void*>(kShade<2>)
+                   : which == 3 ? reinterpret_cast<const void*>(kShade<3>)
                                 : reinterpret_cast<const void*>(kConnect);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0) != cudaSuccess || per < 1) per = 1;
     return sms * per;

@@ -10,7 +10,8 @@ namespace bte {
 
 void launchGenerate(const DevPaths& P, const FrameParams& f, cudaStream_t st);
 void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
-void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block, cudaStream_t st);
+void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block,
+                 int minBlocks, cudaStream_t st);
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    cudaStream_t st);

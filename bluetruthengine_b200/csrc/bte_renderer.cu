@@ -87,12 +87,13 @@ struct Renderer {
     // acceleration structure
     DeviceBuffer bvhNodes, leafTris;
     int rootIsLeaf = 0, rootCode = ~0;
-    int maxLeaf = 8;
+    int maxLeaf = 1;          // autotuned on B200: single-triangle leaves traverse fastest
+    int shadeMinBlocks = 3;   // autotuned on B200: 3 resident shade blocks per SM
     bool accelReady = false;
     float msBvh = 0.0f;
     // camera / frame
     CameraData camera{};
-    BteRenderConfig cfg{1, 200, 3, BTE_ENV_SAMPLING_CDF, 256, 0};
+    BteRenderConfig cfg{1, 200, 3, BTE_ENV_SAMPLING_CDF, 128, 0};
     int renderMode = BTE_RENDER_WAVEFRONT;
     bool denoiser = false;
     uint32_t frameIndex = 0;
@@ -256,10 +257,10 @@ void renderFrame(int w, int h)
     const int slots = slotsFor();
     if (slots > 32) throw CudaError{"bte_render: at most 30 spotlights are supported"};
     ensureWavefront(paths, slots, depth);
-    const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 256;
+    const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
     if (g.gridBlock != block) {
         g.gridExtend = occupancyGrid(0, block);
-        g.gridShade = occupancyGrid(1, block);
+        g.gridShade = occupancyGrid(g.shadeMinBlocks == 3 ? 3 : 1, block);
         g.gridConnect = occupancyGrid(2, block);
         g.gridBlock = block;
     }
@@ -297,7 +298,7 @@ void renderFrame(int w, int h)
         launchGenerate(P, f, st);
         for (int b = 0; b < depth; ++b) {
             launchExtend(s, P, b, g.gridExtend, block, st);
-            launchShade(s, P, f, b, g.gridShade, block, st);
+            launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
             launchConnect(s, P, b, g.gridConnect, block, st);
         }
         launchPresent(P, f, g.accum.as<float>(), g.accumD.as<double>(), g.framebuffer.as<uint32_t>(), g.extFramebuffer, st);
@@ -315,7 +316,7 @@ void renderFrame(int w, int h)
         timed(0, [&] { launchGenerate(P, f, st); });
         for (int b = 0; b < depth; ++b) {
             timed(1, [&] { launchExtend(s, P, b, g.gridExtend, block, st); });
-            timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, st); });
+            timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st); });
             timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
         }
         timed(4, [&] {
@@ -698,6 +699,18 @@ int bte_set_frame_index(uint32_t frameIndex)
 {
     return guarded([&] { g.frameIndex = frameIndex; return 0; });
 }
+int bte_set_tuning(int maxLeafTriangles, int shadeMinBlocks)
+{
+    return guarded([&] {
+        if (maxLeafTriangles < 1 || maxLeafTriangles > kMaxLeafTris) throw CudaError{"bte_set_tuning: maxLeafTriangles in [1, 64]"};
+        if (shadeMinBlocks != 2 && shadeMinBlocks != 3) throw CudaError{"bte_set_tuning: shadeMinBlocks must be 2 or 3"};
+        g.maxLeaf = maxLeafTriangles;
+        g.shadeMinBlocks = shadeMinBlocks;
+        g.gridBlock = 0;   // recompute persistent grids
+        return 0;
+    });
+}
+
 int bte_set_hit_log(int enabled)
 {
     return guarded([&] { g.hitLogEnabled = enabled != 0; if (!g.hitLogEnabled) g.hitLog.release(); return 0; });

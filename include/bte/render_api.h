@@ -105,6 +105,10 @@ int bte_read_accum_f64(double* hostRGBSum);          /* FP64 running sum of samp
 int bte_read_sample_radiance(float* hostRGB, int count);  /* per-path radiance of the last frame [W*H*spp*3] */
 int bte_read_hit_log(int* hostTri, int count);       /* per-bounce closest-hit triangle of the last frame */
 int bte_set_hit_log(int enabled);                    /* record [path][bounce] hit triangles (debug/parity) */
+/* Acceleration-structure and kernel tuning (used by the autotuner): maximum
+ * triangles per BVH leaf (1-64, applied at the next bte_init_accel) and the
+ * minimum resident blocks per SM the shade kernel is compiled for (2 or 3). */
+int bte_set_tuning(int maxLeafTriangles, int shadeMinBlocks);
 
 /* ---- debug/parity entry points over device-resident state ---- */
 /* closest hit for n rays [origin, dir] (host arrays): triangle index (-1 miss) and t, u, v */
