@@ -200,8 +200,9 @@ def run_ours(args):
     env_mode = bte.ENV_ALIAS if args.env == "alias" else bte.ENV_CDF
     r.set_config(samples_per_frame=args.spp, max_depth=args.depth, rr_start=3, env_sampling=env_mode)
     r.reset_accumulation(W, H)
-    # disjoint sample ranges per rank
-    r.set_frame_index(rank * (args.steps + args.warmup + 8) * args.spp)
+    # disjoint sample ranges per rank (every frame below draws from this rank's range)
+    from bluetruthengine_b200 import distributed as D
+    r.set_frame_index(D.sample_base(rank, args.steps * 2 + args.warmup + 2, args.spp))
     host_fb = torch.empty(W * H, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
 
     def step_e2e():
@@ -231,12 +232,7 @@ def run_ours(args):
         shd += st.shadowRays
     barrier()
     clk = clocks.stop()
-    t_dev = sum(ms) / 1e3
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([t_dev], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev = float(t.item())
+    t_dev = D.max_over_ranks(sum(ms) / 1e3, device="cuda") if world > 1 else sum(ms) / 1e3
     samples_per_rank = W * H * args.spp * args.steps
     value = samples_per_rank * world / t_dev / 1e6
 
@@ -248,10 +244,7 @@ def run_ours(args):
     barrier()
     t_e2e = time.perf_counter() - t0
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+        t_e2e = D.max_over_ranks(t_e2e, device="cuda")
     e2e = samples_per_rank * world / t_e2e / 1e6
 
     # --- per-stage split (separate, untimed pass) for the roofline of the dominant kernel ---

@@ -179,7 +179,7 @@ class SceneView:
     """An OScene over a bluetruthengine_b200.Scene (keeps the arrays alive)."""
 
     def __init__(self, scene, env_mode: int = 0, oracle: Optional[Oracle] = None, build_accel: Optional[bool] = None,
-                 env_tables=None):
+                 env_tables=None, textures=None, mr_textures=None):
         self.scene = scene
         self.keep = []
         s = OScene()
@@ -208,6 +208,19 @@ class SceneView:
         if s.spotCount:
             s.spots = keep(np.ascontiguousarray(scene.spotlights))
         s.textureCount = 0
+        if textures:
+            def table(imgs):
+                arrs = [None if im is None else np.ascontiguousarray(im, dtype=np.uint8) for im in imgs]
+                self.keep.extend(a for a in arrs if a is not None)
+                ptrs = (C.c_void_p * len(arrs))(*[None if a is None else a.ctypes.data for a in arrs])
+                ws = np.array([0 if a is None else a.shape[1] for a in arrs], dtype=np.int32)
+                hs = np.array([0 if a is None else a.shape[0] for a in arrs], dtype=np.int32)
+                self.keep.extend([ptrs, ws, hs])
+                return C.cast(ptrs, C.c_void_p), _p(ws), _p(hs)
+            s.texPixels, s.texW, s.texH = table(textures)
+            s.textureCount = len(textures)
+            if mr_textures:
+                s.mrPixels, s.mrW, s.mrH = table(mr_textures)
         if scene.env_rgba is not None:
             env = np.ascontiguousarray(scene.env_rgba, dtype=np.float32)
             h, w = env.shape[:2]

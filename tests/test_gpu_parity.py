@@ -269,3 +269,32 @@ def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode):
     eq = np.all(bits(g[pix]) == bits(o), axis=1)
     assert eq.all(), f"{np.sum(~eq)} of {len(pix)} samples differ"
     assert st.extends > W * H and np.isfinite(g).all()
+
+
+def test_textured_materials_bitexact(renderer, oracle_mod, random_scene):
+    """Albedo textures (RGBA8, wrap, bilinear) on diffuse/microfacet/Disney materials and a
+    metallic-roughness map on the Disney material (rt_material.cuh:15-59): GPU == oracle."""
+    rng = np.random.default_rng(17)
+    tex = [rng.integers(0, 256, size=(19, 23, 4), dtype=np.uint8), rng.integers(0, 256, size=(8, 64, 4), dtype=np.uint8),
+           None, None, rng.integers(0, 256, size=(33, 7, 4), dtype=np.uint8)]
+    mr = [rng.integers(0, 256, size=(16, 16, 4), dtype=np.uint8), None, None, None, None]
+    sc = random_scene
+    W, H, spp, depth = sc.width, sc.height, 2, 10
+    _upload(renderer, sc, env_mode=1, spp=spp, depth=depth)
+    renderer.init_textures(tex)
+    renderer.init_mr_textures(mr)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    g = renderer.read_sample_radiance(W * H * spp)
+    orc = oracle_mod.Oracle(libm=False)
+    view = oracle_mod.SceneView(sc, env_mode=1, oracle=orc, textures=tex, mr_textures=mr)
+    pix = np.tile(np.arange(W * H, dtype=np.uint32), spp)
+    smp = np.repeat(np.arange(spp, dtype=np.uint32), W * H)
+    o, _, _ = oracle_mod.render_samples(orc.lib, view, sc.camera, W, H, depth, pix, smp)
+    plain = oracle_mod.SceneView(sc, env_mode=1, oracle=orc)
+    p, _, _ = oracle_mod.render_samples(orc.lib, plain, sc.camera, W, H, depth, pix, smp)
+    assert not np.array_equal(bits(o), bits(p)), "textures had no effect"
+    eq = np.all(bits(g) == bits(o), axis=1)
+    assert eq.all(), f"{np.sum(~eq)} of {len(o)} samples differ"
+    renderer.init_textures(None)
+    renderer.init_mr_textures(None)

@@ -131,3 +131,24 @@ def test_present_welford_and_gamma(oracle_mod):
         pr = np.empty(n, np.uint32)
         ref.lib.ref_present(_p(acc_r), _p(x), n, C.c_uint32(f), _p(pr))
         assert np.array_equal(bits(acc_o), bits(acc_r)) and np.array_equal(po, pr)
+
+
+def test_textured_scene_matches_reference(oracle_mod, random_scene):
+    """Albedo + metallic-roughness textures through the reference's loadBsdfForTriangle
+    (rt_material.cuh:15-59) with the documented filter: oracle == reference headers."""
+    if not oracle_mod.Ref.available():
+        pytest.skip("reference harness not built")
+    rng = np.random.default_rng(17)
+    tex = [rng.integers(0, 256, size=(19, 23, 4), dtype=np.uint8), rng.integers(0, 256, size=(8, 64, 4), dtype=np.uint8),
+           None, None, rng.integers(0, 256, size=(33, 7, 4), dtype=np.uint8)]
+    mr = [rng.integers(0, 256, size=(16, 16, 4), dtype=np.uint8), None, None, None, None]
+    orc = oracle_mod.Oracle(libm=True)
+    ref = oracle_mod.Ref()
+    sc = random_scene
+    v = oracle_mod.SceneView(sc, env_mode=0, oracle=orc, textures=tex, mr_textures=mr)
+    W, H = sc.width, sc.height
+    pix = np.arange(W * H, dtype=np.uint32)
+    smp = np.full(W * H, 5, np.uint32)
+    a, ha, _ = oracle_mod.render_samples(orc.lib, v, sc.camera, W, H, 10, pix, smp, hit_log=True)
+    b, hb, _ = oracle_mod.render_samples(ref.lib, v, sc.camera, W, H, 10, pix, smp, hit_log=True, prefix="ref_")
+    assert np.array_equal(ha, hb) and np.array_equal(bits(a), bits(b))
