@@ -42,6 +42,12 @@ CAMERA_DTYPE = np.dtype([("origin", "<f4", 3), ("forward", "<f4", 3), ("right", 
 assert TRIANGLE_DTYPE.itemsize == 96 and BSDF_DTYPE.itemsize == 68 and CAMERA_DTYPE.itemsize == 56
 
 
+class Tuning(C.Structure):
+    """BteTuning (include/bte/render_api.h)."""
+    _fields_ = [("bvhWidth", C.c_int), ("maxLeafTriangles", C.c_int), ("shadeMinBlocks", C.c_int),
+                ("postponePercent", C.c_int)]
+
+
 class RenderConfig(C.Structure):
     _fields_ = [("samplesPerFrame", C.c_int), ("maxDepth", C.c_int), ("rrStart", C.c_int), ("envSampling", C.c_int),
                 ("blockSize", C.c_int), ("useGraph", C.c_int)]
@@ -298,8 +304,20 @@ class Renderer:
     def set_stage_timing(self, on: bool):
         _check(self.lib.bte_set_stage_timing(1 if on else 0))
 
-    def set_tuning(self, max_leaf: int = 8, shade_min_blocks: int = 2):
-        _check(self.lib.bte_set_tuning(int(max_leaf), int(shade_min_blocks)))
+    def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
+                   postpone_percent: int = 20):
+        t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent))
+        _check(self.lib.bte_set_tuning(C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(self.lib.bte_get_tuning(C.byref(t)))
+        return {f: getattr(t, f) for f, _ in Tuning._fields_}
+
+    def accel_info(self) -> dict:
+        w, n, d, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.bte_get_accel_info(C.byref(w), C.byref(n), C.byref(d), C.byref(ms)))
+        return {"width": w.value, "nodes": n.value, "depth": d.value, "ms_build": ms.value}
 
     def set_hit_log(self, on: bool):
         _check(self.lib.bte_set_hit_log(1 if on else 0))

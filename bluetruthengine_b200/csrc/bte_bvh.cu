@@ -12,13 +12,16 @@
 //   5. bottom-up refit with one atomic arrival counter per node, with a
 //      surface-area cost decision collapsing small subtrees (contiguous
 //      ranges of the sorted triangles) into multi-triangle leaves
-//   6. output: 64-byte BVH2 nodes holding both child boxes, and the triangles
-//      in leaf order as three float4 each (v0|original index, v1, v2)
+//   6. output: 64-byte BVH2 nodes holding both child boxes, or an 8-wide tree
+//      of 80-byte nodes with quantised boxes collapsed from the binary one,
+//      and the triangles in leaf order as three float4 each (v0|original
+//      index, v1, v2)
 // All integer steps are deterministic; the result does not depend on thread
 // scheduling.
 #include "bte_kernels.h"
 
 #include <cfloat>
+#include <climits>
 #include <vector>
 
 namespace bte {
@@ -328,14 +331,274 @@ __global__ void kEmitNodes(const int2* __restrict__ children, const float* __res
     nodes[i] = nd;
 }
 
+// ---------------------------------------------------------------- 8-wide collapse
+// Top-down, one level of the wide tree per pass.  A wide node rooted at a
+// binary node takes its two children and then repeatedly opens the child of
+// largest surface area that holds more than kWideLeafMax triangles (then, if
+// slots remain, any child with two or more), up to eight children.  Children
+// holding at most leafMax triangles become leaf slots; their triangles are
+// copied next to each other in slot order.  Per-level prefix sums give every
+// node its children's and triangles' positions, so the layout is
+// deterministic.
+constexpr int kNoChild = INT_MIN;
+
+__device__ __forceinline__ int subtreeCount(const int2* range, int c)
+{
+    return c >= 0 ? range[c].y - range[c].x + 1 : 1;
+}
+
+__global__ void kWideCollect(const int2* __restrict__ items, int m, const int2* __restrict__ children,
+                             const int2* __restrict__ range, const float* __restrict__ innerBox, int leafMax,
+                             int* outCodes, int* cntI, int* cntT)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > m) return;
+    if (i == m) { cntI[m] = 0; cntT[m] = 0; return; }
+    const int code = items[i].x;
+    int C[8];
+    int k;
+    if (code >= 0) { const int2 c = children[code]; C[0] = c.x; C[1] = c.y; k = 2; }
+    else { C[0] = code; k = 1; }
+    while (k < 8) {
+        int best = -1;
+        float bestA = -1.0f;
+        for (int phase = 0; phase < 2 && best < 0; ++phase) {
+            for (int j = 0; j < k; ++j) {
+                const int c = C[j];
+                if (c < 0) continue;
+                const int cnt = subtreeCount(range, c);
+                if (phase == 0 ? cnt <= leafMax : cnt < 2) continue;
+                const float A = halfArea(innerBox + 6 * static_cast<size_t>(c));
+                if (A > bestA) { bestA = A; best = j; }
+            }
+        }
+        if (best < 0) break;
+        const int2 cc = children[C[best]];
+        C[best] = cc.x;
+        C[k++] = cc.y;
+    }
+    int I = 0, T = 0;
+    for (int j = 0; j < 8; ++j) {
+        if (j < k) {
+            const int cnt = subtreeCount(range, C[j]);
+            if (C[j] >= 0 && cnt > leafMax) ++I; else T += cnt;
+        }
+        outCodes[8 * static_cast<size_t>(i) + j] = j < k ? C[j] : kNoChild;
+    }
+    cntI[i] = I;
+    cntT[i] = T;
+}
+
+__device__ __forceinline__ uint32_t wideScaleBits(uint32_t e) { return e << 23; }
+// p + q * 2^(e-127) in double (exact for the magnitudes a scene has), the
+// plane the traversal's fused slab test measures against
+__device__ __forceinline__ double wideDecodeExact(uint32_t q, uint32_t e, float p)
+{
+    const double scale = __longlong_as_double(static_cast<long long>(static_cast<int>(e) - 127 + 1023) << 52);
+    return static_cast<double>(p) + static_cast<double>(q) * scale;
+}
+
+// smallest biased exponent e in [1, 254] with p + 255 * 2^(e-127) >= hi
+__device__ uint32_t wideExponent(float lo, float hi)
+{
+    const float ext = hi - lo;
+    int e = 1;
+    if (ext > 0.0f) e = max(1, static_cast<int>((__float_as_uint(ext) >> 23) & 0xffu) - 8);
+    while (e < 254 && wideDecodeExact(255u, static_cast<uint32_t>(e), lo) < static_cast<double>(hi)) ++e;
+    return static_cast<uint32_t>(e);
+}
+
+__device__ uint32_t quantLo(float v, float p, uint32_t e)
+{
+    const float sc = __uint_as_float(wideScaleBits(e));
+    float f = floorf((v - p) / sc);
+    int q = static_cast<int>(fminf(fmaxf(f, 0.0f), 255.0f));
+    const double dv = static_cast<double>(v);
+    while (q > 0 && wideDecodeExact(static_cast<uint32_t>(q), e, p) > dv) --q;
+    while (q < 255 && wideDecodeExact(static_cast<uint32_t>(q + 1), e, p) <= dv) ++q;
+    return static_cast<uint32_t>(q);
+}
+
+__device__ uint32_t quantHi(float v, float p, uint32_t e)
+{
+    const float sc = __uint_as_float(wideScaleBits(e));
+    float f = ceilf((v - p) / sc);
+    int q = static_cast<int>(fminf(fmaxf(f, 0.0f), 255.0f));
+    const double dv = static_cast<double>(v);
+    while (q < 255 && wideDecodeExact(static_cast<uint32_t>(q), e, p) < dv) ++q;
+    while (q > 0 && wideDecodeExact(static_cast<uint32_t>(q - 1), e, p) >= dv) --q;
+    return static_cast<uint32_t>(q);
+}
+
+__global__ void kWideEmit(const int2* __restrict__ items, int m, const int* __restrict__ codes,
+                          const int* __restrict__ scanI, const int* __restrict__ scanT, const int2* __restrict__ range,
+                          const float* __restrict__ innerBox, const float* __restrict__ leafBox,
+                          const float4* __restrict__ sortedTris, int leafMax, int nextBase, int triCursor,
+                          WideNode* nodes, int2* nextItems, float4* wideTris, unsigned int* errorFlag)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int w = items[i].y;
+    int C[8];
+    int k = 0;
+    float bx[8][6];
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int j = 0; j < 8; ++j) {
+        const int c = codes[8 * static_cast<size_t>(i) + j];
+        if (c == kNoChild) break;
+        C[k] = c;
+        const float* b = c >= 0 ? innerBox + 6 * static_cast<size_t>(c) : leafBox + 6 * static_cast<size_t>(~c);
+        for (int q = 0; q < 6; ++q) bx[k][q] = b[q];
+        for (int a = 0; a < 3; ++a) { lo[a] = fminf(lo[a], b[a]); hi[a] = fmaxf(hi[a], b[3 + a]); }
+        ++k;
+    }
+    // slot assignment: child j to slot s maximising the offset of its centre
+    // towards corner s of the parent box (bit a of s set = high side of axis a)
+    float pc[3];
+    for (int a = 0; a < 3; ++a) pc[a] = 0.5f * (lo[a] + hi[a]);
+    int slotOf[8];
+    int childAt[8];
+    for (int j = 0; j < 8; ++j) { slotOf[j] = -1; childAt[j] = -1; }
+    for (int it = 0; it < k; ++it) {
+        float bestV = -FLT_MAX;
+        int bj = -1, bs = -1;
+        for (int j = 0; j < k; ++j) {
+            if (slotOf[j] >= 0) continue;
+            float d[3];
+            for (int a = 0; a < 3; ++a) d[a] = 0.5f * (bx[j][a] + bx[j][3 + a]) - pc[a];
+            for (int sl = 0; sl < 8; ++sl) {
+                if (childAt[sl] >= 0) continue;
+                const float v = ((sl & 1) ? d[0] : -d[0]) + ((sl & 2) ? d[1] : -d[1]) + ((sl & 4) ? d[2] : -d[2]);
+                if (bj < 0 || v > bestV) { bestV = v; bj = j; bs = sl; }
+            }
+        }
+        slotOf[bj] = bs;
+        childAt[bs] = bj;
+    }
+    uint32_t e[3];
+    for (int a = 0; a < 3; ++a) e[a] = wideExponent(lo[a], hi[a]);
+    WideNode nd;
+    nd.px = lo[0]; nd.py = lo[1]; nd.pz = lo[2];
+    nd.childBase = nextBase + scanI[i];
+    nd.triBase = triCursor + scanT[i];
+    uint32_t imask = 0;
+    uint32_t meta[2] = {0u, 0u};
+    uint32_t q[6][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}};
+    int r = 0, toff = 0;
+    for (int sl = 0; sl < 8; ++sl) {
+        const int j = childAt[sl];
+        if (j < 0) continue;
+        const int c = C[j];
+        const int word = sl >> 2, sh = 8 * (sl & 3);
+        for (int a = 0; a < 3; ++a) {
+            q[a][word] |= quantLo(bx[j][a], lo[a], e[a]) << sh;
+            q[3 + a][word] |= quantHi(bx[j][3 + a], lo[a], e[a]) << sh;
+        }
+        const int cnt = subtreeCount(range, c);
+        if (c >= 0 && cnt > leafMax) {
+            imask |= 1u << sl;
+            nextItems[scanI[i] + r] = make_int2(c, nextBase + scanI[i] + r);
+            ++r;
+        } else {
+            if (cnt > 7 || toff + cnt > 32) { atomicOr(errorFlag, 1u); continue; }
+            meta[word] |= static_cast<uint32_t>(toff | (cnt << 5)) << sh;
+            const int start = c >= 0 ? range[c].x : ~c;
+            const size_t dst = 3 * (static_cast<size_t>(nd.triBase) + static_cast<size_t>(toff));
+            for (int t = 0; t < cnt; ++t) {
+                const size_t src = 3 * static_cast<size_t>(start + t);
+                wideTris[dst + 3 * t] = sortedTris[src];
+                wideTris[dst + 3 * t + 1] = sortedTris[src + 1];
+                wideTris[dst + 3 * t + 2] = sortedTris[src + 2];
+            }
+            toff += cnt;
+        }
+    }
+    nd.expImask = e[0] | (e[1] << 8) | (e[2] << 16) | (imask << 24);
+    nd.meta[0] = meta[0]; nd.meta[1] = meta[1];
+    nd.qlox[0] = q[0][0]; nd.qlox[1] = q[0][1];
+    nd.qloy[0] = q[1][0]; nd.qloy[1] = q[1][1];
+    nd.qloz[0] = q[2][0]; nd.qloz[1] = q[2][1];
+    nd.qhix[0] = q[3][0]; nd.qhix[1] = q[3][1];
+    nd.qhiy[0] = q[4][0]; nd.qhiy[1] = q[4][1];
+    nd.qhiz[0] = q[5][0]; nd.qhiz[1] = q[5][1];
+    nodes[w] = nd;
+}
+
 }  // namespace
 
 #define BVH_CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { err = std::string("LBVH build: ") + cudaGetErrorString(e_); goto fail; } } while (0)
 
-int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, BvhBuildResult& out, cudaStream_t st, std::string& err)
+// Collapse the binary tree into the 8-wide tree, level by level.
+static int buildWide(int n, int leafMax, const int2* children, const int2* range, const float* innerBox,
+                     const float* leafBox, const float4* sortedTris, BvhBuildResult& out, cudaStream_t st,
+                     std::string& err)
+{
+    int2 *itemsA = nullptr, *itemsB = nullptr;
+    int *codes = nullptr, *cntI = nullptr, *cntT = nullptr;
+    unsigned int* flag = nullptr;
+    WideNode* scratch = nullptr;
+    int rc = -1;
+    int wideCount = 1, triCursor = 0, m = 1, levels = 0;
+    const size_t cap = static_cast<size_t>(n > 1 ? n : 1);
+    {
+        BVH_CK(cudaMalloc(&itemsA, sizeof(int2) * cap));
+        BVH_CK(cudaMalloc(&itemsB, sizeof(int2) * cap));
+        BVH_CK(cudaMalloc(&codes, sizeof(int) * 8 * cap));
+        BVH_CK(cudaMalloc(&cntI, sizeof(int) * (cap + 1)));
+        BVH_CK(cudaMalloc(&cntT, sizeof(int) * (cap + 1)));
+        BVH_CK(cudaMalloc(&flag, sizeof(unsigned int)));
+        BVH_CK(cudaMalloc(&scratch, sizeof(WideNode) * cap));
+        BVH_CK(cudaMalloc(&out.leafTris, sizeof(float4) * 3 * static_cast<size_t>(n)));
+        BVH_CK(cudaMemsetAsync(flag, 0, sizeof(unsigned int), st));
+        const int2 root = make_int2(n > 1 ? 0 : ~0, 0);
+        BVH_CK(cudaMemcpyAsync(itemsA, &root, sizeof(int2), cudaMemcpyHostToDevice, st));
+        while (m > 0) {
+            const int B = 128;
+            kWideCollect<<<(m + 1 + B - 1) / B, B, 0, st>>>(itemsA, m, children, range, innerBox, leafMax, codes, cntI,
+                                                          cntT);
+            kScanSingle<<<1, 1024, 0, st>>>(cntI, m + 1);
+            kScanSingle<<<1, 1024, 0, st>>>(cntT, m + 1);
+            kWideEmit<<<(m + B - 1) / B, B, 0, st>>>(itemsA, m, codes, cntI, cntT, range, innerBox, leafBox, sortedTris,
+                                                     leafMax, wideCount, triCursor, scratch, itemsB, out.leafTris, flag);
+            BVH_CK(cudaGetLastError());
+            int tot[2] = {0, 0};
+            BVH_CK(cudaMemcpyAsync(&tot[0], cntI + m, sizeof(int), cudaMemcpyDeviceToHost, st));
+            BVH_CK(cudaMemcpyAsync(&tot[1], cntT + m, sizeof(int), cudaMemcpyDeviceToHost, st));
+            BVH_CK(cudaStreamSynchronize(st));
+            ++levels;
+            wideCount += tot[0];
+            triCursor += tot[1];
+            m = tot[0];
+            int2* t = itemsA; itemsA = itemsB; itemsB = t;
+            if (static_cast<size_t>(wideCount) > cap) { err = "LBVH build: 8-wide node count exceeds its bound"; goto fail; }
+        }
+        unsigned int hflag = 0;
+        BVH_CK(cudaMemcpyAsync(&hflag, flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+        BVH_CK(cudaStreamSynchronize(st));
+        if (hflag || triCursor != n) { err = "LBVH build: 8-wide collapse lost triangles"; goto fail; }
+        BVH_CK(cudaMalloc(&out.wnodes, sizeof(WideNode) * wideCount));
+        BVH_CK(cudaMemcpyAsync(out.wnodes, scratch, sizeof(WideNode) * wideCount, cudaMemcpyDeviceToDevice, st));
+        BVH_CK(cudaStreamSynchronize(st));
+        out.nodeCount = wideCount;
+        out.depth = levels;
+        rc = 0;
+    }
+fail:
+    cudaFree(itemsA); cudaFree(itemsB); cudaFree(codes); cudaFree(cntI); cudaFree(cntT); cudaFree(flag);
+    cudaFree(scratch);
+    if (rc != 0) {
+        cudaFree(out.leafTris); out.leafTris = nullptr;
+        cudaFree(out.wnodes); out.wnodes = nullptr;
+    }
+    return rc;
+}
+
+int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, BvhBuildResult& out, cudaStream_t st,
+              std::string& err)
 {
     out = BvhBuildResult{};
     if (n <= 0) return 0;
+    if (width != 2 && width != 8) { err = "LBVH build: tree width must be 2 or 8"; return -1; }
     if (n > kLeafStartMask) { err = "LBVH build: too many triangles for the leaf encoding"; return -1; }
     if (maxLeaf < 1) maxLeaf = 1;
     if (maxLeaf > kMaxLeafTris) maxLeaf = kMaxLeafTris;
@@ -347,6 +610,7 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, BvhBuildResult& out
     int *parentInner = nullptr, *parentLeaf = nullptr, *arrivals = nullptr, *collapsed = nullptr;
     float *innerBox = nullptr, *leafBox = nullptr, *cost = nullptr;
     int2* range = nullptr;
+    float4* sorted = nullptr;   // triangles in sorted (binary leaf) order
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     const int numTiles = (n + kSortTile - 1) / kSortTile;
     const int inner = n > 1 ? n - 1 : 1;
@@ -370,8 +634,8 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, BvhBuildResult& out
         BVH_CK(cudaMalloc(&range, sizeof(int2) * inner));
         BVH_CK(cudaMalloc(&innerBox, sizeof(float) * 6 * inner));
         BVH_CK(cudaMalloc(&leafBox, sizeof(float) * 6 * n));
-        BVH_CK(cudaMalloc(&out.leafTris, sizeof(float4) * 3 * static_cast<size_t>(n)));
-        BVH_CK(cudaMalloc(&out.nodes, sizeof(BvhNode) * inner));
+        BVH_CK(cudaMalloc(&sorted, sizeof(float4) * 3 * static_cast<size_t>(n)));
+        if (width == 2) BVH_CK(cudaMalloc(&out.nodes, sizeof(BvhNode) * inner));
         {
             const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
             BVH_CK(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st));
@@ -392,17 +656,32 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, BvhBuildResult& out
         if (n > 1) {
             kKarras<<<(n - 1 + B - 1) / B, B, 0, st>>>(kin, n, children, parentInner, parentLeaf, range);
         }
-        kRefit<<<G, B, 0, st>>>(dTris, vin, n, children, parentInner, parentLeaf, range, out.leafTris, innerBox, leafBox,
+        kRefit<<<G, B, 0, st>>>(dTris, vin, n, children, parentInner, parentLeaf, range, sorted, innerBox, leafBox,
                                 arrivals, cost, collapsed, maxLeaf);
-        if (n > 1) kEmitNodes<<<(n - 1 + B - 1) / B, B, 0, st>>>(children, innerBox, leafBox, range, collapsed, n, out.nodes);
         BVH_CK(cudaGetLastError());
-        BVH_CK(cudaEventRecord(e1, st));
-        BVH_CK(cudaEventSynchronize(e1));
-        BVH_CK(cudaEventElapsedTime(&out.msBuild, e0, e1));
-        out.nodeCount = n > 1 ? n - 1 : 0;
+        out.width = width;
+        if (width == 8) {
+            if (buildWide(n, maxLeaf < kWideLeafMax ? maxLeaf : kWideLeafMax, children, range, innerBox, leafBox, sorted,
+                          out, st, err) != 0)
+                goto fail;
+            BVH_CK(cudaEventRecord(e1, st));
+            BVH_CK(cudaEventSynchronize(e1));
+            BVH_CK(cudaEventElapsedTime(&out.msBuild, e0, e1));
+            cudaFree(sorted);
+            sorted = nullptr;
+        } else {
+            if (n > 1) kEmitNodes<<<(n - 1 + B - 1) / B, B, 0, st>>>(children, innerBox, leafBox, range, collapsed, n, out.nodes);
+            BVH_CK(cudaGetLastError());
+            BVH_CK(cudaEventRecord(e1, st));
+            BVH_CK(cudaEventSynchronize(e1));
+            BVH_CK(cudaEventElapsedTime(&out.msBuild, e0, e1));
+            out.leafTris = sorted;
+            sorted = nullptr;
+            out.nodeCount = n > 1 ? n - 1 : 0;
+        }
         out.rootIsLeaf = n == 1 ? 1 : 0;
         out.rootCode = ~0;
-        if (n > 1) {   // a scene small enough to be one leaf
+        if (width == 2 && n > 1) {   // a scene small enough to be one leaf
             int rootCollapsed = 0;
             BVH_CK(cudaMemcpyAsync(&rootCollapsed, collapsed, sizeof(int), cudaMemcpyDeviceToHost, st));
             BVH_CK(cudaStreamSynchronize(st));
@@ -417,8 +696,8 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, BvhBuildResult& out
 fail:
     cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
     cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
-    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range);
-    cudaFree(out.leafTris); cudaFree(out.nodes);
+    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range); cudaFree(sorted);
+    cudaFree(out.leafTris); cudaFree(out.nodes); cudaFree(out.wnodes);
     out = BvhBuildResult{};
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);

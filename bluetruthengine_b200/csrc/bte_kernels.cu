@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
 // ---------------------------------------------------------------- extend
 // src/wavefront/ray_extend.cu:49-72 with src/optix_programs.cu:110-148 moved
 // to shade (the hit record is t, u, v, triangle).
+template <int Width>
 __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
         const float4 d = P.d[idx];
         const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
         float t = 0.0f, u = 0.0f, v = 0.0f;
-        const int tri = traceClosest(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
+        const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
         P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
         if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
     }
@@ -199,6 +200,7 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
 // ---------------------------------------------------------------- connect
 // src/wavefront/ray_connect.cu:52-72: occlusion in (1e-4, tMax); an occluded
 // slot loses its visibility bit.
+template <int Width>
 __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.shadowCount[bounce];
@@ -210,7 +212,75 @@ __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int boun
         const float4 o = P.shOrigin[path];
         const float4 d = P.shDir[e];
         const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
-        if (traceOccluded(s, r, kEps, d.w, P.errorFlags)) atomicAnd(P.shMask + path, ~(1u << slot));
+        if (traceOccludedW<Width>(s, r, kEps, d.w, P.errorFlags)) atomicAnd(P.shMask + path, ~(1u << slot));
+    }
+}
+
+// ---------------------------------------------------------------- extend / connect over the 8-wide tree
+// Same results as kExtend / kConnect, but each lane keeps its walk state
+// across iterations and takes a new ray (warp-aggregated fetch from a
+// per-bounce counter) as soon as its current one ends, so that lanes do not
+// idle until the slowest ray of their warp finishes.
+__global__ void __launch_bounds__(256) kExtendWide(DevScene s, DevPaths P, int bounce)
+{
+    const int count = P.rayCount[bounce];
+    const int* __restrict__ q = P.queue[bounce & 1];
+    int* fetch = P.fetch + bounce;
+    WideWalk<false> w;
+    uint2 stack[kWideStack];
+    int idx = -1;
+    while (true) {
+        if (idx < 0) {
+            const int slot = appendCoalesced(fetch);
+            if (slot >= count) break;
+            idx = q[slot];
+            const float4 o = P.o[idx];
+            const float4 d = P.d[idx];
+            const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+            if (!r.valid || s.triCount <= 0) {
+                P.hit[idx] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+                if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = -1;
+                idx = -1;
+                continue;
+            }
+            w.start(r, kEps, 1e30f);
+        }
+        if (w.step(s, stack, P.errorFlags)) {
+            const int tri = w.best;
+            P.hit[idx] = tri >= 0 ? make_float4(w.bt, w.bu, w.bv, __int_as_float(tri))
+                                  : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+            if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
+            idx = -1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int bounce)
+{
+    const int count = P.shadowCount[bounce];
+    int* fetch = P.fetch + (P.maxDepth + 1) + bounce;
+    WideWalk<true> w;
+    uint2 stack[kWideStack];
+    int e = -1;
+    while (true) {
+        if (e < 0) {
+            const int slot = appendCoalesced(fetch);
+            if (slot >= count) break;
+            e = P.shadowQueue[slot];
+            const int path = e / P.slots;
+            const float4 o = P.shOrigin[path];
+            const float4 d = P.shDir[e];
+            const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+            if (!r.valid || s.triCount <= 0) { e = -1; continue; }
+            w.start(r, kEps, d.w);
+        }
+        if (w.step(s, stack, P.errorFlags)) {
+            if (w.hit) {
+                const int path = e / P.slots;
+                atomicAnd(P.shMask + path, ~(1u << (e - path * P.slots)));
+            }
+            e = -1;
+        }
     }
 }
 
@@ -247,6 +317,7 @@ __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float
 }
 
 // ---------------------------------------------------------------- debug / parity kernels
+template <int Width>
 __global__ void kTraceClosestRays(DevScene s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -254,18 +325,19 @@ __global__ void kTraceClosestRays(DevScene s, const float* rays, int n, int* out
     const float* r6 = rays + 6 * static_cast<size_t>(i);
     const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5], s.sceneMaxAbs);
     float t = 0.0f, u = 0.0f, v = 0.0f;
-    const int tri = traceClosest(s, r, kEps, 1e30f, t, u, v, err);
+    const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, err);
     outTri[i] = tri;
     outTuv[3 * i] = t; outTuv[3 * i + 1] = u; outTuv[3 * i + 2] = v;
 }
 
+template <int Width>
 __global__ void kTraceOccludedRays(DevScene s, const float* rays, const float* tmax, int n, uint8_t* out, unsigned int* err)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* r6 = rays + 6 * static_cast<size_t>(i);
     const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5], s.sceneMaxAbs);
-    out[i] = traceOccluded(s, r, kEps, tmax[i], err) ? 1 : 0;
+    out[i] = traceOccludedW<Width>(s, r, kEps, tmax[i], err) ? 1 : 0;
 }
 
 __global__ void kEnvQuery(DevScene s, int op, const float* in, int n, float* out)
@@ -365,7 +437,8 @@ void launchGenerate(const DevPaths& P, const FrameParams& f, cudaStream_t st)
 }
 void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
 {
-    kExtend<<<grid, block, 0, st>>>(s, P, bounce);
+    if (s.bvhWidth == 8) kExtendWide<<<grid, block, 0, st>>>(s, P, bounce);
+    else kExtend<2><<<grid, block, 0, st>>>(s, P, bounce);
 }
 void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block,
                  int minBlocks, cudaStream_t st)
@@ -375,7 +448,8 @@ void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int
 }
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
 {
-    kConnect<<<grid, block, 0, st>>>(s, P, bounce);
+    if (s.bvhWidth == 8) kConnectWide<<<grid, block, 0, st>>>(s, P, bounce);
+    else kConnect<2><<<grid, block, 0, st>>>(s, P, bounce);
 }
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    cudaStream_t st)
@@ -386,12 +460,14 @@ void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double
 void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
                             cudaStream_t st)
 {
-    kTraceClosestRays<<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
+    if (s.bvhWidth == 8) kTraceClosestRays<8><<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
+    else kTraceClosestRays<2><<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
 }
 void launchTraceOccludedRays(const DevScene& s, const float* rays, const float* tmax, int n, uint8_t* out, unsigned int* err,
                              cudaStream_t st)
 {
-    kTraceOccludedRays<<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
+    if (s.bvhWidth == 8) kTraceOccludedRays<8><<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
+    else kTraceOccludedRays<2><<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
 }
 void launchEnvQuery(const DevScene& s, int op, const float* in, int n, float* out, cudaStream_t st)
 {
@@ -416,10 +492,12 @@ int occupancyGrid(int which, int block)
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const void* fn = which == 0 ? reinterpret_cast<const void*>(kExtend)
+    const void* fn = which == 0 ? reinterpret_cast<const void*>(kExtend<2>)
                    : which == 1 ? reinterpret_cast<const void*>(kShade<2>)
                    : which == 3 ? reinterpret_cast<const void*>(kShade<3>)
-                                : reinterpret_cast<const void*>(kConnect);
+                   : which == 4 ? reinterpret_cast<const void*>(kExtendWide)
+                   : which == 5 ? reinterpret_cast<const void*>(kConnectWide)
+                                : reinterpret_cast<const void*>(kConnect<2>);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0) != cudaSuccess || per < 1) per = 1;
     return sms * per;
 }

@@ -28,15 +28,20 @@ int occupancyGrid(int which, int block);
 
 // LBVH build over device triangles (bte_bvh.cu).  Allocates `nodes` and
 // `leafTris`; the caller frees them.  Returns 0 or a CUDA error code.
+// width 2: BVH2 `nodes`; width 8: the 8-wide tree `wnodes` collapsed from the
+// same binary tree.  `leafTris` is in the leaf order of the tree built.
 struct BvhBuildResult {
     BvhNode* nodes = nullptr;
+    WideNode* wnodes = nullptr;
     float4* leafTris = nullptr;
+    int width = 2;
     int nodeCount = 0;
+    int depth = 0;          // levels of the 8-wide tree
     int rootIsLeaf = 0;
     int rootCode = ~0;      // leaf code of the root when rootIsLeaf
     float msBuild = 0.0f;
 };
-int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, BvhBuildResult& out, cudaStream_t st,
+int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, int width, BvhBuildResult& out, cudaStream_t st,
               std::string& err);
 
 // Env-map tables (bte_env.cu).

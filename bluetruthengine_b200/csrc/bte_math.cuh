@@ -27,8 +27,12 @@
 
 #ifdef __CUDACC__
 #define BTE_HD __host__ __device__ __forceinline__
+// The public functions keep one out-of-line copy per kernel: inlined at every
+// call site of the shading code they overflow the instruction cache.
+#define BTE_HDN __host__ __device__ __noinline__ inline
 #else
 #define BTE_HD inline
+#define BTE_HDN inline
 #endif
 
 namespace bte {
@@ -202,19 +206,19 @@ BTE_HD double atan2D(double y, double x)
 }
 
 // ---- float entry points ----
-BTE_HD float sinf_(float x)
+BTE_HDN float sinf_(float x)
 {
     if (x == 0.0f || isnanf_(x)) return x + x * 0.0f;
     if (isinff_(x)) return NAN;
     return static_cast<float>(sinD(static_cast<double>(x)));
 }
-BTE_HD float cosf_(float x)
+BTE_HDN float cosf_(float x)
 {
     if (isnanf_(x)) return x;
     if (isinff_(x)) return NAN;
     return static_cast<float>(cosD(static_cast<double>(x)));
 }
-BTE_HD float tanf_(float x)
+BTE_HDN float tanf_(float x)
 {
     if (x == 0.0f || isnanf_(x)) return x + x * 0.0f;
     if (isinff_(x)) return NAN;
@@ -223,14 +227,14 @@ BTE_HD float tanf_(float x)
     const double s = sinPoly(r), c = cosPoly(r);
     return static_cast<float>((q & 1) ? (-c / s) : (s / c));
 }
-BTE_HD float expf_(float x)
+BTE_HDN float expf_(float x)
 {
     if (isnanf_(x)) return x;
     if (x > 89.0f) return INFINITY;
     if (x < -104.0f) return 0.0f;
     return static_cast<float>(expD(static_cast<double>(x)));
 }
-BTE_HD float logf_(float x)
+BTE_HDN float logf_(float x)
 {
     if (isnanf_(x)) return x;
     if (x < 0.0f) return NAN;
@@ -244,7 +248,7 @@ BTE_HD bool isOddIntF(float y)
     if (!isIntF(y) || fabsf(y) >= 16777216.0f) return false;
     return (static_cast<int64_t>(y) & 1) != 0;
 }
-BTE_HD float powf_(float x, float y)
+BTE_HDN float powf_(float x, float y)
 {
     if (y == 0.0f) return 1.0f;
     if (x == 1.0f) return 1.0f;
@@ -297,7 +301,7 @@ BTE_HD float pow2f_(float x)
 }
 // sin and cos of one argument with a single reduction; bit-identical to
 // sinf_(x) and cosf_(x).
-BTE_HD void sincosf_(float x, float& s, float& c)
+BTE_HDN void sincosf_(float x, float& s, float& c)
 {
     if (isnanf_(x)) { s = x + x * 0.0f; c = x; return; }
     if (isinff_(x)) { s = NAN; c = NAN; return; }
@@ -312,7 +316,7 @@ BTE_HD void sincosf_(float x, float& s, float& c)
     default: s = static_cast<float>(-cp); c = static_cast<float>(sp); break;
     }
 }
-BTE_HD float atan2f_(float y, float x)
+BTE_HDN float atan2f_(float y, float x)
 {
     if (isnanf_(x) || isnanf_(y)) return NAN;
     if (y == 0.0f) {
@@ -329,7 +333,7 @@ BTE_HD float atan2f_(float y, float x)
     if (x == 0.0f) return (y > 0.0f) ? static_cast<float>(kPio2_1) : -static_cast<float>(kPio2_1);
     return static_cast<float>(atan2D(static_cast<double>(y), static_cast<double>(x)));
 }
-BTE_HD float acosf_(float x)
+BTE_HDN float acosf_(float x)
 {
     if (isnanf_(x)) return x;
     if (x > 1.0f || x < -1.0f) return NAN;

@@ -85,9 +85,13 @@ struct Renderer {
     double envTotalPowerD = 0.0;
     bool hasEnv = false;
     // acceleration structure
-    DeviceBuffer bvhNodes, leafTris;
+    DeviceBuffer bvhNodes, wideNodes, leafTris;
     int rootIsLeaf = 0, rootCode = ~0;
-    int maxLeaf = 1;          // autotuned on B200: single-triangle leaves traverse fastest
+    int maxLeaf = 2;          // autotuned on B200 (8-wide tree, 1.04M-triangle scene): up to 2 triangles per leaf
+    int bvhWidth = 8;         // tree built by the next bte_init_accel
+    int postponePct = 20;     // 8-wide walk: leaf-test postponing threshold
+    int builtWidth = 2;       // tree in use
+    int accelNodes = 0, accelDepth = 0;
     int shadeMinBlocks = 3;   // autotuned on B200: 3 resident shade blocks per SM
     bool accelReady = false;
     float msBvh = 0.0f;
@@ -101,8 +105,8 @@ struct Renderer {
     DeviceBuffer accum, accumD, framebuffer;
     uint32_t* extFramebuffer = nullptr;
     // wavefront buffers
-    DeviceBuffer pO, pD, pTp, pL, pHit, q0, q1, rayCount, shadowCount, shadowQueue, shOrigin, shDir, shContrib, shMask,
-        hitLog, errorFlags;
+    DeviceBuffer pO, pD, pTp, pL, pHit, q0, q1, rayCount, shadowCount, fetch, shadowQueue, shOrigin, shDir, shContrib,
+        shMask, hitLog, errorFlags;
     int pathCap = 0, slotCap = 0, depthCap = 0;
     bool hitLogEnabled = false;
     bool stageTiming = false;
@@ -135,6 +139,10 @@ DevScene makeDevScene()
     s.triCount = g.accelReady ? g.triCount : 0;
     s.leafTris = g.leafTris.as<float4>();
     s.nodes = g.bvhNodes.as<BvhNode>();
+    s.wnodes = g.wideNodes.as<WideNode>();
+    s.bvhWidth = g.builtWidth;
+    s.wideNodeCount = g.builtWidth == 8 ? g.accelNodes : 0;
+    s.postponePct = g.postponePct;
     s.rootIsLeaf = g.rootIsLeaf;
     s.rootCode = g.rootCode;
     s.sceneMaxAbs = g.sceneMaxAbs;
@@ -194,7 +202,7 @@ void rebuildTriEmitter()
 
 void releaseWavefront()
 {
-    for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.shadowQueue,
+    for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch, &g.shadowQueue,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
         b->release();
     g.pathCap = g.slotCap = g.depthCap = 0;
@@ -211,6 +219,7 @@ void ensureWavefront(int paths, int slots, int depth)
         ensure(g.q0, P * 4); ensure(g.q1, P * 4);
         ensure(g.rayCount, sizeof(int) * (depth + 1));
         ensure(g.shadowCount, sizeof(int) * (depth + 1));
+        ensure(g.fetch, sizeof(int) * 2 * (depth + 1));
         ensure(g.shadowQueue, P * S * 4);
         ensure(g.shOrigin, P * 16);
         ensure(g.shDir, P * S * 16);
@@ -259,9 +268,9 @@ void renderFrame(int w, int h)
     ensureWavefront(paths, slots, depth);
     const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
     if (g.gridBlock != block) {
-        g.gridExtend = occupancyGrid(0, block);
+        g.gridExtend = occupancyGrid(g.builtWidth == 8 ? 4 : 0, block);
         g.gridShade = occupancyGrid(g.shadeMinBlocks == 3 ? 3 : 1, block);
-        g.gridConnect = occupancyGrid(2, block);
+        g.gridConnect = occupancyGrid(g.builtWidth == 8 ? 5 : 2, block);
         g.gridBlock = block;
     }
     DevPaths P{};
@@ -270,6 +279,7 @@ void renderFrame(int w, int h)
     P.queue[0] = g.q0.as<int>(); P.queue[1] = g.q1.as<int>();
     P.rayCount = g.rayCount.as<int>();
     P.shadowCount = g.shadowCount.as<int>();
+    P.fetch = g.fetch.as<int>();
     P.shadowQueue = g.shadowQueue.as<int>();
     P.shOrigin = g.shOrigin.as<float4>();
     P.shDir = g.shDir.as<float4>();
@@ -290,6 +300,7 @@ void renderFrame(int w, int h)
     cudaStream_t st = g.stream;
     ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
     ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
     ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
     if (g.hitLogEnabled) ck(cudaMemsetAsync(g.hitLog.p, 0xfe, static_cast<size_t>(paths) * depth * 4, st), "cudaMemsetAsync");
     float stage[5] = {0, 0, 0, 0, 0};
@@ -344,6 +355,7 @@ void renderFrame(int w, int h)
     g.frameIndex += static_cast<uint32_t>(spp);
     g.lastPaths = paths; g.lastDepth = depth; g.lastSpp = spp; g.lastW = w; g.lastH = h; g.lastSlots = slots;
     if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
+    if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
 }
 
 template <typename F>
@@ -370,6 +382,17 @@ void setError(const std::string& msg) { g_lastError = msg; }
 
 using namespace bte;
 
+namespace {
+void checkTraceFlags(const unsigned int* dFlags)
+{
+    unsigned int f = 0;
+    ck(cudaMemcpyAsync(&f, dFlags, 4, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+    ck(cudaStreamSynchronize(g.stream), "sync");
+    if (f & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
+    if (f & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+}
+}  // namespace
+
 extern "C" {
 
 const char* bte_last_error(void) { return g_lastError.c_str(); }
@@ -382,7 +405,7 @@ int bte_init_scene(const TriangleData* triangles, int triangleCount, const Float
     (void)imageWidth; (void)imageHeight;
     return guarded([&] {
         g.tris.release(); g.materials.release(); g.triMatIds.release();
-        g.bvhNodes.release(); g.leafTris.release(); g.accelReady = false;
+        g.bvhNodes.release(); g.wideNodes.release(); g.leafTris.release(); g.accelReady = false;
         g.triCount = triangleCount > 0 ? triangleCount : 0;
         g.materialCount = materialCount > 0 ? materialCount : 0;
         if (triangleCount > 0) upload(g.tris, triangles, sizeof(TriangleData) * triangleCount, g.stream);
@@ -411,12 +434,25 @@ int bte_init(const TriangleData* tri, const Float3* color, int imageWidth, int i
 int bte_init_accel(void)
 {
     return guarded([&] {
-        g.bvhNodes.release(); g.leafTris.release(); g.accelReady = false;
+        g.bvhNodes.release(); g.wideNodes.release(); g.leafTris.release(); g.accelReady = false;
         if (!g.tris.p || g.triCount <= 0) throw CudaError{"bte_init_accel: call bte_init_scene first"};
         BvhBuildResult r;
         std::string err;
-        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, r, g.stream, err) != 0) throw CudaError{err};
-        g.bvhNodes.p = r.nodes; g.bvhNodes.bytes = sizeof(BvhNode) * (r.nodeCount > 0 ? r.nodeCount : 1);
+        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, g.bvhWidth, r, g.stream, err) != 0)
+            throw CudaError{err};
+        if (r.width == 8 && 2 * r.depth > kWideStack) {   // node + postponed-leaf groups could overflow: binary tree
+            cudaFree(r.wnodes); cudaFree(r.leafTris);
+            if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, 2, r, g.stream, err) != 0) throw CudaError{err};
+        }
+        if (r.width == 8) {
+            g.wideNodes.p = r.wnodes; g.wideNodes.bytes = sizeof(WideNode) * r.nodeCount;
+        } else {
+            g.bvhNodes.p = r.nodes; g.bvhNodes.bytes = sizeof(BvhNode) * (r.nodeCount > 0 ? r.nodeCount : 1);
+        }
+        g.builtWidth = r.width;
+        g.accelNodes = r.nodeCount;
+        g.accelDepth = r.depth;
+        g.gridBlock = 0;
         g.leafTris.p = r.leafTris; g.leafTris.bytes = sizeof(float4) * 3 * static_cast<size_t>(g.triCount);
         g.rootIsLeaf = r.rootIsLeaf;
         g.rootCode = r.rootCode;
@@ -651,7 +687,7 @@ int bte_cleanup(void)
                                 &g.emitters, &g.emitterTriIndices, &g.emitterTriCdf, &g.sceneEmitterCdf, &g.bsdfs,
                                 &g.triBsdfIds, &g.spots, &g.texTable, &g.texTableMr, &g.envTexels, &g.envMarginal,
                                 &g.envConditional, &g.envRowProb, &g.envRowAlias, &g.envColProb, &g.envColAlias,
-                                &g.envPixelPdf, &g.bvhNodes, &g.leafTris, &g.accum, &g.accumD, &g.framebuffer})
+                                &g.envPixelPdf, &g.bvhNodes, &g.wideNodes, &g.leafTris, &g.accum, &g.accumD, &g.framebuffer})
             b->release();
         for (auto& b : g.tex) b.release();
         for (auto& b : g.texMr) b.release();
@@ -699,14 +735,45 @@ int bte_set_frame_index(uint32_t frameIndex)
 {
     return guarded([&] { g.frameIndex = frameIndex; return 0; });
 }
-int bte_set_tuning(int maxLeafTriangles, int shadeMinBlocks)
+int bte_set_tuning(const BteTuning* t)
 {
     return guarded([&] {
-        if (maxLeafTriangles < 1 || maxLeafTriangles > kMaxLeafTris) throw CudaError{"bte_set_tuning: maxLeafTriangles in [1, 64]"};
-        if (shadeMinBlocks != 2 && shadeMinBlocks != 3) throw CudaError{"bte_set_tuning: shadeMinBlocks must be 2 or 3"};
-        g.maxLeaf = maxLeafTriangles;
-        g.shadeMinBlocks = shadeMinBlocks;
+        if (!t) throw CudaError{"bte_set_tuning: null tuning"};
+        if (t->bvhWidth != 2 && t->bvhWidth != 8) throw CudaError{"bte_set_tuning: bvhWidth must be 2 or 8"};
+        const int leafMax = t->bvhWidth == 8 ? kWideLeafMax : kMaxLeafTris;
+        if (t->maxLeafTriangles < 1 || t->maxLeafTriangles > leafMax)
+            throw CudaError{"bte_set_tuning: maxLeafTriangles must be in [1, 64] (binary) or [1, 3] (8-wide)"};
+        if (t->shadeMinBlocks != 2 && t->shadeMinBlocks != 3) throw CudaError{"bte_set_tuning: shadeMinBlocks must be 2 or 3"};
+        if (t->postponePercent < 0 || t->postponePercent > 100) throw CudaError{"bte_set_tuning: postponePercent in [0, 100]"};
+        g.bvhWidth = t->bvhWidth;
+        g.maxLeaf = t->maxLeafTriangles;
+        g.shadeMinBlocks = t->shadeMinBlocks;
+        g.postponePct = t->postponePercent;
         g.gridBlock = 0;   // recompute persistent grids
+        return 0;
+    });
+}
+
+int bte_get_tuning(BteTuning* t)
+{
+    return guarded([&] {
+        if (!t) throw CudaError{"bte_get_tuning: null tuning"};
+        t->bvhWidth = g.bvhWidth;
+        t->maxLeafTriangles = g.maxLeaf;
+        t->shadeMinBlocks = g.shadeMinBlocks;
+        t->postponePercent = g.postponePct;
+        return 0;
+    });
+}
+
+int bte_get_accel_info(int* width, int* nodeCount, int* depth, float* msBuild)
+{
+    return guarded([&] {
+        if (!g.accelReady) throw CudaError{"bte_get_accel_info: no acceleration structure (bte_init_accel)"};
+        if (width) *width = g.builtWidth;
+        if (nodeCount) *nodeCount = g.accelNodes;
+        if (depth) *depth = g.accelDepth;
+        if (msBuild) *msBuild = g.msBvh;
         return 0;
     });
 }
@@ -795,6 +862,7 @@ int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv)
         ck(cudaStreamSynchronize(g.stream), "trace");
         ck(cudaMemcpyAsync(outTri, di.p, sizeof(int) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         ck(cudaMemcpyAsync(outTuv, dt.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        checkTraceFlags(de.p);
         return 0;
     });
 }
@@ -814,6 +882,7 @@ int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* out
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "trace");
         ck(cudaMemcpyAsync(outOccluded, dout.p, n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
+        checkTraceFlags(de.p);
         return 0;
     });
 }

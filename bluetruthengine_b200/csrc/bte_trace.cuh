@@ -1,4 +1,4 @@
-// bte_trace.cuh -- ray traversal: watertight ray/triangle test and BVH2 walk.
+// bte_trace.cuh -- ray traversal: watertight ray/triangle test, BVH2 and 8-wide walks.
 //
 // Replaces the OptiX calls of the reference (rt_optix_shading.cuh:57-95,
 // closest hit in [1e-4, 1e30] and first-hit occlusion in [1e-4, tMax]) with
@@ -32,7 +32,7 @@ struct RayPre {
     bool valid;
 };
 
-constexpr float kTriErrK = 64.0f;
+constexpr float kTriErrK = 96.0f;
 
 BTE_DI float comp3(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
 
@@ -209,6 +209,191 @@ BTE_DI bool traceOccluded(const DevScene& s, const RayPre& r, float tmin, float 
         node = stack[--sp];
     }
     return false;
+}
+
+// ---------------------------------------------------------------- 8-wide traversal
+// One ray per thread over WideNode.  A node fetch tests all eight child boxes
+// (decoded exactly as the build decoded them, then the same robust slab test
+// as above), giving a mask of internal children to visit, keyed by
+// slot ^ octant so that the lowest set bit is the child nearest the ray's
+// origin side, and a mask of the node's leaf triangles to test.  The stack
+// holds (childBase, remaining keys << 8 | imask) groups and deferred leaf
+// groups (triBase, kTriGroup | mask): when few lanes of a warp have leaf
+// tests, they are pushed and run later with more lanes (the postponing of
+// Ylitie, Karras and Laine, HPG 2017).
+BTE_DI float wideScale(uint32_t e) { return __uint_as_float(e << 23); }
+// byte (selected by `sel` from x) as a float: 0x4b0000qq is 2^23 + q exactly
+constexpr uint32_t kTriGroup = 0x80000000u;   // stack entry holds (triBase, leaf-test mask)
+
+BTE_DI float byteToFloat(uint32_t x, uint32_t sel)
+{
+    return __uint_as_float(__byte_perm(x, 0x4b000000u, sel)) - 8388608.0f;
+}
+
+// The walk's state, advanced one iteration at a time so that a kernel can
+// give a lane a new ray as soon as its current one ends.
+template <bool AnyHit>
+struct WideWalk {
+    RayPre r;
+    int sp, visits, best;
+    uint32_t oct, nBase, nBits, tBase, tHits;
+    float tmin, tmax, bt, bu, bv;
+    bool hit;   // any-hit result
+
+    BTE_DI void start(const RayPre& ray, float t0, float t1)
+    {
+        r = ray;
+        tmin = t0; tmax = t1;
+        oct = (r.ix < 0.0f ? 1u : 0u) | (r.iy < 0.0f ? 2u : 0u) | (r.iz < 0.0f ? 4u : 0u);
+        sp = 0; visits = 0; best = -1;
+        bt = t1; bu = 0.0f; bv = 0.0f;
+        nBase = 0; nBits = ((1u << oct) << 8) | 1u;     // the root as the only child of a virtual parent
+        tBase = 0; tHits = 0;
+        hit = false;
+    }
+
+    // One iteration: at most one node fetch, then that node's (or a deferred
+    // group's) leaf tests, then a pop.  Returns true when the walk has ended.
+    // `stack` is the lane's kWideStack-entry array (kept outside the struct
+    // so that the scalar state stays in registers).
+    BTE_DI bool step(const DevScene& s, uint2* stack, unsigned int* errorFlags)
+    {
+        if (nBits >> 8) {
+            const uint32_t hits = nBits >> 8;
+            const uint32_t key = static_cast<uint32_t>(__ffs(hits) - 1);
+            const uint32_t rest = hits & (hits - 1u);
+            const uint32_t slot = key ^ oct;
+            const uint32_t imaskP = nBits & 0xffu;
+            const int child = static_cast<int>(nBase) + __popc(imaskP & ((1u << slot) - 1u));
+            if (child < 0 || child >= s.wideNodeCount || ++visits > s.wideNodeCount) {   // never true for a built tree
+                if (errorFlags) atomicOr(errorFlags, 2u);
+                return true;
+            }
+            if (rest) {
+                if (sp < kWideStack) stack[sp++] = make_uint2(nBase, (rest << 8) | imaskP);
+                else if (errorFlags) atomicOr(errorFlags, 1u);
+            }
+            const float4* np = reinterpret_cast<const float4*>(s.wnodes) + 5 * static_cast<size_t>(child);
+            const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3), f4 = __ldg(np + 4);
+            const uint32_t em = __float_as_uint(f0.w);
+            const uint32_t imask = em >> 24;
+            // Child plane distance t = (p + q * 2^e - o) / d evaluated as fma(q, 2^e / d, (p - o) / d): the
+            // power-of-two product is exact, and the two remaining roundings are covered by the per-ray slab
+            // widening (|p + q 2^e| stays within a small multiple of the scene extent).
+            const float ax = wideScale(em & 0xffu) * r.ix, ay = wideScale((em >> 8) & 0xffu) * r.iy,
+                        az = wideScale((em >> 16) & 0xffu) * r.iz;
+            const float cx = (f0.x - r.ox) * r.ix, cy = (f0.y - r.oy) * r.iy, cz = (f0.z - r.oz) * r.iz;
+            // slab widening folded into the offsets (its rounding is far inside the widening's margin)
+            const float cnx = cx - r.px, cfx = cx + r.px, cny = cy - r.py, cfy = cy + r.py, cnz = cz - r.pz,
+                        cfz = cz + r.pz;
+            const uint32_t meta[2] = {__float_as_uint(f1.z), __float_as_uint(f1.w)};
+            // near plane = low side where the direction is positive, high side where it is negative
+            const bool sxn = oct & 1u, syn = oct & 2u, szn = oct & 4u;
+            const uint32_t nx[2] = {__float_as_uint(sxn ? f3.z : f2.x), __float_as_uint(sxn ? f3.w : f2.y)};
+            const uint32_t fx[2] = {__float_as_uint(sxn ? f2.x : f3.z), __float_as_uint(sxn ? f2.y : f3.w)};
+            const uint32_t ny[2] = {__float_as_uint(syn ? f4.x : f2.z), __float_as_uint(syn ? f4.y : f2.w)};
+            const uint32_t fy[2] = {__float_as_uint(syn ? f2.z : f4.x), __float_as_uint(syn ? f2.w : f4.y)};
+            const uint32_t nz[2] = {__float_as_uint(szn ? f4.z : f3.x), __float_as_uint(szn ? f4.w : f3.y)};
+            const uint32_t fz[2] = {__float_as_uint(szn ? f3.x : f4.z), __float_as_uint(szn ? f3.y : f4.w)};
+            const float cull = AnyHit ? tmax * kCullMargin : bt * kCullMargin;
+            uint32_t newHits = 0, triMask = 0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int w = c >> 2;
+                const uint32_t sel = static_cast<uint32_t>(c & 3) | 0x7440u;   // byte c, two zero bytes, 0x4b
+                const uint32_t mb = (meta[w] >> (8 * (c & 3))) & 0xffu;
+                const bool inner = (imask >> c) & 1u;
+                if (!inner && mb == 0u) continue;
+                const float tnx = __fmaf_rn(byteToFloat(nx[w], sel), ax, cnx);
+                const float tfx = __fmaf_rn(byteToFloat(fx[w], sel), ax, cfx);
+                const float tny = __fmaf_rn(byteToFloat(ny[w], sel), ay, cny);
+                const float tfy = __fmaf_rn(byteToFloat(fy[w], sel), ay, cfy);
+                const float tnz = __fmaf_rn(byteToFloat(nz[w], sel), az, cnz);
+                const float tfz = __fmaf_rn(byteToFloat(fz[w], sel), az, cfz);
+                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, cull)) * kBoxGrow;
+                if (tn <= tf) {
+                    if (inner) newHits |= 1u << (static_cast<uint32_t>(c) ^ oct);
+                    else triMask |= ((1u << (mb >> 5)) - 1u) << (mb & 31u);
+                }
+            }
+            nBase = static_cast<uint32_t>(__float_as_int(f1.x));
+            nBits = (newHits << 8) | imask;
+            tBase = static_cast<uint32_t>(__float_as_int(f1.y));
+            tHits = triMask;
+        }
+        {   // defer this node's leaf tests while few lanes of the warp have any (more will join later)
+            const uint32_t conv = __activemask();
+            const uint32_t want = __ballot_sync(conv, tHits != 0u);
+            if (tHits != 0u && (nBits >> 8) != 0u && sp < kWideStack &&
+                100u * static_cast<uint32_t>(__popc(want)) < static_cast<uint32_t>(s.postponePct * __popc(conv))) {
+                stack[sp++] = make_uint2(tBase, kTriGroup | tHits);
+                tHits = 0;
+            }
+        }
+        while (tHits) {
+            const int k = __ffs(tHits) - 1;
+            tHits &= tHits - 1u;
+            if (tBase + static_cast<uint32_t>(k) >= static_cast<uint32_t>(s.triCount)) {
+                if (errorFlags) atomicOr(errorFlags, 2u);
+                continue;
+            }
+            const float4* tp = s.leafTris + 3 * (static_cast<size_t>(tBase) + static_cast<size_t>(k));
+            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t, u, v;
+            if (isectTri(r, a, b, c, tmin, AnyHit ? tmax : bt, t, u, v)) {
+                if (AnyHit) { hit = true; return true; }
+                const int idx = __float_as_int(a.w);
+                if (best < 0 || t < bt || (t == bt && idx < best)) { best = idx; bt = t; bu = u; bv = v; }
+            }
+        }
+        if ((nBits >> 8) == 0u) {
+            if (sp == 0) return true;
+            const uint2 e = stack[--sp];
+            if (e.y & kTriGroup) {   // a deferred leaf group: test it next, with no node work pending
+                tBase = e.x;
+                tHits = e.y & ~kTriGroup;
+                nBits = 0;
+            } else {
+                nBase = e.x;
+                nBits = e.y;
+            }
+        }
+        return false;
+    }
+};
+
+template <bool AnyHit>
+BTE_DI int traceWide(const DevScene& s, const RayPre& r, float tmin, float tmax, float& tOut, float& uOut, float& vOut,
+                     unsigned int* errorFlags)
+{
+    if (!r.valid || s.triCount <= 0) return -1;
+    WideWalk<AnyHit> w;
+    uint2 stack[kWideStack];
+    w.start(r, tmin, tmax);
+    while (!w.step(s, stack, errorFlags)) {
+    }
+    if (AnyHit) return w.hit ? 1 : -1;
+    if (w.best >= 0) { tOut = w.bt; uOut = w.bu; vOut = w.bv; }
+    return w.best;
+}
+
+// Dispatch on the tree the scene was built with (uniform across a launch).
+template <int Width>
+BTE_DI int traceClosestW(const DevScene& s, const RayPre& r, float tmin, float tmax, float& t, float& u, float& v,
+                         unsigned int* errorFlags)
+{
+    if (Width == 8) return traceWide<false>(s, r, tmin, tmax, t, u, v, errorFlags);
+    return traceClosest(s, r, tmin, tmax, t, u, v, errorFlags);
+}
+template <int Width>
+BTE_DI bool traceOccludedW(const DevScene& s, const RayPre& r, float tmin, float tmax, unsigned int* errorFlags)
+{
+    if (Width == 8) {
+        float t, u, v;
+        return traceWide<true>(s, r, tmin, tmax, t, u, v, errorFlags) >= 0;
+    }
+    return traceOccluded(s, r, tmin, tmax, errorFlags);
 }
 
 }  // namespace bte

@@ -43,12 +43,36 @@ constexpr int kLeafCountShift = 25;
 constexpr int kLeafStartMask = (1 << kLeafCountShift) - 1;
 constexpr int kMaxLeafTris = 64;
 
+// 8-wide node with 8-bit quantised child boxes (80 bytes, five 16-byte
+// loads).  Child box coordinate = fma(q, 2^(e-127), p) per axis, which the
+// build makes contain the child's exact box.  Internal children are stored
+// consecutively from childBase in slot order (child of slot s =
+// childBase + popc(imask & ((1<<s)-1))); a leaf slot's meta byte is
+// offset | count << 5 into the node's triangles starting at triBase; a slot
+// with neither is empty.  Slots are assigned so that a ray of direction
+// octant q visits them in increasing (slot ^ q) order, near side first.
+struct WideNode {
+    float px, py, pz;
+    uint32_t expImask;            // ex | ey << 8 | ez << 16 | imask << 24
+    int childBase;
+    int triBase;
+    uint32_t meta[2];
+    uint32_t qlox[2], qloy[2], qloz[2], qhix[2], qhiy[2], qhiz[2];
+};
+static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
+constexpr int kWideLeafMax = 3;
+constexpr int kWideStack = 64;    // traversal stack entries; trees deeper than half of it use the binary tree
+
 struct DevScene {
     // geometry
     const TriangleData* tris;         // reference AoS, original triangle order
     int triCount;
-    const float4* leafTris;           // [triCount*3] v0.xyz|origIndex, v1.xyz, v2.xyz in leaf order
+    const float4* leafTris;           // [triCount*3] v0.xyz|origIndex, v1.xyz, v2.xyz in leaf order of the tree in use
     const BvhNode* nodes;             // root = node 0 (triCount >= 2) or a single-leaf root
+    const WideNode* wnodes;           // 8-wide tree (root = node 0) when bvhWidth == 8
+    int bvhWidth;                     // 2 or 8
+    int wideNodeCount;
+    int postponePct;                  // leaf-test postponing threshold of the 8-wide walk (percent of lanes)
     int rootIsLeaf;                   // the whole scene is one leaf
     int rootCode;                     // its leaf code
     float sceneMaxAbs;                // max |coordinate| over all vertices (traversal error bound)
@@ -80,6 +104,7 @@ struct DevPaths {
     int* queue[2];    // ping-pong ray queues of path indices
     int* rayCount;    // [maxDepth+1] active paths per bounce
     int* shadowCount; // [maxDepth] shadow rays per bounce
+    int* fetch;       // [2*(maxDepth+1)] ray-fetch counters of the extend / connect launches
     int* shadowQueue; // entries path*slots + slot
     float4* shOrigin; // [paths] hit point of the NEE rays of the current bounce
     float4* shDir;    // [paths*slots] direction | tmax
@@ -89,7 +114,7 @@ struct DevPaths {
     int slots;        // 1 (area) + spotCount + 1 (env)
     int maxDepth;
     int count;        // paths in the frame
-    unsigned int* errorFlags;   // bit 0: traversal stack overflow
+    unsigned int* errorFlags;   // bit 0: traversal stack overflow; bit 1: malformed tree (index out of range)
 };
 
 struct FrameParams {

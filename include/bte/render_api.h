@@ -105,10 +105,20 @@ int bte_read_accum_f64(double* hostRGBSum);          /* FP64 running sum of samp
 int bte_read_sample_radiance(float* hostRGB, int count);  /* per-path radiance of the last frame [W*H*spp*3] */
 int bte_read_hit_log(int* hostTri, int count);       /* per-bounce closest-hit triangle of the last frame */
 int bte_set_hit_log(int enabled);                    /* record [path][bounce] hit triangles (debug/parity) */
-/* Acceleration-structure and kernel tuning (used by the autotuner): maximum
- * triangles per BVH leaf (1-64, applied at the next bte_init_accel) and the
- * minimum resident blocks per SM the shade kernel is compiled for (2 or 3). */
-int bte_set_tuning(int maxLeafTriangles, int shadeMinBlocks);
+/* Acceleration-structure and kernel tuning (what the autotuner sweeps).
+ * Width and leaf size apply at the next bte_init_accel, the rest at once. */
+typedef struct {
+    int bvhWidth;          /* 2: binary LBVH; 8: 8-wide tree with 8-bit quantised child boxes */
+    int maxLeafTriangles;  /* 1-64 (binary tree), 1-3 (8-wide tree) */
+    int shadeMinBlocks;    /* resident blocks per SM the shade kernel is compiled for: 2 or 3 */
+    int postponePercent;   /* 8-wide walk: a lane defers its leaf tests while fewer than this
+                            * percentage of the warp's lanes have leaf tests (0 = never, 0-100) */
+} BteTuning;
+int bte_set_tuning(const BteTuning* tuning);
+int bte_get_tuning(BteTuning* tuning);
+/* The acceleration structure in use: width (2 or 8), node count, levels of
+ * the 8-wide tree (0 for width 2) and device build time. */
+int bte_get_accel_info(int* width, int* nodeCount, int* depth, float* msBuild);
 
 /* ---- debug/parity entry points over device-resident state ---- */
 /* closest hit for n rays [origin, dir] (host arrays): triangle index (-1 miss) and t, u, v */

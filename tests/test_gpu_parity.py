@@ -49,16 +49,21 @@ def test_math_functions_bitexact(renderer, oracle_mod):
         assert len(bad) == 0, f"fn {fn}: {len(bad)} mismatches"
 
 
-def _upload(renderer, scene, env_mode=0, spp=1, depth=8):
+def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1):
     renderer.cleanup()
+    renderer.set_tuning(max_leaf, 3, bvh_width)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
 
+@pytest.mark.parametrize("tree", [(8, 1), (8, 3), (2, 1), (2, 4)])
 @pytest.mark.parametrize("scene_name", ["cornell_scene", "random_scene"])
-def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name):
+def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, tree):
+    """Closest hit (triangle, t, u, v) and any-hit occlusion for 40k rays, both tree widths and several
+    leaf sizes, against the oracle's brute force over all triangles."""
     scene = request.getfixturevalue(scene_name)
-    _upload(renderer, scene)
+    _upload(renderer, scene, bvh_width=tree[0], max_leaf=tree[1])
+    assert renderer.accel_info()["width"] == tree[0]
     orc = oracle_mod.Oracle(libm=False)
     view = oracle_mod.SceneView(scene, oracle=orc, build_accel=False)
     tri = scene.triangles
@@ -243,14 +248,19 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode", [1, 0])
-def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode):
+@pytest.mark.parametrize("env_mode,bvh_width", [(1, 8), (0, 8), (1, 2)])
+def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
     pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
-    _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth)
+    _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width)
+    info = renderer.accel_info()
+    print("accel", info)
+    assert info["width"] == bvh_width
+    if bvh_width == 8:
+        assert 0 < info["depth"] <= 64 and info["nodes"] < scene.triangle_count // 2
     renderer.set_hit_log(True)
     renderer.reset_accumulation(W, H)
     renderer.render(W, H)
@@ -298,3 +308,15 @@ def test_textured_materials_bitexact(renderer, oracle_mod, random_scene):
     assert eq.all(), f"{np.sum(~eq)} of {len(o)} samples differ"
     renderer.init_textures(None)
     renderer.init_mr_textures(None)
+
+
+def test_tuning_roundtrip_and_validation(renderer):
+    """bte_set_tuning / bte_get_tuning: values round-trip; out-of-range values are rejected with a message."""
+    import bluetruthengine_b200 as B
+    renderer.set_tuning(2, 2, 8, 35)
+    assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35}
+    for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101)]:
+        with pytest.raises(B.BteError):
+            renderer.set_tuning(*bad)
+    renderer.set_tuning()
+    assert renderer.tuning()["bvhWidth"] == 8
