@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of replaying the frame graph")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -211,7 +212,8 @@ def run_ours(args):
     r = bte.Renderer()
     r.upload(scene)
     env_mode = bte.ENV_ALIAS if args.env == "alias" else bte.ENV_CDF
-    r.set_config(samples_per_frame=args.spp, max_depth=args.depth, rr_start=3, env_sampling=env_mode)
+    r.set_config(samples_per_frame=args.spp, max_depth=args.depth, rr_start=3, env_sampling=env_mode,
+                 use_graph=0 if args.no_graph else 1)
     r.reset_accumulation(W, H)
     # disjoint sample ranges per rank (every frame below draws from this rank's range)
     from bluetruthengine_b200 import distributed as D
@@ -287,7 +289,8 @@ def run_ours(args):
            "config": {"workload": "disney_spheres_1080p", "width": W, "height": H, "spp_per_step": args.spp,
                       "max_depth": args.depth, "triangles": int(scene.triangle_count), "env_sampling": args.env,
                       "l2": "inputs larger than L2 (path state %d MB per step)" % (spp_samples * 150 // (1 << 20)),
-                      "parallelism": "replicas over sample ranges x%d" % world},
+                      "parallelism": "replicas over sample ranges x%d" % world,
+                      "frame_launch": "stream" if args.no_graph else "cuda graph", "tuning": r.tuning()},
            "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": 56,
                    "d2h_bytes_per_step": W * H * 4 + (3 * (args.depth + 1) * 4)},
            "gpu_launches": launches_per_frame * args.steps,

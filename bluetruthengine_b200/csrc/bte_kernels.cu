@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
     const int pix = i % wh;
     const int s = i / wh;
     const int px = pix % f.width, py = pix / f.width;
-    uint32_t rng = rngSeed(static_cast<uint32_t>(pix), f.frameIndex + static_cast<uint32_t>(s));
+    uint32_t rng = rngSeed(static_cast<uint32_t>(pix), *f.frameIndex + static_cast<uint32_t>(s));
     const float jx = rngNext(rng) - 0.5f;
     const float jy = rngNext(rng) - 0.5f;
     V3 o, d;
@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float
     const int pix = blockIdx.x * blockDim.x + threadIdx.x;
     const int wh = f.width * f.height;
     if (pix >= wh) return;
+    const uint32_t frameIndex = *f.frameIndex;
     float ax = accum[3 * pix], ay = accum[3 * pix + 1], az = accum[3 * pix + 2];
     double sx = accumD[3 * pix], sy = accumD[3 * pix + 1], sz = accumD[3 * pix + 2];
     for (int s = 0; s < f.spp; ++s) {
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float
         const float4 L4 = P.L[idx];
         V3 L = resolveShadows(P, idx, v3(L4.x, L4.y, L4.z));
         P.L[idx] = make_float4(L.x, L.y, L.z, L4.w);
-        const float n = static_cast<float>(f.frameIndex + static_cast<uint32_t>(s) + 1u);
+        const float n = static_cast<float>(frameIndex + static_cast<uint32_t>(s) + 1u);
         ax = ax + (L.x - ax) / n;
         ay = ay + (L.y - ay) / n;
         az = az + (L.z - az) / n;

@@ -113,6 +113,13 @@ struct Renderer {
     int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
     BteFrameStats stats{};
     int gridExtend = 0, gridShade = 0, gridConnect = 0, gridBlock = 0;
+    // frame index read by the kernels from device memory (pinned host word -> device word each frame)
+    uint32_t* hFrameIndex = nullptr;
+    DeviceBuffer dFrameIndex;
+    // captured frame (memsets, generate, the bounce loop, present) and the launch parameters it was captured with
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+    std::vector<unsigned char> graphKey;
 };
 
 Renderer g;
@@ -129,12 +136,15 @@ void ensureInit()
     ck(cudaEventCreate(&g.ev0), "cudaEventCreate");
     ck(cudaEventCreate(&g.ev1), "cudaEventCreate");
     for (auto& e : g.stageEv) ck(cudaEventCreate(&e), "cudaEventCreate");
+    ck(cudaHostAlloc(reinterpret_cast<void**>(&g.hFrameIndex), sizeof(uint32_t), cudaHostAllocDefault), "cudaHostAlloc");
+    ensure(g.dFrameIndex, sizeof(uint32_t));
     g.init = true;
 }
 
 DevScene makeDevScene()
 {
-    DevScene s{};
+    DevScene s;
+    std::memset(&s, 0, sizeof(s));   // padding too: the struct's bytes key the captured frame graph
     s.tris = g.tris.as<TriangleData>();
     s.triCount = g.accelReady ? g.triCount : 0;
     s.leafTris = g.leafTris.as<float4>();
@@ -200,8 +210,18 @@ void rebuildTriEmitter()
     upload(g.triEmitter, t.data(), t.size() * sizeof(int), g.stream);
 }
 
+void releaseGraph()
+{
+    if (g.graphExec) cudaGraphExecDestroy(g.graphExec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g.graphExec = nullptr;
+    g.graph = nullptr;
+    g.graphKey.clear();
+}
+
 void releaseWavefront()
 {
+    releaseGraph();
     for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch, &g.shadowQueue,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
         b->release();
@@ -273,7 +293,8 @@ void renderFrame(int w, int h)
         g.gridConnect = occupancyGrid(g.builtWidth == 8 ? 5 : 2, block);
         g.gridBlock = block;
     }
-    DevPaths P{};
+    DevPaths P;
+    std::memset(&P, 0, sizeof(P));
     P.o = g.pO.as<float4>(); P.d = g.pD.as<float4>(); P.tp = g.pTp.as<float4>(); P.L = g.pL.as<float4>();
     P.hit = g.pHit.as<float4>();
     P.queue[0] = g.q0.as<int>(); P.queue[1] = g.q1.as<int>();
@@ -290,30 +311,75 @@ void renderFrame(int w, int h)
     P.maxDepth = depth;
     P.count = paths;
     P.errorFlags = g.errorFlags.as<unsigned int>();
-    FrameParams f{};
+    FrameParams f;
+    std::memset(&f, 0, sizeof(f));
     f.width = w; f.height = h; f.spp = spp;
-    f.frameIndex = g.frameIndex;
+    f.frameIndex = g.dFrameIndex.as<uint32_t>();
     f.rrStart = g.cfg.rrStart;
     f.tanHalf = m::tanf_(0.5f * g.camera.fovYRadians);
     f.cam = g.camera;
     const DevScene s = makeDevScene();
     cudaStream_t st = g.stream;
-    ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
-    if (g.hitLogEnabled) ck(cudaMemsetAsync(g.hitLog.p, 0xfe, static_cast<size_t>(paths) * depth * 4, st), "cudaMemsetAsync");
-    float stage[5] = {0, 0, 0, 0, 0};
-    ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
-    if (!g.stageTiming) {
+    *g.hFrameIndex = g.frameIndex;   // the previous frame synchronised, so no copy still reads this word
+    float* accumF = g.accum.as<float>();
+    double* accumDv = g.accumD.as<double>();
+    uint32_t* fb = g.framebuffer.as<uint32_t>();
+    auto prologue = [&] {
+        ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+        if (g.hitLogEnabled) ck(cudaMemsetAsync(g.hitLog.p, 0xfe, static_cast<size_t>(paths) * depth * 4, st), "cudaMemsetAsync");
+        ck(cudaMemcpyAsync(g.dFrameIndex.p, g.hFrameIndex, sizeof(uint32_t), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+    };
+    auto frameLaunches = [&] {
         launchGenerate(P, f, st);
         for (int b = 0; b < depth; ++b) {
             launchExtend(s, P, b, g.gridExtend, block, st);
             launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
             launchConnect(s, P, b, g.gridConnect, block, st);
         }
-        launchPresent(P, f, g.accum.as<float>(), g.accumD.as<double>(), g.framebuffer.as<uint32_t>(), g.extFramebuffer, st);
+        launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, st);
+    };
+    float stage[5] = {0, 0, 0, 0, 0};
+    if (g.cfg.useGraph && !g.stageTiming) {
+        // One graph per launch configuration: every kernel argument is part of the key, so a change of
+        // scene, buffers, image size, depth or tuning re-captures; the frame index travels through memory.
+        std::vector<unsigned char> key;
+        auto put = [&](const void* p, size_t n) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            key.insert(key.end(), c, c + n);
+        };
+        const int ints[8] = {depth, block, g.gridExtend, g.gridShade, g.gridConnect, g.shadeMinBlocks, paths,
+                             g.hitLogEnabled ? 1 : 0};
+        const void* ptrs[4] = {accumF, accumDv, fb, g.extFramebuffer};
+        put(&P, sizeof(P)); put(&f, sizeof(f)); put(&s, sizeof(s)); put(ints, sizeof(ints)); put(ptrs, sizeof(ptrs));
+        if (!g.graphExec || key != g.graphKey) {
+            releaseGraph();
+            ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            try {
+                prologue();
+                frameLaunches();
+                ck(cudaGetLastError(), "kernel launch (capture)");
+            } catch (...) {
+                cudaGraph_t broken = nullptr;
+                cudaStreamEndCapture(st, &broken);
+                if (broken) cudaGraphDestroy(broken);
+                throw;
+            }
+            ck(cudaStreamEndCapture(st, &g.graph), "cudaStreamEndCapture");
+            ck(cudaGraphInstantiate(&g.graphExec, g.graph, 0), "cudaGraphInstantiate");
+            g.graphKey = key;
+        }
+        ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+        ck(cudaGraphLaunch(g.graphExec, st), "cudaGraphLaunch");
+    } else if (!g.stageTiming) {
+        ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+        prologue();
+        frameLaunches();
     } else {
+        prologue();
+        ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
         // per-stage device time, summed over bounces (adds a sync per stage)
         auto timed = [&](int k, auto&& fn) {
             ck(cudaEventRecord(g.stageEv[0], st), "cudaEventRecord");
@@ -330,9 +396,7 @@ void renderFrame(int w, int h)
             timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st); });
             timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
         }
-        timed(4, [&] {
-            launchPresent(P, f, g.accum.as<float>(), g.accumD.as<double>(), g.framebuffer.as<uint32_t>(), g.extFramebuffer, st);
-        });
+        timed(4, [&] { launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, st); });
     }
     ck(cudaGetLastError(), "kernel launch");
     ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
@@ -692,6 +756,7 @@ int bte_cleanup(void)
         for (auto& b : g.tex) b.release();
         for (auto& b : g.texMr) b.release();
         g.tex.clear(); g.texMr.clear();
+        releaseGraph();
         releaseWavefront();
         g.triCount = g.materialCount = g.emitterCount = g.bsdfCount = g.spotCount = g.textureCount = 0;
         g.hasEnv = false; g.hasMr = false; g.accelReady = false;

@@ -119,7 +119,8 @@ struct DevPaths {
 
 struct FrameParams {
     int width, height, spp;
-    uint32_t frameIndex;          // samples accumulated before this frame
+    const uint32_t* frameIndex;   // device word: samples accumulated before this frame (read by the kernels,
+                                  // so a captured frame graph replays with a new value)
     int rrStart;
     float tanHalf;
     CameraData cam;
