@@ -304,6 +304,16 @@ class Renderer:
     def set_stage_timing(self, on: bool):
         _check(self.lib.bte_set_stage_timing(1 if on else 0))
 
+    def set_aov(self, enabled: bool):
+        """Accumulate first-hit albedo and shading normal per pixel (denoiser features)."""
+        _check(self.lib.bte_set_aov(1 if enabled else 0))
+
+    def read_aov(self, width: int, height: int):
+        """(albedo [H, W, 3], normal [H, W, 3]) running means, float32."""
+        out = np.empty((height, width, 6), dtype=np.float32)
+        _check(self.lib.bte_read_aov(out.ctypes.data_as(C.c_void_p)))
+        return out[..., :3].copy(), out[..., 3:].copy()
+
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
                    postpone_percent: int = 20):
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent))

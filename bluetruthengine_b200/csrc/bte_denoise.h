@@ -1,0 +1,33 @@
+// bte_denoise.h -- launchers of the denoiser kernels (bte_denoise_kernels.cu).
+// Tensors are NHWC bf16 (passed as void*), channel counts multiples of 16.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace bte {
+namespace dn {
+
+// Y = act(conv3x3(X, Wk) + bias); Wk[9][Cout][Cin] bf16, zero padding at the borders.
+void conv3x3(const void* X, int N, int H, int W, int Cin, const void* Wk, const float* bias, int Cout, bool relu, void* Y,
+             cudaStream_t st);
+// dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
+void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
+void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);
+void reluMask(const void* Y, const void* dY, void* out, long long elems, cudaStream_t st);
+void pool2(const void* X, int N, int H, int W, int C, void* Y, cudaStream_t st);
+void pool2Back(const void* dY, int N, int H, int W, int C, void* dX, cudaStream_t st);   // adds into dX
+void upCat(const void* A, int Ca, const void* B, int Cb, int N, int H, int W, void* out, cudaStream_t st);
+void upCatBack(const void* dOut, int Ca, int Cb, int N, int H, int W, void* dA, void* dB, bool addB, cudaStream_t st);
+void assemble(const float* rad, const float* feat, int N, int H, int W, int Hp, int Wp, void* out, cudaStream_t st);
+void output(const void* net, const void* in, int N, int H, int W, int Hp, int Wp, float* rad, cudaStream_t st);
+void lossL1(const void* net, const void* in, const float* target, long long pixels, void* dNet, float* lossSum,
+            cudaStream_t st);
+void adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps, float c1,
+          float c2, cudaStream_t st);
+void weightCopies(const float* w, int Cin, int Cout, void* wk, void* wd, cudaStream_t st);
+// batch of crops from a device-resident set of images (training)
+void gatherBatch(const float* noisy, const float* feat, const float* target, int width, int height, const int* params,
+                 int batch, int crop, float* bRad, float* bFeat, float* bTarget, cudaStream_t st);
+
+}  // namespace dn
+}  // namespace bte

@@ -130,6 +130,10 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
         const float4 hv = P.hit[idx];
         const int tri = __float_as_int(hv.w);
         if (tri < 0) {
+            if (bounce == 0 && P.aovAlbedo) {
+                P.aovAlbedo[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                P.aovNormal[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
             accumulateEnvHit(s, p);
             P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z, L4.w);
             continue;
@@ -148,6 +152,12 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
             h.v = w0 * T.uv0.y + u * T.uv1.y + v * T.uv2.y;
         }
         const Bsdf b = loadBsdf(s, tri, h.u, h.v);
+        if (bounce == 0 && P.aovAlbedo) {   // denoiser features: the material colour and normal seen first
+            const float4 a = b.type == BSDF_Dielectric ? make_float4(1.0f, 1.0f, 1.0f, 0.0f)
+                                                       : make_float4(b.p0.x, b.p0.y, b.p0.z, 0.0f);
+            P.aovAlbedo[idx] = a;
+            P.aovNormal[idx] = make_float4(h.n.x, h.n.y, h.n.z, 0.0f);
+        }
         if (s.emitterFlags[tri] != 0) accumulateEmitterHit(s, p, h);
 
         const Frame fr = makeFrame(h.n);
@@ -289,7 +299,7 @@ __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int 
 // FP32 Welford mean (rt_path_integrator.cuh:72-87) in sample order, an FP64
 // running sum, and the gamma-2.2 RGBA8 pack (:93-105).
 __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float* accum, double* accumD,
-                                                uint32_t* framebuffer, uint32_t* extFramebuffer)
+                                                uint32_t* framebuffer, uint32_t* extFramebuffer, float* aovAccum)
 {
     const int pix = blockIdx.x * blockDim.x + threadIdx.x;
     const int wh = f.width * f.height;
@@ -312,6 +322,18 @@ __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float
     }
     accum[3 * pix] = ax; accum[3 * pix + 1] = ay; accum[3 * pix + 2] = az;
     accumD[3 * pix] = sx; accumD[3 * pix + 1] = sy; accumD[3 * pix + 2] = sz;
+    if (aovAccum && P.aovAlbedo) {   // running means of the first-hit albedo and normal, [W*H][6]
+        float m[6];
+        for (int c = 0; c < 6; ++c) m[c] = aovAccum[6 * static_cast<size_t>(pix) + c];
+        for (int s = 0; s < f.spp; ++s) {
+            const int idx = s * wh + pix;
+            const float4 a = P.aovAlbedo[idx], nn = P.aovNormal[idx];
+            const float x[6] = {a.x, a.y, a.z, nn.x, nn.y, nn.z};
+            const float n = static_cast<float>(frameIndex + static_cast<uint32_t>(s) + 1u);
+            for (int c = 0; c < 6; ++c) m[c] = m[c] + (x[c] - m[c]) / n;
+        }
+        for (int c = 0; c < 6; ++c) aovAccum[6 * static_cast<size_t>(pix) + c] = m[c];
+    }
     const uint32_t px = packGamma(ax, ay, az);
     framebuffer[pix] = px;
     if (extFramebuffer) extFramebuffer[pix] = px;
@@ -453,10 +475,10 @@ void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, i
     else kConnect<2><<<grid, block, 0, st>>>(s, P, bounce);
 }
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
-                   cudaStream_t st)
+                   float* aovAccum, cudaStream_t st)
 {
     const int wh = f.width * f.height;
-    kPresent<<<(wh + 255) / 256, 256, 0, st>>>(P, f, accum, accumD, fb, extFb);
+    kPresent<<<(wh + 255) / 256, 256, 0, st>>>(P, f, accum, accumD, fb, extFb, aovAccum);
 }
 void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
                             cudaStream_t st)

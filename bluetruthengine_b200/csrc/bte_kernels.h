@@ -14,7 +14,7 @@ void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int
                  int minBlocks, cudaStream_t st);
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
-                   cudaStream_t st);
+                   float* aovAccum, cudaStream_t st);
 void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
                             cudaStream_t st);
 void launchTraceOccludedRays(const DevScene& s, const float* rays, const float* tmax, int n, uint8_t* out,

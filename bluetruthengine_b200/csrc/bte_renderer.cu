@@ -109,6 +109,8 @@ struct Renderer {
         shMask, hitLog, errorFlags;
     int pathCap = 0, slotCap = 0, depthCap = 0;
     bool hitLogEnabled = false;
+    bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
+    DeviceBuffer aovAlbedo, aovNormal, aovAccum;
     bool stageTiming = false;
     int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
     BteFrameStats stats{};
@@ -225,6 +227,7 @@ void releaseWavefront()
     for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch, &g.shadowQueue,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
         b->release();
+    g.aovAlbedo.release(); g.aovNormal.release();
     g.pathCap = g.slotCap = g.depthCap = 0;
 }
 
@@ -251,6 +254,22 @@ void ensureWavefront(int paths, int slots, int depth)
     if (g.hitLogEnabled) ensure(g.hitLog, static_cast<size_t>(g.pathCap) * g.depthCap * 4);
 }
 
+void ensureAov(int paths)
+{
+    if (!g.aovEnabled) return;
+    if (g.aovAlbedo.bytes < static_cast<size_t>(paths) * 16) {
+        g.aovAlbedo.release(); g.aovNormal.release();
+        ensure(g.aovAlbedo, static_cast<size_t>(paths) * 16);
+        ensure(g.aovNormal, static_cast<size_t>(paths) * 16);
+    }
+    const size_t n = static_cast<size_t>(g.accumW) * g.accumH * 6 * sizeof(float);
+    if (g.aovAccum.bytes != n) {
+        g.aovAccum.release();
+        ensure(g.aovAccum, n);
+        ck(cudaMemsetAsync(g.aovAccum.p, 0, n, g.stream), "cudaMemsetAsync");
+    }
+}
+
 void ensureAccum(int w, int h)
 {
     const size_t n = static_cast<size_t>(w) * h;
@@ -264,6 +283,10 @@ void ensureAccum(int w, int h)
     ck(cudaMemsetAsync(g.accum.p, 0, n * 12, g.stream), "cudaMemsetAsync");
     ck(cudaMemsetAsync(g.accumD.p, 0, n * 24, g.stream), "cudaMemsetAsync");
     ck(cudaMemsetAsync(g.framebuffer.p, 0, n * 4, g.stream), "cudaMemsetAsync");
+    if (g.aovAccum.p) {
+        if (g.aovAccum.bytes == n * 24) ck(cudaMemsetAsync(g.aovAccum.p, 0, n * 24, g.stream), "cudaMemsetAsync");
+        else g.aovAccum.release();
+    }
     ck(cudaStreamSynchronize(g.stream), "cudaStreamSynchronize");
     g.frameIndex = 0;
 }
@@ -286,6 +309,7 @@ void renderFrame(int w, int h)
     const int slots = slotsFor();
     if (slots > 32) throw CudaError{"bte_render: at most 30 spotlights are supported"};
     ensureWavefront(paths, slots, depth);
+    ensureAov(paths);
     const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
     if (g.gridBlock != block) {
         g.gridExtend = occupancyGrid(g.builtWidth == 8 ? 4 : 0, block);
@@ -307,6 +331,8 @@ void renderFrame(int w, int h)
     P.shContrib = g.shContrib.as<float4>();
     P.shMask = g.shMask.as<uint32_t>();
     P.hitLog = g.hitLogEnabled ? g.hitLog.as<int>() : nullptr;
+    P.aovAlbedo = g.aovEnabled ? g.aovAlbedo.as<float4>() : nullptr;
+    P.aovNormal = g.aovEnabled ? g.aovNormal.as<float4>() : nullptr;
     P.slots = slots;
     P.maxDepth = depth;
     P.count = paths;
@@ -324,6 +350,7 @@ void renderFrame(int w, int h)
     float* accumF = g.accum.as<float>();
     double* accumDv = g.accumD.as<double>();
     uint32_t* fb = g.framebuffer.as<uint32_t>();
+    float* aovAcc = g.aovEnabled ? g.aovAccum.as<float>() : nullptr;
     auto prologue = [&] {
         ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
@@ -339,7 +366,7 @@ void renderFrame(int w, int h)
             launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
             launchConnect(s, P, b, g.gridConnect, block, st);
         }
-        launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, st);
+        launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st);
     };
     float stage[5] = {0, 0, 0, 0, 0};
     if (g.cfg.useGraph && !g.stageTiming) {
@@ -352,7 +379,7 @@ void renderFrame(int w, int h)
         };
         const int ints[8] = {depth, block, g.gridExtend, g.gridShade, g.gridConnect, g.shadeMinBlocks, paths,
                              g.hitLogEnabled ? 1 : 0};
-        const void* ptrs[4] = {accumF, accumDv, fb, g.extFramebuffer};
+        const void* ptrs[5] = {accumF, accumDv, fb, g.extFramebuffer, aovAcc};
         put(&P, sizeof(P)); put(&f, sizeof(f)); put(&s, sizeof(s)); put(ints, sizeof(ints)); put(ptrs, sizeof(ptrs));
         if (!g.graphExec || key != g.graphKey) {
             releaseGraph();
@@ -396,7 +423,7 @@ void renderFrame(int w, int h)
             timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st); });
             timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
         }
-        timed(4, [&] { launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, st); });
+        timed(4, [&] { launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st); });
     }
     ck(cudaGetLastError(), "kernel launch");
     ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
@@ -839,6 +866,25 @@ int bte_get_accel_info(int* width, int* nodeCount, int* depth, float* msBuild)
         if (nodeCount) *nodeCount = g.accelNodes;
         if (depth) *depth = g.accelDepth;
         if (msBuild) *msBuild = g.msBvh;
+        return 0;
+    });
+}
+
+int bte_set_aov(int enabled)
+{
+    return guarded([&] {
+        g.aovEnabled = enabled != 0;
+        if (!g.aovEnabled) { g.aovAlbedo.release(); g.aovNormal.release(); g.aovAccum.release(); }
+        return 0;
+    });
+}
+
+int bte_read_aov(float* hostAlbedoNormal)
+{
+    return guarded([&] {
+        if (!g.aovEnabled || !g.aovAccum.p) throw CudaError{"bte_read_aov: features not enabled (bte_set_aov) or not rendered"};
+        ck(cudaMemcpyAsync(hostAlbedoNormal, g.aovAccum.p, g.aovAccum.bytes, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(g.stream), "sync");
         return 0;
     });
 }

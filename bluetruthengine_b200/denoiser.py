@@ -1,0 +1,103 @@
+"""Python side of the learned denoiser (C-ABI: bte_denoiser_* in include/bte/render_api.h).
+
+The network replaces the reference's vendor denoiser stage (src/host/denoiser.cu:72-109,
+cudaToggleDenoiser in include/render_kernel.h:187).  It is trained only on image pairs this
+renderer produces: low-spp radiance plus first-hit albedo/normal (bte_read_aov) as input, long-run
+FP64-accumulated radiance as target.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _check, load_library
+
+
+def rel_mse(x: np.ndarray, ref: np.ndarray, eps: float = 1e-2) -> float:
+    """Mean over pixels and channels of (x - r)^2 / (r^2 + eps)."""
+    x = np.asarray(x, dtype=np.float64)
+    r = np.asarray(ref, dtype=np.float64)
+    return float(np.mean((x - r) ** 2 / (r * r + eps)))
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Denoiser:
+    def __init__(self):
+        self.lib = load_library()
+
+    def init(self, seed: int = 1):
+        _check(self.lib.bte_denoiser_init(C.c_uint64(seed)))
+
+    def param_count(self) -> int:
+        n = C.c_longlong()
+        _check(self.lib.bte_denoiser_param_count(C.byref(n)))
+        return n.value
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), dtype=np.float32)
+        _check(self.lib.bte_denoiser_get_params(out.ctypes.data_as(C.c_void_p), C.c_longlong(out.size)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = _f32(p)
+        _check(self.lib.bte_denoiser_set_params(p.ctypes.data_as(C.c_void_p), C.c_longlong(p.size)))
+
+    def save(self, path: str):
+        np.save(path, self.params())
+
+    def load(self, path: str):
+        self.set_params(np.load(path))
+
+    def set_dataset(self, noisy: np.ndarray, features: np.ndarray, target: np.ndarray):
+        """noisy [S, H, W, 3], features [S, H, W, 6], target [S, H, W, 3]."""
+        noisy, features, target = _f32(noisy), _f32(features), _f32(target)
+        S, H, W, _ = noisy.shape
+        assert features.shape == (S, H, W, 6) and target.shape == (S, H, W, 3)
+        self._keep = (noisy, features, target)
+        _check(self.lib.bte_denoiser_set_dataset(noisy.ctypes.data_as(C.c_void_p), features.ctypes.data_as(C.c_void_p),
+                                                 target.ctypes.data_as(C.c_void_p), S, W, H))
+
+    def train(self, steps: int, batch: int = 8, crop: int = 128, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        loss = np.empty(steps, dtype=np.float32)
+        _check(self.lib.bte_denoiser_train(int(steps), int(batch), int(crop), C.c_float(lr), C.c_uint64(seed),
+                                           loss.ctypes.data_as(C.c_void_p)))
+        return loss
+
+    def denoise(self, radiance: np.ndarray, features: np.ndarray | None) -> np.ndarray:
+        radiance = _f32(radiance)
+        H, W, _ = radiance.shape
+        out = np.empty((H, W, 3), dtype=np.float32)
+        fp = None
+        if features is not None:
+            features = _f32(features)
+            assert features.shape == (H, W, 6)
+            fp = features.ctypes.data_as(C.c_void_p)
+        _check(self.lib.bte_denoiser_denoise(radiance.ctypes.data_as(C.c_void_p), fp, W, H, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        _check(self.lib.bte_denoiser_last_ms(C.byref(ms)))
+        return ms.value
+
+    def debug_conv(self, op: int, x=None, w=None, bias=None, dy=None, shape=(1, 16, 16, 16, 16), relu=True):
+        """op 0: forward, 1: data gradient, 2: weight gradient (+ bias gradient) of one 3x3 conv layer.
+        shape = (N, H, W, Cin, Cout); x [N,H,W,Cin], w [9][Cout][Cin], dy [N,H,W,Cout]."""
+        n, h, wd, cin, cout = shape
+        ptr = lambda a: None if a is None else _f32(a).ctypes.data_as(C.c_void_p)
+        keep = [None if a is None else _f32(a) for a in (x, w, bias, dy)]
+        if op == 0:
+            out = np.empty((n, h, wd, cout), dtype=np.float32)
+        elif op == 1:
+            out = np.empty((n, h, wd, cin), dtype=np.float32)
+        else:
+            out = np.empty(9 * cout * cin + cout, dtype=np.float32)
+        ptrs = [None if a is None else a.ctypes.data_as(C.c_void_p) for a in keep]
+        _check(self.lib.bte_denoiser_debug_conv(op, ptrs[0], ptrs[1], ptrs[2], ptrs[3], n, h, wd, cin, cout,
+                                                1 if relu else 0, out.ctypes.data_as(C.c_void_p)))
+        del ptr
+        return out

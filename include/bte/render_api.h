@@ -105,6 +105,11 @@ int bte_read_accum_f64(double* hostRGBSum);          /* FP64 running sum of samp
 int bte_read_sample_radiance(float* hostRGB, int count);  /* per-path radiance of the last frame [W*H*spp*3] */
 int bte_read_hit_log(int* hostTri, int count);       /* per-bounce closest-hit triangle of the last frame */
 int bte_set_hit_log(int enabled);                    /* record [path][bounce] hit triangles (debug/parity) */
+/* Denoiser features: per-pixel running means of the first-hit material colour
+ * (BsdfData p0.xyz after textures; 1 for dielectrics; 0 on a miss) and shading
+ * normal, accumulated with the radiance.  Read as [W*H][albedo.xyz, normal.xyz]. */
+int bte_set_aov(int enabled);
+int bte_read_aov(float* hostAlbedoNormal);
 /* Acceleration-structure and kernel tuning (what the autotuner sweeps).
  * Width and leaf size apply at the next bte_init_accel, the rest at once. */
 typedef struct {
@@ -119,6 +124,24 @@ int bte_get_tuning(BteTuning* tuning);
 /* The acceleration structure in use: width (2 or 8), node count, levels of
  * the 8-wide tree (0 for width 2) and device build time. */
 int bte_get_accel_info(int* width, int* nodeCount, int* depth, float* msBuild);
+
+/* ---- learned denoiser (replaces the vendor denoiser stage, render_kernel.h:187 / src/host/denoiser.cu) ----
+ * A 5-level U-Net (3x3 convolutions, 32-128 channels) over log(1 + radiance)
+ * plus first-hit albedo and normal, BF16 tensor-core convolutions with FP32
+ * accumulation, FP32 master weights trained with Adam on L1 in log space.
+ * Images are row-major [H][W][3] radiance and [H][W][6] features (albedo xyz,
+ * normal xyz, as bte_read_aov returns them). */
+int bte_denoiser_init(uint64_t seed);                            /* random (He) initialisation */
+int bte_denoiser_param_count(long long* count);
+int bte_denoiser_get_params(float* hostParams, long long count);
+int bte_denoiser_set_params(const float* hostParams, long long count);
+int bte_denoiser_set_dataset(const float* noisy, const float* features, const float* target, int count, int width,
+                             int height);                        /* training images, copied to the device */
+int bte_denoiser_train(int steps, int batch, int crop, float learningRate, uint64_t seed, float* lossPerStep);
+int bte_denoiser_denoise(const float* radiance, const float* features, int width, int height, float* out);
+int bte_denoiser_last_ms(float* ms);                             /* device time of the last denoise / train call */
+int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float* bias, const float* dy, int n, int h,
+                            int w_, int cin, int cout, int relu, float* out);
 
 /* ---- debug/parity entry points over device-resident state ---- */
 /* closest hit for n rays [origin, dir] (host arrays): triangle index (-1 miss) and t, u, v */

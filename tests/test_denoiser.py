@@ -1,0 +1,111 @@
+"""The denoiser's tensor-core kernels against a plain PyTorch FP32 reference of the same op, and its
+training / inference path end to end.
+
+Inputs are rounded to bf16 before the FP32 reference runs, so the reference sees exactly the operands
+the kernels see; the remaining differences are FP32 summation order and the bf16 rounding of the
+kernels' outputs, bounded below as a fraction of the output's largest magnitude."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(2, 20, 37, 32, 48), (1, 16, 64, 16, 32), (1, 9, 70, 224, 96), (2, 8, 24, 80, 16)]
+
+
+def _bf16(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16).to(torch.float32).numpy()
+
+
+def _torch_conv(x, w, bias=None):
+    """x [N,H,W,Cin], w [9][Cout][Cin] -> y [N,H,W,Cout] in FP32 (cross-correlation, zero padding)."""
+    import torch
+    cout, cin = w.shape[1], w.shape[2]
+    wt = torch.from_numpy(w).reshape(3, 3, cout, cin).permute(2, 3, 0, 1).contiguous()
+    xt = torch.from_numpy(x).permute(0, 3, 1, 2).contiguous().requires_grad_(True)
+    wt.requires_grad_(True)
+    y = torch.nn.functional.conv2d(xt, wt, None if bias is None else torch.from_numpy(bias), padding=1)
+    return xt, wt, y
+
+
+@pytest.fixture(scope="module")
+def dn():
+    from bluetruthengine_b200.denoiser import Denoiser
+    return Denoiser()
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_conv_forward_matches_torch(dn, shape):
+    n, h, w, cin, cout = shape
+    rng = np.random.default_rng(cin * 7 + cout)
+    x = _bf16(rng.normal(size=(n, h, w, cin)))
+    wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
+    b = rng.normal(size=cout).astype(np.float32)
+    got = dn.debug_conv(0, x=x, w=wt, bias=b, shape=shape, relu=True)
+    _, _, y = _torch_conv(x, wt, b)
+    ref = np.maximum(y.detach().permute(0, 2, 3, 1).numpy(), 0.0)
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    print("forward", shape, "max error / max |y|", err)
+    assert err < 1e-2
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_conv_data_gradient_matches_torch(dn, shape):
+    n, h, w, cin, cout = shape
+    rng = np.random.default_rng(cin * 5 + cout)
+    x = _bf16(rng.normal(size=(n, h, w, cin)))
+    wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
+    dy = _bf16(rng.normal(size=(n, h, w, cout)))
+    got = dn.debug_conv(1, w=wt, dy=dy, shape=shape)
+    import torch
+    xt, wt_t, y = _torch_conv(x, wt)
+    y.backward(torch.from_numpy(dy).permute(0, 3, 1, 2))
+    ref = xt.grad.permute(0, 2, 3, 1).numpy()
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    print("data gradient", shape, err)
+    assert err < 1e-2
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_conv_weight_gradient_matches_torch(dn, shape):
+    n, h, w, cin, cout = shape
+    rng = np.random.default_rng(cin * 3 + cout)
+    x = _bf16(rng.normal(size=(n, h, w, cin)))
+    wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
+    dy = _bf16(rng.normal(size=(n, h, w, cout)))
+    got = dn.debug_conv(2, x=x, dy=dy, shape=shape)
+    import torch
+    xt, wt_t, y = _torch_conv(x, wt, np.zeros(cout, np.float32))
+    y.backward(torch.from_numpy(dy).permute(0, 3, 1, 2))
+    ref_w = wt_t.grad.permute(2, 3, 0, 1).reshape(9, cout, cin).numpy()
+    ref_b = dy.reshape(-1, cout).sum(0)
+    gw = got[:9 * cout * cin].reshape(9, cout, cin)
+    gb = got[9 * cout * cin:]
+    ew = np.abs(gw - ref_w).max() / np.abs(ref_w).max()
+    eb = np.abs(gb - ref_b).max() / max(np.abs(ref_b).max(), 1e-6)
+    print("weight gradient", shape, ew, eb)
+    assert ew < 1e-3 and eb < 1e-3
+
+
+def test_training_reduces_loss_and_denoise_runs(dn):
+    """A short training run on synthetic pairs (smooth targets, noisy inputs) lowers the L1 loss; the
+    trained network then denoises an image of a size that is not a multiple of 16."""
+    rng = np.random.default_rng(3)
+    S, H, W = 6, 64, 64
+    yy, xx = np.mgrid[0:H, 0:W] / 64.0
+    target = np.stack([np.stack([0.5 + 0.4 * np.sin(6 * xx + k), 0.3 + 0.2 * yy, 0.2 + 0.1 * np.cos(4 * yy + k)], -1)
+                       for k in range(S)]).astype(np.float32)
+    noisy = (target * rng.exponential(1.0, size=target.shape)).astype(np.float32)
+    feat = np.concatenate([target / target.max(), np.broadcast_to([0, 1, 0], target.shape)], -1).astype(np.float32)
+    dn.init(7)
+    dn.set_dataset(noisy, feat, target)
+    loss = dn.train(steps=60, batch=4, crop=48, lr=2e-3, seed=1)
+    print("loss first/last", loss[:5].mean(), loss[-5:].mean())
+    assert np.isfinite(loss).all() and loss[-5:].mean() < 0.7 * loss[:5].mean()
+    out = dn.denoise(noisy[0, :50, :61], feat[0, :50, :61])
+    assert out.shape == (50, 61, 3) and np.isfinite(out).all() and (out >= 0).all()
+    from bluetruthengine_b200.denoiser import rel_mse
+    assert rel_mse(out, target[0, :50, :61]) < rel_mse(noisy[0, :50, :61], target[0, :50, :61])
+    p = dn.params()
+    dn.set_params(p)
+    assert np.array_equal(dn.params(), p)

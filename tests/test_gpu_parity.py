@@ -344,3 +344,35 @@ def test_graph_frames_match_stream_frames(renderer, random_scene):
         assert np.array_equal(bits(a[1]), bits(b[1]))
         assert a[2:] == b[2:]
     renderer.set_config(samples_per_frame=1, max_depth=8, rr_start=3, env_sampling=0, use_graph=0)
+
+
+def test_aov_features(renderer, random_scene):
+    """First-hit albedo/normal features: with one sample per pixel the albedo equals the hit triangle's
+    BSDF colour (1 for dielectrics, 0 for misses), the normal is unit length, and enabling the features
+    leaves the radiance bit-identical."""
+    sc = random_scene
+    W, H = sc.width, sc.height
+    _upload(renderer, sc, env_mode=1, spp=1, depth=6)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    plain = renderer.read_sample_radiance(W * H).copy()
+    _upload(renderer, sc, env_mode=1, spp=1, depth=6)
+    renderer.set_aov(True)
+    renderer.set_hit_log(True)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    rad = renderer.read_sample_radiance(W * H)
+    hits = renderer.read_hit_log(W * H * 6).reshape(W * H, 6)[:, 0]
+    alb, nrm = renderer.read_aov(W, H)
+    renderer.set_hit_log(False)
+    renderer.set_aov(False)
+    assert np.array_equal(bits(plain), bits(rad))
+    alb = alb.reshape(-1, 3)
+    nrm = nrm.reshape(-1, 3)
+    b = sc.bsdfs[sc.triangle_bsdf_ids[np.maximum(hits, 0)]]
+    expect = np.where((b["type"] == 2)[:, None], 1.0, b["p0"][:, :3]).astype(np.float32)   # 2 = dielectric
+    expect[hits < 0] = 0.0
+    assert np.array_equal(alb, expect)
+    ln = np.linalg.norm(nrm, axis=1)
+    assert np.all(np.abs(ln[hits >= 0] - 1.0) < 1e-5) and np.all(ln[hits < 0] == 0.0)
+    assert (hits >= 0).mean() > 0.3
