@@ -290,9 +290,6 @@ class Renderer:
     def get_render_mode(self) -> int:
         return int(self.lib.bte_get_render_mode())
 
-    def toggle_denoiser(self) -> bool:
-        return bool(_check(self.lib.bte_toggle_denoiser()))
-
     def cleanup(self):
         _check(self.lib.bte_cleanup())
 
@@ -303,6 +300,15 @@ class Renderer:
 
     def set_stage_timing(self, on: bool):
         _check(self.lib.bte_set_stage_timing(1 if on else 0))
+
+    def toggle_denoiser(self) -> bool:
+        """cudaToggleDenoiser: returns the new state; needs denoiser weights loaded."""
+        return bool(_check(self.lib.bte_toggle_denoiser()))
+
+    def read_denoised(self, width: int, height: int) -> np.ndarray:
+        out = np.empty((height, width, 3), dtype=np.float32)
+        _check(self.lib.bte_read_denoised(out.ctypes.data_as(C.c_void_p)))
+        return out
 
     def set_aov(self, enabled: bool):
         """Accumulate first-hit albedo and shading normal per pixel (denoiser features)."""

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <mutex>
 #include <random>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -187,7 +188,9 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
     net.aN = N; net.aHp = Hp; net.aWp = Wp; net.aGrad = withGrad;
 }
 
-void forward(int N, int Hp, int Wp)
+// Training keeps the concatenated decoder inputs (the weight gradients read
+// them); inference lets the decoder convolutions read upsample + skip in place.
+void forward(int N, int Hp, int Wp, bool training)
 {
     cudaStream_t st = net.stream;
     for (int k = 0; k < kStepCount; ++k) {
@@ -196,11 +199,20 @@ void forward(int N, int Hp, int Wp)
         const int H = Hp >> ts.level, W = Wp >> ts.level;
         if (s.op == kConvOp) {
             const Conv& c = kConvs[s.conv];
-            conv3x3(net.act[s.src].p, N, H, W, c.cin, net.wk.as<unsigned short>() + net.bfOff[s.conv],
-                    net.w.as<float>() + net.bOff[s.conv], c.cout, c.relu, net.act[s.dst].p, st);
+            const Step* prev = k > 0 ? &kSteps[k - 1] : nullptr;
+            if (!training && prev && prev->op == kUpCatOp && prev->dst == s.src) {
+                const TensorSpec& low = kTensors[prev->src];
+                const TensorSpec& skip = kTensors[prev->src2];
+                conv3x3Cat(net.act[prev->src].p, low.c, true, net.act[prev->src2].p, skip.c, N, H, W,
+                           net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
+                           c.relu, net.act[s.dst].p, st);
+            } else {
+                conv3x3(net.act[s.src].p, N, H, W, c.cin, net.wk.as<unsigned short>() + net.bfOff[s.conv],
+                        net.w.as<float>() + net.bOff[s.conv], c.cout, c.relu, net.act[s.dst].p, st);
+            }
         } else if (s.op == kPoolOp) {
             pool2(net.act[s.src].p, N, H, W, ts.c, net.act[s.dst].p, st);
-        } else {
+        } else if (training) {
             const TensorSpec& skip = kTensors[s.src2];
             upCat(net.act[s.src].p, ts.c, net.act[s.src2].p, skip.c, N, Hp >> skip.level, Wp >> skip.level,
                   net.act[s.dst].p, st);
@@ -271,7 +283,7 @@ void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, f
     }
     ck(cudaEventRecord(net.ev0, st), "cudaEventRecord");
     assemble(dRad, dFeat, N, H, W, Hp, Wp, net.act[0].p, st);
-    forward(N, Hp, Wp);
+    forward(N, Hp, Wp, false);
     output(net.act[27].p, net.act[0].p, N, H, W, Hp, Wp, dOut, st);
     ck(cudaGetLastError(), "denoiser launch");
     ck(cudaEventRecord(net.ev1, st), "cudaEventRecord");
@@ -279,7 +291,22 @@ void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, f
     ck(cudaEventElapsedTime(&net.lastMs, net.ev0, net.ev1), "cudaEventElapsedTime");
 }
 
-bool denoiserReady() { return net.ready; }
+bool denoiserReady()
+{
+    std::lock_guard<std::mutex> lk(netMutex);
+    return net.ready;
+}
+
+void denoiseForRenderer(const float* dRad, const float* dFeat, int N, int H, int W, float* dOut, cudaStream_t waitOn)
+{
+    std::lock_guard<std::mutex> lk(netMutex);
+    try {
+        ensureNet();
+        denoiseDevice(dRad, dFeat, N, H, W, dOut, waitOn);
+    } catch (const CudaErr& e) {
+        throw std::runtime_error(e.msg);
+    }
+}
 
 }  // namespace dn
 }  // namespace bte
@@ -386,7 +413,7 @@ int bte_denoiser_train(int steps, int batch, int crop, float learningRate, uint6
                         net.params.as<int>() + static_cast<size_t>(4) * batch * s, batch, crop, net.rad.as<float>(),
                         net.feat.as<float>(), net.target.as<float>(), st);
             assemble(net.rad.as<float>(), net.feat.as<float>(), batch, crop, crop, crop, crop, net.act[0].p, st);
-            forward(batch, crop, crop);
+            forward(batch, crop, crop, true);
             lossL1(net.act[27].p, net.act[0].p, net.target.as<float>(), static_cast<long long>(px), net.gact[27].p,
                    net.lossSum.as<float>() + s, st);
             backward(batch, crop, crop);

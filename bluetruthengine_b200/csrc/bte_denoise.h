@@ -10,6 +10,10 @@ namespace dn {
 // Y = act(conv3x3(X, Wk) + bias); Wk[9][Cout][Cin] bf16, zero padding at the borders.
 void conv3x3(const void* X, int N, int H, int W, int Cin, const void* Wk, const float* bias, int Cout, bool relu, void* Y,
              cudaStream_t st);
+// Same with the input concat(up ? nearest-upsample-2x(X1) : X1, X2) read in
+// place (X1 has C1 channels, X2 has C2, Wk's Cin = C1 + C2).
+void conv3x3Cat(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+                const float* bias, int Cout, bool relu, void* Y, cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);
@@ -28,6 +32,12 @@ void weightCopies(const float* w, int Cin, int Cout, void* wk, void* wd, cudaStr
 // batch of crops from a device-resident set of images (training)
 void gatherBatch(const float* noisy, const float* feat, const float* target, int width, int height, const int* params,
                  int batch, int crop, float* bRad, float* bFeat, float* bTarget, cudaStream_t st);
+
+// Denoise the renderer's accumulation: dRad [N][H][W][3] mean radiance,
+// dFeat [N][H][W][6] (or null) -> dOut [N][H][W][3]; waits for `waitOn`
+// first and returns when done.  Throws std::runtime_error.
+void denoiseForRenderer(const float* dRad, const float* dFeat, int N, int H, int W, float* dOut, cudaStream_t waitOn);
+bool denoiserReady();
 
 }  // namespace dn
 }  // namespace bte

@@ -50,60 +50,119 @@ __device__ __forceinline__ uint32_t packBf16(float lo, float hi)
 }
 
 // ------------------------------------------------------------ 3x3 convolution (forward / data gradient)
-// A CTA of 4 warps covers 64 consecutive pixels of one image row and 8*NT
-// output channels (blockIdx.z = image * colBlocks + column block); a warp
-// owns 16 pixels.  A fragments are gathered straight from global memory
-// (the 3x3 neighbourhood re-reads hit L1), B fragments from the weights.
-template <int NT, bool Relu>
-__global__ void __launch_bounds__(128) kConv3x3(const bf16* __restrict__ X, int H, int W, int Cin,
-                                                const bf16* __restrict__ Wk, const float* __restrict__ bias, int Cout,
-                                                int colBlocks, bf16* __restrict__ Y)
+// The input is concat(Up ? nearest-upsample-2x(X1) : X1, X2): C1 channels
+// from X1 ([N, H/2, W/2, C1] when Up, else [N, H, W, C1]) followed by C2
+// channels of X2 ([N, H, W, C2]; C2 may be 0), so the decoder's
+// upsample-and-concatenate is read in place.  A CTA computes 16 consecutive
+// pixels of one row x 8*NT output channels; its four warps split the nine
+// taps (w, w+4, w+8) and their partial sums meet in shared memory, so that
+// the small low-resolution layers still put enough warps on the machine.
+// Per 16-channel step a warp issues one m16n8k16 BF16 MMA per 8 output
+// channels; A fragments are gathered from global memory (the neighbourhood
+// re-reads hit L1), B fragments from the weights, one step ahead.
+template <int NT>
+struct ConvFrag {
+    uint32_t a[4];
+    uint32_t b[NT][2];
+};
+
+template <int NT, bool Up>
+__device__ __forceinline__ void convLoad(ConvFrag<NT>& f, const bf16* __restrict__ X1, int C1, const bf16* __restrict__ X2,
+                                         int C2, int n, int H, int W, int y, int xa, int xb, int tap, int c0,
+                                         const bf16* __restrict__ Wk, int Cout, int co0, int g, int t)
 {
+    const int Cin = C1 + C2;
+    const int yy = y + tap / 3 - 1;
+    const int dx = tap % 3 - 1;
+    const int xxa = xa + dx, xxb = xb + dx;
+    const bool rowOk = yy >= 0 && yy < H;
+    const bool okA = rowOk && xxa >= 0 && xxa < W;
+    const bool okB = rowOk && xxb >= 0 && xxb < W;
+    const bf16 *pa, *pb;
+    if (c0 < C1) {
+        const int Hs = Up ? H / 2 : H, Ws = Up ? W / 2 : W;
+        const int ys = rowOk ? (Up ? yy / 2 : yy) : 0;
+        const size_t rowBase = (static_cast<size_t>(n) * Hs + ys) * Ws;
+        pa = X1 + (rowBase + (okA ? (Up ? xxa / 2 : xxa) : 0)) * C1 + c0 + 2 * t;
+        pb = X1 + (rowBase + (okB ? (Up ? xxb / 2 : xxb) : 0)) * C1 + c0 + 2 * t;
+    } else {
+        const size_t rowBase = (static_cast<size_t>(n) * H + (rowOk ? yy : 0)) * W;
+        pa = X2 + (rowBase + (okA ? xxa : 0)) * C2 + (c0 - C1) + 2 * t;
+        pb = X2 + (rowBase + (okB ? xxb : 0)) * C2 + (c0 - C1) + 2 * t;
+    }
+    f.a[0] = okA ? ld32(pa) : 0u;
+    f.a[1] = okB ? ld32(pb) : 0u;
+    f.a[2] = okA ? ld32(pa + 8) : 0u;
+    f.a[3] = okB ? ld32(pb + 8) : 0u;
+    const bf16* wt = Wk + (static_cast<size_t>(tap) * Cout + co0 + g) * Cin + c0 + 2 * t;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+        f.b[j][0] = ld32(wt + static_cast<size_t>(j * 8) * Cin);
+        f.b[j][1] = ld32(wt + static_cast<size_t>(j * 8) * Cin + 8);
+    }
+}
+
+template <int NT>
+__device__ __forceinline__ void convMma(float (&acc)[NT][4], const ConvFrag<NT>& f)
+{
+#pragma unroll
+    for (int j = 0; j < NT; ++j) mma16816(acc[j], f.a[0], f.a[1], f.a[2], f.a[3], f.b[j][0], f.b[j][1]);
+}
+
+template <int NT, bool Relu, bool Up>
+__global__ void __launch_bounds__(128) kConv3x3(const bf16* __restrict__ X1, int C1, const bf16* __restrict__ X2, int C2,
+                                                int H, int W, const bf16* __restrict__ Wk, const float* __restrict__ bias,
+                                                int Cout, int colBlocks, bf16* __restrict__ Y)
+{
+    __shared__ float part[4][16][8 * NT + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     const int n = blockIdx.z / colBlocks;
     const int co0 = (blockIdx.z - n * colBlocks) * (8 * NT);
     const int y = blockIdx.y;
-    const int x0 = blockIdx.x * 64 + warp * 16;
-    if (x0 >= W) return;
+    const int x0 = blockIdx.x * 16;
+    const int xa = x0 + g, xb = x0 + g + 8;
+    const int Cin = C1 + C2;
+    const int chunks = Cin / 16;
+    const int myTaps = warp == 0 ? 3 : 2;   // taps warp, warp + 4, warp + 8
+    const int steps = myTaps * chunks;
     float acc[NT][4];
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-    const int xa = x0 + g, xb = x0 + g + 8;
-    for (int tap = 0; tap < 9; ++tap) {
-        const int yy = y + tap / 3 - 1;
-        const int dx = tap % 3 - 1;
-        const int xxa = xa + dx, xxb = xb + dx;
-        const bool rowOk = yy >= 0 && yy < H;
-        const bool okA = rowOk && xxa >= 0 && xxa < W;
-        const bool okB = rowOk && xxb >= 0 && xxb < W;
-        const size_t rowBase = (static_cast<size_t>(n) * H + (rowOk ? yy : 0)) * W;
-        const bf16* pa = X + (rowBase + (okA ? xxa : 0)) * Cin + 2 * t;
-        const bf16* pb = X + (rowBase + (okB ? xxb : 0)) * Cin + 2 * t;
-        const bf16* wt = Wk + (static_cast<size_t>(tap) * Cout + co0 + g) * Cin + 2 * t;
-        for (int c0 = 0; c0 < Cin; c0 += 16) {
-            const uint32_t a0 = okA ? ld32(pa + c0) : 0u;
-            const uint32_t a1 = okB ? ld32(pb + c0) : 0u;
-            const uint32_t a2 = okA ? ld32(pa + c0 + 8) : 0u;
-            const uint32_t a3 = okB ? ld32(pb + c0 + 8) : 0u;
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-                const bf16* wp = wt + static_cast<size_t>(j * 8) * Cin + c0;
-                mma16816(acc[j], a0, a1, a2, a3, ld32(wp), ld32(wp + 8));
-            }
+    ConvFrag<NT> fa, fb;
+    convLoad<NT, Up>(fa, X1, C1, X2, C2, n, H, W, y, xa, xb, warp, 0, Wk, Cout, co0, g, t);
+    for (int s = 0; s < steps; s += 2) {
+        if (s + 1 < steps) {
+            const int tp = warp + 4 * ((s + 1) / chunks), c0 = 16 * ((s + 1) % chunks);
+            convLoad<NT, Up>(fb, X1, C1, X2, C2, n, H, W, y, xa, xb, tp, c0, Wk, Cout, co0, g, t);
         }
+        convMma<NT>(acc, fa);
+        if (s + 1 >= steps) break;
+        if (s + 2 < steps) {
+            const int tp = warp + 4 * ((s + 2) / chunks), c0 = 16 * ((s + 2) % chunks);
+            convLoad<NT, Up>(fa, X1, C1, X2, C2, n, H, W, y, xa, xb, tp, c0, Wk, Cout, co0, g, t);
+        }
+        convMma<NT>(acc, fb);
     }
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
-        const int co = co0 + j * 8 + 2 * t;
-        const float b0 = bias ? bias[co] : 0.0f, b1 = bias ? bias[co + 1] : 0.0f;
-        float v00 = acc[j][0] + b0, v01 = acc[j][1] + b1, v10 = acc[j][2] + b0, v11 = acc[j][3] + b1;
-        if (Relu) {
-            v00 = fmaxf(v00, 0.0f); v01 = fmaxf(v01, 0.0f); v10 = fmaxf(v10, 0.0f); v11 = fmaxf(v11, 0.0f);
-        }
-        const size_t rowOut = (static_cast<size_t>(n) * H + y) * W;
-        if (xa < W) *reinterpret_cast<uint32_t*>(Y + (rowOut + xa) * Cout + co) = packBf16(v00, v01);
-        if (xb < W) *reinterpret_cast<uint32_t*>(Y + (rowOut + xb) * Cout + co) = packBf16(v10, v11);
+        part[warp][g][j * 8 + 2 * t] = acc[j][0];
+        part[warp][g][j * 8 + 2 * t + 1] = acc[j][1];
+        part[warp][g + 8][j * 8 + 2 * t] = acc[j][2];
+        part[warp][g + 8][j * 8 + 2 * t + 1] = acc[j][3];
+    }
+    __syncthreads();
+    // 16 pixels x 4*NT channel pairs, summed over the four warps
+    for (int e = threadIdx.x; e < 16 * 4 * NT; e += 128) {
+        const int px = e / (4 * NT), cp = 2 * (e % (4 * NT));
+        const int x = x0 + px;
+        if (x >= W) continue;
+        float v0 = part[0][px][cp] + part[1][px][cp] + part[2][px][cp] + part[3][px][cp];
+        float v1 = part[0][px][cp + 1] + part[1][px][cp + 1] + part[2][px][cp + 1] + part[3][px][cp + 1];
+        const int co = co0 + cp;
+        if (bias) { v0 += bias[co]; v1 += bias[co + 1]; }
+        if (Relu) { v0 = fmaxf(v0, 0.0f); v1 = fmaxf(v1, 0.0f); }
+        *reinterpret_cast<uint32_t*>(Y + ((static_cast<size_t>(n) * H + y) * W + x) * Cout + co) = packBf16(v0, v1);
     }
 }
 
@@ -443,19 +502,19 @@ int gridFor(long long n, int block = 256)
     return static_cast<int>(g < 1 ? 1 : g);
 }
 
-template <bool Relu>
-void launchConvNT(int nt, dim3 grid, const bf16* X, int H, int W, int Cin, const bf16* Wk, const float* bias, int Cout,
-                  int colBlocks, bf16* Y, cudaStream_t st)
+template <bool Relu, bool Up>
+void launchConvNT(int nt, dim3 grid, const bf16* X1, int C1, const bf16* X2, int C2, int H, int W, const bf16* Wk,
+                  const float* bias, int Cout, int colBlocks, bf16* Y, cudaStream_t st)
 {
     switch (nt) {
-    case 1: kConv3x3<1, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    case 2: kConv3x3<2, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    case 3: kConv3x3<3, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    case 4: kConv3x3<4, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    case 5: kConv3x3<5, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    case 6: kConv3x3<6, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    case 7: kConv3x3<7, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
-    default: kConv3x3<8, Relu><<<grid, 128, 0, st>>>(X, H, W, Cin, Wk, bias, Cout, colBlocks, Y); break;
+    case 1: kConv3x3<1, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    case 2: kConv3x3<2, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    case 3: kConv3x3<3, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    case 4: kConv3x3<4, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    case 5: kConv3x3<5, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    case 6: kConv3x3<6, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    case 7: kConv3x3<7, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    default: kConv3x3<8, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
     }
 }
 
@@ -472,15 +531,26 @@ static int pickNT(int cout)
 void conv3x3(const void* X, int N, int H, int W, int Cin, const void* Wk, const float* bias, int Cout, bool relu, void* Y,
              cudaStream_t st)
 {
+    conv3x3Cat(X, Cin, false, nullptr, 0, N, H, W, Wk, bias, Cout, relu, Y, st);
+}
+
+void conv3x3Cat(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+                const float* bias, int Cout, bool relu, void* Y, cudaStream_t st)
+{
     const int nt = pickNT(Cout);
     const int colBlocks = Cout / (8 * nt);
-    const dim3 grid((W + 63) / 64, H, N * colBlocks);
-    if (relu)
-        launchConvNT<true>(nt, grid, static_cast<const bf16*>(X), H, W, Cin, static_cast<const bf16*>(Wk), bias, Cout,
-                           colBlocks, static_cast<bf16*>(Y), st);
-    else
-        launchConvNT<false>(nt, grid, static_cast<const bf16*>(X), H, W, Cin, static_cast<const bf16*>(Wk), bias, Cout,
-                            colBlocks, static_cast<bf16*>(Y), st);
+    const dim3 grid((W + 15) / 16, H, N * colBlocks);
+    const bf16* a = static_cast<const bf16*>(X1);
+    const bf16* b = static_cast<const bf16*>(X2);
+    const bf16* w = static_cast<const bf16*>(Wk);
+    bf16* y = static_cast<bf16*>(Y);
+    if (relu) {
+        if (up) launchConvNT<true, true>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
+        else launchConvNT<true, false>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
+    } else {
+        if (up) launchConvNT<false, true>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
+        else launchConvNT<false, false>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
+    }
 }
 
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st)

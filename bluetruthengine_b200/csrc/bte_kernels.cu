@@ -480,6 +480,19 @@ void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double
     const int wh = f.width * f.height;
     kPresent<<<(wh + 255) / 256, 256, 0, st>>>(P, f, accum, accumD, fb, extFb, aovAccum);
 }
+// gamma-packed RGBA8 of an RGB float image (the denoised frame)
+__global__ void kPackImage(const float* __restrict__ rgb, int n, uint32_t* fb, uint32_t* extFb)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t px = packGamma(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]);
+    fb[i] = px;
+    if (extFb) extFb[i] = px;
+}
+void launchPackImage(const float* rgb, int n, uint32_t* fb, uint32_t* extFb, cudaStream_t st)
+{
+    kPackImage<<<(n + 255) / 256, 256, 0, st>>>(rgb, n, fb, extFb);
+}
 void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
                             cudaStream_t st)
 {

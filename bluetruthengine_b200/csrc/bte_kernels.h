@@ -25,6 +25,7 @@ void launchBsdfQuery(const BsdfData& g, int op, const float* wi, const float* x,
 void launchTexCompare(cudaTextureObject_t tex, const float4* texels, int w, int h, int wrapV, const float* uv, int n,
                       float* outHw, float* outSw, cudaStream_t st);
 int occupancyGrid(int which, int block);
+void launchPackImage(const float* rgb, int n, uint32_t* fb, uint32_t* extFb, cudaStream_t st);
 
 // LBVH build over device triangles (bte_bvh.cu).  Allocates `nodes` and
 // `leafTris`; the caller frees them.  Returns 0 or a CUDA error code.

@@ -7,6 +7,7 @@
 // an LBVH instead of the OptiX GAS, and a frame that is a fixed,
 // host-synchronisation-free launch sequence.  Every entry point returns a
 // status and records a message for bte_last_error() instead of exiting.
+#include "bte_denoise.h"
 #include "bte_internal.h"
 #include "bte_kernels.h"
 #include "bte_math.cuh"
@@ -111,6 +112,7 @@ struct Renderer {
     bool hitLogEnabled = false;
     bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
     DeviceBuffer aovAlbedo, aovNormal, aovAccum;
+    DeviceBuffer denoised;            // [W*H*3] denoised mean radiance of the last frame (denoiser on)
     bool stageTiming = false;
     int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
     BteFrameStats stats{};
@@ -443,6 +445,14 @@ void renderFrame(int w, int h)
     }
     ck(cudaEventElapsedTime(&S.msTotal, g.ev0, g.ev1), "cudaEventElapsedTime");
     S.msGenerate = stage[0]; S.msExtend = stage[1]; S.msShade = stage[2]; S.msConnect = stage[3]; S.msPresent = stage[4];
+    if (g.denoiser && !(errFlags & 3u)) {
+        const size_t bytes = static_cast<size_t>(w) * h * 12;
+        if (g.denoised.bytes != bytes) { g.denoised.release(); ensure(g.denoised, bytes); }
+        dn::denoiseForRenderer(accumF, aovAcc, 1, h, w, g.denoised.as<float>(), st);
+        launchPackImage(g.denoised.as<float>(), w * h, fb, g.extFramebuffer, st);
+        ck(cudaGetLastError(), "pack launch");
+        ck(cudaStreamSynchronize(st), "denoise present");
+    }
     g.frameIndex += static_cast<uint32_t>(spp);
     g.lastPaths = paths; g.lastDepth = depth; g.lastSpp = spp; g.lastW = w; g.lastH = h; g.lastSlots = slots;
     if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
@@ -749,10 +759,31 @@ int bte_render(int imageWidth, int imageHeight)
     });
 }
 
+// render_kernel.h:187 (cudaToggleDenoiser): returns the new state.  Turning
+// it on needs denoiser weights (bte_denoiser_set_params / bte_denoiser_init)
+// and switches the first-hit features on; each frame then presents the
+// denoised accumulation.  Plain accumulation stays the buffer of record.
 int bte_toggle_denoiser(void)
 {
     return guarded([&]() -> int {
-        throw CudaError{"bte_toggle_denoiser: the learned denoiser is not part of this build; plain accumulation only"};
+        if (!g.denoiser && !dn::denoiserReady())
+            throw CudaError{"bte_toggle_denoiser: no denoiser weights (bte_denoiser_set_params or bte_denoiser_init)"};
+        g.denoiser = !g.denoiser;
+        if (g.denoiser && !g.aovEnabled) {
+            g.aovEnabled = true;
+            if (g.accumW > 0) ensureAccum(g.accumW, g.accumH);   // features and radiance restart together
+        }
+        return g.denoiser ? 1 : 0;
+    });
+}
+
+int bte_read_denoised(float* hostRGB)
+{
+    return guarded([&] {
+        if (!g.denoised.p) throw CudaError{"bte_read_denoised: no denoised frame (bte_toggle_denoiser, then bte_render)"};
+        ck(cudaMemcpyAsync(hostRGB, g.denoised.p, g.denoised.bytes, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(g.stream), "sync");
+        return 0;
     });
 }
 
@@ -778,7 +809,8 @@ int bte_cleanup(void)
                                 &g.emitters, &g.emitterTriIndices, &g.emitterTriCdf, &g.sceneEmitterCdf, &g.bsdfs,
                                 &g.triBsdfIds, &g.spots, &g.texTable, &g.texTableMr, &g.envTexels, &g.envMarginal,
                                 &g.envConditional, &g.envRowProb, &g.envRowAlias, &g.envColProb, &g.envColAlias,
-                                &g.envPixelPdf, &g.bvhNodes, &g.wideNodes, &g.leafTris, &g.accum, &g.accumD, &g.framebuffer})
+                                &g.envPixelPdf, &g.bvhNodes, &g.wideNodes, &g.leafTris, &g.accum, &g.accumD, &g.framebuffer,
+                                &g.aovAccum, &g.denoised})
             b->release();
         for (auto& b : g.tex) b.release();
         for (auto& b : g.texMr) b.release();
@@ -873,7 +905,7 @@ int bte_get_accel_info(int* width, int* nodeCount, int* depth, float* msBuild)
 int bte_set_aov(int enabled)
 {
     return guarded([&] {
-        g.aovEnabled = enabled != 0;
+        g.aovEnabled = enabled != 0 || g.denoiser;   // the denoiser keeps its features
         if (!g.aovEnabled) { g.aovAlbedo.release(); g.aovNormal.release(); g.aovAccum.release(); }
         return 0;
     });

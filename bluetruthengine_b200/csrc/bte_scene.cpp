@@ -28,6 +28,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace bte {
@@ -403,10 +404,16 @@ ObjData readObj(const std::string& path)
     return o;
 }
 
+// Parsed OBJ files of the scene being loaded: a file referenced by several
+// <mesh> elements (instances with different transforms) is parsed once.
+thread_local std::unordered_map<std::string, ObjData> t_objCache;
+
 // src/main.cpp:267-401
 std::vector<TriangleData> loadTriangles(const std::string& path, const TransformDesc& xf)
 {
-    const ObjData o = readObj(path);
+    auto it = t_objCache.find(path);
+    if (it == t_objCache.end()) it = t_objCache.emplace(path, readObj(path)).first;
+    const ObjData& o = it->second;
     std::vector<TriangleData> tris;
     auto V = [&](int i) -> Float3 {
         if (i < 0 || static_cast<size_t>(3 * i + 2) >= o.v.size()) fail("invalid vertex index in \"" + path + "\"");
@@ -576,6 +583,8 @@ std::string resolve(const std::string& scenePath, const std::string& p)
 // src/main.cpp:523-930, minus the window/GL parts.
 int sceneLoad(const char* path, SceneData& S, std::string& err)
 {
+    struct CacheReset { ~CacheReset() { t_objCache.clear(); } } cacheReset;
+    t_objCache.clear();
     try {
         const std::string sp(path ? path : "");
         SceneDesc d = parseScene(sp);

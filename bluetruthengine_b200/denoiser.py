@@ -47,10 +47,12 @@ class Denoiser:
         _check(self.lib.bte_denoiser_set_params(p.ctypes.data_as(C.c_void_p), C.c_longlong(p.size)))
 
     def save(self, path: str):
-        np.save(path, self.params())
+        np.savez_compressed(path, params=self.params().astype(np.float16))
 
     def load(self, path: str):
-        self.set_params(np.load(path))
+        """Weights saved by `save` or by train_denoiser (float16 on disk, float32 masters on the device)."""
+        with np.load(path) as z:
+            self.set_params(z["params"].astype(np.float32))
 
     def set_dataset(self, noisy: np.ndarray, features: np.ndarray, target: np.ndarray):
         """noisy [S, H, W, 3], features [S, H, W, 6], target [S, H, W, 3]."""
@@ -88,7 +90,6 @@ class Denoiser:
         """op 0: forward, 1: data gradient, 2: weight gradient (+ bias gradient) of one 3x3 conv layer.
         shape = (N, H, W, Cin, Cout); x [N,H,W,Cin], w [9][Cout][Cin], dy [N,H,W,Cout]."""
         n, h, wd, cin, cout = shape
-        ptr = lambda a: None if a is None else _f32(a).ctypes.data_as(C.c_void_p)
         keep = [None if a is None else _f32(a) for a in (x, w, bias, dy)]
         if op == 0:
             out = np.empty((n, h, wd, cout), dtype=np.float32)
@@ -99,5 +100,4 @@ class Denoiser:
         ptrs = [None if a is None else a.ctypes.data_as(C.c_void_p) for a in keep]
         _check(self.lib.bte_denoiser_debug_conv(op, ptrs[0], ptrs[1], ptrs[2], ptrs[3], n, h, wd, cin, cout,
                                                 1 if relu else 0, out.ctypes.data_as(C.c_void_p)))
-        del ptr
         return out

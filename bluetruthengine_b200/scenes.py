@@ -349,3 +349,182 @@ def random_scene(seed: int, n_tris: int = 200, extent: float = 10.0) -> str:
         f.write(xml)
     _mark(d)
     return path
+
+
+def _c4_assets() -> str:
+    """Shared meshes of the denoiser training scenes (one directory, one XML per scene)."""
+    d = os.path.join(CACHE_ROOT, "c4_assets_v%d" % GENERATOR_VERSION)
+    os.makedirs(d, exist_ok=True)
+    if _done(d):
+        return d
+    L = 555.0
+    walls = {
+        "floor": quad((0, 0, 0), (0, 0, L), (L, 0, L), (L, 0, 0)),
+        "ceiling": quad((0, L, 0), (L, L, 0), (L, L, L), (0, L, L)),
+        "back": quad((0, 0, L), (0, L, L), (L, L, L), (L, 0, L)),
+        "left": quad((L, 0, 0), (L, 0, L), (L, L, L), (L, L, 0)),
+        "right": quad((0, 0, 0), (0, L, 0), (0, L, L), (0, 0, L)),
+        # unit light quad in the xz plane facing -y (scaled and placed per scene)
+        "lightq": quad((-0.5, 0, -0.5), (0.5, 0, -0.5), (0.5, 0, 0.5), (-0.5, 0, 0.5)),
+    }
+    for name, (v, f) in walls.items():
+        write_obj(os.path.join(d, name + ".obj"), v, f)
+    cv, cf = unit_cube()
+    write_obj(os.path.join(d, "cube.obj"), cv, cf)
+    sv, sf = icosphere(3)
+    write_obj(os.path.join(d, "sphere.obj"), sv, sf, normals=sv)
+    _mark(d)
+    return d
+
+
+def c4_scene(seed: int, width: int = 256, height: int = 256) -> str:
+    """Denoiser training scene: a Cornell box (the 555-unit box of the plain-method scene) with seeded
+    wall colours, light size/colour, 0-2 diffuse boxes, 1-3 dielectric spheres (IOR U[1.3, 1.8]) and,
+    sometimes, a mirror or rough-conductor-like microfacet object; camera jittered.  Returns the XML path."""
+    d = _c4_assets()
+    path = os.path.join(d, "c4_%d_%dx%d.xml" % (seed, width, height))
+    if os.path.exists(path):
+        return path
+    rng = np.random.default_rng(1_000_003 * seed + 17)
+    L = 555.0
+    col = lambda lo, hi: rng.uniform(lo, hi, 3)
+    white = rng.uniform(0.55, 0.85)
+    left = col(0.03, 0.8)
+    right = col(0.03, 0.8)
+    le = np.array([17.0, 12.0, 4.0]) * rng.uniform(0.5, 2.0) * rng.uniform(0.7, 1.3, 3)
+    lw, ld = 130.0 * rng.uniform(0.6, 1.6), 105.0 * rng.uniform(0.6, 1.6)
+    f3 = lambda v: "R=\"%.5f\" {0}G=\"%.5f\" {0}B=\"%.5f\"" % tuple(v)
+    bs = [f'<bsdf name="white" type="diffuse" albedoR="{white:.5f}" albedoG="{white:.5f}" albedoB="{white:.5f}" />',
+          '<bsdf name="left" type="diffuse" albedo%s />' % (f3(left).format("albedo")),
+          '<bsdf name="right" type="diffuse" albedo%s />' % (f3(right).format("albedo")),
+          '<bsdf name="lightb" type="diffuse" albedoR="0.78" albedoG="0.78" albedoB="0.78" />']
+    meshes = ['<mesh filename="floor.obj" material="mWhite" />', '<mesh filename="ceiling.obj" material="mWhite" />',
+              '<mesh filename="back.obj" material="mWhite" />', '<mesh filename="left.obj" material="mLeft" />',
+              '<mesh filename="right.obj" material="mRight" />',
+              '<mesh filename="lightq.obj" material="mLight" isEmitter="true" radianceR="%.4f" radianceG="%.4f" '
+              'radianceB="%.4f" scaleX="%.3f" scaleY="1" scaleZ="%.3f" posX="277.5" posY="554.5" posZ="277.5" />'
+              % (le[0], le[1], le[2], lw, ld)]
+    mats = ['<material name="mWhite" bsdf="white" />', '<material name="mLeft" bsdf="left" />',
+            '<material name="mRight" bsdf="right" />', '<material name="mLight" bsdf="lightb" />']
+    for k in range(int(rng.integers(0, 3))):
+        sx, sy, sz = rng.uniform(80, 200), rng.uniform(80, 350), rng.uniform(80, 200)
+        c = col(0.2, 0.85)
+        bs.append('<bsdf name="box%d" type="diffuse" albedo%s />' % (k, f3(c).format("albedo")))
+        mats.append('<material name="mBox%d" bsdf="box%d" />' % (k, k))
+        meshes.append('<mesh filename="cube.obj" material="mBox%d" scaleX="%.3f" scaleY="%.3f" scaleZ="%.3f" rotY="%.3f" '
+                      'posX="%.3f" posY="%.3f" posZ="%.3f" />'
+                      % (k, sx, sy, sz, rng.uniform(-45, 45), rng.uniform(110, 445), sy / 2, rng.uniform(110, 445)))
+    for k in range(int(rng.integers(1, 4))):
+        r = rng.uniform(40, 100)
+        ior = rng.uniform(1.3, 1.8)
+        bs.append('<bsdf name="glass%d" type="dielectric" intIOR="%.4f" extIOR="1.0" />' % (k, ior))
+        mats.append('<material name="mGlass%d" bsdf="glass%d" />' % (k, k))
+        y = r if rng.uniform() < 0.7 else rng.uniform(r, L - 150 - r)
+        meshes.append('<mesh filename="sphere.obj" material="mGlass%d" scaleX="%.3f" scaleY="%.3f" scaleZ="%.3f" '
+                      'posX="%.3f" posY="%.3f" posZ="%.3f" />'
+                      % (k, r, r, r, rng.uniform(r, L - r), y, rng.uniform(r, L - r)))
+    if rng.uniform() < 0.35:
+        r = rng.uniform(40, 90)
+        if rng.uniform() < 0.5:
+            bs.append('<bsdf name="extra" type="mirror" albedo%s />' % (f3(col(0.7, 0.95)).format("albedo")))
+        else:
+            bs.append('<bsdf name="extra" type="microfacet" albedo%s alpha="%.3f" intIOR="1.6" extIOR="1.0" />'
+                      % (f3(col(0.1, 0.7)).format("albedo"), rng.uniform(0.05, 0.5)))
+        mats.append('<material name="mExtra" bsdf="extra" />')
+        meshes.append('<mesh filename="sphere.obj" material="mExtra" scaleX="%.3f" scaleY="%.3f" scaleZ="%.3f" '
+                      'posX="%.3f" posY="%.3f" posZ="%.3f" />' % (r, r, r, rng.uniform(r, L - r), r, rng.uniform(r, L - r)))
+    eye = np.array([277.5, 277.5, -790.0]) + rng.uniform(-40, 40, 3)
+    fov = 39.5 + rng.uniform(-5, 5)
+    xml = "<scene>\n    " + "\n    ".join(bs + mats + meshes) + "\n"
+    xml += '    <window width="%d" height="%d" />\n' % (width, height)
+    xml += ('    <camera eyeX="%.3f" eyeY="%.3f" eyeZ="%.3f" lookAtX="277.5" lookAtY="277.5" lookAtZ="277.5" '
+            'upX="0" upY="1" upZ="0" fovY="%.3f" />\n</scene>\n' % (eye[0], eye[1], eye[2], fov))
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        f.write(xml)
+    os.replace(tmp, path)
+    return path
+
+
+def blob_mesh(seed: int, nu: int = 125, nv: int = 100):
+    """Seeded closed mesh of exactly 2*nu*nv triangles: a torus of random proportions whose surface is
+    displaced along its normal by a few random low-frequency harmonics.  Returns (verts, faces, normals)."""
+    rng = np.random.default_rng(seed)
+    R, r = 1.0, rng.uniform(0.25, 0.6)
+    u = np.arange(nu) * (2 * np.pi / nu)
+    v = np.arange(nv) * (2 * np.pi / nv)
+    U, V = np.meshgrid(u, v, indexing="ij")
+    disp = np.zeros_like(U)
+    for _ in range(4):
+        a, b = rng.integers(1, 6), rng.integers(1, 5)
+        disp += rng.uniform(0.03, 0.12) * r * np.sin(a * U + rng.uniform(0, 2 * np.pi)) * np.cos(b * V + rng.uniform(0, 2 * np.pi))
+    rr = r + disp
+    x = (R + rr * np.cos(V)) * np.cos(U)
+    y = rr * np.sin(V) * rng.uniform(0.6, 1.4)
+    z = (R + rr * np.cos(V)) * np.sin(U)
+    verts = np.stack([x, y, z], -1).reshape(-1, 3)
+    i = np.arange(nu)[:, None] * nv + np.arange(nv)[None, :]
+    i1 = ((np.arange(nu)[:, None] + 1) % nu) * nv + np.arange(nv)[None, :]
+    i2 = np.arange(nu)[:, None] * nv + (np.arange(nv)[None, :] + 1) % nv
+    i3 = ((np.arange(nu)[:, None] + 1) % nu) * nv + (np.arange(nv)[None, :] + 1) % nv
+    faces = np.concatenate([np.stack([i.ravel(), i2.ravel(), i3.ravel()], 1), np.stack([i.ravel(), i3.ravel(), i1.ravel()], 1)])
+    # area-weighted vertex normals, oriented outward from the torus core
+    fn = np.cross(verts[faces[:, 1]] - verts[faces[:, 0]], verts[faces[:, 2]] - verts[faces[:, 0]])
+    core = np.stack([R * np.cos(U), np.zeros_like(U), R * np.sin(U)], -1).reshape(-1, 3)
+    if np.sum(fn * (verts[faces[:, 0]] - core[faces[:, 0]])) < 0:
+        faces = faces[:, [0, 2, 1]]
+        fn = -fn
+    n = np.zeros_like(verts)
+    for k in range(3):
+        np.add.at(n, faces[:, k], fn)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-12)
+    return verts, faces, n
+
+
+def large_instanced(seed: int = 5, width: int = 3840, height: int = 2160, n_instances: int = 400, n_meshes: int = 8,
+                    env_w: int = 2048, env_h: int = 1024) -> str:
+    """The large configuration: n_instances placements of n_meshes seed-generated 25,000-triangle meshes
+    (10M triangles flattened), each instance mirror, dielectric or microfacet (alpha U[0.01, 0.5]), on a
+    diffuse ground under the procedural sky; returns the scene.xml path."""
+    d = _scene_dir("large_%dx%d_n%d_m%d" % (width, height, n_instances, n_meshes), seed)
+    path = os.path.join(d, "scene.xml")
+    if _done(d):
+        return path
+    rng = np.random.default_rng(seed)
+    for m in range(n_meshes):
+        v, f, n = blob_mesh(seed * 100 + m)
+        write_obj(os.path.join(d, "blob%d.obj" % m), v, f, normals=n)
+    gv, gf = quad((-200, 0, -200), (-200, 0, 200), (200, 0, 200), (200, 0, -200))
+    write_obj(os.path.join(d, "ground.obj"), gv, gf)
+    write_hdr(os.path.join(d, "sky.hdr"), sky_env(env_w, env_h))
+    bs = ['<bsdf name="ground" type="diffuse" albedoR="0.45" albedoG="0.42" albedoB="0.38" />']
+    mats = ['<material name="mGround" bsdf="ground" />']
+    meshes = ['<mesh filename="ground.obj" material="mGround" />']
+    side = int(np.ceil(np.sqrt(n_instances)))
+    for k in range(n_instances):
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            c = rng.uniform(0.6, 0.95, 3)
+            bs.append('<bsdf name="b%d" type="mirror" albedoR="%.4f" albedoG="%.4f" albedoB="%.4f" />' % (k, *c))
+        elif kind == 1:
+            bs.append('<bsdf name="b%d" type="dielectric" intIOR="%.4f" extIOR="1.0" />' % (k, rng.uniform(1.3, 1.8)))
+        else:
+            c = rng.uniform(0.05, 0.8, 3)
+            bs.append('<bsdf name="b%d" type="microfacet" albedoR="%.4f" albedoG="%.4f" albedoB="%.4f" alpha="%.4f" '
+                      'intIOR="1.5" extIOR="1.0" />' % (k, *c, rng.uniform(0.01, 0.5)))
+        mats.append('<material name="m%d" bsdf="b%d" />' % (k, k))
+        gx, gz = k % side, k // side
+        s = rng.uniform(0.6, 1.4)
+        meshes.append('<mesh filename="blob%d.obj" material="m%d" scaleX="%.3f" scaleY="%.3f" scaleZ="%.3f" rotY="%.2f" '
+                      'rotX="%.2f" posX="%.3f" posY="%.3f" posZ="%.3f" />'
+                      % (int(rng.integers(0, n_meshes)), k, s, s, s, rng.uniform(0, 360), rng.uniform(-30, 30),
+                         (gx - side / 2 + rng.uniform(-0.25, 0.25)) * 3.2, s * 0.9, (gz - side / 2 + rng.uniform(-0.25, 0.25)) * 3.2))
+    xml = "<scene>\n    " + "\n    ".join(bs + mats + meshes) + "\n"
+    xml += '    <environment map="sky.hdr" intensity="1.0" rotation="0.0" />\n'
+    xml += '    <window width="%d" height="%d" />\n' % (width, height)
+    xml += ('    <camera eyeX="0" eyeY="22" eyeZ="-48" lookAtX="0" lookAtY="0" lookAtZ="4" upX="0" upY="1" upZ="0" '
+            'fovY="50" />\n</scene>\n')
+    with open(path, "w") as f:
+        f.write(xml)
+    _mark(d)
+    return path

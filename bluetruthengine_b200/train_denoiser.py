@@ -1,0 +1,72 @@
+"""Train the denoiser on pairs this renderer generates and save its weights.
+
+    python -m bluetruthengine_b200.train_denoiser --scenes 512 --steps 4000 \
+        --out bluetruthengine_b200/weights/denoiser_c4.npz
+
+Training scenes are the seeded Cornell-box variants of `scenes.c4_scene` (wall colours, light, boxes,
+1-3 dielectric spheres with IOR U[1.3, 1.8], an occasional mirror or microfacet sphere) at 256x256;
+inputs mix 2-32 spp so that one network serves several noise levels; targets are independent
+FP64-accumulated long runs.  Weights are stored as float16 (`params`) with the training record.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scenes", type=int, default=512)
+    ap.add_argument("--first-seed", type=int, default=1000)
+    ap.add_argument("--spp-target", type=int, default=2048)
+    ap.add_argument("--depth", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--crop", type=int, default=128)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "denoiser_c4.npz"))
+    args = ap.parse_args(argv)
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bluetruthengine_b200 as bte
+    from bluetruthengine_b200 import scenes
+    from bluetruthengine_b200.denoise_data import make_dataset
+    from bluetruthengine_b200.denoiser import Denoiser
+    log = lambda m: print(m, flush=True)
+    r = bte.Renderer()
+    paths = [scenes.c4_scene(args.first_seed + i) for i in range(args.scenes)]
+    t0 = time.perf_counter()
+    noisy, feat, target = make_dataset(r, paths, spp_target=args.spp_target, depth=args.depth, seed=args.seed, log=log)
+    t_data = time.perf_counter() - t0
+    dn = Denoiser()
+    dn.init(args.seed)
+    dn.set_dataset(noisy, feat, target)
+    losses = []
+    t1 = time.perf_counter()
+    chunk = 250
+    lr = args.lr
+    for s in range(0, args.steps, chunk):
+        k = min(chunk, args.steps - s)
+        lr_s = lr * (0.1 if s >= 0.8 * args.steps else 1.0)   # one step decay for the last fifth
+        l = dn.train(k, batch=args.batch, crop=args.crop, lr=lr_s, seed=args.seed * 7919 + s)
+        losses.extend(l.tolist())
+        log("step %d loss %.5f (%.1f ms / step)" % (s + k, float(np.mean(l[-50:])), dn.last_ms() / k))
+    t_train = time.perf_counter() - t1
+    p = dn.params()
+    rec = {"scenes": args.scenes, "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
+           "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
+           "seconds_data": t_data, "seconds_train": t_train, "loss_first": float(np.mean(losses[:50])),
+           "loss_last": float(np.mean(losses[-50:]))}
+    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    np.savez_compressed(args.out, params=p.astype(np.float16), record=json.dumps(rec))
+    log(json.dumps(rec))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -87,7 +87,8 @@ int bte_init_env_map(const float* rgba, int width, int height, float intensity, 
 int bte_set_output_buffer(uint32_t* deviceRGBA8);   /* replaces cudaRegisterPBO :177 (no GL on the box) */
 int bte_reset_accumulation(int imageWidth, int imageHeight);                    /* :183 */
 int bte_render(int imageWidth, int imageHeight);                                /* :187 */
-int bte_toggle_denoiser(void);                      /* :192; returns new state (0/1) or <0 */
+int bte_toggle_denoiser(void);                      /* :192; returns new state (0/1) or <0; needs denoiser weights */
+int bte_read_denoised(float* hostRGB);               /* W*H*3 denoised mean radiance of the last frame (denoiser on) */
 int bte_set_render_mode(int mode);                                              /* :205 */
 int bte_get_render_mode(void);                                                  /* :208 */
 int bte_cleanup(void);                                                          /* :211 */

@@ -109,3 +109,87 @@ def test_training_reduces_loss_and_denoise_runs(dn):
     p = dn.params()
     dn.set_params(p)
     assert np.array_equal(dn.params(), p)
+
+
+def test_renderer_denoiser_toggle(dn, bte, cornell_scene):
+    """cudaToggleDenoiser path: with weights loaded, each frame presents the denoised accumulation
+    (read back as floats and as the packed framebuffer); plain accumulation is unchanged by it."""
+    from conftest import bits
+    r = bte.Renderer()
+    sc = cornell_scene
+    W, H = sc.width, sc.height
+    r.cleanup()
+    r.upload(sc)
+    r.set_config(samples_per_frame=2, max_depth=6, rr_start=3, env_sampling=0)
+    r.reset_accumulation(W, H)
+    r.render(W, H)
+    plain = r.read_accum(W, H).copy()
+    dn.init(5)
+    assert r.toggle_denoiser() is True
+    r.reset_accumulation(W, H)
+    r.render(W, H)
+    acc = r.read_accum(W, H)
+    den = r.read_denoised(W, H)
+    fb = r.read_framebuffer(W, H)
+    feat = np.concatenate(r.read_aov(W, H), -1)
+    assert r.toggle_denoiser() is False
+    assert np.array_equal(bits(plain), bits(acc))
+    assert den.shape == (H, W, 3) and np.isfinite(den).all()
+    assert np.array_equal(den, dn.denoise(acc.reshape(H, W, 3), feat))
+    assert fb.size == W * H
+
+
+CONVS = [(16, 32), (32, 32), (32, 48), (48, 48), (48, 64), (64, 64), (64, 96), (96, 96), (96, 128), (128, 128),
+         (224, 96), (96, 96), (160, 64), (64, 64), (112, 48), (48, 48), (80, 32), (32, 32), (32, 16)]
+
+
+def _torch_unet(params, rad, feat):
+    """The denoiser's network in PyTorch FP32, rounding activations to bf16 where the kernels store them."""
+    import torch
+    import torch.nn.functional as F
+    bf = lambda t: t.to(torch.bfloat16).to(torch.float32)
+    H, W = rad.shape[:2]
+    Hp, Wp = (H + 15) // 16 * 16, (W + 15) // 16 * 16
+    pad = lambda a: np.pad(a, ((0, Hp - H), (0, Wp - W), (0, 0)), mode="edge")
+    x = np.concatenate([np.log1p(np.maximum(pad(rad), 0)), pad(feat), np.zeros((Hp, Wp, 7), np.float32)], -1)
+    x = bf(torch.from_numpy(x.astype(np.float32)).permute(2, 0, 1)[None])
+    ws, off = [], 0
+    for cin, cout in CONVS:
+        w = torch.from_numpy(params[off:off + 9 * cout * cin].reshape(3, 3, cout, cin)).permute(2, 3, 0, 1)
+        off += 9 * cout * cin
+        b = torch.from_numpy(params[off:off + cout])
+        off += cout
+        ws.append((bf(w), b))
+    conv = lambda t, i, relu=True: bf(F.relu(F.conv2d(t, *ws[i], padding=1)) if relu else F.conv2d(t, *ws[i], padding=1))
+    pool = lambda t: bf(F.avg_pool2d(t, 2))
+    up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")
+    e0 = conv(conv(x, 0), 1)
+    e1 = conv(conv(pool(e0), 2), 3)
+    e2 = conv(conv(pool(e1), 4), 5)
+    e3 = conv(conv(pool(e2), 6), 7)
+    e4 = conv(conv(pool(e3), 8), 9)
+    d3 = conv(conv(torch.cat([up(e4), e3], 1), 10), 11)
+    d2 = conv(conv(torch.cat([up(d3), e2], 1), 12), 13)
+    d1 = conv(conv(torch.cat([up(d2), e1], 1), 14), 15)
+    d0 = conv(conv(torch.cat([up(d1), e0], 1), 16), 17)
+    out = conv(d0, 18, relu=False)
+    pred = out[0, :3] + x[0, :3]
+    return np.maximum(np.expm1(pred.permute(1, 2, 0).numpy()), 0)[:H, :W]
+
+
+def test_network_inference_matches_torch(dn):
+    """The whole inference path (feature assembly, edge padding, encoder, in-place upsample+concat decoder,
+    residual output) against the same network written in PyTorch, on a trained-like random network."""
+    from bluetruthengine_b200.denoiser import Denoiser
+    dn.init(11)
+    p = dn.params()
+    rng = np.random.default_rng(5)
+    H, W = 72, 100
+    rad = rng.exponential(0.4, size=(H, W, 3)).astype(np.float32)
+    feat = np.concatenate([rng.uniform(0, 1, (H, W, 3)), rng.normal(size=(H, W, 3))], -1).astype(np.float32)
+    got = dn.denoise(rad, feat)
+    ref = _torch_unet(p, rad, feat)
+    lg, lr = np.log1p(got), np.log1p(ref)
+    err = np.abs(lg - lr)
+    print("log-space error max", err.max(), "mean", err.mean())
+    assert err.mean() < 5e-3 and err.max() < 0.1
