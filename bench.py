@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of replaying the frame graph")
+    ap.add_argument("--no-denoise", action="store_true", help="skip the denoised time-to-relMSE leg")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -130,6 +131,56 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_bf16_tflops():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured (burst)"
+    return 1590.0, "fallback"
+
+
+# Denoiser FLOPs per pixel (forward): sum over its 3x3 convolutions of 2*9*Cin*Cout / 4^level,
+# with the channel counts of bte_denoise.cu (input 16, levels 32/48/64/96/128, output 16).
+DENOISER_CONVS = [(16, 32, 0), (32, 32, 0), (32, 48, 1), (48, 48, 1), (48, 64, 2), (64, 64, 2), (64, 96, 3), (96, 96, 3),
+                  (96, 128, 4), (128, 128, 4), (224, 96, 3), (96, 96, 3), (160, 64, 2), (64, 64, 2), (112, 48, 1),
+                  (48, 48, 1), (80, 32, 0), (32, 32, 0), (32, 16, 0)]
+DENOISER_FLOP_PER_PIXEL = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in DENOISER_CONVS)
+
+
+def denoise_leg():
+    """Second half of the metric: device time to relMSE <= 2e-3 against the FP64 16384-spp image, plain
+    accumulation vs denoised low-spp, on the Cornell box (256x256, depth 8); plus the denoiser's inference
+    time at 1920x1080 against the measured BF16 tensor-core peak."""
+    weights = os.path.join(ROOT, "bluetruthengine_b200", "weights", "denoiser_c4.npz")
+    if not os.path.exists(weights):
+        return {"unavailable": "no trained weights at bluetruthengine_b200/weights/denoiser_c4.npz"}
+    from bluetruthengine_b200.denoise_eval import evaluate
+    from bluetruthengine_b200.denoiser import Denoiser
+    res = evaluate("cornell", weights)
+    out = {"metric": "device ms to relMSE<=2e-3 vs FP64 16384-spp reference", "scene": "cornell 256x256 depth 8",
+           "plain": res["plain"], "denoised": res["denoised"], "speedup": res.get("speedup"),
+           "denoised_sweep": res["denoised_sweep"]}
+    dn = Denoiser()
+    dn.load(weights)
+    rng = np.random.default_rng(0)
+    H, W = 1080, 1920
+    rad = rng.exponential(0.5, size=(H, W, 3)).astype(np.float32)
+    feat = rng.uniform(0, 1, size=(H, W, 6)).astype(np.float32)
+    for _ in range(2):
+        dn.denoise(rad, feat)
+    ms = []
+    for _ in range(5):
+        dn.denoise(rad, feat)
+        ms.append(dn.last_ms())
+    t = statistics.median(ms)
+    flops = DENOISER_FLOP_PER_PIXEL * W * ((H + 15) // 16 * 16)
+    peak, kind = measured_bf16_tflops()
+    out["inference_1080p"] = {"ms": t, "gflop": flops / 1e9, "tflops": flops / (t / 1e3) / 1e12,
+                              "peak_tflops": peak, "peak_source": kind, "frac": flops / (t / 1e3) / 1e12 / peak}
+    return out
 
 
 class ReferenceCpu:
@@ -308,6 +359,11 @@ def run_ours(args):
             out["cpu_baseline"] = cpu_baseline(scene, args, seconds=args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never the product
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0 and not args.no_denoise:
+        try:
+            out["denoise"] = denoise_leg()
+        except Exception as e:
+            out["denoise"] = {"unavailable": str(e)}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

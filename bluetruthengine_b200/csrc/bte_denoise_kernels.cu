@@ -109,47 +109,62 @@ __device__ __forceinline__ void convMma(float (&acc)[NT][4], const ConvFrag<NT>&
     for (int j = 0; j < NT; ++j) mma16816(acc[j], f.a[0], f.a[1], f.a[2], f.a[3], f.b[j][0], f.b[j][1]);
 }
 
-template <int NT, bool Relu, bool Up>
+template <int NT, bool Relu, bool Up, bool Split>
 __global__ void __launch_bounds__(128) kConv3x3(const bf16* __restrict__ X1, int C1, const bf16* __restrict__ X2, int C2,
                                                 int H, int W, const bf16* __restrict__ Wk, const float* __restrict__ bias,
                                                 int Cout, int colBlocks, bf16* __restrict__ Y)
 {
-    __shared__ float part[4][16][8 * NT + 1];
+    __shared__ float part[Split ? 4 : 1][16][8 * NT + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     const int n = blockIdx.z / colBlocks;
     const int co0 = (blockIdx.z - n * colBlocks) * (8 * NT);
     const int y = blockIdx.y;
-    const int x0 = blockIdx.x * 16;
+    const int x0 = Split ? blockIdx.x * 16 : blockIdx.x * 64 + warp * 16;
+    if (!Split && x0 >= W) return;
     const int xa = x0 + g, xb = x0 + g + 8;
     const int Cin = C1 + C2;
     const int chunks = Cin / 16;
-    const int myTaps = warp == 0 ? 3 : 2;   // taps warp, warp + 4, warp + 8
-    const int steps = myTaps * chunks;
+    const int steps = (Split ? (warp == 0 ? 3 : 2) : 9) * chunks;   // split: taps warp, warp + 4, warp + 8
+    auto tapOf = [&](int step) { return Split ? warp + 4 * (step / chunks) : step / chunks; };
     float acc[NT][4];
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
     ConvFrag<NT> fa, fb;
-    convLoad<NT, Up>(fa, X1, C1, X2, C2, n, H, W, y, xa, xb, warp, 0, Wk, Cout, co0, g, t);
+    convLoad<NT, Up>(fa, X1, C1, X2, C2, n, H, W, y, xa, xb, tapOf(0), 0, Wk, Cout, co0, g, t);
     for (int s = 0; s < steps; s += 2) {
-        if (s + 1 < steps) {
-            const int tp = warp + 4 * ((s + 1) / chunks), c0 = 16 * ((s + 1) % chunks);
-            convLoad<NT, Up>(fb, X1, C1, X2, C2, n, H, W, y, xa, xb, tp, c0, Wk, Cout, co0, g, t);
-        }
+        if (s + 1 < steps)
+            convLoad<NT, Up>(fb, X1, C1, X2, C2, n, H, W, y, xa, xb, tapOf(s + 1), 16 * ((s + 1) % chunks), Wk, Cout, co0,
+                             g, t);
         convMma<NT>(acc, fa);
         if (s + 1 >= steps) break;
-        if (s + 2 < steps) {
-            const int tp = warp + 4 * ((s + 2) / chunks), c0 = 16 * ((s + 2) % chunks);
-            convLoad<NT, Up>(fa, X1, C1, X2, C2, n, H, W, y, xa, xb, tp, c0, Wk, Cout, co0, g, t);
-        }
+        if (s + 2 < steps)
+            convLoad<NT, Up>(fa, X1, C1, X2, C2, n, H, W, y, xa, xb, tapOf(s + 2), 16 * ((s + 2) % chunks), Wk, Cout, co0,
+                             g, t);
         convMma<NT>(acc, fb);
     }
+    if (!Split) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const int co = co0 + j * 8 + 2 * t;
+            const float b0 = bias ? bias[co] : 0.0f, b1 = bias ? bias[co + 1] : 0.0f;
+            float v00 = acc[j][0] + b0, v01 = acc[j][1] + b1, v10 = acc[j][2] + b0, v11 = acc[j][3] + b1;
+            if (Relu) {
+                v00 = fmaxf(v00, 0.0f); v01 = fmaxf(v01, 0.0f); v10 = fmaxf(v10, 0.0f); v11 = fmaxf(v11, 0.0f);
+            }
+            const size_t rowOut = (static_cast<size_t>(n) * H + y) * W;
+            if (xa < W) *reinterpret_cast<uint32_t*>(Y + (rowOut + xa) * Cout + co) = packBf16(v00, v01);
+            if (xb < W) *reinterpret_cast<uint32_t*>(Y + (rowOut + xb) * Cout + co) = packBf16(v10, v11);
+        }
+        return;
+    }
+    const int pw = Split ? warp : 0;
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
-        part[warp][g][j * 8 + 2 * t] = acc[j][0];
-        part[warp][g][j * 8 + 2 * t + 1] = acc[j][1];
-        part[warp][g + 8][j * 8 + 2 * t] = acc[j][2];
-        part[warp][g + 8][j * 8 + 2 * t + 1] = acc[j][3];
+        part[pw][g][j * 8 + 2 * t] = acc[j][0];
+        part[pw][g][j * 8 + 2 * t + 1] = acc[j][1];
+        part[pw][g + 8][j * 8 + 2 * t] = acc[j][2];
+        part[pw][g + 8][j * 8 + 2 * t + 1] = acc[j][3];
     }
     __syncthreads();
     // 16 pixels x 4*NT channel pairs, summed over the four warps
@@ -157,8 +172,9 @@ __global__ void __launch_bounds__(128) kConv3x3(const bf16* __restrict__ X1, int
         const int px = e / (4 * NT), cp = 2 * (e % (4 * NT));
         const int x = x0 + px;
         if (x >= W) continue;
-        float v0 = part[0][px][cp] + part[1][px][cp] + part[2][px][cp] + part[3][px][cp];
-        float v1 = part[0][px][cp + 1] + part[1][px][cp + 1] + part[2][px][cp + 1] + part[3][px][cp + 1];
+        float v0 = 0.0f, v1 = 0.0f;
+#pragma unroll
+        for (int q = 0; q < (Split ? 4 : 1); ++q) { v0 += part[q][px][cp]; v1 += part[q][px][cp + 1]; }
         const int co = co0 + cp;
         if (bias) { v0 += bias[co]; v1 += bias[co + 1]; }
         if (Relu) { v0 = fmaxf(v0, 0.0f); v1 = fmaxf(v1, 0.0f); }
@@ -502,20 +518,32 @@ int gridFor(long long n, int block = 256)
     return static_cast<int>(g < 1 ? 1 : g);
 }
 
-template <bool Relu, bool Up>
+template <bool Relu, bool Up, bool Split>
 void launchConvNT(int nt, dim3 grid, const bf16* X1, int C1, const bf16* X2, int C2, int H, int W, const bf16* Wk,
                   const float* bias, int Cout, int colBlocks, bf16* Y, cudaStream_t st)
 {
+#define BTE_CONV_CASE(K) \
+    case K: kConv3x3<K, Relu, Up, Split><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
     switch (nt) {
-    case 1: kConv3x3<1, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    case 2: kConv3x3<2, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    case 3: kConv3x3<3, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    case 4: kConv3x3<4, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    case 5: kConv3x3<5, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    case 6: kConv3x3<6, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    case 7: kConv3x3<7, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
-    default: kConv3x3<8, Relu, Up><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
+    BTE_CONV_CASE(1) BTE_CONV_CASE(2) BTE_CONV_CASE(3) BTE_CONV_CASE(4) BTE_CONV_CASE(5) BTE_CONV_CASE(6) BTE_CONV_CASE(7)
+    default: kConv3x3<8, Relu, Up, Split><<<grid, 128, 0, st>>>(X1, C1, X2, C2, H, W, Wk, bias, Cout, colBlocks, Y); break;
     }
+#undef BTE_CONV_CASE
+}
+
+template <bool Relu, bool Up>
+void launchConv(int nt, int N, int H, int W, const bf16* X1, int C1, const bf16* X2, int C2, const bf16* Wk,
+                const float* bias, int Cout, int colBlocks, bf16* Y, cudaStream_t st)
+{
+    // Unsplit CTAs (64 pixels, each warp all nine taps) when they fill the
+    // machine several times over; otherwise 16-pixel CTAs whose warps split the taps.
+    const long long whole = static_cast<long long>((W + 63) / 64) * H * N * colBlocks;
+    if (whole >= 148LL * 16)
+        launchConvNT<Relu, Up, false>(nt, dim3((W + 63) / 64, H, N * colBlocks), X1, C1, X2, C2, H, W, Wk, bias, Cout,
+                                      colBlocks, Y, st);
+    else
+        launchConvNT<Relu, Up, true>(nt, dim3((W + 15) / 16, H, N * colBlocks), X1, C1, X2, C2, H, W, Wk, bias, Cout,
+                                     colBlocks, Y, st);
 }
 
 }  // namespace
@@ -539,17 +567,16 @@ void conv3x3Cat(const void* X1, int C1, bool up, const void* X2, int C2, int N, 
 {
     const int nt = pickNT(Cout);
     const int colBlocks = Cout / (8 * nt);
-    const dim3 grid((W + 15) / 16, H, N * colBlocks);
     const bf16* a = static_cast<const bf16*>(X1);
     const bf16* b = static_cast<const bf16*>(X2);
     const bf16* w = static_cast<const bf16*>(Wk);
     bf16* y = static_cast<bf16*>(Y);
     if (relu) {
-        if (up) launchConvNT<true, true>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
-        else launchConvNT<true, false>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
+        if (up) launchConv<true, true>(nt, N, H, W, a, C1, b, C2, w, bias, Cout, colBlocks, y, st);
+        else launchConv<true, false>(nt, N, H, W, a, C1, b, C2, w, bias, Cout, colBlocks, y, st);
     } else {
-        if (up) launchConvNT<false, true>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
-        else launchConvNT<false, false>(nt, grid, a, C1, b, C2, H, W, w, bias, Cout, colBlocks, y, st);
+        if (up) launchConv<false, true>(nt, N, H, W, a, C1, b, C2, w, bias, Cout, colBlocks, y, st);
+        else launchConv<false, false>(nt, N, H, W, a, C1, b, C2, w, bias, Cout, colBlocks, y, st);
     }
 }
 

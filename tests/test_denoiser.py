@@ -9,7 +9,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(2, 20, 37, 32, 48), (1, 16, 64, 16, 32), (1, 9, 70, 224, 96), (2, 8, 24, 80, 16)]
+# small shapes run the tap-split kernel, the last (3 x 300 x 4 = 3600 CTAs of 64 pixels) the unsplit one
+SHAPES = [(2, 20, 37, 32, 48), (1, 16, 64, 16, 32), (1, 9, 70, 224, 96), (2, 8, 24, 80, 16), (4, 300, 130, 32, 48)]
 
 
 def _bf16(a):
@@ -177,14 +178,15 @@ def _torch_unet(params, rad, feat):
     return np.maximum(np.expm1(pred.permute(1, 2, 0).numpy()), 0)[:H, :W]
 
 
-def test_network_inference_matches_torch(dn):
+@pytest.mark.parametrize("size", [(72, 100), (470, 640)])
+def test_network_inference_matches_torch(dn, size):
     """The whole inference path (feature assembly, edge padding, encoder, in-place upsample+concat decoder,
-    residual output) against the same network written in PyTorch, on a trained-like random network."""
-    from bluetruthengine_b200.denoiser import Denoiser
+    residual output) against the same network written in PyTorch, on a random network; the larger size
+    runs the full-resolution layers on the unsplit convolution kernel."""
     dn.init(11)
     p = dn.params()
     rng = np.random.default_rng(5)
-    H, W = 72, 100
+    H, W = size
     rad = rng.exponential(0.4, size=(H, W, 3)).astype(np.float32)
     feat = np.concatenate([rng.uniform(0, 1, (H, W, 3)), rng.normal(size=(H, W, 3))], -1).astype(np.float32)
     got = dn.denoise(rad, feat)
