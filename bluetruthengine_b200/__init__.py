@@ -45,7 +45,7 @@ assert TRIANGLE_DTYPE.itemsize == 96 and BSDF_DTYPE.itemsize == 68 and CAMERA_DT
 class Tuning(C.Structure):
     """BteTuning (include/bte/render_api.h)."""
     _fields_ = [("bvhWidth", C.c_int), ("maxLeafTriangles", C.c_int), ("shadeMinBlocks", C.c_int),
-                ("postponePercent", C.c_int)]
+                ("postponePercent", C.c_int), ("sortShading", C.c_int)]
 
 
 class RenderConfig(C.Structure):
@@ -321,8 +321,8 @@ class Renderer:
         return out[..., :3].copy(), out[..., 3:].copy()
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
-                   postpone_percent: int = 20):
-        t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent))
+                   postpone_percent: int = 20, sort_shading: int = 1):
+        t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading))
         _check(self.lib.bte_set_tuning(C.byref(t)))
 
     def tuning(self) -> dict:

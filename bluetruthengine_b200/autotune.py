@@ -6,6 +6,7 @@ Sweeps the knobs that decide throughput on a given scene and GPU:
   * threads per block of the persistent stage kernels,
   * residency the shade kernel is compiled for (2 or 3 blocks per SM),
   * the leaf-test postponing threshold of the 8-wide walk,
+  * material-sorted shading on or off,
 timing whole frames on the device (CUDA events), and leaves the renderer in
 the fastest configuration.  Results are deterministic in value (every
 configuration renders the same bits); only speed differs.
@@ -24,19 +25,21 @@ class TuneResult:
     block_size: int
     shade_min_blocks: int
     postpone_percent: int
+    sort_shading: int
     ms_per_frame: float
     msamples_per_s: float
 
 
 def autotune(renderer, width: int, height: int, samples_per_frame: int, max_depth: int, env_sampling: int,
              trees=((8, 1), (8, 2), (8, 3), (2, 1)), blocks=(128, 256), shade_min_blocks=(2, 3),
-             postpone=(0, 20), frames: int = 3, verbose: bool = False):
+             postpone=(0, 20), sort_shading=(1,), frames: int = 3, verbose: bool = False):
     results = []
     for bvh_width, leaf in trees:
         renderer.set_tuning(leaf, 2, bvh_width)
         renderer.init_accel()
-        for blk, smb, pp in itertools.product(blocks, shade_min_blocks, postpone if bvh_width == 8 else (0,)):
-            renderer.set_tuning(leaf, smb, bvh_width, pp)
+        for blk, smb, pp, srt in itertools.product(blocks, shade_min_blocks, postpone if bvh_width == 8 else (0,),
+                                                   sort_shading):
+            renderer.set_tuning(leaf, smb, bvh_width, pp, srt)
             renderer.set_config(samples_per_frame=samples_per_frame, max_depth=max_depth, rr_start=3,
                                 env_sampling=env_sampling, block_size=blk)
             renderer.render(width, height)          # warm-up at this configuration
@@ -45,12 +48,12 @@ def autotune(renderer, width: int, height: int, samples_per_frame: int, max_dept
                 renderer.render(width, height)
                 ms += renderer.stats().msTotal
             ms /= frames
-            r = TuneResult(bvh_width, leaf, blk, smb, pp, ms, width * height * samples_per_frame / ms / 1e3)
+            r = TuneResult(bvh_width, leaf, blk, smb, pp, srt, ms, width * height * samples_per_frame / ms / 1e3)
             results.append(r)
             if verbose:
                 print(json.dumps(asdict(r)), flush=True)
     best = min(results, key=lambda r: r.ms_per_frame)
-    renderer.set_tuning(best.max_leaf, best.shade_min_blocks, best.bvh_width, best.postpone_percent)
+    renderer.set_tuning(best.max_leaf, best.shade_min_blocks, best.bvh_width, best.postpone_percent, best.sort_shading)
     renderer.init_accel()
     renderer.set_config(samples_per_frame=samples_per_frame, max_depth=max_depth, rr_start=3,
                         env_sampling=env_sampling, block_size=best.block_size)

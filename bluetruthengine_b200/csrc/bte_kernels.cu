@@ -38,6 +38,27 @@ BTE_DI int appendCoalesced(int* counter)
     return base + static_cast<int>(g.thread_rank());
 }
 
+// warp-aggregated append into one of several counters (lanes grouped by key)
+BTE_DI int appendKeyed(int* counters, int key)
+{
+    const unsigned active = __activemask();
+    const unsigned same = __match_any_sync(active, key);
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int leader = __ffs(same) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counters + key, __popc(same));
+    base = __shfl_sync(same, base, leader);
+    return base + __popc(same & ((1u << lane) - 1u));
+}
+
+// bucket of a path for material-sorted shading: 0 miss, else the BSDF type of the hit triangle
+BTE_DI void sortAppend(const DevScene& s, const DevPaths& P, int bounce, int idx, int tri)
+{
+    const int key = tri < 0 ? 0 : s.bsdfs[s.triBsdfIds[tri]].type;
+    const int k = (key >= 0 && key < kSortKeys) ? key : 0;
+    P.sortQueue[static_cast<size_t>(k) * P.count + appendKeyed(P.sortCount + bounce * kSortKeys, k)] = idx;
+}
+
 BTE_DI V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 
 // Adds the contributions of the visible NEE slots in slot order and clears the mask.
@@ -101,6 +122,7 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
         const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
         P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
         if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
+        if (P.sortQueue) sortAppend(s, P, bounce, idx, tri);
     }
 }
 
@@ -113,8 +135,23 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
     const int* __restrict__ q = P.queue[bounce & 1];
     int* qn = P.queue[(bounce + 1) & 1];
     const int stride = gridDim.x * blockDim.x;
+    int bucketEnd[kSortKeys];
+    if (P.sortQueue) {
+        int run = 0;
+#pragma unroll
+        for (int k = 0; k < kSortKeys; ++k) { run += P.sortCount[bounce * kSortKeys + k]; bucketEnd[k] = run; }
+    }
     for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += stride) {
-        const int idx = q[slot];
+        int idx;
+        if (P.sortQueue) {
+            int k = 0, start = 0;
+#pragma unroll
+            for (int j = 0; j < kSortKeys - 1; ++j)
+                if (slot >= bucketEnd[j]) { k = j + 1; start = bucketEnd[j]; }
+            idx = P.sortQueue[static_cast<size_t>(k) * P.count + (slot - start)];
+        } else {
+            idx = q[slot];
+        }
         const float4 o4 = P.o[idx], d4 = P.d[idx], tp4 = P.tp[idx], L4 = P.L[idx];
         uint32_t rng = __float_as_uint(o4.w);
         PathReg p;
@@ -250,6 +287,7 @@ __global__ void __launch_bounds__(256) kExtendWide(DevScene s, DevPaths P, int b
             if (!r.valid || s.triCount <= 0) {
                 P.hit[idx] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
                 if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = -1;
+                if (P.sortQueue) sortAppend(s, P, bounce, idx, -1);
                 idx = -1;
                 continue;
             }
@@ -260,6 +298,7 @@ __global__ void __launch_bounds__(256) kExtendWide(DevScene s, DevPaths P, int b
             P.hit[idx] = tri >= 0 ? make_float4(w.bt, w.bu, w.bv, __int_as_float(tri))
                                   : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
             if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
+            if (P.sortQueue) sortAppend(s, P, bounce, idx, tri);
             idx = -1;
         }
     }

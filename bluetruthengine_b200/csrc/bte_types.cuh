@@ -61,6 +61,7 @@ struct WideNode {
 };
 static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
 constexpr int kWideLeafMax = 3;
+constexpr int kSortKeys = 6;
 constexpr int kWideStack = 64;    // traversal stack entries; trees deeper than half of it use the binary tree
 
 struct DevScene {
@@ -116,6 +117,10 @@ struct DevPaths {
     int slots;        // 1 (area) + spotCount + 1 (env)
     int maxDepth;
     int count;        // paths in the frame
+    // material-sorted shading: extend appends each path to bucket 0 (miss) or its hit's BSDF type (1-5); shade
+    // consumes the buckets in order, so that a warp runs one BSDF's code
+    int* sortQueue;   // [kSortKeys * count] or null (sorting off)
+    int* sortCount;   // [(maxDepth + 1) * kSortKeys]
     unsigned int* errorFlags;   // bit 0: traversal stack overflow; bit 1: malformed tree (index out of range)
 };
 

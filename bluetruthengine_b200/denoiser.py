@@ -101,3 +101,31 @@ class Denoiser:
         _check(self.lib.bte_denoiser_debug_conv(op, ptrs[0], ptrs[1], ptrs[2], ptrs[3], n, h, wd, cin, cout,
                                                 1 if relu else 0, out.ctypes.data_as(C.c_void_p)))
         return out
+
+
+def _main(argv=None):
+    """Time inference: python -m bluetruthengine_b200.denoiser --width 1920 --height 1080 --iters 5"""
+    import argparse
+    import json
+    import os
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--iters", type=int, default=5)
+    ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
+                                                      "denoiser_c4.npz"))
+    args = ap.parse_args(argv)
+    dn = Denoiser()
+    dn.load(args.weights)
+    rng = np.random.default_rng(0)
+    rad = rng.exponential(0.5, size=(args.height, args.width, 3)).astype(np.float32)
+    feat = rng.uniform(0, 1, size=(args.height, args.width, 6)).astype(np.float32)
+    ms = []
+    for _ in range(args.iters):
+        dn.denoise(rad, feat)
+        ms.append(dn.last_ms())
+    print(json.dumps({"width": args.width, "height": args.height, "ms": ms}), flush=True)
+
+
+if __name__ == "__main__":
+    _main()

@@ -119,6 +119,8 @@ typedef struct {
     int shadeMinBlocks;    /* resident blocks per SM the shade kernel is compiled for: 2 or 3 */
     int postponePercent;   /* 8-wide walk: a lane defers its leaf tests while fewer than this
                             * percentage of the warp's lanes have leaf tests (0 = never, 0-100) */
+    int sortShading;       /* 1: extend buckets paths by hit material (miss, BSDF type) and shade runs the
+                            * buckets in order; 0: shade runs the extend queue as it is */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);

@@ -49,9 +49,9 @@ def test_math_functions_bitexact(renderer, oracle_mod):
         assert len(bad) == 0, f"fn {fn}: {len(bad)} mismatches"
 
 
-def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1):
+def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0):
     renderer.cleanup()
-    renderer.set_tuning(max_leaf, 3, bvh_width)
+    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
@@ -89,8 +89,8 @@ def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, t
     assert np.array_equal(go, oo)
 
 
-def _render_and_compare(renderer, oracle_mod, scene, env_mode, spp, depth, frames=1):
-    _upload(renderer, scene, env_mode=env_mode, spp=spp, depth=depth)
+def _render_and_compare(renderer, oracle_mod, scene, env_mode, spp, depth, frames=1, sort_shading=0):
+    _upload(renderer, scene, env_mode=env_mode, spp=spp, depth=depth, sort_shading=sort_shading)
     renderer.set_hit_log(True)
     W, H = scene.width, scene.height
     renderer.reset_accumulation(W, H)
@@ -146,9 +146,11 @@ def test_cornell_frame_bitexact(renderer, oracle_mod, cornell_scene):
     assert np.isfinite(o).all() and o.mean() > 0.05
 
 
+@pytest.mark.parametrize("sort_shading", [0, 1])
 @pytest.mark.parametrize("env_mode", [0, 1])
-def test_random_scene_bitexact(renderer, oracle_mod, random_scene, env_mode):
-    _render_and_compare(renderer, oracle_mod, random_scene, env_mode=env_mode, spp=3, depth=12)
+def test_random_scene_bitexact(renderer, oracle_mod, random_scene, env_mode, sort_shading):
+    """All five BSDFs, area light, spotlight and env map; with and without material-sorted shading."""
+    _render_and_compare(renderer, oracle_mod, random_scene, env_mode=env_mode, spp=3, depth=12, sort_shading=sort_shading)
 
 
 def test_random_scene_vs_reference_headers(renderer, oracle_mod, random_scene):
@@ -248,14 +250,14 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode,bvh_width", [(1, 8), (0, 8), (1, 2)])
-def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width):
+@pytest.mark.parametrize("env_mode,bvh_width,sort_shading", [(1, 8, 0), (0, 8, 0), (1, 2, 0), (1, 8, 1)])
+def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
     pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
-    _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width)
+    _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading)
     info = renderer.accel_info()
     print("accel", info)
     assert info["width"] == bvh_width
@@ -313,9 +315,10 @@ def test_textured_materials_bitexact(renderer, oracle_mod, random_scene):
 def test_tuning_roundtrip_and_validation(renderer):
     """bte_set_tuning / bte_get_tuning: values round-trip; out-of-range values are rejected with a message."""
     import bluetruthengine_b200 as B
-    renderer.set_tuning(2, 2, 8, 35)
-    assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35}
-    for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101)]:
+    renderer.set_tuning(2, 2, 8, 35, 1)
+    assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
+                                 "sortShading": 1}
+    for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
