@@ -101,6 +101,8 @@ struct Net {
     Buf dsNoisy, dsFeat, dsTarget;
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
+    bool useTc = false;   // tcgen05 convolutions for the full-resolution layers
+    Buf errFlag;          // set by a tcgen05 convolution that timed out
 };
 
 Net net;
@@ -132,6 +134,8 @@ void refreshCopies()
 void ensureNet()
 {
     if (net.stream) return;
+    net.errFlag.ensure(sizeof(unsigned int));
+    ck(cudaMemset(net.errFlag.p, 0, sizeof(unsigned int)), "cudaMemset");
     ck(cudaStreamCreateWithFlags(&net.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     ck(cudaEventCreate(&net.ev0), "cudaEventCreate");
     ck(cudaEventCreate(&net.ev1), "cudaEventCreate");
@@ -188,6 +192,28 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
     net.aN = N; net.aHp = Hp; net.aWp = Wp; net.aGrad = withGrad;
 }
 
+// One 3x3 convolution over concat(up ? upsample(X1) : X1, X2): the tcgen05 kernel for layers large
+// enough to fill the machine with 128-pixel tiles, the warp-level kernel otherwise.
+void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+                  const float* bias, int Cout, bool relu, void* Y, cudaStream_t st, int force = -1)
+{
+    const long long px = static_cast<long long>(N) * H * W;
+    const bool tc = force >= 0 ? force == 1 : (net.useTc && convTcSupported(C1 + C2, Cout) && px >= 128LL * 148 * 4);
+    if (tc) conv3x3Tc(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
+    else conv3x3Cat(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, st);
+}
+
+void checkTcFlag()
+{
+    unsigned int f = 0;
+    ck(cudaMemcpyAsync(&f, net.errFlag.p, sizeof(f), cudaMemcpyDeviceToHost, net.stream), "cudaMemcpyAsync");
+    ck(cudaStreamSynchronize(net.stream), "sync");
+    if (f) {
+        ck(cudaMemsetAsync(net.errFlag.p, 0, sizeof(f), net.stream), "cudaMemsetAsync");
+        throw CudaErr{"denoiser: a tensor-core convolution timed out waiting for its pipeline"};
+    }
+}
+
 // Training keeps the concatenated decoder inputs (the weight gradients read
 // them); inference lets the decoder convolutions read upsample + skip in place.
 void forward(int N, int Hp, int Wp, bool training)
@@ -203,12 +229,13 @@ void forward(int N, int Hp, int Wp, bool training)
             if (!training && prev && prev->op == kUpCatOp && prev->dst == s.src) {
                 const TensorSpec& low = kTensors[prev->src];
                 const TensorSpec& skip = kTensors[prev->src2];
-                conv3x3Cat(net.act[prev->src].p, low.c, true, net.act[prev->src2].p, skip.c, N, H, W,
-                           net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
-                           c.relu, net.act[s.dst].p, st);
+                convDispatch(net.act[prev->src].p, low.c, true, net.act[prev->src2].p, skip.c, N, H, W,
+                             net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
+                             c.relu, net.act[s.dst].p, st);
             } else {
-                conv3x3(net.act[s.src].p, N, H, W, c.cin, net.wk.as<unsigned short>() + net.bfOff[s.conv],
-                        net.w.as<float>() + net.bOff[s.conv], c.cout, c.relu, net.act[s.dst].p, st);
+                convDispatch(net.act[s.src].p, c.cin, false, nullptr, 0, N, H, W,
+                             net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
+                             c.relu, net.act[s.dst].p, st);
             }
         } else if (s.op == kPoolOp) {
             pool2(net.act[s.src].p, N, H, W, ts.c, net.act[s.dst].p, st);
@@ -236,8 +263,8 @@ void backward(int N, int Hp, int Wp)
             convWgrad(net.act[s.src].p, net.gact[s.dst].p, N, H, W, c.cin, c.cout, net.grad.as<float>() + net.wOff[s.conv], st);
             biasGrad(net.gact[s.dst].p, static_cast<long long>(N) * H * W, c.cout, net.grad.as<float>() + net.bOff[s.conv], st);
             if (s.src != 0)
-                conv3x3(net.gact[s.dst].p, N, H, W, c.cout, net.wd.as<unsigned short>() + net.bfOff[s.conv], nullptr,
-                        c.cin, false, net.gact[s.src].p, st);
+                convDispatch(net.gact[s.dst].p, c.cout, false, nullptr, 0, N, H, W,
+                             net.wd.as<unsigned short>() + net.bfOff[s.conv], nullptr, c.cin, false, net.gact[s.src].p, st);
         } else if (s.op == kPoolOp) {
             // the pooled tensor's other consumer (the decoder concatenation) wrote its gradient already
             pool2Back(net.gact[s.dst].p, N, H, W, ts.c, net.gact[s.src].p, st);
@@ -289,6 +316,7 @@ void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, f
     ck(cudaEventRecord(net.ev1, st), "cudaEventRecord");
     ck(cudaEventSynchronize(net.ev1), "denoise");
     ck(cudaEventElapsedTime(&net.lastMs, net.ev0, net.ev1), "cudaEventElapsedTime");
+    checkTcFlag();
 }
 
 bool denoiserReady()
@@ -430,6 +458,7 @@ int bte_denoiser_train(int steps, int batch, int crop, float learningRate, uint6
         ck(cudaMemcpyAsync(sums.data(), net.lossSum.p, sizeof(float) * steps, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         ck(cudaStreamSynchronize(st), "train");
         ck(cudaEventElapsedTime(&net.lastMs, net.ev0, net.ev1), "cudaEventElapsedTime");
+        checkTcFlag();
         if (lossPerStep)
             for (int s = 0; s < steps; ++s) lossPerStep[s] = sums[static_cast<size_t>(s)] / static_cast<float>(px * 3);
         return 0;
@@ -455,6 +484,12 @@ int bte_denoiser_denoise(const float* radiance, const float* features, int width
         ck(cudaStreamSynchronize(net.stream), "sync");
         return 0;
     });
+}
+
+// 1: full-resolution convolutions on the tcgen05 kernel; 0: the warp-level mma.sync kernel only
+int bte_denoiser_set_tcgen05(int enabled)
+{
+    return guardedDn([&] { ensureNet(); net.useTc = enabled != 0; return 0; });
 }
 
 int bte_denoiser_last_ms(float* ms)
@@ -489,6 +524,8 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
             weightCopies(bf32.as<float>(), static_cast<int>(padded / 9), 1, dst.p, nullptr, st);
             ck(cudaStreamSynchronize(st), "sync");
         };
+        const int force = op >= 3 ? 1 : 0;   // ops 3 and 4: ops 0 and 1 on the tcgen05 kernel
+        if (op >= 3) op -= 3;
         if (op == 0 || op == 1) {
             const int inC = op == 0 ? cin : cout, outC = op == 0 ? cout : cin;
             convert(op == 0 ? x : dy, px * inC, bx);
@@ -504,9 +541,10 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
                 ck(cudaMemcpyAsync(bb.p, bias, cout * 4ull, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
             }
             bo.ensure(px * outC * 2);
-            conv3x3(bx.p, n, h, wd, inC, op == 0 ? bwk.p : bwd.p, op == 0 && bias ? bb.as<float>() : nullptr, outC,
-                    op == 0 && relu, bo.p, st);
+            convDispatch(bx.p, inC, false, nullptr, 0, n, h, wd, op == 0 ? bwk.p : bwd.p,
+                         op == 0 && bias ? bb.as<float>() : nullptr, outC, op == 0 && relu, bo.p, st, force);
             ck(cudaGetLastError(), "conv launch");
+            checkTcFlag();
             // bf16 -> float on the host
             std::vector<unsigned short> hb(px * outC);
             ck(cudaMemcpyAsync(hb.data(), bo.p, hb.size() * 2, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");

@@ -14,6 +14,11 @@ void conv3x3(const void* X, int N, int H, int W, int Cin, const void* Wk, const 
 // place (X1 has C1 channels, X2 has C2, Wk's Cin = C1 + C2).
 void conv3x3Cat(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                 const float* bias, int Cout, bool relu, void* Y, cudaStream_t st);
+// The same convolution on the tcgen05 tensor cores (accumulator in TMEM);
+// sets *errorFlag on an internal timeout.  Cout: multiple of 16, <= 256.
+bool convTcSupported(int Cin, int Cout);
+void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+               const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);

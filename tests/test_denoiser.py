@@ -35,35 +35,38 @@ def dn():
     return Denoiser()
 
 
+@pytest.mark.parametrize("kernel", ["mma", "tcgen05"])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_conv_forward_matches_torch(dn, shape):
+def test_conv_forward_matches_torch(dn, shape, kernel):
+    """Forward 3x3 conv + bias + ReLU, warp-level MMA kernel and tcgen05/TMEM kernel."""
     n, h, w, cin, cout = shape
     rng = np.random.default_rng(cin * 7 + cout)
     x = _bf16(rng.normal(size=(n, h, w, cin)))
     wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
     b = rng.normal(size=cout).astype(np.float32)
-    got = dn.debug_conv(0, x=x, w=wt, bias=b, shape=shape, relu=True)
+    got = dn.debug_conv(0 if kernel == "mma" else 3, x=x, w=wt, bias=b, shape=shape, relu=True)
     _, _, y = _torch_conv(x, wt, b)
     ref = np.maximum(y.detach().permute(0, 2, 3, 1).numpy(), 0.0)
     err = np.abs(got - ref).max() / np.abs(ref).max()
-    print("forward", shape, "max error / max |y|", err)
+    print("forward", kernel, shape, "max error / max |y|", err)
     assert err < 1e-2
 
 
+@pytest.mark.parametrize("kernel", ["mma", "tcgen05"])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_conv_data_gradient_matches_torch(dn, shape):
+def test_conv_data_gradient_matches_torch(dn, shape, kernel):
     n, h, w, cin, cout = shape
     rng = np.random.default_rng(cin * 5 + cout)
     x = _bf16(rng.normal(size=(n, h, w, cin)))
     wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
     dy = _bf16(rng.normal(size=(n, h, w, cout)))
-    got = dn.debug_conv(1, w=wt, dy=dy, shape=shape)
+    got = dn.debug_conv(1 if kernel == "mma" else 4, w=wt, dy=dy, shape=shape)
     import torch
     xt, wt_t, y = _torch_conv(x, wt)
     y.backward(torch.from_numpy(dy).permute(0, 3, 1, 2))
     ref = xt.grad.permute(0, 2, 3, 1).numpy()
     err = np.abs(got - ref).max() / np.abs(ref).max()
-    print("data gradient", shape, err)
+    print("data gradient", kernel, shape, err)
     assert err < 1e-2
 
 
