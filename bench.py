@@ -319,12 +319,12 @@ def run_ours(args):
     st = r.stats()
     r.set_stage_timing(False)
     stages = {"generate": st.msGenerate, "extend": st.msExtend, "shade": st.msShade, "connect": st.msConnect,
-              "present": st.msPresent}
-    dom = max(stages, key=stages.get)
+              "present": st.msPresent, "tail": st.msTail}
+    dom = max((k for k in stages if k != "tail"), key=stages.get)
     launches_per_frame = 2 + 3 * args.depth
-    ext_f, sh_f = st.extends, st.shadowRays
+    ext_f, sh_f = st.extends - st.tailExtends, st.shadowRays - st.tailShadowRays   # rays of the wavefront stages
     bytes_dom = {"extend": ext_f * BYTES_PER_EXTEND_RAY, "shade": ext_f * BYTES_PER_SHADE_SEGMENT,
-                 "connect": sh_f * BYTES_PER_CONNECT_RAY,
+                 "connect": sh_f * BYTES_PER_CONNECT_RAY, "tail": 0,
                  "generate": W * H * args.spp * 73, "present": W * H * args.spp * 40}[dom]
     launches_dom = 1 if dom in ("generate", "present") else args.depth
     peak, peak_kind = measured_peaks()

@@ -45,7 +45,7 @@ assert TRIANGLE_DTYPE.itemsize == 96 and BSDF_DTYPE.itemsize == 68 and CAMERA_DT
 class Tuning(C.Structure):
     """BteTuning (include/bte/render_api.h)."""
     _fields_ = [("bvhWidth", C.c_int), ("maxLeafTriangles", C.c_int), ("shadeMinBlocks", C.c_int),
-                ("postponePercent", C.c_int), ("sortShading", C.c_int)]
+                ("postponePercent", C.c_int), ("sortShading", C.c_int), ("tailPaths", C.c_int)]
 
 
 class RenderConfig(C.Structure):
@@ -56,7 +56,9 @@ class RenderConfig(C.Structure):
 class FrameStats(C.Structure):
     _fields_ = [("samples", C.c_int64), ("extends", C.c_int64), ("shadowRays", C.c_int64),
                 ("maxBounceReached", C.c_int), ("msTotal", C.c_float), ("msGenerate", C.c_float),
-                ("msExtend", C.c_float), ("msShade", C.c_float), ("msConnect", C.c_float), ("msPresent", C.c_float)]
+                ("msExtend", C.c_float), ("msShade", C.c_float), ("msConnect", C.c_float), ("msPresent", C.c_float),
+                ("msTail", C.c_float), ("tailBounce", C.c_int), ("tailExtends", C.c_int64),
+                ("tailShadowRays", C.c_int64)]
 
 
 class _SceneArrays(C.Structure):
@@ -321,8 +323,9 @@ class Renderer:
         return out[..., :3].copy(), out[..., 3:].copy()
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
-                   postpone_percent: int = 20, sort_shading: int = 1):
-        t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading))
+                   postpone_percent: int = 20, sort_shading: int = 1, tail_paths: int = 0):
+        t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),
+                   int(tail_paths))
         _check(self.lib.bte_set_tuning(C.byref(t)))
 
     def tuning(self) -> dict:

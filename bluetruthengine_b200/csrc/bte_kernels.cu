@@ -61,6 +61,13 @@ BTE_DI void sortAppend(const DevScene& s, const DevPaths& P, int bounce, int idx
 
 BTE_DI V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 
+// The wavefront stops at the first bounce whose queue holds fewer than tailPaths paths; kTail then
+// finishes those paths one thread each (the few long paths no longer pay a launch per bounce).
+BTE_DI bool tailTakesOver(const DevPaths& P, int bounce)
+{
+    return P.tailPaths > 0 && P.rayCount[bounce] < P.tailPaths;
+}
+
 // Adds the contributions of the visible NEE slots in slot order and clears the mask.
 BTE_DI V3 resolveShadows(const DevPaths& P, int idx, V3 L)
 {
@@ -111,6 +118,7 @@ template <int Width>
 __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
+    if (tailTakesOver(P, bounce)) return;
     const int* __restrict__ q = P.queue[bounce & 1];
     const int stride = gridDim.x * blockDim.x;
     for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += stride) {
@@ -128,11 +136,108 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
 
 // ---------------------------------------------------------------- shade
 // src/wavefront/ray_shade.cu:103-183 (rt_optix_shading.cuh:412-447 order).
+// One path's shading at `bounce` (src/wavefront/ray_shade.cu:103-183, rt_optix_shading.cuh:412-447
+// order): pending shadow contributions, emitter/env hit, NEE records in the path's slots, scatter,
+// roulette; writes the path state back.  Shadow records are queued for kConnect when queueShadows,
+// else left in the slots (shMask) for the caller to trace.  Returns whether the path continues.
+BTE_DI bool shadePath(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int idx, bool queueShadows)
+{
+    const float4 o4 = P.o[idx], d4 = P.d[idx], tp4 = P.tp[idx], L4 = P.L[idx];
+    uint32_t rng = __float_as_uint(o4.w);
+    PathReg p;
+    p.o = xyz(o4); p.d = xyz(d4); p.tp = xyz(tp4); p.L = xyz(L4);
+    p.eta = d4.w;
+    p.brdfPdf = tp4.w;
+    const uint32_t bits = __float_as_uint(L4.w);
+    p.bounce = static_cast<int>(bits & 0xffffu);
+    p.specular = ((bits >> 16) & 1u) != 0u;
+
+    p.L = resolveShadows(P, idx, p.L);
+
+    const float4 hv = P.hit[idx];
+    const int tri = __float_as_int(hv.w);
+    if (tri < 0) {
+        if (bounce == 0 && P.aovAlbedo) {
+            P.aovAlbedo[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            P.aovNormal[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        accumulateEnvHit(s, p);
+        P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z, L4.w);
+        return false;
+    }
+    // closest-hit attributes, src/optix_programs.cu:121-140
+    HitReg h;
+    h.tri = tri;
+    {
+        const float t = hv.x, u = hv.y, v = hv.z;
+        const float w0 = 1.0f - u - v;
+        const TriangleData& T = s.tris[tri];
+        h.p = v3(p.o.x + t * p.d.x, p.o.y + t * p.d.y, p.o.z + t * p.d.z);
+        h.n = normalize3(v3(w0 * T.n0.x + u * T.n1.x + v * T.n2.x, w0 * T.n0.y + u * T.n1.y + v * T.n2.y,
+                            w0 * T.n0.z + u * T.n1.z + v * T.n2.z));
+        h.u = w0 * T.uv0.x + u * T.uv1.x + v * T.uv2.x;
+        h.v = w0 * T.uv0.y + u * T.uv1.y + v * T.uv2.y;
+    }
+    const Bsdf b = loadBsdf(s, tri, h.u, h.v);
+    if (bounce == 0 && P.aovAlbedo) {   // denoiser features: the material colour and normal seen first
+        const float4 a = b.type == BSDF_Dielectric ? make_float4(1.0f, 1.0f, 1.0f, 0.0f)
+                                                   : make_float4(b.p0.x, b.p0.y, b.p0.z, 0.0f);
+        P.aovAlbedo[idx] = a;
+        P.aovNormal[idx] = make_float4(h.n.x, h.n.y, h.n.z, 0.0f);
+    }
+    if (s.emitterFlags[tri] != 0) accumulateEmitterHit(s, p, h);
+
+    const Frame fr = makeFrame(h.n);
+    const V3 wiLocal = toLocal(fr, mul3(p.d, -1.0f));
+    if (bsdfIsDiffuseClass(b.type)) {
+        p.specular = false;
+        uint32_t newMask = 0u;
+        ShadowRec sr;
+        const size_t base = static_cast<size_t>(idx) * P.slots;
+        if (prepareArea(s, p, rng, h, b, wiLocal, fr, sr)) {
+            P.shDir[base] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
+            P.shContrib[base] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
+            newMask |= 1u;
+            if (queueShadows) P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base);
+        }
+        for (int si = 0; si < s.spotCount; ++si) {
+            if (prepareSpot(s, p, h, b, si, wiLocal, fr, sr)) {
+                P.shDir[base + 1 + si] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
+                P.shContrib[base + 1 + si] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
+                newMask |= 1u << (1 + si);
+                if (queueShadows) P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base + 1 + si);
+            }
+        }
+        if (prepareEnv(s, p, rng, h, b, wiLocal, fr, sr)) {
+            const int es = P.slots - 1;
+            P.shDir[base + es] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
+            P.shContrib[base + es] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
+            newMask |= 1u << es;
+            if (queueShadows) P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base + es);
+        }
+        if (newMask != 0u) {
+            P.shOrigin[idx] = make_float4(h.p.x, h.p.y, h.p.z, 0.0f);
+            P.shMask[idx] = newMask;
+        }
+    } else {
+        p.specular = true;
+    }
+    scatter(p, rng, h, b, wiLocal, fr);
+    const bool alive = roulette(p, rng, f.rrStart);
+    if (alive) p.bounce++;
+    P.o[idx] = make_float4(p.o.x, p.o.y, p.o.z, __uint_as_float(rng));
+    P.d[idx] = make_float4(p.d.x, p.d.y, p.d.z, p.eta);
+    P.tp[idx] = make_float4(p.tp.x, p.tp.y, p.tp.z, p.brdfPdf);
+    P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z,
+                           __uint_as_float(static_cast<uint32_t>(p.bounce) | (p.specular ? (1u << 16) : 0u)));
+    return alive;
+}
+
 template <int MinBlocks>
 __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P, FrameParams f, int bounce)
 {
     const int count = P.rayCount[bounce];
-    const int* __restrict__ q = P.queue[bounce & 1];
+    if (tailTakesOver(P, bounce)) return;
     int* qn = P.queue[(bounce + 1) & 1];
     const int stride = gridDim.x * blockDim.x;
     int bucketEnd[kSortKeys];
@@ -141,6 +246,7 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
 #pragma unroll
         for (int k = 0; k < kSortKeys; ++k) { run += P.sortCount[bounce * kSortKeys + k]; bucketEnd[k] = run; }
     }
+    const int* __restrict__ q = P.queue[bounce & 1];
     for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += stride) {
         int idx;
         if (P.sortQueue) {
@@ -152,94 +258,7 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
         } else {
             idx = q[slot];
         }
-        const float4 o4 = P.o[idx], d4 = P.d[idx], tp4 = P.tp[idx], L4 = P.L[idx];
-        uint32_t rng = __float_as_uint(o4.w);
-        PathReg p;
-        p.o = xyz(o4); p.d = xyz(d4); p.tp = xyz(tp4); p.L = xyz(L4);
-        p.eta = d4.w;
-        p.brdfPdf = tp4.w;
-        const uint32_t bits = __float_as_uint(L4.w);
-        p.bounce = static_cast<int>(bits & 0xffffu);
-        p.specular = ((bits >> 16) & 1u) != 0u;
-
-        p.L = resolveShadows(P, idx, p.L);
-
-        const float4 hv = P.hit[idx];
-        const int tri = __float_as_int(hv.w);
-        if (tri < 0) {
-            if (bounce == 0 && P.aovAlbedo) {
-                P.aovAlbedo[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                P.aovNormal[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            }
-            accumulateEnvHit(s, p);
-            P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z, L4.w);
-            continue;
-        }
-        // closest-hit attributes, src/optix_programs.cu:121-140
-        HitReg h;
-        h.tri = tri;
-        {
-            const float t = hv.x, u = hv.y, v = hv.z;
-            const float w0 = 1.0f - u - v;
-            const TriangleData& T = s.tris[tri];
-            h.p = v3(p.o.x + t * p.d.x, p.o.y + t * p.d.y, p.o.z + t * p.d.z);
-            h.n = normalize3(v3(w0 * T.n0.x + u * T.n1.x + v * T.n2.x, w0 * T.n0.y + u * T.n1.y + v * T.n2.y,
-                                w0 * T.n0.z + u * T.n1.z + v * T.n2.z));
-            h.u = w0 * T.uv0.x + u * T.uv1.x + v * T.uv2.x;
-            h.v = w0 * T.uv0.y + u * T.uv1.y + v * T.uv2.y;
-        }
-        const Bsdf b = loadBsdf(s, tri, h.u, h.v);
-        if (bounce == 0 && P.aovAlbedo) {   // denoiser features: the material colour and normal seen first
-            const float4 a = b.type == BSDF_Dielectric ? make_float4(1.0f, 1.0f, 1.0f, 0.0f)
-                                                       : make_float4(b.p0.x, b.p0.y, b.p0.z, 0.0f);
-            P.aovAlbedo[idx] = a;
-            P.aovNormal[idx] = make_float4(h.n.x, h.n.y, h.n.z, 0.0f);
-        }
-        if (s.emitterFlags[tri] != 0) accumulateEmitterHit(s, p, h);
-
-        const Frame fr = makeFrame(h.n);
-        const V3 wiLocal = toLocal(fr, mul3(p.d, -1.0f));
-        if (bsdfIsDiffuseClass(b.type)) {
-            p.specular = false;
-            uint32_t newMask = 0u;
-            ShadowRec sr;
-            const size_t base = static_cast<size_t>(idx) * P.slots;
-            if (prepareArea(s, p, rng, h, b, wiLocal, fr, sr)) {
-                P.shDir[base] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
-                P.shContrib[base] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
-                newMask |= 1u;
-                P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base);
-            }
-            for (int si = 0; si < s.spotCount; ++si) {
-                if (prepareSpot(s, p, h, b, si, wiLocal, fr, sr)) {
-                    P.shDir[base + 1 + si] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
-                    P.shContrib[base + 1 + si] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
-                    newMask |= 1u << (1 + si);
-                    P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base + 1 + si);
-                }
-            }
-            if (prepareEnv(s, p, rng, h, b, wiLocal, fr, sr)) {
-                const int es = P.slots - 1;
-                P.shDir[base + es] = make_float4(sr.d.x, sr.d.y, sr.d.z, sr.tmax);
-                P.shContrib[base + es] = make_float4(sr.c.x, sr.c.y, sr.c.z, 0.0f);
-                newMask |= 1u << es;
-                P.shadowQueue[appendCoalesced(P.shadowCount + bounce)] = static_cast<int>(base + es);
-            }
-            if (newMask != 0u) {
-                P.shOrigin[idx] = make_float4(h.p.x, h.p.y, h.p.z, 0.0f);
-                P.shMask[idx] = newMask;
-            }
-        } else {
-            p.specular = true;
-        }
-        scatter(p, rng, h, b, wiLocal, fr);
-        const bool alive = roulette(p, rng, f.rrStart);
-        if (alive) p.bounce++;
-        P.o[idx] = make_float4(p.o.x, p.o.y, p.o.z, __uint_as_float(rng));
-        P.d[idx] = make_float4(p.d.x, p.d.y, p.d.z, p.eta);
-        P.tp[idx] = make_float4(p.tp.x, p.tp.y, p.tp.z, p.brdfPdf);
-        P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z,
-                               __uint_as_float(static_cast<uint32_t>(p.bounce) | (p.specular ? (1u << 16) : 0u)));
+        const bool alive = shadePath(s, P, f, bounce, idx, true);
         if (alive && bounce + 1 < P.maxDepth) qn[appendCoalesced(P.rayCount + bounce + 1)] = idx;
     }
 }
@@ -251,6 +270,7 @@ template <int Width>
 __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.shadowCount[bounce];
+    if (tailTakesOver(P, bounce)) return;
     const int stride = gridDim.x * blockDim.x;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += stride) {
         const int e = P.shadowQueue[k];
@@ -271,6 +291,7 @@ __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int boun
 __global__ void __launch_bounds__(256) kExtendWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
+    if (tailTakesOver(P, bounce)) return;
     const int* __restrict__ q = P.queue[bounce & 1];
     int* fetch = P.fetch + bounce;
     WideWalk<false> w;
@@ -307,6 +328,7 @@ __global__ void __launch_bounds__(256) kExtendWide(DevScene s, DevPaths P, int b
 __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.shadowCount[bounce];
+    if (tailTakesOver(P, bounce)) return;
     int* fetch = P.fetch + (P.maxDepth + 1) + bounce;
     WideWalk<true> w;
     uint2 stack[kWideStack];
@@ -330,6 +352,49 @@ __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int 
             }
             e = -1;
         }
+    }
+}
+
+// ---------------------------------------------------------------- tail
+// Finishes the paths of the first bounce the wavefront left (tailTakesOver): per path, closest hit,
+// shading and its shadow rays, bounce after bounce, with the same per-path operations and counters
+// as the wavefront stages.
+template <int Width>
+__global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams f)
+{
+    if (P.tailPaths <= 0) return;
+    int b0 = -1;
+    for (int b = 0; b < P.maxDepth; ++b)
+        if (P.rayCount[b] < P.tailPaths) { b0 = b; break; }
+    if (b0 < 0) return;
+    const int count = P.rayCount[b0];
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= count) return;
+    const int idx = P.queue[b0 & 1][slot];
+    for (int b = b0; b < P.maxDepth; ++b) {
+        if (b > b0) atomicAdd(P.rayCount + b, 1);
+        const float4 o = P.o[idx];
+        const float4 d = P.d[idx];
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+        float t = 0.0f, u = 0.0f, v = 0.0f;
+        const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
+        P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
+        if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + b] = tri;
+        const bool alive = shadePath(s, P, f, b, idx, false);
+        uint32_t mask = P.shMask[idx];
+        if (mask) {
+            atomicAdd(P.shadowCount + b, __popc(mask));
+            const float4 so = P.shOrigin[idx];
+            const size_t base = static_cast<size_t>(idx) * P.slots;
+            for (uint32_t m = mask; m; m &= m - 1u) {
+                const int sl = __ffs(m) - 1;
+                const float4 sd = P.shDir[base + sl];
+                const RayPre sr = rayPre(so.x, so.y, so.z, sd.x, sd.y, sd.z, s.sceneMaxAbs);
+                if (traceOccludedW<Width>(s, sr, kEps, sd.w, P.errorFlags)) mask &= ~(1u << sl);
+            }
+            P.shMask[idx] = mask;
+        }
+        if (!alive || b + 1 >= P.maxDepth) break;
     }
 }
 
@@ -512,6 +577,14 @@ void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, i
 {
     if (s.bvhWidth == 8) kConnectWide<<<grid, block, 0, st>>>(s, P, bounce);
     else kConnect<2><<<grid, block, 0, st>>>(s, P, bounce);
+}
+void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cudaStream_t st)
+{
+    if (P.tailPaths <= 0) return;
+    const int n = P.tailPaths < P.count ? P.tailPaths : P.count;
+    const int blocks = (n + 127) / 128;
+    if (s.bvhWidth == 8) kTail<8><<<blocks, 128, 0, st>>>(s, P, f);
+    else kTail<2><<<blocks, 128, 0, st>>>(s, P, f);
 }
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    float* aovAccum, cudaStream_t st)

@@ -92,6 +92,7 @@ struct Renderer {
     int bvhWidth = 8;         // tree built by the next bte_init_accel
     int postponePct = 20;     // 8-wide walk: leaf-test postponing threshold
     int sortShading = 1;      // material-sorted shading (shade 5.9 -> 2.6 ms per frame on the 1080p bench scene)
+    int tailPaths = 0;        // bounce queues shorter than this finish in the tail kernel
     int builtWidth = 2;       // tree in use
     int accelNodes = 0, accelDepth = 0;
     int shadeMinBlocks = 3;   // autotuned on B200: 3 resident shade blocks per SM
@@ -345,6 +346,10 @@ void renderFrame(int w, int h)
     P.errorFlags = g.errorFlags.as<unsigned int>();
     P.sortQueue = g.sortShading ? g.sortQueue.as<int>() : nullptr;
     P.sortCount = g.sortCount.as<int>();
+    // Megakernel mode (optix_programs.cu:54-108, RenderMode::Megakernel): one thread runs each path from
+    // generation to termination in a single kernel (the tail kernel from bounce 0), with the same per-path
+    // sample streams, so its images equal the wavefront's bit for bit -- a cross-check of the stage kernels.
+    P.tailPaths = g.renderMode == BTE_RENDER_MEGAKERNEL ? 0x7fffffff : g.tailPaths;
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
     f.width = w; f.height = h; f.spp = spp;
@@ -375,9 +380,10 @@ void renderFrame(int w, int h)
             launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
             launchConnect(s, P, b, g.gridConnect, block, st);
         }
+        launchTail(s, P, f, st);
         launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st);
     };
-    float stage[5] = {0, 0, 0, 0, 0};
+    float stage[6] = {0, 0, 0, 0, 0, 0};
     if (g.cfg.useGraph && !g.stageTiming) {
         // One graph per launch configuration: every kernel argument is part of the key, so a change of
         // scene, buffers, image size, depth or tuning re-captures; the frame index travels through memory.
@@ -432,6 +438,7 @@ void renderFrame(int w, int h)
             timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st); });
             timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
         }
+        timed(5, [&] { launchTail(s, P, f, st); });
         timed(4, [&] { launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st); });
     }
     ck(cudaGetLastError(), "kernel launch");
@@ -452,6 +459,17 @@ void renderFrame(int w, int h)
     }
     ck(cudaEventElapsedTime(&S.msTotal, g.ev0, g.ev1), "cudaEventElapsedTime");
     S.msGenerate = stage[0]; S.msExtend = stage[1]; S.msShade = stage[2]; S.msConnect = stage[3]; S.msPresent = stage[4];
+    S.msTail = stage[5];
+    S.tailBounce = -1;
+    if (P.tailPaths > 0) {
+        for (int b = 0; b < depth; ++b)
+            if (rc[static_cast<size_t>(b)] < P.tailPaths) { S.tailBounce = b; break; }
+        if (S.tailBounce >= 0)
+            for (int b = S.tailBounce; b < depth; ++b) {
+                S.tailExtends += rc[static_cast<size_t>(b)];
+                S.tailShadowRays += sc[static_cast<size_t>(b)];
+            }
+    }
     if (g.denoiser && !(errFlags & 3u)) {
         const size_t bytes = static_cast<size_t>(w) * h * 12;
         if (g.denoised.bytes != bytes) { g.denoised.release(); ensure(g.denoised, bytes); }
@@ -877,11 +895,13 @@ int bte_set_tuning(const BteTuning* t)
         if (t->shadeMinBlocks != 2 && t->shadeMinBlocks != 3) throw CudaError{"bte_set_tuning: shadeMinBlocks must be 2 or 3"};
         if (t->postponePercent < 0 || t->postponePercent > 100) throw CudaError{"bte_set_tuning: postponePercent in [0, 100]"};
         if (t->sortShading != 0 && t->sortShading != 1) throw CudaError{"bte_set_tuning: sortShading must be 0 or 1"};
+        if (t->tailPaths < 0) throw CudaError{"bte_set_tuning: tailPaths must be >= 0"};
         g.bvhWidth = t->bvhWidth;
         g.maxLeaf = t->maxLeafTriangles;
         g.shadeMinBlocks = t->shadeMinBlocks;
         g.postponePct = t->postponePercent;
         g.sortShading = t->sortShading;
+        g.tailPaths = t->tailPaths;
         g.gridBlock = 0;   // recompute persistent grids
         return 0;
     });
@@ -896,6 +916,7 @@ int bte_get_tuning(BteTuning* t)
         t->shadeMinBlocks = g.shadeMinBlocks;
         t->postponePercent = g.postponePct;
         t->sortShading = g.sortShading;
+        t->tailPaths = g.tailPaths;
         return 0;
     });
 }

@@ -121,6 +121,7 @@ struct DevPaths {
     // consumes the buckets in order, so that a warp runs one BSDF's code
     int* sortQueue;   // [kSortKeys * count] or null (sorting off)
     int* sortCount;   // [(maxDepth + 1) * kSortKeys]
+    int tailPaths;    // a bounce queue shorter than this is finished by kTail (0: wavefront to the end)
     unsigned int* errorFlags;   // bit 0: traversal stack overflow; bit 1: malformed tree (index out of range)
 };
 

@@ -61,6 +61,10 @@ typedef struct {
     int maxBounceReached;  /* deepest bounce with a non-empty queue */
     float msTotal;         /* device time of the last frame (CUDA events) */
     float msGenerate, msExtend, msShade, msConnect, msPresent;  /* per stage (only with timing enabled) */
+    float msTail;          /* the tail kernel (BteTuning.tailPaths), timing enabled */
+    int tailBounce;        /* first bounce finished by the tail kernel, or -1 */
+    int64_t tailExtends;   /* closest-hit rays traced by the tail kernel (included in extends) */
+    int64_t tailShadowRays;/* shadow rays traced by the tail kernel (included in shadowRays) */
 } BteFrameStats;
 
 const char* bte_last_error(void);
@@ -121,6 +125,9 @@ typedef struct {
                             * percentage of the warp's lanes have leaf tests (0 = never, 0-100) */
     int sortShading;       /* 1: extend buckets paths by hit material (miss, BSDF type) and shade runs the
                             * buckets in order; 0: shade runs the extend queue as it is */
+    int tailPaths;         /* from the first bounce whose queue is shorter than this, one thread per path
+                            * finishes the path (extend + shade + shadow rays per bounce) in one kernel;
+                            * 0: the wavefront runs every bounce */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);

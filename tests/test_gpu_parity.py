@@ -49,9 +49,9 @@ def test_math_functions_bitexact(renderer, oracle_mod):
         assert len(bad) == 0, f"fn {fn}: {len(bad)} mismatches"
 
 
-def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0):
+def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0):
     renderer.cleanup()
-    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading)
+    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
@@ -89,8 +89,8 @@ def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, t
     assert np.array_equal(go, oo)
 
 
-def _render_and_compare(renderer, oracle_mod, scene, env_mode, spp, depth, frames=1, sort_shading=0):
-    _upload(renderer, scene, env_mode=env_mode, spp=spp, depth=depth, sort_shading=sort_shading)
+def _render_and_compare(renderer, oracle_mod, scene, env_mode, spp, depth, frames=1, sort_shading=0, tail_paths=0):
+    _upload(renderer, scene, env_mode=env_mode, spp=spp, depth=depth, sort_shading=sort_shading, tail_paths=tail_paths)
     renderer.set_hit_log(True)
     W, H = scene.width, scene.height
     renderer.reset_accumulation(W, H)
@@ -146,11 +146,13 @@ def test_cornell_frame_bitexact(renderer, oracle_mod, cornell_scene):
     assert np.isfinite(o).all() and o.mean() > 0.05
 
 
-@pytest.mark.parametrize("sort_shading", [0, 1])
+@pytest.mark.parametrize("sort_shading,tail_paths", [(0, 0), (1, 0), (1, 4000), (0, 1 << 30)])
 @pytest.mark.parametrize("env_mode", [0, 1])
-def test_random_scene_bitexact(renderer, oracle_mod, random_scene, env_mode, sort_shading):
-    """All five BSDFs, area light, spotlight and env map; with and without material-sorted shading."""
-    _render_and_compare(renderer, oracle_mod, random_scene, env_mode=env_mode, spp=3, depth=12, sort_shading=sort_shading)
+def test_random_scene_bitexact(renderer, oracle_mod, random_scene, env_mode, sort_shading, tail_paths):
+    """All five BSDFs, area light, spotlight and env map; with and without material-sorted shading, and
+    with the tail kernel taking over from a middle bounce or (threshold above the path count) from bounce 0."""
+    _render_and_compare(renderer, oracle_mod, random_scene, env_mode=env_mode, spp=3, depth=12, sort_shading=sort_shading,
+                        tail_paths=tail_paths)
 
 
 def test_random_scene_vs_reference_headers(renderer, oracle_mod, random_scene):
@@ -250,14 +252,16 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode,bvh_width,sort_shading", [(1, 8, 0), (0, 8, 0), (1, 2, 0), (1, 8, 1)])
-def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading):
+@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths",
+                         [(1, 8, 0, 0), (0, 8, 0, 0), (1, 2, 0, 0), (1, 8, 1, 0), (1, 8, 1, 200000)])
+def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading, tail_paths):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
     pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
-    _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading)
+    _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading,
+            tail_paths=tail_paths)
     info = renderer.accel_info()
     print("accel", info)
     assert info["width"] == bvh_width
@@ -315,10 +319,11 @@ def test_textured_materials_bitexact(renderer, oracle_mod, random_scene):
 def test_tuning_roundtrip_and_validation(renderer):
     """bte_set_tuning / bte_get_tuning: values round-trip; out-of-range values are rejected with a message."""
     import bluetruthengine_b200 as B
-    renderer.set_tuning(2, 2, 8, 35, 1)
+    renderer.set_tuning(2, 2, 8, 35, 1, 4096)
     assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
-                                 "sortShading": 1}
-    for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2)]:
+                                 "sortShading": 1, "tailPaths": 4096}
+    for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2),
+                (1, 3, 8, 20, 1, -1)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
@@ -379,3 +384,24 @@ def test_aov_features(renderer, random_scene):
     ln = np.linalg.norm(nrm, axis=1)
     assert np.all(np.abs(ln[hits >= 0] - 1.0) < 1e-5) and np.all(ln[hits < 0] == 0.0)
     assert (hits >= 0).mean() > 0.3
+
+
+def test_megakernel_mode_matches_wavefront(renderer, random_scene):
+    """RenderMode::Megakernel runs each path start to end in one kernel; per-sample radiance, hit counts and
+    the accumulation equal the wavefront's bit for bit."""
+    sc = random_scene
+    W, H = sc.width, sc.height
+    out = {}
+    for mode in (1, 0):   # BTE_RENDER_WAVEFRONT, BTE_RENDER_MEGAKERNEL
+        _upload(renderer, sc, env_mode=1, spp=2, depth=12)
+        renderer.set_render_mode(mode)
+        renderer.reset_accumulation(W, H)
+        renderer.render(W, H)
+        st = renderer.stats()
+        out[mode] = (renderer.read_sample_radiance(W * H * 2).copy(), renderer.read_accum(W, H).copy(), st.extends,
+                     st.shadowRays, st.tailBounce)
+    renderer.set_render_mode(1)
+    assert out[0][4] == 0 and out[1][4] == -1
+    assert np.array_equal(bits(out[0][0]), bits(out[1][0]))
+    assert np.array_equal(bits(out[0][1]), bits(out[1][1]))
+    assert out[0][2:4] == out[1][2:4]
