@@ -288,7 +288,8 @@ __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int boun
 // across iterations and takes a new ray (warp-aggregated fetch from a
 // per-bounce counter) as soon as its current one ends, so that lanes do not
 // idle until the slowest ray of their warp finishes.
-__global__ void __launch_bounds__(256) kExtendWide(DevScene s, DevPaths P, int bounce)
+// 72 registers keep 7 blocks of 128 threads resident per SM (74 would allow only 6)
+__global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
     if (tailTakesOver(P, bounce)) return;
