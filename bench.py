@@ -41,6 +41,9 @@ BYTES_PER_SHADOW = 112            # 44 W + 44 R + 24 radiance RMW
 BYTES_PER_EXTEND_RAY = 64         # extend stage alone: queue 4 + ray 24 + hit 36
 BYTES_PER_SHADE_SEGMENT = 182
 BYTES_PER_CONNECT_RAY = 68        # 44 R + 24 RMW
+# DRAM bytes per frame of each stage kernel on this workload, from one ncu capture
+# (profiles/traffic_stage_kernels_disney_spheres_1080p.md; dram__bytes_read.sum + dram__bytes_write.sum)
+STAGE_DRAM_BYTES_PER_FRAME = {"extend": 758.0e6, "shade": 3845.6e6, "connect": 441.8e6}
 
 
 def parse():
@@ -346,7 +349,11 @@ def run_ours(args):
                    "d2h_bytes_per_step": W * H * 4 + (3 * (args.depth + 1) * 4)},
            "gpu_launches": launches_per_frame * args.steps,
            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                        "frac": achieved / peak, "peak_source": peak_kind,
+                        "traffic": (STAGE_DRAM_BYTES_PER_FRAME[dom] / args.depth
+                                    if dom in STAGE_DRAM_BYTES_PER_FRAME and W == 1920 and H == 1080 and args.spp == 2
+                                    and args.depth == 16 else None),
+                        "traffic_source": "profiles/traffic_stage_kernels_disney_spheres_1080p.md (ncu, per launch)",
                         "algorithmic_bytes_per_launch": bytes_dom / launches_dom,
                         "stage_ms": stages},
            "path_stats": {"extends_per_sample": s_mean, "shadow_rays_per_sample": r_mean,
