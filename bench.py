@@ -153,6 +153,51 @@ DENOISER_CONVS = [(16, 32, 0), (32, 32, 0), (32, 48, 1), (48, 48, 1), (48, 64, 2
 DENOISER_FLOP_PER_PIXEL = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in DENOISER_CONVS)
 
 
+def batched_views_leg(scene, args):
+    """Several camera views of the bench scene in one launch sequence (bte_render_views): 8 seeded views with
+    resolutions from {320x240, 640x480, 1280x720, 1920x1080} and 1, 2 or 4 samples per frame, against the
+    same views rendered one bte_render at a time."""
+    import bluetruthengine_b200 as bte
+    r = bte.Renderer()
+    base = np.asarray(scene.camera, dtype=bte.CAMERA_DTYPE).copy()
+    rng = np.random.default_rng(3)
+    sizes = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
+    views = []
+    for k in range(8):
+        w, h = sizes[rng.integers(0, 4)]
+        cam = base.copy()
+        cam["origin"] = cam["origin"] + np.float32(0.3 * k) * cam["right"]
+        cam["aspect"] = np.float32(w / h)
+        views.append((cam, w, h, int(rng.choice([1, 2, 4]))))
+    samples = sum(w * h * s for _, w, h, s in views)
+    env = bte.ENV_ALIAS if args.env == "alias" else bte.ENV_CDF
+    r.set_config(samples_per_frame=1, max_depth=args.depth, rr_start=3, env_sampling=env)
+    r.reset_views()
+    for _ in range(2):
+        r.render_views(views)
+    ms = []
+    for _ in range(5):
+        r.render_views(views)
+        ms.append(r.stats().msTotal)
+    tb = statistics.median(ms)
+    seq = 0.0
+    for cam, w, h, spp in views:
+        r.init_camera(cam)
+        r.set_config(samples_per_frame=spp, max_depth=args.depth, rr_start=3, env_sampling=env, use_graph=1)
+        r.reset_accumulation(w, h)
+        for _ in range(2):
+            r.render(w, h)
+        m = []
+        for _ in range(5):
+            r.render(w, h)
+            m.append(r.stats().msTotal)
+        seq += statistics.median(m)
+    r.reset_views()
+    return {"views": [[w, h, s] for _, w, h, s in views], "samples_per_frame": samples,
+            "batched_ms": tb, "batched_msamples_per_s": samples / tb / 1e3,
+            "one_view_at_a_time_ms": seq, "one_view_at_a_time_msamples_per_s": samples / seq / 1e3}
+
+
 def denoise_leg():
     """Second half of the metric: device time to relMSE <= 2e-3 against the FP64 16384-spp image, plain
     accumulation vs denoised low-spp, on the Cornell box (256x256, depth 8); plus the denoiser's inference
@@ -366,6 +411,11 @@ def run_ours(args):
             out["cpu_baseline"] = cpu_baseline(scene, args, seconds=args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never the product
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0 and world == 1:
+        try:
+            out["batched_views"] = batched_views_leg(scene, args)
+        except Exception as e:
+            out["batched_views"] = {"unavailable": str(e)}
     if rank == 0 and not args.no_denoise:
         try:
             out["denoise"] = denoise_leg()

@@ -40,6 +40,7 @@ SPOT_DTYPE = np.dtype([("position", "<f4", 3), ("direction", "<f4", 3), ("radian
 CAMERA_DTYPE = np.dtype([("origin", "<f4", 3), ("forward", "<f4", 3), ("right", "<f4", 3), ("up", "<f4", 3),
                          ("fovYRadians", "<f4"), ("aspect", "<f4")])
 assert TRIANGLE_DTYPE.itemsize == 96 and BSDF_DTYPE.itemsize == 68 and CAMERA_DTYPE.itemsize == 56
+VIEW_DTYPE = np.dtype([("camera", CAMERA_DTYPE), ("width", "<i4"), ("height", "<i4"), ("samplesPerFrame", "<i4")])
 
 
 class Tuning(C.Structure):
@@ -311,6 +312,25 @@ class Renderer:
         out = np.empty((height, width, 3), dtype=np.float32)
         _check(self.lib.bte_read_denoised(out.ctypes.data_as(C.c_void_p)))
         return out
+
+    def render_views(self, views):
+        """One frame of several camera views (sequence of (camera, width, height, samples_per_frame)) in one launch
+        sequence; view slot i accumulates across calls."""
+        arr = np.zeros(len(views), dtype=VIEW_DTYPE)
+        for i, (cam, w, h, spp) in enumerate(views):
+            arr[i]["camera"] = np.asarray(cam, dtype=CAMERA_DTYPE)
+            arr[i]["width"], arr[i]["height"], arr[i]["samplesPerFrame"] = w, h, spp
+        _check(self.lib.bte_render_views(_ptr(arr), len(views)))
+
+    def read_view_accum(self, view: int, width: int, height: int):
+        """(FP32 running mean [W*H, 3], FP64 running sum [W*H, 3]) of a batched view."""
+        mean = np.empty((width * height, 3), dtype=np.float32)
+        total = np.empty((width * height, 3), dtype=np.float64)
+        _check(self.lib.bte_read_view_accum(int(view), _ptr(mean), _ptr(total)))
+        return mean, total
+
+    def reset_views(self):
+        _check(self.lib.bte_reset_views())
 
     def set_aov(self, enabled: bool):
         """Accumulate first-hit albedo and shading normal per pixel (denoiser features)."""

@@ -94,15 +94,30 @@ __global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) P.rayCount[0] = P.count;
     if (i >= P.count) return;
-    const int wh = f.width * f.height;
-    const int pix = i % wh;
-    const int s = i / wh;
-    const int px = pix % f.width, py = pix / f.width;
-    uint32_t rng = rngSeed(static_cast<uint32_t>(pix), *f.frameIndex + static_cast<uint32_t>(s));
+    int width = f.width, height = f.height, local = i;
+    uint32_t frameIndex;
+    const CameraData* cam = &f.cam;
+    float tanHalf = f.tanHalf;
+    if (f.viewCount > 0) {   // batched views: find the view holding path i
+        int v = 0;
+        while (v + 1 < f.viewCount && i >= f.views[v + 1].pathOffset) ++v;
+        const ViewDesc& vd = f.views[v];
+        width = vd.width; height = vd.height; local = i - vd.pathOffset;
+        frameIndex = vd.frameIndex;
+        cam = &vd.cam;
+        tanHalf = vd.tanHalf;
+    } else {
+        frameIndex = *f.frameIndex;
+    }
+    const int wh = width * height;
+    const int pix = local % wh;
+    const int s = local / wh;
+    const int px = pix % width, py = pix / width;
+    uint32_t rng = rngSeed(static_cast<uint32_t>(pix), frameIndex + static_cast<uint32_t>(s));
     const float jx = rngNext(rng) - 0.5f;
     const float jy = rngNext(rng) - 0.5f;
     V3 o, d;
-    primaryRay(px, py, f.width, f.height, f.cam, f.tanHalf, jx, jy, o, d);
+    primaryRay(px, py, width, height, *cam, tanHalf, jx, jy, o, d);
     P.o[i] = make_float4(o.x, o.y, o.z, __uint_as_float(rng));
     P.d[i] = make_float4(d.x, d.y, d.z, 1.0f);
     P.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -444,6 +459,36 @@ __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float
     if (extFramebuffer) extFramebuffer[pix] = px;
 }
 
+// present for batched views: one thread per pixel of the frame's pixel space
+__global__ void __launch_bounds__(256) kPresentViews(DevPaths P, FrameParams f, int totalPixels)
+{
+    const int gpix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gpix >= totalPixels) return;
+    int v = 0;
+    while (v + 1 < f.viewCount && gpix >= f.views[v + 1].pixelOffset) ++v;
+    const ViewDesc& vd = f.views[v];
+    const int pix = gpix - vd.pixelOffset;
+    const int wh = vd.width * vd.height;
+    float ax = vd.accum[3 * pix], ay = vd.accum[3 * pix + 1], az = vd.accum[3 * pix + 2];
+    double sx = vd.accumD[3 * pix], sy = vd.accumD[3 * pix + 1], sz = vd.accumD[3 * pix + 2];
+    for (int s = 0; s < vd.spp; ++s) {
+        const int idx = vd.pathOffset + s * wh + pix;
+        const float4 L4 = P.L[idx];
+        V3 L = resolveShadows(P, idx, v3(L4.x, L4.y, L4.z));
+        P.L[idx] = make_float4(L.x, L.y, L.z, L4.w);
+        const float n = static_cast<float>(vd.frameIndex + static_cast<uint32_t>(s) + 1u);
+        ax = ax + (L.x - ax) / n;
+        ay = ay + (L.y - ay) / n;
+        az = az + (L.z - az) / n;
+        sx += static_cast<double>(L.x);
+        sy += static_cast<double>(L.y);
+        sz += static_cast<double>(L.z);
+    }
+    vd.accum[3 * pix] = ax; vd.accum[3 * pix + 1] = ay; vd.accum[3 * pix + 2] = az;
+    vd.accumD[3 * pix] = sx; vd.accumD[3 * pix + 1] = sy; vd.accumD[3 * pix + 2] = sz;
+    vd.framebuffer[pix] = packGamma(ax, ay, az);
+}
+
 // ---------------------------------------------------------------- debug / parity kernels
 template <int Width>
 __global__ void kTraceClosestRays(DevScene s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err)
@@ -578,6 +623,10 @@ void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, i
 {
     if (s.bvhWidth == 8) kConnectWide<<<grid, block, 0, st>>>(s, P, bounce);
     else kConnect<2><<<grid, block, 0, st>>>(s, P, bounce);
+}
+void launchPresentViews(const DevPaths& P, const FrameParams& f, int totalPixels, cudaStream_t st)
+{
+    kPresentViews<<<(totalPixels + 255) / 256, 256, 0, st>>>(P, f, totalPixels);
 }
 void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cudaStream_t st)
 {

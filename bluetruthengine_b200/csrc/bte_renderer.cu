@@ -115,6 +115,14 @@ struct Renderer {
     bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
     DeviceBuffer aovAlbedo, aovNormal, aovAccum;
     DeviceBuffer denoised;            // [W*H*3] denoised mean radiance of the last frame (denoiser on)
+    // batched views (bte_render_views): accumulation per view slot
+    struct ViewState {
+        int w = 0, h = 0;
+        uint32_t frameIndex = 0;
+        DeviceBuffer accum, accumD, fb;
+    };
+    std::vector<ViewState> views;
+    DeviceBuffer viewTable;
     bool stageTiming = false;
     int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
     BteFrameStats stats{};
@@ -130,6 +138,7 @@ struct Renderer {
 
 Renderer g;
 std::mutex g_mutex;
+constexpr int kMaxViews = 64;
 
 void ensureInit()
 {
@@ -484,6 +493,126 @@ void renderFrame(int w, int h)
     if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
 }
 
+// Several camera views of the scene in one frame: one launch sequence over the concatenated paths of all
+// views (each view's paths sample-major as in bte_render), each view accumulating into its own buffers.
+void renderViews(const BteView* views, int count)
+{
+    if (!views || count <= 0) throw CudaError{"bte_render_views: no views"};
+    if (count > kMaxViews) throw CudaError{"bte_render_views: at most 64 views per frame"};
+    if (!g.tris.p || g.triCount <= 0 || !g.accelReady || !g.bsdfs.p || !g.triBsdfIds.p || !g.emitterFlags.p)
+        throw CudaError{"bte_render_views: scene, acceleration structure, BSDFs and emitter flags must be uploaded"};
+    const int depth = g.cfg.maxDepth > 0 ? g.cfg.maxDepth : 1;
+    const int slots = slotsFor();
+    if (slots > 32) throw CudaError{"bte_render_views: at most 30 spotlights are supported"};
+    if (static_cast<int>(g.views.size()) != count) g.views.resize(static_cast<size_t>(count));
+    std::vector<ViewDesc> vd(static_cast<size_t>(count));
+    long long paths64 = 0, pixels64 = 0;
+    for (int v = 0; v < count; ++v) {
+        const BteView& in = views[v];
+        if (in.width <= 0 || in.height <= 0 || in.samplesPerFrame <= 0)
+            throw CudaError{"bte_render_views: view sizes and samplesPerFrame must be positive"};
+        Renderer::ViewState& st = g.views[static_cast<size_t>(v)];
+        const size_t n = static_cast<size_t>(in.width) * in.height;
+        if (st.w != in.width || st.h != in.height || !st.accum.p) {   // new or resized view: fresh accumulation
+            st.accum.release(); st.accumD.release(); st.fb.release();
+            ensure(st.accum, n * 12); ensure(st.accumD, n * 24); ensure(st.fb, n * 4);
+            ck(cudaMemsetAsync(st.accum.p, 0, n * 12, g.stream), "cudaMemsetAsync");
+            ck(cudaMemsetAsync(st.accumD.p, 0, n * 24, g.stream), "cudaMemsetAsync");
+            ck(cudaMemsetAsync(st.fb.p, 0, n * 4, g.stream), "cudaMemsetAsync");
+            st.w = in.width; st.h = in.height; st.frameIndex = 0;
+        }
+        ViewDesc& d = vd[static_cast<size_t>(v)];
+        std::memset(&d, 0, sizeof(d));
+        d.cam = in.camera;
+        d.tanHalf = m::tanf_(0.5f * in.camera.fovYRadians);
+        d.width = in.width; d.height = in.height; d.spp = in.samplesPerFrame;
+        d.frameIndex = st.frameIndex;
+        d.pathOffset = static_cast<int>(paths64);
+        d.pixelOffset = static_cast<int>(pixels64);
+        d.accum = st.accum.as<float>(); d.accumD = st.accumD.as<double>(); d.framebuffer = st.fb.as<uint32_t>();
+        paths64 += static_cast<long long>(n) * in.samplesPerFrame;
+        pixels64 += static_cast<long long>(n);
+        if (paths64 > (1LL << 30)) throw CudaError{"bte_render_views: too many paths per frame (sum W*H*spp > 2^30)"};
+    }
+    const int paths = static_cast<int>(paths64);
+    ensureWavefront(paths, slots, depth);
+    const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
+    if (g.gridBlock != block) {
+        g.gridExtend = occupancyGrid(g.builtWidth == 8 ? 4 : 0, block);
+        g.gridShade = occupancyGrid(g.shadeMinBlocks == 3 ? 3 : 1, block);
+        g.gridConnect = occupancyGrid(g.builtWidth == 8 ? 5 : 2, block);
+        g.gridBlock = block;
+    }
+    ensure(g.viewTable, sizeof(ViewDesc) * kMaxViews);
+    ck(cudaMemcpyAsync(g.viewTable.p, vd.data(), sizeof(ViewDesc) * count, cudaMemcpyHostToDevice, g.stream),
+       "cudaMemcpyAsync");
+    DevPaths P;
+    std::memset(&P, 0, sizeof(P));
+    P.o = g.pO.as<float4>(); P.d = g.pD.as<float4>(); P.tp = g.pTp.as<float4>(); P.L = g.pL.as<float4>();
+    P.hit = g.pHit.as<float4>();
+    P.queue[0] = g.q0.as<int>(); P.queue[1] = g.q1.as<int>();
+    P.rayCount = g.rayCount.as<int>();
+    P.shadowCount = g.shadowCount.as<int>();
+    P.fetch = g.fetch.as<int>();
+    P.shadowQueue = g.shadowQueue.as<int>();
+    P.shOrigin = g.shOrigin.as<float4>();
+    P.shDir = g.shDir.as<float4>();
+    P.shContrib = g.shContrib.as<float4>();
+    P.shMask = g.shMask.as<uint32_t>();
+    P.slots = slots;
+    P.maxDepth = depth;
+    P.count = paths;
+    P.errorFlags = g.errorFlags.as<unsigned int>();
+    P.sortQueue = g.sortShading ? g.sortQueue.as<int>() : nullptr;
+    P.sortCount = g.sortCount.as<int>();
+    P.tailPaths = g.renderMode == BTE_RENDER_MEGAKERNEL ? 0x7fffffff : g.tailPaths;
+    FrameParams f;
+    std::memset(&f, 0, sizeof(f));
+    f.frameIndex = g.dFrameIndex.as<uint32_t>();
+    f.rrStart = g.cfg.rrStart;
+    f.views = g.viewTable.as<ViewDesc>();
+    f.viewCount = count;
+    const DevScene s = makeDevScene();
+    cudaStream_t st = g.stream;
+    ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+    ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+    launchGenerate(P, f, st);
+    for (int b = 0; b < depth; ++b) {
+        launchExtend(s, P, b, g.gridExtend, block, st);
+        launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
+        launchConnect(s, P, b, g.gridConnect, block, st);
+    }
+    launchTail(s, P, f, st);
+    launchPresentViews(P, f, static_cast<int>(pixels64), st);
+    ck(cudaGetLastError(), "kernel launch");
+    ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
+    std::vector<int> rc(static_cast<size_t>(depth + 1)), sc(static_cast<size_t>(depth + 1));
+    unsigned int errFlags = 0;
+    ck(cudaMemcpyAsync(rc.data(), g.rayCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    ck(cudaMemcpyAsync(sc.data(), g.shadowCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    ck(cudaMemcpyAsync(&errFlags, g.errorFlags.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    ck(cudaStreamSynchronize(st), "frame");
+    BteFrameStats& S = g.stats;
+    S = BteFrameStats{};
+    S.samples = paths;
+    S.tailBounce = -1;
+    for (int b = 0; b < depth; ++b) {
+        S.extends += rc[static_cast<size_t>(b)];
+        S.shadowRays += sc[static_cast<size_t>(b)];
+        if (rc[static_cast<size_t>(b)] > 0) S.maxBounceReached = b;
+    }
+    ck(cudaEventElapsedTime(&S.msTotal, g.ev0, g.ev1), "cudaEventElapsedTime");
+    for (int v = 0; v < count; ++v)
+        g.views[static_cast<size_t>(v)].frameIndex += static_cast<uint32_t>(views[v].samplesPerFrame);
+    g.lastPaths = 0;   // per-path debug readbacks refer to single-view frames
+    if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
+    if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+}
+
 template <typename F>
 int guarded(F&& fn)
 {
@@ -788,6 +917,38 @@ int bte_render(int imageWidth, int imageHeight)
 // it on needs denoiser weights (bte_denoiser_set_params / bte_denoiser_init)
 // and switches the first-hit features on; each frame then presents the
 // denoised accumulation.  Plain accumulation stays the buffer of record.
+int bte_render_views(const BteView* views, int count)
+{
+    return guarded([&] {
+        renderViews(views, count);
+        return 0;
+    });
+}
+
+int bte_read_view_accum(int view, float* hostRGB, double* hostRGBSum)
+{
+    return guarded([&] {
+        if (view < 0 || view >= static_cast<int>(g.views.size()) || !g.views[static_cast<size_t>(view)].accum.p)
+            throw CudaError{"bte_read_view_accum: no such view (bte_render_views)"};
+        const Renderer::ViewState& v = g.views[static_cast<size_t>(view)];
+        if (hostRGB)
+            ck(cudaMemcpyAsync(hostRGB, v.accum.p, v.accum.bytes, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+        if (hostRGBSum)
+            ck(cudaMemcpyAsync(hostRGBSum, v.accumD.p, v.accumD.bytes, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(g.stream), "sync");
+        return 0;
+    });
+}
+
+int bte_reset_views(void)
+{
+    return guarded([&] {
+        for (auto& v : g.views) { v.accum.release(); v.accumD.release(); v.fb.release(); }
+        g.views.clear();
+        return 0;
+    });
+}
+
 int bte_toggle_denoiser(void)
 {
     return guarded([&]() -> int {

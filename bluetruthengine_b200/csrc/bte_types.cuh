@@ -125,6 +125,21 @@ struct DevPaths {
     unsigned int* errorFlags;   // bit 0: traversal stack overflow; bit 1: malformed tree (index out of range)
 };
 
+// One camera view of a batched frame (bte_render_views): its paths are
+// [pathOffset, pathOffset + width*height*spp) of the frame, sample-major as
+// in a single-view frame, and its pixels [pixelOffset, + width*height) of
+// the frame's pixel space.
+struct ViewDesc {
+    CameraData cam;
+    float tanHalf;
+    int width, height, spp;
+    uint32_t frameIndex;          // samples of this view accumulated before this frame
+    int pathOffset, pixelOffset;
+    float* accum;                 // [W*H*3] FP32 running mean
+    double* accumD;               // [W*H*3] FP64 running sum
+    uint32_t* framebuffer;        // [W*H] packed RGBA8
+};
+
 struct FrameParams {
     int width, height, spp;
     const uint32_t* frameIndex;   // device word: samples accumulated before this frame (read by the kernels,
@@ -132,6 +147,8 @@ struct FrameParams {
     int rrStart;
     float tanHalf;
     CameraData cam;
+    const ViewDesc* views;        // batched views (viewCount > 0) instead of the single camera above
+    int viewCount;
 };
 
 }  // namespace bte

@@ -91,6 +91,18 @@ int bte_init_env_map(const float* rgba, int width, int height, float intensity, 
 int bte_set_output_buffer(uint32_t* deviceRGBA8);   /* replaces cudaRegisterPBO :177 (no GL on the box) */
 int bte_reset_accumulation(int imageWidth, int imageHeight);                    /* :183 */
 int bte_render(int imageWidth, int imageHeight);                                /* :187 */
+/* Batched views (no reference counterpart; the reference renders one camera per cudaRender): several
+ * camera views of the current scene, each of its own size and samples per frame, rendered in one launch
+ * sequence over their concatenated paths.  View slot i keeps its own accumulation across calls (a changed
+ * size restarts it); the per-view images equal those of bte_render with that camera, bit for bit. */
+typedef struct {
+    CameraData camera;
+    int width, height;
+    int samplesPerFrame;
+} BteView;
+int bte_render_views(const BteView* views, int count);            /* at most 64 views */
+int bte_read_view_accum(int view, float* hostRGB, double* hostRGBSum);   /* W*H*3 each; either may be NULL */
+int bte_reset_views(void);
 int bte_toggle_denoiser(void);                      /* :192; returns new state (0/1) or <0; needs denoiser weights */
 int bte_read_denoised(float* hostRGB);               /* W*H*3 denoised mean radiance of the last frame (denoiser on) */
 int bte_set_render_mode(int mode);                                              /* :205 */
