@@ -483,7 +483,9 @@ __global__ void kWideEmit(const int2* __restrict__ items, int m, const int* __re
     nd.triBase = triCursor + scanT[i];
     uint32_t imask = 0;
     uint32_t meta[2] = {0u, 0u};
-    uint32_t q[6][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}};
+    // empty slots keep lo = 255, hi = 0 on every axis: a box inverted by the parent's whole extent, which the
+    // traversal's near/far-plane test rejects without a separate validity check
+    uint32_t q[6][2] = {{~0u, ~0u}, {~0u, ~0u}, {~0u, ~0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}};
     int r = 0, toff = 0;
     for (int sl = 0; sl < 8; ++sl) {
         const int j = childAt[sl];
@@ -491,7 +493,7 @@ __global__ void kWideEmit(const int2* __restrict__ items, int m, const int* __re
         const int c = C[j];
         const int word = sl >> 2, sh = 8 * (sl & 3);
         for (int a = 0; a < 3; ++a) {
-            q[a][word] |= quantLo(bx[j][a], lo[a], e[a]) << sh;
+            q[a][word] = (q[a][word] & ~(0xffu << sh)) | (quantLo(bx[j][a], lo[a], e[a]) << sh);
             q[3 + a][word] |= quantHi(bx[j][3 + a], lo[a], e[a]) << sh;
         }
         const int cnt = subtreeCount(range, c);

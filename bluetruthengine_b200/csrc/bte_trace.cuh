@@ -296,14 +296,12 @@ struct WideWalk {
             const uint32_t nz[2] = {__float_as_uint(szn ? f4.z : f3.x), __float_as_uint(szn ? f4.w : f3.y)};
             const uint32_t fz[2] = {__float_as_uint(szn ? f3.x : f4.z), __float_as_uint(szn ? f3.y : f4.w)};
             const float cull = AnyHit ? tmax * kCullMargin : bt * kCullMargin;
-            uint32_t newHits = 0, triMask = 0;
+            uint32_t hitBits = 0;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int w = c >> 2;
                 const uint32_t sel = static_cast<uint32_t>(c & 3) | 0x7440u;   // byte c, two zero bytes, 0x4b
-                const uint32_t mb = (meta[w] >> (8 * (c & 3))) & 0xffu;
-                const bool inner = (imask >> c) & 1u;
-                if (!inner && mb == 0u) continue;
+                // (empty slots are inverted boxes; one that still passes has no triangles and no child)
                 const float tnx = __fmaf_rn(byteToFloat(nx[w], sel), ax, cnx);
                 const float tfx = __fmaf_rn(byteToFloat(fx[w], sel), ax, cfx);
                 const float tny = __fmaf_rn(byteToFloat(ny[w], sel), ay, cny);
@@ -312,10 +310,19 @@ struct WideWalk {
                 const float tfz = __fmaf_rn(byteToFloat(fz[w], sel), az, cfz);
                 const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
                 const float tf = fminf(fminf(tfx, tfy), fminf(tfz, cull)) * kBoxGrow;
-                if (tn <= tf) {
-                    if (inner) newHits |= 1u << (static_cast<uint32_t>(c) ^ oct);
-                    else triMask |= ((1u << (mb >> 5)) - 1u) << (mb & 31u);
-                }
+                hitBits |= (tn <= tf ? 1u : 0u) << c;
+            }
+            // internal children that were hit, re-keyed to slot ^ octant (bit c -> bit c ^ oct)
+            uint32_t newHits = hitBits & imask;
+            if (oct & 1u) newHits = ((newHits & 0x55u) << 1) | ((newHits >> 1) & 0x55u);
+            if (oct & 2u) newHits = ((newHits & 0x33u) << 2) | ((newHits >> 2) & 0x33u);
+            if (oct & 4u) newHits = ((newHits & 0x0fu) << 4) | ((newHits >> 4) & 0x0fu);
+            // triangles of the leaf slots that were hit
+            uint32_t triMask = 0;
+            for (uint32_t lh = hitBits & ~imask; lh; lh &= lh - 1u) {
+                const int c = __ffs(lh) - 1;
+                const uint32_t mb = (((c & 4) ? meta[1] : meta[0]) >> (8 * (c & 3))) & 0xffu;
+                triMask |= ((1u << (mb >> 5)) - 1u) << (mb & 31u);
             }
             nBase = static_cast<uint32_t>(__float_as_int(f1.x));
             nBits = (newHits << 8) | imask;
