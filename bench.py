@@ -49,7 +49,7 @@ STAGE_DRAM_BYTES_PER_FRAME = {"extend": 758.0e6, "shade": 3845.6e6, "connect": 4
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--spp", type=int, default=2, help="paths per pixel per step")
@@ -92,7 +92,7 @@ class Clocks:
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -261,7 +261,7 @@ class ReferenceCpu:
         """One bounded sample of ~`seconds` of CPU work; returns a cpu_baseline record."""
         if self.rate is None:
             self.run(4096)
-        n = int(min(max(self.rate * seconds, 4096), self.scene.width * self.scene.height * 4))
+        n = int(min(max(self.rate * seconds, 4096), self.scene.width * self.scene.height * 32))
         n, dt, ext, sh = self.run(n)
         return {"value": n / dt / 1e6, "unit": "Msamples/s", "cores": self.cores, "kind": "reference",
                 "sample": "%d random pixels x 1 spp of the same %dx%d view, depth %d, CDF env sampling "

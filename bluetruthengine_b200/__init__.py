@@ -343,7 +343,7 @@ class Renderer:
         return out[..., :3].copy(), out[..., 3:].copy()
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
-                   postpone_percent: int = 20, sort_shading: int = 1, tail_paths: int = 0):
+                   postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 0):
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),
                    int(tail_paths))
         _check(self.lib.bte_set_tuning(C.byref(t)))

@@ -225,6 +225,20 @@ BTE_DI float wideScale(uint32_t e) { return __uint_as_float(e << 23); }
 // byte (selected by `sel` from x) as a float: 0x4b0000qq is 2^23 + q exactly
 constexpr uint32_t kTriGroup = 0x80000000u;   // stack entry holds (triBase, leaf-test mask)
 
+// three-input max / min (one instruction on sm_100); NaN operands are ignored, as by fmaxf / fminf chains
+BTE_DI float max3f(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+BTE_DI float min3f(float a, float b, float c)
+{
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 BTE_DI float byteToFloat(uint32_t x, uint32_t sel)
 {
     return __uint_as_float(__byte_perm(x, 0x4b000000u, sel)) - 8388608.0f;
@@ -308,8 +322,8 @@ struct WideWalk {
                 const float tfy = __fmaf_rn(byteToFloat(fy[w], sel), ay, cfy);
                 const float tnz = __fmaf_rn(byteToFloat(nz[w], sel), az, cnz);
                 const float tfz = __fmaf_rn(byteToFloat(fz[w], sel), az, cfz);
-                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, cull)) * kBoxGrow;
+                const float tn = max3f(tnx, tny, fmaxf(tnz, tmin));
+                const float tf = min3f(tfx, tfy, fminf(tfz, cull)) * kBoxGrow;
                 hitBits |= (tn <= tf ? 1u : 0u) << c;
             }
             // internal children that were hit, re-keyed to slot ^ octant (bit c -> bit c ^ oct)
