@@ -46,7 +46,8 @@ VIEW_DTYPE = np.dtype([("camera", CAMERA_DTYPE), ("width", "<i4"), ("height", "<
 class Tuning(C.Structure):
     """BteTuning (include/bte/render_api.h)."""
     _fields_ = [("bvhWidth", C.c_int), ("maxLeafTriangles", C.c_int), ("shadeMinBlocks", C.c_int),
-                ("postponePercent", C.c_int), ("sortShading", C.c_int), ("tailPaths", C.c_int)]
+                ("postponePercent", C.c_int), ("sortShading", C.c_int), ("tailPaths", C.c_int),
+                ("bvhBuilder", C.c_int), ("plocRadius", C.c_int), ("overlapConnect", C.c_int)]
 
 
 class RenderConfig(C.Structure):
@@ -343,9 +344,11 @@ class Renderer:
         return out[..., :3].copy(), out[..., 3:].copy()
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
-                   postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 0):
+                   postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 0, bvh_builder: int = 1,
+                   ploc_radius: int = 8, overlap_connect: int = 1):
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),
-                   int(tail_paths))
+                   int(tail_paths), int(bvh_builder), int(ploc_radius),
+                   int(overlap_connect))
         _check(self.lib.bte_set_tuning(C.byref(t)))
 
     def tuning(self) -> dict:
@@ -356,7 +359,9 @@ class Renderer:
     def accel_info(self) -> dict:
         w, n, d, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
         _check(self.lib.bte_get_accel_info(C.byref(w), C.byref(n), C.byref(d), C.byref(ms)))
-        return {"width": w.value, "nodes": n.value, "depth": d.value, "ms_build": ms.value}
+        b = C.c_int()
+        _check(self.lib.bte_get_accel_builder(C.byref(b)))
+        return {"width": w.value, "nodes": n.value, "depth": d.value, "ms_build": ms.value, "builder": b.value}
 
     def set_hit_log(self, on: bool):
         _check(self.lib.bte_set_hit_log(1 if on else 0))

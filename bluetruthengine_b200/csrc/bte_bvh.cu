@@ -331,6 +331,241 @@ __global__ void kEmitNodes(const int2* __restrict__ children, const float* __res
     nodes[i] = nd;
 }
 
+// ---------------------------------------------------------------- PLOC
+// Parallel locally-ordered clustering (D. Meister, J. Bittner, "Parallel
+// Locally-Ordered Clustering for Bounding Volume Hierarchy Construction",
+// IEEE TVCG 24(3), 2018), the alternative to the Morton-prefix hierarchy.
+// Clusters start as the triangles in Morton order.  Each round every cluster
+// picks, among the clusters at most `radius` positions away, the one whose
+// union box has the smallest surface area, ties going to the lower position.
+// That makes the choice the minimum of a strict total order over pairs
+// (area, lower position, higher position), so the best pair of the round is
+// always mutual and every round merges.  Mutual pairs merge into a new inner
+// node at the lower position; survivors are compacted in order.  Inner node
+// ids are handed out downwards from n-2, so the last merge is the root 0.
+// The tree is then relabelled in depth-first order (subtree triangle counts,
+// first-leaf offsets) so that every subtree is a contiguous range of leaves,
+// which is what the refit, the leaf collapse and the 8-wide collapse expect.
+constexpr int kPlocBlock = 256;
+constexpr int kPlocItems = 4;
+constexpr int kPlocTile = kPlocBlock * kPlocItems;
+
+struct Cluster {
+    float4 lo;   // box min, w: node code (>= 0 inner node, ~k Morton-order triangle k)
+    float4 hi;   // box max, w: triangles below
+};
+
+__global__ void kPlocInit(const TriangleData* __restrict__ tris, const int* __restrict__ sortedTri, int n, Cluster* c)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const Box b = triBox(tris[sortedTri[k]]);
+    c[k].lo = make_float4(b.lx, b.ly, b.lz, __int_as_float(~k));
+    c[k].hi = make_float4(b.hx, b.hy, b.hz, __int_as_float(1));
+}
+
+__device__ __forceinline__ float unionArea(const float4& alo, const float4& ahi, const float4& blo, const float4& bhi)
+{
+    const float dx = fmaxf(fmaxf(ahi.x, bhi.x) - fminf(alo.x, blo.x), 0.0f);
+    const float dy = fmaxf(fmaxf(ahi.y, bhi.y) - fminf(alo.y, blo.y), 0.0f);
+    const float dz = fmaxf(fmaxf(ahi.z, bhi.z) - fminf(alo.z, blo.z), 0.0f);
+    const float a = dx * dy + dy * dz + dz * dx;
+    return (a == a) ? a : INFINITY;   // NaN coordinates: the farthest, still ordered by position
+}
+
+// nn[i] = the chosen neighbour of cluster i (-1 only when m == 1)
+__global__ void __launch_bounds__(kPlocBlock) kPlocNearest(const Cluster* __restrict__ c, int m, int radius, int* nn)
+{
+    __shared__ float4 sLo[kPlocBlock + 2 * kPlocMaxRadius], sHi[kPlocBlock + 2 * kPlocMaxRadius];
+    const int start = blockIdx.x * kPlocBlock - radius;
+    for (int t = threadIdx.x; t < kPlocBlock + 2 * radius; t += kPlocBlock) {
+        const int j = start + t;
+        if (j >= 0 && j < m) { sLo[t] = c[j].lo; sHi[t] = c[j].hi; }
+    }
+    __syncthreads();
+    const int i = blockIdx.x * kPlocBlock + threadIdx.x;
+    if (i >= m) return;
+    const float4 alo = sLo[i - start], ahi = sHi[i - start];
+    const int jlo = max(0, i - radius), jhi = min(m - 1, i + radius);
+    float best = INFINITY;
+    int bestJ = -1;
+    for (int j = jlo; j <= jhi; ++j) {
+        if (j == i) continue;
+        const float a = unionArea(alo, ahi, sLo[j - start], sHi[j - start]);
+        if (bestJ < 0 || a < best) { best = a; bestJ = j; }   // ascending j: ties keep the lower position
+    }
+    nn[i] = bestJ;
+}
+
+// (survives, owns a merge) of cluster i
+__device__ __forceinline__ int2 plocFlags(const int* __restrict__ nn, int m, int i)
+{
+    if (i >= m) return make_int2(0, 0);
+    const int j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    return make_int2((mutual && i > j) ? 0 : 1, (mutual && i < j) ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(kPlocBlock) kPlocCount(const int* __restrict__ nn, int m, int2* tileSums)
+{
+    __shared__ int2 warpSums[kPlocBlock / 32];
+    const int base = blockIdx.x * kPlocTile;
+    int2 s = make_int2(0, 0);
+    for (int q = 0; q < kPlocItems; ++q) {
+        const int2 f = plocFlags(nn, m, base + q * kPlocBlock + threadIdx.x);
+        s.x += f.x; s.y += f.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) warpSums[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int2 t = make_int2(0, 0);
+        for (int w = 0; w < kPlocBlock / 32; ++w) { t.x += warpSums[w].x; t.y += warpSums[w].y; }
+        tileSums[blockIdx.x] = t;
+    }
+}
+
+// exclusive scan of tileSums[0..tiles) by one block of 1024 threads;
+// tileSums[tiles] = totals
+__global__ void __launch_bounds__(1024) kPlocScanTiles(int2* tileSums, int tiles)
+{
+    __shared__ int2 warpSums[32];
+    __shared__ int2 carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = make_int2(0, 0);
+    __syncthreads();
+    for (int base = 0; base < tiles; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int2 v = (i < tiles) ? tileSums[i] : make_int2(0, 0);
+        int2 x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int yx = __shfl_up_sync(0xffffffffu, x.x, o), yy = __shfl_up_sync(0xffffffffu, x.y, o);
+            if (lane >= o) { x.x += yx; x.y += yy; }
+        }
+        if (lane == 31) warpSums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int2 w = warpSums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int yx = __shfl_up_sync(0xffffffffu, w.x, o), yy = __shfl_up_sync(0xffffffffu, w.y, o);
+                if (lane >= o) { w.x += yx; w.y += yy; }
+            }
+            warpSums[lane] = w;
+        }
+        __syncthreads();
+        const int2 wp = (warp > 0) ? warpSums[warp - 1] : make_int2(0, 0);
+        const int2 incl = make_int2(x.x + wp.x, x.y + wp.y);
+        if (i < tiles) tileSums[i] = make_int2(carry.x + incl.x - v.x, carry.y + incl.y - v.y);
+        __syncthreads();
+        if (threadIdx.x == 1023) { carry.x += incl.x; carry.y += incl.y; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tileSums[tiles] = carry;
+}
+
+// Survivors to their compacted position; each mutual pair's lower member
+// becomes the new inner node `nextId - (merges before it)`.
+__global__ void __launch_bounds__(kPlocBlock) kPlocCompact(const Cluster* __restrict__ c, const int* __restrict__ nn,
+                                                           int m, const int2* __restrict__ tileScan, int nextId,
+                                                           Cluster* out, int2* children, int* counts)
+{
+    __shared__ int2 warpSums[kPlocBlock / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int first = blockIdx.x * kPlocTile + t * kPlocItems;   // thread-major: keeps positions in order
+    int2 f[kPlocItems];
+    int2 s = make_int2(0, 0);
+    for (int q = 0; q < kPlocItems; ++q) { f[q] = plocFlags(nn, m, first + q); s.x += f[q].x; s.y += f[q].y; }
+    int2 x = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int yx = __shfl_up_sync(0xffffffffu, x.x, o), yy = __shfl_up_sync(0xffffffffu, x.y, o);
+        if (lane >= o) { x.x += yx; x.y += yy; }
+    }
+    if (lane == 31) warpSums[warp] = x;
+    __syncthreads();
+    int2 pre = tileScan[blockIdx.x];
+    for (int w = 0; w < warp; ++w) { pre.x += warpSums[w].x; pre.y += warpSums[w].y; }
+    pre.x += x.x - s.x; pre.y += x.y - s.y;   // exclusive prefix of this thread's first item
+    for (int q = 0; q < kPlocItems; ++q) {
+        const int i = first + q;
+        if (f[q].x) {
+            Cluster a = c[i];
+            if (f[q].y) {
+                const Cluster b = c[nn[i]];
+                const int id = nextId - pre.y;
+                children[id] = make_int2(__float_as_int(a.lo.w), __float_as_int(b.lo.w));
+                const int cnt = __float_as_int(a.hi.w) + __float_as_int(b.hi.w);
+                counts[id] = cnt;
+                a.lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), __int_as_float(id));
+                a.hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), __int_as_float(cnt));
+            }
+            out[pre.x] = a;
+        }
+        pre.x += f[q].x; pre.y += f[q].y;
+    }
+}
+
+__global__ void kPlocParents(const int2* __restrict__ children, int inner, int* parentInner, int* parentMorton)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= inner) return;
+    const int2 c = children[id];
+    if (c.x >= 0) parentInner[c.x] = id; else parentMorton[~c.x] = id;
+    if (c.y >= 0) parentInner[c.y] = id; else parentMorton[~c.y] = id;
+    if (id == 0) parentInner[0] = -1;
+}
+
+__device__ __forceinline__ int subtreeCount(const int* counts, int code) { return code >= 0 ? counts[code] : 1; }
+
+// first leaf (depth-first order) of every inner node, by a walk to the root;
+// depthMax = the deepest leaf's depth
+__global__ void kPlocFirstInner(const int2* __restrict__ children, const int* __restrict__ parentInner,
+                                const int* __restrict__ counts, int inner, int* firstInner, int* depthMax)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= inner) return;
+    int first = 0, cur = id, depth = 1;
+    for (int p = parentInner[cur]; p >= 0 && depth <= inner; cur = p, p = parentInner[p], ++depth) {
+        const int2 c = children[p];
+        if (c.y == cur) first += subtreeCount(counts, c.x);
+    }
+    firstInner[id] = first;
+    atomicMax(depthMax, depth + 1);
+}
+
+// depth-first relabel: leaf codes, ranges, triangle order, leaf parents
+__global__ void kPlocRelabel(int2* children, const int* __restrict__ counts, const int* __restrict__ firstInner,
+                             const int* __restrict__ parentMorton, const int* __restrict__ sortedMorton, int n,
+                             int2* range, int* sortedTri, int* parentLeaf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {   // leaf i in Morton order
+        const int p = parentMorton[i];
+        const int2 c = children[p];
+        const int pos = firstInner[p] + ((c.y == ~i) ? subtreeCount(counts, c.x) : 0);
+        sortedTri[pos] = sortedMorton[i];
+        parentLeaf[pos] = p;
+    }
+    if (i < n - 1) {
+        const int f = firstInner[i];
+        range[i] = make_int2(f, f + counts[i] - 1);
+    }
+}
+
+__global__ void kPlocLeafCodes(int2* children, const int* __restrict__ counts, const int* __restrict__ firstInner,
+                               int inner)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= inner) return;
+    int2 c = children[id];
+    const int f = firstInner[id];
+    if (c.x < 0) c.x = ~f;                               // the left child starts the parent's range
+    if (c.y < 0) c.y = ~(f + subtreeCount(counts, c.x));
+    children[id] = c;
+}
+
 // ---------------------------------------------------------------- 8-wide collapse
 // Top-down, one level of the wide tree per pass.  A wide node rooted at a
 // binary node takes its two children and then repeatedly opens the child of
@@ -595,8 +830,70 @@ fail:
     return rc;
 }
 
-int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, BvhBuildResult& out, cudaStream_t st,
-              std::string& err)
+// PLOC hierarchy over the Morton-sorted triangles `sortedMorton`: fills
+// children / parentInner / parentLeaf / range like kKarras, with the leaves in
+// depth-first order, and that order's triangles in `sortedDfs`.  *depth = the
+// deepest leaf's depth (root = 1).
+static int buildPloc(const TriangleData* dTris, const int* sortedMorton, int n, int radius, int2* children,
+                     int* parentInner, int* parentLeaf, int2* range, int* sortedDfs, int* depth, cudaStream_t st,
+                     std::string& err)
+{
+    Cluster *cA = nullptr, *cB = nullptr;
+    int *nn = nullptr, *counts = nullptr, *firstInner = nullptr, *parentMorton = nullptr, *dDepth = nullptr;
+    int2* tileSums = nullptr;
+    int rc = -1;
+    const int inner = n - 1;
+    const int maxTiles = (n + kPlocTile - 1) / kPlocTile;
+    {
+        BVH_CK(cudaMalloc(&cA, sizeof(Cluster) * n));
+        BVH_CK(cudaMalloc(&cB, sizeof(Cluster) * n));
+        BVH_CK(cudaMalloc(&nn, sizeof(int) * n));
+        BVH_CK(cudaMalloc(&counts, sizeof(int) * inner));
+        BVH_CK(cudaMalloc(&firstInner, sizeof(int) * inner));
+        BVH_CK(cudaMalloc(&parentMorton, sizeof(int) * n));
+        BVH_CK(cudaMalloc(&dDepth, sizeof(int)));
+        BVH_CK(cudaMalloc(&tileSums, sizeof(int2) * (maxTiles + 1)));
+        const int B = 256;
+        kPlocInit<<<(n + B - 1) / B, B, 0, st>>>(dTris, sortedMorton, n, cA);
+        int m = n, nextId = n - 2, rounds = 0;
+        while (m > 1) {
+            const int tiles = (m + kPlocTile - 1) / kPlocTile;
+            kPlocNearest<<<(m + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(cA, m, radius, nn);
+            kPlocCount<<<tiles, kPlocBlock, 0, st>>>(nn, m, tileSums);
+            kPlocScanTiles<<<1, 1024, 0, st>>>(tileSums, tiles);
+            kPlocCompact<<<tiles, kPlocBlock, 0, st>>>(cA, nn, m, tileSums, nextId, cB, children, counts);
+            BVH_CK(cudaGetLastError());
+            int2 tot = make_int2(0, 0);
+            BVH_CK(cudaMemcpyAsync(&tot, tileSums + tiles, sizeof(int2), cudaMemcpyDeviceToHost, st));
+            BVH_CK(cudaStreamSynchronize(st));
+            if (tot.y <= 0 || tot.x != m - tot.y || tot.y > nextId + 1 || ++rounds > n) {
+                err = "PLOC build: a clustering round merged no pair";
+                goto fail;
+            }
+            m = tot.x;
+            nextId -= tot.y;
+            Cluster* t = cA; cA = cB; cB = t;
+        }
+        if (nextId != -1) { err = "PLOC build: merge count differs from n-1"; goto fail; }
+        BVH_CK(cudaMemsetAsync(dDepth, 0, sizeof(int), st));
+        kPlocParents<<<(inner + B - 1) / B, B, 0, st>>>(children, inner, parentInner, parentMorton);
+        kPlocFirstInner<<<(inner + B - 1) / B, B, 0, st>>>(children, parentInner, counts, inner, firstInner, dDepth);
+        kPlocRelabel<<<(n + B - 1) / B, B, 0, st>>>(children, counts, firstInner, parentMorton, sortedMorton, n, range,
+                                                    sortedDfs, parentLeaf);
+        kPlocLeafCodes<<<(inner + B - 1) / B, B, 0, st>>>(children, counts, firstInner, inner);
+        BVH_CK(cudaGetLastError());
+        BVH_CK(cudaMemcpyAsync(depth, dDepth, sizeof(int), cudaMemcpyDeviceToHost, st));
+        BVH_CK(cudaStreamSynchronize(st));
+        rc = 0;
+    }
+fail:
+    cudaFree(cA); cudaFree(cB); cudaFree(nn); cudaFree(counts); cudaFree(firstInner); cudaFree(parentMorton);
+    cudaFree(dDepth); cudaFree(tileSums);
+    return rc;
+}
+
+int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int builder, int radius, BvhBuildResult& out,
+              cudaStream_t st, std::string& err)
 {
     out = BvhBuildResult{};
     if (n <= 0) return 0;
@@ -655,7 +952,17 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, BvhBuild
             unsigned long long* tk = kin; kin = kout; kout = tk;
             int* tv = vin; vin = vout; vout = tv;
         }
-        if (n > 1) {
+        out.builder = 0;
+        if (n > 1 && builder == 1) {
+            int depth = 0;
+            if (buildPloc(dTris, vin, n, radius, children, parentInner, parentLeaf, range, vout, &depth, st, err) != 0)
+                goto fail;
+            if (width == 8 || depth - 1 <= kTraversalStack) {   // else the binary walk's stack could overflow
+                int* tv = vin; vin = vout; vout = tv;
+                out.builder = 1;
+            }
+        }
+        if (n > 1 && out.builder == 0) {
             kKarras<<<(n - 1 + B - 1) / B, B, 0, st>>>(kin, n, children, parentInner, parentLeaf, range);
         }
         kRefit<<<G, B, 0, st>>>(dTris, vin, n, children, parentInner, parentLeaf, range, sorted, innerBox, leafBox,

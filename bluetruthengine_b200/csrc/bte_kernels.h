@@ -42,10 +42,13 @@ struct BvhBuildResult {
     int depth = 0;          // levels of the 8-wide tree
     int rootIsLeaf = 0;
     int rootCode = ~0;      // leaf code of the root when rootIsLeaf
+    int builder = 0;        // hierarchy built: 0 Morton-prefix (Karras), 1 PLOC
     float msBuild = 0.0f;
 };
-int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, int width, BvhBuildResult& out, cudaStream_t st,
-              std::string& err);
+// builder 1 asks for PLOC with neighbour search radius `radius`; a binary
+// tree too deep for the traversal stack falls back to the Morton-prefix one.
+int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, int width, int builder, int radius,
+              BvhBuildResult& out, cudaStream_t st, std::string& err);
 
 // Env-map tables (bte_env.cu).
 int buildEnvCdf(const float4* dTexels, int w, int h, const float* hSinTheta, float* dMarginal, float* dConditional,

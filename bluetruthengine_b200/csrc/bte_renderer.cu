@@ -63,6 +63,8 @@ struct Renderer {
     bool init = false;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;         // shadow-ray stage of a bounce, beside the next bounce's extend
+    cudaEvent_t evShade = nullptr, evConnect = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t stageEv[8] = {};
 
@@ -93,6 +95,11 @@ struct Renderer {
     int postponePct = 0;      // 8-wide walk: leaf-test postponing threshold (0: never; neutral on the bench scene)
     int sortShading = 1;      // material-sorted shading (shade 5.9 -> 2.6 ms per frame on the 1080p bench scene)
     int tailPaths = 0;        // bounce queues shorter than this finish in the tail kernel
+    int bvhBuilder = 1;       // binary hierarchy of the next bte_init_accel: 0 Morton-prefix (Karras), 1 PLOC
+                              // (PLOC: frame 10.96 -> 10.54 ms on the 1080p bench scene)
+    int plocRadius = 8;       // PLOC neighbour search radius (8 measured best of 8/16/32)
+    int builtBuilder = 0;     // hierarchy in use
+    int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
     int builtWidth = 2;       // tree in use
     int accelNodes = 0, accelDepth = 0;
     int shadeMinBlocks = 3;   // autotuned on B200: 3 resident shade blocks per SM
@@ -148,6 +155,9 @@ void ensureInit()
     if (n <= 0) throw CudaError{"no CUDA device"};
     ck(cudaGetDevice(&g.device), "cudaGetDevice");
     ck(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&g.evShade, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&g.evConnect, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreate(&g.ev0), "cudaEventCreate");
     ck(cudaEventCreate(&g.ev1), "cudaEventCreate");
     for (auto& e : g.stageEv) ck(cudaEventCreate(&e), "cudaEventCreate");
@@ -309,6 +319,28 @@ void ensureAccum(int w, int h)
 
 int slotsFor() { return 1 + g.spotCount + 1; }
 
+// The bounce loop.  Bounce b's shadow rays (connect) only clear visibility bits that bounce b+1's shade
+// reads, and bounce b+1's closest-hit rays (extend) only need bounce b's shade, so with overlapConnect
+// connect(b) runs on the side stream beside extend(b+1): shade(b) -> {connect(b) | extend(b+1)} ->
+// shade(b+1).  The few-ray launches of the last bounces are latency-bound, and the two overlap there.
+void launchBounces(const DevScene& s, const DevPaths& P, const FrameParams& f, int depth, int block, cudaStream_t st)
+{
+    for (int b = 0; b < depth; ++b) {
+        launchExtend(s, P, b, g.gridExtend, block, st);
+        if (g.overlapConnect && b > 0) ck(cudaStreamWaitEvent(st, g.evConnect, 0), "cudaStreamWaitEvent");
+        launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
+        if (g.overlapConnect) {
+            ck(cudaEventRecord(g.evShade, st), "cudaEventRecord");
+            ck(cudaStreamWaitEvent(g.side, g.evShade, 0), "cudaStreamWaitEvent");
+            launchConnect(s, P, b, g.gridConnect, block, g.side);
+            ck(cudaEventRecord(g.evConnect, g.side), "cudaEventRecord");
+        } else {
+            launchConnect(s, P, b, g.gridConnect, block, st);
+        }
+    }
+    if (g.overlapConnect && depth > 0) ck(cudaStreamWaitEvent(st, g.evConnect, 0), "cudaStreamWaitEvent");
+}
+
 void renderFrame(int w, int h)
 {
     if (w <= 0 || h <= 0) throw CudaError{"bte_render: image size must be positive"};
@@ -384,11 +416,7 @@ void renderFrame(int w, int h)
     };
     auto frameLaunches = [&] {
         launchGenerate(P, f, st);
-        for (int b = 0; b < depth; ++b) {
-            launchExtend(s, P, b, g.gridExtend, block, st);
-            launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
-            launchConnect(s, P, b, g.gridConnect, block, st);
-        }
+        launchBounces(s, P, f, depth, block, st);
         launchTail(s, P, f, st);
         launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st);
     };
@@ -401,8 +429,8 @@ void renderFrame(int w, int h)
             const unsigned char* c = static_cast<const unsigned char*>(p);
             key.insert(key.end(), c, c + n);
         };
-        const int ints[8] = {depth, block, g.gridExtend, g.gridShade, g.gridConnect, g.shadeMinBlocks, paths,
-                             g.hitLogEnabled ? 1 : 0};
+        const int ints[9] = {depth, block, g.gridExtend, g.gridShade, g.gridConnect, g.shadeMinBlocks, paths,
+                             g.hitLogEnabled ? 1 : 0, g.overlapConnect};
         const void* ptrs[5] = {accumF, accumDv, fb, g.extFramebuffer, aovAcc};
         put(&P, sizeof(P)); put(&f, sizeof(f)); put(&s, sizeof(s)); put(ints, sizeof(ints)); put(ptrs, sizeof(ptrs));
         if (!g.graphExec || key != g.graphKey) {
@@ -581,11 +609,7 @@ void renderViews(const BteView* views, int count)
     ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
     ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
     launchGenerate(P, f, st);
-    for (int b = 0; b < depth; ++b) {
-        launchExtend(s, P, b, g.gridExtend, block, st);
-        launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
-        launchConnect(s, P, b, g.gridConnect, block, st);
-    }
+    launchBounces(s, P, f, depth, block, st);
     launchTail(s, P, f, st);
     launchPresentViews(P, f, static_cast<int>(pixels64), st);
     ck(cudaGetLastError(), "kernel launch");
@@ -693,11 +717,11 @@ int bte_init_accel(void)
         if (!g.tris.p || g.triCount <= 0) throw CudaError{"bte_init_accel: call bte_init_scene first"};
         BvhBuildResult r;
         std::string err;
-        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, g.bvhWidth, r, g.stream, err) != 0)
+        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, g.bvhWidth, g.bvhBuilder, g.plocRadius, r, g.stream, err) != 0)
             throw CudaError{err};
         if (r.width == 8 && 2 * r.depth > kWideStack) {   // node + postponed-leaf groups could overflow: binary tree
             cudaFree(r.wnodes); cudaFree(r.leafTris);
-            if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, 2, r, g.stream, err) != 0) throw CudaError{err};
+            if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, 2, g.bvhBuilder, g.plocRadius, r, g.stream, err) != 0) throw CudaError{err};
         }
         if (r.width == 8) {
             g.wideNodes.p = r.wnodes; g.wideNodes.bytes = sizeof(WideNode) * r.nodeCount;
@@ -705,6 +729,7 @@ int bte_init_accel(void)
             g.bvhNodes.p = r.nodes; g.bvhNodes.bytes = sizeof(BvhNode) * (r.nodeCount > 0 ? r.nodeCount : 1);
         }
         g.builtWidth = r.width;
+        g.builtBuilder = r.builder;
         g.accelNodes = r.nodeCount;
         g.accelDepth = r.depth;
         g.gridBlock = 0;
@@ -1057,12 +1082,18 @@ int bte_set_tuning(const BteTuning* t)
         if (t->postponePercent < 0 || t->postponePercent > 100) throw CudaError{"bte_set_tuning: postponePercent in [0, 100]"};
         if (t->sortShading != 0 && t->sortShading != 1) throw CudaError{"bte_set_tuning: sortShading must be 0 or 1"};
         if (t->tailPaths < 0) throw CudaError{"bte_set_tuning: tailPaths must be >= 0"};
+        if (t->bvhBuilder != 0 && t->bvhBuilder != 1) throw CudaError{"bte_set_tuning: bvhBuilder must be 0 or 1"};
+        if (t->plocRadius < 1 || t->plocRadius > kPlocMaxRadius) throw CudaError{"bte_set_tuning: plocRadius in [1, 32]"};
+        if (t->overlapConnect != 0 && t->overlapConnect != 1) throw CudaError{"bte_set_tuning: overlapConnect must be 0 or 1"};
         g.bvhWidth = t->bvhWidth;
         g.maxLeaf = t->maxLeafTriangles;
         g.shadeMinBlocks = t->shadeMinBlocks;
         g.postponePct = t->postponePercent;
         g.sortShading = t->sortShading;
         g.tailPaths = t->tailPaths;
+        g.bvhBuilder = t->bvhBuilder;
+        g.plocRadius = t->plocRadius;
+        g.overlapConnect = t->overlapConnect;
         g.gridBlock = 0;   // recompute persistent grids
         return 0;
     });
@@ -1078,6 +1109,19 @@ int bte_get_tuning(BteTuning* t)
         t->postponePercent = g.postponePct;
         t->sortShading = g.sortShading;
         t->tailPaths = g.tailPaths;
+        t->bvhBuilder = g.bvhBuilder;
+        t->plocRadius = g.plocRadius;
+        t->overlapConnect = g.overlapConnect;
+        return 0;
+    });
+}
+
+int bte_get_accel_builder(int* builder)
+{
+    return guarded([&] {
+        if (!g.accelReady) throw CudaError{"bte_get_accel_builder: no acceleration structure (bte_init_accel)"};
+        if (!builder) throw CudaError{"bte_get_accel_builder: null builder"};
+        *builder = g.builtBuilder;
         return 0;
     });
 }

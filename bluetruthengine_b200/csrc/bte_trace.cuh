@@ -20,8 +20,6 @@
 
 namespace bte {
 
-constexpr int kTraversalStack = 96;
-
 struct RayPre {
     float ox, oy, oz;
     int kx, ky, kz;

@@ -63,6 +63,8 @@ static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
 constexpr int kWideLeafMax = 3;
 constexpr int kSortKeys = 6;
 constexpr int kWideStack = 64;    // traversal stack entries; trees deeper than half of it use the binary tree
+constexpr int kTraversalStack = 96;   // binary-tree traversal stack entries; deeper PLOC trees fall back to LBVH
+constexpr int kPlocMaxRadius = 32;   // PLOC neighbour search radius limit (positions each side)
 
 struct DevScene {
     // geometry

@@ -140,12 +140,20 @@ typedef struct {
     int tailPaths;         /* from the first bounce whose queue is shorter than this, one thread per path
                             * finishes the path (extend + shade + shadow rays per bounce) in one kernel;
                             * 0: the wavefront runs every bounce */
+    int bvhBuilder;        /* binary hierarchy the trees are built from: 0 Morton-prefix splits (Karras 2012);
+                            * 1 PLOC, locally-ordered clustering over the Morton order (Meister & Bittner 2018) */
+    int plocRadius;        /* PLOC neighbour search radius in positions, 1-32 */
+    int overlapConnect;    /* 1: bounce b's shadow rays run on a second stream beside bounce b+1's closest-hit
+                            * rays (they share no data); 0: the stages run one after another */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);
 /* The acceleration structure in use: width (2 or 8), node count, levels of
  * the 8-wide tree (0 for width 2) and device build time. */
 int bte_get_accel_info(int* width, int* nodeCount, int* depth, float* msBuild);
+/* The binary hierarchy the structure in use was built from (BteTuning.bvhBuilder; a
+ * PLOC tree too deep for the binary walk's stack is rebuilt with Morton-prefix splits). */
+int bte_get_accel_builder(int* builder);
 
 /* ---- learned denoiser (replaces the vendor denoiser stage, render_kernel.h:187 / src/host/denoiser.cu) ----
  * A 5-level U-Net (3x3 convolutions, 32-128 channels) over log(1 + radiance)

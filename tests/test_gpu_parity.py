@@ -49,21 +49,25 @@ def test_math_functions_bitexact(renderer, oracle_mod):
         assert len(bad) == 0, f"fn {fn}: {len(bad)} mismatches"
 
 
-def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0):
+def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0,
+            builder=1, radius=8):
     renderer.cleanup()
-    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths)
+    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
 
-@pytest.mark.parametrize("tree", [(8, 1), (8, 3), (2, 1), (2, 4)])
+@pytest.mark.parametrize("tree", [(8, 1, 0, 16), (8, 3, 0, 16), (2, 1, 0, 16), (2, 4, 0, 16), (8, 2, 1, 16),
+                                  (8, 1, 1, 1), (2, 1, 1, 32), (2, 3, 1, 4)])
 @pytest.mark.parametrize("scene_name", ["cornell_scene", "random_scene"])
 def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, tree):
-    """Closest hit (triangle, t, u, v) and any-hit occlusion for 40k rays, both tree widths and several
-    leaf sizes, against the oracle's brute force over all triangles."""
+    """Closest hit (triangle, t, u, v) and any-hit occlusion for 40k rays, both tree widths, several
+    leaf sizes and both hierarchy builders (Morton-prefix splits; PLOC at several search radii), against
+    the oracle's brute force over all triangles."""
     scene = request.getfixturevalue(scene_name)
-    _upload(renderer, scene, bvh_width=tree[0], max_leaf=tree[1])
-    assert renderer.accel_info()["width"] == tree[0]
+    _upload(renderer, scene, bvh_width=tree[0], max_leaf=tree[1], builder=tree[2], radius=tree[3])
+    info = renderer.accel_info()
+    assert info["width"] == tree[0] and info["builder"] == tree[2]
     orc = oracle_mod.Oracle(libm=False)
     view = oracle_mod.SceneView(scene, oracle=orc, build_accel=False)
     tri = scene.triangles
@@ -252,19 +256,21 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths",
-                         [(1, 8, 0, 0), (0, 8, 0, 0), (1, 2, 0, 0), (1, 8, 1, 0), (1, 8, 1, 200000)])
-def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading, tail_paths):
+@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder",
+                         [(1, 8, 0, 0, 0), (0, 8, 0, 0, 0), (1, 2, 0, 0, 0), (1, 8, 1, 0, 0), (1, 8, 1, 200000, 0),
+                          (1, 8, 1, 0, 1), (0, 2, 0, 0, 1)])
+def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading, tail_paths,
+                                     builder):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
     pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
     _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading,
-            tail_paths=tail_paths)
+            tail_paths=tail_paths, max_leaf=1 if bvh_width == 2 else 2, builder=builder)
     info = renderer.accel_info()
     print("accel", info)
-    assert info["width"] == bvh_width
+    assert info["width"] == bvh_width and info["builder"] == builder
     if bvh_width == 8:
         assert 0 < info["depth"] <= 64 and info["nodes"] < scene.triangle_count // 2
     renderer.set_hit_log(True)
@@ -319,15 +325,45 @@ def test_textured_materials_bitexact(renderer, oracle_mod, random_scene):
 def test_tuning_roundtrip_and_validation(renderer):
     """bte_set_tuning / bte_get_tuning: values round-trip; out-of-range values are rejected with a message."""
     import bluetruthengine_b200 as B
-    renderer.set_tuning(2, 2, 8, 35, 1, 4096)
+    renderer.set_tuning(2, 2, 8, 35, 1, 4096, 1, 7)
     assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
-                                 "sortShading": 1, "tailPaths": 4096}
+                                 "sortShading": 1, "tailPaths": 4096, "bvhBuilder": 1, "plocRadius": 7,
+                                 "overlapConnect": 1}
     for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2),
-                (1, 3, 8, 20, 1, -1)]:
+                (1, 3, 8, 20, 1, -1), (1, 3, 8, 20, 1, 0, 2), (1, 3, 8, 20, 1, 0, 1, 0), (1, 3, 8, 20, 1, 0, 1, 33),
+                (1, 3, 8, 20, 1, 0, 1, 16, 2)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
     assert renderer.tuning()["bvhWidth"] == 8
+
+
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_overlapped_connect_matches_serial_stages(renderer, random_scene, use_graph):
+    """Shadow rays of bounce b on the side stream beside bounce b+1's closest-hit rays give the same
+    per-sample radiance, hit log and accumulation, bit for bit, as the stages run one after another."""
+    from conftest import bits
+    sc = random_scene
+    W, H, spp, depth = sc.width, sc.height, 3, 12
+    out = []
+    for overlap in (0, 1, 0, 1):
+        renderer.cleanup()
+        renderer.set_tuning(2, 3, 8, 0, 1, 0, 1, 8, overlap)
+        renderer.upload(sc)
+        renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=1, use_graph=use_graph)
+        renderer.set_hit_log(True)
+        renderer.reset_accumulation(W, H)
+        for _ in range(2):
+            renderer.render(W, H)
+        n = W * H * spp
+        out.append((renderer.read_sample_radiance(n).copy(), renderer.read_hit_log(n * depth).copy(),
+                    renderer.read_accum(W, H).copy()))
+        renderer.set_hit_log(False)
+    for o in out[1:]:
+        assert np.array_equal(bits(o[0]), bits(out[0][0]))
+        assert np.array_equal(o[1], out[0][1])
+        assert np.array_equal(bits(o[2]), bits(out[0][2]))
+    renderer.set_tuning()
 
 
 def test_graph_frames_match_stream_frames(renderer, random_scene):
