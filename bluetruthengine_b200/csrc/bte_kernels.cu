@@ -298,6 +298,16 @@ __global__ void __launch_bounds__(256) kConnect(DevScene s, DevPaths P, int boun
     }
 }
 
+// Persistent lanes with ray refill need only ceil(count / 32) warps: those take every ray between them
+// (any non-empty subset of warps drains the queue), so the warps above that leave before touching the
+// shared fetch counter.  With the few rays of the last bounces this spares thousands of same-address
+// atomics per launch.
+BTE_DI bool warpNotNeeded(int count)
+{
+    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    return warp * 32 >= count;
+}
+
 // ---------------------------------------------------------------- extend / connect over the 8-wide tree
 // Same results as kExtend / kConnect, but each lane keeps its walk state
 // across iterations and takes a new ray (warp-aggregated fetch from a
@@ -309,9 +319,27 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
     const int count = P.rayCount[bounce];
     if (tailTakesOver(P, bounce)) return;
     const int* __restrict__ q = P.queue[bounce & 1];
+    uint2 stack[kWideStack];
+    if (count <= static_cast<int>((gridDim.x * blockDim.x) >> 3)) {   // few rays: eight lanes per ray
+        const int g = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+        if (g >= count) return;
+        const int idx = q[g];
+        const float4 o = P.o[idx];
+        const float4 d = P.d[idx];
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+        float t = 0.0f, u = 0.0f, v = 0.0f;
+        int tri = -1;
+        if (r.valid && s.triCount > 0) tri = traceWideGroup<false>(s, r, kEps, 1e30f, stack, P.errorFlags, t, u, v);
+        if ((threadIdx.x & 7u) == 0u) {
+            P.hit[idx] = tri >= 0 ? make_float4(t, u, v, __int_as_float(tri)) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+            if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
+            if (P.sortQueue) sortAppend(s, P, bounce, idx, tri);
+        }
+        return;
+    }
+    if (warpNotNeeded(count)) return;
     int* fetch = P.fetch + bounce;
     WideWalk<false> w;
-    uint2 stack[kWideStack];
     int idx = -1;
     while (true) {
         if (idx < 0) {
@@ -345,9 +373,24 @@ __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int 
 {
     const int count = P.shadowCount[bounce];
     if (tailTakesOver(P, bounce)) return;
+    uint2 stack[kWideStack];
+    if (count <= static_cast<int>((gridDim.x * blockDim.x) >> 3)) {   // few rays: eight lanes per ray
+        const int g = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+        if (g >= count) return;
+        const int e = P.shadowQueue[g];
+        const int path = e / P.slots;
+        const float4 o = P.shOrigin[path];
+        const float4 d = P.shDir[e];
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+        if (!r.valid || s.triCount <= 0) return;
+        float t, u, v;
+        if (traceWideGroup<true>(s, r, kEps, d.w, stack, P.errorFlags, t, u, v) >= 0 && (threadIdx.x & 7u) == 0u)
+            atomicAnd(P.shMask + path, ~(1u << (e - path * P.slots)));
+        return;
+    }
+    if (warpNotNeeded(count)) return;
     int* fetch = P.fetch + (P.maxDepth + 1) + bounce;
     WideWalk<true> w;
-    uint2 stack[kWideStack];
     int e = -1;
     while (true) {
         if (e < 0) {

@@ -382,6 +382,145 @@ struct WideWalk {
     }
 };
 
+// ---------------------------------------------------------------- 8-wide traversal, 8 lanes per ray
+// For the last bounces, whose few rays leave the GPU latency-bound, a group of
+// eight lanes walks one ray: lane c decodes and tests child slot c of the
+// fetched node (the same decode and slab test as WideWalk), tests the
+// triangles of its slot when that slot is a leaf, and the group merges the
+// candidates by (t, index).  The nearest internal child (lowest slot ^ octant
+// key) is visited next; the others are pushed so that lower keys pop first.
+// The stack is spread over the group: entry p lives in lane p % 8 at index
+// p / 8 of that lane's own array, so a group holds 8 * kWideStack entries.
+// Popped entries carry their entry distance and are dropped once it exceeds
+// the current best by more than the box test's margins (the box would fail
+// the test now).  Any order of visits gives the same result (closest hit is
+// the minimum of (t, index) over all accepted triangles; culling is
+// conservative), so this walk returns exactly what WideWalk returns.
+// All eight lanes of a group must call it with the same ray.
+template <bool AnyHit>
+BTE_DI int traceWideGroup(const DevScene& s, const RayPre& r, float tmin, float tmax, uint2* stack,
+                          unsigned int* errorFlags, float& tOut, float& uOut, float& vOut)
+{
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int c = lane & 7;
+    const unsigned gmask = 0xffu << (lane & ~7);
+    const uint32_t oct = (r.ix < 0.0f ? 1u : 0u) | (r.iy < 0.0f ? 2u : 0u) | (r.iz < 0.0f ? 4u : 0u);
+    int node = 0, sp = 0, visits = 0, best = -1;
+    float bt = tmax, bu = 0.0f, bv = 0.0f;
+    while (true) {
+        if (node < 0) {
+            if (sp == 0) break;
+            --sp;
+            const uint2 mine = stack[sp >> 3];
+            const int e = __shfl_sync(gmask, static_cast<int>(mine.x), sp & 7, 8);
+            const float te = __shfl_sync(gmask, __uint_as_float(mine.y), sp & 7, 8);
+            if (!AnyHit && te > (bt * kCullMargin) * kBoxGrow) continue;
+            node = e;
+        }
+        if (node >= s.wideNodeCount || ++visits > s.wideNodeCount) {   // never true for a built tree
+            if (errorFlags && c == 0) atomicOr(errorFlags, 2u);
+            break;
+        }
+        const float4* np = reinterpret_cast<const float4*>(s.wnodes) + 5 * static_cast<size_t>(node);
+        const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3), f4 = __ldg(np + 4);
+        const uint32_t em = __float_as_uint(f0.w);
+        const uint32_t imask = em >> 24;
+        // child slot c: the decode and slab test of WideWalk::step for one slot
+        const float ax = wideScale(em & 0xffu) * r.ix, ay = wideScale((em >> 8) & 0xffu) * r.iy,
+                    az = wideScale((em >> 16) & 0xffu) * r.iz;
+        const float cx = (f0.x - r.ox) * r.ix, cy = (f0.y - r.oy) * r.iy, cz = (f0.z - r.oz) * r.iz;
+        const float cnx = cx - r.px, cfx = cx + r.px, cny = cy - r.py, cfy = cy + r.py, cnz = cz - r.pz,
+                    cfz = cz + r.pz;
+        const bool sxn = oct & 1u, syn = oct & 2u, szn = oct & 4u;
+        const bool hiWord = c >= 4;
+        const uint32_t nx = __float_as_uint(sxn ? (hiWord ? f3.w : f3.z) : (hiWord ? f2.y : f2.x));
+        const uint32_t fx = __float_as_uint(sxn ? (hiWord ? f2.y : f2.x) : (hiWord ? f3.w : f3.z));
+        const uint32_t ny = __float_as_uint(syn ? (hiWord ? f4.y : f4.x) : (hiWord ? f2.w : f2.z));
+        const uint32_t fy = __float_as_uint(syn ? (hiWord ? f2.w : f2.z) : (hiWord ? f4.y : f4.x));
+        const uint32_t nz = __float_as_uint(szn ? (hiWord ? f4.w : f4.z) : (hiWord ? f3.y : f3.x));
+        const uint32_t fz = __float_as_uint(szn ? (hiWord ? f3.y : f3.x) : (hiWord ? f4.w : f4.z));
+        const float cull = AnyHit ? tmax * kCullMargin : bt * kCullMargin;
+        const uint32_t sel = static_cast<uint32_t>(c & 3) | 0x7440u;
+        const float tnx = __fmaf_rn(byteToFloat(nx, sel), ax, cnx);
+        const float tfx = __fmaf_rn(byteToFloat(fx, sel), ax, cfx);
+        const float tny = __fmaf_rn(byteToFloat(ny, sel), ay, cny);
+        const float tfy = __fmaf_rn(byteToFloat(fy, sel), ay, cfy);
+        const float tnz = __fmaf_rn(byteToFloat(nz, sel), az, cnz);
+        const float tfz = __fmaf_rn(byteToFloat(fz, sel), az, cfz);
+        const float tn = max3f(tnx, tny, fmaxf(tnz, tmin));
+        const float tf = min3f(tfx, tfy, fminf(tfz, cull)) * kBoxGrow;
+        const bool slotHit = tn <= tf;
+        const bool internal = (imask >> c) & 1u;
+        // the triangles of a leaf slot that was hit
+        int lbest = -1;
+        bool lhit = false;
+        float lt = bt, lu = 0.0f, lv = 0.0f;
+        if (slotHit && !internal) {
+            const uint32_t mb = ((c >= 4 ? __float_as_uint(f1.w) : __float_as_uint(f1.z)) >> (8 * (c & 3))) & 0xffu;
+            const int first = __float_as_int(f1.y) + static_cast<int>(mb & 31u);
+            for (int k = 0; k < static_cast<int>(mb >> 5); ++k) {
+                if (static_cast<uint32_t>(first + k) >= static_cast<uint32_t>(s.triCount)) {
+                    if (errorFlags) atomicOr(errorFlags, 2u);
+                    break;
+                }
+                const float4* tp = s.leafTris + 3 * static_cast<size_t>(first + k);
+                const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+                float t, u, v;
+                if (isectTri(r, a, b, cc, tmin, AnyHit ? tmax : lt, t, u, v)) {
+                    if (AnyHit) { lhit = true; break; }
+                    const int idx = __float_as_int(a.w);
+                    if (lbest < 0 || t < lt || (t == lt && idx < lbest)) { lbest = idx; lt = t; lu = u; lv = v; }
+                }
+            }
+        }
+        if (AnyHit) {
+            if (__any_sync(gmask, lhit)) { best = 1; break; }
+        } else if (__any_sync(gmask, lbest >= 0)) {
+            // group minimum of (t, index); lanes without a candidate hold (+inf, INT_MAX)
+            float mt = lbest >= 0 ? lt : INFINITY;
+            int mi = lbest >= 0 ? lbest : 0x7fffffff;
+            float mu = lu, mv = lv;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const float ot = __shfl_xor_sync(gmask, mt, o, 8);
+                const int oi = __shfl_xor_sync(gmask, mi, o, 8);
+                const float ou = __shfl_xor_sync(gmask, mu, o, 8);
+                const float ov = __shfl_xor_sync(gmask, mv, o, 8);
+                if (ot < mt || (ot == mt && oi < mi)) { mt = ot; mi = oi; mu = ou; mv = ov; }
+            }
+            if (best < 0 || mt < bt || (mt == bt && mi < best)) { best = mi; bt = mt; bu = mu; bv = mv; }
+        }
+        // internal children hit, keyed slot ^ octant; the lowest key is visited next
+        const uint32_t hits = (__ballot_sync(gmask, slotHit && internal) >> (lane & ~7)) & 0xffu;
+        uint32_t keys = 0;
+        for (uint32_t h = hits; h; h &= h - 1u) keys |= 1u << ((__ffs(h) - 1) ^ oct);
+        if (keys == 0u) { node = -1; continue; }
+        const uint32_t childBase = static_cast<uint32_t>(__float_as_int(f1.x));
+        const uint32_t nearSlot = static_cast<uint32_t>(__ffs(keys) - 1) ^ oct;
+        node = static_cast<int>(childBase) + __popc(imask & ((1u << nearSlot) - 1u));
+        const uint32_t rest = keys & (keys - 1u);
+        const int n = __popc(rest);
+        if (n == 0) continue;
+        if (sp + n > 8 * kWideStack) {
+            if (errorFlags && c == 0) atomicOr(errorFlags, 1u);
+            break;
+        }
+        // position sp + j (j = 0 .. n-1) holds the key of ascending rank n-1-j, so the lowest pops first;
+        // this lane owns the position congruent to it mod 8
+        const int j = (c - sp) & 7;
+        uint32_t pick = rest;
+        for (int q = 0; q < n - 1 - j && pick; ++q) pick &= pick - 1u;
+        const uint32_t slot = (j < n && pick) ? (static_cast<uint32_t>(__ffs(pick) - 1) ^ oct) : static_cast<uint32_t>(c);
+        const float tSlot = __shfl_sync(gmask, tn, static_cast<int>(slot), 8);
+        if (j < n)
+            stack[(sp + j) >> 3] = make_uint2(childBase + static_cast<uint32_t>(__popc(imask & ((1u << slot) - 1u))),
+                                              __float_as_uint(tSlot));
+        sp += n;
+    }
+    if (!AnyHit && best >= 0) { tOut = bt; uOut = bu; vOut = bv; }
+    return best;
+}
+
 template <bool AnyHit>
 BTE_DI int traceWide(const DevScene& s, const RayPre& r, float tmin, float tmax, float& tOut, float& uOut, float& vOut,
                      unsigned int* errorFlags)
