@@ -43,7 +43,7 @@ BYTES_PER_SHADE_SEGMENT = 182
 BYTES_PER_CONNECT_RAY = 68        # 44 R + 24 RMW
 # DRAM bytes per frame of each stage kernel on this workload, from one ncu capture
 # (profiles/traffic_stage_kernels_disney_spheres_1080p.md; dram__bytes_read.sum + dram__bytes_write.sum)
-STAGE_DRAM_BYTES_PER_FRAME = {"extend": 758.0e6, "shade": 3845.6e6, "connect": 441.8e6}
+STAGE_DRAM_BYTES_PER_FRAME = {"extend": 756.0e6, "shade": 3794.5e6, "connect": 432.1e6}
 
 
 def parse():

@@ -400,19 +400,19 @@ class Renderer:
         return out
 
     # ---- parity probes ----
-    def trace_closest(self, rays: np.ndarray):
+    def trace_closest(self, rays: np.ndarray, lanes: int = 1):
         r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
         n = len(r)
         tri = np.empty(n, dtype=np.int32)
         tuv = np.empty((n, 3), dtype=np.float32)
-        _check(self.lib.bte_trace_closest(_ptr(r), n, _ptr(tri), _ptr(tuv)))
+        _check(self.lib.bte_trace_closest_lanes(_ptr(r), n, int(lanes), _ptr(tri), _ptr(tuv)))
         return tri, tuv
 
-    def trace_occluded(self, rays: np.ndarray, tmax: np.ndarray):
+    def trace_occluded(self, rays: np.ndarray, tmax: np.ndarray, lanes: int = 1):
         r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
         t = np.ascontiguousarray(tmax, dtype=np.float32)
         out = np.empty(len(r), dtype=np.uint8)
-        _check(self.lib.bte_trace_occluded(_ptr(r), _ptr(t), len(r), _ptr(out)))
+        _check(self.lib.bte_trace_occluded_lanes(_ptr(r), _ptr(t), len(r), int(lanes), _ptr(out)))
         return out
 
     def env_query(self, op: int, x: np.ndarray) -> np.ndarray:

@@ -556,6 +556,35 @@ __global__ void kTraceOccludedRays(DevScene s, const float* rays, const float* t
     out[i] = traceOccludedW<Width>(s, r, kEps, tmax[i], err) ? 1 : 0;
 }
 
+// the same queries through the 8-lanes-per-ray walk (8-wide tree): ray i is walked by lanes 8i .. 8i+7
+__global__ void kTraceClosestRaysGroup(DevScene s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err)
+{
+    const int i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+    if (i >= n) return;
+    const float* r6 = rays + 6 * static_cast<size_t>(i);
+    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5], s.sceneMaxAbs);
+    float t = 0.0f, u = 0.0f, v = 0.0f;
+    uint2 stack[kWideStack];
+    const int tri = (r.valid && s.triCount > 0) ? traceWideGroup<false>(s, r, kEps, 1e30f, stack, err, t, u, v) : -1;
+    if ((threadIdx.x & 7u) == 0u) {
+        outTri[i] = tri;
+        outTuv[3 * i] = t; outTuv[3 * i + 1] = u; outTuv[3 * i + 2] = v;
+    }
+}
+
+__global__ void kTraceOccludedRaysGroup(DevScene s, const float* rays, const float* tmax, int n, uint8_t* out,
+                                        unsigned int* err)
+{
+    const int i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+    if (i >= n) return;
+    const float* r6 = rays + 6 * static_cast<size_t>(i);
+    const RayPre r = rayPre(r6[0], r6[1], r6[2], r6[3], r6[4], r6[5], s.sceneMaxAbs);
+    float t, u, v;
+    uint2 stack[kWideStack];
+    const bool occ = r.valid && s.triCount > 0 && traceWideGroup<true>(s, r, kEps, tmax[i], stack, err, t, u, v) >= 0;
+    if ((threadIdx.x & 7u) == 0u) out[i] = occ ? 1 : 0;
+}
+
 __global__ void kEnvQuery(DevScene s, int op, const float* in, int n, float* out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -699,15 +728,17 @@ void launchPackImage(const float* rgb, int n, uint32_t* fb, uint32_t* extFb, cud
     kPackImage<<<(n + 255) / 256, 256, 0, st>>>(rgb, n, fb, extFb);
 }
 void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
-                            cudaStream_t st)
+                            int lanes, cudaStream_t st)
 {
-    if (s.bvhWidth == 8) kTraceClosestRays<8><<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
+    if (lanes == 8) kTraceClosestRaysGroup<<<(n + 15) / 16, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
+    else if (s.bvhWidth == 8) kTraceClosestRays<8><<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
     else kTraceClosestRays<2><<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, outTri, outTuv, err);
 }
 void launchTraceOccludedRays(const DevScene& s, const float* rays, const float* tmax, int n, uint8_t* out, unsigned int* err,
-                             cudaStream_t st)
+                             int lanes, cudaStream_t st)
 {
-    if (s.bvhWidth == 8) kTraceOccludedRays<8><<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
+    if (lanes == 8) kTraceOccludedRaysGroup<<<(n + 15) / 16, 128, 0, st>>>(s, rays, tmax, n, out, err);
+    else if (s.bvhWidth == 8) kTraceOccludedRays<8><<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
     else kTraceOccludedRays<2><<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, out, err);
 }
 void launchEnvQuery(const DevScene& s, int op, const float* in, int n, float* out, cudaStream_t st)

@@ -17,10 +17,11 @@ void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cuda
 void launchPresentViews(const DevPaths& P, const FrameParams& f, int totalPixels, cudaStream_t st);
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    float* aovAccum, cudaStream_t st);
+// lanes 1: one lane per ray (the tree in use); lanes 8: eight lanes per ray (8-wide tree only)
 void launchTraceClosestRays(const DevScene& s, const float* rays, int n, int* outTri, float* outTuv, unsigned int* err,
-                            cudaStream_t st);
+                            int lanes, cudaStream_t st);
 void launchTraceOccludedRays(const DevScene& s, const float* rays, const float* tmax, int n, uint8_t* out,
-                             unsigned int* err, cudaStream_t st);
+                             unsigned int* err, int lanes, cudaStream_t st);
 void launchEnvQuery(const DevScene& s, int op, const float* in, int n, float* out, cudaStream_t st);
 void launchMathEval(int fn, const float* a, const float* b, float* out, int n, cudaStream_t st);
 void launchBsdfQuery(const BsdfData& g, int op, const float* wi, const float* x, int n, float* out, cudaStream_t st);

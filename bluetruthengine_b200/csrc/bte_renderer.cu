@@ -670,6 +670,12 @@ void checkTraceFlags(const unsigned int* dFlags)
     if (f & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
     if (f & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
 }
+void checkLanes(int lanes)
+{
+    if (lanes != 1 && lanes != 8) throw CudaError{"trace: lanesPerRay must be 1 or 8"};
+    if (lanes == 8 && g.builtWidth != 8) throw CudaError{"trace: eight lanes per ray need the 8-wide tree"};
+}
+
 }  // namespace
 
 extern "C" {
@@ -1226,17 +1232,18 @@ struct Tmp {
 
 extern "C" {
 
-int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv)
+int bte_trace_closest_lanes(const float* rays, int n, int lanesPerRay, int* outTri, float* outTuv)
 {
     return guarded([&] {
         if (n <= 0) return 0;
         if (!g.accelReady) throw CudaError{"bte_trace_closest: no acceleration structure"};
+        checkLanes(lanesPerRay);
         Tmp<float> dr(6 * static_cast<size_t>(n)), dt(3 * static_cast<size_t>(n));
         Tmp<int> di(n);
         Tmp<unsigned int> de(1);
         ck(cudaMemcpyAsync(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
         ck(cudaMemsetAsync(de.p, 0, 4, g.stream), "cudaMemsetAsync");
-        launchTraceClosestRays(makeDevScene(), dr.p, n, di.p, dt.p, de.p, g.stream);
+        launchTraceClosestRays(makeDevScene(), dr.p, n, di.p, dt.p, de.p, lanesPerRay, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "trace");
         ck(cudaMemcpyAsync(outTri, di.p, sizeof(int) * n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
@@ -1246,24 +1253,35 @@ int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv)
     });
 }
 
-int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* outOccluded)
+int bte_trace_occluded_lanes(const float* rays, const float* tmax, int n, int lanesPerRay, uint8_t* outOccluded)
 {
     return guarded([&] {
         if (n <= 0) return 0;
         if (!g.accelReady) throw CudaError{"bte_trace_occluded: no acceleration structure"};
+        checkLanes(lanesPerRay);
         Tmp<float> dr(6 * static_cast<size_t>(n)), dm(n);
         Tmp<uint8_t> dout(n);
         Tmp<unsigned int> de(1);
         ck(cudaMemcpyAsync(dr.p, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
         ck(cudaMemcpyAsync(dm.p, tmax, sizeof(float) * n, cudaMemcpyHostToDevice, g.stream), "cudaMemcpyAsync");
         ck(cudaMemsetAsync(de.p, 0, 4, g.stream), "cudaMemsetAsync");
-        launchTraceOccludedRays(makeDevScene(), dr.p, dm.p, n, dout.p, de.p, g.stream);
+        launchTraceOccludedRays(makeDevScene(), dr.p, dm.p, n, dout.p, de.p, lanesPerRay, g.stream);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(g.stream), "trace");
         ck(cudaMemcpyAsync(outOccluded, dout.p, n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         checkTraceFlags(de.p);
         return 0;
     });
+}
+
+int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv)
+{
+    return bte_trace_closest_lanes(rays, n, 1, outTri, outTuv);
+}
+
+int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* outOccluded)
+{
+    return bte_trace_occluded_lanes(rays, tmax, n, 1, outOccluded);
 }
 
 int bte_env_query(int op, const float* in, int n, float* out)

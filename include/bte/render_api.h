@@ -178,6 +178,10 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
 /* closest hit for n rays [origin, dir] (host arrays): triangle index (-1 miss) and t, u, v */
 int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv);
 int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* outOccluded);
+/* The same with the walk chosen: lanesPerRay 1 (one lane per ray, the walk of the bulk of a frame) or
+ * 8 (eight lanes per ray, the walk of the last bounces; needs the 8-wide tree).  Same results. */
+int bte_trace_closest_lanes(const float* rays, int n, int lanesPerRay, int* outTri, float* outTuv);
+int bte_trace_occluded_lanes(const float* rays, const float* tmax, int n, int lanesPerRay, uint8_t* outOccluded);
 /* env-map queries through the device tables */
 int bte_env_query(int op, const float* in, int n, float* out);   /* op 0 eval, 1 pdf, 2 sample */
 int bte_env_tables(float* marginal, float* conditional, float* totalPower);      /* CDF mode tables */

@@ -62,8 +62,9 @@ def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1
 @pytest.mark.parametrize("scene_name", ["cornell_scene", "random_scene"])
 def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, tree):
     """Closest hit (triangle, t, u, v) and any-hit occlusion for 40k rays, both tree widths, several
-    leaf sizes and both hierarchy builders (Morton-prefix splits; PLOC at several search radii), against
-    the oracle's brute force over all triangles."""
+    leaf sizes and both hierarchy builders (Morton-prefix splits; PLOC at several search radii), with one
+    lane per ray and (8-wide tree) eight lanes per ray, against the oracle's brute force over all
+    triangles."""
     scene = request.getfixturevalue(scene_name)
     _upload(renderer, scene, bvh_width=tree[0], max_leaf=tree[1], builder=tree[2], radius=tree[3])
     info = renderer.accel_info()
@@ -91,6 +92,15 @@ def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, t
     orc.lib.or_trace_occluded(view.ptr(), rays.ctypes.data_as(C.c_void_p), tmax.ctypes.data_as(C.c_void_p),
                               len(rays), oo.ctypes.data_as(C.c_void_p))
     assert np.array_equal(go, oo)
+    if tree[0] == 8:   # the eight-lanes-per-ray walk of the last bounces, on the same rays
+        g8, g8uv = renderer.trace_closest(rays, lanes=8)
+        assert np.array_equal(g8, ot), f"{np.sum(g8 != ot)} triangle mismatches (8 lanes per ray)"
+        assert np.array_equal(bits(g8uv[hit]), bits(otuv[hit]))
+        assert np.array_equal(renderer.trace_occluded(rays, tmax, lanes=8), oo)
+    else:
+        import bluetruthengine_b200 as B
+        with pytest.raises(B.BteError):
+            renderer.trace_closest(rays[:4], lanes=8)
 
 
 def _render_and_compare(renderer, oracle_mod, scene, env_mode, spp, depth, frames=1, sort_shading=0, tail_paths=0):
