@@ -688,7 +688,8 @@ void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, in
 void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block,
                  int minBlocks, cudaStream_t st)
 {
-    if (minBlocks == 3) kShade<3><<<grid, block, 0, st>>>(s, P, f, bounce);
+    if (minBlocks == 4) kShade<4><<<grid, block, 0, st>>>(s, P, f, bounce);
+    else if (minBlocks == 3) kShade<3><<<grid, block, 0, st>>>(s, P, f, bounce);
     else kShade<2><<<grid, block, 0, st>>>(s, P, f, bounce);
 }
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
@@ -767,6 +768,7 @@ int occupancyGrid(int which, int block)
     const void* fn = which == 0 ? reinterpret_cast<const void*>(kExtend<2>)
                    : which == 1 ? reinterpret_cast<const void*>(kShade<2>)
                    : which == 3 ? reinterpret_cast<const void*>(kShade<3>)
+                   : which == 6 ? reinterpret_cast<const void*>(kShade<4>)
                    : which == 4 ? reinterpret_cast<const void*>(kExtendWide)
                    : which == 5 ? reinterpret_cast<const void*>(kConnectWide)
                                 : reinterpret_cast<const void*>(kConnect<2>);

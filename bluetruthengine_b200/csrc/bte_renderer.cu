@@ -361,7 +361,7 @@ void renderFrame(int w, int h)
     const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
     if (g.gridBlock != block) {
         g.gridExtend = occupancyGrid(g.builtWidth == 8 ? 4 : 0, block);
-        g.gridShade = occupancyGrid(g.shadeMinBlocks == 3 ? 3 : 1, block);
+        g.gridShade = occupancyGrid(g.shadeMinBlocks == 4 ? 6 : g.shadeMinBlocks == 3 ? 3 : 1, block);
         g.gridConnect = occupancyGrid(g.builtWidth == 8 ? 5 : 2, block);
         g.gridBlock = block;
     }
@@ -567,7 +567,7 @@ void renderViews(const BteView* views, int count)
     const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
     if (g.gridBlock != block) {
         g.gridExtend = occupancyGrid(g.builtWidth == 8 ? 4 : 0, block);
-        g.gridShade = occupancyGrid(g.shadeMinBlocks == 3 ? 3 : 1, block);
+        g.gridShade = occupancyGrid(g.shadeMinBlocks == 4 ? 6 : g.shadeMinBlocks == 3 ? 3 : 1, block);
         g.gridConnect = occupancyGrid(g.builtWidth == 8 ? 5 : 2, block);
         g.gridBlock = block;
     }
@@ -1084,7 +1084,7 @@ int bte_set_tuning(const BteTuning* t)
         const int leafMax = t->bvhWidth == 8 ? kWideLeafMax : kMaxLeafTris;
         if (t->maxLeafTriangles < 1 || t->maxLeafTriangles > leafMax)
             throw CudaError{"bte_set_tuning: maxLeafTriangles must be in [1, 64] (binary) or [1, 3] (8-wide)"};
-        if (t->shadeMinBlocks != 2 && t->shadeMinBlocks != 3) throw CudaError{"bte_set_tuning: shadeMinBlocks must be 2 or 3"};
+        if (t->shadeMinBlocks < 2 || t->shadeMinBlocks > 4) throw CudaError{"bte_set_tuning: shadeMinBlocks must be 2, 3 or 4"};
         if (t->postponePercent < 0 || t->postponePercent > 100) throw CudaError{"bte_set_tuning: postponePercent in [0, 100]"};
         if (t->sortShading != 0 && t->sortShading != 1) throw CudaError{"bte_set_tuning: sortShading must be 0 or 1"};
         if (t->tailPaths < 0) throw CudaError{"bte_set_tuning: tailPaths must be >= 0"};

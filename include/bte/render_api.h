@@ -132,7 +132,7 @@ int bte_read_aov(float* hostAlbedoNormal);
 typedef struct {
     int bvhWidth;          /* 2: binary LBVH; 8: 8-wide tree with 8-bit quantised child boxes */
     int maxLeafTriangles;  /* 1-64 (binary tree), 1-3 (8-wide tree) */
-    int shadeMinBlocks;    /* resident blocks per SM the shade kernel is compiled for: 2 or 3 */
+    int shadeMinBlocks;    /* resident blocks per SM the shade kernel is compiled for: 2, 3 or 4 */
     int postponePercent;   /* 8-wide walk: a lane defers its leaf tests while fewer than this
                             * percentage of the warp's lanes have leaf tests (0 = never, 0-100) */
     int sortShading;       /* 1: extend buckets paths by hit material (miss, BSDF type) and shade runs the
