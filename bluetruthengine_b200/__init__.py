@@ -72,7 +72,10 @@ class _SceneArrays(C.Structure):
                 ("emitterTriCdfCount", C.c_int), ("sceneEmitterCdf", C.c_void_p), ("spotlights", C.c_void_p),
                 ("spotlightCount", C.c_int), ("envRGBA", C.c_void_p), ("envWidth", C.c_int), ("envHeight", C.c_int),
                 ("envIntensity", C.c_float), ("envRotationDeg", C.c_float), ("camera", C.c_ubyte * 56),
-                ("width", C.c_int), ("height", C.c_int)]
+                ("width", C.c_int), ("height", C.c_int),
+                ("albedoPixels", C.POINTER(C.c_void_p)), ("albedoWidths", C.POINTER(C.c_int)),
+                ("albedoHeights", C.POINTER(C.c_int)), ("mrPixels", C.POINTER(C.c_void_p)),
+                ("mrWidths", C.POINTER(C.c_int)), ("mrHeights", C.POINTER(C.c_int))]
 
 
 def library_path() -> str:
@@ -139,10 +142,25 @@ class Scene:
     camera: np.ndarray              # CAMERA_DTYPE scalar
     width: int
     height: int
+    albedo_textures: list = None    # per material: uint8 [H,W,4] or None
+    mr_textures: list = None        # per material: uint8 [H,W,4] or None (metallic-roughness maps)
 
     @property
     def triangle_count(self) -> int:
         return int(self.triangles.shape[0])
+
+
+def decode_image(data: bytes) -> np.ndarray:
+    """PNG / JPEG bytes -> uint8 [H,W,4] (the library's texture decoder; no GPU needed)."""
+    lib = load_library()
+    buf = np.frombuffer(data, dtype=np.uint8)
+    w, h, c = C.c_int(), C.c_int(), C.c_int()
+    _check(lib.bte_image_decode(_ptr(buf), C.c_longlong(len(buf)), None, C.c_longlong(0), C.byref(w), C.byref(h),
+                                C.byref(c)))
+    out = np.empty((h.value, w.value, 4), dtype=np.uint8)
+    _check(lib.bte_image_decode(_ptr(buf), C.c_longlong(len(buf)), _ptr(out), C.c_longlong(out.size), C.byref(w),
+                                C.byref(h), C.byref(c)))
+    return out
 
 
 def load_scene(path: str) -> Scene:
@@ -159,6 +177,18 @@ def load_scene(path: str) -> Scene:
             env = _view(a.envRGBA, np.float32, a.envWidth * a.envHeight * 4).reshape(a.envHeight, a.envWidth, 4)
         cam = np.frombuffer(bytes(a.camera), dtype=CAMERA_DTYPE, count=1)[0].copy()
         E = a.emitterCount
+
+        def images(px, ws, hs):
+            out = []
+            for i in range(a.materialCount):
+                if not px or not px[i]:
+                    out.append(None)
+                else:
+                    out.append(_view(px[i], np.uint8, ws[i] * hs[i] * 4).reshape(hs[i], ws[i], 4))
+            return out
+
+        albedo = images(a.albedoPixels, a.albedoWidths, a.albedoHeights)
+        mr = images(a.mrPixels, a.mrWidths, a.mrHeights)
         return Scene(
             triangles=_view(a.triangles, TRIANGLE_DTYPE, T),
             materials=_view(a.materials, np.float32, 3 * a.materialCount).reshape(-1, 3),
@@ -173,7 +203,7 @@ def load_scene(path: str) -> Scene:
             scene_emitter_cdf=_view(a.sceneEmitterCdf, np.float32, E + 1 if E > 0 else 1),
             spotlights=_view(a.spotlights, SPOT_DTYPE, a.spotlightCount),
             env_rgba=env, env_intensity=float(a.envIntensity), env_rotation_deg=float(a.envRotationDeg),
-            camera=cam, width=int(a.width), height=int(a.height))
+            camera=cam, width=int(a.width), height=int(a.height), albedo_textures=albedo, mr_textures=mr)
     finally:
         lib.bte_scene_free(h)
 
@@ -261,8 +291,9 @@ class Renderer:
     def upload(self, scene: Scene):
         """All uploads in the order of src/main.cpp:819-930."""
         self.init_camera(scene.camera)
-        self.init_textures(None)
-        self.init_mr_textures(None)
+        any_tex = lambda ims: ims is not None and any(im is not None for im in ims)
+        self.init_textures(scene.albedo_textures if any_tex(scene.albedo_textures) else None)
+        self.init_mr_textures(scene.mr_textures if any_tex(scene.mr_textures) else None)
         self.init_scene(scene.triangles, scene.materials, scene.triangle_material_ids, scene.width, scene.height)
         self.init_accel()
         self.init_triangle_emission(scene.triangle_emission)

@@ -25,9 +25,19 @@ struct SceneData {
     float envIntensity = 1.0f, envRotationDeg = 0.0f;
     CameraData camera{};
     int width = 0, height = 0;
+    // per material: RGBA8 albedo and metallic-roughness images (empty: none), as
+    // src/main.cpp:603-612 builds them for cudaInitTextures / cudaInitMrTextures
+    std::vector<std::vector<uint8_t>> albedoImages, mrImages;
+    std::vector<int> albedoWidths, albedoHeights, mrWidths, mrHeights;
 };
 
 int sceneLoad(const char* path, SceneData& out, std::string& err);
+
+// PNG / JPEG file or bytes -> RGBA8 rows top to bottom (bte_image.cpp); false with `err` on failure.
+bool decodeImageRGBA8(const uint8_t* data, size_t size, std::vector<uint8_t>& rgba, int& width, int& height,
+                      int& channelsInFile, std::string& err);
+bool loadImageRGBA8(const std::string& path, std::vector<uint8_t>& rgba, int& width, int& height, int& channelsInFile,
+                    std::string& err);
 
 void setError(const std::string& msg);
 

@@ -617,10 +617,36 @@ int sceneLoad(const char* path, SceneData& S, std::string& err)
             S.camera.aspect = static_cast<float>(d.width) / static_cast<float>(d.height);
         }
         for (size_t i = 0; i < d.materials.size(); ++i) {
-            if (!d.materials[i].albedoTexture.empty())
-                std::fprintf(stderr, "[bte] albedoTexture \"%s\" is not decoded by this build; using the BSDF colour\n",
-                             d.materials[i].albedoTexture.c_str());
-            S.materials.push_back({1.0f, 1.0f, 1.0f});
+            // loadTextureAverage + loadImageRGBA, src/main.cpp:407-470 and :600-612: the material colour is the
+            // texture's mean (per-pixel value / 255 summed in double, divided by the pixel count), white when
+            // there is no texture or it fails to load; the image itself becomes the material's albedo texture.
+            Float3 colour = {1.0f, 1.0f, 1.0f};
+            std::vector<uint8_t> px;
+            int tw = 1, th = 1, tc = 0;
+            const std::string& tex = d.materials[i].albedoTexture;
+            if (!tex.empty()) {
+                std::string e2;
+                if (loadImageRGBA8(resolve(sp, tex), px, tw, th, tc, e2)) {
+                    double acc[3] = {0.0, 0.0, 0.0};
+                    const size_t np = static_cast<size_t>(tw) * th;
+                    for (size_t k = 0; k < np; ++k)
+                        for (int c = 0; c < 3; ++c) acc[c] += px[4 * k + c] / 255.0;
+                    colour = {static_cast<float>(acc[0] / static_cast<double>(np)),
+                              static_cast<float>(acc[1] / static_cast<double>(np)),
+                              static_cast<float>(acc[2] / static_cast<double>(np))};
+                } else {
+                    std::fprintf(stderr, "[bte] texture %s; material will use its BSDF colour\n", e2.c_str());
+                    px.clear();
+                    tw = th = 1;
+                }
+            }
+            S.materials.push_back(colour);
+            S.albedoImages.push_back(std::move(px));
+            S.albedoWidths.push_back(tw);
+            S.albedoHeights.push_back(th);
+            S.mrImages.emplace_back();   // XML materials have no metallic-roughness map
+            S.mrWidths.push_back(1);
+            S.mrHeights.push_back(1);
         }
         if (d.modelCount > 0)
             std::fprintf(stderr, "[bte] %d <model> (glTF) entries skipped: glTF loading is not part of this build\n",

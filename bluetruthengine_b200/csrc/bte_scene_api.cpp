@@ -6,6 +6,7 @@
 
 struct BteScene {
     bte::SceneData data;
+    std::vector<const uint8_t*> albedoPtrs, mrPtrs;
 };
 
 extern "C" {
@@ -48,6 +49,15 @@ int bte_scene_arrays(const BteScene* scene, BteSceneArrays* o)
     o->envIntensity = d.envIntensity; o->envRotationDeg = d.envRotationDeg;
     o->camera = d.camera;
     o->width = d.width; o->height = d.height;
+    BteScene* s = const_cast<BteScene*>(scene);
+    s->albedoPtrs.clear();
+    s->mrPtrs.clear();
+    for (const auto& im : d.albedoImages) s->albedoPtrs.push_back(im.empty() ? nullptr : im.data());
+    for (const auto& im : d.mrImages) s->mrPtrs.push_back(im.empty() ? nullptr : im.data());
+    o->albedoPixels = s->albedoPtrs.empty() ? nullptr : s->albedoPtrs.data();
+    o->albedoWidths = d.albedoWidths.data(); o->albedoHeights = d.albedoHeights.data();
+    o->mrPixels = s->mrPtrs.empty() ? nullptr : s->mrPtrs.data();
+    o->mrWidths = d.mrWidths.data(); o->mrHeights = d.mrHeights.data();
     return 0;
 }
 
@@ -60,8 +70,15 @@ int bte_scene_upload(const BteScene* scene)
     const bte::SceneData& d = scene->data;
     const int T = static_cast<int>(d.triangles.size());
     int rc = bte_init_camera(&d.camera);
-    if (rc == 0) rc = bte_init_textures(nullptr, nullptr, nullptr, 0);
-    if (rc == 0) rc = bte_init_mr_textures(nullptr, nullptr, nullptr, 0);
+    {   // uploadLayer, src/main.cpp:819-838: one entry per material, NULL where it has no image
+        std::vector<const uint8_t*> a, m;
+        for (const auto& im : d.albedoImages) a.push_back(im.empty() ? nullptr : im.data());
+        for (const auto& im : d.mrImages) m.push_back(im.empty() ? nullptr : im.data());
+        if (rc == 0) rc = bte_init_textures(a.empty() ? nullptr : a.data(), d.albedoWidths.data(), d.albedoHeights.data(),
+                                            static_cast<int>(a.size()));
+        if (rc == 0) rc = bte_init_mr_textures(m.empty() ? nullptr : m.data(), d.mrWidths.data(), d.mrHeights.data(),
+                                               static_cast<int>(m.size()));
+    }
     if (rc == 0) rc = bte_init_scene(d.triangles.data(), T, d.materials.data(), static_cast<int>(d.materials.size()),
                                      d.triangleMaterialIds.data(), d.width, d.height);
     if (rc == 0) rc = bte_init_accel();

@@ -228,7 +228,16 @@ typedef struct {
     const float* envRGBA; int envWidth, envHeight; float envIntensity, envRotationDeg;
     CameraData camera;
     int width, height;
+    /* per material (count = materialCount): RGBA8 albedo / metallic-roughness images, NULL where a material
+     * has none, with their sizes (1 x 1 for none): the arguments of bte_init_textures / bte_init_mr_textures */
+    const uint8_t* const* albedoPixels; const int* albedoWidths; const int* albedoHeights;
+    const uint8_t* const* mrPixels; const int* mrWidths; const int* mrHeights;
 } BteSceneArrays;
+/* PNG or JPEG bytes -> RGBA8, rows top to bottom, the decoding stbi_load(..., 4) gives the reference's
+ * textures (src/main.cpp:407-470).  With outRGBA NULL only the size and the file's channel count are
+ * returned; otherwise `capacity` must hold width*height*4 bytes. */
+int bte_image_decode(const uint8_t* bytes, long long size, uint8_t* outRGBA, long long capacity, int* width,
+                     int* height, int* channelsInFile);
 int bte_scene_load(const char* scenePath, BteScene** out);
 int bte_scene_arrays(const BteScene* scene, BteSceneArrays* out);
 void bte_scene_free(BteScene* scene);

@@ -6,13 +6,17 @@
  * transforms (include/mesh_transform.h), glued as src/main.cpp:267-401 and
  * :629-758 flatten a scene (that glue is restated here because main.cpp also
  * pulls in the window/GL stack).  Produces the flattened triangle, BSDF and
- * emitter arrays for comparison with the product's loader.
+ * emitter arrays for comparison with the product's loader, and per material
+ * the texture colour and RGBA8 image of loadTextureAverage / loadImageRGBA
+ * (src/main.cpp:407-470) through the reference's vendored stb_image.
  * Built by oracle/Makefile into oracle/_ref/libbteref_loader.so.
  */
 #include "scene.h"
 #include "mesh_transform.h"
 #define TINYOBJLOADER_IMPLEMENTATION
 #include "tiny_obj_loader.h"
+#define STB_IMAGE_IMPLEMENTATION
+#include "stb_image.h"
 
 #include <cmath>
 #include <cstring>
@@ -27,6 +31,9 @@ std::vector<BsdfData> g_bsdfs;
 std::vector<int> g_triBsdf, g_triMat, g_emTri;
 std::vector<float> g_emCdf, g_sceneCdf, g_cam;
 std::vector<uint8_t> g_flags;
+std::vector<float> g_matColour;                 // 3 per material
+std::vector<std::vector<uint8_t>> g_matImage;   // RGBA8 per material (empty: none)
+std::vector<int> g_matW, g_matH;
 
 std::string resolve(const std::string& scenePath, const std::string& p)
 {
@@ -101,6 +108,31 @@ REF_API int refl_load(const char* scenePath)
     g_tris.clear(); g_bsdfs.clear(); g_triBsdf.clear(); g_triMat.clear(); g_emTri.clear(); g_emCdf.clear();
     g_sceneCdf.clear(); g_flags.clear(); g_cam.clear();
     const SceneDescription d = loadSceneDescription(scenePath);   // src/scene.cpp:83
+    g_matColour.clear(); g_matImage.clear(); g_matW.clear(); g_matH.clear();
+    for (const auto& m : d.materials) {   // src/main.cpp:407-470, :600-612
+        float col[3] = {1.0f, 1.0f, 1.0f};
+        std::vector<uint8_t> img;
+        int w = 1, h = 1, ch = 0;
+        if (!m.albedoTexture.empty()) {
+            // the path as written, relative to the working directory (main.cpp passes it to stbi_load unchanged)
+            unsigned char* px = stbi_load(m.albedoTexture.c_str(), &w, &h, &ch, 4);
+            if (px) {
+                double acc[4] = {0.0, 0.0, 0.0, 0.0};
+                const int total = w * h;
+                for (int i = 0; i < total; ++i)
+                    for (int c = 0; c < 4; ++c) acc[c] += px[4 * i + c] / 255.0;
+                for (int c = 0; c < 3; ++c) col[c] = (float)(acc[c] / (double)total);
+                img.assign(px, px + (size_t)total * 4);
+                stbi_image_free(px);
+            } else {
+                w = h = 1;
+            }
+        }
+        g_matColour.insert(g_matColour.end(), col, col + 3);
+        g_matImage.push_back(img);
+        g_matW.push_back(w);
+        g_matH.push_back(h);
+    }
     for (const auto& b : d.bsdfs) {   // src/main.cpp:629-665
         BsdfData x{};
         if (b.type == "diffuse") { x.type = BSDF_Diffuse; x.p0 = {b.albedoR, b.albedoG, b.albedoB, 0.0f}; }
@@ -153,6 +185,19 @@ REF_API int refl_load(const char* scenePath)
     g_cam = {c.eyeX, c.eyeY, c.eyeZ, c.lookAtX, c.lookAtY, c.lookAtZ, c.upX, c.upY, c.upZ, c.fovYDegrees,
              (float)d.windowWidth, (float)d.windowHeight, d.envMapIntensity, d.envMapRotation, (float)d.spotlights.size()};
     return (int)g_tris.size();
+}
+
+REF_API int refl_material_count(void) { return (int)g_matW.size(); }
+
+// colour[3], image size; returns 1 when the material has an image (copied to `rgba` when non-null)
+REF_API int refl_material(int i, float* colour, int* w, int* h, uint8_t* rgba)
+{
+    std::memcpy(colour, &g_matColour[3 * (size_t)i], 3 * sizeof(float));
+    *w = g_matW[(size_t)i];
+    *h = g_matH[(size_t)i];
+    if (g_matImage[(size_t)i].empty()) return 0;
+    if (rgba) std::memcpy(rgba, g_matImage[(size_t)i].data(), g_matImage[(size_t)i].size());
+    return 1;
 }
 
 REF_API int refl_counts(int* out)

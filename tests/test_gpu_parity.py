@@ -7,6 +7,8 @@ t/u/v, per-sample radiance, accumulation buffers and packed pixels.  Against
 the reference's own headers compiled with glibc math the tolerance is the
 north-star one, 1e-4 relative per sample.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -330,6 +332,34 @@ def test_textured_materials_bitexact(renderer, oracle_mod, random_scene):
     assert eq.all(), f"{np.sum(~eq)} of {len(o)} samples differ"
     renderer.init_textures(None)
     renderer.init_mr_textures(None)
+
+
+def test_loader_textured_scene_bitexact(renderer, oracle_mod, bte, tmp_path):
+    """A scene.xml whose materials name PNG / JPEG albedo textures: the loader decodes them, the upload hands
+    them to bte_init_textures per material (src/main.cpp:819-838), and the frame equals the oracle's."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__)))
+    from test_image import _textured_cornell
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "images", "fixtures.npz"))
+    fx = (z, [str(n) for n in z["names"]], None)
+    path = _textured_cornell(tmp_path, fx, {"whiteMat": ("jstb_q90_75x100", "jpg"), "redMat": ("rgb8i_48x64", "png")})
+    sc = bte.load_scene(path)
+    assert sc.albedo_textures[0] is not None and sc.albedo_textures[1] is not None
+    W, H, spp, depth = sc.width, sc.height, 1, 8
+    _upload(renderer, sc, env_mode=0, spp=spp, depth=depth)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    g = renderer.read_sample_radiance(W * H * spp)
+    orc = oracle_mod.Oracle(libm=False)
+    view = oracle_mod.SceneView(sc, env_mode=0, oracle=orc, textures=sc.albedo_textures)
+    pix = np.arange(W * H, dtype=np.uint32)
+    o, _, _ = oracle_mod.render_samples(orc.lib, view, sc.camera, W, H, depth, pix, np.zeros(W * H, np.uint32))
+    plain = oracle_mod.SceneView(sc, env_mode=0, oracle=orc)
+    p, _, _ = oracle_mod.render_samples(orc.lib, plain, sc.camera, W, H, depth, pix, np.zeros(W * H, np.uint32))
+    assert not np.array_equal(bits(o), bits(p)), "textures had no effect"
+    eq = np.all(bits(g) == bits(o), axis=1)
+    assert eq.all(), f"{np.sum(~eq)} of {len(o)} samples differ"
+    renderer.init_textures(None)
 
 
 def test_tuning_roundtrip_and_validation(renderer):
