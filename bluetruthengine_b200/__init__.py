@@ -163,6 +163,18 @@ def decode_image(data: bytes) -> np.ndarray:
     return out
 
 
+def encode_png(rgba: np.ndarray) -> bytes:
+    """uint8 [H,W,4] (first row first) -> PNG bytes (the library's encoder; no GPU needed)."""
+    lib = load_library()
+    a = np.ascontiguousarray(rgba, dtype=np.uint8)
+    h, w = a.shape[:2]
+    n = C.c_longlong()
+    _check(lib.bte_encode_png(_ptr(a), w, h, None, C.c_longlong(0), C.byref(n)))
+    out = np.empty(n.value, dtype=np.uint8)
+    _check(lib.bte_encode_png(_ptr(a), w, h, _ptr(out), C.c_longlong(n.value), C.byref(n)))
+    return out.tobytes()
+
+
 def load_scene(path: str) -> Scene:
     """Parse scene.xml + OBJ (+ .hdr) with the library's loader (no GPU needed)."""
     lib = load_library()
@@ -404,6 +416,32 @@ class Renderer:
 
     def set_frame_index(self, i: int):
         _check(self.lib.bte_set_frame_index(C.c_uint32(i)))
+
+    # ---- headless output ----
+    def write_png(self, path: str):
+        _check(self.lib.bte_write_png(str(path).encode()))
+
+    def capture_screenshot(self) -> str:
+        buf = C.create_string_buffer(64)
+        _check(self.lib.bte_capture_screenshot(buf, 64))
+        return buf.value.decode()
+
+    def record_start(self, raw_path: Optional[str] = None, fps: int = 30):
+        _check(self.lib.bte_record_start(None if raw_path is None else str(raw_path).encode(), int(fps)))
+
+    def record_frame(self):
+        _check(self.lib.bte_record_frame())
+
+    def record_stop(self):
+        _check(self.lib.bte_record_stop())
+
+    def mark_scene_changed(self):
+        _check(self.lib.bte_mark_scene_changed())
+
+    def framebuffer_size(self):
+        w, h = C.c_int(), C.c_int()
+        _check(self.lib.bte_get_framebuffer_size(C.byref(w), C.byref(h)))
+        return w.value, h.value
 
     def read_framebuffer(self, width, height) -> np.ndarray:
         out = np.empty(width * height, dtype=np.uint32)

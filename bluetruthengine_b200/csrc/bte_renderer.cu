@@ -100,6 +100,7 @@ struct Renderer {
     int plocRadius = 8;       // PLOC neighbour search radius (8 measured best of 8/16/32)
     int builtBuilder = 0;     // hierarchy in use
     int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
+    bool sceneChanged = false;   // bte_mark_scene_changed: the next bte_render resets accumulation first
     int builtWidth = 2;       // tree in use
     int accelNodes = 0, accelDepth = 0;
     int shadeMinBlocks = 3;   // autotuned on B200: 3 resident shade blocks per SM
@@ -939,7 +940,26 @@ int bte_reset_accumulation(int imageWidth, int imageHeight)
 int bte_render(int imageWidth, int imageHeight)
 {
     return guarded([&] {
+        if (g.sceneChanged) {   // src/main.cpp:947-952: reset before the frame that follows a change
+            ensureAccum(imageWidth, imageHeight);
+            g.sceneChanged = false;
+        }
         renderFrame(imageWidth, imageHeight);
+        return 0;
+    });
+}
+
+int bte_mark_scene_changed(void)
+{
+    return guarded([&] { g.sceneChanged = true; return 0; });
+}
+
+int bte_get_framebuffer_size(int* width, int* height)
+{
+    return guarded([&] {
+        if (!g.framebuffer.p) throw CudaError{"bte_get_framebuffer_size: nothing rendered"};
+        if (width) *width = g.accumW;
+        if (height) *height = g.accumH;
         return 0;
     });
 }

@@ -210,6 +210,24 @@ int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* 
 int bte_env_build_alias_noalloc(const float* dTexelsRGBA, int width, int height, float* dRowProb, int* dRowAlias,
                                 float* dColProb, int* dColAlias, float* dPixelPdf, double* dTotalPower, void* stream);
 
+/* ---- headless output (replaces the window of src/main.cpp: screenshots :118-142, recording :72-116 and
+ * :990-997, the scene-changed reset of :947-952) ---- */
+int bte_get_framebuffer_size(int* width, int* height);   /* of the last frame's packed RGBA8 framebuffer */
+int bte_mark_scene_changed(void);    /* markSceneChanged: the next bte_render resets accumulation first */
+/* The last frame as a PNG, top row first (the framebuffer's row 0 is the bottom row, as in the reference's
+ * pixel buffer; captureScreenshot flips it the same way). */
+int bte_write_png(const char* path);
+/* captureScreenshot: screenshot_0000.png, _0001, ... in the working directory; the name goes to nameOut. */
+int bte_capture_screenshot(char* nameOut, int nameCapacity);
+/* startRecording / per-frame capture / stopRecording.  rawPath NULL: the reference's FFmpeg pipe (output.mp4,
+ * H.264, `fps` playback); otherwise raw RGBA frames, rows bottom first, appended to that file per call of
+ * bte_record_frame. */
+int bte_record_start(const char* rawPath, int fps);
+int bte_record_frame(void);
+int bte_record_stop(void);
+/* RGBA8 rows (first row first) -> PNG bytes; with out NULL only *size is set. */
+int bte_encode_png(const uint8_t* rgba, int width, int height, uint8_t* out, long long capacity, long long* size);
+
 /* ---- scene.xml / OBJ loader (src/scene.cpp:83-523, src/main.cpp:267-930) ---- */
 typedef struct BteScene BteScene;
 typedef struct {

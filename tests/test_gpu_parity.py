@@ -362,6 +362,41 @@ def test_loader_textured_scene_bitexact(renderer, oracle_mod, bte, tmp_path):
     renderer.init_textures(None)
 
 
+def test_headless_output(renderer, bte, cornell_scene, tmp_path, monkeypatch):
+    """Screenshots (top row first, src/main.cpp:118-142), raw recording frames (rows bottom first, as the
+    reference pipes them to FFmpeg, :990-997) and the scene-changed reset (:947-952)."""
+    from conftest import bits
+    sc = cornell_scene
+    W, H = sc.width, sc.height
+    _upload(renderer, sc, env_mode=0, spp=1, depth=6)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    first = renderer.read_accum(W, H).copy()
+    fb = renderer.read_framebuffer(W, H)
+    rgba = fb.view(np.uint8).reshape(H, W, 4)
+    assert renderer.framebuffer_size() == (W, H)
+    p = tmp_path / "frame.png"
+    renderer.write_png(str(p))
+    assert np.array_equal(bte.decode_image(p.read_bytes()), rgba[::-1])
+    monkeypatch.chdir(tmp_path)
+    assert renderer.capture_screenshot() == "screenshot_0000.png"
+    assert renderer.capture_screenshot() == "screenshot_0001.png"
+    assert np.array_equal(bte.decode_image((tmp_path / "screenshot_0001.png").read_bytes()), rgba[::-1])
+    raw = tmp_path / "frames.rgba"
+    renderer.record_start(str(raw))
+    frames = []
+    for _ in range(2):
+        renderer.render(W, H)
+        renderer.record_frame()
+        frames.append(renderer.read_framebuffer(W, H).view(np.uint8).copy())
+    renderer.record_stop()
+    data = np.frombuffer(raw.read_bytes(), np.uint8)
+    assert data.size == 2 * W * H * 4 and np.array_equal(data, np.concatenate(frames))
+    renderer.mark_scene_changed()
+    renderer.render(W, H)
+    assert np.array_equal(bits(renderer.read_accum(W, H)), bits(first))
+
+
 def test_tuning_roundtrip_and_validation(renderer):
     """bte_set_tuning / bte_get_tuning: values round-trip; out-of-range values are rejected with a message."""
     import bluetruthengine_b200 as B

@@ -171,3 +171,64 @@ def test_textured_materials_match_reference_loader(bte, tmp_path, fixtures):
             assert sc.albedo_textures[i] is None
     assert sc.albedo_textures[3] is None and np.array_equal(sc.materials[3], [1, 1, 1])
     assert all(m is None for m in sc.mr_textures)
+
+
+def _png_pixels_via_zlib(png: bytes) -> np.ndarray:
+    """A third decoder for our own files (RGBA8, non-interlaced): Python's zlib and the five filters."""
+    import struct
+    import zlib
+    assert png[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat = 8, b""
+    w = h = 0
+    while pos < len(png):
+        n, t = struct.unpack(">I4s", png[pos:pos + 8])
+        data = png[pos + 8:pos + 8 + n]
+        assert struct.unpack(">I", png[pos + 8 + n:pos + 12 + n])[0] == zlib.crc32(t + data) & 0xffffffff
+        if t == b"IHDR":
+            w, h, depth, color = struct.unpack(">IIBB", data[:10])
+            assert (depth, color) == (8, 6)
+        elif t == b"IDAT":
+            idat += data
+        pos += 12 + n
+    raw = zlib.decompress(idat)
+    out = np.zeros((h, w * 4), np.int64)
+    prior = np.zeros(w * 4, np.int64)
+    for y in range(h):
+        f = raw[y * (w * 4 + 1)]
+        row = np.frombuffer(raw[y * (w * 4 + 1) + 1:(y + 1) * (w * 4 + 1)], np.uint8).astype(np.int64)
+        cur = np.zeros(w * 4, np.int64)
+        for i in range(w * 4):
+            a = cur[i - 4] if i >= 4 else 0
+            b = prior[i]
+            c = prior[i - 4] if i >= 4 else 0
+            p = a + b - c
+            pa, pb, pc = abs(p - a), abs(p - b), abs(p - c)
+            pred = [0, a, b, (a + b) // 2, a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)][f]
+            cur[i] = (row[i] + pred) & 255
+        out[y] = cur
+        prior = cur
+    return out.reshape(h, w, 4).astype(np.uint8)
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (7, 5), (40, 33), (64, 128)])
+def test_png_encoder_roundtrip(bte, shape):
+    """The screenshot encoder's files decode to the exact pixels with the library's decoder, with a plain
+    zlib reader (CRCs checked), and with the reference's stb_image when it is built."""
+    import ctypes as C
+    rng = np.random.default_rng(shape[0] * 31 + shape[1])
+    h, w = shape
+    img = np.concatenate([rng.integers(0, 256, size=(h, w // 2 + 1, 4)), np.tile(rng.integers(0, 256, size=(h, 1, 4)),
+                                                                                (1, w - w // 2 - 1, 1))], 1)[:, :w]
+    img = np.ascontiguousarray(img.astype(np.uint8))
+    png = bte.encode_png(img)
+    assert np.array_equal(bte.decode_image(png), img)
+    assert np.array_equal(_png_pixels_via_zlib(png), img)
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libstbref.so")
+    if os.path.exists(lib_path):
+        ref = C.CDLL(lib_path)
+        buf = np.frombuffer(png, np.uint8)
+        out = np.empty_like(img)
+        ww, hh, cc = C.c_int(), C.c_int(), C.c_int()
+        assert ref.ref_stbi_decode_rgba(buf.ctypes.data_as(C.c_void_p), len(buf), out.ctypes.data_as(C.c_void_p),
+                                        C.c_longlong(out.size), C.byref(ww), C.byref(hh), C.byref(cc)) == 0
+        assert np.array_equal(out, img)
