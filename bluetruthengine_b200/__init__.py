@@ -175,6 +175,36 @@ def encode_png(rgba: np.ndarray) -> bytes:
     return out.tobytes()
 
 
+def load_gltf(path: str, transform=None) -> dict:
+    """A glTF / GLB model flattened as the reference's loadGltfModel does (no GPU needed).  transform: posX/Y/Z,
+    rotX/Y/Z (degrees), scaleX/Y/Z.  Returns triangles, material_ids and per material bsdf, emission,
+    is_emitter, albedo / mr images (uint8 [H,W,4] or None), and the number of outlier primitives skipped."""
+    lib = load_library()
+    h = C.c_void_p()
+    xf = None if transform is None else np.ascontiguousarray(transform, dtype=np.float32)
+    _check(lib.bte_gltf_load(str(path).encode(), _ptr(xf), C.byref(h)))
+    try:
+        t, m, sk = C.c_int(), C.c_int(), C.c_int()
+        _check(lib.bte_gltf_counts(h, C.byref(t), C.byref(m), C.byref(sk)))
+        tris = np.empty(t.value, TRIANGLE_DTYPE)
+        ids = np.empty(t.value, np.int32)
+        _check(lib.bte_gltf_triangles(h, _ptr(tris), _ptr(ids)))
+        mats = []
+        for i in range(m.value):
+            b = np.zeros(1, BSDF_DTYPE)
+            em = np.zeros(3, np.float32)
+            ie = C.c_int()
+            awh, mwh = np.zeros(2, np.int32), np.zeros(2, np.int32)
+            _check(lib.bte_gltf_material(h, i, _ptr(b), _ptr(em), C.byref(ie), _ptr(awh), _ptr(mwh), None, None))
+            alb = np.empty((awh[1], awh[0], 4), np.uint8) if awh[0] else None
+            mr = np.empty((mwh[1], mwh[0], 4), np.uint8) if mwh[0] else None
+            _check(lib.bte_gltf_material(h, i, None, None, None, None, None, _ptr(alb), _ptr(mr)))
+            mats.append({"bsdf": b[0], "emission": em, "is_emitter": bool(ie.value), "albedo": alb, "mr": mr})
+        return {"triangles": tris, "material_ids": ids, "materials": mats, "skipped_outliers": sk.value}
+    finally:
+        lib.bte_gltf_free(h)
+
+
 def load_scene(path: str) -> Scene:
     """Parse scene.xml + OBJ (+ .hdr) with the library's loader (no GPU needed)."""
     lib = load_library()

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
           "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-I", INCLUDE]
 SOURCES = ["bte_kernels.cu", "bte_bvh.cu", "bte_env.cu", "bte_renderer.cu", "bte_scene.cpp", "bte_scene_api.cpp",
-           "bte_image.cpp", "bte_output.cpp",
+           "bte_image.cpp", "bte_output.cpp", "bte_gltf.cpp",
            "bte_compat.cpp", "bte_denoise_kernels.cu", "bte_denoise_tc.cu", "bte_denoise.cu"]
 
 

@@ -320,7 +320,8 @@ void pngPixel(const PngInfo& I, const uint8_t* row, uint32_t x, uint8_t* out)
     }
 }
 
-void decodePng(const uint8_t* d, size_t n, std::vector<uint8_t>& rgba, int& w, int& h, int& channelsInFile)
+void decodePng(const uint8_t* d, size_t n, std::vector<uint8_t>& rgba, int& w, int& h, int& channelsInFile,
+               std::vector<uint8_t>* rgba16 = nullptr)
 {
     static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
     if (n < 8 || std::memcmp(d, sig, 8) != 0) bad("PNG: bad signature");
@@ -415,6 +416,47 @@ void decodePng(const uint8_t* d, size_t n, std::vector<uint8_t>& rgba, int& w, i
         bool alpha = false;
         for (int i = 0; i < I.paletteSize; ++i) alpha = alpha || I.palette[i][3] != 255;
         channelsInFile = alpha ? 4 : 3;
+    }
+    if (rgba16) {   // 16-bit samples, 4 channels (alpha 65535 where the file has none, 0 under a colour key)
+        rgba16->clear();
+        if (I.depth != 16) return;
+        rgba16->assign(static_cast<size_t>(w) * h * 8, 0);
+        auto put16 = [&](const uint8_t* row, uint32_t x, size_t o) {
+            uint16_t s[4];
+            for (int c = 0; c < I.channels; ++c) s[c] = sampleAt(row, 16, static_cast<size_t>(x) * I.channels + c);
+            uint16_t px[4];
+            if (I.color == 0) { px[0] = px[1] = px[2] = s[0]; px[3] = (I.hasKey && s[0] == I.key[0]) ? 0 : 65535; }
+            else if (I.color == 2) {
+                px[0] = s[0]; px[1] = s[1]; px[2] = s[2];
+                px[3] = (I.hasKey && s[0] == I.key[0] && s[1] == I.key[1] && s[2] == I.key[2]) ? 0 : 65535;
+            } else if (I.color == 4) { px[0] = px[1] = px[2] = s[0]; px[3] = s[1]; }
+            else { px[0] = s[0]; px[1] = s[1]; px[2] = s[2]; px[3] = s[3]; }
+            for (int c = 0; c < 4; ++c) {
+                (*rgba16)[o + 2 * c] = static_cast<uint8_t>(px[c] & 0xff);
+                (*rgba16)[o + 2 * c + 1] = static_cast<uint8_t>(px[c] >> 8);
+            }
+        };
+        if (I.interlace == 0) {
+            const size_t rb = rowBytes(I.w);
+            unfilter(raw.data(), I.h, rb, bpp);
+            for (uint32_t y = 0; y < I.h; ++y)
+                for (uint32_t x = 0; x < I.w; ++x) put16(raw.data() + y * (rb + 1) + 1, x, (static_cast<size_t>(y) * I.w + x) * 8);
+        } else {
+            size_t off = 0;
+            for (const auto& p : a7) {
+                if (I.w <= static_cast<uint32_t>(p[0]) || I.h <= static_cast<uint32_t>(p[1])) continue;
+                const uint32_t pw = (I.w - p[0] + p[2] - 1) / p[2], ph = (I.h - p[1] + p[3] - 1) / p[3];
+                if (!pw || !ph) continue;
+                const size_t rb = rowBytes(pw);
+                unfilter(raw.data() + off, ph, rb, bpp);
+                for (uint32_t j = 0; j < ph; ++j)
+                    for (uint32_t i = 0; i < pw; ++i)
+                        put16(raw.data() + off + j * (rb + 1) + 1, i,
+                              (static_cast<size_t>(p[1] + j * p[3]) * I.w + p[0] + i * p[2]) * 8);
+                off += static_cast<size_t>(ph) * (rb + 1);
+            }
+        }
+        return;
     }
     rgba.assign(static_cast<size_t>(w) * h * 4, 0);
     if (I.interlace == 0) {
@@ -955,6 +997,20 @@ bool decodeImageRGBA8(const uint8_t* data, size_t size, std::vector<uint8_t>& rg
     rgba.clear();
     width = height = channelsInFile = 0;
     return false;
+}
+
+bool decodeImageRGBA16(const uint8_t* data, size_t size, std::vector<uint8_t>& rgba16le)
+{
+    rgba16le.clear();
+    if (!(size >= 8 && data[0] == 137 && data[1] == 'P' && data[2] == 'N' && data[3] == 'G')) return false;
+    try {
+        std::vector<uint8_t> unused;
+        int w = 0, h = 0, c = 0;
+        decodePng(data, size, unused, w, h, c, &rgba16le);
+    } catch (const ImageError&) {
+        rgba16le.clear();
+    }
+    return !rgba16le.empty();
 }
 
 bool loadImageRGBA8(const std::string& path, std::vector<uint8_t>& rgba, int& width, int& height, int& channelsInFile,

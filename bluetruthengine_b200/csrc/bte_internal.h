@@ -38,6 +38,25 @@ bool decodeImageRGBA8(const uint8_t* data, size_t size, std::vector<uint8_t>& rg
                       int& channelsInFile, std::string& err);
 bool loadImageRGBA8(const std::string& path, std::vector<uint8_t>& rgba, int& width, int& height, int& channelsInFile,
                     std::string& err);
+// A 16-bit PNG as 4 channels of 16-bit samples, little-endian bytes (false for any other image).
+bool decodeImageRGBA16(const uint8_t* data, size_t size, std::vector<uint8_t>& rgba16le);
+
+// glTF / GLB model flattened as the reference's loadGltfModel does (bte_gltf.cpp).
+struct GltfSlot {
+    BsdfData bsdf{};
+    std::vector<uint8_t> albedo, mr;   // RGBA8, empty when none
+    int albedoWidth = 0, albedoHeight = 0, mrWidth = 0, mrHeight = 0;
+    Float3 emission{0.0f, 0.0f, 0.0f};
+    bool isEmitter = false;
+};
+struct GltfResult {
+    std::vector<TriangleData> triangles;
+    std::vector<int> materialIds;   // per triangle, into materials
+    std::vector<GltfSlot> materials;
+    int skippedOutliers = 0;
+};
+// xf: posX/Y/Z, rotX/Y/Z (degrees), scaleX/Y/Z of the <model> element
+bool loadGltf(const std::string& path, const float xf[9], GltfResult& out, std::string& err);
 
 void setError(const std::string& msg);
 

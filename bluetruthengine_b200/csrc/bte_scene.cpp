@@ -63,9 +63,13 @@ struct SpotDesc {
 struct CameraDesc {
     float eyeX = 0, eyeY = 0, eyeZ = 0, lookAtX = 0, lookAtY = 0, lookAtZ = 0, upX = 0, upY = 1, upZ = 0, fovY = 45;
 };
+struct ModelDesc {
+    std::string filename;
+    TransformDesc transform;
+};
 struct SceneDesc {
     std::vector<MeshDesc> meshes;
-    int modelCount = 0;
+    std::vector<ModelDesc> models;
     std::vector<MaterialDesc> materials;
     std::vector<BsdfDesc> bsdfs;
     std::vector<SpotDesc> spots;
@@ -224,12 +228,19 @@ SceneDesc parseScene(const std::string& path)
             d.meshes.push_back(m);
         }
     }
-    {   // <model> (glTF drop-ins): counted; loading them is not supported by this build
+    {   // <model> (glTF / GLB drop-ins), src/scene.cpp:274-317
         size_t from = 0;
         std::string t;
         while (nextTag(xml, "model", from, t)) {
-            if (attr(t, "filename").empty()) fail("<model> missing required attribute `filename`");
-            d.modelCount++;
+            ModelDesc m;
+            m.filename = attr(t, "filename");
+            const std::string w = "<model filename=\"" + m.filename + "\">";
+            TransformDesc& x = m.transform;
+            readOpt(t, "posX", x.posX, w); readOpt(t, "posY", x.posY, w); readOpt(t, "posZ", x.posZ, w);
+            readOpt(t, "rotX", x.rotX, w); readOpt(t, "rotY", x.rotY, w); readOpt(t, "rotZ", x.rotZ, w);
+            readOpt(t, "scaleX", x.scaleX, w); readOpt(t, "scaleY", x.scaleY, w); readOpt(t, "scaleZ", x.scaleZ, w);
+            if (m.filename.empty()) fail("<model> missing required attribute `filename`");
+            d.models.push_back(m);
         }
     }
     for (const auto& mesh : d.meshes) {
@@ -291,7 +302,7 @@ SceneDesc parseScene(const std::string& path)
         c.upX = req("upX"); c.upY = req("upY"); c.upZ = req("upZ");
         c.fovY = req("fovY");
     }
-    if (d.meshes.empty() && d.modelCount == 0) fail("no <mesh> or <model> elements found in \"" + path + "\"");
+    if (d.meshes.empty() && d.models.empty()) fail("no <mesh> or <model> elements found in \"" + path + "\"");
     if (!d.meshes.empty() && d.materials.empty()) fail("no <material ...> elements found; OBJ <mesh> entries require materials");
     if (!d.meshes.empty() && d.bsdfs.empty()) fail("no <bsdf ...> elements found; OBJ <mesh> entries require BSDFs");
     return d;
@@ -648,9 +659,6 @@ int sceneLoad(const char* path, SceneData& S, std::string& err)
             S.mrWidths.push_back(1);
             S.mrHeights.push_back(1);
         }
-        if (d.modelCount > 0)
-            std::fprintf(stderr, "[bte] %d <model> (glTF) entries skipped: glTF loading is not part of this build\n",
-                         d.modelCount);
         for (const auto& b : d.bsdfs) {   // src/main.cpp:629-665
             BsdfData x{};
             if (b.type == "diffuse") {
@@ -685,6 +693,20 @@ int sceneLoad(const char* path, SceneData& S, std::string& err)
         };
         S.sceneEmitterCdf.push_back(0.0f);
         float weightSum = 0.0f;
+        auto finishEmitter = [&](int triOff, int cdfOff, float area, const Float3& em) {   // src/main.cpp:686-701
+            const float lum = 0.2126f * em.x + 0.7152f * em.y + 0.0722f * em.z;
+            const float w = area * lum;
+            weightSum += w;
+            S.sceneEmitterCdf.push_back(weightSum);
+            EmitterData e{};
+            e.triIndexOffset = triOff;
+            e.triCount = static_cast<int>(S.emitterTriIndices.size()) - triOff;
+            e.cdfOffset = cdfOff;
+            e.radiance = em;
+            e.areaSum = area;
+            e.powerWeight = w;
+            S.emitters.push_back(e);
+        };
         for (const auto& mesh : d.meshes) {   // src/main.cpp:704-758
             const int matId = matIndex(mesh.materialName);
             std::vector<TriangleData> mt = loadTriangles(resolve(sp, mesh.filename), mesh.transform);
@@ -712,22 +734,54 @@ int sceneLoad(const char* path, SceneData& S, std::string& err)
                     S.triangleEmission.push_back({0.0f, 0.0f, 0.0f});
                 }
             }
-            if (mesh.isEmitter) {   // finishEmitter, src/main.cpp:670-686
-                const float lum = 0.2126f * em.x + 0.7152f * em.y + 0.0722f * em.z;
-                const float w = area * lum;
-                weightSum += w;
-                S.sceneEmitterCdf.push_back(weightSum);
-                EmitterData e{};
-                e.triIndexOffset = triOff;
-                e.triCount = static_cast<int>(S.emitterTriIndices.size()) - triOff;
-                e.cdfOffset = cdfOff;
-                e.radiance = em;
-                e.areaSum = area;
-                e.powerWeight = w;
-                S.emitters.push_back(e);
+            if (mesh.isEmitter) finishEmitter(triOff, cdfOff, area, em);
+        }
+        for (const auto& md : d.models) {   // glTF / GLB drop-ins, src/main.cpp:760-817
+            const TransformDesc& x = md.transform;
+            const float xf[9] = {x.posX, x.posY, x.posZ, x.rotX, x.rotY, x.rotZ, x.scaleX, x.scaleY, x.scaleZ};
+            GltfResult g;
+            std::string e2;
+            if (!loadGltf(resolve(sp, md.filename), xf, g, e2)) fail("glTF model \"" + md.filename + "\": " + e2);
+            const int matOffset = static_cast<int>(S.materials.size());
+            const int bsdfOffset = static_cast<int>(S.bsdfs.size());
+            const int firstTri = static_cast<int>(S.triangles.size());
+            for (auto& slot : g.materials) {
+                S.bsdfs.push_back(slot.bsdf);
+                S.materials.push_back({1.0f, 1.0f, 1.0f});
+                S.albedoWidths.push_back(slot.albedoWidth > 0 ? slot.albedoWidth : 1);
+                S.albedoHeights.push_back(slot.albedoHeight > 0 ? slot.albedoHeight : 1);
+                S.albedoImages.push_back(std::move(slot.albedo));
+                S.mrWidths.push_back(slot.mrWidth > 0 ? slot.mrWidth : 1);
+                S.mrHeights.push_back(slot.mrHeight > 0 ? slot.mrHeight : 1);
+                S.mrImages.push_back(std::move(slot.mr));
+            }
+            for (size_t i = 0; i < g.triangles.size(); ++i) {
+                const int local = g.materialIds[i];
+                const GltfSlot& slot = g.materials[static_cast<size_t>(local)];
+                S.triangles.push_back(g.triangles[i]);
+                S.triangleMaterialIds.push_back(matOffset + local);
+                S.triangleBsdfIds.push_back(bsdfOffset + local);
+                S.triangleEmitterFlags.push_back(slot.isEmitter ? 1 : 0);
+                S.triangleEmission.push_back(slot.isEmitter ? slot.emission : Float3{0.0f, 0.0f, 0.0f});
+            }
+            for (size_t mi = 0; mi < g.materials.size(); ++mi) {   // one emitter per emissive material
+                const GltfSlot& slot = g.materials[mi];
+                if (!slot.isEmitter) continue;
+                const int triOff = static_cast<int>(S.emitterTriIndices.size());
+                const int cdfOff = static_cast<int>(S.emitterTriCdf.size());
+                S.emitterTriCdf.push_back(0.0f);
+                float area = 0.0f;
+                const int matId = matOffset + static_cast<int>(mi);
+                for (int ti = firstTri; ti < static_cast<int>(S.triangles.size()); ++ti) {
+                    if (S.triangleMaterialIds[static_cast<size_t>(ti)] != matId) continue;
+                    area += triangleArea(S.triangles[static_cast<size_t>(ti)]);
+                    S.emitterTriIndices.push_back(ti);
+                    S.emitterTriCdf.push_back(area);
+                }
+                if (area > 0.0f) finishEmitter(triOff, cdfOff, area, slot.emission);
             }
         }
-        if (S.triangles.empty()) fail("scene has no triangles after loading meshes");
+        if (S.triangles.empty()) fail("scene has no triangles after loading meshes and models");
         for (const auto& sd : d.spots) {   // src/main.cpp:879-904
             SpotlightData sp2{};
             sp2.position = {sd.posX, sd.posY, sd.posZ};

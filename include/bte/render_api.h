@@ -228,6 +228,18 @@ int bte_record_stop(void);
 /* RGBA8 rows (first row first) -> PNG bytes; with out NULL only *size is set. */
 int bte_encode_png(const uint8_t* rgba, int width, int height, uint8_t* out, long long capacity, long long* size);
 
+/* ---- glTF 2.0 / GLB models: loadGltfModel (include/gltf_loader.h:25-30, src/gltf_loader.cpp:768-846) ----
+ * Triangles (with the <model> transform posX/Y/Z, rotX/Y/Z degrees, scaleX/Y/Z applied after the node graph;
+ * NULL = identity), per-triangle material slots, and per slot a Disney BSDF, emission and RGBA8 albedo /
+ * metallic-roughness images (width = height = 0 when absent).  bte_scene_load reads <model> entries with it. */
+typedef struct BteGltf BteGltf;
+int bte_gltf_load(const char* path, const float* transform9, BteGltf** out);
+int bte_gltf_counts(const BteGltf* model, int* triangles, int* materials, int* skippedOutliers);
+int bte_gltf_triangles(const BteGltf* model, TriangleData* triangles, int* materialIds);
+int bte_gltf_material(const BteGltf* model, int index, BsdfData* bsdf, float* emission3, int* isEmitter,
+                      int* albedoWidthHeight, int* mrWidthHeight, uint8_t* albedoRGBA, uint8_t* mrRGBA);
+void bte_gltf_free(BteGltf* model);
+
 /* ---- scene.xml / OBJ loader (src/scene.cpp:83-523, src/main.cpp:267-930) ---- */
 typedef struct BteScene BteScene;
 typedef struct {

@@ -8,11 +8,14 @@
  * pulls in the window/GL stack).  Produces the flattened triangle, BSDF and
  * emitter arrays for comparison with the product's loader, and per material
  * the texture colour and RGBA8 image of loadTextureAverage / loadImageRGBA
- * (src/main.cpp:407-470) through the reference's vendored stb_image.
+ * (src/main.cpp:407-470) through the reference's vendored stb_image.  <model>
+ * entries go through the reference's own loadGltfModel (src/gltf_loader.cpp,
+ * linked in with the GLM shim) and the merge of src/main.cpp:760-817.
  * Built by oracle/Makefile into oracle/_ref/libbteref_loader.so.
  */
 #include "scene.h"
 #include "mesh_transform.h"
+#include "gltf_loader.h"
 #define TINYOBJLOADER_IMPLEMENTATION
 #include "tiny_obj_loader.h"
 #define STB_IMAGE_IMPLEMENTATION
@@ -34,6 +37,9 @@ std::vector<uint8_t> g_flags;
 std::vector<float> g_matColour;                 // 3 per material
 std::vector<std::vector<uint8_t>> g_matImage;   // RGBA8 per material (empty: none)
 std::vector<int> g_matW, g_matH;
+std::vector<std::vector<uint8_t>> g_matMr;      // metallic-roughness RGBA8 per material (empty: none)
+std::vector<int> g_mrW, g_mrH;
+int g_emitterCount = 0;
 
 std::string resolve(const std::string& scenePath, const std::string& p)
 {
@@ -109,6 +115,7 @@ REF_API int refl_load(const char* scenePath)
     g_sceneCdf.clear(); g_flags.clear(); g_cam.clear();
     const SceneDescription d = loadSceneDescription(scenePath);   // src/scene.cpp:83
     g_matColour.clear(); g_matImage.clear(); g_matW.clear(); g_matH.clear();
+    g_matMr.clear(); g_mrW.clear(); g_mrH.clear(); g_emitterCount = 0;
     for (const auto& m : d.materials) {   // src/main.cpp:407-470, :600-612
         float col[3] = {1.0f, 1.0f, 1.0f};
         std::vector<uint8_t> img;
@@ -132,6 +139,9 @@ REF_API int refl_load(const char* scenePath)
         g_matImage.push_back(img);
         g_matW.push_back(w);
         g_matH.push_back(h);
+        g_matMr.emplace_back();
+        g_mrW.push_back(1);
+        g_mrH.push_back(1);
     }
     for (const auto& b : d.bsdfs) {   // src/main.cpp:629-665
         BsdfData x{};
@@ -179,6 +189,48 @@ REF_API int refl_load(const char* scenePath)
             const float lum = 0.2126f * m.radianceR + 0.7152f * m.radianceG + 0.0722f * m.radianceB;
             wsum += a * lum;
             g_sceneCdf.push_back(wsum);
+            ++g_emitterCount;
+        }
+    }
+    for (const auto& md : d.models) {   // src/main.cpp:760-817
+        const GltfLoadResult gl = loadGltfModel(resolve(scenePath, md.filename), md.transform);
+        const int matOffset = (int)g_matW.size(), bsdfOffset = (int)g_bsdfs.size(), firstTri = (int)g_tris.size();
+        for (const auto& slot : gl.materials) {
+            g_bsdfs.push_back(slot.bsdf);
+            const float one[3] = {1.0f, 1.0f, 1.0f};
+            g_matColour.insert(g_matColour.end(), one, one + 3);
+            g_matImage.push_back(slot.albedo.pixels);
+            g_matW.push_back(slot.albedo.width > 0 ? slot.albedo.width : 1);
+            g_matH.push_back(slot.albedo.height > 0 ? slot.albedo.height : 1);
+            g_matMr.push_back(slot.metallicRoughness.pixels);
+            g_mrW.push_back(slot.metallicRoughness.width > 0 ? slot.metallicRoughness.width : 1);
+            g_mrH.push_back(slot.metallicRoughness.height > 0 ? slot.metallicRoughness.height : 1);
+        }
+        for (size_t i = 0; i < gl.triangles.size(); ++i) {
+            const int local = gl.materialIds[i];
+            g_tris.push_back(gl.triangles[i]);
+            g_triMat.push_back(matOffset + local);
+            g_triBsdf.push_back(bsdfOffset + local);
+            g_flags.push_back(gl.materials[(size_t)local].isEmitter ? 1 : 0);
+        }
+        for (size_t mi = 0; mi < gl.materials.size(); ++mi) {
+            const auto& slot = gl.materials[mi];
+            if (!slot.isEmitter) continue;
+            g_emCdf.push_back(0.0f);
+            float areaSum = 0.0f;
+            const int matId = matOffset + (int)mi;
+            for (int ti = firstTri; ti < (int)g_tris.size(); ++ti) {
+                if (g_triMat[(size_t)ti] != matId) continue;
+                areaSum += area(g_tris[(size_t)ti]);
+                g_emTri.push_back(ti);
+                g_emCdf.push_back(areaSum);
+            }
+            if (areaSum > 0.0f) {
+                const float lum = 0.2126f * slot.emission.x + 0.7152f * slot.emission.y + 0.0722f * slot.emission.z;
+                wsum += areaSum * lum;
+                g_sceneCdf.push_back(wsum);
+                ++g_emitterCount;
+            }
         }
     }
     const CameraDesc& c = d.camera;
@@ -188,6 +240,17 @@ REF_API int refl_load(const char* scenePath)
 }
 
 REF_API int refl_material_count(void) { return (int)g_matW.size(); }
+REF_API int refl_emitter_count(void) { return g_emitterCount; }
+
+// metallic-roughness image of material i: sizes; returns 1 when present (copied to `rgba` when non-null)
+REF_API int refl_material_mr(int i, int* w, int* h, uint8_t* rgba)
+{
+    *w = g_mrW[(size_t)i];
+    *h = g_mrH[(size_t)i];
+    if (g_matMr[(size_t)i].empty()) return 0;
+    if (rgba) std::memcpy(rgba, g_matMr[(size_t)i].data(), g_matMr[(size_t)i].size());
+    return 1;
+}
 
 // colour[3], image size; returns 1 when the material has an image (copied to `rgba` when non-null)
 REF_API int refl_material(int i, float* colour, int* w, int* h, uint8_t* rgba)

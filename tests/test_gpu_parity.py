@@ -362,6 +362,33 @@ def test_loader_textured_scene_bitexact(renderer, oracle_mod, bte, tmp_path):
     renderer.init_textures(None)
 
 
+def test_gltf_scene_bitexact(renderer, oracle_mod, bte, tmp_path):
+    """A scene.xml with two glTF drop-ins (textured and metallic-roughness-mapped Disney materials, an
+    emissive glTF material acting as an area light, KHR extensions) rendered by the GPU equals the oracle."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    sys.path.insert(0, os.path.dirname(__file__))
+    import gltf_models
+    from test_gltf import _scene_with_models
+    models = gltf_models.write_models(str(tmp_path / "models"))
+    sc = bte.load_scene(_scene_with_models(tmp_path, models))
+    assert len(sc.emitters) >= 2 and any(t is not None for t in sc.mr_textures)
+    W, H, spp, depth = sc.width, sc.height, 1, 10
+    _upload(renderer, sc, env_mode=0, spp=spp, depth=depth)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    g = renderer.read_sample_radiance(W * H * spp)
+    orc = oracle_mod.Oracle(libm=False)
+    view = oracle_mod.SceneView(sc, env_mode=0, oracle=orc, textures=sc.albedo_textures, mr_textures=sc.mr_textures)
+    pix = np.arange(W * H, dtype=np.uint32)
+    o, _, _ = oracle_mod.render_samples(orc.lib, view, sc.camera, W, H, depth, pix, np.zeros(W * H, np.uint32))
+    eq = np.all(bits(g) == bits(o), axis=1)
+    assert eq.all(), f"{np.sum(~eq)} of {len(o)} samples differ"
+    assert np.isfinite(g).all() and g.mean() > 0
+    renderer.init_textures(None)
+    renderer.init_mr_textures(None)
+
+
 def test_headless_output(renderer, bte, cornell_scene, tmp_path, monkeypatch):
     """Screenshots (top row first, src/main.cpp:118-142), raw recording frames (rows bottom first, as the
     reference pipes them to FFmpeg, :990-997) and the scene-changed reset (:947-952)."""
