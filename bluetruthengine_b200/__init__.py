@@ -418,7 +418,7 @@ class Renderer:
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
                    postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 0, bvh_builder: int = 1,
-                   ploc_radius: int = 8, overlap_connect: int = 1):
+                   ploc_radius: int = 4, overlap_connect: int = 1):
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),
                    int(tail_paths), int(bvh_builder), int(ploc_radius),
                    int(overlap_connect))

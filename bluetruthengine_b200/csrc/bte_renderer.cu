@@ -97,7 +97,7 @@ struct Renderer {
     int tailPaths = 0;        // bounce queues shorter than this finish in the tail kernel
     int bvhBuilder = 1;       // binary hierarchy of the next bte_init_accel: 0 Morton-prefix (Karras), 1 PLOC
                               // (PLOC: frame 10.96 -> 10.54 ms on the 1080p bench scene)
-    int plocRadius = 8;       // PLOC neighbour search radius (8 measured best of 8/16/32)
+    int plocRadius = 4;       // PLOC neighbour search radius (measured on the 1080p scene: 4 best of 4/6/8/12/16/32)
     int builtBuilder = 0;     // hierarchy in use
     int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
     bool sceneChanged = false;   // bte_mark_scene_changed: the next bte_render resets accumulation first
