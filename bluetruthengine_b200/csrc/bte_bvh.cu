@@ -624,6 +624,125 @@ __global__ void kWideCollect(const int2* __restrict__ items, int m, const int2* 
     cntT[i] = T;
 }
 
+// ---- surface-area-optimal choice of each wide node's children (the dynamic
+// program of Ylitie, Karras and Laine, "Efficient Incoherent Ray Traversal on
+// GPUs Through Compressed Wide BVHs", HPG 2017, with leaf slots decided by
+// triangle count as above).  For a binary subtree x and j = 1..8,
+// C(x, j) = the least cost of x as at most j slots of its parent:
+//   C(x, 1) = A(x) cTri count(x)            when count(x) <= leafMax (a leaf slot)
+//           = A(x) cNode + min_j D(x, j)     otherwise (an 8-wide node of its own)
+//   D(x, j) = min_k C(left, k) + C(right, j - k)   (x's slots split between its children)
+//   C(x, j) = min(C(x, j - 1), D(x, j)) for j >= 2.
+// A bottom-up pass (arrival counters, as the refit) stores C and the choices;
+// a wide node rooted at x then takes the slots of its best split, following
+// the stored choices down.  Ties keep the fewer slots / the smaller k, so the
+// tree does not depend on scheduling.
+constexpr float kSahNode = 1.0f;
+constexpr float kSahTri = 1.0f;   // cost of one triangle test in node visits (measured: 0.8-1.5 best of 0.1-1.5)
+
+struct WideChoice {
+    float c[9];          // C(x, 1..8) in c[1..8]
+    uint8_t split[9];    // per j: 0 = fewer slots (j - 1), else k slots go to the left child
+    uint8_t expandJ, expandK;   // the best split of x's own 8-wide node
+};
+
+__global__ void kWideCost(const int2* __restrict__ children, const int* __restrict__ parentInner,
+                          const int* __restrict__ parentLeaf, const int2* __restrict__ range,
+                          const float* __restrict__ innerBox, const float* __restrict__ leafBox, int n, int leafMax,
+                          float cTri, int* arrivals, WideChoice* ch)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || n < 2) return;
+    int node = parentLeaf[k];
+    while (node >= 0) {
+        if (atomicAdd(&arrivals[node], 1) == 0) return;   // the sibling's subtree is not done yet
+        __threadfence();
+        const int2 c = children[node];
+        float cl[9], cr[9];
+        for (int side = 0; side < 2; ++side) {
+            const int x = side ? c.y : c.x;
+            float* out = side ? cr : cl;
+            if (x >= 0) {
+                for (int j = 1; j <= 8; ++j) out[j] = __ldcg(&ch[x].c[j]);
+            } else {
+                const float a = halfArea(leafBox + 6 * static_cast<size_t>(~x)) * cTri;
+                for (int j = 1; j <= 8; ++j) out[j] = a;
+            }
+        }
+        WideChoice w;
+        float dist[9];
+        uint8_t distK[9];
+        float bestD = 0.0f;
+        int bestJ = 2;
+        for (int j = 2; j <= 8; ++j) {
+            float best = cl[1] + cr[j - 1];
+            int bk = 1;
+            for (int kk = 2; kk < j; ++kk) {
+                const float v = cl[kk] + cr[j - kk];
+                if (v < best) { best = v; bk = kk; }
+            }
+            dist[j] = best;
+            distK[j] = static_cast<uint8_t>(bk);
+            if (j == 2 || best < bestD) { bestD = best; bestJ = j; }
+        }
+        const int cnt = range[node].y - range[node].x + 1;
+        const float A = halfArea(innerBox + 6 * static_cast<size_t>(node));
+        w.c[0] = 0.0f;
+        w.c[1] = cnt <= leafMax ? A * cTri * static_cast<float>(cnt) : A * kSahNode + bestD;
+        w.split[0] = w.split[1] = 0;
+        for (int j = 2; j <= 8; ++j) {
+            if (dist[j] < w.c[j - 1]) { w.c[j] = dist[j]; w.split[j] = distK[j]; }
+            else { w.c[j] = w.c[j - 1]; w.split[j] = 0; }
+        }
+        w.expandJ = static_cast<uint8_t>(bestJ);
+        w.expandK = distK[bestJ];
+        ch[node] = w;
+        __threadfence();
+        node = parentInner[node];
+    }
+}
+
+__global__ void kWideCollectSah(const int2* __restrict__ items, int m, const int2* __restrict__ children,
+                                const int2* __restrict__ range, const WideChoice* __restrict__ ch, int leafMax,
+                                int* outCodes, int* cntI, int* cntT)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > m) return;
+    if (i == m) { cntI[m] = 0; cntT[m] = 0; return; }
+    const int code = items[i].x;
+    int C[8];
+    int k = 0;
+    if (code < 0) {
+        C[k++] = code;
+    } else {
+        int sx[16], sj[16], sp = 0;   // pending (subtree, slots); at most 8 slots, so at most 8 pending
+        const WideChoice& r = ch[code];
+        const int2 c = children[code];
+        sx[sp] = c.y; sj[sp++] = r.expandJ - r.expandK;
+        sx[sp] = c.x; sj[sp++] = r.expandK;
+        while (sp > 0 && k < 8) {
+            const int x = sx[--sp];
+            int j = sj[sp];
+            if (x >= 0) while (j > 1 && ch[x].split[j] == 0) --j;
+            if (x < 0 || j <= 1 || sp + 2 > 16) { C[k++] = x; continue; }
+            const int kk = ch[x].split[j];
+            const int2 cc = children[x];
+            sx[sp] = cc.y; sj[sp++] = j - kk;
+            sx[sp] = cc.x; sj[sp++] = kk;
+        }
+    }
+    int I = 0, T = 0;
+    for (int j = 0; j < 8; ++j) {
+        if (j < k) {
+            const int cnt = subtreeCount(range, C[j]);
+            if (C[j] >= 0 && cnt > leafMax) ++I; else T += cnt;
+        }
+        outCodes[8 * static_cast<size_t>(i) + j] = j < k ? C[j] : kNoChild;
+    }
+    cntI[i] = I;
+    cntT[i] = T;
+}
+
 __device__ __forceinline__ uint32_t wideScaleBits(uint32_t e) { return e << 23; }
 // p + q * 2^(e-127) in double (exact for the magnitudes a scene has), the
 // plane the traversal's fused slab test measures against
@@ -767,8 +886,8 @@ __global__ void kWideEmit(const int2* __restrict__ items, int m, const int* __re
 
 // Collapse the binary tree into the 8-wide tree, level by level.
 static int buildWide(int n, int leafMax, const int2* children, const int2* range, const float* innerBox,
-                     const float* leafBox, const float4* sortedTris, BvhBuildResult& out, cudaStream_t st,
-                     std::string& err)
+                     const float* leafBox, const float4* sortedTris, const WideChoice* choice, BvhBuildResult& out,
+                     cudaStream_t st, std::string& err)
 {
     int2 *itemsA = nullptr, *itemsB = nullptr;
     int *codes = nullptr, *cntI = nullptr, *cntT = nullptr;
@@ -791,8 +910,12 @@ static int buildWide(int n, int leafMax, const int2* children, const int2* range
         BVH_CK(cudaMemcpyAsync(itemsA, &root, sizeof(int2), cudaMemcpyHostToDevice, st));
         while (m > 0) {
             const int B = 128;
-            kWideCollect<<<(m + 1 + B - 1) / B, B, 0, st>>>(itemsA, m, children, range, innerBox, leafMax, codes, cntI,
-                                                          cntT);
+            if (choice)
+                kWideCollectSah<<<(m + 1 + B - 1) / B, B, 0, st>>>(itemsA, m, children, range, choice, leafMax, codes,
+                                                                 cntI, cntT);
+            else
+                kWideCollect<<<(m + 1 + B - 1) / B, B, 0, st>>>(itemsA, m, children, range, innerBox, leafMax, codes,
+                                                              cntI, cntT);
             kScanSingle<<<1, 1024, 0, st>>>(cntI, m + 1);
             kScanSingle<<<1, 1024, 0, st>>>(cntT, m + 1);
             kWideEmit<<<(m + B - 1) / B, B, 0, st>>>(itemsA, m, codes, cntI, cntT, range, innerBox, leafBox, sortedTris,
@@ -892,9 +1015,10 @@ fail:
     return rc;
 }
 
-int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int builder, int radius, BvhBuildResult& out,
-              cudaStream_t st, std::string& err)
+int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int builder, int radius, int wideCollapse,
+              BvhBuildResult& out, cudaStream_t st, std::string& err)
 {
+    WideChoice* choice = nullptr;
     out = BvhBuildResult{};
     if (n <= 0) return 0;
     if (width != 2 && width != 8) { err = "LBVH build: tree width must be 2 or 8"; return -1; }
@@ -970,8 +1094,15 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int buil
         BVH_CK(cudaGetLastError());
         out.width = width;
         if (width == 8) {
-            if (buildWide(n, maxLeaf < kWideLeafMax ? maxLeaf : kWideLeafMax, children, range, innerBox, leafBox, sorted,
-                          out, st, err) != 0)
+            const int wideLeaf = maxLeaf < kWideLeafMax ? maxLeaf : kWideLeafMax;
+            if (wideCollapse == 1 && n > 1) {   // surface-area-optimal children of each wide node
+                BVH_CK(cudaMalloc(&choice, sizeof(WideChoice) * inner));
+                BVH_CK(cudaMemsetAsync(arrivals, 0, sizeof(int) * inner, st));
+                kWideCost<<<G, B, 0, st>>>(children, parentInner, parentLeaf, range, innerBox, leafBox, n, wideLeaf,
+                                           kSahTri, arrivals, choice);
+                BVH_CK(cudaGetLastError());
+            }
+            if (buildWide(n, wideLeaf, children, range, innerBox, leafBox, sorted, choice, out, st, err) != 0)
                 goto fail;
             BVH_CK(cudaEventRecord(e1, st));
             BVH_CK(cudaEventSynchronize(e1));
@@ -999,13 +1130,13 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int buil
     }
     cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
     cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
-    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range);
+    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range); cudaFree(choice);
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     return 0;
 fail:
     cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB); cudaFree(hist);
     cudaFree(children); cudaFree(parentInner); cudaFree(parentLeaf); cudaFree(arrivals); cudaFree(innerBox);
-    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range); cudaFree(sorted);
+    cudaFree(leafBox); cudaFree(collapsed); cudaFree(cost); cudaFree(range); cudaFree(sorted); cudaFree(choice);
     cudaFree(out.leafTris); cudaFree(out.nodes); cudaFree(out.wnodes);
     out = BvhBuildResult{};
     if (e0) cudaEventDestroy(e0);

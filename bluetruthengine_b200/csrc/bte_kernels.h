@@ -48,7 +48,8 @@ struct BvhBuildResult {
 };
 // builder 1 asks for PLOC with neighbour search radius `radius`; a binary
 // tree too deep for the traversal stack falls back to the Morton-prefix one.
-int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, int width, int builder, int radius,
+// wideCollapse: 0 greedy (largest surface area opened first), 1 surface-area-optimal dynamic program
+int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, int width, int builder, int radius, int wideCollapse,
               BvhBuildResult& out, cudaStream_t st, std::string& err);
 
 // Env-map tables (bte_env.cu).

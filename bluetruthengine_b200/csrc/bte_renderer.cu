@@ -97,6 +97,7 @@ struct Renderer {
     int tailPaths = 0;        // bounce queues shorter than this finish in the tail kernel
     int bvhBuilder = 1;       // binary hierarchy of the next bte_init_accel: 0 Morton-prefix (Karras), 1 PLOC
                               // (PLOC: frame 10.96 -> 10.54 ms on the 1080p bench scene)
+    int wideCollapse = 1;     // 8-wide node children: 0 greedy by surface area, 1 surface-area-optimal (DP)
     int plocRadius = 4;       // PLOC neighbour search radius (measured on the 1080p scene: 4 best of 4/6/8/12/16/32)
     int builtBuilder = 0;     // hierarchy in use
     int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
@@ -724,11 +725,11 @@ int bte_init_accel(void)
         if (!g.tris.p || g.triCount <= 0) throw CudaError{"bte_init_accel: call bte_init_scene first"};
         BvhBuildResult r;
         std::string err;
-        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, g.bvhWidth, g.bvhBuilder, g.plocRadius, r, g.stream, err) != 0)
+        if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, g.bvhWidth, g.bvhBuilder, g.plocRadius, g.wideCollapse, r, g.stream, err) != 0)
             throw CudaError{err};
         if (r.width == 8 && 2 * r.depth > kWideStack) {   // node + postponed-leaf groups could overflow: binary tree
             cudaFree(r.wnodes); cudaFree(r.leafTris);
-            if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, 2, g.bvhBuilder, g.plocRadius, r, g.stream, err) != 0) throw CudaError{err};
+            if (buildLbvh(g.tris.as<TriangleData>(), g.triCount, g.maxLeaf, 2, g.bvhBuilder, g.plocRadius, g.wideCollapse, r, g.stream, err) != 0) throw CudaError{err};
         }
         if (r.width == 8) {
             g.wideNodes.p = r.wnodes; g.wideNodes.bytes = sizeof(WideNode) * r.nodeCount;
@@ -1111,6 +1112,7 @@ int bte_set_tuning(const BteTuning* t)
         if (t->bvhBuilder != 0 && t->bvhBuilder != 1) throw CudaError{"bte_set_tuning: bvhBuilder must be 0 or 1"};
         if (t->plocRadius < 1 || t->plocRadius > kPlocMaxRadius) throw CudaError{"bte_set_tuning: plocRadius in [1, 32]"};
         if (t->overlapConnect != 0 && t->overlapConnect != 1) throw CudaError{"bte_set_tuning: overlapConnect must be 0 or 1"};
+        if (t->wideCollapse != 0 && t->wideCollapse != 1) throw CudaError{"bte_set_tuning: wideCollapse must be 0 or 1"};
         g.bvhWidth = t->bvhWidth;
         g.maxLeaf = t->maxLeafTriangles;
         g.shadeMinBlocks = t->shadeMinBlocks;
@@ -1120,6 +1122,7 @@ int bte_set_tuning(const BteTuning* t)
         g.bvhBuilder = t->bvhBuilder;
         g.plocRadius = t->plocRadius;
         g.overlapConnect = t->overlapConnect;
+        g.wideCollapse = t->wideCollapse;
         g.gridBlock = 0;   // recompute persistent grids
         return 0;
     });
@@ -1138,6 +1141,7 @@ int bte_get_tuning(BteTuning* t)
         t->bvhBuilder = g.bvhBuilder;
         t->plocRadius = g.plocRadius;
         t->overlapConnect = g.overlapConnect;
+        t->wideCollapse = g.wideCollapse;
         return 0;
     });
 }

@@ -145,6 +145,8 @@ typedef struct {
     int plocRadius;        /* PLOC neighbour search radius in positions, 1-32 */
     int overlapConnect;    /* 1: bounce b's shadow rays run on a second stream beside bounce b+1's closest-hit
                             * rays (they share no data); 0: the stages run one after another */
+    int wideCollapse;      /* children of each 8-wide node: 0 greedy (open the largest-area child first);
+                            * 1 surface-area-optimal (dynamic program of Ylitie, Karras & Laine 2017) */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);

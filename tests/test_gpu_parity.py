@@ -52,15 +52,15 @@ def test_math_functions_bitexact(renderer, oracle_mod):
 
 
 def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0,
-            builder=1, radius=8):
+            builder=1, radius=8, collapse=1):
     renderer.cleanup()
-    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius)
+    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius, 1, collapse)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
 
 @pytest.mark.parametrize("tree", [(8, 1, 0, 16), (8, 3, 0, 16), (2, 1, 0, 16), (2, 4, 0, 16), (8, 2, 1, 16),
-                                  (8, 1, 1, 1), (2, 1, 1, 32), (2, 3, 1, 4)])
+                                  (8, 1, 1, 1), (2, 1, 1, 32), (2, 3, 1, 4), (8, 2, 1, 4, 0), (8, 3, 0, 16, 0)])
 @pytest.mark.parametrize("scene_name", ["cornell_scene", "random_scene"])
 def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, tree):
     """Closest hit (triangle, t, u, v) and any-hit occlusion for 40k rays, both tree widths, several
@@ -68,7 +68,8 @@ def test_closest_hit_matches_oracle(request, renderer, oracle_mod, scene_name, t
     lane per ray and (8-wide tree) eight lanes per ray, against the oracle's brute force over all
     triangles."""
     scene = request.getfixturevalue(scene_name)
-    _upload(renderer, scene, bvh_width=tree[0], max_leaf=tree[1], builder=tree[2], radius=tree[3])
+    _upload(renderer, scene, bvh_width=tree[0], max_leaf=tree[1], builder=tree[2], radius=tree[3],
+            collapse=tree[4] if len(tree) > 4 else 1)
     info = renderer.accel_info()
     assert info["width"] == tree[0] and info["builder"] == tree[2]
     orc = oracle_mod.Oracle(libm=False)
@@ -430,10 +431,10 @@ def test_tuning_roundtrip_and_validation(renderer):
     renderer.set_tuning(2, 2, 8, 35, 1, 4096, 1, 7)
     assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
                                  "sortShading": 1, "tailPaths": 4096, "bvhBuilder": 1, "plocRadius": 7,
-                                 "overlapConnect": 1}
+                                 "overlapConnect": 1, "wideCollapse": 1}
     for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2),
                 (1, 3, 8, 20, 1, -1), (1, 3, 8, 20, 1, 0, 2), (1, 3, 8, 20, 1, 0, 1, 0), (1, 3, 8, 20, 1, 0, 1, 33),
-                (1, 3, 8, 20, 1, 0, 1, 16, 2)]:
+                (1, 3, 8, 20, 1, 0, 1, 16, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 2)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
