@@ -101,7 +101,7 @@ struct Net {
     Buf dsNoisy, dsFeat, dsTarget;
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
-    bool useTc = false;   // tcgen05 convolutions for the full-resolution layers
+    int tcMode = 0;   // full-resolution convs: 0 warp-level mma.sync, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
     Buf errFlag;          // set by a tcgen05 convolution that timed out
 };
 
@@ -192,14 +192,28 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
     net.aN = N; net.aHp = Hp; net.aWp = Wp; net.aGrad = withGrad;
 }
 
-// One 3x3 convolution over concat(up ? upsample(X1) : X1, X2): the tcgen05 kernel for layers large
-// enough to fill the machine with 128-pixel tiles, the warp-level kernel otherwise.
+// One 3x3 convolution over concat(up ? upsample(X1) : X1, X2).  Layers large enough to fill the machine
+// with 128-pixel tiles go to a tcgen05 kernel (tcMode 2: row tiles, when the layer's weights and two input
+// slabs fit in shared memory; tcMode 1: pixel tiles); the rest to the warp-level kernel.  force: -1 by
+// tcMode, 0 warp-level, 1 pixel tiles, 2 row tiles.
 void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                   const float* bias, int Cout, bool relu, void* Y, cudaStream_t st, int force = -1)
 {
     const long long px = static_cast<long long>(N) * H * W;
-    const bool tc = force >= 0 ? force == 1 : (net.useTc && convTcSupported(C1 + C2, Cout) && px >= 128LL * 148 * 4);
-    if (tc) conv3x3Tc(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
+    int kind = force;
+    if (kind < 0) {
+        kind = 0;
+        if (px >= 128LL * 148 * 4) {
+            if (net.tcMode == 2 && convTcRowSupported(C1, C2, Cout)) kind = 2;
+            else if (net.tcMode == 1 && convTcSupported(C1 + C2, Cout)) kind = 1;
+        }
+    }
+    if (kind == 2 && !convTcRowSupported(C1, C2, Cout))
+        throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64, weights and slabs in shared memory)"};
+    if (kind == 1 && !convTcSupported(C1 + C2, Cout))
+        throw CudaErr{"denoiser: the tcgen05 pixel-tile kernel does not take this layer"};
+    if (kind == 2) conv3x3TcRow(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
+    else if (kind == 1) conv3x3Tc(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
     else conv3x3Cat(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, st);
 }
 
@@ -486,10 +500,15 @@ int bte_denoiser_denoise(const float* radiance, const float* features, int width
     });
 }
 
-// 1: full-resolution convolutions on the tcgen05 kernel; 0: the warp-level mma.sync kernel only
-int bte_denoiser_set_tcgen05(int enabled)
+// full-resolution convolutions: 0 the warp-level mma.sync kernel only; 1 tcgen05 pixel tiles; 2 tcgen05 row tiles
+int bte_denoiser_set_tcgen05(int mode)
 {
-    return guardedDn([&] { ensureNet(); net.useTc = enabled != 0; return 0; });
+    return guardedDn([&] {
+        if (mode < 0 || mode > 2) throw CudaErr{"bte_denoiser_set_tcgen05: mode must be 0, 1 or 2"};
+        ensureNet();
+        net.tcMode = mode;
+        return 0;
+    });
 }
 
 int bte_denoiser_last_ms(float* ms)
@@ -502,7 +521,8 @@ int bte_denoiser_last_ms(float* ms)
 
 // Kernel-level entry for numerical checks: op 0 forward conv (x, w, bias ->
 // out [N,H,W,Cout]), op 1 data gradient (dy, w -> out [N,H,W,Cin]), op 2 weight
-// gradient (x, dy -> out [9][Cout][Cin] followed by [Cout] bias gradient).
+// gradient (x, dy -> out [9][Cout][Cin] followed by [Cout] bias gradient); ops 3, 4
+// and 5, 6 are ops 0, 1 on the tcgen05 pixel-tile and row-tile kernels.
 // Host FP32 arrays are rounded to bf16 on the device; w is [9][Cout][Cin].
 int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float* bias, const float* dy, int n, int h,
                             int wd, int cin, int cout, int relu, float* out)
@@ -524,8 +544,11 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
             weightCopies(bf32.as<float>(), static_cast<int>(padded / 9), 1, dst.p, nullptr, st);
             ck(cudaStreamSynchronize(st), "sync");
         };
-        const int force = op >= 3 ? 1 : 0;   // ops 3 and 4: ops 0 and 1 on the tcgen05 kernel
-        if (op >= 3) op -= 3;
+        if (op < 0 || op > 6) throw CudaErr{"bte_denoiser_debug_conv: op must be 0 to 6"};
+        // ops 3 and 4: ops 0 and 1 on the tcgen05 pixel-tile kernel; ops 5 and 6 on the row-tile kernel
+        const int force = op >= 5 ? 2 : (op >= 3 ? 1 : 0);
+        if (op >= 5) op -= 5;
+        else if (op >= 3) op -= 3;
         if (op == 0 || op == 1) {
             const int inC = op == 0 ? cin : cout, outC = op == 0 ? cout : cin;
             convert(op == 0 ? x : dy, px * inC, bx);
@@ -567,7 +590,7 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
             ck(cudaStreamSynchronize(st), "sync");
             g.release();
         } else {
-            throw CudaErr{"bte_denoiser_debug_conv: op must be 0, 1 or 2"};
+            throw CudaErr{"bte_denoiser_debug_conv: op must be 0 to 6"};
         }
         bx.release(); bb.release(); bdy.release(); bo.release(); bf32.release(); bwk.release(); bwd.release();
         return 0;

@@ -81,9 +81,11 @@ class Denoiser:
         _check(self.lib.bte_denoiser_denoise(radiance.ctypes.data_as(C.c_void_p), fp, W, H, out.ctypes.data_as(C.c_void_p)))
         return out
 
-    def set_tcgen05(self, enabled: bool):
-        """Full-resolution convolutions on the tcgen05 (TMEM) kernel, or the warp-level MMA kernel only."""
-        _check(self.lib.bte_denoiser_set_tcgen05(1 if enabled else 0))
+    def set_tcgen05(self, mode):
+        """Kernel for the full-resolution convolutions: 0 (or False) the warp-level MMA kernel only, 1 (or True)
+        the tcgen05 pixel-tile kernel, 2 the tcgen05 row-tile kernel (layers it does not take stay on the
+        warp-level kernel)."""
+        _check(self.lib.bte_denoiser_set_tcgen05(int(mode)))
 
     def last_ms(self) -> float:
         ms = C.c_float()
@@ -92,13 +94,13 @@ class Denoiser:
 
     def debug_conv(self, op: int, x=None, w=None, bias=None, dy=None, shape=(1, 16, 16, 16, 16), relu=True):
         """op 0: forward, 1: data gradient, 2: weight gradient (+ bias gradient) of one 3x3 conv layer;
-        ops 3 and 4: ops 0 and 1 on the tcgen05 kernel.
+        ops 3 and 4: ops 0 and 1 on the tcgen05 pixel-tile kernel; ops 5 and 6 on the row-tile kernel.
         shape = (N, H, W, Cin, Cout); x [N,H,W,Cin], w [9][Cout][Cin], dy [N,H,W,Cout]."""
         n, h, wd, cin, cout = shape
         keep = [None if a is None else _f32(a) for a in (x, w, bias, dy)]
-        if op in (0, 3):
+        if op in (0, 3, 5):
             out = np.empty((n, h, wd, cout), dtype=np.float32)
-        elif op in (1, 4):
+        elif op in (1, 4, 6):
             out = np.empty((n, h, wd, cin), dtype=np.float32)
         else:
             out = np.empty(9 * cout * cin + cout, dtype=np.float32)

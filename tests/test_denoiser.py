@@ -35,16 +35,27 @@ def dn():
     return Denoiser()
 
 
-@pytest.mark.parametrize("kernel", ["mma", "tcgen05"])
+KERNEL_OPS = {"mma": (0, 1), "tcgen05": (3, 4), "tcgen05_row": (5, 6)}
+
+
+def _row_ok(cin, cout):
+    """Shapes the row-tile kernel takes (Cout 16..64 in steps of 16, weights + two slabs in 200 KB)."""
+    w = (9 * cout * cin * 2 + 1023) // 1024 * 1024
+    return cout in (16, 32, 48, 64) and cin % 16 == 0 and (200 * 1024 - w) // (3 * (cin // 8) * 137 * 16) >= 2
+
+
+@pytest.mark.parametrize("kernel", ["mma", "tcgen05", "tcgen05_row"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_conv_forward_matches_torch(dn, shape, kernel):
-    """Forward 3x3 conv + bias + ReLU, warp-level MMA kernel and tcgen05/TMEM kernel."""
+    """Forward 3x3 conv + bias + ReLU: warp-level MMA kernel, tcgen05 pixel-tile and row-tile kernels."""
     n, h, w, cin, cout = shape
+    if kernel == "tcgen05_row" and not _row_ok(cin, cout):
+        pytest.skip("layer outside the row-tile kernel's shapes")
     rng = np.random.default_rng(cin * 7 + cout)
     x = _bf16(rng.normal(size=(n, h, w, cin)))
     wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
     b = rng.normal(size=cout).astype(np.float32)
-    got = dn.debug_conv(0 if kernel == "mma" else 3, x=x, w=wt, bias=b, shape=shape, relu=True)
+    got = dn.debug_conv(KERNEL_OPS[kernel][0], x=x, w=wt, bias=b, shape=shape, relu=True)
     _, _, y = _torch_conv(x, wt, b)
     ref = np.maximum(y.detach().permute(0, 2, 3, 1).numpy(), 0.0)
     err = np.abs(got - ref).max() / np.abs(ref).max()
@@ -52,15 +63,17 @@ def test_conv_forward_matches_torch(dn, shape, kernel):
     assert err < 1e-2
 
 
-@pytest.mark.parametrize("kernel", ["mma", "tcgen05"])
+@pytest.mark.parametrize("kernel", ["mma", "tcgen05", "tcgen05_row"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_conv_data_gradient_matches_torch(dn, shape, kernel):
     n, h, w, cin, cout = shape
+    if kernel == "tcgen05_row" and not _row_ok(cout, cin):
+        pytest.skip("layer outside the row-tile kernel's shapes")
     rng = np.random.default_rng(cin * 5 + cout)
     x = _bf16(rng.normal(size=(n, h, w, cin)))
     wt = _bf16(rng.normal(size=(9, cout, cin)) / np.sqrt(9 * cin))
     dy = _bf16(rng.normal(size=(n, h, w, cout)))
-    got = dn.debug_conv(1 if kernel == "mma" else 4, w=wt, dy=dy, shape=shape)
+    got = dn.debug_conv(KERNEL_OPS[kernel][1], w=wt, dy=dy, shape=shape)
     import torch
     xt, wt_t, y = _torch_conv(x, wt)
     y.backward(torch.from_numpy(dy).permute(0, 3, 1, 2))
@@ -181,18 +194,24 @@ def _torch_unet(params, rad, feat):
     return np.maximum(np.expm1(pred.permute(1, 2, 0).numpy()), 0)[:H, :W]
 
 
+@pytest.mark.parametrize("tc", [0, 2])
 @pytest.mark.parametrize("size", [(72, 100), (470, 640)])
-def test_network_inference_matches_torch(dn, size):
+def test_network_inference_matches_torch(dn, size, tc):
     """The whole inference path (feature assembly, edge padding, encoder, in-place upsample+concat decoder,
     residual output) against the same network written in PyTorch, on a random network; the larger size
-    runs the full-resolution layers on the unsplit convolution kernel."""
+    runs the full-resolution layers on the unsplit warp-level kernel (tc 0) or on the tcgen05 row-tile
+    kernel, the upsample + concat layer included (tc 2)."""
     dn.init(11)
     p = dn.params()
     rng = np.random.default_rng(5)
     H, W = size
     rad = rng.exponential(0.4, size=(H, W, 3)).astype(np.float32)
     feat = np.concatenate([rng.uniform(0, 1, (H, W, 3)), rng.normal(size=(H, W, 3))], -1).astype(np.float32)
-    got = dn.denoise(rad, feat)
+    dn.set_tcgen05(tc)
+    try:
+        got = dn.denoise(rad, feat)
+    finally:
+        dn.set_tcgen05(0)
     ref = _torch_unet(p, rad, feat)
     lg, lr = np.log1p(got), np.log1p(ref)
     err = np.abs(lg - lr)
