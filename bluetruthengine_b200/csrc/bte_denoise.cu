@@ -204,11 +204,11 @@ void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
     if (kind < 0) {
         kind = 0;
         if (px >= 128LL * 148 * 4) {
-            if (net.tcMode == 2 && convTcRowSupported(C1, C2, Cout)) kind = 2;
+            if (net.tcMode == 2 && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
             else if (net.tcMode == 1 && convTcSupported(C1 + C2, Cout)) kind = 1;
         }
     }
-    if (kind == 2 && !convTcRowSupported(C1, C2, Cout))
+    if (kind == 2 && !convTcRowSupported(C1, C2, up, Cout))
         throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64, weights and slabs in shared memory)"};
     if (kind == 1 && !convTcSupported(C1 + C2, Cout))
         throw CudaErr{"denoiser: the tcgen05 pixel-tile kernel does not take this layer"};

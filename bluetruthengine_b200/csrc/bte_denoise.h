@@ -22,7 +22,7 @@ void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, i
 // The row-tile tcgen05 kernel: 128-pixel row segments, the 3-row input slab
 // staged once per tile, weights resident in shared memory, warp-specialised
 // copy / MMA / epilogue.  Cout 16, 32, 48 or 64; Cin a multiple of 16, C1 of 8.
-bool convTcRowSupported(int C1, int C2, int Cout);
+bool convTcRowSupported(int C1, int C2, bool up, int Cout);
 void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                   const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).

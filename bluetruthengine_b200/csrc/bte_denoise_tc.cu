@@ -23,9 +23,14 @@
 // issuing, waits (bounded) for what it issued and frees its tensor memory.
 #include "bte_denoise.h"
 
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <type_traits>
 
 namespace bte {
 namespace dn {
@@ -255,31 +260,46 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
 // ---------------------------------------------------------------- row tiles, warp-specialised
 // For the full-resolution layers (few channels, many pixels): a tile is 128
 // consecutive pixels of one image row.  Its input is the 3-row x 130-pixel
-// slab around it (all Cin channels), copied into shared memory once in the
+// slab around it (all Cin channels), staged in shared memory once in the
 // canonical K-major layout without swizzle: the 16-byte channel chunk j of
-// slab row r of input row d at (d * C8 + j) * LBO + 16 r, rows 16 bytes apart.
-// The A operand of tap (dy, dx) is then the same slab seen from 16 * dx bytes
-// further on (a row shift is a 16-byte address offset), so the nine taps are
-// nine descriptors over one copy and nothing is gathered twice.  The layer's
-// weights stay in shared memory for the CTA's whole run.
+// slab pixel r of input row d at j * kSlabJStride + d * 2080 + 16 r.  The A
+// operand of tap (dy, dx) is then the same slab seen from dy * 2080 + 16 dx
+// bytes on (a pixel shift is a 16-byte address offset), so the nine taps are
+// nine descriptors over one copy.  The layer's weights stay in shared memory
+// for the CTA's whole run.
+//   warps 4-7   producers.  Chunks read in place (X2, and X1 unless it is
+//               upsampled) come by TMA: one cp.async.bulk.tensor per chunk, a
+//               box of 8 channels x 130 pixels x 3 rows whose out-of-image part
+//               the copy engine fills with zeros.  An upsampled X1 comes by TMA
+//               at its own resolution (8 channels x 66 pixels x 2 rows per
+//               chunk, one tile ahead, into a double-buffered staging area) and
+//               the 128 producer threads expand it into the slab with 16-byte
+//               shared-memory copies, walking their chunks with running
+//               counters (no division).
+//   warp 8      one thread issues 9 x Cin/16 tcgen05.mma (M = 128, N = Cout,
+//               K = 16) per tile, fully unrolled (Cin/16 is a template
+//               parameter) so that every descriptor is a base plus a constant:
+//               small MMAs are bound by their issue rate, and a runtime loop
+//               around them costs up to three times the issue time.  The MMAs
+//               are committed to the slab-free and accumulator-full barriers.
 //   warps 0-3   epilogue: tcgen05.ld of TMEM lanes 32w.., bias, ReLU, bf16 stores
-//   warps 4-7   producers: cp.async of the next slab, completion signalled to an
-//               mbarrier (cp.async.mbarrier.arrive.noinc)
-//   warp 8      one thread issues 9 x Cin/16 tcgen05.mma (M = 128, N = Cout, K = 16)
-//               per tile and commits them to the slab-free and accumulator-full barriers
-// A ring of 2-4 slab buffers (as many as shared memory holds) and two TMEM
-// accumulators let copy, MMA and epilogue of consecutive tiles overlap; CTAs
-// are persistent over tiles.  The producers walk their chunks with running
-// (chunk, slab row, input row) counters, so no division is left in the copy
-// loop.  Every wait is bounded: a timeout raises the error flag and stops all
-// roles, and the MMA thread waits (bounded) for its last MMAs before the
-// tensor memory is freed.
+// A ring of 2-4 slab buffers (as many as shared memory holds) and a ring of
+// 2-4 TMEM accumulators let copy, MMA and epilogue of consecutive tiles
+// overlap; CTAs are persistent over tiles.  Every wait is bounded: a timeout
+// raises the error flag and stops all roles, and the MMA thread waits
+// (bounded) for its last MMAs before the tensor memory is freed.
 constexpr int kRowPx = 128;
-constexpr int kSlabRows = 137;          // 130 used; odd, so chunks of one slab row fall on different banks
-constexpr int kSlabLbo = kSlabRows * 16;
+constexpr int kSlabPx = kRowPx + 2;
+constexpr int kSlabDStride = kSlabPx * 16;                          // 2080: one input row of one chunk
+constexpr int kSlabJStride = (3 * kSlabDStride + 127) / 128 * 128;  // 6272: one chunk (TMA box), 128-byte aligned
+constexpr int kStgPx = kRowPx / 2 + 2;                              // 66 source pixels of an upsampled input
+constexpr int kStgDStride = kStgPx * 16;                            // 1056: one source row of one chunk
+constexpr int kStgJStride = (2 * kStgDStride + 127) / 128 * 128;    // 2176: one chunk (2 source rows), 128-byte aligned
 constexpr int kRowThreads = 288;
 constexpr int kRowMaxStages = 4;
+constexpr int kRowMaxAccs = 4;
 constexpr int kRowSmemBudget = 200 * 1024;
+constexpr int kRowMaxK16 = 6;           // Cin up to 96
 constexpr unsigned kRowSpin = 1u << 24;
 
 __device__ __forceinline__ bool mbarWaitRow(uint32_t bar, uint32_t parity, volatile int* abortFlag)
@@ -302,26 +322,83 @@ __device__ __forceinline__ void mbarArrive(uint32_t bar)
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(bar));
 }
 
-template <bool Relu, bool Up>
-__global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const bf16* __restrict__ X1, int C1, const bf16* __restrict__ X2,
-                                                             int C2, int N, int H, int W, const bf16* __restrict__ Wk,
-                                                             const float* __restrict__ bias, int Cout, bf16* __restrict__ Y,
-                                                             int stages, unsigned int* errorFlag)
+__device__ __forceinline__ uint4 ldShared16(uint32_t addr)
+{
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
+    return v;
+}
+
+__device__ __forceinline__ void stShared16(uint32_t addr, uint4 v)
+{
+    asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w));
+}
+
+// 32 lanes x 16 consecutive 32-bit columns of tensor memory into v[0..15], without waiting
+__device__ __forceinline__ void tmemLd16NoWait(uint32_t taddr, uint32_t* v)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void mbarArriveExpectTx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(bar), "r"(bytes));
+}
+
+// one box (8 channels x pixels x rows) of an NHWC bf16 tensor into shared memory (no multicast)
+__device__ __forceinline__ void tmaLoadBox(uint32_t dst, const CUtensorMap* map, int c, int x, int y, int n, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+                 ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(n), "r"(bar)
+                 : "memory");
+}
+
+// the nine taps x K16 k-steps of one tile, descriptors as constant offsets from the tile's bases
+template <int K16>
+__device__ __forceinline__ void issueRowTile(uint32_t acc, uint64_t aDesc0, uint64_t bDesc0, uint32_t bStep, uint32_t idesc)
+{
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+#pragma unroll
+        for (int kk = 0; kk < K16; ++kk) {
+            const uint64_t da = aDesc0 + static_cast<uint32_t>(((t / 3) * kSlabDStride + (t % 3) * 16 + kk * 2 * kSlabJStride) / 16);
+            const uint64_t db = bDesc0 + static_cast<uint32_t>(t * K16 + kk) * bStep;
+            umma(acc, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+        }
+    }
+}
+
+template <bool Relu, bool Up, int K16>
+__global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_constant__ CUtensorMap mapX1,
+                                                             const __grid_constant__ CUtensorMap mapX2,
+                                                             int C1, int C2, int N, int H, int W,
+                                                             const bf16* __restrict__ Wk, const float* __restrict__ bias,
+                                                             int Cout, bf16* __restrict__ Y, int stages, int accs,
+                                                             int tmemCols, unsigned int* errorFlag)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t slabFull[kRowMaxStages], slabEmpty[kRowMaxStages], accFull[2], accEmpty[2];
+    __shared__ uint64_t slabFull[kRowMaxStages], slabEmpty[kRowMaxStages], accFull[kRowMaxAccs], accEmpty[kRowMaxAccs];
+    __shared__ uint64_t stgFull[2], stgEmpty[2];
     __shared__ float sBias[64];
     __shared__ uint32_t tmemBase;
     __shared__ volatile int abortFlag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int Cin = C1 + C2, C8 = Cin / 8;
+    const int Cin = 16 * K16, C8 = 2 * K16, J1 = C1 / 8;   // Cin = C1 + C2, checked by the launcher
+    const int cpJ = Up ? J1 : 0;   // chunks [0, cpJ) expanded from the staging area, [cpJ, C8) by TMA
     const int tilesPerRow = (W + kRowPx - 1) / kRowPx;
-    const long long numTiles = static_cast<long long>(N) * H * tilesPerRow;
+    const int numTiles = N * H * tilesPerRow;   // < 2^31, checked by the launcher
     const uint32_t sW = smemAddr(smem);
     const uint32_t wBytes = 9u * Cout * Cin * 2u;
-    const uint32_t slabBytes = 3u * C8 * kSlabLbo;
+    const uint32_t slabBytes = static_cast<uint32_t>(C8) * kSlabJStride;
     const uint32_t sSlab = sW + ((wBytes + 1023u) & ~1023u);
-    const uint32_t tmemCols = 2 * Cout <= 32 ? 32 : (2 * Cout <= 64 ? 64 : 128);
+    const uint32_t sStg = sSlab + stages * slabBytes, stgBytes = static_cast<uint32_t>(J1) * kStgJStride;
+    if (sW & 1023u) {   // TMA boxes need 128-byte aligned destinations; the layout assumes a 1024-byte aligned base
+        if (tid == 0 && errorFlag) atomicOr(errorFlag, 1u);
+        return;
+    }
 
     // the layer's weights: tap t, output channel co, chunk j at t * Cout*Cin*2 + j * Cout*16 + co * 16
     for (int e = tid; e < 9 * Cout * C8; e += kRowThreads) {
@@ -337,12 +414,16 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const bf16* __restr
     if (tid < Cout) sBias[tid] = bias ? bias[tid] : 0.0f;
     if (tid == 0) {
         for (int b = 0; b < stages; ++b) {
-            mbarInit(smemAddr(&slabFull[b]), 128);
+            mbarInit(smemAddr(&slabFull[b]), 129);   // 128 producer threads + the TMA thread's expect-tx arrival
             mbarInit(smemAddr(&slabEmpty[b]), 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < accs; ++b) {
             mbarInit(smemAddr(&accFull[b]), 1);
             mbarInit(smemAddr(&accEmpty[b]), 4);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbarInit(smemAddr(&stgFull[b]), 1);
+            mbarInit(smemAddr(&stgEmpty[b]), 128);
         }
         abortFlag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
@@ -353,135 +434,164 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const bf16* __restr
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     const uint32_t tmem = tmemBase;
-    const long long first = blockIdx.x, stride = gridDim.x;
-    const int local = first < numTiles ? static_cast<int>((numTiles - first + stride - 1) / stride) : 0;
+    const int first = blockIdx.x, stride = gridDim.x;
+    const int local = first < numTiles ? (numTiles - first + stride - 1) / stride : 0;
     auto tileOf = [&](int i, int& n, int& y, int& x0) {
-        const long long t = first + static_cast<long long>(i) * stride;
-        x0 = static_cast<int>(t % tilesPerRow) * kRowPx;
-        const long long r = t / tilesPerRow;
-        y = static_cast<int>(r % H);
-        n = static_cast<int>(r / H);
+        const unsigned t = static_cast<unsigned>(first + i * stride), r = t / tilesPerRow;
+        x0 = static_cast<int>(t - r * tilesPerRow) * kRowPx;
+        y = static_cast<int>(r % static_cast<unsigned>(H));
+        n = static_cast<int>(r / static_cast<unsigned>(H));
     };
 
     if (warp >= 4 && warp < 8) {   // ---- producers
-        // chunk e = pt + 128 k of the slab is (input row d, slab row r, channel chunk j) with
-        // e = (d * 130 + r) * C8 + j; stepping e by 128 steps (r, j) by (128 / C8, 128 % C8)
-        const int pt = tid - 128, J1 = C1 / 8, total = 3 * 130 * C8;
-        const int stepJ = 128 % C8, stepR = 128 / C8, j0 = pt % C8, r0 = pt / C8;
-        const int Hs = Up ? H / 2 : H, Ws = Up ? W / 2 : W;
+        // expanded chunk e = pt + 128 k is (input row d, chunk j, slab pixel r) with e = (d * cpJ + j) * 130 + r:
+        // a warp copies 32 consecutive pixels of one chunk (conflict-free 16-byte shared accesses)
+        const int pt = tid - 128, total = 3 * kSlabPx * cpJ;
+        const uint32_t txBytes = static_cast<uint32_t>(C8 - cpJ) * 3u * kSlabDStride;
+        // staging TMA of local tile ii (upsampled input at its own resolution) into buffer ii & 1
+        auto issueStage = [&](int ii) {
+            int n2, y2, x2;
+            tileOf(ii, n2, y2, x2);
+            const uint32_t dst = sStg + (ii & 1) * stgBytes, bar = smemAddr(&stgFull[ii & 1]);
+            mbarArriveExpectTx(bar, static_cast<uint32_t>(J1) * 2u * kStgDStride);
+            for (int j = 0; j < J1; ++j) tmaLoadBox(dst + j * kStgJStride, &mapX1, 8 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
+        };
+        if (Up && pt == 0 && local > 0) issueStage(0);
         int b = 0, round = 0;
         for (int i = 0; i < local && !abortFlag; ++i) {
+            int n, y, x0;
+            tileOf(i, n, y, x0);
             if (round > 0 && !mbarWaitRow(smemAddr(&slabEmpty[b]), static_cast<uint32_t>((round - 1) & 1), &abortFlag)) {
                 abortFlag = 1;
                 break;
             }
-            int n, y, x0;
-            tileOf(i, n, y, x0);
             const uint32_t slab = sSlab + b * slabBytes;
-            // element offsets of input row y - 1 + d in X1 (at its own resolution) and X2
-            long long o1 = 0, o2 = 0;
-            bool rowIn = false;
-            auto rowSetup = [&](int d) {
-                const int yy = y - 1 + d;
-                rowIn = yy >= 0 && yy < H;
-                o1 = ((static_cast<long long>(n) * Hs + (Up ? (yy >> 1) : yy)) * Ws) * C1;
-                o2 = ((static_cast<long long>(n) * H + yy) * W) * C2;
-            };
-            int j = j0, r = r0, d = 0;
-            rowSetup(0);
-            for (int e = pt; e < total; e += 128) {
-                const int xx = x0 - 1 + r;
-                const bool inImg = rowIn && xx >= 0 && xx < W;
-                const bf16* src = X1;
-                if (inImg)
-                    src = j < J1 ? X1 + o1 + static_cast<long long>(Up ? (xx >> 1) : xx) * C1 + 8 * j
-                                 : X2 + o2 + static_cast<long long>(xx) * C2 + 8 * (j - J1);
-                cpAsync16(slab + (d * C8 + j) * kSlabLbo + r * 16, src, inImg);
-                j += stepJ;
-                r += stepR;
-                if (j >= C8) { j -= C8; ++r; }
-                if (r >= 130) { r -= 130; ++d; rowSetup(d); }
+            const uint32_t full = smemAddr(&slabFull[b]);
+            if (pt == 0) {
+                mbarArriveExpectTx(full, txBytes);
+                for (int j = cpJ; j < C8; ++j) {
+                    if (j < J1) tmaLoadBox(slab + j * kSlabJStride, &mapX1, 8 * j, x0 - 1, y - 1, n, full);
+                    else tmaLoadBox(slab + j * kSlabJStride, &mapX2, 8 * (j - J1), x0 - 1, y - 1, n, full);
+                }
             }
-            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smemAddr(&slabFull[b])));
+            if (Up) {
+                // the next tile's staging goes into the buffer tile i - 1 used, once all producers released it
+                if (pt == 0 && i + 1 < local) {
+                    if (i >= 1 && !mbarWaitRow(smemAddr(&stgEmpty[(i + 1) & 1]), static_cast<uint32_t>(((i - 1) >> 1) & 1), &abortFlag)) {
+                        abortFlag = 1;
+                        break;
+                    }
+                    issueStage(i + 1);
+                }
+                if (!mbarWaitRow(smemAddr(&stgFull[i & 1]), static_cast<uint32_t>((i >> 1) & 1), &abortFlag)) {
+                    abortFlag = 1;
+                    break;
+                }
+                // slab pixel r of input row d is source pixel ((x0 - 1 + r) >> 1) of source row ((y - 1 + d) >> 1);
+                // the staging box starts at source pixel (x0 - 1) >> 1 and source row (y - 1) >> 1
+                const int sx0 = (x0 - 1) >> 1, sy0 = (y - 1) >> 1;
+                const uint32_t stg = sStg + (i & 1) * stgBytes;
+                int j = 0, r = pt, d = 0, srow = 0;
+                for (int e = pt; e < total; e += 128) {
+                    const int sx = ((x0 - 1 + r) >> 1) - sx0;
+                    stShared16(slab + j * kSlabJStride + d * kSlabDStride + r * 16,
+                               ldShared16(stg + j * kStgJStride + srow * kStgDStride + sx * 16));
+                    r += 128;
+                    if (r >= kSlabPx) {   // 128 < 130: at most one wrap per step
+                        r -= kSlabPx;
+                        if (++j == cpJ) {
+                            j = 0;
+                            ++d;
+                            srow = ((y - 1 + d) >> 1) - sy0;
+                        }
+                    }
+                }
+                asm volatile("fence.proxy.async.shared::cta;\n" ::);   // the tensor cores read what was written here
+                mbarArrive(smemAddr(&stgEmpty[i & 1]));
+            }
+            mbarArrive(full);
             if (++b == stages) { b = 0; ++round; }
         }
-        cpAsyncWait<0>();
     } else if (warp == 8) {   // ---- MMA issue
         if (lane == 0) {
             const uint32_t idesc = instrDesc(Cout);
             const uint32_t lboB = Cout * 16;
-            int issued = -1, b = 0, round = 0;
+            // descriptor start fields advance by (byte offset >> 4); shared addresses stay below 2^18, so the
+            // 14-bit field never carries into the stride fields.  Weights of (tap t, k-step kk) start
+            // (t * K16 + kk) * 2 * Cout * 16 bytes into the weight block.
+            const uint64_t bDesc0 = smemDesc(sW, lboB, 128);
+            const uint32_t bStep = 2 * Cout;
+            int issued = 0, b = 0, round = 0, a = 0, aRound = 0, lastA = 0, lastRound = 0;
             for (int i = 0; i < local && !abortFlag; ++i) {
                 if (!mbarWaitRow(smemAddr(&slabFull[b]), static_cast<uint32_t>(round & 1), &abortFlag) ||
-                    (i >= 2 && !mbarWaitRow(smemAddr(&accEmpty[i & 1]), static_cast<uint32_t>(((i - 2) >> 1) & 1), &abortFlag))) {
+                    (aRound > 0 && !mbarWaitRow(smemAddr(&accEmpty[a]), static_cast<uint32_t>((aRound - 1) & 1), &abortFlag))) {
                     abortFlag = 1;
                     break;
                 }
                 asm volatile("fence.proxy.async.shared::cta;\n" ::);
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-                const uint32_t slab = sSlab + b * slabBytes;
-                const uint32_t acc = tmem + static_cast<uint32_t>((i & 1) * Cout);
-                for (int t = 0; t < 9; ++t) {
-                    const int dy = t / 3, dx = t % 3;
-                    for (int kk = 0; kk < Cin / 16; ++kk) {
-                        const uint64_t da = smemDesc(slab + (dy * C8 + 2 * kk) * kSlabLbo + dx * 16, kSlabLbo, 128);
-                        const uint64_t db = smemDesc(sW + t * Cout * Cin * 2 + 2 * kk * lboB, lboB, 128);
-                        umma(acc, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
-                    }
-                }
+                issueRowTile<K16>(tmem + static_cast<uint32_t>(a * Cout), smemDesc(sSlab + b * slabBytes, kSlabJStride, 128),
+                                  bDesc0, bStep, idesc);
                 ummaCommit(smemAddr(&slabEmpty[b]));
-                ummaCommit(smemAddr(&accFull[i & 1]));
-                issued = i;
+                ummaCommit(smemAddr(&accFull[a]));
+                issued = 1;
+                lastA = a;
+                lastRound = aRound;
                 if (++b == stages) { b = 0; ++round; }
+                if (++a == accs) { a = 0; ++aRound; }
             }
             // whatever happened, the last MMAs must be done before the tensor memory is freed
-            if (issued >= 0 && !mbarWaitRow(smemAddr(&accFull[issued & 1]), static_cast<uint32_t>((issued >> 1) & 1), &abortFlag)) {
+            if (issued && !mbarWaitRow(smemAddr(&accFull[lastA]), static_cast<uint32_t>(lastRound & 1), &abortFlag)) {
                 for (unsigned s = 0; s < kRowSpin; ++s) {   // on abort, wait on (bounded) without the abort exit
                     uint32_t done;
                     asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                                  "selp.u32 %0, 1, 0, p;\n\t}\n"
                                  : "=r"(done)
-                                 : "r"(smemAddr(&accFull[issued & 1])), "r"(static_cast<uint32_t>((issued >> 1) & 1)));
+                                 : "r"(smemAddr(&accFull[lastA])), "r"(static_cast<uint32_t>(lastRound & 1)));
                     if (done) break;
                 }
             }
         }
     } else {   // ---- epilogue, warps 0-3: TMEM lanes 32w..32w+31 = tile pixels 32w..32w+31
+        int a = 0, aRound = 0;
         for (int i = 0; i < local && !abortFlag; ++i) {
-            const int a = i & 1;
-            if (!mbarWaitRow(smemAddr(&accFull[a]), static_cast<uint32_t>((i >> 1) & 1), &abortFlag)) {
+            int n, y, x0;
+            tileOf(i, n, y, x0);
+            if (!mbarWaitRow(smemAddr(&accFull[a]), static_cast<uint32_t>(aRound & 1), &abortFlag)) {
                 abortFlag = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-            int n, y, x0;
-            tileOf(i, n, y, x0);
             const int x = x0 + warp * 32 + lane;
-            for (int c = 0; c < Cout; c += 16) {
-                uint32_t v[16];
-                const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * Cout + c);
-                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                               "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                             : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
-                if (x < W) {
+            // all of the pixel's Cout (<= 64) accumulator columns in flight at once, one wait
+            uint32_t v[64];
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * Cout);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (16 * q < Cout) tmemLd16NoWait(taddr + 16 * q, v + 16 * q);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+            if (x < W) {
+                uint4* dst = reinterpret_cast<uint4*>(Y + ((static_cast<size_t>(n) * H + y) * W + x) * Cout);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (16 * q >= Cout) break;
                     uint32_t w8[8];
+#pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        float p = __uint_as_float(v[2 * k]) + sBias[c + 2 * k];
-                        float q = __uint_as_float(v[2 * k + 1]) + sBias[c + 2 * k + 1];
-                        if (Relu) { p = fmaxf(p, 0.0f); q = fmaxf(q, 0.0f); }
-                        const __nv_bfloat162 h = __floats2bfloat162_rn(p, q);
+                        float p = __uint_as_float(v[16 * q + 2 * k]) + sBias[16 * q + 2 * k];
+                        float r = __uint_as_float(v[16 * q + 2 * k + 1]) + sBias[16 * q + 2 * k + 1];
+                        if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
                         w8[k] = *reinterpret_cast<const uint32_t*>(&h);
                     }
-                    uint4* dst = reinterpret_cast<uint4*>(Y + ((static_cast<size_t>(n) * H + y) * W + x) * Cout + c);
-                    dst[0] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
-                    dst[1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                    dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
+                    dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
             __syncwarp();
             if (lane == 0) mbarArrive(smemAddr(&accEmpty[a]));
+            if (++a == accs) { a = 0; ++aRound; }
         }
     }
     __syncthreads();
@@ -522,50 +632,125 @@ void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, i
     }
 }
 
-// slab buffers that fit beside the layer's weights (at most kRowMaxStages; fewer than 2 = unsupported)
-int convTcRowStages(int Cin, int Cout)
+namespace {
+
+// shared memory: the weights, then the slab ring, then (upsampled X1) two staging buffers
+long long rowFixedBytes(int C1, int C2, bool up, int Cout)
 {
-    const long long w = (9LL * Cout * Cin * 2 + 1023) & ~1023LL, slab = 3LL * (Cin / 8) * kSlabLbo;
-    const long long fit = (kRowSmemBudget - w) / slab;
+    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up ? 2LL * (C1 / 8) * kStgJStride : 0);
+}
+
+// slab buffers that fit beside the rest (at most kRowMaxStages; fewer than 2 = unsupported)
+int convTcRowStages(int C1, int C2, bool up, int Cout)
+{
+    const long long fit = (kRowSmemBudget - rowFixedBytes(C1, C2, up, Cout)) / (static_cast<long long>((C1 + C2) / 8) * kSlabJStride);
     return static_cast<int>(fit < kRowMaxStages ? fit : kRowMaxStages);
 }
 
-int convTcRowSmem(int Cin, int Cout)
+int convTcRowSmem(int C1, int C2, bool up, int Cout)
 {
-    return static_cast<int>(((9LL * Cout * Cin * 2 + 1023) & ~1023LL) + convTcRowStages(Cin, Cout) * 3LL * (Cin / 8) * kSlabLbo);
+    return static_cast<int>(rowFixedBytes(C1, C2, up, Cout) +
+                            static_cast<long long>(convTcRowStages(C1, C2, up, Cout)) * ((C1 + C2) / 8) * kSlabJStride);
 }
 
-bool convTcRowSupported(int C1, int C2, int Cout)
+}  // namespace
+
+bool convTcRowSupported(int C1, int C2, bool up, int Cout)
 {
     const int Cin = C1 + C2;
-    return (Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64) && Cin % 16 == 0 && C1 % 8 == 0 && Cin >= 16 &&
-           convTcRowStages(Cin, Cout) >= 2;
+    return (Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64) && Cin % 16 == 0 && C1 % 8 == 0 && C2 % 8 == 0 &&
+           Cin >= 16 && Cin <= 16 * kRowMaxK16 && convTcRowStages(C1, C2, up, Cout) >= 2;
 }
+
+namespace {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library links the runtime only)
+PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            throw std::runtime_error("conv3x3TcRow: cuTensorMapEncodeTiled is not available");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// NHWC bf16 tensor [N][H][W][C] read in boxes of 8 channels x boxW pixels x boxH rows, zeros outside
+CUtensorMap slabMap(const void* base, int C, int N, int H, int W, int boxW, int boxH)
+{
+    CUtensorMap m;
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(C), static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
+                                static_cast<cuuint64_t>(N)};
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(C) * 2, static_cast<cuuint64_t>(W) * C * 2,
+                                   static_cast<cuuint64_t>(H) * W * C * 2};
+    const cuuint32_t box[4] = {8, static_cast<cuuint32_t>(boxW), static_cast<cuuint32_t>(boxH), 1}, elem[4] = {1, 1, 1, 1};
+    const CUresult r = tensorMapEncoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box,
+                                          elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("conv3x3TcRow: cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+}  // namespace
 
 void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                   const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st)
 {
-    const int smemBytes = convTcRowSmem(C1 + C2, Cout), stages = convTcRowStages(C1 + C2, Cout);
+    if (!convTcRowSupported(C1, C2, up, Cout)) throw std::runtime_error("conv3x3TcRow: unsupported layer shape");
+    if (up && ((H | W) & 1)) throw std::runtime_error("conv3x3TcRow: an upsampled input needs even H and W");
+    const int smemBytes = convTcRowSmem(C1, C2, up, Cout), stages = convTcRowStages(C1, C2, up, Cout);
+    const long long tiles = static_cast<long long>(N) * H * ((W + kRowPx - 1) / kRowPx);
+    if (tiles >= (1LL << 31)) throw std::runtime_error("conv3x3TcRow: more than 2^31 row tiles");
+    if ((reinterpret_cast<uintptr_t>(X1) | reinterpret_cast<uintptr_t>(X2)) & 15)
+        throw std::runtime_error("conv3x3TcRow: inputs must be 16-byte aligned");
+    CUtensorMap m1, m2;
+    std::memset(&m1, 0, sizeof(m1));
+    std::memset(&m2, 0, sizeof(m2));
+    m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, 2) : slabMap(X1, C1, N, H, W, kSlabPx, 3);
+    if (C2 > 0) m2 = slabMap(X2, C2, N, H, W, kSlabPx, 3);
     auto launch = [&](auto kernel) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smemBytes);
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowThreads, smemBytes) != cudaSuccess || per < 1) per = 1;
-        const int tmemCols = 2 * Cout <= 32 ? 32 : (2 * Cout <= 64 ? 64 : 128);
-        if (per * tmemCols > 512) per = 512 / tmemCols;   // every resident CTA gets its tensor memory at once
-        const long long tiles = static_cast<long long>(N) * H * ((W + kRowPx - 1) / kRowPx);
+        // accumulator ring: up to kRowMaxAccs tiles of Cout columns in a power-of-two allocation, every
+        // resident CTA holding its tensor memory at once (512 columns per SM)
+        int tmemCols = 32;
+        while (tmemCols < 2 * Cout) tmemCols *= 2;
+        if (per * tmemCols > 512) per = 512 / tmemCols;
+        while (tmemCols / Cout < kRowMaxAccs && per * tmemCols * 2 <= 512) tmemCols *= 2;
+        const int accs = tmemCols / Cout < kRowMaxAccs ? tmemCols / Cout : kRowMaxAccs;
         const long long grid = tiles < static_cast<long long>(sms) * per ? tiles : static_cast<long long>(sms) * per;
-        kernel<<<static_cast<unsigned>(grid), kRowThreads, smemBytes, st>>>(
-            static_cast<const bf16*>(X1), C1, static_cast<const bf16*>(X2), C2, N, H, W, static_cast<const bf16*>(Wk), bias,
-            Cout, static_cast<bf16*>(Y), stages, errorFlag);
+        kernel<<<static_cast<unsigned>(grid), kRowThreads, smemBytes, st>>>(m1, m2, C1, C2, N, H, W,
+                                                                           static_cast<const bf16*>(Wk), bias, Cout,
+                                                                           static_cast<bf16*>(Y), stages, accs, tmemCols,
+                                                                           errorFlag);
     };
+    auto byK = [&](auto relu_, auto up_) {
+        constexpr bool R = decltype(relu_)::value, U = decltype(up_)::value;
+        switch ((C1 + C2) / 16) {
+            case 1: launch(kConvTcRow<R, U, 1>); break;
+            case 2: launch(kConvTcRow<R, U, 2>); break;
+            case 3: launch(kConvTcRow<R, U, 3>); break;
+            case 4: launch(kConvTcRow<R, U, 4>); break;
+            case 5: launch(kConvTcRow<R, U, 5>); break;
+            case 6: launch(kConvTcRow<R, U, 6>); break;
+            default: throw std::runtime_error("conv3x3TcRow: Cin must be 16 to 96");
+        }
+    };
+    using T = std::true_type;
+    using F = std::false_type;
     if (relu) {
-        if (up) launch(kConvTcRow<true, true>);
-        else launch(kConvTcRow<true, false>);
+        if (up) byK(T{}, T{});
+        else byK(T{}, F{});
     } else {
-        if (up) launch(kConvTcRow<false, true>);
-        else launch(kConvTcRow<false, false>);
+        if (up) byK(F{}, T{});
+        else byK(F{}, F{});
     }
 }
 
