@@ -103,6 +103,7 @@ struct Net {
     float lastMs = 0.0f;
     int tcMode = 0;   // full-resolution convs: 0 warp-level mma.sync, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
     Buf errFlag;          // set by a tcgen05 convolution that timed out
+    Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
 };
 
 Net net;
@@ -209,10 +210,15 @@ void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
         }
     }
     if (kind == 2 && !convTcRowSupported(C1, C2, up, Cout))
-        throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64, weights and slabs in shared memory)"};
+        throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64, Cin in 16-channel passes)"};
     if (kind == 1 && !convTcSupported(C1 + C2, Cout))
         throw CudaErr{"denoiser: the tcgen05 pixel-tile kernel does not take this layer"};
-    if (kind == 2) conv3x3TcRow(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
+    if (kind == 2) {
+        const size_t scratch = convTcRowScratchBytes(C1, C2, up, Cout, N, H, W);
+        if (scratch) net.rowScratch.ensure(scratch);
+        conv3x3TcRow(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, scratch ? net.rowScratch.p : nullptr,
+                     net.errFlag.as<unsigned int>(), st);
+    }
     else if (kind == 1) conv3x3Tc(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
     else conv3x3Cat(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, st);
 }

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
+
 namespace bte {
 namespace dn {
 
@@ -20,11 +22,15 @@ bool convTcSupported(int Cin, int Cout);
 void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st);
 // The row-tile tcgen05 kernel: 128-pixel row segments, the 3-row input slab
-// staged once per tile, weights resident in shared memory, warp-specialised
-// copy / MMA / epilogue.  Cout 16, 32, 48 or 64; Cin a multiple of 16, C1 of 8.
+// staged once per tile (TMA), weights resident in shared memory, warp-
+// specialised copy / MMA / epilogue.  Cout 16, 32, 48 or 64; C1 and C2
+// multiples of 8 with Cin a multiple of 16.  A layer whose weights and slabs
+// do not fit shared memory runs in passes over its input channels, summing in
+// an FP32 scratch buffer of convTcRowScratchBytes (0 for a single pass).
 bool convTcRowSupported(int C1, int C2, bool up, int Cout);
+size_t convTcRowScratchBytes(int C1, int C2, bool up, int Cout, int N, int H, int W);
 void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
-                  const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st);
+                  const float* bias, int Cout, bool relu, void* Y, void* scratch, unsigned int* errorFlag, cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);

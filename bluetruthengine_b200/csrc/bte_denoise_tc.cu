@@ -31,6 +31,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <type_traits>
+#include <vector>
 
 namespace bte {
 namespace dn {
@@ -371,13 +372,23 @@ __device__ __forceinline__ void issueRowTile(uint32_t acc, uint64_t aDesc0, uint
     }
 }
 
+// One pass of a layer whose weights and slabs do not fit shared memory at once: the input channels
+// [c1lo, c1lo + C1) of X1 and [c2lo, c2lo + C2) of X2, weight columns [wOff, wOff + C1 + C2) of rows
+// wStride long.  partIn (FP32 [pixel][Cout], may alias partOut) is added to the accumulator; with partOut
+// the sum is stored there in FP32, otherwise bias and ReLU follow and Y receives bf16.
+struct RowPass {
+    int c1lo, c2lo, wStride, wOff;
+    const float* partIn;
+    float* partOut;
+};
+
 template <bool Relu, bool Up, int K16>
 __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_constant__ CUtensorMap mapX1,
                                                              const __grid_constant__ CUtensorMap mapX2,
                                                              int C1, int C2, int N, int H, int W,
                                                              const bf16* __restrict__ Wk, const float* __restrict__ bias,
-                                                             int Cout, bf16* __restrict__ Y, int stages, int accs,
-                                                             int tmemCols, unsigned int* errorFlag)
+                                                             int Cout, bf16* __restrict__ Y, RowPass pass, int stages,
+                                                             int accs, int tmemCols, unsigned int* errorFlag)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint64_t slabFull[kRowMaxStages], slabEmpty[kRowMaxStages], accFull[kRowMaxAccs], accEmpty[kRowMaxAccs];
@@ -400,10 +411,11 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
         return;
     }
 
-    // the layer's weights: tap t, output channel co, chunk j at t * Cout*Cin*2 + j * Cout*16 + co * 16
+    // the pass's weights: tap t, output channel co, chunk j at t * Cout*Cin*2 + j * Cout*16 + co * 16
     for (int e = tid; e < 9 * Cout * C8; e += kRowThreads) {
         const int j = e % C8, co = (e / C8) % Cout, t = e / (C8 * Cout);
-        cpAsync16(sW + t * Cout * Cin * 2 + j * Cout * 16 + co * 16, Wk + (static_cast<size_t>(t) * Cout + co) * Cin + 8 * j, true);
+        cpAsync16(sW + t * Cout * Cin * 2 + j * Cout * 16 + co * 16,
+                  Wk + (static_cast<size_t>(t) * Cout + co) * pass.wStride + pass.wOff + 8 * j, true);
     }
     cpAsyncCommit();
     if (warp == 0) {
@@ -454,7 +466,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             tileOf(ii, n2, y2, x2);
             const uint32_t dst = sStg + (ii & 1) * stgBytes, bar = smemAddr(&stgFull[ii & 1]);
             mbarArriveExpectTx(bar, static_cast<uint32_t>(J1) * 2u * kStgDStride);
-            for (int j = 0; j < J1; ++j) tmaLoadBox(dst + j * kStgJStride, &mapX1, 8 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
+            for (int j = 0; j < J1; ++j)
+                tmaLoadBox(dst + j * kStgJStride, &mapX1, pass.c1lo + 8 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
         };
         if (Up && pt == 0 && local > 0) issueStage(0);
         int b = 0, round = 0;
@@ -470,8 +483,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             if (pt == 0) {
                 mbarArriveExpectTx(full, txBytes);
                 for (int j = cpJ; j < C8; ++j) {
-                    if (j < J1) tmaLoadBox(slab + j * kSlabJStride, &mapX1, 8 * j, x0 - 1, y - 1, n, full);
-                    else tmaLoadBox(slab + j * kSlabJStride, &mapX2, 8 * (j - J1), x0 - 1, y - 1, n, full);
+                    if (j < J1) tmaLoadBox(slab + j * kSlabJStride, &mapX1, pass.c1lo + 8 * j, x0 - 1, y - 1, n, full);
+                    else tmaLoadBox(slab + j * kSlabJStride, &mapX2, pass.c2lo + 8 * (j - J1), x0 - 1, y - 1, n, full);
                 }
             }
             if (Up) {
@@ -571,21 +584,44 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 if (16 * q < Cout) tmemLd16NoWait(taddr + 16 * q, v + 16 * q);
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
             if (x < W) {
-                uint4* dst = reinterpret_cast<uint4*>(Y + ((static_cast<size_t>(n) * H + y) * W + x) * Cout);
+                const size_t px = (static_cast<size_t>(n) * H + y) * W + x;
+                if (pass.partIn) {   // earlier passes' FP32 sums
+                    const float4* pin = reinterpret_cast<const float4*>(pass.partIn + px * Cout);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (16 * q >= Cout) break;
-                    uint32_t w8[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        float p = __uint_as_float(v[16 * q + 2 * k]) + sBias[16 * q + 2 * k];
-                        float r = __uint_as_float(v[16 * q + 2 * k + 1]) + sBias[16 * q + 2 * k + 1];
-                        if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
-                        const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
-                        w8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                    for (int q = 0; q < 16; ++q) {
+                        if (4 * q >= Cout) break;
+                        const float4 f = pin[q];
+                        v[4 * q] = __float_as_uint(__uint_as_float(v[4 * q]) + f.x);
+                        v[4 * q + 1] = __float_as_uint(__uint_as_float(v[4 * q + 1]) + f.y);
+                        v[4 * q + 2] = __float_as_uint(__uint_as_float(v[4 * q + 2]) + f.z);
+                        v[4 * q + 3] = __float_as_uint(__uint_as_float(v[4 * q + 3]) + f.w);
                     }
-                    dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
-                    dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                }
+                if (pass.partOut) {
+                    float4* pout = reinterpret_cast<float4*>(pass.partOut + px * Cout);
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        if (4 * q >= Cout) break;
+                        pout[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                                              __uint_as_float(v[4 * q + 3]));
+                    }
+                } else {
+                    uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (16 * q >= Cout) break;
+                        uint32_t w8[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            float p = __uint_as_float(v[16 * q + 2 * k]) + sBias[16 * q + 2 * k];
+                            float r = __uint_as_float(v[16 * q + 2 * k + 1]) + sBias[16 * q + 2 * k + 1];
+                            if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
+                            const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
+                            w8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                        }
+                        dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
+                        dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                    }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -637,29 +673,71 @@ namespace {
 // shared memory: the weights, then the slab ring, then (upsampled X1) two staging buffers
 long long rowFixedBytes(int C1, int C2, bool up, int Cout)
 {
-    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up ? 2LL * (C1 / 8) * kStgJStride : 0);
+    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up && C1 > 0 ? 2LL * (C1 / 8) * kStgJStride : 0);
 }
 
-// slab buffers that fit beside the rest (at most kRowMaxStages; fewer than 2 = unsupported)
-int convTcRowStages(int C1, int C2, bool up, int Cout)
+// slab buffers that fit beside the rest (at most kRowMaxStages; fewer than 2 = does not fit)
+int rowStages(int C1, int C2, bool up, int Cout)
 {
     const long long fit = (kRowSmemBudget - rowFixedBytes(C1, C2, up, Cout)) / (static_cast<long long>((C1 + C2) / 8) * kSlabJStride);
     return static_cast<int>(fit < kRowMaxStages ? fit : kRowMaxStages);
 }
 
-int convTcRowSmem(int C1, int C2, bool up, int Cout)
+int rowSmem(int C1, int C2, bool up, int Cout)
 {
     return static_cast<int>(rowFixedBytes(C1, C2, up, Cout) +
-                            static_cast<long long>(convTcRowStages(C1, C2, up, Cout)) * ((C1 + C2) / 8) * kSlabJStride);
+                            static_cast<long long>(rowStages(C1, C2, up, Cout)) * ((C1 + C2) / 8) * kSlabJStride);
+}
+
+bool rowPassFits(int n1, int n2, bool up, int Cout)
+{
+    const int cin = n1 + n2;
+    return cin >= 16 && cin % 16 == 0 && cin <= 16 * kRowMaxK16 && rowStages(n1, n2, up, Cout) >= 2;
+}
+
+struct PassPlan {
+    int c1lo, n1, c2lo, n2;
+};
+
+// Split the layer's input channels (X1's, then X2's) into passes whose weights and slabs fit in shared
+// memory: one pass when the whole layer fits, else greedy runs of 16 channels.  False if no split works.
+bool planRowPasses(int C1, int C2, bool up, int Cout, std::vector<PassPlan>* plan)
+{
+    if (!(Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64) || C1 < 0 || C2 < 0 || C1 % 8 || C2 % 8) return false;
+    std::vector<PassPlan> out;
+    if (rowPassFits(C1, C2, up, Cout)) {
+        out.push_back({0, C1, 0, C2});
+    } else {
+        if (C1 % 16 || C2 % 16) return false;
+        PassPlan cur{0, 0, 0, 0};
+        for (int u = 0; u < (C1 + C2) / 16; ++u) {
+            PassPlan next = cur;
+            if (16 * u < C1) next.n1 += 16;
+            else next.n2 += 16;
+            if (rowPassFits(next.n1, next.n2, up, Cout)) {
+                cur = next;
+                continue;
+            }
+            if (cur.n1 + cur.n2 == 0) return false;   // not even 16 channels fit
+            out.push_back(cur);
+            cur = 16 * u < C1 ? PassPlan{16 * u, 16, 0, 0} : PassPlan{C1, 0, 16 * u - C1, 16};
+            if (!rowPassFits(cur.n1, cur.n2, up, Cout)) return false;
+        }
+        out.push_back(cur);
+    }
+    if (plan) *plan = out;
+    return true;
 }
 
 }  // namespace
 
-bool convTcRowSupported(int C1, int C2, bool up, int Cout)
+bool convTcRowSupported(int C1, int C2, bool up, int Cout) { return planRowPasses(C1, C2, up, Cout, nullptr); }
+
+size_t convTcRowScratchBytes(int C1, int C2, bool up, int Cout, int N, int H, int W)
 {
-    const int Cin = C1 + C2;
-    return (Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64) && Cin % 16 == 0 && C1 % 8 == 0 && C2 % 8 == 0 &&
-           Cin >= 16 && Cin <= 16 * kRowMaxK16 && convTcRowStages(C1, C2, up, Cout) >= 2;
+    std::vector<PassPlan> plan;
+    if (!planRowPasses(C1, C2, up, Cout, &plan) || plan.size() < 2) return 0;
+    return static_cast<size_t>(N) * H * W * Cout * sizeof(float);
 }
 
 namespace {
@@ -698,11 +776,13 @@ CUtensorMap slabMap(const void* base, int C, int N, int H, int W, int boxW, int 
 }  // namespace
 
 void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
-                  const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st)
+                  const float* bias, int Cout, bool relu, void* Y, void* scratch, unsigned int* errorFlag, cudaStream_t st)
 {
-    if (!convTcRowSupported(C1, C2, up, Cout)) throw std::runtime_error("conv3x3TcRow: unsupported layer shape");
+    std::vector<PassPlan> plan;
+    if (!planRowPasses(C1, C2, up, Cout, &plan)) throw std::runtime_error("conv3x3TcRow: unsupported layer shape");
+    if (plan.size() > 1 && (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 15)))
+        throw std::runtime_error("conv3x3TcRow: this layer runs in passes and needs a 16-byte aligned scratch buffer");
     if (up && ((H | W) & 1)) throw std::runtime_error("conv3x3TcRow: an upsampled input needs even H and W");
-    const int smemBytes = convTcRowSmem(C1, C2, up, Cout), stages = convTcRowStages(C1, C2, up, Cout);
     const long long tiles = static_cast<long long>(N) * H * ((W + kRowPx - 1) / kRowPx);
     if (tiles >= (1LL << 31)) throw std::runtime_error("conv3x3TcRow: more than 2^31 row tiles");
     if ((reinterpret_cast<uintptr_t>(X1) | reinterpret_cast<uintptr_t>(X2)) & 15)
@@ -710,47 +790,56 @@ void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
     CUtensorMap m1, m2;
     std::memset(&m1, 0, sizeof(m1));
     std::memset(&m2, 0, sizeof(m2));
-    m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, 2) : slabMap(X1, C1, N, H, W, kSlabPx, 3);
+    if (C1 > 0) m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, 2) : slabMap(X1, C1, N, H, W, kSlabPx, 3);
     if (C2 > 0) m2 = slabMap(X2, C2, N, H, W, kSlabPx, 3);
-    auto launch = [&](auto kernel) {
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smemBytes);
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowThreads, smemBytes) != cudaSuccess || per < 1) per = 1;
-        // accumulator ring: up to kRowMaxAccs tiles of Cout columns in a power-of-two allocation, every
-        // resident CTA holding its tensor memory at once (512 columns per SM)
-        int tmemCols = 32;
-        while (tmemCols < 2 * Cout) tmemCols *= 2;
-        if (per * tmemCols > 512) per = 512 / tmemCols;
-        while (tmemCols / Cout < kRowMaxAccs && per * tmemCols * 2 <= 512) tmemCols *= 2;
-        const int accs = tmemCols / Cout < kRowMaxAccs ? tmemCols / Cout : kRowMaxAccs;
-        const long long grid = tiles < static_cast<long long>(sms) * per ? tiles : static_cast<long long>(sms) * per;
-        kernel<<<static_cast<unsigned>(grid), kRowThreads, smemBytes, st>>>(m1, m2, C1, C2, N, H, W,
-                                                                           static_cast<const bf16*>(Wk), bias, Cout,
-                                                                           static_cast<bf16*>(Y), stages, accs, tmemCols,
-                                                                           errorFlag);
-    };
-    auto byK = [&](auto relu_, auto up_) {
-        constexpr bool R = decltype(relu_)::value, U = decltype(up_)::value;
-        switch ((C1 + C2) / 16) {
-            case 1: launch(kConvTcRow<R, U, 1>); break;
-            case 2: launch(kConvTcRow<R, U, 2>); break;
-            case 3: launch(kConvTcRow<R, U, 3>); break;
-            case 4: launch(kConvTcRow<R, U, 4>); break;
-            case 5: launch(kConvTcRow<R, U, 5>); break;
-            case 6: launch(kConvTcRow<R, U, 6>); break;
-            default: throw std::runtime_error("conv3x3TcRow: Cin must be 16 to 96");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (size_t k = 0; k < plan.size(); ++k) {
+        const PassPlan& pp = plan[k];
+        const bool passUp = up && pp.n1 > 0;
+        const int smemBytes = rowSmem(pp.n1, pp.n2, passUp, Cout), stages = rowStages(pp.n1, pp.n2, passUp, Cout);
+        RowPass pass{pp.c1lo, pp.c2lo, C1 + C2, pp.n1 > 0 ? pp.c1lo : C1 + pp.c2lo,
+                     k > 0 ? static_cast<const float*>(scratch) : nullptr,
+                     k + 1 < plan.size() ? static_cast<float*>(scratch) : nullptr};
+        auto launch = [&](auto kernel) {
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smemBytes);
+            int per = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowThreads, smemBytes) != cudaSuccess || per < 1) per = 1;
+            // accumulator ring: up to kRowMaxAccs tiles of Cout columns in a power-of-two allocation, every
+            // resident CTA holding its tensor memory at once (512 columns per SM)
+            int tmemCols = 32;
+            while (tmemCols < 2 * Cout) tmemCols *= 2;
+            if (per * tmemCols > 512) per = 512 / tmemCols;
+            while (tmemCols / Cout < kRowMaxAccs && per * tmemCols * 2 <= 512) tmemCols *= 2;
+            const int accs = tmemCols / Cout < kRowMaxAccs ? tmemCols / Cout : kRowMaxAccs;
+            const long long grid = tiles < static_cast<long long>(sms) * per ? tiles : static_cast<long long>(sms) * per;
+            kernel<<<static_cast<unsigned>(grid), kRowThreads, smemBytes, st>>>(m1, m2, pp.n1, pp.n2, N, H, W,
+                                                                               static_cast<const bf16*>(Wk), bias, Cout,
+                                                                               static_cast<bf16*>(Y), pass, stages, accs,
+                                                                               tmemCols, errorFlag);
+        };
+        auto byK = [&](auto relu_, auto up_) {
+            constexpr bool R = decltype(relu_)::value, U = decltype(up_)::value;
+            switch ((pp.n1 + pp.n2) / 16) {
+                case 1: launch(kConvTcRow<R, U, 1>); break;
+                case 2: launch(kConvTcRow<R, U, 2>); break;
+                case 3: launch(kConvTcRow<R, U, 3>); break;
+                case 4: launch(kConvTcRow<R, U, 4>); break;
+                case 5: launch(kConvTcRow<R, U, 5>); break;
+                case 6: launch(kConvTcRow<R, U, 6>); break;
+                default: throw std::runtime_error("conv3x3TcRow: a pass takes 16 to 96 channels");
+            }
+        };
+        using T = std::true_type;
+        using F = std::false_type;
+        if (relu) {
+            if (passUp) byK(T{}, T{});
+            else byK(T{}, F{});
+        } else {
+            if (passUp) byK(F{}, T{});
+            else byK(F{}, F{});
         }
-    };
-    using T = std::true_type;
-    using F = std::false_type;
-    if (relu) {
-        if (up) byK(T{}, T{});
-        else byK(T{}, F{});
-    } else {
-        if (up) byK(F{}, T{});
-        else byK(F{}, F{});
     }
 }
 
