@@ -101,7 +101,7 @@ struct Net {
     Buf dsNoisy, dsFeat, dsTarget;
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
-    int tcMode = 0;   // full-resolution convs: 0 warp-level mma.sync, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
+    int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
 };
@@ -193,10 +193,11 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
     net.aN = N; net.aHp = Hp; net.aWp = Wp; net.aGrad = withGrad;
 }
 
-// One 3x3 convolution over concat(up ? upsample(X1) : X1, X2).  Layers large enough to fill the machine
-// with 128-pixel tiles go to a tcgen05 kernel (tcMode 2: row tiles, when the layer's weights and two input
-// slabs fit in shared memory; tcMode 1: pixel tiles); the rest to the warp-level kernel.  force: -1 by
-// tcMode, 0 warp-level, 1 pixel tiles, 2 row tiles.
+// One 3x3 convolution over concat(up ? upsample(X1) : X1, X2).  tcMode 2: layers with at least one
+// 128-pixel row tile per SM and Cout 16..64, 96 or 128 go to the tcgen05 row-tile kernel (in passes over
+// the input channels where weights and slabs do not fit shared memory at once); tcMode 1: layers that
+// fill the machine four times over with 128-pixel tiles go to the pixel-tile kernel; the rest to the
+// warp-level kernel.  force: -1 by tcMode, 0 warp-level, 1 pixel tiles, 2 row tiles.
 void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                   const float* bias, int Cout, bool relu, void* Y, cudaStream_t st, int force = -1)
 {
@@ -204,13 +205,12 @@ void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
     int kind = force;
     if (kind < 0) {
         kind = 0;
-        if (px >= 128LL * 148 * 4) {
-            if (net.tcMode == 2 && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
-            else if (net.tcMode == 1 && convTcSupported(C1 + C2, Cout)) kind = 1;
-        }
+        const long long rowTiles = static_cast<long long>(N) * H * ((W + 127) / 128);
+        if (net.tcMode == 2 && rowTiles >= 148 && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
+        else if (net.tcMode == 1 && px >= 128LL * 148 * 4 && convTcSupported(C1 + C2, Cout)) kind = 1;
     }
     if (kind == 2 && !convTcRowSupported(C1, C2, up, Cout))
-        throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64, Cin in 16-channel passes)"};
+        throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64/96/128, Cin in 16-channel passes)"};
     if (kind == 1 && !convTcSupported(C1 + C2, Cout))
         throw CudaErr{"denoiser: the tcgen05 pixel-tile kernel does not take this layer"};
     if (kind == 2) {

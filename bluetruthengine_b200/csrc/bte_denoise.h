@@ -23,7 +23,7 @@ void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, i
                const float* bias, int Cout, bool relu, void* Y, unsigned int* errorFlag, cudaStream_t st);
 // The row-tile tcgen05 kernel: 128-pixel row segments, the 3-row input slab
 // staged once per tile (TMA), weights resident in shared memory, warp-
-// specialised copy / MMA / epilogue.  Cout 16, 32, 48 or 64; C1 and C2
+// specialised copy / MMA / epilogue.  Cout 16, 32, 48, 64, 96 or 128; C1 and C2
 // multiples of 8 with Cin a multiple of 16.  A layer whose weights and slabs
 // do not fit shared memory runs in passes over its input channels, summing in
 // an FP32 scratch buffer of convTcRowScratchBytes (0 for a single pass).

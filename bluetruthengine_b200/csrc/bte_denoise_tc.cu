@@ -300,7 +300,8 @@ constexpr int kRowThreads = 288;
 constexpr int kRowMaxStages = 4;
 constexpr int kRowMaxAccs = 4;
 constexpr int kRowSmemBudget = 200 * 1024;
-constexpr int kRowMaxK16 = 6;           // Cin up to 96
+constexpr int kRowMaxK16 = 6;           // Cin up to 96 per pass
+constexpr int kRowMaxCout = 128;
 constexpr unsigned kRowSpin = 1u << 24;
 
 __device__ __forceinline__ bool mbarWaitRow(uint32_t bar, uint32_t parity, volatile int* abortFlag)
@@ -393,7 +394,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint64_t slabFull[kRowMaxStages], slabEmpty[kRowMaxStages], accFull[kRowMaxAccs], accEmpty[kRowMaxAccs];
     __shared__ uint64_t stgFull[2], stgEmpty[2];
-    __shared__ float sBias[64];
+    __shared__ float sBias[kRowMaxCout];
     __shared__ uint32_t tmemBase;
     __shared__ volatile int abortFlag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -576,11 +577,11 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
             const int x = x0 + warp * 32 + lane;
-            // all of the pixel's Cout (<= 64) accumulator columns in flight at once, one wait
-            uint32_t v[64];
+            // all of the pixel's Cout (<= 128) accumulator columns in flight at once, one wait
+            uint32_t v[kRowMaxCout];
             const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * Cout);
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < kRowMaxCout / 16; ++q)
                 if (16 * q < Cout) tmemLd16NoWait(taddr + 16 * q, v + 16 * q);
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
             if (x < W) {
@@ -588,7 +589,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 if (pass.partIn) {   // earlier passes' FP32 sums
                     const float4* pin = reinterpret_cast<const float4*>(pass.partIn + px * Cout);
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) {
+                    for (int q = 0; q < kRowMaxCout / 4; ++q) {
                         if (4 * q >= Cout) break;
                         const float4 f = pin[q];
                         v[4 * q] = __float_as_uint(__uint_as_float(v[4 * q]) + f.x);
@@ -600,7 +601,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 if (pass.partOut) {
                     float4* pout = reinterpret_cast<float4*>(pass.partOut + px * Cout);
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) {
+                    for (int q = 0; q < kRowMaxCout / 4; ++q) {
                         if (4 * q >= Cout) break;
                         pout[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
                                               __uint_as_float(v[4 * q + 3]));
@@ -608,7 +609,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 } else {
                     uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
+                    for (int q = 0; q < kRowMaxCout / 16; ++q) {
                         if (16 * q >= Cout) break;
                         uint32_t w8[8];
 #pragma unroll
@@ -703,7 +704,7 @@ struct PassPlan {
 // memory: one pass when the whole layer fits, else greedy runs of 16 channels.  False if no split works.
 bool planRowPasses(int C1, int C2, bool up, int Cout, std::vector<PassPlan>* plan)
 {
-    if (!(Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64) || C1 < 0 || C2 < 0 || C1 % 8 || C2 % 8) return false;
+    if (!(Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64 || Cout == 96 || Cout == 128) || C1 < 0 || C2 < 0 || C1 % 8 || C2 % 8) return false;
     std::vector<PassPlan> out;
     if (rowPassFits(C1, C2, up, Cout)) {
         out.push_back({0, C1, 0, C2});

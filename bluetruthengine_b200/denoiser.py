@@ -82,9 +82,9 @@ class Denoiser:
         return out
 
     def set_tcgen05(self, mode):
-        """Kernel for the full-resolution convolutions: 0 (or False) the warp-level MMA kernel only, 1 (or True)
-        the tcgen05 pixel-tile kernel, 2 the tcgen05 row-tile kernel (layers it does not take stay on the
-        warp-level kernel)."""
+        """Convolution kernels: 0 (or False) the warp-level MMA kernel only, 1 (or True) the tcgen05 pixel-tile
+        kernel for the full-resolution layers, 2 (the default) the tcgen05 row-tile kernel for every layer
+        with at least one 128-pixel row tile per SM (layers it does not take stay on the warp-level kernel)."""
         _check(self.lib.bte_denoiser_set_tcgen05(int(mode)))
 
     def last_ms(self) -> float:
@@ -111,7 +111,7 @@ class Denoiser:
 
 
 def _main(argv=None):
-    """Time inference: python -m bluetruthengine_b200.denoiser --width 1920 --height 1080 --iters 5"""
+    """Time inference: python -m bluetruthengine_b200.denoiser --width 1920 --height 1080 --iters 5 [--kernels 0|1|2]"""
     import argparse
     import json
     import os
@@ -119,11 +119,13 @@ def _main(argv=None):
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--iters", type=int, default=5)
+    ap.add_argument("--kernels", type=int, default=2, help="0 warp-level MMA only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                       "denoiser_c4.npz"))
     args = ap.parse_args(argv)
     dn = Denoiser()
     dn.load(args.weights)
+    dn.set_tcgen05(args.kernels)
     rng = np.random.default_rng(0)
     rad = rng.exponential(0.5, size=(args.height, args.width, 3)).astype(np.float32)
     feat = rng.uniform(0, 1, size=(args.height, args.width, 6)).astype(np.float32)
