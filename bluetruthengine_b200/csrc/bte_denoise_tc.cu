@@ -262,21 +262,22 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
 // For the full-resolution layers (few channels, many pixels): a tile is 128
 // consecutive pixels of one image row.  Its input is the 3-row x 130-pixel
 // slab around it (all Cin channels), staged in shared memory once in the
-// canonical K-major layout without swizzle: the 16-byte channel chunk j of
-// slab pixel r of input row d at j * kSlabJStride + d * 2080 + 16 r.  The A
-// operand of tap (dy, dx) is then the same slab seen from dy * 2080 + 16 dx
-// bytes on (a pixel shift is a 16-byte address offset), so the nine taps are
-// nine descriptors over one copy.  The layer's weights stay in shared memory
-// for the CTA's whole run.
-//   warps 4-7   producers.  Chunks read in place (X2, and X1 unless it is
-//               upsampled) come by TMA: one cp.async.bulk.tensor per chunk, a
-//               box of 8 channels x 130 pixels x 3 rows whose out-of-image part
-//               the copy engine fills with zeros.  An upsampled X1 comes by TMA
-//               at its own resolution (8 channels x 66 pixels x 2 rows per
-//               chunk, one tile ahead, into a double-buffered staging area) and
-//               the 128 producer threads expand it into the slab with 16-byte
-//               shared-memory copies, walking their chunks with running
-//               counters (no division).
+// canonical K-major layout with 32-byte swizzling: block jb of 16 channels
+// holds slab pixel r of input row d as one 32-byte row at
+// jb * kSlabJStride + (d * 130 + r) * 32, its two 16-byte halves exchanged
+// when bit 7 of the address is set.  The A operand of tap (dy, dx) is the
+// same block seen from (dy * 130 + dx) * 32 bytes on (a pixel shift is one
+// row), so the nine taps are nine descriptors over one copy.  The layer's
+// weights stay in shared memory for the CTA's whole run.
+//   warps 4-7   producers.  Blocks read in place (X2, and X1 unless it is
+//               upsampled) come by TMA: one cp.async.bulk.tensor per block, a
+//               box of 16 channels x 130 pixels x 3 rows (32-byte rows, the
+//               copy engine swizzles and fills the out-of-image part with
+//               zeros).  An upsampled X1 comes by TMA at its own resolution
+//               (16 channels x 66 pixels x 2 rows per block, one tile ahead,
+//               into a double-buffered staging area) and the 128 producer
+//               threads expand it into the slab with 16-byte shared-memory
+//               copies, walking their chunks with running counters.
 //   warp 8      one thread issues 9 x Cin/16 tcgen05.mma (M = 128, N = Cout,
 //               K = 16) per tile, fully unrolled (Cin/16 is a template
 //               parameter) so that every descriptor is a base plus a constant:
@@ -291,11 +292,11 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
 // (bounded) for its last MMAs before the tensor memory is freed.
 constexpr int kRowPx = 128;
 constexpr int kSlabPx = kRowPx + 2;
-constexpr int kSlabDStride = kSlabPx * 16;                          // 2080: one input row of one chunk
-constexpr int kSlabJStride = (3 * kSlabDStride + 127) / 128 * 128;  // 6272: one chunk (TMA box), 128-byte aligned
+constexpr int kSlabDStride = kSlabPx * 32;                          // 4160: one input row of one 16-channel block
+constexpr int kSlabJStride = (3 * kSlabDStride + 255) / 256 * 256;  // 12544: one block (TMA box), swizzle-atom aligned
 constexpr int kStgPx = kRowPx / 2 + 2;                              // 66 source pixels of an upsampled input
-constexpr int kStgDStride = kStgPx * 16;                            // 1056: one source row of one chunk
-constexpr int kStgJStride = (2 * kStgDStride + 127) / 128 * 128;    // 2176: one chunk (2 source rows), 128-byte aligned
+constexpr int kStgDStride = kStgPx * 32;                            // 2112: one source row of one block
+constexpr int kStgJStride = (2 * kStgDStride + 255) / 256 * 256;    // 4352: one block (2 source rows), atom aligned
 constexpr int kRowThreads = 288;
 constexpr int kRowMaxStages = 4;
 constexpr int kRowMaxAccs = 4;
@@ -322,6 +323,16 @@ __device__ __forceinline__ bool mbarWaitRow(uint32_t bar, uint32_t parity, volat
 __device__ __forceinline__ void mbarArrive(uint32_t bar)
 {
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(bar));
+}
+
+// 32-byte swizzle (the TMA's CU_TENSOR_MAP_SWIZZLE_32B and the MMA's 32B layout): the 16-byte half of a
+// 32-byte row is exchanged when address bit 7 is set
+__device__ __forceinline__ uint32_t sw32(uint32_t addr) { return addr ^ ((addr >> 3) & 16u); }
+
+// K-major 32-byte-swizzled operand: rows of 32 bytes, 8-row groups 256 bytes apart
+__device__ __forceinline__ uint64_t smemDescSw32(uint32_t addr)
+{
+    return smemDesc(addr, 16, 256) | (6ull << 61);
 }
 
 __device__ __forceinline__ uint4 ldShared16(uint32_t addr)
@@ -366,7 +377,7 @@ __device__ __forceinline__ void issueRowTile(uint32_t acc, uint64_t aDesc0, uint
     for (int t = 0; t < 9; ++t) {
 #pragma unroll
         for (int kk = 0; kk < K16; ++kk) {
-            const uint64_t da = aDesc0 + static_cast<uint32_t>(((t / 3) * kSlabDStride + (t % 3) * 16 + kk * 2 * kSlabJStride) / 16);
+            const uint64_t da = aDesc0 + static_cast<uint32_t>(((t / 3) * kSlabDStride + (t % 3) * 32 + kk * kSlabJStride) / 16);
             const uint64_t db = bDesc0 + static_cast<uint32_t>(t * K16 + kk) * bStep;
             umma(acc, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
         }
@@ -398,13 +409,13 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     __shared__ uint32_t tmemBase;
     __shared__ volatile int abortFlag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int Cin = 16 * K16, C8 = 2 * K16, J1 = C1 / 8;   // Cin = C1 + C2, checked by the launcher
-    const int cpJ = Up ? J1 : 0;   // chunks [0, cpJ) expanded from the staging area, [cpJ, C8) by TMA
+    const int Cin = 16 * K16, C8 = Cin / 8, J1 = C1 / 16;   // Cin = C1 + C2 (multiples of 16), checked by the launcher
+    const int cpJ = Up ? J1 : 0;   // blocks [0, cpJ) expanded from the staging area, [cpJ, K16) by TMA
     const int tilesPerRow = (W + kRowPx - 1) / kRowPx;
     const int numTiles = N * H * tilesPerRow;   // < 2^31, checked by the launcher
     const uint32_t sW = smemAddr(smem);
     const uint32_t wBytes = 9u * Cout * Cin * 2u;
-    const uint32_t slabBytes = static_cast<uint32_t>(C8) * kSlabJStride;
+    const uint32_t slabBytes = static_cast<uint32_t>(K16) * kSlabJStride;
     const uint32_t sSlab = sW + ((wBytes + 1023u) & ~1023u);
     const uint32_t sStg = sSlab + stages * slabBytes, stgBytes = static_cast<uint32_t>(J1) * kStgJStride;
     if (sW & 1023u) {   // TMA boxes need 128-byte aligned destinations; the layout assumes a 1024-byte aligned base
@@ -457,10 +468,10 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     };
 
     if (warp >= 4 && warp < 8) {   // ---- producers
-        // expanded chunk e = pt + 128 k is (input row d, chunk j, slab pixel r) with e = (d * cpJ + j) * 130 + r:
-        // a warp copies 32 consecutive pixels of one chunk (conflict-free 16-byte shared accesses)
-        const int pt = tid - 128, total = 3 * kSlabPx * cpJ;
-        const uint32_t txBytes = static_cast<uint32_t>(C8 - cpJ) * 3u * kSlabDStride;
+        // expanded 16-byte unit e = pt + 128 k is (input row d, block j, slab pixel r, half h) with
+        // e = ((d * cpJ + j) * 130 + r) * 2 + h: a warp copies 16 consecutive pixels of one block
+        const int pt = tid - 128, total = 3 * kSlabPx * cpJ * 2, h = pt & 1;
+        const uint32_t txBytes = static_cast<uint32_t>(K16 - cpJ) * 3u * kSlabDStride;
         // staging TMA of local tile ii (upsampled input at its own resolution) into buffer ii & 1
         auto issueStage = [&](int ii) {
             int n2, y2, x2;
@@ -468,7 +479,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             const uint32_t dst = sStg + (ii & 1) * stgBytes, bar = smemAddr(&stgFull[ii & 1]);
             mbarArriveExpectTx(bar, static_cast<uint32_t>(J1) * 2u * kStgDStride);
             for (int j = 0; j < J1; ++j)
-                tmaLoadBox(dst + j * kStgJStride, &mapX1, pass.c1lo + 8 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
+                tmaLoadBox(dst + j * kStgJStride, &mapX1, pass.c1lo + 16 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
         };
         if (Up && pt == 0 && local > 0) issueStage(0);
         int b = 0, round = 0;
@@ -483,9 +494,9 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             const uint32_t full = smemAddr(&slabFull[b]);
             if (pt == 0) {
                 mbarArriveExpectTx(full, txBytes);
-                for (int j = cpJ; j < C8; ++j) {
-                    if (j < J1) tmaLoadBox(slab + j * kSlabJStride, &mapX1, pass.c1lo + 8 * j, x0 - 1, y - 1, n, full);
-                    else tmaLoadBox(slab + j * kSlabJStride, &mapX2, pass.c2lo + 8 * (j - J1), x0 - 1, y - 1, n, full);
+                for (int j = cpJ; j < K16; ++j) {
+                    if (j < J1) tmaLoadBox(slab + j * kSlabJStride, &mapX1, pass.c1lo + 16 * j, x0 - 1, y - 1, n, full);
+                    else tmaLoadBox(slab + j * kSlabJStride, &mapX2, pass.c2lo + 16 * (j - J1), x0 - 1, y - 1, n, full);
                 }
             }
             if (Up) {
@@ -505,13 +516,13 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 // the staging box starts at source pixel (x0 - 1) >> 1 and source row (y - 1) >> 1
                 const int sx0 = (x0 - 1) >> 1, sy0 = (y - 1) >> 1;
                 const uint32_t stg = sStg + (i & 1) * stgBytes;
-                int j = 0, r = pt, d = 0, srow = 0;
+                int j = 0, r = pt >> 1, d = 0, srow = 0;
                 for (int e = pt; e < total; e += 128) {
                     const int sx = ((x0 - 1 + r) >> 1) - sx0;
-                    stShared16(slab + j * kSlabJStride + d * kSlabDStride + r * 16,
-                               ldShared16(stg + j * kStgJStride + srow * kStgDStride + sx * 16));
-                    r += 128;
-                    if (r >= kSlabPx) {   // 128 < 130: at most one wrap per step
+                    stShared16(sw32(slab + j * kSlabJStride + d * kSlabDStride + r * 32 + h * 16),
+                               ldShared16(sw32(stg + j * kStgJStride + srow * kStgDStride + sx * 32 + h * 16)));
+                    r += 64;
+                    if (r >= kSlabPx) {   // 64 < 130: at most one wrap per step
                         r -= kSlabPx;
                         if (++j == cpJ) {
                             j = 0;
@@ -544,7 +555,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 }
                 asm volatile("fence.proxy.async.shared::cta;\n" ::);
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-                issueRowTile<K16>(tmem + static_cast<uint32_t>(a * Cout), smemDesc(sSlab + b * slabBytes, kSlabJStride, 128),
+                issueRowTile<K16>(tmem + static_cast<uint32_t>(a * Cout), smemDescSw32(sSlab + b * slabBytes),
                                   bDesc0, bStep, idesc);
                 ummaCommit(smemAddr(&slabEmpty[b]));
                 ummaCommit(smemAddr(&accFull[a]));
@@ -674,26 +685,26 @@ namespace {
 // shared memory: the weights, then the slab ring, then (upsampled X1) two staging buffers
 long long rowFixedBytes(int C1, int C2, bool up, int Cout)
 {
-    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up && C1 > 0 ? 2LL * (C1 / 8) * kStgJStride : 0);
+    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up && C1 > 0 ? 2LL * (C1 / 16) * kStgJStride : 0);
 }
 
 // slab buffers that fit beside the rest (at most kRowMaxStages; fewer than 2 = does not fit)
 int rowStages(int C1, int C2, bool up, int Cout)
 {
-    const long long fit = (kRowSmemBudget - rowFixedBytes(C1, C2, up, Cout)) / (static_cast<long long>((C1 + C2) / 8) * kSlabJStride);
+    const long long fit = (kRowSmemBudget - rowFixedBytes(C1, C2, up, Cout)) / (static_cast<long long>((C1 + C2) / 16) * kSlabJStride);
     return static_cast<int>(fit < kRowMaxStages ? fit : kRowMaxStages);
 }
 
 int rowSmem(int C1, int C2, bool up, int Cout)
 {
     return static_cast<int>(rowFixedBytes(C1, C2, up, Cout) +
-                            static_cast<long long>(rowStages(C1, C2, up, Cout)) * ((C1 + C2) / 8) * kSlabJStride);
+                            static_cast<long long>(rowStages(C1, C2, up, Cout)) * ((C1 + C2) / 16) * kSlabJStride);
 }
 
 bool rowPassFits(int n1, int n2, bool up, int Cout)
 {
     const int cin = n1 + n2;
-    return cin >= 16 && cin % 16 == 0 && cin <= 16 * kRowMaxK16 && rowStages(n1, n2, up, Cout) >= 2;
+    return cin >= 16 && n1 % 16 == 0 && n2 % 16 == 0 && cin <= 16 * kRowMaxK16 && rowStages(n1, n2, up, Cout) >= 2;
 }
 
 struct PassPlan {
@@ -704,12 +715,13 @@ struct PassPlan {
 // memory: one pass when the whole layer fits, else greedy runs of 16 channels.  False if no split works.
 bool planRowPasses(int C1, int C2, bool up, int Cout, std::vector<PassPlan>* plan)
 {
-    if (!(Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64 || Cout == 96 || Cout == 128) || C1 < 0 || C2 < 0 || C1 % 8 || C2 % 8) return false;
+    if (!(Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64 || Cout == 96 || Cout == 128) || C1 < 0 || C2 < 0 || C1 % 16 ||
+        C2 % 16)
+        return false;
     std::vector<PassPlan> out;
     if (rowPassFits(C1, C2, up, Cout)) {
         out.push_back({0, C1, 0, C2});
     } else {
-        if (C1 % 16 || C2 % 16) return false;
         PassPlan cur{0, 0, 0, 0};
         for (int u = 0; u < (C1 + C2) / 16; ++u) {
             PassPlan next = cur;
@@ -758,7 +770,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder()
     return fn;
 }
 
-// NHWC bf16 tensor [N][H][W][C] read in boxes of 8 channels x boxW pixels x boxH rows, zeros outside
+// NHWC bf16 tensor [N][H][W][C] read in boxes of 16 channels (32-byte rows, 32-byte swizzle) x boxW pixels x boxH
+// rows, zeros outside
 CUtensorMap slabMap(const void* base, int C, int N, int H, int W, int boxW, int boxH)
 {
     CUtensorMap m;
@@ -766,9 +779,9 @@ CUtensorMap slabMap(const void* base, int C, int N, int H, int W, int boxW, int 
                                 static_cast<cuuint64_t>(N)};
     const cuuint64_t strides[3] = {static_cast<cuuint64_t>(C) * 2, static_cast<cuuint64_t>(W) * C * 2,
                                    static_cast<cuuint64_t>(H) * W * C * 2};
-    const cuuint32_t box[4] = {8, static_cast<cuuint32_t>(boxW), static_cast<cuuint32_t>(boxH), 1}, elem[4] = {1, 1, 1, 1};
+    const cuuint32_t box[4] = {16, static_cast<cuuint32_t>(boxW), static_cast<cuuint32_t>(boxH), 1}, elem[4] = {1, 1, 1, 1};
     const CUresult r = tensorMapEncoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box,
-                                          elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                          elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw std::runtime_error("conv3x3TcRow: cuTensorMapEncodeTiled failed");
     return m;
