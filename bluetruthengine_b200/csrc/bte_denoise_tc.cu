@@ -578,23 +578,30 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             }
         }
     } else {   // ---- epilogue, warps 0-3: TMEM lanes 32w..32w+31 = tile pixels 32w..32w+31
+        // the wait is made warp-uniform (__all_sync) so that no lane leaves the loop alone before the
+        // warp-wide tcgen05.ld and __syncwarp
         int a = 0, aRound = 0;
         for (int i = 0; i < local && !abortFlag; ++i) {
             int n, y, x0;
             tileOf(i, n, y, x0);
-            if (!mbarWaitRow(smemAddr(&accFull[a]), static_cast<uint32_t>(aRound & 1), &abortFlag)) {
+            if (!__all_sync(0xffffffffu, mbarWaitRow(smemAddr(&accFull[a]), static_cast<uint32_t>(aRound & 1), &abortFlag))) {
                 abortFlag = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
             const int x = x0 + warp * 32 + lane;
-            // all of the pixel's Cout (<= 128) accumulator columns in flight at once, one wait
+            // all of the pixel's Cout (<= 128) accumulator columns in flight at once, one wait; then the
+            // accumulator goes back to the MMA thread before the stores
             uint32_t v[kRowMaxCout];
             const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * Cout);
 #pragma unroll
             for (int q = 0; q < kRowMaxCout / 16; ++q)
                 if (16 * q < Cout) tmemLd16NoWait(taddr + 16 * q, v + 16 * q);
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+            __syncwarp();
+            if (lane == 0) mbarArrive(smemAddr(&accEmpty[a]));
+            if (++a == accs) { a = 0; ++aRound; }
             if (x < W) {
                 const size_t px = (static_cast<size_t>(n) * H + y) * W + x;
                 if (pass.partIn) {   // earlier passes' FP32 sums
@@ -636,10 +643,6 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                     }
                 }
             }
-            asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
-            __syncwarp();
-            if (lane == 0) mbarArrive(smemAddr(&accEmpty[a]));
-            if (++a == accs) { a = 0; ++aRound; }
         }
     }
     __syncthreads();
