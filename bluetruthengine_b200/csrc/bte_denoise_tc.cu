@@ -232,11 +232,12 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
         for (int c = 0; c < Cout; c += 16) {
             uint32_t v[16];
             const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
+            // load and wait in one statement, so that no use of v is scheduled before the wait
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
                            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                          : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
             if (q < total) {
                 uint32_t w8[8];
                 for (int k = 0; k < 8; ++k) {
@@ -293,10 +294,12 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
 constexpr int kRowPx = 128;
 constexpr int kSlabPx = kRowPx + 2;
 constexpr int kSlabDStride = kSlabPx * 32;                          // 4160: one input row of one 16-channel block
-constexpr int kSlabJStride = (3 * kSlabDStride + 255) / 256 * 256;  // 12544: one block (TMA box), swizzle-atom aligned
 constexpr int kStgPx = kRowPx / 2 + 2;                              // 66 source pixels of an upsampled input
 constexpr int kStgDStride = kStgPx * 32;                            // 2112: one source row of one block
-constexpr int kStgJStride = (2 * kStgDStride + 255) / 256 * 256;    // 4352: one block (2 source rows), atom aligned
+// A tile covers R output rows (1 or 2): its slab holds R + 2 input rows, an upsampled input's staging R + 1
+// source rows; blocks are swizzle-atom (256-byte) aligned
+__host__ __device__ constexpr int slabJStride(int R) { return ((R + 2) * kSlabDStride + 255) / 256 * 256; }
+__host__ __device__ constexpr int stgJStride(int R) { return ((R + 1) * kStgDStride + 255) / 256 * 256; }
 constexpr int kRowThreads = 288;
 constexpr int kRowMaxStages = 4;
 constexpr int kRowMaxAccs = 4;
@@ -347,13 +350,112 @@ __device__ __forceinline__ void stShared16(uint32_t addr, uint4 v)
     asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w));
 }
 
-// 32 lanes x 16 consecutive 32-bit columns of tensor memory into v[0..15], without waiting
-__device__ __forceinline__ void tmemLd16NoWait(uint32_t taddr, uint32_t* v)
+// Cout (16, 32, 48, 64, 96 or 128) consecutive 32-bit TMEM columns of the warp's 32 lanes into v, and the
+// wait for them inside the same asm statement: the registers are defined only once the wait has returned, so
+// the compiler cannot schedule a use of v between the load and the wait
+__device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t (&v)[128])
 {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                 : "r"(taddr));
+    switch (Cout) {
+        case 16:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                         : "r"(taddr + 0u));
+            break;
+        case 32:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                           "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                           "=r"(v[30]), "=r"(v[31])
+                         : "r"(taddr + 0u));
+            break;
+        case 48:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%48];\n"
+                         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%49];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                           "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                           "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]),
+                           "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]),
+                           "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47])
+                         : "r"(taddr + 0u), "r"(taddr + 32u));
+            break;
+        case 64:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                           "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                           "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]),
+                           "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]),
+                           "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]),
+                           "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]),
+                           "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]),
+                           "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+                         : "r"(taddr + 0u));
+            break;
+        case 96:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%96];\n"
+                         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79,%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95}, [%97];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                           "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                           "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]),
+                           "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]),
+                           "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]),
+                           "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]),
+                           "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]),
+                           "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63]), "=r"(v[64]), "=r"(v[65]),
+                           "=r"(v[66]), "=r"(v[67]), "=r"(v[68]), "=r"(v[69]), "=r"(v[70]), "=r"(v[71]),
+                           "=r"(v[72]), "=r"(v[73]), "=r"(v[74]), "=r"(v[75]), "=r"(v[76]), "=r"(v[77]),
+                           "=r"(v[78]), "=r"(v[79]), "=r"(v[80]), "=r"(v[81]), "=r"(v[82]), "=r"(v[83]),
+                           "=r"(v[84]), "=r"(v[85]), "=r"(v[86]), "=r"(v[87]), "=r"(v[88]), "=r"(v[89]),
+                           "=r"(v[90]), "=r"(v[91]), "=r"(v[92]), "=r"(v[93]), "=r"(v[94]), "=r"(v[95])
+                         : "r"(taddr + 0u), "r"(taddr + 64u));
+            break;
+        case 128:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x128.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63,%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79,%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95,%96,%97,%98,%99,%100,%101,%102,%103,%104,%105,%106,%107,%108,%109,%110,%111,%112,%113,%114,%115,%116,%117,%118,%119,%120,%121,%122,%123,%124,%125,%126,%127}, [%128];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                           "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                           "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]),
+                           "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]),
+                           "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]),
+                           "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]),
+                           "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]),
+                           "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63]), "=r"(v[64]), "=r"(v[65]),
+                           "=r"(v[66]), "=r"(v[67]), "=r"(v[68]), "=r"(v[69]), "=r"(v[70]), "=r"(v[71]),
+                           "=r"(v[72]), "=r"(v[73]), "=r"(v[74]), "=r"(v[75]), "=r"(v[76]), "=r"(v[77]),
+                           "=r"(v[78]), "=r"(v[79]), "=r"(v[80]), "=r"(v[81]), "=r"(v[82]), "=r"(v[83]),
+                           "=r"(v[84]), "=r"(v[85]), "=r"(v[86]), "=r"(v[87]), "=r"(v[88]), "=r"(v[89]),
+                           "=r"(v[90]), "=r"(v[91]), "=r"(v[92]), "=r"(v[93]), "=r"(v[94]), "=r"(v[95]),
+                           "=r"(v[96]), "=r"(v[97]), "=r"(v[98]), "=r"(v[99]), "=r"(v[100]), "=r"(v[101]),
+                           "=r"(v[102]), "=r"(v[103]), "=r"(v[104]), "=r"(v[105]), "=r"(v[106]), "=r"(v[107]),
+                           "=r"(v[108]), "=r"(v[109]), "=r"(v[110]), "=r"(v[111]), "=r"(v[112]), "=r"(v[113]),
+                           "=r"(v[114]), "=r"(v[115]), "=r"(v[116]), "=r"(v[117]), "=r"(v[118]), "=r"(v[119]),
+                           "=r"(v[120]), "=r"(v[121]), "=r"(v[122]), "=r"(v[123]), "=r"(v[124]), "=r"(v[125]),
+                           "=r"(v[126]), "=r"(v[127])
+                         : "r"(taddr + 0u));
+            break;
+        default: break;
+    }
 }
 
 __device__ __forceinline__ void mbarArriveExpectTx(uint32_t bar, uint32_t bytes)
@@ -369,17 +471,23 @@ __device__ __forceinline__ void tmaLoadBox(uint32_t dst, const CUtensorMap* map,
                  : "memory");
 }
 
-// the nine taps x K16 k-steps of one tile, descriptors as constant offsets from the tile's bases
-template <int K16>
-__device__ __forceinline__ void issueRowTile(uint32_t acc, uint64_t aDesc0, uint64_t bDesc0, uint32_t bStep, uint32_t idesc)
+// output row r of the tile (accumulator at acc + r * Cout columns): the nine taps x K16 k-steps, descriptors
+// as constant offsets from the tile's bases (tap (dy, dx) reads slab row r + dy from pixel dx on)
+template <int K16, int R>
+__device__ __forceinline__ void issueRowTile(uint32_t acc, uint32_t Cout, uint64_t aDesc0, uint64_t bDesc0, uint32_t bStep,
+                                             uint32_t idesc)
 {
 #pragma unroll
-    for (int t = 0; t < 9; ++t) {
+    for (int r = 0; r < R; ++r) {
 #pragma unroll
-        for (int kk = 0; kk < K16; ++kk) {
-            const uint64_t da = aDesc0 + static_cast<uint32_t>(((t / 3) * kSlabDStride + (t % 3) * 32 + kk * kSlabJStride) / 16);
-            const uint64_t db = bDesc0 + static_cast<uint32_t>(t * K16 + kk) * bStep;
-            umma(acc, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+        for (int t = 0; t < 9; ++t) {
+#pragma unroll
+            for (int kk = 0; kk < K16; ++kk) {
+                const uint64_t da =
+                    aDesc0 + static_cast<uint32_t>(((r + t / 3) * kSlabDStride + (t % 3) * 32 + kk * slabJStride(R)) / 16);
+                const uint64_t db = bDesc0 + static_cast<uint32_t>(t * K16 + kk) * bStep;
+                umma(acc + r * Cout, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+            }
         }
     }
 }
@@ -394,7 +502,7 @@ struct RowPass {
     float* partOut;
 };
 
-template <bool Relu, bool Up, int K16>
+template <bool Relu, bool Up, int K16, int R>
 __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_constant__ CUtensorMap mapX1,
                                                              const __grid_constant__ CUtensorMap mapX2,
                                                              int C1, int C2, int N, int H, int W,
@@ -411,13 +519,14 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int Cin = 16 * K16, C8 = Cin / 8, J1 = C1 / 16;   // Cin = C1 + C2 (multiples of 16), checked by the launcher
     const int cpJ = Up ? J1 : 0;   // blocks [0, cpJ) expanded from the staging area, [cpJ, K16) by TMA
-    const int tilesPerRow = (W + kRowPx - 1) / kRowPx;
-    const int numTiles = N * H * tilesPerRow;   // < 2^31, checked by the launcher
+    constexpr int JS = slabJStride(R), SJS = stgJStride(R);
+    const int tilesPerRow = (W + kRowPx - 1) / kRowPx, rowTiles = (H + R - 1) / R;
+    const int numTiles = N * rowTiles * tilesPerRow;   // < 2^31, checked by the launcher
     const uint32_t sW = smemAddr(smem);
     const uint32_t wBytes = 9u * Cout * Cin * 2u;
-    const uint32_t slabBytes = static_cast<uint32_t>(K16) * kSlabJStride;
+    const uint32_t slabBytes = static_cast<uint32_t>(K16) * JS;
     const uint32_t sSlab = sW + ((wBytes + 1023u) & ~1023u);
-    const uint32_t sStg = sSlab + stages * slabBytes, stgBytes = static_cast<uint32_t>(J1) * kStgJStride;
+    const uint32_t sStg = sSlab + stages * slabBytes, stgBytes = static_cast<uint32_t>(J1) * SJS;
     if (sW & 1023u) {   // TMA boxes need 128-byte aligned destinations; the layout assumes a 1024-byte aligned base
         if (tid == 0 && errorFlag) atomicOr(errorFlag, 1u);
         return;
@@ -460,26 +569,26 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     const uint32_t tmem = tmemBase;
     const int first = blockIdx.x, stride = gridDim.x;
     const int local = first < numTiles ? (numTiles - first + stride - 1) / stride : 0;
-    auto tileOf = [&](int i, int& n, int& y, int& x0) {
+    auto tileOf = [&](int i, int& n, int& y, int& x0) {   // y: the tile's first output row
         const unsigned t = static_cast<unsigned>(first + i * stride), r = t / tilesPerRow;
         x0 = static_cast<int>(t - r * tilesPerRow) * kRowPx;
-        y = static_cast<int>(r % static_cast<unsigned>(H));
-        n = static_cast<int>(r / static_cast<unsigned>(H));
+        y = static_cast<int>(r % static_cast<unsigned>(rowTiles)) * R;
+        n = static_cast<int>(r / static_cast<unsigned>(rowTiles));
     };
 
     if (warp >= 4 && warp < 8) {   // ---- producers
         // expanded 16-byte unit e = pt + 128 k is (input row d, block j, slab pixel r, half h) with
         // e = ((d * cpJ + j) * 130 + r) * 2 + h: a warp copies 16 consecutive pixels of one block
-        const int pt = tid - 128, total = 3 * kSlabPx * cpJ * 2, h = pt & 1;
-        const uint32_t txBytes = static_cast<uint32_t>(K16 - cpJ) * 3u * kSlabDStride;
+        const int pt = tid - 128, total = (R + 2) * kSlabPx * cpJ * 2, h = pt & 1;
+        const uint32_t txBytes = static_cast<uint32_t>(K16 - cpJ) * (R + 2u) * kSlabDStride;
         // staging TMA of local tile ii (upsampled input at its own resolution) into buffer ii & 1
         auto issueStage = [&](int ii) {
             int n2, y2, x2;
             tileOf(ii, n2, y2, x2);
             const uint32_t dst = sStg + (ii & 1) * stgBytes, bar = smemAddr(&stgFull[ii & 1]);
-            mbarArriveExpectTx(bar, static_cast<uint32_t>(J1) * 2u * kStgDStride);
+            mbarArriveExpectTx(bar, static_cast<uint32_t>(J1) * (R + 1u) * kStgDStride);
             for (int j = 0; j < J1; ++j)
-                tmaLoadBox(dst + j * kStgJStride, &mapX1, pass.c1lo + 16 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
+                tmaLoadBox(dst + j * SJS, &mapX1, pass.c1lo + 16 * j, (x2 - 1) >> 1, (y2 - 1) >> 1, n2, bar);
         };
         if (Up && pt == 0 && local > 0) issueStage(0);
         int b = 0, round = 0;
@@ -495,8 +604,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             if (pt == 0) {
                 mbarArriveExpectTx(full, txBytes);
                 for (int j = cpJ; j < K16; ++j) {
-                    if (j < J1) tmaLoadBox(slab + j * kSlabJStride, &mapX1, pass.c1lo + 16 * j, x0 - 1, y - 1, n, full);
-                    else tmaLoadBox(slab + j * kSlabJStride, &mapX2, pass.c2lo + 16 * (j - J1), x0 - 1, y - 1, n, full);
+                    if (j < J1) tmaLoadBox(slab + j * JS, &mapX1, pass.c1lo + 16 * j, x0 - 1, y - 1, n, full);
+                    else tmaLoadBox(slab + j * JS, &mapX2, pass.c2lo + 16 * (j - J1), x0 - 1, y - 1, n, full);
                 }
             }
             if (Up) {
@@ -519,8 +628,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 int j = 0, r = pt >> 1, d = 0, srow = 0;
                 for (int e = pt; e < total; e += 128) {
                     const int sx = ((x0 - 1 + r) >> 1) - sx0;
-                    stShared16(sw32(slab + j * kSlabJStride + d * kSlabDStride + r * 32 + h * 16),
-                               ldShared16(sw32(stg + j * kStgJStride + srow * kStgDStride + sx * 32 + h * 16)));
+                    stShared16(sw32(slab + j * JS + d * kSlabDStride + r * 32 + h * 16),
+                               ldShared16(sw32(stg + j * SJS + srow * kStgDStride + sx * 32 + h * 16)));
                     r += 64;
                     if (r >= kSlabPx) {   // 64 < 130: at most one wrap per step
                         r -= kSlabPx;
@@ -555,8 +664,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 }
                 asm volatile("fence.proxy.async.shared::cta;\n" ::);
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-                issueRowTile<K16>(tmem + static_cast<uint32_t>(a * Cout), smemDescSw32(sSlab + b * slabBytes),
-                                  bDesc0, bStep, idesc);
+                issueRowTile<K16, R>(tmem + static_cast<uint32_t>(a * R * Cout), Cout, smemDescSw32(sSlab + b * slabBytes),
+                                     bDesc0, bStep, idesc);
                 ummaCommit(smemAddr(&slabEmpty[b]));
                 ummaCommit(smemAddr(&accFull[a]));
                 issued = 1;
@@ -590,56 +699,58 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
             const int x = x0 + warp * 32 + lane;
-            // all of the pixel's Cout (<= 128) accumulator columns in flight at once, one wait; then the
-            // accumulator goes back to the MMA thread before the stores
-            uint32_t v[kRowMaxCout];
-            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * Cout);
+            const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * R * Cout);
 #pragma unroll
-            for (int q = 0; q < kRowMaxCout / 16; ++q)
-                if (16 * q < Cout) tmemLd16NoWait(taddr + 16 * q, v + 16 * q);
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
-            asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
-            __syncwarp();
-            if (lane == 0) mbarArrive(smemAddr(&accEmpty[a]));
-            if (++a == accs) { a = 0; ++aRound; }
-            if (x < W) {
-                const size_t px = (static_cast<size_t>(n) * H + y) * W + x;
-                if (pass.partIn) {   // earlier passes' FP32 sums
-                    const float4* pin = reinterpret_cast<const float4*>(pass.partIn + px * Cout);
-#pragma unroll
-                    for (int q = 0; q < kRowMaxCout / 4; ++q) {
-                        if (4 * q >= Cout) break;
-                        const float4 f = pin[q];
-                        v[4 * q] = __float_as_uint(__uint_as_float(v[4 * q]) + f.x);
-                        v[4 * q + 1] = __float_as_uint(__uint_as_float(v[4 * q + 1]) + f.y);
-                        v[4 * q + 2] = __float_as_uint(__uint_as_float(v[4 * q + 2]) + f.z);
-                        v[4 * q + 3] = __float_as_uint(__uint_as_float(v[4 * q + 3]) + f.w);
-                    }
+            for (int orow = 0; orow < R; ++orow) {
+                // all of the pixel's Cout (<= 128) accumulator columns of output row y + orow in flight at once,
+                // one wait; after the last row the accumulator goes back to the MMA thread before the stores
+                uint32_t v[kRowMaxCout];
+                tmemLoadWait(tbase + static_cast<uint32_t>(orow * Cout), Cout, v);
+                if (orow == R - 1) {
+                    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+                    __syncwarp();
+                    if (lane == 0) mbarArrive(smemAddr(&accEmpty[a]));
+                    if (++a == accs) { a = 0; ++aRound; }
                 }
-                if (pass.partOut) {
-                    float4* pout = reinterpret_cast<float4*>(pass.partOut + px * Cout);
+                if (x < W && y + orow < H) {
+                    const size_t px = (static_cast<size_t>(n) * H + y + orow) * W + x;
+                    if (pass.partIn) {   // earlier passes' FP32 sums
+                        const float4* pin = reinterpret_cast<const float4*>(pass.partIn + px * Cout);
 #pragma unroll
-                    for (int q = 0; q < kRowMaxCout / 4; ++q) {
-                        if (4 * q >= Cout) break;
-                        pout[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
-                                              __uint_as_float(v[4 * q + 3]));
-                    }
-                } else {
-                    uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
-#pragma unroll
-                    for (int q = 0; q < kRowMaxCout / 16; ++q) {
-                        if (16 * q >= Cout) break;
-                        uint32_t w8[8];
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            float p = __uint_as_float(v[16 * q + 2 * k]) + sBias[16 * q + 2 * k];
-                            float r = __uint_as_float(v[16 * q + 2 * k + 1]) + sBias[16 * q + 2 * k + 1];
-                            if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
-                            const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
-                            w8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                        for (int q = 0; q < kRowMaxCout / 4; ++q) {
+                            if (4 * q >= Cout) break;
+                            const float4 f = pin[q];
+                            v[4 * q] = __float_as_uint(__uint_as_float(v[4 * q]) + f.x);
+                            v[4 * q + 1] = __float_as_uint(__uint_as_float(v[4 * q + 1]) + f.y);
+                            v[4 * q + 2] = __float_as_uint(__uint_as_float(v[4 * q + 2]) + f.z);
+                            v[4 * q + 3] = __float_as_uint(__uint_as_float(v[4 * q + 3]) + f.w);
                         }
-                        dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
-                        dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                    }
+                    if (pass.partOut) {
+                        float4* pout = reinterpret_cast<float4*>(pass.partOut + px * Cout);
+#pragma unroll
+                        for (int q = 0; q < kRowMaxCout / 4; ++q) {
+                            if (4 * q >= Cout) break;
+                            pout[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                                  __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+                        }
+                    } else {
+                        uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
+#pragma unroll
+                        for (int q = 0; q < kRowMaxCout / 16; ++q) {
+                            if (16 * q >= Cout) break;
+                            uint32_t w8[8];
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) {
+                                float p = __uint_as_float(v[16 * q + 2 * k]) + sBias[16 * q + 2 * k];
+                                float r = __uint_as_float(v[16 * q + 2 * k + 1]) + sBias[16 * q + 2 * k + 1];
+                                if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
+                                const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
+                                w8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                            }
+                            dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
+                            dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                        }
                     }
                 }
             }
@@ -685,29 +796,31 @@ void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, i
 
 namespace {
 
-// shared memory: the weights, then the slab ring, then (upsampled X1) two staging buffers
-long long rowFixedBytes(int C1, int C2, bool up, int Cout)
+// shared memory: the weights, then the slab ring, then (upsampled X1) two staging buffers; R output rows per tile
+long long rowFixedBytes(int C1, int C2, bool up, int Cout, int R)
 {
-    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up && C1 > 0 ? 2LL * (C1 / 16) * kStgJStride : 0);
+    return ((9LL * Cout * (C1 + C2) * 2 + 1023) & ~1023LL) + (up && C1 > 0 ? 2LL * (C1 / 16) * stgJStride(R) : 0);
 }
 
 // slab buffers that fit beside the rest (at most kRowMaxStages; fewer than 2 = does not fit)
-int rowStages(int C1, int C2, bool up, int Cout)
+int rowStages(int C1, int C2, bool up, int Cout, int R)
 {
-    const long long fit = (kRowSmemBudget - rowFixedBytes(C1, C2, up, Cout)) / (static_cast<long long>((C1 + C2) / 16) * kSlabJStride);
+    const long long fit =
+        (kRowSmemBudget - rowFixedBytes(C1, C2, up, Cout, R)) / (static_cast<long long>((C1 + C2) / 16) * slabJStride(R));
     return static_cast<int>(fit < kRowMaxStages ? fit : kRowMaxStages);
 }
 
-int rowSmem(int C1, int C2, bool up, int Cout)
+int rowSmem(int C1, int C2, bool up, int Cout, int R)
 {
-    return static_cast<int>(rowFixedBytes(C1, C2, up, Cout) +
-                            static_cast<long long>(rowStages(C1, C2, up, Cout)) * ((C1 + C2) / 16) * kSlabJStride);
+    return static_cast<int>(rowFixedBytes(C1, C2, up, Cout, R) +
+                            static_cast<long long>(rowStages(C1, C2, up, Cout, R)) * ((C1 + C2) / 16) * slabJStride(R));
 }
 
-bool rowPassFits(int n1, int n2, bool up, int Cout)
+bool rowPassFits(int n1, int n2, bool up, int Cout, int R = 1)
 {
     const int cin = n1 + n2;
-    return cin >= 16 && n1 % 16 == 0 && n2 % 16 == 0 && cin <= 16 * kRowMaxK16 && rowStages(n1, n2, up, Cout) >= 2;
+    return cin >= 16 && n1 % 16 == 0 && n2 % 16 == 0 && cin <= (R == 1 ? 16 * kRowMaxK16 : 64) && R * Cout <= kRowMaxCout &&
+           rowStages(n1, n2, up, Cout, R) >= 2;
 }
 
 struct PassPlan {
@@ -800,22 +913,26 @@ void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
     if (plan.size() > 1 && (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 15)))
         throw std::runtime_error("conv3x3TcRow: this layer runs in passes and needs a 16-byte aligned scratch buffer");
     if (up && ((H | W) & 1)) throw std::runtime_error("conv3x3TcRow: an upsampled input needs even H and W");
-    const long long tiles = static_cast<long long>(N) * H * ((W + kRowPx - 1) / kRowPx);
-    if (tiles >= (1LL << 31)) throw std::runtime_error("conv3x3TcRow: more than 2^31 row tiles");
+    if (static_cast<long long>(N) * H * ((W + kRowPx - 1) / kRowPx) >= (1LL << 31))
+        throw std::runtime_error("conv3x3TcRow: more than 2^31 row tiles");
     if ((reinterpret_cast<uintptr_t>(X1) | reinterpret_cast<uintptr_t>(X2)) & 15)
         throw std::runtime_error("conv3x3TcRow: inputs must be 16-byte aligned");
-    CUtensorMap m1, m2;
-    std::memset(&m1, 0, sizeof(m1));
-    std::memset(&m2, 0, sizeof(m2));
-    if (C1 > 0) m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, 2) : slabMap(X1, C1, N, H, W, kSlabPx, 3);
-    if (C2 > 0) m2 = slabMap(X2, C2, N, H, W, kSlabPx, 3);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     for (size_t k = 0; k < plan.size(); ++k) {
         const PassPlan& pp = plan[k];
         const bool passUp = up && pp.n1 > 0;
-        const int smemBytes = rowSmem(pp.n1, pp.n2, passUp, Cout), stages = rowStages(pp.n1, pp.n2, passUp, Cout);
+        // two output rows per tile (the slab's 4 input rows serve 2 outputs instead of 3 serving 1) where it fits
+        // (up to 64 input channels: beyond that the unrolled descriptors of two rows spill)
+        const int R = rowPassFits(pp.n1, pp.n2, passUp, Cout, 2) ? 2 : 1;
+        const int smemBytes = rowSmem(pp.n1, pp.n2, passUp, Cout, R), stages = rowStages(pp.n1, pp.n2, passUp, Cout, R);
+        const long long tiles = static_cast<long long>(N) * ((H + R - 1) / R) * ((W + kRowPx - 1) / kRowPx);
+        CUtensorMap m1, m2;
+        std::memset(&m1, 0, sizeof(m1));
+        std::memset(&m2, 0, sizeof(m2));
+        if (pp.n1 > 0) m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, R + 1) : slabMap(X1, C1, N, H, W, kSlabPx, R + 2);
+        if (pp.n2 > 0) m2 = slabMap(X2, C2, N, H, W, kSlabPx, R + 2);
         RowPass pass{pp.c1lo, pp.c2lo, C1 + C2, pp.n1 > 0 ? pp.c1lo : C1 + pp.c2lo,
                      k > 0 ? static_cast<const float*>(scratch) : nullptr,
                      k + 1 < plan.size() ? static_cast<float*>(scratch) : nullptr};
@@ -823,39 +940,48 @@ void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
             cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smemBytes);
             int per = 0;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowThreads, smemBytes) != cudaSuccess || per < 1) per = 1;
-            // accumulator ring: up to kRowMaxAccs tiles of Cout columns in a power-of-two allocation, every
+            // accumulator ring: up to kRowMaxAccs tiles of R x Cout columns in a power-of-two allocation, every
             // resident CTA holding its tensor memory at once (512 columns per SM)
             int tmemCols = 32;
-            while (tmemCols < 2 * Cout) tmemCols *= 2;
+            while (tmemCols < 2 * R * Cout) tmemCols *= 2;
             if (per * tmemCols > 512) per = 512 / tmemCols;
-            while (tmemCols / Cout < kRowMaxAccs && per * tmemCols * 2 <= 512) tmemCols *= 2;
-            const int accs = tmemCols / Cout < kRowMaxAccs ? tmemCols / Cout : kRowMaxAccs;
+            while (tmemCols / (R * Cout) < kRowMaxAccs && per * tmemCols * 2 <= 512) tmemCols *= 2;
+            const int accs = tmemCols / (R * Cout) < kRowMaxAccs ? tmemCols / (R * Cout) : kRowMaxAccs;
             const long long grid = tiles < static_cast<long long>(sms) * per ? tiles : static_cast<long long>(sms) * per;
             kernel<<<static_cast<unsigned>(grid), kRowThreads, smemBytes, st>>>(m1, m2, pp.n1, pp.n2, N, H, W,
                                                                                static_cast<const bf16*>(Wk), bias, Cout,
                                                                                static_cast<bf16*>(Y), pass, stages, accs,
                                                                                tmemCols, errorFlag);
         };
-        auto byK = [&](auto relu_, auto up_) {
-            constexpr bool R = decltype(relu_)::value, U = decltype(up_)::value;
+        auto byK = [&](auto relu_, auto up_, auto r_) {
+            constexpr bool RL = decltype(relu_)::value, U = decltype(up_)::value;
+            constexpr int RR = decltype(r_)::value;
             switch ((pp.n1 + pp.n2) / 16) {
-                case 1: launch(kConvTcRow<R, U, 1>); break;
-                case 2: launch(kConvTcRow<R, U, 2>); break;
-                case 3: launch(kConvTcRow<R, U, 3>); break;
-                case 4: launch(kConvTcRow<R, U, 4>); break;
-                case 5: launch(kConvTcRow<R, U, 5>); break;
-                case 6: launch(kConvTcRow<R, U, 6>); break;
+                case 1: launch(kConvTcRow<RL, U, 1, RR>); break;
+                case 2: launch(kConvTcRow<RL, U, 2, RR>); break;
+                case 3: launch(kConvTcRow<RL, U, 3, RR>); break;
+                case 4: launch(kConvTcRow<RL, U, 4, RR>); break;
+                case 5:
+                    if constexpr (RR == 1) launch(kConvTcRow<RL, U, 5, 1>);
+                    break;
+                case 6:
+                    if constexpr (RR == 1) launch(kConvTcRow<RL, U, 6, 1>);
+                    break;
                 default: throw std::runtime_error("conv3x3TcRow: a pass takes 16 to 96 channels");
             }
+        };
+        auto byR = [&](auto relu_, auto up_) {
+            if (R == 2) byK(relu_, up_, std::integral_constant<int, 2>{});
+            else byK(relu_, up_, std::integral_constant<int, 1>{});
         };
         using T = std::true_type;
         using F = std::false_type;
         if (relu) {
-            if (passUp) byK(T{}, T{});
-            else byK(T{}, F{});
+            if (passUp) byR(T{}, T{});
+            else byR(T{}, F{});
         } else {
-            if (passUp) byK(F{}, T{});
-            else byK(F{}, F{});
+            if (passUp) byR(F{}, T{});
+            else byR(F{}, F{});
         }
     }
 }
