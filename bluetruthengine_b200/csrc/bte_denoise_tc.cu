@@ -494,8 +494,11 @@ __device__ __forceinline__ void issueRowTile(uint32_t acc, uint32_t Cout, uint64
 
 // One pass of a layer whose weights and slabs do not fit shared memory at once: the input channels
 // [c1lo, c1lo + C1) of X1 and [c2lo, c2lo + C2) of X2, weight columns [wOff, wOff + C1 + C2) of rows
-// wStride long.  partIn (FP32 [pixel][Cout], may alias partOut) is added to the accumulator; with partOut
-// the sum is stored there in FP32, otherwise bias and ReLU follow and Y receives bf16.
+// wStride long.  partIn (FP32, may alias partOut) is added to the accumulator; with partOut the sum is
+// stored there in FP32, otherwise bias and ReLU follow and Y receives bf16.  The partial sums are private
+// to the passes and laid out per 128-pixel row segment, channel-major inside it:
+// [(n * H + y) * tilesPerRow + x / 128][Cout][128], so a warp's 32 pixels of one channel are 128
+// contiguous bytes.
 struct RowPass {
     int c1lo, c2lo, wStride, wOff;
     const float* partIn;
@@ -714,25 +717,25 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 }
                 if (x < W && y + orow < H) {
                     const size_t px = (static_cast<size_t>(n) * H + y + orow) * W + x;
+                    const size_t seg = ((static_cast<size_t>(n) * H + y + orow) * tilesPerRow + x0 / kRowPx) * Cout * kRowPx +
+                                       (x - x0);   // this pixel's channel 0 in the partial-sum layout
                     if (pass.partIn) {   // earlier passes' FP32 sums
-                        const float4* pin = reinterpret_cast<const float4*>(pass.partIn + px * Cout);
 #pragma unroll
-                        for (int q = 0; q < kRowMaxCout / 4; ++q) {
-                            if (4 * q >= Cout) break;
-                            const float4 f = pin[q];
-                            v[4 * q] = __float_as_uint(__uint_as_float(v[4 * q]) + f.x);
-                            v[4 * q + 1] = __float_as_uint(__uint_as_float(v[4 * q + 1]) + f.y);
-                            v[4 * q + 2] = __float_as_uint(__uint_as_float(v[4 * q + 2]) + f.z);
-                            v[4 * q + 3] = __float_as_uint(__uint_as_float(v[4 * q + 3]) + f.w);
+                        for (int q = 0; q < kRowMaxCout / 16; ++q) {
+                            if (16 * q >= Cout) break;
+#pragma unroll
+                            for (int k = 0; k < 16; ++k)
+                                v[16 * q + k] = __float_as_uint(__uint_as_float(v[16 * q + k]) +
+                                                                pass.partIn[seg + static_cast<size_t>(16 * q + k) * kRowPx]);
                         }
                     }
                     if (pass.partOut) {
-                        float4* pout = reinterpret_cast<float4*>(pass.partOut + px * Cout);
 #pragma unroll
-                        for (int q = 0; q < kRowMaxCout / 4; ++q) {
-                            if (4 * q >= Cout) break;
-                            pout[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                                                  __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+                        for (int q = 0; q < kRowMaxCout / 16; ++q) {
+                            if (16 * q >= Cout) break;
+#pragma unroll
+                            for (int k = 0; k < 16; ++k)
+                                pass.partOut[seg + static_cast<size_t>(16 * q + k) * kRowPx] = __uint_as_float(v[16 * q + k]);
                         }
                     } else {
                         uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
@@ -866,7 +869,7 @@ size_t convTcRowScratchBytes(int C1, int C2, bool up, int Cout, int N, int H, in
 {
     std::vector<PassPlan> plan;
     if (!planRowPasses(C1, C2, up, Cout, &plan) || plan.size() < 2) return 0;
-    return static_cast<size_t>(N) * H * W * Cout * sizeof(float);
+    return static_cast<size_t>(N) * H * ((W + kRowPx - 1) / kRowPx) * kRowPx * Cout * sizeof(float);
 }
 
 namespace {
