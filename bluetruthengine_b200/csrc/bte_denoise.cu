@@ -198,8 +198,10 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
 // the input channels where weights and slabs do not fit shared memory at once); tcMode 1: layers that
 // fill the machine four times over with 128-pixel tiles go to the pixel-tile kernel; the rest to the
 // warp-level kernel.  force: -1 by tcMode, 0 warp-level, 1 pixel tiles, 2 row tiles.
-void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
-                  const float* bias, int Cout, bool relu, void* Y, cudaStream_t st, int force = -1)
+// pool (optional, row tiles only): also write the 2x2 average pool of Y there if the kernel can; returns
+// whether it did.
+bool convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+                  const float* bias, int Cout, bool relu, void* Y, cudaStream_t st, int force = -1, void* pool = nullptr)
 {
     const long long px = static_cast<long long>(N) * H * W;
     int kind = force;
@@ -216,11 +218,12 @@ void convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
     if (kind == 2) {
         const size_t scratch = convTcRowScratchBytes(C1, C2, up, Cout, N, H, W);
         if (scratch) net.rowScratch.ensure(scratch);
-        conv3x3TcRow(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, scratch ? net.rowScratch.p : nullptr,
-                     net.errFlag.as<unsigned int>(), st);
+        return conv3x3TcRow(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, scratch ? net.rowScratch.p : nullptr, pool,
+                            net.errFlag.as<unsigned int>(), st);
     }
-    else if (kind == 1) conv3x3Tc(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
+    if (kind == 1) conv3x3Tc(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, net.errFlag.as<unsigned int>(), st);
     else conv3x3Cat(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, st);
+    return false;
 }
 
 void checkTcFlag()
@@ -253,9 +256,13 @@ void forward(int N, int Hp, int Wp, bool training)
                              net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
                              c.relu, net.act[s.dst].p, st);
             } else {
-                convDispatch(net.act[s.src].p, c.cin, false, nullptr, 0, N, H, W,
-                             net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
-                             c.relu, net.act[s.dst].p, st);
+                // an inference conv whose output feeds the next step's pool may write the pool in its epilogue
+                const Step* next = k + 1 < kStepCount ? &kSteps[k + 1] : nullptr;
+                const bool fuse = !training && next && next->op == kPoolOp && next->src == s.dst;
+                if (convDispatch(net.act[s.src].p, c.cin, false, nullptr, 0, N, H, W,
+                                 net.wk.as<unsigned short>() + net.bfOff[s.conv], net.w.as<float>() + net.bOff[s.conv], c.cout,
+                                 c.relu, net.act[s.dst].p, st, -1, fuse ? net.act[next->dst].p : nullptr))
+                    ++k;   // the pool step is done
             }
         } else if (s.op == kPoolOp) {
             pool2(net.act[s.src].p, N, H, W, ts.c, net.act[s.dst].p, st);

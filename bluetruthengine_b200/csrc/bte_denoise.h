@@ -29,8 +29,11 @@ void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, i
 // an FP32 scratch buffer of convTcRowScratchBytes (0 for a single pass).
 bool convTcRowSupported(int C1, int C2, bool up, int Cout);
 size_t convTcRowScratchBytes(int C1, int C2, bool up, int Cout, int N, int H, int W);
-void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
-                  const float* bias, int Cout, bool relu, void* Y, void* scratch, unsigned int* errorFlag, cudaStream_t st);
+// pool (optional): also write the 2x2 average pool of Y there when the last pass runs two-row tiles;
+// returns whether it did.
+bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+                  const float* bias, int Cout, bool relu, void* Y, void* scratch, void* pool, unsigned int* errorFlag,
+                  cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);

@@ -353,7 +353,8 @@ __device__ __forceinline__ void stShared16(uint32_t addr, uint4 v)
 // Cout (16, 32, 48, 64, 96 or 128) consecutive 32-bit TMEM columns of the warp's 32 lanes into v, and the
 // wait for them inside the same asm statement: the registers are defined only once the wait has returned, so
 // the compiler cannot schedule a use of v between the load and the wait
-__device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t (&v)[128])
+template <int NV>
+__device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t (&v)[NV])
 {
     switch (Cout) {
         case 16:
@@ -406,6 +407,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                          : "r"(taddr + 0u));
             break;
         case 96:
+            if constexpr (NV >= 96) {
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%96];\n"
                          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79,%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95}, [%97];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
@@ -426,8 +428,10 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                            "=r"(v[84]), "=r"(v[85]), "=r"(v[86]), "=r"(v[87]), "=r"(v[88]), "=r"(v[89]),
                            "=r"(v[90]), "=r"(v[91]), "=r"(v[92]), "=r"(v[93]), "=r"(v[94]), "=r"(v[95])
                          : "r"(taddr + 0u), "r"(taddr + 64u));
+            }
             break;
         case 128:
+            if constexpr (NV >= 128) {
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x128.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63,%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79,%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95,%96,%97,%98,%99,%100,%101,%102,%103,%104,%105,%106,%107,%108,%109,%110,%111,%112,%113,%114,%115,%116,%117,%118,%119,%120,%121,%122,%123,%124,%125,%126,%127}, [%128];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
@@ -453,6 +457,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                            "=r"(v[120]), "=r"(v[121]), "=r"(v[122]), "=r"(v[123]), "=r"(v[124]), "=r"(v[125]),
                            "=r"(v[126]), "=r"(v[127])
                          : "r"(taddr + 0u));
+            }
             break;
         default: break;
     }
@@ -498,11 +503,14 @@ __device__ __forceinline__ void issueRowTile(uint32_t acc, uint32_t Cout, uint64
 // stored there in FP32, otherwise bias and ReLU follow and Y receives bf16.  The partial sums are private
 // to the passes and laid out per 128-pixel row segment, channel-major inside it:
 // [(n * H + y) * tilesPerRow + x / 128][Cout][128], so a warp's 32 pixels of one channel are 128
-// contiguous bytes.
+// contiguous bytes.  With pool (two output rows per tile, even H and W) the epilogue also writes the
+// 2x2 average of the bf16 outputs, summed in the order (y, x), (y, x + 1), (y + 1, x), (y + 1, x + 1) as the
+// separate pooling kernel does.
 struct RowPass {
     int c1lo, c2lo, wStride, wOff;
     const float* partIn;
     float* partOut;
+    bf16* pool;   // two-row tiles of the last pass: also the 2x2 average pool of Y ([N][H/2][W/2][Cout]), or null
 };
 
 template <bool Relu, bool Up, int K16, int R>
@@ -703,12 +711,19 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
             const int x = x0 + warp * 32 + lane;
             const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * R * Cout);
+            // the bf16 pairs of each output row, kept for the fused pool (two-row tiles have Cout <= 64)
+            uint32_t pk[R][32];
+#pragma unroll
+            for (int orow = 0; orow < R; ++orow)
+#pragma unroll
+                for (int q = 0; q < 32; ++q) pk[orow][q] = 0u;
 #pragma unroll
             for (int orow = 0; orow < R; ++orow) {
                 // all of the pixel's Cout (<= 128) accumulator columns of output row y + orow in flight at once,
                 // one wait; after the last row the accumulator goes back to the MMA thread before the stores
-                uint32_t v[kRowMaxCout];
-                tmemLoadWait(tbase + static_cast<uint32_t>(orow * Cout), Cout, v);
+                constexpr int NV = R == 2 ? 64 : kRowMaxCout;   // two-row tiles have Cout <= 64
+                uint32_t v[NV];
+                tmemLoadWait<NV>(tbase + static_cast<uint32_t>(orow * Cout), Cout, v);
                 if (orow == R - 1) {
                     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
                     __syncwarp();
@@ -721,7 +736,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                                        (x - x0);   // this pixel's channel 0 in the partial-sum layout
                     if (pass.partIn) {   // earlier passes' FP32 sums
 #pragma unroll
-                        for (int q = 0; q < kRowMaxCout / 16; ++q) {
+                        for (int q = 0; q < NV / 16; ++q) {
                             if (16 * q >= Cout) break;
 #pragma unroll
                             for (int k = 0; k < 16; ++k)
@@ -731,7 +746,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                     }
                     if (pass.partOut) {
 #pragma unroll
-                        for (int q = 0; q < kRowMaxCout / 16; ++q) {
+                        for (int q = 0; q < NV / 16; ++q) {
                             if (16 * q >= Cout) break;
 #pragma unroll
                             for (int k = 0; k < 16; ++k)
@@ -740,7 +755,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                     } else {
                         uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
 #pragma unroll
-                        for (int q = 0; q < kRowMaxCout / 16; ++q) {
+                        for (int q = 0; q < NV / 16; ++q) {
                             if (16 * q >= Cout) break;
                             uint32_t w8[8];
 #pragma unroll
@@ -753,7 +768,41 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                             }
                             dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
                             dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                            if (R == 2 && q < 4) {
+#pragma unroll
+                                for (int k = 0; k < 8; ++k) pk[orow][8 * q + k] = w8[k];
+                            }
                         }
+                    }
+                }
+            }
+            if (R == 2 && pass.pool) {   // fused 2x2 average pool: pairs of lanes hold x and x + 1 (warp-uniform)
+                const bool writer = (lane & 1) == 0 && x < W;
+                bf16* pdst = pass.pool + ((static_cast<size_t>(n) * (H >> 1) + (y >> 1)) * (W >> 1) + (x >> 1)) * Cout;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (16 * q >= Cout) break;
+                    uint32_t o8[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t a0 = pk[0][8 * q + k], c0 = pk[R - 1][8 * q + k];
+                        const uint32_t b0 = __shfl_xor_sync(0xffffffffu, a0, 1), d0 = __shfl_xor_sync(0xffffffffu, c0, 1);
+                        const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a0));
+                        const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&b0));
+                        const float2 fc = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&c0));
+                        const float2 fd = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&d0));
+                        float s0 = 0.0f, s1 = 0.0f;
+                        s0 += fa.x; s1 += fa.y;
+                        s0 += fb.x; s1 += fb.y;
+                        s0 += fc.x; s1 += fc.y;
+                        s0 += fd.x; s1 += fd.y;
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(0.25f * s0, 0.25f * s1);
+                        o8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                    }
+                    if (writer) {
+                        uint4* pd = reinterpret_cast<uint4*>(pdst + 16 * q);
+                        pd[0] = make_uint4(o8[0], o8[1], o8[2], o8[3]);
+                        pd[1] = make_uint4(o8[4], o8[5], o8[6], o8[7]);
                     }
                 }
             }
@@ -908,9 +957,11 @@ CUtensorMap slabMap(const void* base, int C, int N, int H, int W, int boxW, int 
 
 }  // namespace
 
-void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
-                  const float* bias, int Cout, bool relu, void* Y, void* scratch, unsigned int* errorFlag, cudaStream_t st)
+bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
+                  const float* bias, int Cout, bool relu, void* Y, void* scratch, void* pool, unsigned int* errorFlag,
+                  cudaStream_t st)
 {
+    bool pooled = false;
     std::vector<PassPlan> plan;
     if (!planRowPasses(C1, C2, up, Cout, &plan)) throw std::runtime_error("conv3x3TcRow: unsupported layer shape");
     if (plan.size() > 1 && (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 15)))
@@ -936,9 +987,12 @@ void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
         std::memset(&m2, 0, sizeof(m2));
         if (pp.n1 > 0) m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, R + 1) : slabMap(X1, C1, N, H, W, kSlabPx, R + 2);
         if (pp.n2 > 0) m2 = slabMap(X2, C2, N, H, W, kSlabPx, R + 2);
+        const bool last = k + 1 == plan.size();
+        const bool poolHere = pool && last && R == 2 && ((H | W) & 1) == 0;
         RowPass pass{pp.c1lo, pp.c2lo, C1 + C2, pp.n1 > 0 ? pp.c1lo : C1 + pp.c2lo,
-                     k > 0 ? static_cast<const float*>(scratch) : nullptr,
-                     k + 1 < plan.size() ? static_cast<float*>(scratch) : nullptr};
+                     k > 0 ? static_cast<const float*>(scratch) : nullptr, last ? nullptr : static_cast<float*>(scratch),
+                     poolHere ? static_cast<bf16*>(pool) : nullptr};
+        pooled = pooled || poolHere;
         auto launch = [&](auto kernel) {
             cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smemBytes);
             int per = 0;
@@ -987,6 +1041,7 @@ void conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
             else byR(F{}, F{});
         }
     }
+    return pooled;
 }
 
 }  // namespace dn
