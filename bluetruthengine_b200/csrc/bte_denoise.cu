@@ -16,8 +16,10 @@
 #include "bte_denoise.h"
 #include "bte_internal.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <iterator>
 #include <mutex>
 #include <random>
 #include <stdexcept>
@@ -104,6 +106,11 @@ struct Net {
     int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
+    // inference sequence (assemble, convolutions, output) captured in a CUDA graph for one shape, kernel
+    // choice and set of buffers; replayed while all of them stay the same
+    cudaGraphExec_t fwdExec = nullptr;
+    int fwdKey[6] = {};
+    const void* fwdPtrs[7] = {};
 };
 
 Net net;
@@ -324,7 +331,52 @@ int guardedDn(F&& fn)
 
 }  // namespace
 
-// Denoise [N, H, W] radiance (+ features) held on the device into `outRad`.
+namespace {
+
+void inferenceSequence(const float* dRad, const float* dFeat, int N, int H, int W, int Hp, int Wp, float* dOut, cudaStream_t st)
+{
+    assemble(dRad, dFeat, N, H, W, Hp, Wp, net.act[0].p, st);
+    forward(N, Hp, Wp, false);
+    output(net.act[27].p, net.act[0].p, N, H, W, Hp, Wp, dOut, st);
+}
+
+// Capture the sequence just run eagerly (buffers already allocated) for the next calls with the same key;
+// on any failure the denoiser simply stays eager.
+void captureInference(const float* dRad, const float* dFeat, int N, int H, int W, int Hp, int Wp, float* dOut,
+                      const int (&key)[6], const void* const (&ptrs)[7])
+{
+    if (net.fwdExec) {
+        cudaGraphExecDestroy(net.fwdExec);
+        net.fwdExec = nullptr;
+    }
+    cudaStream_t st = net.stream;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    bool ok = true;
+    try {
+        inferenceSequence(dRad, dFeat, N, H, W, Hp, Wp, dOut, st);
+    } catch (...) {
+        ok = false;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    cudaGraphExec_t exec = nullptr;
+    if (ok && e == cudaSuccess && g && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+        net.fwdExec = exec;
+        std::copy(std::begin(key), std::end(key), net.fwdKey);
+        std::copy(std::begin(ptrs), std::end(ptrs), net.fwdPtrs);
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+}
+
+}  // namespace
+
+// Denoise [N, H, W] radiance (+ features) held on the device into `outRad`.  The first call for a shape runs
+// eagerly and captures the sequence in a CUDA graph; later calls with the same shape, kernel choice and
+// buffers replay it (no per-kernel host work).
 void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, float* dOut, cudaStream_t waitOn)
 {
     if (!net.ready) throw CudaErr{"denoiser: no weights (bte_denoiser_init / bte_denoiser_set_params)"};
@@ -335,10 +387,19 @@ void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, f
         ck(cudaEventRecord(net.ev0, waitOn), "cudaEventRecord");
         ck(cudaStreamWaitEvent(st, net.ev0, 0), "cudaStreamWaitEvent");
     }
+    const int key[6] = {N, H, W, Hp, Wp, net.tcMode};
+    const void* const ptrs[7] = {dRad, dFeat, dOut, net.act[0].p, net.wk.p, net.w.p, net.rowScratch.p};
+    const bool replay = net.fwdExec && std::equal(std::begin(key), std::end(key), net.fwdKey) &&
+                        std::equal(std::begin(ptrs), std::end(ptrs), net.fwdPtrs);
     ck(cudaEventRecord(net.ev0, st), "cudaEventRecord");
-    assemble(dRad, dFeat, N, H, W, Hp, Wp, net.act[0].p, st);
-    forward(N, Hp, Wp, false);
-    output(net.act[27].p, net.act[0].p, N, H, W, Hp, Wp, dOut, st);
+    if (replay) {
+        ck(cudaGraphLaunch(net.fwdExec, st), "cudaGraphLaunch");
+    } else {
+        inferenceSequence(dRad, dFeat, N, H, W, Hp, Wp, dOut, st);
+        ck(cudaGetLastError(), "denoiser launch");
+        const void* const after[7] = {dRad, dFeat, dOut, net.act[0].p, net.wk.p, net.w.p, net.rowScratch.p};
+        captureInference(dRad, dFeat, N, H, W, Hp, Wp, dOut, key, after);
+    }
     ck(cudaGetLastError(), "denoiser launch");
     ck(cudaEventRecord(net.ev1, st), "cudaEventRecord");
     ck(cudaEventSynchronize(net.ev1), "denoise");
