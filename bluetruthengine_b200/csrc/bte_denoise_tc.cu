@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 #include <type_traits>
 #include <vector>
 
@@ -527,6 +528,9 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     __shared__ float sBias[kRowMaxCout];
     __shared__ uint32_t tmemBase;
     __shared__ volatile int abortFlag;
+    // programmatic dependent launch: the next convolution may start its prologue (weights, barriers, tensor
+    // memory) as soon as SMs free up; everything that reads or writes activations waits for this grid below
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int Cin = 16 * K16, C8 = Cin / 8, J1 = C1 / 16;   // Cin = C1 + C2 (multiples of 16), checked by the launcher
     const int cpJ = Up ? J1 : 0;   // blocks [0, cpJ) expanded from the staging area, [cpJ, K16) by TMA
@@ -577,6 +581,9 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    // the previous kernel in the stream (its activations, partial sums) has completed past this point; only
+    // the weights and bias, which no kernel in flight writes, were read before it
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     const uint32_t tmem = tmemBase;
     const int first = blockIdx.x, stride = gridDim.x;
     const int local = first < numTiles ? (numTiles - first + stride - 1) / stride : 0;
@@ -1005,10 +1012,21 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
             while (tmemCols / (R * Cout) < kRowMaxAccs && per * tmemCols * 2 <= 512) tmemCols *= 2;
             const int accs = tmemCols / (R * Cout) < kRowMaxAccs ? tmemCols / (R * Cout) : kRowMaxAccs;
             const long long grid = tiles < static_cast<long long>(sms) * per ? tiles : static_cast<long long>(sms) * per;
-            kernel<<<static_cast<unsigned>(grid), kRowThreads, smemBytes, st>>>(m1, m2, pp.n1, pp.n2, N, H, W,
-                                                                               static_cast<const bf16*>(Wk), bias, Cout,
-                                                                               static_cast<bf16*>(Y), pass, stages, accs,
-                                                                               tmemCols, errorFlag);
+            // launched as a programmatic dependent of the previous kernel in the stream (the kernel waits
+            // with griddepcontrol.wait before it touches activations)
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(static_cast<unsigned>(grid));
+            cfg.blockDim = dim3(kRowThreads);
+            cfg.dynamicSmemBytes = static_cast<size_t>(smemBytes);
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, m1, m2, pp.n1, pp.n2, N, H, W, static_cast<const bf16*>(Wk),
+                                                     bias, Cout, static_cast<bf16*>(Y), pass, stages, accs, tmemCols, errorFlag);
+            if (e != cudaSuccess) throw std::runtime_error(std::string("conv3x3TcRow: launch failed: ") + cudaGetErrorString(e));
         };
         auto byK = [&](auto relu_, auto up_, auto r_) {
             constexpr bool RL = decltype(relu_)::value, U = decltype(up_)::value;
