@@ -201,7 +201,7 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
 }
 
 // One 3x3 convolution over concat(up ? upsample(X1) : X1, X2).  tcMode 2: layers with at least 32
-// 128-pixel row tiles and Cout 16..64, 96 or 128 go to the tcgen05 row-tile kernel (in passes over
+// 128-pixel row tiles (64 if they run in passes) and Cout 16..64, 96 or 128 go to the tcgen05 row-tile kernel (in passes over
 // the input channels where weights and slabs do not fit shared memory at once); tcMode 1: layers that
 // fill the machine four times over with 128-pixel tiles go to the pixel-tile kernel; the rest to the
 // warp-level kernel.  force: -1 by tcMode, 0 warp-level, 1 pixel tiles, 2 row tiles.
@@ -215,7 +215,9 @@ bool convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
     if (kind < 0) {
         kind = 0;
         const long long rowTiles = static_cast<long long>(N) * H * ((W + 127) / 128);
-        if (net.tcMode == 2 && rowTiles >= 32 && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
+        // a layer that runs in passes pays one launch per pass: it needs twice the tiles of a one-pass layer
+        const bool passes = convTcRowScratchBytes(C1, C2, up, Cout, N, H, W) > 0;
+        if (net.tcMode == 2 && rowTiles >= (passes ? 64 : 32) && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
         else if (net.tcMode == 1 && px >= 128LL * 148 * 4 && convTcSupported(C1 + C2, Cout)) kind = 1;
     }
     if (kind == 2 && !convTcRowSupported(C1, C2, up, Cout))
