@@ -106,10 +106,12 @@ struct Net {
     int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
+    Buf upBuf;            // a decoder layer's upsampled input at full resolution (row-tile kernel)
+    unsigned allocGen = 0;   // bumped whenever a buffer the inference graph refers to is (re)allocated
     // inference sequence (assemble, convolutions, output) captured in a CUDA graph for one shape, kernel
     // choice and set of buffers; replayed while all of them stay the same
     cudaGraphExec_t fwdExec = nullptr;
-    int fwdKey[6] = {};
+    int fwdKey[7] = {};
     const void* fwdPtrs[7] = {};
 };
 
@@ -198,6 +200,7 @@ void ensureActs(int N, int Hp, int Wp, bool withGrad)
         if (withGrad) net.gact[t].ensure(elems * 2);
     }
     net.aN = N; net.aHp = Hp; net.aWp = Wp; net.aGrad = withGrad;
+    ++net.allocGen;
 }
 
 // One 3x3 convolution over concat(up ? upsample(X1) : X1, X2).  tcMode 2: layers with at least 32
@@ -224,9 +227,25 @@ bool convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
         throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64/96/128, Cin in 16-channel passes)"};
     if (kind == 1 && !convTcSupported(C1 + C2, Cout))
         throw CudaErr{"denoiser: the tcgen05 pixel-tile kernel does not take this layer"};
+    if (kind == 2 && up && convTcRowScratchBytes(C1, C2, up, Cout, N, H, W) == 0) {
+        // a one-pass layer reads its upsampled input fastest as a full-resolution tensor: upsample it first (one
+        // HBM pass) instead of expanding the half-resolution slab in shared memory per tile (measured on the
+        // level-0 decoder layer: 39 + 215 us against 282 us; the layers that run in passes are faster without)
+        const size_t need = static_cast<size_t>(N) * H * W * C1 * 2;
+        if (net.upBuf.bytes < need || !net.upBuf.p) {
+            net.upBuf.ensure(need);
+            ++net.allocGen;
+        }
+        upsample2(X1, N, H / 2, W / 2, C1, net.upBuf.p, st);
+        X1 = net.upBuf.p;
+        up = false;
+    }
     if (kind == 2) {
         const size_t scratch = convTcRowScratchBytes(C1, C2, up, Cout, N, H, W);
-        if (scratch) net.rowScratch.ensure(scratch);
+        if (scratch && (net.rowScratch.bytes < scratch || !net.rowScratch.p)) {
+            net.rowScratch.ensure(scratch);
+            ++net.allocGen;
+        }
         return conv3x3TcRow(X1, C1, up, X2, C2, N, H, W, Wk, bias, Cout, relu, Y, scratch ? net.rowScratch.p : nullptr, pool,
                             net.errFlag.as<unsigned int>(), st);
     }
@@ -345,7 +364,7 @@ void inferenceSequence(const float* dRad, const float* dFeat, int N, int H, int 
 // Capture the sequence just run eagerly (buffers already allocated) for the next calls with the same key;
 // on any failure the denoiser simply stays eager.
 void captureInference(const float* dRad, const float* dFeat, int N, int H, int W, int Hp, int Wp, float* dOut,
-                      const int (&key)[6], const void* const (&ptrs)[7])
+                      const int (&key)[7], const void* const (&ptrs)[7])
 {
     if (net.fwdExec) {
         cudaGraphExecDestroy(net.fwdExec);
@@ -389,7 +408,7 @@ void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, f
         ck(cudaEventRecord(net.ev0, waitOn), "cudaEventRecord");
         ck(cudaStreamWaitEvent(st, net.ev0, 0), "cudaStreamWaitEvent");
     }
-    const int key[6] = {N, H, W, Hp, Wp, net.tcMode};
+    const int key[7] = {N, H, W, Hp, Wp, net.tcMode, static_cast<int>(net.allocGen)};
     const void* const ptrs[7] = {dRad, dFeat, dOut, net.act[0].p, net.wk.p, net.w.p, net.rowScratch.p};
     const bool replay = net.fwdExec && std::equal(std::begin(key), std::end(key), net.fwdKey) &&
                         std::equal(std::begin(ptrs), std::end(ptrs), net.fwdPtrs);
@@ -399,8 +418,10 @@ void denoiseDevice(const float* dRad, const float* dFeat, int N, int H, int W, f
     ck(cudaGetLastError(), "denoiser launch");
     ck(cudaEventRecord(net.ev1, st), "cudaEventRecord");
     if (!replay) {   // capture after the timing event, so that the host work of the capture is not timed
+        // the eager run may have allocated buffers (generation bumped): the graph is keyed on the state after it
+        const int afterKey[7] = {N, H, W, Hp, Wp, net.tcMode, static_cast<int>(net.allocGen)};
         const void* const after[7] = {dRad, dFeat, dOut, net.act[0].p, net.wk.p, net.w.p, net.rowScratch.p};
-        captureInference(dRad, dFeat, N, H, W, Hp, Wp, dOut, key, after);
+        captureInference(dRad, dFeat, N, H, W, Hp, Wp, dOut, afterKey, after);
     }
     ck(cudaEventSynchronize(net.ev1), "denoise");
     ck(cudaEventElapsedTime(&net.lastMs, net.ev0, net.ev1), "cudaEventElapsedTime");

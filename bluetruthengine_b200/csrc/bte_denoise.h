@@ -41,6 +41,8 @@ void reluMask(const void* Y, const void* dY, void* out, long long elems, cudaStr
 void pool2(const void* X, int N, int H, int W, int C, void* Y, cudaStream_t st);
 void pool2Back(const void* dY, int N, int H, int W, int C, void* dX, cudaStream_t st);   // adds into dX
 void upCat(const void* A, int Ca, const void* B, int Cb, int N, int H, int W, void* out, cudaStream_t st);
+// nearest 2x upsampling of X [N][Hs][Ws][C] (C a multiple of 8) into Y [N][2Hs][2Ws][C]
+void upsample2(const void* X, int N, int Hs, int Ws, int C, void* Y, cudaStream_t st);
 void upCatBack(const void* dOut, int Ca, int Cb, int N, int H, int W, void* dA, void* dB, bool addB, cudaStream_t st);
 void assemble(const float* rad, const float* feat, int N, int H, int W, int Hp, int Wp, void* out, cudaStream_t st);
 void output(const void* net, const void* in, int N, int H, int W, int Hp, int Wp, float* rad, cudaStream_t st);

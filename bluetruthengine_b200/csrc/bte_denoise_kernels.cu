@@ -365,6 +365,27 @@ __global__ void kUpCat(const bf16* __restrict__ A, int Ca, const bf16* __restric
     }
 }
 
+// nearest 2x upsampling Y[N][2Hs][2Ws][C] = X[N][Hs][Ws][C]: one 16-byte chunk of a source pixel per
+// thread, written to its four destination pixels
+__global__ void kUpsample2(const uint4* __restrict__ X, int N, int Hs, int Ws, int C8, uint4* __restrict__ Y)
+{
+    const long long total = static_cast<long long>(N) * Hs * Ws * C8;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C8);
+        long long r = i / C8;
+        const int x = static_cast<int>(r % Ws); r /= Ws;
+        const int y = static_cast<int>(r % Hs);
+        const int n = static_cast<int>(r / Hs);
+        const uint4 v = X[i];
+        const size_t row0 = (static_cast<size_t>(n) * 2 * Hs + 2 * y) * (2 * Ws), row1 = row0 + 2 * Ws;
+        Y[(row0 + 2 * x) * C8 + c] = v;
+        Y[(row0 + 2 * x + 1) * C8 + c] = v;
+        Y[(row1 + 2 * x) * C8 + c] = v;
+        Y[(row1 + 2 * x + 1) * C8 + c] = v;
+    }
+}
+
 // gradient of kUpCat: dA = sum of the 2x2 block (written), dB = slice (written, or added if addB)
 __global__ void kUpCatBack(const bf16* __restrict__ dOut, int Ca, int Cb, int N, int H, int W, bf16* __restrict__ dA,
                            bf16* __restrict__ dB, int addB)
@@ -623,6 +644,12 @@ void upCat(const void* A, int Ca, const void* B, int Cb, int N, int H, int W, vo
 {
     kUpCat<<<gridFor(static_cast<long long>(N) * H * W * ((Ca + Cb) / 2)), 256, 0, st>>>(
         static_cast<const bf16*>(A), Ca, static_cast<const bf16*>(B), Cb, N, H, W, static_cast<bf16*>(out));
+}
+
+void upsample2(const void* X, int N, int Hs, int Ws, int C, void* Y, cudaStream_t st)
+{
+    kUpsample2<<<gridFor(static_cast<long long>(N) * Hs * Ws * (C / 8)), 256, 0, st>>>(static_cast<const uint4*>(X), N, Hs, Ws,
+                                                                                    C / 8, static_cast<uint4*>(Y));
 }
 
 void upCatBack(const void* dOut, int Ca, int Cb, int N, int H, int W, void* dA, void* dB, bool addB, cudaStream_t st)
