@@ -304,7 +304,7 @@ __host__ __device__ constexpr int stgJStride(int R) { return ((R + 1) * kStgDStr
 constexpr int kRowThreads = 288;
 constexpr int kRowMaxStages = 4;
 constexpr int kRowMaxAccs = 4;
-constexpr int kRowSmemBudget = 200 * 1024;
+constexpr int kRowSmemBudget = 218 * 1024;
 constexpr int kRowMaxK16 = 6;           // Cin up to 96 per pass
 constexpr int kRowMaxCout = 128;
 constexpr unsigned kRowSpin = 1u << 24;
