@@ -1,5 +1,8 @@
 // bte_denoise_tc.cu -- the denoiser's 3x3 convolution on the 5th-generation
-// tensor cores (tcgen05.mma, accumulator in tensor memory).
+// tensor cores (tcgen05.mma, accumulator in tensor memory).  Two kernels:
+// kConvTcRow (the default, further below: persistent, warp-specialised, row
+// tiles fed by TMA, weights resident) and kConvTc, the first version described
+// here (pixel tiles, operands gathered per tile by cp.async).
 //
 // Implicit GEMM: D[p][co] = sum_{tap, ci} A[p][(tap, ci)] * B[co][(tap, ci)]
 // over a CTA tile of 128 consecutive output pixels (flattened n, y, x) and
