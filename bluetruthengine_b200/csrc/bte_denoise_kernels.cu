@@ -302,8 +302,13 @@ __global__ void kReluMask(const bf16* __restrict__ Y, const bf16* __restrict__ d
 
 // ------------------------------------------------------------ pooling / upsampling
 // 2x2 average pool: [N, H, W, C] -> [N, H/2, W/2, C]
+// The pool, upsample and output kernels are launched as programmatic dependents of the convolution before
+// them (launchAfterConv): they wait for it here before touching memory.
+__device__ __forceinline__ void waitForPredecessor() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 __global__ void kPool2(const bf16* __restrict__ X, int N, int H, int W, int C, bf16* __restrict__ Y)
 {
+    waitForPredecessor();
     const int Ho = H / 2, Wo = W / 2, C2 = C / 2;
     const long long total = static_cast<long long>(N) * Ho * Wo * C2;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -369,6 +374,7 @@ __global__ void kUpCat(const bf16* __restrict__ A, int Ca, const bf16* __restric
 // thread, written to its four destination pixels
 __global__ void kUpsample2(const uint4* __restrict__ X, int N, int Hs, int Ws, int C8, uint4* __restrict__ Y)
 {
+    waitForPredecessor();
     const long long total = static_cast<long long>(N) * Hs * Ws * C8;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -456,6 +462,7 @@ __global__ void kAssemble(const float* __restrict__ rad, const float* __restrict
 __global__ void kOutput(const bf16* __restrict__ net, const bf16* __restrict__ in, int N, int H, int W, int Hp, int Wp,
                         float* __restrict__ rad)
 {
+    waitForPredecessor();
     const long long total = static_cast<long long>(N) * H * W;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -628,10 +635,27 @@ void reluMask(const void* Y, const void* dY, void* out, long long elems, cudaStr
                                                   static_cast<bf16*>(out), elems / 2);
 }
 
+// a small kernel as a programmatic dependent of the previous kernel in the stream: its blocks may be scheduled
+// while a convolution finishes (the convolutions signal their dependents early) and wait in the kernel
+template <typename Kernel, typename... Args>
+void launchAfterConv(Kernel kernel, int grid, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);   // errors surface through cudaGetLastError
+}
+
 void pool2(const void* X, int N, int H, int W, int C, void* Y, cudaStream_t st)
 {
-    kPool2<<<gridFor(static_cast<long long>(N) * (H / 2) * (W / 2) * (C / 2)), 256, 0, st>>>(
-        static_cast<const bf16*>(X), N, H, W, C, static_cast<bf16*>(Y));
+    launchAfterConv(kPool2, gridFor(static_cast<long long>(N) * (H / 2) * (W / 2) * (C / 2)), st, static_cast<const bf16*>(X), N,
+                    H, W, C, static_cast<bf16*>(Y));
 }
 
 void pool2Back(const void* dY, int N, int H, int W, int C, void* dX, cudaStream_t st)
@@ -648,8 +672,8 @@ void upCat(const void* A, int Ca, const void* B, int Cb, int N, int H, int W, vo
 
 void upsample2(const void* X, int N, int Hs, int Ws, int C, void* Y, cudaStream_t st)
 {
-    kUpsample2<<<gridFor(static_cast<long long>(N) * Hs * Ws * (C / 8)), 256, 0, st>>>(static_cast<const uint4*>(X), N, Hs, Ws,
-                                                                                    C / 8, static_cast<uint4*>(Y));
+    launchAfterConv(kUpsample2, gridFor(static_cast<long long>(N) * Hs * Ws * (C / 8)), st, static_cast<const uint4*>(X), N, Hs,
+                    Ws, C / 8, static_cast<uint4*>(Y));
 }
 
 void upCatBack(const void* dOut, int Ca, int Cb, int N, int H, int W, void* dA, void* dB, bool addB, cudaStream_t st)
@@ -667,8 +691,8 @@ void assemble(const float* rad, const float* feat, int N, int H, int W, int Hp, 
 
 void output(const void* net, const void* in, int N, int H, int W, int Hp, int Wp, float* rad, cudaStream_t st)
 {
-    kOutput<<<gridFor(static_cast<long long>(N) * H * W), 256, 0, st>>>(static_cast<const bf16*>(net),
-                                                                        static_cast<const bf16*>(in), N, H, W, Hp, Wp, rad);
+    launchAfterConv(kOutput, gridFor(static_cast<long long>(N) * H * W), st, static_cast<const bf16*>(net), static_cast<const bf16*>(in),
+                    N, H, W, Hp, Wp, rad);
 }
 
 void lossL1(const void* net, const void* in, const float* target, long long pixels, void* dNet, float* lossSum,
