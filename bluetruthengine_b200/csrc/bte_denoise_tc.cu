@@ -274,22 +274,27 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
 // same block seen from (dy * 130 + dx) * 32 bytes on (a pixel shift is one
 // row), so the nine taps are nine descriptors over one copy.  The layer's
 // weights stay in shared memory for the CTA's whole run.
-//   warps 4-7   producers.  Blocks read in place (X2, and X1 unless it is
-//               upsampled) come by TMA: one cp.async.bulk.tensor per block, a
-//               box of 16 channels x 130 pixels x 3 rows (32-byte rows, the
-//               copy engine swizzles and fills the out-of-image part with
-//               zeros).  An upsampled X1 comes by TMA at its own resolution
-//               (16 channels x 66 pixels x 2 rows per block, one tile ahead,
-//               into a double-buffered staging area) and the 128 producer
-//               threads expand it into the slab with 16-byte shared-memory
-//               copies, walking their chunks with running counters.
-//   warp 8      one thread issues 9 x Cin/16 tcgen05.mma (M = 128, N = Cout,
-//               K = 16) per tile, fully unrolled (Cin/16 is a template
-//               parameter) so that every descriptor is a base plus a constant:
-//               small MMAs are bound by their issue rate, and a runtime loop
-//               around them costs up to three times the issue time.  The MMAs
-//               are committed to the slab-free and accumulator-full barriers.
-//   warps 0-3   epilogue: tcgen05.ld of TMEM lanes 32w.., bias, ReLU, bf16 stores
+//   producers   blocks read in place (X2, and X1 unless it is upsampled) come
+//               by TMA: one cp.async.bulk.tensor per block, a box of 16
+//               channels x 130 pixels x R + 2 rows (32-byte rows, the copy
+//               engine swizzles and fills the out-of-image part with zeros),
+//               issued by one thread (lane 0 of warp 9).  With an upsampled X1
+//               (layers that run in passes) warps 4-7 produce instead: X1 comes
+//               by TMA at its own resolution (16 channels x 66 pixels x R + 1
+//               rows per block, one tile ahead, into a double-buffered staging
+//               area) and their 128 threads expand it into the slab with
+//               16-byte shared-memory copies, walking running counters.
+//   warp 8      one thread issues R x 9 x Cin/16 tcgen05.mma (M = 128, N =
+//               Cout, K = 16) per tile, fully unrolled (Cin/16 and R are
+//               template parameters) so that every descriptor is a base plus a
+//               constant: small MMAs are bound by their issue rate, and a
+//               runtime loop around them costs up to three times the issue
+//               time.  The MMAs are committed to the slab-free and
+//               accumulator-full barriers.
+//   epilogue    warps 0-7 (0-3 with an upsampled X1): tcgen05.ld of the TMEM
+//               lanes of warp w % 4, each of a pair of warps taking half of the
+//               output channels; the accumulator is released once read; bias,
+//               ReLU, bf16 stores (or FP32 partial sums), and the fused pool.
 // A ring of 2-4 slab buffers (as many as shared memory holds) and a ring of
 // 2-4 TMEM accumulators let copy, MMA and epilogue of consecutive tiles
 // overlap; CTAs are persistent over tiles.  Every wait is bounded: a timeout
@@ -304,7 +309,7 @@ constexpr int kStgDStride = kStgPx * 32;                            // 2112: one
 // source rows; blocks are swizzle-atom (256-byte) aligned
 __host__ __device__ constexpr int slabJStride(int R) { return ((R + 2) * kSlabDStride + 255) / 256 * 256; }
 __host__ __device__ constexpr int stgJStride(int R) { return ((R + 1) * kStgDStride + 255) / 256 * 256; }
-constexpr int kRowThreads = 288;
+constexpr int kRowThreads = 320;   // 10 warps: 0-7 epilogue / producers, 8 MMA, 9 TMA
 constexpr int kRowMaxStages = 4;
 constexpr int kRowMaxAccs = 4;
 constexpr int kRowSmemBudget = 218 * 1024;
@@ -354,13 +359,28 @@ __device__ __forceinline__ void stShared16(uint32_t addr, uint4 v)
     asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w));
 }
 
-// Cout (16, 32, 48, 64, 96 or 128) consecutive 32-bit TMEM columns of the warp's 32 lanes into v, and the
+// Cout (8, 16, 24, 32, 48, 64, 96 or 128) consecutive 32-bit TMEM columns of the warp's 32 lanes into v, and the
 // wait for them inside the same asm statement: the registers are defined only once the wait has returned, so
 // the compiler cannot schedule a use of v between the load and the wait
 template <int NV>
 __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t (&v)[NV])
 {
     switch (Cout) {
+        case 8:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                         : "r"(taddr));
+            break;
+        case 24:
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%24];\n"
+                         "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16,%17,%18,%19,%20,%21,%22,%23}, [%25];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+                           "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23])
+                         : "r"(taddr), "r"(taddr + 16u));
+            break;
         case 16:
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
@@ -381,6 +401,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                          : "r"(taddr + 0u));
             break;
         case 48:
+            if constexpr (NV >= 48) {
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%48];\n"
                          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%49];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
@@ -393,8 +414,10 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                            "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]),
                            "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47])
                          : "r"(taddr + 0u), "r"(taddr + 32u));
+            }
             break;
         case 64:
+            if constexpr (NV >= 64) {
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
@@ -409,6 +432,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                            "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]),
                            "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
                          : "r"(taddr + 0u));
+            }
             break;
         case 96:
             if constexpr (NV >= 96) {
@@ -565,12 +589,13 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
     if (tid < Cout) sBias[tid] = bias ? bias[tid] : 0.0f;
     if (tid == 0) {
         for (int b = 0; b < stages; ++b) {
-            mbarInit(smemAddr(&slabFull[b]), 129);   // 128 producer threads + the TMA thread's expect-tx arrival
+            // upsampled input: 128 expanding producer threads + the TMA thread's expect-tx arrival; else the latter only
+            mbarInit(smemAddr(&slabFull[b]), Up ? 129 : 1);
             mbarInit(smemAddr(&slabEmpty[b]), 1);
         }
         for (int b = 0; b < accs; ++b) {
             mbarInit(smemAddr(&accFull[b]), 1);
-            mbarInit(smemAddr(&accEmpty[b]), 4);
+            mbarInit(smemAddr(&accEmpty[b]), Up ? 4 : 8);   // one arrival per epilogue warp
         }
         for (int b = 0; b < 2; ++b) {
             mbarInit(smemAddr(&stgFull[b]), 1);
@@ -597,10 +622,15 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
         n = static_cast<int>(r / static_cast<unsigned>(rowTiles));
     };
 
-    if (warp >= 4 && warp < 8) {   // ---- producers
+    // roles: upsampled input -- warps 4-7 produce (TMA by thread 128, expansion by all), warps 0-3 epilogue;
+    // otherwise -- lane 0 of warp 9 produces (TMA), warps 0-7 epilogue (two per TMEM lane group, each taking
+    // half of the output channels); warp 8 issues the MMAs
+    const bool producer = Up ? (warp >= 4 && warp < 8) : (warp == 9 && lane == 0);
+    const bool epilogue = Up ? warp < 4 : warp < 8;
+    if (producer) {   // ---- producers
         // expanded 16-byte unit e = pt + 128 k is (input row d, block j, slab pixel r, half h) with
         // e = ((d * cpJ + j) * 130 + r) * 2 + h: a warp copies 16 consecutive pixels of one block
-        const int pt = tid - 128, total = (R + 2) * kSlabPx * cpJ * 2, h = pt & 1;
+        const int pt = Up ? tid - 128 : 0, total = (R + 2) * kSlabPx * cpJ * 2, h = pt & 1;
         const uint32_t txBytes = static_cast<uint32_t>(K16 - cpJ) * (R + 2u) * kSlabDStride;
         // staging TMA of local tile ii (upsampled input at its own resolution) into buffer ii & 1
         auto issueStage = [&](int ii) {
@@ -664,7 +694,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 asm volatile("fence.proxy.async.shared::cta;\n" ::);   // the tensor cores read what was written here
                 mbarArrive(smemAddr(&stgEmpty[i & 1]));
             }
-            mbarArrive(full);
+            if (Up) mbarArrive(full);
             if (++b == stages) { b = 0; ++round; }
         }
     } else if (warp == 8) {   // ---- MMA issue
@@ -707,9 +737,12 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 }
             }
         }
-    } else {   // ---- epilogue, warps 0-3: TMEM lanes 32w..32w+31 = tile pixels 32w..32w+31
+    } else if (epilogue) {   // ---- epilogue: TMEM lanes 32 (w % 4).. = tile pixels, channels [c0, c0 + Cc)
         // the wait is made warp-uniform (__all_sync) so that no lane leaves the loop alone before the
         // warp-wide tcgen05.ld and __syncwarp
+        const int grp = warp & 3, Cc = Up ? Cout : Cout >> 1, c0 = Up ? 0 : (warp >> 2) * Cc;
+        // registers per thread: its channels of one output row (two-row tiles have Cout <= 64)
+        constexpr int NV = R == 2 ? (Up ? 64 : 32) : (Up ? kRowMaxCout : kRowMaxCout / 2);
         int a = 0, aRound = 0;
         for (int i = 0; i < local && !abortFlag; ++i) {
             int n, y, x0;
@@ -719,21 +752,19 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-            const int x = x0 + warp * 32 + lane;
-            const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(a * R * Cout);
-            // the bf16 pairs of each output row, kept for the fused pool (two-row tiles have Cout <= 64)
-            uint32_t pk[R][32];
+            const int x = x0 + grp * 32 + lane;
+            const uint32_t tbase = tmem + (static_cast<uint32_t>(grp * 32) << 16) + static_cast<uint32_t>(a * R * Cout + c0);
+            uint32_t pk[R][NV / 2];   // the bf16 pairs of each output row, kept for the fused pool
 #pragma unroll
             for (int orow = 0; orow < R; ++orow)
 #pragma unroll
-                for (int q = 0; q < 32; ++q) pk[orow][q] = 0u;
+                for (int q = 0; q < NV / 2; ++q) pk[orow][q] = 0u;
 #pragma unroll
             for (int orow = 0; orow < R; ++orow) {
-                // all of the pixel's Cout (<= 128) accumulator columns of output row y + orow in flight at once,
-                // one wait; after the last row the accumulator goes back to the MMA thread before the stores
-                constexpr int NV = R == 2 ? 64 : kRowMaxCout;   // two-row tiles have Cout <= 64
+                // this thread's Cc accumulator columns of output row y + orow in flight at once, one wait; after the
+                // last row the accumulator goes back to the MMA thread before the stores
                 uint32_t v[NV];
-                tmemLoadWait<NV>(tbase + static_cast<uint32_t>(orow * Cout), Cout, v);
+                tmemLoadWait<NV>(tbase + static_cast<uint32_t>(orow * Cout), Cc, v);
                 if (orow == R - 1) {
                     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
                     __syncwarp();
@@ -743,44 +774,43 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                 if (x < W && y + orow < H) {
                     const size_t px = (static_cast<size_t>(n) * H + y + orow) * W + x;
                     const size_t seg = ((static_cast<size_t>(n) * H + y + orow) * tilesPerRow + x0 / kRowPx) * Cout * kRowPx +
-                                       (x - x0);   // this pixel's channel 0 in the partial-sum layout
+                                       static_cast<size_t>(c0) * kRowPx + (x - x0);   // channel c0 in the partial-sum layout
                     if (pass.partIn) {   // earlier passes' FP32 sums
 #pragma unroll
-                        for (int q = 0; q < NV / 16; ++q) {
-                            if (16 * q >= Cout) break;
+                        for (int q = 0; q < NV / 8; ++q) {
+                            if (8 * q >= Cc) break;
 #pragma unroll
-                            for (int k = 0; k < 16; ++k)
-                                v[16 * q + k] = __float_as_uint(__uint_as_float(v[16 * q + k]) +
-                                                                pass.partIn[seg + static_cast<size_t>(16 * q + k) * kRowPx]);
+                            for (int k = 0; k < 8; ++k)
+                                v[8 * q + k] = __float_as_uint(__uint_as_float(v[8 * q + k]) +
+                                                               pass.partIn[seg + static_cast<size_t>(8 * q + k) * kRowPx]);
                         }
                     }
                     if (pass.partOut) {
 #pragma unroll
-                        for (int q = 0; q < NV / 16; ++q) {
-                            if (16 * q >= Cout) break;
+                        for (int q = 0; q < NV / 8; ++q) {
+                            if (8 * q >= Cc) break;
 #pragma unroll
-                            for (int k = 0; k < 16; ++k)
-                                pass.partOut[seg + static_cast<size_t>(16 * q + k) * kRowPx] = __uint_as_float(v[16 * q + k]);
+                            for (int k = 0; k < 8; ++k)
+                                pass.partOut[seg + static_cast<size_t>(8 * q + k) * kRowPx] = __uint_as_float(v[8 * q + k]);
                         }
                     } else {
-                        uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout);
+                        uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout + c0);
 #pragma unroll
-                        for (int q = 0; q < NV / 16; ++q) {
-                            if (16 * q >= Cout) break;
-                            uint32_t w8[8];
+                        for (int q = 0; q < NV / 8; ++q) {   // 8 channels (16 bytes) at a time
+                            if (8 * q >= Cc) break;
+                            uint32_t w4[4];
 #pragma unroll
-                            for (int k = 0; k < 8; ++k) {
-                                float p = __uint_as_float(v[16 * q + 2 * k]) + sBias[16 * q + 2 * k];
-                                float r = __uint_as_float(v[16 * q + 2 * k + 1]) + sBias[16 * q + 2 * k + 1];
+                            for (int k = 0; k < 4; ++k) {
+                                float p = __uint_as_float(v[8 * q + 2 * k]) + sBias[c0 + 8 * q + 2 * k];
+                                float r = __uint_as_float(v[8 * q + 2 * k + 1]) + sBias[c0 + 8 * q + 2 * k + 1];
                                 if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
                                 const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
-                                w8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                                w4[k] = *reinterpret_cast<const uint32_t*>(&h);
                             }
-                            dst[2 * q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
-                            dst[2 * q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
-                            if (R == 2 && q < 4) {
+                            dst[q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                            if (R == 2) {
 #pragma unroll
-                                for (int k = 0; k < 8; ++k) pk[orow][8 * q + k] = w8[k];
+                                for (int k = 0; k < 4; ++k) pk[orow][4 * q + k] = w4[k];
                             }
                         }
                     }
@@ -788,18 +818,18 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             }
             if (R == 2 && pass.pool) {   // fused 2x2 average pool: pairs of lanes hold x and x + 1 (warp-uniform)
                 const bool writer = (lane & 1) == 0 && x < W;
-                bf16* pdst = pass.pool + ((static_cast<size_t>(n) * (H >> 1) + (y >> 1)) * (W >> 1) + (x >> 1)) * Cout;
+                bf16* pdst = pass.pool + ((static_cast<size_t>(n) * (H >> 1) + (y >> 1)) * (W >> 1) + (x >> 1)) * Cout + c0;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (16 * q >= Cout) break;
-                    uint32_t o8[8];
+                for (int q = 0; q < NV / 8; ++q) {
+                    if (8 * q >= Cc) break;
+                    uint32_t o4[4];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const uint32_t a0 = pk[0][8 * q + k], c0 = pk[R - 1][8 * q + k];
-                        const uint32_t b0 = __shfl_xor_sync(0xffffffffu, a0, 1), d0 = __shfl_xor_sync(0xffffffffu, c0, 1);
+                    for (int k = 0; k < 4; ++k) {
+                        const uint32_t a0 = pk[0][4 * q + k], e0 = pk[R - 1][4 * q + k];
+                        const uint32_t b0 = __shfl_xor_sync(0xffffffffu, a0, 1), d0 = __shfl_xor_sync(0xffffffffu, e0, 1);
                         const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a0));
                         const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&b0));
-                        const float2 fc = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&c0));
+                        const float2 fc = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&e0));
                         const float2 fd = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&d0));
                         float s0 = 0.0f, s1 = 0.0f;
                         s0 += fa.x; s1 += fa.y;
@@ -807,13 +837,9 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                         s0 += fc.x; s1 += fc.y;
                         s0 += fd.x; s1 += fd.y;
                         const __nv_bfloat162 h = __floats2bfloat162_rn(0.25f * s0, 0.25f * s1);
-                        o8[k] = *reinterpret_cast<const uint32_t*>(&h);
+                        o4[k] = *reinterpret_cast<const uint32_t*>(&h);
                     }
-                    if (writer) {
-                        uint4* pd = reinterpret_cast<uint4*>(pdst + 16 * q);
-                        pd[0] = make_uint4(o8[0], o8[1], o8[2], o8[3]);
-                        pd[1] = make_uint4(o8[4], o8[5], o8[6], o8[7]);
-                    }
+                    if (writer) reinterpret_cast<uint4*>(pdst)[q] = make_uint4(o4[0], o4[1], o4[2], o4[3]);
                 }
             }
         }
