@@ -373,6 +373,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                          : "r"(taddr));
             break;
         case 24:
+            if constexpr (NV >= 24) {
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%24];\n"
                          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16,%17,%18,%19,%20,%21,%22,%23}, [%25];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
@@ -380,6 +381,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
                            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23])
                          : "r"(taddr), "r"(taddr + 16u));
+            }
             break;
         case 16:
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
@@ -390,6 +392,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                          : "r"(taddr + 0u));
             break;
         case 32:
+            if constexpr (NV >= 32) {
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
                          "tcgen05.wait::ld.sync.aligned;\n"
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
@@ -399,6 +402,7 @@ __device__ __forceinline__ void tmemLoadWait(uint32_t taddr, int Cout, uint32_t 
                            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
                            "=r"(v[30]), "=r"(v[31])
                          : "r"(taddr + 0u));
+            }
             break;
         case 48:
             if constexpr (NV >= 48) {
@@ -742,7 +746,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
         // warp-wide tcgen05.ld and __syncwarp
         const int grp = warp & 3, Cc = Up ? Cout : Cout >> 1, c0 = Up ? 0 : (warp >> 2) * Cc;
         // registers per thread: its channels of one output row (two-row tiles have Cout <= 64)
-        constexpr int NV = R == 2 ? (Up ? 64 : 32) : (Up ? kRowMaxCout : kRowMaxCout / 2);
+        constexpr int NV = R == 4 ? 16 : R == 2 ? (Up ? 64 : 32) : (Up ? kRowMaxCout : kRowMaxCout / 2);
         int a = 0, aRound = 0;
         for (int i = 0; i < local && !abortFlag; ++i) {
             int n, y, x0;
@@ -808,7 +812,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                                 w4[k] = *reinterpret_cast<const uint32_t*>(&h);
                             }
                             dst[q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
-                            if (R == 2) {
+                            if (R >= 2) {
 #pragma unroll
                                 for (int k = 0; k < 4; ++k) pk[orow][4 * q + k] = w4[k];
                             }
@@ -816,16 +820,19 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                     }
                 }
             }
-            if (R == 2 && pass.pool) {   // fused 2x2 average pool: pairs of lanes hold x and x + 1 (warp-uniform)
-                const bool writer = (lane & 1) == 0 && x < W;
-                bf16* pdst = pass.pool + ((static_cast<size_t>(n) * (H >> 1) + (y >> 1)) * (W >> 1) + (x >> 1)) * Cout + c0;
+            if (R >= 2 && pass.pool) {   // fused 2x2 average pool: pairs of lanes hold x and x + 1 (warp-uniform)
+#pragma unroll
+              for (int pr = 0; pr < R / 2; ++pr) {   // output rows y + 2 pr, y + 2 pr + 1 -> pooled row y / 2 + pr
+                const bool writer = (lane & 1) == 0 && x < W && y + 2 * pr < H;
+                bf16* pdst =
+                    pass.pool + ((static_cast<size_t>(n) * (H >> 1) + (y >> 1) + pr) * (W >> 1) + (x >> 1)) * Cout + c0;
 #pragma unroll
                 for (int q = 0; q < NV / 8; ++q) {
                     if (8 * q >= Cc) break;
                     uint32_t o4[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        const uint32_t a0 = pk[0][4 * q + k], e0 = pk[R - 1][4 * q + k];
+                        const uint32_t a0 = pk[2 * pr][4 * q + k], e0 = pk[2 * pr + 1][4 * q + k];
                         const uint32_t b0 = __shfl_xor_sync(0xffffffffu, a0, 1), d0 = __shfl_xor_sync(0xffffffffu, e0, 1);
                         const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&a0));
                         const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&b0));
@@ -841,6 +848,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                     }
                     if (writer) reinterpret_cast<uint4*>(pdst)[q] = make_uint4(o4[0], o4[1], o4[2], o4[3]);
                 }
+              }
             }
         }
     }
@@ -907,6 +915,7 @@ int rowSmem(int C1, int C2, bool up, int Cout, int R)
 bool rowPassFits(int n1, int n2, bool up, int Cout, int R = 1)
 {
     const int cin = n1 + n2;
+    if (R == 4 && (up || cin > 32 || Cout > 32)) return false;   // four-row tiles: small layers only
     return cin >= 16 && n1 % 16 == 0 && n2 % 16 == 0 && cin <= (R == 1 ? 16 * kRowMaxK16 : 64) && R * Cout <= kRowMaxCout &&
            rowStages(n1, n2, up, Cout, R) >= 2;
 }
@@ -1015,7 +1024,7 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
         const bool passUp = up && pp.n1 > 0;
         // two output rows per tile (the slab's 4 input rows serve 2 outputs instead of 3 serving 1) where it fits
         // (up to 64 input channels: beyond that the unrolled descriptors of two rows spill)
-        const int R = rowPassFits(pp.n1, pp.n2, passUp, Cout, 2) ? 2 : 1;
+        const int R = rowPassFits(pp.n1, pp.n2, passUp, Cout, 4) ? 4 : rowPassFits(pp.n1, pp.n2, passUp, Cout, 2) ? 2 : 1;
         const int smemBytes = rowSmem(pp.n1, pp.n2, passUp, Cout, R), stages = rowStages(pp.n1, pp.n2, passUp, Cout, R);
         const long long tiles = static_cast<long long>(N) * ((H + R - 1) / R) * ((W + kRowPx - 1) / kRowPx);
         CUtensorMap m1, m2;
@@ -1024,7 +1033,7 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
         if (pp.n1 > 0) m1 = up ? slabMap(X1, C1, N, H / 2, W / 2, kStgPx, R + 1) : slabMap(X1, C1, N, H, W, kSlabPx, R + 2);
         if (pp.n2 > 0) m2 = slabMap(X2, C2, N, H, W, kSlabPx, R + 2);
         const bool last = k + 1 == plan.size();
-        const bool poolHere = pool && last && R == 2 && ((H | W) & 1) == 0;
+        const bool poolHere = pool && last && R >= 2 && ((H | W) & 1) == 0;
         RowPass pass{pp.c1lo, pp.c2lo, C1 + C2, pp.n1 > 0 ? pp.c1lo : C1 + pp.c2lo,
                      k > 0 ? static_cast<const float*>(scratch) : nullptr, last ? nullptr : static_cast<float*>(scratch),
                      poolHere ? static_cast<bf16*>(pool) : nullptr};
@@ -1063,8 +1072,12 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
             switch ((pp.n1 + pp.n2) / 16) {
                 case 1: launch(kConvTcRow<RL, U, 1, RR>); break;
                 case 2: launch(kConvTcRow<RL, U, 2, RR>); break;
-                case 3: launch(kConvTcRow<RL, U, 3, RR>); break;
-                case 4: launch(kConvTcRow<RL, U, 4, RR>); break;
+                case 3:
+                    if constexpr (RR <= 2) launch(kConvTcRow<RL, U, 3, RR>);
+                    break;
+                case 4:
+                    if constexpr (RR <= 2) launch(kConvTcRow<RL, U, 4, RR>);
+                    break;
                 case 5:
                     if constexpr (RR == 1) launch(kConvTcRow<RL, U, 5, 1>);
                     break;
@@ -1075,7 +1088,8 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
             }
         };
         auto byR = [&](auto relu_, auto up_) {
-            if (R == 2) byK(relu_, up_, std::integral_constant<int, 2>{});
+            if (R == 4) byK(relu_, up_, std::integral_constant<int, 4>{});
+            else if (R == 2) byK(relu_, up_, std::integral_constant<int, 2>{});
             else byK(relu_, up_, std::integral_constant<int, 1>{});
         };
         using T = std::true_type;

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 # small shapes run the tap-split kernel, the last (3 x 300 x 4 = 3600 CTAs of 64 pixels) the unsplit one
 SHAPES = [(2, 20, 37, 32, 48), (1, 16, 64, 16, 32), (1, 9, 70, 224, 96), (2, 8, 24, 80, 16), (4, 300, 130, 32, 48),
-          (1, 12, 150, 112, 48), (1, 10, 140, 96, 128)]
+          (1, 12, 150, 112, 48), (1, 10, 140, 96, 128), (1, 10, 140, 32, 16)]
 
 
 def _bf16(a):
