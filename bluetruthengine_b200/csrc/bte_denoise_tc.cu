@@ -264,9 +264,10 @@ __global__ void __launch_bounds__(128, 1) kConvTc(const bf16* __restrict__ X1, i
 
 
 // ---------------------------------------------------------------- row tiles, warp-specialised
-// For the full-resolution layers (few channels, many pixels): a tile is 128
-// consecutive pixels of one image row.  Its input is the 3-row x 130-pixel
-// slab around it (all Cin channels), staged in shared memory once in the
+// For every layer with enough pixels: a tile is 128 consecutive pixels of R
+// consecutive image rows (R = 1, 2 or 4 by the layer's size).  Its input is
+// the (R + 2)-row x 130-pixel slab around it (the pass's input channels),
+// staged in shared memory once in the
 // canonical K-major layout with 32-byte swizzling: block jb of 16 channels
 // holds slab pixel r of input row d as one 32-byte row at
 // jb * kSlabJStride + (d * 130 + r) * 32, its two 16-byte halves exchanged
@@ -305,7 +306,7 @@ constexpr int kSlabPx = kRowPx + 2;
 constexpr int kSlabDStride = kSlabPx * 32;                          // 4160: one input row of one 16-channel block
 constexpr int kStgPx = kRowPx / 2 + 2;                              // 66 source pixels of an upsampled input
 constexpr int kStgDStride = kStgPx * 32;                            // 2112: one source row of one block
-// A tile covers R output rows (1 or 2): its slab holds R + 2 input rows, an upsampled input's staging R + 1
+// A tile covers R output rows (1, 2 or 4): its slab holds R + 2 input rows, an upsampled input's staging R + 1
 // source rows; blocks are swizzle-atom (256-byte) aligned
 __host__ __device__ constexpr int slabJStride(int R) { return ((R + 2) * kSlabDStride + 255) / 256 * 256; }
 __host__ __device__ constexpr int stgJStride(int R) { return ((R + 1) * kStgDStride + 255) / 256 * 256; }
@@ -745,7 +746,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
         // the wait is made warp-uniform (__all_sync) so that no lane leaves the loop alone before the
         // warp-wide tcgen05.ld and __syncwarp
         const int grp = warp & 3, Cc = Up ? Cout : Cout >> 1, c0 = Up ? 0 : (warp >> 2) * Cc;
-        // registers per thread: its channels of one output row (two-row tiles have Cout <= 64)
+        // registers per thread: its channels of one output row (two-row tiles have Cout <= 64, four-row ones <= 32)
         constexpr int NV = R == 4 ? 16 : R == 2 ? (Up ? 64 : 32) : (Up ? kRowMaxCout : kRowMaxCout / 2);
         int a = 0, aRound = 0;
         for (int i = 0; i < local && !abortFlag; ++i) {
