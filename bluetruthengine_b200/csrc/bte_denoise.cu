@@ -103,7 +103,7 @@ struct Net {
     Buf dsNoisy, dsFeat, dsTarget;
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
-    int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles
+    int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2/3 tcgen05 row tiles
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
     Buf upBuf;            // a decoder layer's upsampled input at full resolution (row-tile kernel)
@@ -220,17 +220,17 @@ bool convDispatch(const void* X1, int C1, bool up, const void* X2, int C2, int N
         const long long rowTiles = static_cast<long long>(N) * H * ((W + 127) / 128);
         // a layer that runs in passes pays one launch per pass: it needs twice the tiles of a one-pass layer
         const bool passes = convTcRowScratchBytes(C1, C2, up, Cout, N, H, W) > 0;
-        if (net.tcMode == 2 && rowTiles >= (passes ? 64 : 32) && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
+        if ((net.tcMode == 2 || net.tcMode == 3) && rowTiles >= (passes ? 64 : 32) && convTcRowSupported(C1, C2, up, Cout)) kind = 2;
         else if (net.tcMode == 1 && px >= 128LL * 148 * 4 && convTcSupported(C1 + C2, Cout)) kind = 1;
     }
     if (kind == 2 && !convTcRowSupported(C1, C2, up, Cout))
         throw CudaErr{"denoiser: the tcgen05 row-tile kernel does not take this layer (Cout 16/32/48/64/96/128, Cin in 16-channel passes)"};
     if (kind == 1 && !convTcSupported(C1 + C2, Cout))
         throw CudaErr{"denoiser: the tcgen05 pixel-tile kernel does not take this layer"};
-    if (kind == 2 && up && convTcRowScratchBytes(C1, C2, up, Cout, N, H, W) == 0) {
-        // a one-pass layer reads its upsampled input fastest as a full-resolution tensor: upsample it first (one
-        // HBM pass) instead of expanding the half-resolution slab in shared memory per tile (measured on the
-        // level-0 decoder layer: 39 + 215 us against 282 us; the layers that run in passes are faster without)
+    if (kind == 2 && up && net.tcMode != 3) {
+        // the row-tile kernel reads an upsampled input fastest as a full-resolution tensor: upsample it first (one
+        // HBM pass) instead of expanding the half-resolution slab in shared memory per tile (measured over the
+        // network at 1080p: 1.205 ms against 1.24 ms; mode 3 keeps the in-kernel expansion)
         const size_t need = static_cast<size_t>(N) * H * W * C1 * 2;
         if (net.upBuf.bytes < need || !net.upBuf.p) {
             net.upBuf.ensure(need);
@@ -595,11 +595,12 @@ int bte_denoiser_denoise(const float* radiance, const float* features, int width
     });
 }
 
-// full-resolution convolutions: 0 the warp-level mma.sync kernel only; 1 tcgen05 pixel tiles; 2 tcgen05 row tiles
+// convolution kernels: 0 the warp-level mma.sync kernel only; 1 tcgen05 pixel tiles; 2 tcgen05 row tiles (decoder
+// inputs upsampled first); 3 tcgen05 row tiles expanding upsampled inputs in shared memory
 int bte_denoiser_set_tcgen05(int mode)
 {
     return guardedDn([&] {
-        if (mode < 0 || mode > 2) throw CudaErr{"bte_denoiser_set_tcgen05: mode must be 0, 1 or 2"};
+        if (mode < 0 || mode > 3) throw CudaErr{"bte_denoiser_set_tcgen05: mode must be 0, 1, 2 or 3"};
         ensureNet();
         net.tcMode = mode;
         return 0;

@@ -83,8 +83,9 @@ class Denoiser:
 
     def set_tcgen05(self, mode):
         """Convolution kernels: 0 (or False) the warp-level MMA kernel only, 1 (or True) the tcgen05 pixel-tile
-        kernel for the full-resolution layers, 2 (the default) the tcgen05 row-tile kernel for every layer
-        with at least one 128-pixel row tile per SM (layers it does not take stay on the warp-level kernel)."""
+        kernel for the full-resolution layers, 2 (the default) the tcgen05 row-tile kernel for every layer with
+        enough 128-pixel row tiles (layers it does not take stay on the warp-level kernel), decoder inputs
+        upsampled beforehand; 3 the same with the upsampling done inside the row-tile kernel."""
         _check(self.lib.bte_denoiser_set_tcgen05(int(mode)))
 
     def last_ms(self) -> float:
@@ -119,7 +120,8 @@ def _main(argv=None):
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--iters", type=int, default=5)
-    ap.add_argument("--kernels", type=int, default=2, help="0 warp-level MMA only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles")
+    ap.add_argument("--kernels", type=int, default=2,
+                    help="0 warp-level MMA only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles, 3 row tiles upsampling in-kernel")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                       "denoiser_c4.npz"))
     args = ap.parse_args(argv)

@@ -195,13 +195,13 @@ def _torch_unet(params, rad, feat):
     return np.maximum(np.expm1(pred.permute(1, 2, 0).numpy()), 0)[:H, :W]
 
 
-@pytest.mark.parametrize("tc", [0, 2])
+@pytest.mark.parametrize("tc", [0, 2, 3])
 @pytest.mark.parametrize("size", [(72, 100), (470, 640)])
 def test_network_inference_matches_torch(dn, size, tc):
     """The whole inference path (feature assembly, edge padding, encoder, in-place upsample+concat decoder,
     residual output) against the same network written in PyTorch, on a random network; the larger size
     runs the full-resolution layers on the unsplit warp-level kernel (tc 0) or on the tcgen05 row-tile
-    kernel, the upsample + concat layer included (tc 2)."""
+    kernel, the upsample + concat layers included, upsampled beforehand (tc 2) or inside the kernel (tc 3)."""
     dn.init(11)
     p = dn.params()
     rng = np.random.default_rng(5)
@@ -220,8 +220,9 @@ def test_network_inference_matches_torch(dn, size, tc):
     assert err.mean() < 5e-3 and err.max() < 0.1
 
 
+@pytest.mark.parametrize("tc", [2, 3])
 @pytest.mark.parametrize("size", [(560, 720), (976, 1280)])
-def test_network_inference_row_passes_match_torch(dn, size):
+def test_network_inference_row_passes_match_torch(dn, size, tc):
     """The row-tile kernel on layers that run in passes over their input channels with FP32 partial sums:
     at these sizes the level-1 decoder layer (upsampled 64 + 48 channels -> 48) and, at the larger one,
     the level-2 decoder layer (upsampled 96 + 64 -> 64) are large enough for the tensor-core path."""
@@ -231,7 +232,7 @@ def test_network_inference_row_passes_match_torch(dn, size):
     H, W = size
     rad = rng.exponential(0.4, size=(H, W, 3)).astype(np.float32)
     feat = np.concatenate([rng.uniform(0, 1, (H, W, 3)), rng.normal(size=(H, W, 3))], -1).astype(np.float32)
-    dn.set_tcgen05(2)
+    dn.set_tcgen05(tc)
     try:
         got = dn.denoise(rad, feat)
     finally:
