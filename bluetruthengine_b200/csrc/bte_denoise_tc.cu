@@ -800,22 +800,36 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                         }
                     } else {
                         uint4* dst = reinterpret_cast<uint4*>(Y + px * Cout + c0);
+                        // 16 channels (32 bytes, one sector) per 256-bit store where the channel group is 32-byte
+                        // aligned, else 8 channels per 128-bit store
+                        const bool wide = (c0 & 15) == 0 && (Cc & 15) == 0;
 #pragma unroll
-                        for (int q = 0; q < NV / 8; ++q) {   // 8 channels (16 bytes) at a time
+                        for (int q = 0; q < NV / 8; q += 2) {   // 8-channel units q and q + 1
                             if (8 * q >= Cc) break;
-                            uint32_t w4[4];
+                            const bool second = 8 * (q + 1) < Cc;
+                            uint32_t w8[8];
 #pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                float p = __uint_as_float(v[8 * q + 2 * k]) + sBias[c0 + 8 * q + 2 * k];
-                                float r = __uint_as_float(v[8 * q + 2 * k + 1]) + sBias[c0 + 8 * q + 2 * k + 1];
-                                if (Relu) { p = fmaxf(p, 0.0f); r = fmaxf(r, 0.0f); }
-                                const __nv_bfloat162 h = __floats2bfloat162_rn(p, r);
-                                w4[k] = *reinterpret_cast<const uint32_t*>(&h);
+                            for (int k = 0; k < 8; ++k) {
+                                const int ch = 8 * q + 2 * k;   // units q (k < 4) and q + 1 (k >= 4)
+                                if (k >= 4 && !second) { w8[k] = 0u; continue; }
+                                float pv = __uint_as_float(v[ch]) + sBias[c0 + ch];
+                                float rv = __uint_as_float(v[ch + 1]) + sBias[c0 + ch + 1];
+                                if (Relu) { pv = fmaxf(pv, 0.0f); rv = fmaxf(rv, 0.0f); }
+                                const __nv_bfloat162 h = __floats2bfloat162_rn(pv, rv);
+                                w8[k] = *reinterpret_cast<const uint32_t*>(&h);
                             }
-                            dst[q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                            if (wide) {
+                                asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};\n" ::"l"(dst + q), "r"(w8[0]),
+                                             "r"(w8[1]), "r"(w8[2]), "r"(w8[3]), "r"(w8[4]), "r"(w8[5]), "r"(w8[6]), "r"(w8[7])
+                                             : "memory");
+                            } else {
+                                dst[q] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
+                                if (second) dst[q + 1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+                            }
                             if (R >= 2) {
 #pragma unroll
-                                for (int k = 0; k < 4; ++k) pk[orow][4 * q + k] = w4[k];
+                                for (int k = 0; k < 8; ++k)
+                                    if (4 * q + k < NV / 2) pk[orow][4 * q + k] = w8[k];
                             }
                         }
                     }
