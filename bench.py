@@ -198,6 +198,69 @@ def batched_views_leg(scene, args):
             "one_view_at_a_time_ms": seq, "one_view_at_a_time_msamples_per_s": samples / seq / 1e3}
 
 
+def multi_scene_leg(scene, args):
+    """Several scenes in one batch (bte_render_scene_batch): the bench scene in slot 0 and five seeded instanced
+    scenes in slots 1-5 (2, 8, 20, 40 and 80 placements of 25,000-triangle meshes: 50k to 2M triangles, under the
+    procedural sky), each with 8 seeded views from {320x240, 640x480, 1280x720, 1920x1080} at 1, 2 or 4 samples
+    per frame (48 views); one batch frame against the same six scenes rendered one bte_render_views call after
+    another.  Host wall clock around each call (each ends with its frames finished), median of 5."""
+    import time
+    import bluetruthengine_b200 as bte
+    from bluetruthengine_b200 import scenes
+    r = bte.Renderer()
+    env = bte.ENV_ALIAS if args.env == "alias" else bte.ENV_CDF
+    rng = np.random.default_rng(4)
+    sizes = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
+    batch, tris = [], []
+    try:
+        for slot, n_inst in enumerate([0, 2, 8, 20, 40, 80]):
+            r.select_scene(slot)
+            sc = scene
+            if n_inst:
+                sc = bte.load_scene(scenes.large_instanced(seed=10 + slot, width=640, height=480, n_instances=n_inst,
+                                                           n_meshes=4, env_w=1024, env_h=512))
+                r.cleanup()
+                r.upload(sc)
+            r.set_config(samples_per_frame=1, max_depth=args.depth, rr_start=3, env_sampling=env)
+            r.reset_views()
+            base = np.asarray(sc.camera, dtype=bte.CAMERA_DTYPE).copy()
+            views = []
+            for k in range(8):
+                w, h = sizes[rng.integers(0, 4)]
+                cam = base.copy()
+                cam["origin"] = cam["origin"] + np.float32(0.3 * k) * cam["right"]
+                cam["aspect"] = np.float32(w / h)
+                views.append((cam, w, h, int(rng.choice([1, 2, 4]))))
+            batch.append((slot, views))
+            tris.append(int(len(sc.triangles)))
+        r.select_scene(0)
+        samples = sum(w * h * s for _, v in batch for _, w, h, s in v)
+        for _ in range(2):
+            r.render_scene_batch(batch)
+        tb, ts = [], []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            r.render_scene_batch(batch)
+            tb.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            for slot, views in batch:
+                r.select_scene(slot)
+                r.render_views(views)
+            ts.append(time.perf_counter() - t0)
+            r.select_scene(0)
+        tb, ts = statistics.median(tb) * 1e3, statistics.median(ts) * 1e3
+    finally:
+        for slot in range(1, len(batch)):
+            r.select_scene(slot)
+            r.reset_views()
+            r.cleanup()
+        r.select_scene(0)
+        r.reset_views()
+    return {"scenes": len(batch), "triangles": tris, "views": sum(len(v) for _, v in batch),
+            "samples_per_frame": samples, "batch_ms": tb, "batch_msamples_per_s": samples / tb / 1e3,
+            "scene_at_a_time_ms": ts, "scene_at_a_time_msamples_per_s": samples / ts / 1e3}
+
+
 def denoise_leg():
     """Second half of the metric: device time to relMSE <= 2e-3 against the FP64 16384-spp image, plain
     accumulation vs denoised low-spp, on the Cornell box (256x256, depth 8); plus the denoiser's inference
@@ -416,6 +479,10 @@ def run_ours(args):
             out["batched_views"] = batched_views_leg(scene, args)
         except Exception as e:
             out["batched_views"] = {"unavailable": str(e)}
+        try:
+            out["multi_scene"] = multi_scene_leg(scene, args)
+        except Exception as e:
+            out["multi_scene"] = {"unavailable": str(e)}
     if rank == 0 and not args.no_denoise:
         try:
             out["denoise"] = denoise_leg()

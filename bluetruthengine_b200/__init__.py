@@ -407,6 +407,27 @@ class Renderer:
     def reset_views(self):
         _check(self.lib.bte_reset_views())
 
+    def select_scene(self, scene: int):
+        """Make scene slot 0..7 the one every upload, configuration and render call acts on."""
+        _check(self.lib.bte_select_scene(int(scene)))
+
+    def selected_scene(self) -> int:
+        out = C.c_int(0)
+        _check(self.lib.bte_get_selected_scene(C.byref(out)))
+        return out.value
+
+    def render_scene_batch(self, batch):
+        """One frame of several scene slots' views (sequence of (slot, views), views as for render_views): every
+        scene's launch sequence is enqueued on its own streams before any wait, so the scenes run side by side."""
+        slots = np.array([int(k) for k, _ in batch], dtype=np.int32)
+        counts = np.array([len(v) for _, v in batch], dtype=np.int32)
+        flat = [view for _, v in batch for view in v]
+        arr = np.zeros(len(flat), dtype=VIEW_DTYPE)
+        for i, (cam, w, h, spp) in enumerate(flat):
+            arr[i]["camera"] = np.asarray(cam, dtype=CAMERA_DTYPE)
+            arr[i]["width"], arr[i]["height"], arr[i]["samplesPerFrame"] = w, h, spp
+        _check(self.lib.bte_render_scene_batch(_ptr(slots), _ptr(counts), _ptr(arr), len(batch)))
+
     def set_aov(self, enabled: bool):
         """Accumulate first-hit albedo and shading normal per pixel (denoiser features)."""
         _check(self.lib.bte_set_aov(1 if enabled else 0))

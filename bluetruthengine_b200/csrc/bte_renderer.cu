@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace bte {
@@ -132,6 +133,8 @@ struct Renderer {
     };
     std::vector<ViewState> views;
     DeviceBuffer viewTable;
+    ViewDesc* hViewTable = nullptr;   // pinned staging of the view table: its upload does not block the host
+    int pendDepth = 0, pendPaths = 0, pendCount = 0;   // a view frame enqueued and not yet finished
     bool stageTiming = false;
     int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
     BteFrameStats stats{};
@@ -145,9 +148,23 @@ struct Renderer {
     std::vector<unsigned char> graphKey;
 };
 
+// Scene slots: the selected slot's state lives in g, the others are parked in g_parked (the selected
+// slot's own entry there is empty).  Every upload and render entry point acts on g.
+constexpr int kMaxScenes = 8;
 Renderer g;
+Renderer g_parked[kMaxScenes];
+int g_scene = 0;
 std::mutex g_mutex;
 constexpr int kMaxViews = 64;
+
+void selectScene(int k)
+{
+    if (k < 0 || k >= kMaxScenes) throw CudaError{"bte_select_scene: scene slot out of range (0..7)"};
+    if (k == g_scene) return;
+    std::swap(g, g_parked[g_scene]);
+    std::swap(g, g_parked[k]);
+    g_scene = k;
+}
 
 void ensureInit()
 {
@@ -525,7 +542,9 @@ void renderFrame(int w, int h)
 
 // Several camera views of the scene in one frame: one launch sequence over the concatenated paths of all
 // views (each view's paths sample-major as in bte_render), each view accumulating into its own buffers.
-void renderViews(const BteView* views, int count)
+// launchViews only enqueues (no host wait once the buffers exist); finishViews waits for the frame and
+// reads its counters, so several scenes' frames can be enqueued on their own streams before any wait.
+void launchViews(const BteView* views, int count)
 {
     if (!views || count <= 0) throw CudaError{"bte_render_views: no views"};
     if (count > kMaxViews) throw CudaError{"bte_render_views: at most 64 views per frame"};
@@ -574,7 +593,11 @@ void renderViews(const BteView* views, int count)
         g.gridBlock = block;
     }
     ensure(g.viewTable, sizeof(ViewDesc) * kMaxViews);
-    ck(cudaMemcpyAsync(g.viewTable.p, vd.data(), sizeof(ViewDesc) * count, cudaMemcpyHostToDevice, g.stream),
+    if (!g.hViewTable)
+        ck(cudaHostAlloc(reinterpret_cast<void**>(&g.hViewTable), sizeof(ViewDesc) * kMaxViews, cudaHostAllocDefault),
+           "cudaHostAlloc");
+    std::memcpy(g.hViewTable, vd.data(), sizeof(ViewDesc) * count);   // the previous view frame has finished
+    ck(cudaMemcpyAsync(g.viewTable.p, g.hViewTable, sizeof(ViewDesc) * count, cudaMemcpyHostToDevice, g.stream),
        "cudaMemcpyAsync");
     DevPaths P;
     std::memset(&P, 0, sizeof(P));
@@ -616,6 +639,15 @@ void renderViews(const BteView* views, int count)
     launchPresentViews(P, f, static_cast<int>(pixels64), st);
     ck(cudaGetLastError(), "kernel launch");
     ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
+    g.pendDepth = depth; g.pendPaths = paths; g.pendCount = count;
+}
+
+void finishViews(const BteView* views)
+{
+    const int depth = g.pendDepth, paths = g.pendPaths, count = g.pendCount;
+    g.pendCount = 0;
+    if (count <= 0) return;
+    cudaStream_t st = g.stream;
     std::vector<int> rc(static_cast<size_t>(depth + 1)), sc(static_cast<size_t>(depth + 1));
     unsigned int errFlags = 0;
     ck(cudaMemcpyAsync(rc.data(), g.rayCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
@@ -637,6 +669,53 @@ void renderViews(const BteView* views, int count)
     g.lastPaths = 0;   // per-path debug readbacks refer to single-view frames
     if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
     if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+}
+
+void renderViews(const BteView* views, int count)
+{
+    launchViews(views, count);
+    finishViews(views);
+}
+
+// One batch over several scene slots: every scene's view frame is enqueued on its own streams first, then
+// each is finished in turn, so the scenes' launch sequences run side by side on the GPU.  Each scene's
+// views accumulate exactly as bte_render_views would leave them; the selected slot is restored.
+void renderSceneBatch(const int* scenes, const int* viewCounts, const BteView* views, int sceneCount)
+{
+    if (!scenes || !viewCounts || !views || sceneCount <= 0 || sceneCount > kMaxScenes)
+        throw CudaError{"bte_render_scene_batch: 1..8 scenes with their view counts and views are required"};
+    bool seen[kMaxScenes] = {};
+    std::vector<int> offset(static_cast<size_t>(sceneCount) + 1, 0);
+    for (int i = 0; i < sceneCount; ++i) {
+        if (scenes[i] < 0 || scenes[i] >= kMaxScenes) throw CudaError{"bte_render_scene_batch: scene slot out of range (0..7)"};
+        if (seen[scenes[i]]) throw CudaError{"bte_render_scene_batch: a scene slot appears twice"};
+        seen[scenes[i]] = true;
+        if (viewCounts[i] <= 0 || viewCounts[i] > kMaxViews)
+            throw CudaError{"bte_render_scene_batch: each scene needs 1..64 views"};
+        offset[static_cast<size_t>(i) + 1] = offset[static_cast<size_t>(i)] + viewCounts[i];
+    }
+    const int home = g_scene;
+    std::string firstError;
+    int launched = 0;
+    for (; launched < sceneCount && firstError.empty(); ++launched) {
+        selectScene(scenes[launched]);
+        try {
+            ensureInit();
+            launchViews(views + offset[static_cast<size_t>(launched)], viewCounts[launched]);
+        } catch (const CudaError& e) {
+            firstError = e.msg;
+        }
+    }
+    for (int i = 0; i < launched; ++i) {   // finish every enqueued frame, even after an error
+        selectScene(scenes[i]);
+        try {
+            finishViews(views + offset[static_cast<size_t>(i)]);
+        } catch (const CudaError& e) {
+            if (firstError.empty()) firstError = e.msg;
+        }
+    }
+    selectScene(home);
+    if (!firstError.empty()) throw CudaError{firstError};
 }
 
 template <typename F>
@@ -997,6 +1076,32 @@ int bte_reset_views(void)
     return guarded([&] {
         for (auto& v : g.views) { v.accum.release(); v.accumD.release(); v.fb.release(); }
         g.views.clear();
+        return 0;
+    });
+}
+
+int bte_select_scene(int scene)
+{
+    return guarded([&] {
+        selectScene(scene);
+        ensureInit();
+        return 0;
+    });
+}
+
+int bte_get_selected_scene(int* scene)
+{
+    return guarded([&] {
+        if (!scene) throw CudaError{"bte_get_selected_scene: null pointer"};
+        *scene = g_scene;
+        return 0;
+    });
+}
+
+int bte_render_scene_batch(const int* scenes, const int* viewCounts, const BteView* views, int sceneCount)
+{
+    return guarded([&] {
+        renderSceneBatch(scenes, viewCounts, views, sceneCount);
         return 0;
     });
 }

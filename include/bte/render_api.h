@@ -103,6 +103,16 @@ typedef struct {
 int bte_render_views(const BteView* views, int count);            /* at most 64 views */
 int bte_read_view_accum(int view, float* hostRGB, double* hostRGBSum);   /* W*H*3 each; either may be NULL */
 int bte_reset_views(void);
+/* Scene slots (no reference counterpart; the reference holds one scene): up to 8 independent scenes, each
+ * with its own geometry, tree, materials, lights, env map, configuration, streams and view accumulations.
+ * Every upload, configuration and render call acts on the selected slot (slot 0 at start). */
+int bte_select_scene(int scene);                    /* 0..7 */
+int bte_get_selected_scene(int* scene);
+/* Several scenes' view batches in one call: scene scenes[i] renders the next viewCounts[i] entries of views.
+ * Every scene's launch sequence is enqueued on its own streams before any host wait, so the scenes run side by
+ * side on the GPU; each scene's views accumulate exactly as bte_render_views on that slot would leave them.
+ * Slots must be distinct; the selected slot is unchanged afterwards. */
+int bte_render_scene_batch(const int* scenes, const int* viewCounts, const BteView* views, int sceneCount);
 int bte_toggle_denoiser(void);                      /* :192; returns new state (0/1) or <0; needs denoiser weights */
 int bte_read_denoised(float* hostRGB);               /* W*H*3 denoised mean radiance of the last frame (denoiser on) */
 int bte_set_render_mode(int mode);                                              /* :205 */

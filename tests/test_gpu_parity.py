@@ -573,3 +573,59 @@ def test_batched_views_match_single_view_frames(renderer, bte, random_scene):
         assert np.array_equal(bits(renderer.read_accum(w, h)), bits(bm))
         assert np.array_equal(renderer.read_accum_f64(w, h).view(np.uint64), bs.view(np.uint64))
     renderer.reset_views()
+
+
+def _views_of(bte, scene, sizes):
+    base = np.asarray(scene.camera, dtype=bte.CAMERA_DTYPE).copy()
+    views = []
+    for k, (w, h, spp) in enumerate(sizes):
+        cam = base.copy()
+        cam["origin"] = cam["origin"] + np.float32(0.3 * k) * cam["right"]
+        cam["aspect"] = np.float32(w / h)
+        views.append((cam, w, h, spp))
+    return views
+
+
+def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene):
+    """Two scene slots (the random scene with its env map, the Cornell box), each with views of uneven size and
+    samples per frame, rendered side by side in one batch for two frames: every view's FP32 mean and FP64 sum
+    equal those of bte_render_views on that slot alone, bit for bit; the selected slot is restored."""
+    scenes = [(random_scene, 1, 10, [(64, 48, 1), (40, 30, 2)]),
+              (cornell_scene, 0, 8, [(50, 50, 2), (32, 24, 1), (70, 20, 3)])]
+    batch = []
+    try:
+        for slot, (sc, env_mode, depth, sizes) in enumerate(scenes):
+            renderer.select_scene(slot)
+            _upload(renderer, sc, env_mode=env_mode, spp=1, depth=depth)
+            renderer.reset_views()
+            batch.append((slot, _views_of(bte, sc, sizes)))
+        renderer.select_scene(0)
+        for _ in range(2):
+            renderer.render_scene_batch(batch)
+        assert renderer.selected_scene() == 0
+        got = []
+        for slot, views in batch:
+            renderer.select_scene(slot)
+            got.append([renderer.read_view_accum(i, w, h) for i, (_, w, h, _) in enumerate(views)])
+            st = renderer.stats()
+            assert st.samples == sum(w * h * s for _, w, h, s in views)
+        for slot, views in batch:   # the same views, one slot at a time
+            renderer.select_scene(slot)
+            renderer.reset_views()
+            for _ in range(2):
+                renderer.render_views(views)
+            for i, (_, w, h, _) in enumerate(views):
+                m, t = renderer.read_view_accum(i, w, h)
+                assert np.array_equal(bits(m), bits(got[slot][i][0]))
+                assert np.array_equal(t.view(np.uint64), got[slot][i][1].view(np.uint64))
+        assert not np.array_equal(bits(got[0][0][0][:50]), bits(got[1][0][0][:50]))
+        with pytest.raises(RuntimeError, match="appears twice"):
+            renderer.render_scene_batch([(1, batch[1][1]), (1, batch[1][1])])
+        with pytest.raises(RuntimeError, match="out of range"):
+            renderer.select_scene(8)
+    finally:
+        renderer.select_scene(1)
+        renderer.reset_views()
+        renderer.cleanup()
+        renderer.select_scene(0)
+        renderer.reset_views()
