@@ -202,8 +202,9 @@ def multi_scene_leg(scene, args):
     """Several scenes in one batch (bte_render_scene_batch): the bench scene in slot 0 and five seeded instanced
     scenes in slots 1-5 (2, 8, 20, 40 and 80 placements of 25,000-triangle meshes: 50k to 2M triangles, under the
     procedural sky), each with 8 seeded views from {320x240, 640x480, 1280x720, 1920x1080} at 1, 2 or 4 samples
-    per frame (48 views); one batch frame against the same six scenes rendered one bte_render_views call after
-    another.  Host wall clock around each call (each ends with its frames finished), median of 5."""
+    per frame (48 views); one batch frame (one launch of a graph holding each scene's captured view frame) against
+    the same six scenes rendered one bte_render_views call after another (each a captured view frame too).  Host
+    wall clock around each call (each ends with its frames finished), median of 5."""
     import time
     import bluetruthengine_b200 as bte
     from bluetruthengine_b200 import scenes
@@ -221,7 +222,7 @@ def multi_scene_leg(scene, args):
                                                            n_meshes=4, env_w=1024, env_h=512))
                 r.cleanup()
                 r.upload(sc)
-            r.set_config(samples_per_frame=1, max_depth=args.depth, rr_start=3, env_sampling=env)
+            r.set_config(samples_per_frame=1, max_depth=args.depth, rr_start=3, env_sampling=env, use_graph=1)
             r.reset_views()
             base = np.asarray(sc.camera, dtype=bte.CAMERA_DTYPE).copy()
             views = []

@@ -135,6 +135,11 @@ struct Renderer {
     DeviceBuffer viewTable;
     ViewDesc* hViewTable = nullptr;   // pinned staging of the view table: its upload does not block the host
     int pendDepth = 0, pendPaths = 0, pendCount = 0;   // a view frame enqueued and not yet finished
+    // captured view frame (memsets, generate, bounces, tail, present) and its key; viewGen numbers captures
+    cudaGraph_t viewGraph = nullptr;
+    cudaGraphExec_t viewExec = nullptr;
+    std::vector<unsigned char> viewKey;
+    unsigned long long viewGen = 0;
     bool stageTiming = false;
     int lastPaths = 0, lastDepth = 0, lastSpp = 0, lastW = 0, lastH = 0, lastSlots = 0;
     BteFrameStats stats{};
@@ -165,6 +170,18 @@ void selectScene(int k)
     std::swap(g, g_parked[k]);
     g_scene = k;
 }
+
+// A batch of scenes whose view frames are all captured: one parent graph holding each scene's view graph as a
+// child node (no edges between them), launched once on its own stream.
+struct BatchGraph {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned long long> key;   // (slot, capture number) per child
+};
+BatchGraph g_batch;
+unsigned long long g_captures = 0;
 
 void ensureInit()
 {
@@ -263,9 +280,19 @@ void releaseGraph()
     g.graphKey.clear();
 }
 
+void releaseViewGraph()
+{
+    if (g.viewExec) cudaGraphExecDestroy(g.viewExec);
+    if (g.viewGraph) cudaGraphDestroy(g.viewGraph);
+    g.viewExec = nullptr;
+    g.viewGraph = nullptr;
+    g.viewKey.clear();
+}
+
 void releaseWavefront()
 {
     releaseGraph();
+    releaseViewGraph();
     for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch,
                             &g.sortQueue, &g.sortCount, &g.shadowQueue,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
@@ -544,7 +571,7 @@ void renderFrame(int w, int h)
 // views (each view's paths sample-major as in bte_render), each view accumulating into its own buffers.
 // launchViews only enqueues (no host wait once the buffers exist); finishViews waits for the frame and
 // reads its counters, so several scenes' frames can be enqueued on their own streams before any wait.
-void launchViews(const BteView* views, int count)
+void launchViews(const BteView* views, int count, bool deferToBatch = false)
 {
     if (!views || count <= 0) throw CudaError{"bte_render_views: no views"};
     if (count > kMaxViews) throw CudaError{"bte_render_views: at most 64 views per frame"};
@@ -627,19 +654,59 @@ void launchViews(const BteView* views, int count)
     f.viewCount = count;
     const DevScene s = makeDevScene();
     cudaStream_t st = g.stream;
-    ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
-    ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+    auto body = [&] {
+        ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
+        ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+        launchGenerate(P, f, st);
+        launchBounces(s, P, f, depth, block, st);
+        launchTail(s, P, f, st);
+        launchPresentViews(P, f, static_cast<int>(pixels64), st);
+    };
+    const bool useGraph = g.cfg.useGraph != 0;
+    if (useGraph) {
+        // Every baked launch argument keys the capture; the view table's contents (cameras, per-view frame
+        // indices, accumulation pointers) travel through device memory, uploaded before each launch.
+        std::vector<unsigned char> key;
+        auto put = [&](const void* p, size_t n) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            key.insert(key.end(), c, c + n);
+        };
+        const int ints[8] = {depth, block, g.gridExtend, g.gridShade, g.gridConnect, g.shadeMinBlocks,
+                             static_cast<int>(pixels64), g.overlapConnect};
+        put(&P, sizeof(P)); put(&f, sizeof(f)); put(&s, sizeof(s)); put(ints, sizeof(ints));
+        if (!g.viewExec || key != g.viewKey) {
+            releaseViewGraph();
+            ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            try {
+                body();
+                ck(cudaGetLastError(), "kernel launch (capture)");
+            } catch (...) {
+                cudaGraph_t broken = nullptr;
+                cudaStreamEndCapture(st, &broken);
+                if (broken) cudaGraphDestroy(broken);
+                throw;
+            }
+            ck(cudaStreamEndCapture(st, &g.viewGraph), "cudaStreamEndCapture");
+            ck(cudaGraphInstantiate(&g.viewExec, g.viewGraph, 0), "cudaGraphInstantiate");
+            g.viewKey = key;
+            g.viewGen = ++g_captures;
+        }
+    }
+    g.pendDepth = depth; g.pendPaths = paths; g.pendCount = count;
+    if (deferToBatch) {   // the batch graph runs the captured frame; mark the table upload's end
+        ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+        return;
+    }
     ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
-    launchGenerate(P, f, st);
-    launchBounces(s, P, f, depth, block, st);
-    launchTail(s, P, f, st);
-    launchPresentViews(P, f, static_cast<int>(pixels64), st);
+    if (useGraph)
+        ck(cudaGraphLaunch(g.viewExec, st), "cudaGraphLaunch");
+    else
+        body();
     ck(cudaGetLastError(), "kernel launch");
     ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
-    g.pendDepth = depth; g.pendPaths = paths; g.pendCount = count;
 }
 
 void finishViews(const BteView* views)
@@ -677,6 +744,69 @@ void renderViews(const BteView* views, int count)
     finishViews(views);
 }
 
+// The batch as one graph launch: each scene's captured view frame is a child node of one parent graph (rebuilt
+// when a scene re-captures), launched on the batch stream once every scene's view table is uploaded; each scene
+// then reads its counters after the batch.  Every scene's frame time is the batch's.
+void renderSceneBatchGraph(const int* scenes, const int* viewCounts, const BteView* views, int sceneCount,
+                           const std::vector<int>& offset, int home)
+{
+    if (!g_batch.stream) {
+        ck(cudaStreamCreateWithFlags(&g_batch.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaEventCreateWithFlags(&g_batch.done, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    std::vector<unsigned long long> key;
+    std::vector<cudaGraph_t> children;
+    int prepared = 0;
+    try {
+        for (; prepared < sceneCount; ++prepared) {
+            selectScene(scenes[prepared]);
+            ensureInit();
+            launchViews(views + offset[static_cast<size_t>(prepared)], viewCounts[prepared], true);
+            ck(cudaStreamWaitEvent(g_batch.stream, g.ev0, 0), "cudaStreamWaitEvent");
+            key.push_back(static_cast<unsigned long long>(scenes[prepared]));
+            key.push_back(g.viewGen);
+            children.push_back(g.viewGraph);
+        }
+        if (!g_batch.exec || key != g_batch.key) {
+            if (g_batch.exec) cudaGraphExecDestroy(g_batch.exec);
+            if (g_batch.graph) cudaGraphDestroy(g_batch.graph);
+            g_batch.exec = nullptr;
+            g_batch.graph = nullptr;
+            g_batch.key.clear();
+            ck(cudaGraphCreate(&g_batch.graph, 0), "cudaGraphCreate");
+            for (cudaGraph_t child : children) {
+                cudaGraphNode_t node;
+                ck(cudaGraphAddChildGraphNode(&node, g_batch.graph, nullptr, 0, child), "cudaGraphAddChildGraphNode");
+            }
+            ck(cudaGraphInstantiate(&g_batch.exec, g_batch.graph, 0), "cudaGraphInstantiate");
+            g_batch.key = key;
+        }
+        ck(cudaGraphLaunch(g_batch.exec, g_batch.stream), "cudaGraphLaunch");
+        ck(cudaEventRecord(g_batch.done, g_batch.stream), "cudaEventRecord");
+    } catch (const CudaError&) {
+        for (int i = 0; i < prepared; ++i) {   // nothing of the batch ran: drop the pending frames
+            selectScene(scenes[i]);
+            g.pendCount = 0;
+            cudaStreamSynchronize(g.stream);
+        }
+        selectScene(home);
+        throw;
+    }
+    std::string firstError;
+    for (int i = 0; i < sceneCount; ++i) {
+        selectScene(scenes[i]);
+        try {
+            ck(cudaStreamWaitEvent(g.stream, g_batch.done, 0), "cudaStreamWaitEvent");
+            ck(cudaEventRecord(g.ev1, g.stream), "cudaEventRecord");
+            finishViews(views + offset[static_cast<size_t>(i)]);
+        } catch (const CudaError& e) {
+            if (firstError.empty()) firstError = e.msg;
+        }
+    }
+    selectScene(home);
+    if (!firstError.empty()) throw CudaError{firstError};
+}
+
 // One batch over several scene slots: every scene's view frame is enqueued on its own streams first, then
 // each is finished in turn, so the scenes' launch sequences run side by side on the GPU.  Each scene's
 // views accumulate exactly as bte_render_views would leave them; the selected slot is restored.
@@ -695,6 +825,15 @@ void renderSceneBatch(const int* scenes, const int* viewCounts, const BteView* v
         offset[static_cast<size_t>(i) + 1] = offset[static_cast<size_t>(i)] + viewCounts[i];
     }
     const int home = g_scene;
+    bool allGraph = true;
+    for (int i = 0; i < sceneCount; ++i) {
+        selectScene(scenes[i]);
+        allGraph = allGraph && g.cfg.useGraph != 0;
+    }
+    if (allGraph) {
+        renderSceneBatchGraph(scenes, viewCounts, views, sceneCount, offset, home);
+        return;
+    }
     std::string firstError;
     int launched = 0;
     for (; launched < sceneCount && firstError.empty(); ++launched) {

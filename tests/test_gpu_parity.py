@@ -586,10 +586,13 @@ def _views_of(bte, scene, sizes):
     return views
 
 
-def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene):
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene, use_graph):
     """Two scene slots (the random scene with its env map, the Cornell box), each with views of uneven size and
-    samples per frame, rendered side by side in one batch for two frames: every view's FP32 mean and FP64 sum
-    equal those of bte_render_views on that slot alone, bit for bit; the selected slot is restored."""
+    samples per frame, rendered side by side in one batch for two frames (separate streams, or one launch of a
+    graph holding each scene's captured view frame): every view's FP32 mean and FP64 sum equal those of eager
+    bte_render_views on that slot alone, bit for bit, and so do captured single-slot view frames; the selected
+    slot is restored."""
     scenes = [(random_scene, 1, 10, [(64, 48, 1), (40, 30, 2)]),
               (cornell_scene, 0, 8, [(50, 50, 2), (32, 24, 1), (70, 20, 3)])]
     batch = []
@@ -597,6 +600,8 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
         for slot, (sc, env_mode, depth, sizes) in enumerate(scenes):
             renderer.select_scene(slot)
             _upload(renderer, sc, env_mode=env_mode, spp=1, depth=depth)
+            renderer.set_config(samples_per_frame=1, max_depth=depth, rr_start=3, env_sampling=env_mode,
+                                use_graph=use_graph)
             renderer.reset_views()
             batch.append((slot, _views_of(bte, sc, sizes)))
         renderer.select_scene(0)
@@ -609,15 +614,18 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
             got.append([renderer.read_view_accum(i, w, h) for i, (_, w, h, _) in enumerate(views)])
             st = renderer.stats()
             assert st.samples == sum(w * h * s for _, w, h, s in views)
-        for slot, views in batch:   # the same views, one slot at a time
+        for (slot, views), (_, env_mode, depth, _) in zip(batch, scenes):   # the same views, one slot at a time
             renderer.select_scene(slot)
-            renderer.reset_views()
-            for _ in range(2):
-                renderer.render_views(views)
-            for i, (_, w, h, _) in enumerate(views):
-                m, t = renderer.read_view_accum(i, w, h)
-                assert np.array_equal(bits(m), bits(got[slot][i][0]))
-                assert np.array_equal(t.view(np.uint64), got[slot][i][1].view(np.uint64))
+            for graph in sorted({0, use_graph}):
+                renderer.set_config(samples_per_frame=1, max_depth=depth, rr_start=3, env_sampling=env_mode,
+                                    use_graph=graph)
+                renderer.reset_views()
+                for _ in range(2):
+                    renderer.render_views(views)
+                for i, (_, w, h, _) in enumerate(views):
+                    m, t = renderer.read_view_accum(i, w, h)
+                    assert np.array_equal(bits(m), bits(got[slot][i][0]))
+                    assert np.array_equal(t.view(np.uint64), got[slot][i][1].view(np.uint64))
         assert not np.array_equal(bits(got[0][0][0][:50]), bits(got[1][0][0][:50]))
         with pytest.raises(RuntimeError, match="appears twice"):
             renderer.render_scene_batch([(1, batch[1][1]), (1, batch[1][1])])
