@@ -7,6 +7,8 @@ Sweeps the knobs that decide throughput on a given scene and GPU:
   * residency the shade kernel is compiled for (2 or 3 blocks per SM),
   * the leaf-test postponing threshold of the 8-wide walk,
   * material-sorted shading on or off,
+  * the compaction threshold: bounce queues shorter than it finish in the
+    tail kernel (one thread per remaining path) instead of the stage kernels,
 timing whole frames on the device (CUDA events), and leaves the renderer in
 the fastest configuration.  Results are deterministic in value (every
 configuration renders the same bits); only speed differs.
@@ -26,20 +28,23 @@ class TuneResult:
     shade_min_blocks: int
     postpone_percent: int
     sort_shading: int
+    tail_paths: int
     ms_per_frame: float
     msamples_per_s: float
 
 
 def autotune(renderer, width: int, height: int, samples_per_frame: int, max_depth: int, env_sampling: int,
-             trees=((8, 1), (8, 2), (8, 3), (2, 1)), blocks=(128, 256), shade_min_blocks=(2, 3),
-             postpone=(0, 20), sort_shading=(1,), frames: int = 3, verbose: bool = False):
+             trees=((8, 1), (8, 2), (8, 3), (2, 1)), blocks=(64, 128, 256), shade_min_blocks=(2, 3),
+             postpone=(0, 20), sort_shading=(1,), tail_paths=(0, 1 << 14), frames: int = 3, verbose: bool = False):
+    """Blocks run 64 to 256 threads: the stage kernels are compiled for at most 256 threads per block, which
+    fixes their register budgets."""
     results = []
     for bvh_width, leaf in trees:
         renderer.set_tuning(leaf, 2, bvh_width)
         renderer.init_accel()
-        for blk, smb, pp, srt in itertools.product(blocks, shade_min_blocks, postpone if bvh_width == 8 else (0,),
-                                                   sort_shading):
-            renderer.set_tuning(leaf, smb, bvh_width, pp, srt)
+        for blk, smb, pp, srt, tail in itertools.product(blocks, shade_min_blocks,
+                                                         postpone if bvh_width == 8 else (0,), sort_shading, tail_paths):
+            renderer.set_tuning(leaf, smb, bvh_width, pp, srt, tail)
             renderer.set_config(samples_per_frame=samples_per_frame, max_depth=max_depth, rr_start=3,
                                 env_sampling=env_sampling, block_size=blk)
             renderer.render(width, height)          # warm-up at this configuration
@@ -48,12 +53,13 @@ def autotune(renderer, width: int, height: int, samples_per_frame: int, max_dept
                 renderer.render(width, height)
                 ms += renderer.stats().msTotal
             ms /= frames
-            r = TuneResult(bvh_width, leaf, blk, smb, pp, srt, ms, width * height * samples_per_frame / ms / 1e3)
+            r = TuneResult(bvh_width, leaf, blk, smb, pp, srt, tail, ms, width * height * samples_per_frame / ms / 1e3)
             results.append(r)
             if verbose:
                 print(json.dumps(asdict(r)), flush=True)
     best = min(results, key=lambda r: r.ms_per_frame)
-    renderer.set_tuning(best.max_leaf, best.shade_min_blocks, best.bvh_width, best.postpone_percent, best.sort_shading)
+    renderer.set_tuning(best.max_leaf, best.shade_min_blocks, best.bvh_width, best.postpone_percent, best.sort_shading,
+                        best.tail_paths)
     renderer.init_accel()
     renderer.set_config(samples_per_frame=samples_per_frame, max_depth=max_depth, rr_start=3,
                         env_sampling=env_sampling, block_size=best.block_size)

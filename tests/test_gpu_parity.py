@@ -637,3 +637,25 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
         renderer.cleanup()
         renderer.select_scene(0)
         renderer.reset_views()
+
+
+def test_autotune_picks_fastest_and_keeps_bits(renderer, random_scene):
+    """The autotuner over tree width, block size (64-256) and the compaction threshold (tail kernel below it) keeps
+    the fastest configuration it timed, leaves the renderer in it, and every configuration renders the same bits
+    as a fixed one."""
+    from bluetruthengine_b200.autotune import autotune
+    sc = random_scene
+    W, H = 64, 48
+    _upload(renderer, sc, env_mode=1, spp=1, depth=8)
+    renderer.init_camera(sc.camera)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    fixed = renderer.read_accum(W, H).copy()
+    best, results = autotune(renderer, W, H, 1, 8, 1, trees=((8, 1), (2, 1)), blocks=(64, 256),
+                             shade_min_blocks=(3,), postpone=(0,), tail_paths=(0, 1 << 12), frames=1)
+    assert len(results) == 2 * 2 * 2
+    assert best.ms_per_frame == min(r.ms_per_frame for r in results)
+    t = renderer.tuning()
+    assert (t["bvhWidth"], t["maxLeafTriangles"], t["tailPaths"]) == (best.bvh_width, best.max_leaf, best.tail_paths)
+    renderer.render(W, H)
+    assert np.array_equal(bits(renderer.read_accum(W, H)), bits(fixed))
