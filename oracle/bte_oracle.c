@@ -1701,11 +1701,12 @@ static void o_fillHit(const OScene* s, OF3 o, OF3 d, int tri, float t, float u, 
 /* megakernel's per-path order (src/optix_programs.cu:54-108).         */
 /* ------------------------------------------------------------------ */
 static OF3 o_renderSample(const OScene* s, const OCamera* cam, const OConfig* cfg, uint32_t pixel, uint32_t sampleIndex,
-                          int* hitLog, OStats* st, float* rayLog)
+                          int* hitLog, OStats* st, float* rayLog, uint32_t* rngIO)
 {
     const int px = (int)(pixel % (uint32_t)cfg->width);
     const int py = (int)(pixel / (uint32_t)cfg->width);
-    uint32_t rng = rngMake(or_hash_uint(pixel ^ (sampleIndex * 0x9e3779b9u)));
+    /* rngIO: a stream carried from the previous path of the pixel (megakernel), updated on return */
+    uint32_t rng = rngIO ? *rngIO : rngMake(or_hash_uint(pixel ^ (sampleIndex * 0x9e3779b9u)));
     const float jx = rngNextFloat01(&rng) - 0.5f;
     const float jy = rngNextFloat01(&rng) - 0.5f;
     OPath p;
@@ -1759,6 +1760,7 @@ static OF3 o_renderSample(const OScene* s, const OCamera* cam, const OConfig* cf
         if (!o_roulette(&p, &rng, cfg->rrStart)) break;
         p.bounce++;
     }
+    if (rngIO) *rngIO = rng;
     return p.L;
 }
 
@@ -1774,7 +1776,7 @@ void or_render_samples(const OScene* s, const OCamera* cam, const OConfig* cfg, 
     for (int i = 0; i < n; ++i) {
         OStats local = {0, 0};
         OF3 L = o_renderSample(s, cam, cfg, pixels[i], sampleIndices[i], hitLog ? hitLog + (size_t)i * cfg->maxDepth : NULL,
-                               &local, NULL);
+                               &local, NULL, NULL);
         outRadiance[3 * i] = L.x; outRadiance[3 * i + 1] = L.y; outRadiance[3 * i + 2] = L.z;
         ext += local.extends; sh += local.shadowRays;
     }
@@ -1787,7 +1789,34 @@ void or_path_rays(const OScene* s, const OCamera* cam, const OConfig* cfg, uint3
                   float* rays, int* hits)
 {
     for (int i = 0; i < 6 * cfg->maxDepth; ++i) rays[i] = NAN;
-    (void)o_renderSample(s, cam, cfg, pixel, sampleIndex, hits, NULL, rays);
+    (void)o_renderSample(s, cam, cfg, pixel, sampleIndex, hits, NULL, rays, NULL);
+}
+
+/* one megakernel frame, src/optix_programs.cu:54-108: per pixel one stream,
+   makeRng(hashUint(pixel ^ frameIndex * 0x9e3779b9)), carried through spp
+   paths in turn (each draws its jitter first); the paths' radiance summed in
+   sample order from zero and scaled by 1/spp (div3, rt_cuda_math.cuh:28-33).
+   Writes the frame's mean per pixel [n*3], the input of the Welford update. */
+void or_render_megakernel(const OScene* s, const OCamera* cam, const OConfig* cfg, const uint32_t* pixels, int n,
+                          uint32_t frameIndex, int spp, float* outMean, OStats* stats, int threads)
+{
+    int64_t ext = 0, sh = 0;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads) reduction(+ : ext, sh)
+#endif
+    for (int i = 0; i < n; ++i) {
+        OStats local = {0, 0};
+        uint32_t rng = rngMake(or_hash_uint(pixels[i] ^ (frameIndex * 0x9e3779b9u)));
+        OF3 sum = f3(0.f, 0.f, 0.f);
+        for (int k = 0; k < spp; ++k)
+            sum = add3(sum, o_renderSample(s, cam, cfg, pixels[i], 0u, NULL, &local, NULL, &rng));
+        const float inv = spp != 0 ? 1.0f / (float)spp : 0.0f;
+        outMean[3 * i] = sum.x * inv; outMean[3 * i + 1] = sum.y * inv; outMean[3 * i + 2] = sum.z * inv;
+        ext += local.extends; sh += local.shadowRays;
+    }
+    (void)threads;
+    if (stats) { stats->extends += ext; stats->shadowRays += sh; }
 }
 
 /* ------------------------------------------------------------------ */

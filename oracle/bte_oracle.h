@@ -123,6 +123,10 @@ void or_trace_occluded(const OScene* s, const float* rays, const float* tmax, in
 void or_render_samples(const OScene* s, const OCamera* cam, const OConfig* cfg,
                        const uint32_t* pixels, const uint32_t* sampleIndices, int n,
                        float* outRadiance, int* hitLog, OStats* stats, int threads);
+/* one megakernel frame (src/optix_programs.cu:54-108): per pixel one RNG stream through spp paths; the frame's
+ * mean radiance per pixel [n*3] */
+void or_render_megakernel(const OScene* s, const OCamera* cam, const OConfig* cfg, const uint32_t* pixels, int n,
+                          uint32_t frameIndex, int spp, float* outMean, OStats* stats, int threads);
 
 void or_path_rays(const OScene* s, const OCamera* cam, const OConfig* cfg, uint32_t pixel, uint32_t sampleIndex,
                   float* rays, int* hits);

@@ -289,6 +289,21 @@ def render_samples(lib_or, view: SceneView, cam, width, height, max_depth, pixel
     return out, hl, (int(st.extends), int(st.shadowRays))
 
 
+def render_megakernel(lib_or, view: SceneView, cam, width, height, max_depth, pixels, frame_index, spp=5, rr_start=3,
+                      threads=0, prefix="or_"):
+    """One megakernel frame (src/optix_programs.cu:54-108): per pixel one RNG stream through spp paths; the
+    frame's mean radiance [n,3] and stats."""
+    pixels = np.ascontiguousarray(pixels, dtype=np.uint32)
+    n = len(pixels)
+    out = np.empty((n, 3), dtype=np.float32)
+    st = OStats()
+    cfg = OConfig(width, height, max_depth, rr_start)
+    camc = camera_struct(cam)
+    getattr(lib_or, prefix + "render_megakernel")(view.ptr(), C.byref(camc), C.byref(cfg), _p(pixels), n,
+                                                  C.c_uint32(int(frame_index)), int(spp), _p(out), C.byref(st), threads)
+    return out, (int(st.extends), int(st.shadowRays))
+
+
 class Ref:
     """The reference's own shading headers compiled on the host (oracle/_ref)."""
 

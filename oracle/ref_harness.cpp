@@ -181,12 +181,13 @@ bool occludedRef(const OScene* s, const ShadowRayRecord& sr)
 }
 
 Float3 renderOne(const OScene* s, const WfSceneView& sv, const CameraData& cam, int W, int H, int maxDepth,
-                 uint32_t pixel, uint32_t sampleIndex, int* hitLog, OStats* st)
+                 uint32_t pixel, uint32_t sampleIndex, int* hitLog, OStats* st, RngState* rngIO = nullptr)
 {
     // ray_generate.cu:49-73 (pixel index == path slot; frameIndex == sample index)
     const int px = static_cast<int>(pixel % static_cast<uint32_t>(W));
     const int py = static_cast<int>(pixel / static_cast<uint32_t>(W));
-    RngState rng = makeRng(hashUint(pixel ^ (sampleIndex * 0x9e3779b9u)));
+    // rngIO: the megakernel's per-pixel stream carried from the previous path (optix_programs.cu:64-72)
+    RngState rng = rngIO ? *rngIO : makeRng(hashUint(pixel ^ (sampleIndex * 0x9e3779b9u)));
     const float jx = rngNextFloat01(rng) - 0.5f;
     const float jy = rngNextFloat01(rng) - 0.5f;
     PathState ps;
@@ -242,6 +243,7 @@ Float3 renderOne(const OScene* s, const WfSceneView& sv, const CameraData& cam, 
         if (!russianRoulette(ps, rng)) break;
         ps.bounceCount++;
     }
+    if (rngIO) *rngIO = rng;
     return ps.accumulatedColor;
 }
 }  // namespace
@@ -343,6 +345,33 @@ REF_API void ref_render_samples(const OScene* s, const OCamera* cam, const OConf
         const Float3 L = renderOne(s, rs.sv, c, cfg->width, cfg->height, cfg->maxDepth, pixels[i], sampleIndices[i],
                                    hitLog ? hitLog + static_cast<size_t>(i) * cfg->maxDepth : nullptr, &local);
         outRadiance[3 * i] = L.x; outRadiance[3 * i + 1] = L.y; outRadiance[3 * i + 2] = L.z;
+        ext += local.extends; sh += local.shadowRays;
+    }
+    (void)threads;
+    if (stats) { stats->extends += ext; stats->shadowRays += sh; }
+}
+
+// one megakernel frame, optix_programs.cu:54-99: per pixel one stream through spp paths, summed with add3 and
+// scaled with div3 (the reference's own helpers)
+REF_API void ref_render_megakernel(const OScene* s, const OCamera* cam, const OConfig* cfg, const uint32_t* pixels,
+                                   int n, uint32_t frameIndex, int spp, float* outMean, OStats* stats, int threads)
+{
+    RefScene rs; buildRefScene(s, rs);
+    const CameraData& c = *reinterpret_cast<const CameraData*>(cam);
+    int64_t ext = 0, sh = 0;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads) reduction(+ : ext, sh)
+#endif
+    for (int i = 0; i < n; ++i) {
+        OStats local{0, 0};
+        RngState rng = makeRng(hashUint(pixels[i] ^ (frameIndex * 0x9e3779b9u)));
+        Float3 sum = {0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < spp; ++k)
+            sum = add3(sum, renderOne(s, rs.sv, c, cfg->width, cfg->height, cfg->maxDepth, pixels[i], 0u, nullptr,
+                                      &local, &rng));
+        const Float3 m = div3(sum, static_cast<float>(spp));
+        outMean[3 * i] = m.x; outMean[3 * i + 1] = m.y; outMean[3 * i + 2] = m.z;
         ext += local.extends; sh += local.shadowRays;
     }
     (void)threads;

@@ -94,6 +94,24 @@ def test_oracle_matches_reference_full_frame(oracle_mod, cornell_scene):
     assert sa == sb and np.array_equal(ha, hb) and np.array_equal(bits(a), bits(b))
 
 
+def test_oracle_megakernel_matches_reference(oracle_mod, cornell_scene):
+    """Megakernel frames (one RNG stream per pixel through 5 paths, the mean of the five): oracle (glibc math) ==
+    the reference's headers, bit-for-bit, for frames 0 and 1 of the Cornell box."""
+    if not oracle_mod.Ref.available():
+        pytest.skip("reference harness not built")
+    ref = oracle_mod.Ref()
+    orc = oracle_mod.Oracle(libm=True)
+    sc = cornell_scene
+    W, H = sc.width, sc.height
+    view = oracle_mod.SceneView(sc, env_mode=0, oracle=orc, build_accel=False)
+    pix = np.arange(0, W * H, 7, dtype=np.uint32)
+    for frame in (0, 1):
+        a, sa = oracle_mod.render_megakernel(orc.lib, view, sc.camera, W, H, 8, pix, frame)
+        b, sb = oracle_mod.render_megakernel(ref.lib, view, sc.camera, W, H, 8, pix, frame, prefix="ref_")
+        assert sa == sb and np.array_equal(bits(a), bits(b))
+        assert a.mean() > 0
+
+
 def test_bvh_traversal_equals_brute_force(oracle_mod, random_scene):
     """The oracle's CPU BVH resolves every closest hit exactly as the exhaustive search does."""
     orc = oracle_mod.Oracle(libm=False)
