@@ -457,6 +457,76 @@ __global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams
     }
 }
 
+// RenderMode::Megakernel, src/optix_programs.cu:54-108: one thread per pixel and one RNG stream per pixel and
+// frame, rngSeed(pixel, frameIndex) = makeRng(hashUint(pixel ^ frameIndex * 0x9e3779b9)), carried through f.spp
+// paths in turn, each drawing its jitter first.  Each path runs the tail kernel's bounce loop on the pixel's own
+// path slot (the stream returns through P.o.w); the paths' radiance is summed in sample order from zero, scaled
+// by div3, folded into the FP32 Welford mean once per frame (n = frames so far + 1) and into the FP64 sum, then
+// packed.
+template <int Width>
+__global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, FrameParams f, float* accum,
+                                                   double* accumD, uint32_t* framebuffer, uint32_t* extFramebuffer)
+{
+    const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int wh = f.width * f.height;
+    if (pix >= wh || pix >= P.count) return;
+    const uint32_t frameIndex = *f.frameIndex;
+    const int px = pix % f.width, py = pix / f.width;
+    uint32_t rng = rngSeed(static_cast<uint32_t>(pix), frameIndex);
+    V3 sum = v3(0.0f, 0.0f, 0.0f);
+    for (int k = 0; k < f.spp; ++k) {
+        const float jx = rngNext(rng) - 0.5f;
+        const float jy = rngNext(rng) - 0.5f;
+        V3 o, d;
+        primaryRay(px, py, f.width, f.height, f.cam, f.tanHalf, jx, jy, o, d);
+        P.o[pix] = make_float4(o.x, o.y, o.z, __uint_as_float(rng));
+        P.d[pix] = make_float4(d.x, d.y, d.z, 1.0f);
+        P.tp[pix] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        P.L[pix] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(1u << 16));
+        P.shMask[pix] = 0u;
+        for (int b = 0; b < P.maxDepth; ++b) {
+            atomicAdd(P.rayCount + b, 1);
+            const float4 ro = P.o[pix];
+            const float4 rd = P.d[pix];
+            const RayPre r = rayPre(ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, s.sceneMaxAbs);
+            float t = 0.0f, u = 0.0f, v = 0.0f;
+            const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
+            P.hit[pix] = make_float4(t, u, v, __int_as_float(tri));
+            const bool alive = shadePath(s, P, f, b, pix, false);
+            uint32_t mask = P.shMask[pix];
+            if (mask) {
+                atomicAdd(P.shadowCount + b, __popc(mask));
+                const float4 so = P.shOrigin[pix];
+                const size_t base = static_cast<size_t>(pix) * P.slots;
+                for (uint32_t m = mask; m; m &= m - 1u) {
+                    const int sl = __ffs(m) - 1;
+                    const float4 sd = P.shDir[base + sl];
+                    const RayPre sr = rayPre(so.x, so.y, so.z, sd.x, sd.y, sd.z, s.sceneMaxAbs);
+                    if (traceOccludedW<Width>(s, sr, kEps, sd.w, P.errorFlags)) mask &= ~(1u << sl);
+                }
+                P.shMask[pix] = mask;
+            }
+            if (!alive || b + 1 >= P.maxDepth) break;
+        }
+        const float4 L4 = P.L[pix];
+        sum = add3(sum, resolveShadows(P, pix, v3(L4.x, L4.y, L4.z)));
+        rng = __float_as_uint(P.o[pix].w);
+    }
+    const V3 c = div3(sum, static_cast<float>(f.spp));
+    const float n = static_cast<float>(frameIndex + 1u);
+    float ax = accum[3 * pix], ay = accum[3 * pix + 1], az = accum[3 * pix + 2];
+    ax = ax + (c.x - ax) / n;
+    ay = ay + (c.y - ay) / n;
+    az = az + (c.z - az) / n;
+    accum[3 * pix] = ax; accum[3 * pix + 1] = ay; accum[3 * pix + 2] = az;
+    accumD[3 * pix] += static_cast<double>(c.x);
+    accumD[3 * pix + 1] += static_cast<double>(c.y);
+    accumD[3 * pix + 2] += static_cast<double>(c.z);
+    const uint32_t px32 = packGamma(ax, ay, az);
+    framebuffer[pix] = px32;
+    if (extFramebuffer) extFramebuffer[pix] = px32;
+}
+
 // ---------------------------------------------------------------- present
 // src/wavefront/ray_present.cu:43-62 for spp consecutive samples per pixel:
 // FP32 Welford mean (rt_path_integrator.cuh:72-87) in sample order, an FP64
@@ -708,6 +778,13 @@ void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cuda
     const int blocks = (n + 127) / 128;
     if (s.bvhWidth == 8) kTail<8><<<blocks, 128, 0, st>>>(s, P, f);
     else kTail<2><<<blocks, 128, 0, st>>>(s, P, f);
+}
+void launchMegakernel(const DevScene& s, const DevPaths& P, const FrameParams& f, float* accum, double* accumD,
+                      uint32_t* fb, uint32_t* extFb, cudaStream_t st)
+{
+    const int wh = f.width * f.height;
+    if (s.bvhWidth == 8) kMegakernel<8><<<(wh + 127) / 128, 128, 0, st>>>(s, P, f, accum, accumD, fb, extFb);
+    else kMegakernel<2><<<(wh + 127) / 128, 128, 0, st>>>(s, P, f, accum, accumD, fb, extFb);
 }
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    float* aovAccum, cudaStream_t st)

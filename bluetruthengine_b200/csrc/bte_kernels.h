@@ -14,6 +14,8 @@ void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int
                  int minBlocks, cudaStream_t st);
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
 void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cudaStream_t st);
+void launchMegakernel(const DevScene& s, const DevPaths& P, const FrameParams& f, float* accum, double* accumD,
+                      uint32_t* fb, uint32_t* extFb, cudaStream_t st);
 void launchPresentViews(const DevPaths& P, const FrameParams& f, int totalPixels, cudaStream_t st);
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    float* aovAccum, cudaStream_t st);

@@ -161,6 +161,7 @@ Renderer g_parked[kMaxScenes];
 int g_scene = 0;
 std::mutex g_mutex;
 constexpr int kMaxViews = 64;
+constexpr int kMegakernelSpp = 5;   // SAMPLES_PER_PIXEL, include/rt_constants.cuh:11
 
 void selectScene(int k)
 {
@@ -395,9 +396,11 @@ void renderFrame(int w, int h)
     if (!g.bsdfs.p || !g.triBsdfIds.p) throw CudaError{"bte_render: no BSDFs uploaded (bte_init_bsdfs)"};
     if (!g.emitterFlags.p) throw CudaError{"bte_render: emitter flags missing (bte_init_triangle_emitter_flags)"};
     if (!g.accum.p || g.accumW != w || g.accumH != h) ensureAccum(w, h);   // render_kernel.cu:62-64
-    const int spp = g.cfg.samplesPerFrame > 0 ? g.cfg.samplesPerFrame : 1;
+    // megakernel mode: SAMPLES_PER_PIXEL (rt_constants.cuh:11) paths per pixel on one stream, one path slot a pixel
+    const bool mega = g.renderMode == BTE_RENDER_MEGAKERNEL;
+    const int spp = mega ? kMegakernelSpp : (g.cfg.samplesPerFrame > 0 ? g.cfg.samplesPerFrame : 1);
     const int depth = g.cfg.maxDepth > 0 ? g.cfg.maxDepth : 1;
-    const long long paths64 = static_cast<long long>(w) * h * spp;
+    const long long paths64 = static_cast<long long>(w) * h * (mega ? 1 : spp);
     if (paths64 > (1LL << 30)) throw CudaError{"bte_render: too many paths per frame (W*H*spp > 2^30)"};
     const int paths = static_cast<int>(paths64);
     const int slots = slotsFor();
@@ -424,19 +427,16 @@ void renderFrame(int w, int h)
     P.shDir = g.shDir.as<float4>();
     P.shContrib = g.shContrib.as<float4>();
     P.shMask = g.shMask.as<uint32_t>();
-    P.hitLog = g.hitLogEnabled ? g.hitLog.as<int>() : nullptr;
-    P.aovAlbedo = g.aovEnabled ? g.aovAlbedo.as<float4>() : nullptr;
-    P.aovNormal = g.aovEnabled ? g.aovNormal.as<float4>() : nullptr;
+    P.hitLog = g.hitLogEnabled && !mega ? g.hitLog.as<int>() : nullptr;
+    P.aovAlbedo = g.aovEnabled && !mega ? g.aovAlbedo.as<float4>() : nullptr;
+    P.aovNormal = g.aovEnabled && !mega ? g.aovNormal.as<float4>() : nullptr;
     P.slots = slots;
     P.maxDepth = depth;
     P.count = paths;
     P.errorFlags = g.errorFlags.as<unsigned int>();
     P.sortQueue = g.sortShading ? g.sortQueue.as<int>() : nullptr;
     P.sortCount = g.sortCount.as<int>();
-    // Megakernel mode (optix_programs.cu:54-108, RenderMode::Megakernel): one thread runs each path from
-    // generation to termination in a single kernel (the tail kernel from bounce 0), with the same per-path
-    // sample streams, so its images equal the wavefront's bit for bit -- a cross-check of the stage kernels.
-    P.tailPaths = g.renderMode == BTE_RENDER_MEGAKERNEL ? 0x7fffffff : g.tailPaths;
+    P.tailPaths = mega ? 0 : g.tailPaths;
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
     f.width = w; f.height = h; f.spp = spp;
@@ -461,13 +461,17 @@ void renderFrame(int w, int h)
         ck(cudaMemcpyAsync(g.dFrameIndex.p, g.hFrameIndex, sizeof(uint32_t), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
     };
     auto frameLaunches = [&] {
+        if (mega) {
+            launchMegakernel(s, P, f, accumF, accumDv, fb, g.extFramebuffer, st);
+            return;
+        }
         launchGenerate(P, f, st);
         launchBounces(s, P, f, depth, block, st);
         launchTail(s, P, f, st);
         launchPresent(P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st);
     };
     float stage[6] = {0, 0, 0, 0, 0, 0};
-    if (g.cfg.useGraph && !g.stageTiming) {
+    if (g.cfg.useGraph && (!g.stageTiming || mega)) {
         // One graph per launch configuration: every kernel argument is part of the key, so a change of
         // scene, buffers, image size, depth or tuning re-captures; the frame index travels through memory.
         std::vector<unsigned char> key;
@@ -498,7 +502,7 @@ void renderFrame(int w, int h)
         }
         ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
         ck(cudaGraphLaunch(g.graphExec, st), "cudaGraphLaunch");
-    } else if (!g.stageTiming) {
+    } else if (!g.stageTiming || mega) {
         ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
         prologue();
         frameLaunches();
@@ -534,7 +538,7 @@ void renderFrame(int w, int h)
     ck(cudaStreamSynchronize(st), "frame");
     BteFrameStats& S = g.stats;
     S = BteFrameStats{};
-    S.samples = paths;
+    S.samples = mega ? paths64 * spp : paths;
     for (int b = 0; b < depth; ++b) {
         S.extends += rc[static_cast<size_t>(b)];
         S.shadowRays += sc[static_cast<size_t>(b)];
@@ -561,8 +565,8 @@ void renderFrame(int w, int h)
         ck(cudaGetLastError(), "pack launch");
         ck(cudaStreamSynchronize(st), "denoise present");
     }
-    g.frameIndex += static_cast<uint32_t>(spp);
-    g.lastPaths = paths; g.lastDepth = depth; g.lastSpp = spp; g.lastW = w; g.lastH = h; g.lastSlots = slots;
+    g.frameIndex += mega ? 1u : static_cast<uint32_t>(spp);   // the megakernel counts frames
+    g.lastPaths = mega ? 0 : paths; g.lastDepth = depth; g.lastSpp = spp; g.lastW = w; g.lastH = h; g.lastSlots = slots;
     if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
     if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
 }

@@ -525,25 +525,52 @@ def test_aov_features(renderer, random_scene):
     assert (hits >= 0).mean() > 0.3
 
 
-def test_megakernel_mode_matches_wavefront(renderer, random_scene):
-    """RenderMode::Megakernel runs each path start to end in one kernel; per-sample radiance, hit counts and
-    the accumulation equal the wavefront's bit for bit."""
+def test_tail_from_bounce_zero_matches_wavefront(renderer, random_scene):
+    """Every path run start to end by the tail kernel (compaction threshold above the path count) gives the
+    wavefront's per-sample radiance and accumulation bit for bit, with the same ray counts: a cross-check of
+    the stage kernels."""
     sc = random_scene
     W, H = sc.width, sc.height
     out = {}
-    for mode in (1, 0):   # BTE_RENDER_WAVEFRONT, BTE_RENDER_MEGAKERNEL
-        _upload(renderer, sc, env_mode=1, spp=2, depth=12)
-        renderer.set_render_mode(mode)
+    for key, tail in ((0, 2**31 - 1), (1, 0)):
+        _upload(renderer, sc, env_mode=1, spp=2, depth=12, tail_paths=tail)
         renderer.reset_accumulation(W, H)
         renderer.render(W, H)
         st = renderer.stats()
-        out[mode] = (renderer.read_sample_radiance(W * H * 2).copy(), renderer.read_accum(W, H).copy(), st.extends,
-                     st.shadowRays, st.tailBounce)
-    renderer.set_render_mode(1)
+        out[key] = (renderer.read_sample_radiance(W * H * 2).copy(), renderer.read_accum(W, H).copy(), st.extends,
+                    st.shadowRays, st.tailBounce)
     assert out[0][4] == 0 and out[1][4] == -1
     assert np.array_equal(bits(out[0][0]), bits(out[1][0]))
     assert np.array_equal(bits(out[0][1]), bits(out[1][1]))
     assert out[0][2:4] == out[1][2:4]
+
+
+def test_megakernel_mode_matches_oracle(renderer, oracle_mod, random_scene):
+    """RenderMode::Megakernel (one thread and one RNG stream per pixel through 5 paths, the frame mean folded into
+    the Welford accumulation once per frame): two frames equal the oracle's megakernel frames bit for bit, with the
+    same extend and shadow-ray counts."""
+    sc = random_scene
+    W, H = sc.width, sc.height
+    _upload(renderer, sc, env_mode=1, spp=1, depth=10)
+    renderer.set_render_mode(0)
+    try:
+        renderer.reset_accumulation(W, H)
+        orc = oracle_mod.Oracle(libm=False)
+        view = oracle_mod.SceneView(sc, env_mode=1, oracle=orc)
+        pix = np.arange(W * H, dtype=np.uint32)
+        accum = np.zeros((W * H, 3), dtype=np.float32)
+        for fr in range(2):
+            renderer.render(W, H)
+            st = renderer.stats()
+            mean, (ext, shr) = oracle_mod.render_megakernel(orc.lib, view, sc.camera, W, H, 10, pix, fr)
+            accum = accum + (mean - accum) / np.float32(fr + 1)
+            assert st.samples == W * H * 5
+            assert (st.extends, st.shadowRays) == (ext, shr)
+            got = renderer.read_accum(W, H).reshape(-1, 3)
+            assert np.array_equal(bits(got), bits(accum)), f"frame {fr}: {np.sum(bits(got) != bits(accum))} mismatches"
+        assert renderer.frame_index() == 2
+    finally:
+        renderer.set_render_mode(1)
 
 
 def test_batched_views_match_single_view_frames(renderer, bte, random_scene):
