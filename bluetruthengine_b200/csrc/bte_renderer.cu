@@ -649,6 +649,8 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
     P.errorFlags = g.errorFlags.as<unsigned int>();
     P.sortQueue = g.sortShading ? g.sortQueue.as<int>() : nullptr;
     P.sortCount = g.sortCount.as<int>();
+    // Batched views have no megakernel counterpart in the reference; in that mode every path of the views runs
+    // start to end in the tail kernel (the wavefront's per-sample streams, bit-identical images).
     P.tailPaths = g.renderMode == BTE_RENDER_MEGAKERNEL ? 0x7fffffff : g.tailPaths;
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
