@@ -41,8 +41,9 @@ BYTES_PER_SHADOW = 112            # 44 W + 44 R + 24 radiance RMW
 BYTES_PER_EXTEND_RAY = 64         # extend stage alone: queue 4 + ray 24 + hit 36
 BYTES_PER_SHADE_SEGMENT = 182
 BYTES_PER_CONNECT_RAY = 68        # 44 R + 24 RMW
-# DRAM bytes per frame of each stage kernel on this workload, from one ncu capture
-# (profiles/traffic_stage_kernels_disney_spheres_1080p.md; dram__bytes_read.sum + dram__bytes_write.sum)
+# DRAM bytes per frame of each stage kernel on this workload (1920x1080, 2 paths per pixel, depth 16), summed
+# over the frame's launches of that kernel from one ncu capture of the current build
+# (dram__bytes_read.sum + dram__bytes_write.sum); reported per launch beside the algorithmic bytes.
 STAGE_DRAM_BYTES_PER_FRAME = {"extend": 756.0e6, "shade": 3794.5e6, "connect": 432.1e6}
 
 
@@ -82,12 +83,13 @@ class Clocks:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_r%d.csv" % gpu_index)
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix="bte_clocks_%d_" % self.gpu, suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -122,6 +124,11 @@ class Clocks:
                         reasons.add(name)
         except Exception:
             return None
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
@@ -297,7 +304,9 @@ def denoise_leg():
 
 class ReferenceCpu:
     """The reference's integrator -- its shading headers compiled on the host (oracle/_ref, -O3, OpenMP
-    over all host cores) with the oracle's CPU BVH standing in for OptiX -- on the bench's view."""
+    over all host cores) with the oracle's CPU BVH standing in for OptiX -- on the bench's view.  `scene` is
+    the reference loader's flattening of the scene file (oracle.RefScene) or the product loader's identical
+    arrays."""
 
     def __init__(self, scene, args):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -341,8 +350,11 @@ def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
         return 0
-    import bluetruthengine_b200 as bte
-    scene = bte.load_scene(scene_path(args))
+    # the scene file flattened by the reference's own loader (src/scene.cpp, tinyobjloader, stb_image compiled
+    # from the reference tree), so this arm loads no library of this repository
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    scene = O.RefScene(scene_path(args))
     cpu = ReferenceCpu(scene, args)
     budget = max(2.0, 60.0 / max(args.steps, 1))
     for _ in range(args.warmup):
@@ -462,7 +474,8 @@ def run_ours(args):
                         "traffic": (STAGE_DRAM_BYTES_PER_FRAME[dom] / args.depth
                                     if dom in STAGE_DRAM_BYTES_PER_FRAME and W == 1920 and H == 1080 and args.spp == 2
                                     and args.depth == 16 else None),
-                        "traffic_source": "profiles/traffic_stage_kernels_disney_spheres_1080p.md (ncu, per launch)",
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on this "
+                                          "workload, per launch (one capture of the current build)",
                         "algorithmic_bytes_per_launch": bytes_dom / launches_dom,
                         "stage_ms": stages},
            "path_stats": {"extends_per_sample": s_mean, "shadow_rays_per_sample": r_mean,

@@ -17,7 +17,8 @@ from typing import Optional
 
 import numpy as np
 
-__all__ = ["BteError", "Renderer", "Scene", "load_scene", "library_path", "load_library", "RenderConfig",
+__all__ = ["BteError", "Renderer", "Scene", "load_scene", "library_path", "load_library", "default_variant",
+           "LIBRARIES", "RenderConfig",
            "ENV_CDF", "ENV_ALIAS", "TRIANGLE_DTYPE", "BSDF_DTYPE", "EMITTER_DTYPE", "SPOT_DTYPE", "CAMERA_DTYPE"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -79,28 +80,42 @@ class _SceneArrays(C.Structure):
                 ("mrWidths", C.POINTER(C.c_int)), ("mrHeights", C.POINTER(C.c_int))]
 
 
-def library_path() -> str:
-    return os.path.join(HERE, "libbte_b200.so")
+# The two builds of the library (bluetruthengine_b200/build.py): "fast" is the product (FP32 shading with
+# CUDA's single-precision functions), "parity" matches the CPU checker bit for bit.  BTE_LIBRARY selects the
+# default for this process.
+LIBRARIES = {"fast": "libbte_b200.so", "parity": "libbte_b200_parity.so"}
 
 
-_LIB: Optional[C.CDLL] = None
+def default_variant() -> str:
+    v = os.environ.get("BTE_LIBRARY", "fast")
+    if v not in LIBRARIES:
+        raise BteError(f"BTE_LIBRARY must be one of {sorted(LIBRARIES)}, not {v!r}")
+    return v
 
 
-def load_library(build_if_missing: bool = True) -> C.CDLL:
-    """Load libbte_b200.so (building it with nvcc when absent)."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
-    path = library_path()
+def library_path(variant: Optional[str] = None) -> str:
+    return os.path.join(HERE, LIBRARIES[variant or default_variant()])
+
+
+_LIBS: dict = {}
+
+
+def load_library(build_if_missing: bool = True, variant: Optional[str] = None) -> C.CDLL:
+    """Load one build of the library (default: BTE_LIBRARY, else the product), building both with nvcc when
+    they are absent or older than their sources."""
+    variant = variant or default_variant()
+    if variant in _LIBS:
+        return _LIBS[variant]
+    path = library_path(variant)
     if build_if_missing:
         from . import build as _build
         _build.build()
     if not os.path.exists(path):
-        raise BteError(f"libbte_b200.so not found at {path}; run bluetruthengine_b200/build.py")
+        raise BteError(f"{os.path.basename(path)} not found at {path}; run bluetruthengine_b200/build.py")
     lib = C.CDLL(path)
     lib.bte_last_error.restype = C.c_char_p
     lib.bte_get_render_mode.restype = C.c_int
-    _LIB = lib
+    _LIBS[variant] = lib
     return lib
 
 
@@ -108,9 +123,10 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def _check(rc: int):
+def _check(rc: int, lib: Optional[C.CDLL] = None):
     if rc < 0:
-        raise BteError(load_library(False).bte_last_error().decode("utf-8", "replace"))
+        lib = lib or load_library(False)
+        raise BteError(lib.bte_last_error().decode("utf-8", "replace"))
     return rc
 
 
@@ -257,63 +273,67 @@ class Renderer:
     One renderer state per process, like the reference's globals.
     """
 
-    def __init__(self):
-        self.lib = load_library()
+    def __init__(self, variant: Optional[str] = None):
+        self.variant = variant or default_variant()
+        self.lib = load_library(variant=self.variant)
         self._keep = []
+
+    def _ck(self, rc: int) -> int:
+        return _check(rc, self.lib)
 
     # ---- uploads ----
     def init_scene(self, triangles, materials, triangle_material_ids, width, height):
         t = np.ascontiguousarray(triangles, dtype=TRIANGLE_DTYPE)
         m = np.ascontiguousarray(materials, dtype=np.float32)
         ids = None if triangle_material_ids is None else np.ascontiguousarray(triangle_material_ids, dtype=np.int32)
-        _check(self.lib.bte_init_scene(_ptr(t), len(t), _ptr(m), len(m), _ptr(ids), int(width), int(height)))
+        self._ck(self.lib.bte_init_scene(_ptr(t), len(t), _ptr(m), len(m), _ptr(ids), int(width), int(height)))
 
     def init_accel(self):
-        _check(self.lib.bte_init_accel())
+        self._ck(self.lib.bte_init_accel())
 
     init_optix = init_accel   # the reference name (cudaInitOptix) builds the acceleration structure
 
     def init_camera(self, camera):
         c = np.ascontiguousarray(np.asarray(camera, dtype=CAMERA_DTYPE).reshape(1))
-        _check(self.lib.bte_init_camera(_ptr(c)))
+        self._ck(self.lib.bte_init_camera(_ptr(c)))
 
     def init_triangle_emission(self, emission):
         e = None if emission is None else np.ascontiguousarray(emission, dtype=np.float32)
-        _check(self.lib.bte_init_triangle_emission(_ptr(e), 0 if e is None else len(e)))
+        self._ck(self.lib.bte_init_triangle_emission(_ptr(e), 0 if e is None else len(e)))
 
     def init_triangle_emitter_flags(self, flags):
         f = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
-        _check(self.lib.bte_init_triangle_emitter_flags(_ptr(f), 0 if f is None else len(f)))
+        self._ck(self.lib.bte_init_triangle_emitter_flags(_ptr(f), 0 if f is None else len(f)))
 
     def init_emitter_table(self, emitters, tri_indices, tri_cdf, scene_cdf):
         if emitters is None or len(emitters) == 0:
-            _check(self.lib.bte_init_emitter_table(None, 0, None, 0, None, 0, None))
+            self._ck(self.lib.bte_init_emitter_table(None, 0, None, 0, None, 0, None))
             return
         e = np.ascontiguousarray(emitters, dtype=EMITTER_DTYPE)
         ti = np.ascontiguousarray(tri_indices, dtype=np.int32)
         tc = np.ascontiguousarray(tri_cdf, dtype=np.float32)
         sc = np.ascontiguousarray(scene_cdf, dtype=np.float32)
-        _check(self.lib.bte_init_emitter_table(_ptr(e), len(e), _ptr(ti), len(ti), _ptr(tc), len(tc), _ptr(sc)))
+        self._ck(self.lib.bte_init_emitter_table(_ptr(e), len(e), _ptr(ti), len(ti), _ptr(tc), len(tc), _ptr(sc)))
 
     def init_bsdfs(self, bsdfs, triangle_bsdf_ids):
         b = np.ascontiguousarray(bsdfs, dtype=BSDF_DTYPE)
         ids = np.ascontiguousarray(triangle_bsdf_ids, dtype=np.int32)
-        _check(self.lib.bte_init_bsdfs(_ptr(b), len(b), _ptr(ids), len(ids)))
+        self._ck(self.lib.bte_init_bsdfs(_ptr(b), len(b), _ptr(ids), len(ids)))
 
     def init_spotlights(self, spots):
         if spots is None or len(spots) == 0:
-            _check(self.lib.bte_init_spotlights(None, 0))
+            self._ck(self.lib.bte_init_spotlights(None, 0))
             return
         s = np.ascontiguousarray(spots, dtype=SPOT_DTYPE)
-        _check(self.lib.bte_init_spotlights(_ptr(s), len(s)))
+        self._ck(self.lib.bte_init_spotlights(_ptr(s), len(s)))
 
     def init_env_map(self, rgba, intensity=1.0, rotation_deg=0.0):
         if rgba is None:
-            _check(self.lib.bte_init_env_map(None, 0, 0, C.c_float(0.0), C.c_float(0.0)))
+            self._ck(self.lib.bte_init_env_map(None, 0, 0, C.c_float(0.0), C.c_float(0.0)))
             return
         e = np.ascontiguousarray(rgba, dtype=np.float32)
         h, w = e.shape[0], e.shape[1]
-        _check(self.lib.bte_init_env_map(_ptr(e), w, h, C.c_float(intensity), C.c_float(rotation_deg)))
+        self._ck(self.lib.bte_init_env_map(_ptr(e), w, h, C.c_float(intensity), C.c_float(rotation_deg)))
 
     def init_textures(self, images):
         self._init_tex(self.lib.bte_init_textures, images)
@@ -323,13 +343,13 @@ class Renderer:
 
     def _init_tex(self, fn, images):
         if not images:
-            _check(fn(None, None, None, 0))
+            self._ck(fn(None, None, None, 0))
             return
         arrs = [None if im is None else np.ascontiguousarray(im, dtype=np.uint8) for im in images]
         ptrs = (C.c_void_p * len(arrs))(*[None if a is None else a.ctypes.data for a in arrs])
         ws = np.array([0 if a is None else a.shape[1] for a in arrs], dtype=np.int32)
         hs = np.array([0 if a is None else a.shape[0] for a in arrs], dtype=np.int32)
-        _check(fn(ptrs, _ptr(ws), _ptr(hs), len(arrs)))
+        self._ck(fn(ptrs, _ptr(ws), _ptr(hs), len(arrs)))
 
     def upload(self, scene: Scene):
         """All uploads in the order of src/main.cpp:819-930."""
@@ -351,41 +371,41 @@ class Renderer:
     def set_config(self, samples_per_frame=1, max_depth=200, rr_start=3, env_sampling=ENV_CDF, block_size=0,
                    use_graph=0):
         cfg = RenderConfig(samples_per_frame, max_depth, rr_start, env_sampling, block_size, use_graph)
-        _check(self.lib.bte_set_render_config(C.byref(cfg)))
+        self._ck(self.lib.bte_set_render_config(C.byref(cfg)))
 
     def reset_accumulation(self, width, height):
-        _check(self.lib.bte_reset_accumulation(int(width), int(height)))
+        self._ck(self.lib.bte_reset_accumulation(int(width), int(height)))
 
     def render(self, width, height):
-        _check(self.lib.bte_render(int(width), int(height)))
+        self._ck(self.lib.bte_render(int(width), int(height)))
 
     def set_output_buffer(self, device_ptr: int):
-        _check(self.lib.bte_set_output_buffer(C.c_void_p(device_ptr)))
+        self._ck(self.lib.bte_set_output_buffer(C.c_void_p(device_ptr)))
 
     def set_render_mode(self, mode: int):
-        _check(self.lib.bte_set_render_mode(int(mode)))
+        self._ck(self.lib.bte_set_render_mode(int(mode)))
 
     def get_render_mode(self) -> int:
         return int(self.lib.bte_get_render_mode())
 
     def cleanup(self):
-        _check(self.lib.bte_cleanup())
+        self._ck(self.lib.bte_cleanup())
 
     def stats(self) -> FrameStats:
         s = FrameStats()
-        _check(self.lib.bte_get_frame_stats(C.byref(s)))
+        self._ck(self.lib.bte_get_frame_stats(C.byref(s)))
         return s
 
     def set_stage_timing(self, on: bool):
-        _check(self.lib.bte_set_stage_timing(1 if on else 0))
+        self._ck(self.lib.bte_set_stage_timing(1 if on else 0))
 
     def toggle_denoiser(self) -> bool:
         """cudaToggleDenoiser: returns the new state; needs denoiser weights loaded."""
-        return bool(_check(self.lib.bte_toggle_denoiser()))
+        return bool(self._ck(self.lib.bte_toggle_denoiser()))
 
     def read_denoised(self, width: int, height: int) -> np.ndarray:
         out = np.empty((height, width, 3), dtype=np.float32)
-        _check(self.lib.bte_read_denoised(out.ctypes.data_as(C.c_void_p)))
+        self._ck(self.lib.bte_read_denoised(out.ctypes.data_as(C.c_void_p)))
         return out
 
     def render_views(self, views):
@@ -395,25 +415,25 @@ class Renderer:
         for i, (cam, w, h, spp) in enumerate(views):
             arr[i]["camera"] = np.asarray(cam, dtype=CAMERA_DTYPE)
             arr[i]["width"], arr[i]["height"], arr[i]["samplesPerFrame"] = w, h, spp
-        _check(self.lib.bte_render_views(_ptr(arr), len(views)))
+        self._ck(self.lib.bte_render_views(_ptr(arr), len(views)))
 
     def read_view_accum(self, view: int, width: int, height: int):
         """(FP32 running mean [W*H, 3], FP64 running sum [W*H, 3]) of a batched view."""
         mean = np.empty((width * height, 3), dtype=np.float32)
         total = np.empty((width * height, 3), dtype=np.float64)
-        _check(self.lib.bte_read_view_accum(int(view), _ptr(mean), _ptr(total)))
+        self._ck(self.lib.bte_read_view_accum(int(view), _ptr(mean), _ptr(total)))
         return mean, total
 
     def reset_views(self):
-        _check(self.lib.bte_reset_views())
+        self._ck(self.lib.bte_reset_views())
 
     def select_scene(self, scene: int):
         """Make scene slot 0..7 the one every upload, configuration and render call acts on."""
-        _check(self.lib.bte_select_scene(int(scene)))
+        self._ck(self.lib.bte_select_scene(int(scene)))
 
     def selected_scene(self) -> int:
         out = C.c_int(0)
-        _check(self.lib.bte_get_selected_scene(C.byref(out)))
+        self._ck(self.lib.bte_get_selected_scene(C.byref(out)))
         return out.value
 
     def render_scene_batch(self, batch):
@@ -426,16 +446,16 @@ class Renderer:
         for i, (cam, w, h, spp) in enumerate(flat):
             arr[i]["camera"] = np.asarray(cam, dtype=CAMERA_DTYPE)
             arr[i]["width"], arr[i]["height"], arr[i]["samplesPerFrame"] = w, h, spp
-        _check(self.lib.bte_render_scene_batch(_ptr(slots), _ptr(counts), _ptr(arr), len(batch)))
+        self._ck(self.lib.bte_render_scene_batch(_ptr(slots), _ptr(counts), _ptr(arr), len(batch)))
 
     def set_aov(self, enabled: bool):
         """Accumulate first-hit albedo and shading normal per pixel (denoiser features)."""
-        _check(self.lib.bte_set_aov(1 if enabled else 0))
+        self._ck(self.lib.bte_set_aov(1 if enabled else 0))
 
     def read_aov(self, width: int, height: int):
         """(albedo [H, W, 3], normal [H, W, 3]) running means, float32."""
         out = np.empty((height, width, 6), dtype=np.float32)
-        _check(self.lib.bte_read_aov(out.ctypes.data_as(C.c_void_p)))
+        self._ck(self.lib.bte_read_aov(out.ctypes.data_as(C.c_void_p)))
         return out[..., :3].copy(), out[..., 3:].copy()
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
@@ -444,80 +464,80 @@ class Renderer:
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),
                    int(tail_paths), int(bvh_builder), int(ploc_radius),
                    int(overlap_connect), int(wide_collapse))
-        _check(self.lib.bte_set_tuning(C.byref(t)))
+        self._ck(self.lib.bte_set_tuning(C.byref(t)))
 
     def tuning(self) -> dict:
         t = Tuning()
-        _check(self.lib.bte_get_tuning(C.byref(t)))
+        self._ck(self.lib.bte_get_tuning(C.byref(t)))
         return {f: getattr(t, f) for f, _ in Tuning._fields_}
 
     def accel_info(self) -> dict:
         w, n, d, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
-        _check(self.lib.bte_get_accel_info(C.byref(w), C.byref(n), C.byref(d), C.byref(ms)))
+        self._ck(self.lib.bte_get_accel_info(C.byref(w), C.byref(n), C.byref(d), C.byref(ms)))
         b = C.c_int()
-        _check(self.lib.bte_get_accel_builder(C.byref(b)))
+        self._ck(self.lib.bte_get_accel_builder(C.byref(b)))
         return {"width": w.value, "nodes": n.value, "depth": d.value, "ms_build": ms.value, "builder": b.value}
 
     def set_hit_log(self, on: bool):
-        _check(self.lib.bte_set_hit_log(1 if on else 0))
+        self._ck(self.lib.bte_set_hit_log(1 if on else 0))
 
     def frame_index(self) -> int:
         v = C.c_uint32()
-        _check(self.lib.bte_get_frame_index(C.byref(v)))
+        self._ck(self.lib.bte_get_frame_index(C.byref(v)))
         return int(v.value)
 
     def set_frame_index(self, i: int):
-        _check(self.lib.bte_set_frame_index(C.c_uint32(i)))
+        self._ck(self.lib.bte_set_frame_index(C.c_uint32(i)))
 
     # ---- headless output ----
     def write_png(self, path: str):
-        _check(self.lib.bte_write_png(str(path).encode()))
+        self._ck(self.lib.bte_write_png(str(path).encode()))
 
     def capture_screenshot(self) -> str:
         buf = C.create_string_buffer(64)
-        _check(self.lib.bte_capture_screenshot(buf, 64))
+        self._ck(self.lib.bte_capture_screenshot(buf, 64))
         return buf.value.decode()
 
     def record_start(self, raw_path: Optional[str] = None, fps: int = 30):
-        _check(self.lib.bte_record_start(None if raw_path is None else str(raw_path).encode(), int(fps)))
+        self._ck(self.lib.bte_record_start(None if raw_path is None else str(raw_path).encode(), int(fps)))
 
     def record_frame(self):
-        _check(self.lib.bte_record_frame())
+        self._ck(self.lib.bte_record_frame())
 
     def record_stop(self):
-        _check(self.lib.bte_record_stop())
+        self._ck(self.lib.bte_record_stop())
 
     def mark_scene_changed(self):
-        _check(self.lib.bte_mark_scene_changed())
+        self._ck(self.lib.bte_mark_scene_changed())
 
     def framebuffer_size(self):
         w, h = C.c_int(), C.c_int()
-        _check(self.lib.bte_get_framebuffer_size(C.byref(w), C.byref(h)))
+        self._ck(self.lib.bte_get_framebuffer_size(C.byref(w), C.byref(h)))
         return w.value, h.value
 
     def read_framebuffer(self, width, height) -> np.ndarray:
         out = np.empty(width * height, dtype=np.uint32)
-        _check(self.lib.bte_read_framebuffer(_ptr(out)))
+        self._ck(self.lib.bte_read_framebuffer(_ptr(out)))
         return out
 
     def read_accum(self, width, height) -> np.ndarray:
         out = np.empty((width * height, 3), dtype=np.float32)
-        _check(self.lib.bte_read_accum(_ptr(out)))
+        self._ck(self.lib.bte_read_accum(_ptr(out)))
         return out
 
     def read_accum_f64(self, width, height) -> np.ndarray:
         out = np.empty((width * height, 3), dtype=np.float64)
-        _check(self.lib.bte_read_accum_f64(_ptr(out)))
+        self._ck(self.lib.bte_read_accum_f64(_ptr(out)))
         return out
 
     def read_sample_radiance(self, count: int) -> np.ndarray:
         out = np.empty((count, 3), dtype=np.float32)
-        _check(self.lib.bte_read_sample_radiance(_ptr(out), int(count)))
+        self._ck(self.lib.bte_read_sample_radiance(_ptr(out), int(count)))
         return out
 
     def read_hit_log(self, count: int) -> np.ndarray:
         out = np.empty(count, dtype=np.int32)
-        _check(self.lib.bte_read_hit_log(_ptr(out), int(count)))
+        self._ck(self.lib.bte_read_hit_log(_ptr(out), int(count)))
         return out
 
     # ---- parity probes ----
@@ -526,14 +546,14 @@ class Renderer:
         n = len(r)
         tri = np.empty(n, dtype=np.int32)
         tuv = np.empty((n, 3), dtype=np.float32)
-        _check(self.lib.bte_trace_closest_lanes(_ptr(r), n, int(lanes), _ptr(tri), _ptr(tuv)))
+        self._ck(self.lib.bte_trace_closest_lanes(_ptr(r), n, int(lanes), _ptr(tri), _ptr(tuv)))
         return tri, tuv
 
     def trace_occluded(self, rays: np.ndarray, tmax: np.ndarray, lanes: int = 1):
         r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
         t = np.ascontiguousarray(tmax, dtype=np.float32)
         out = np.empty(len(r), dtype=np.uint8)
-        _check(self.lib.bte_trace_occluded_lanes(_ptr(r), _ptr(t), len(r), int(lanes), _ptr(out)))
+        self._ck(self.lib.bte_trace_occluded_lanes(_ptr(r), _ptr(t), len(r), int(lanes), _ptr(out)))
         return out
 
     def env_query(self, op: int, x: np.ndarray) -> np.ndarray:
@@ -541,14 +561,14 @@ class Renderer:
         n = len(x)
         width = {0: 3, 1: 1, 2: 7}[op]
         out = np.empty((n, width), dtype=np.float32)
-        _check(self.lib.bte_env_query(int(op), _ptr(x), n, _ptr(out)))
+        self._ck(self.lib.bte_env_query(int(op), _ptr(x), n, _ptr(out)))
         return out
 
     def env_tables(self, w, h):
         marg = np.empty(h + 1, dtype=np.float32)
         cond = np.empty(h * (w + 1), dtype=np.float32)
         tp = C.c_float()
-        _check(self.lib.bte_env_tables(_ptr(marg), _ptr(cond), C.byref(tp)))
+        self._ck(self.lib.bte_env_tables(_ptr(marg), _ptr(cond), C.byref(tp)))
         return marg, cond, float(tp.value)
 
     def env_alias_tables(self, w, h):
@@ -557,14 +577,14 @@ class Renderer:
         cp = np.empty(h * w, dtype=np.float32)
         ci = np.empty(h * w, dtype=np.int32)
         pp = np.empty(h * w, dtype=np.float32)
-        _check(self.lib.bte_env_alias_tables(_ptr(rp), _ptr(ri), _ptr(cp), _ptr(ci), _ptr(pp)))
+        self._ck(self.lib.bte_env_alias_tables(_ptr(rp), _ptr(ri), _ptr(cp), _ptr(ci), _ptr(pp)))
         return rp, ri, cp, ci, pp
 
     def math_eval(self, fn: int, a: np.ndarray, b: Optional[np.ndarray] = None) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float32)
         bb = None if b is None else np.ascontiguousarray(b, dtype=np.float32)
         out = np.empty_like(a)
-        _check(self.lib.bte_math_eval(int(fn), _ptr(a), _ptr(bb), _ptr(out), len(a)))
+        self._ck(self.lib.bte_math_eval(int(fn), _ptr(a), _ptr(bb), _ptr(out), len(a)))
         return out
 
     def bsdf_query(self, bsdf, op: int, wi: np.ndarray, x: np.ndarray) -> np.ndarray:
@@ -574,7 +594,7 @@ class Renderer:
         n = len(wi)
         width = {0: 3, 1: 1, 2: 8}[op]
         out = np.empty((n, width), dtype=np.float32)
-        _check(self.lib.bte_bsdf_query(_ptr(b), int(op), _ptr(wi), _ptr(x), n, _ptr(out)))
+        self._ck(self.lib.bte_bsdf_query(_ptr(b), int(op), _ptr(wi), _ptr(x), n, _ptr(out)))
         return out
 
     def tex_hw_vs_sw(self, texels: np.ndarray, wrap_v: bool, uv: np.ndarray):
@@ -584,5 +604,5 @@ class Renderer:
         n = len(uv)
         hw = np.empty((n, 4), dtype=np.float32)
         sw = np.empty((n, 4), dtype=np.float32)
-        _check(self.lib.bte_tex_hw_vs_sw(_ptr(t), w, h, 1 if wrap_v else 0, _ptr(uv), n, _ptr(hw), _ptr(sw)))
+        self._ck(self.lib.bte_tex_hw_vs_sw(_ptr(t), w, h, 1 if wrap_v else 0, _ptr(uv), n, _ptr(hw), _ptr(sw)))
         return hw, sw

@@ -1015,6 +1015,82 @@ fail:
     return rc;
 }
 
+// Steps 1-3: per-triangle centroids and their bounds, 63-bit Morton codes (keysA / valsA = triangle index), and
+// the stable LSD radix sort of (code, index) over 16 passes of 4-bit digits.  *sortedKeys / *sortedVals name the
+// ping-pong buffers holding the sorted pairs, *spareKeys / *spareVals the other two.  bounds holds 6 words and
+// hist kDigits * ceil(n / kSortTile) ints.
+int launchMortonSort(const TriangleData* dTris, int n, float4* cen, unsigned int* bounds, unsigned long long* keysA,
+                     unsigned long long* keysB, int* valsA, int* valsB, int* hist, cudaStream_t st,
+                     unsigned long long** sortedKeys, unsigned long long** spareKeys, int** sortedVals,
+                     int** spareVals, std::string& err)
+{
+    const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    cudaError_t e = cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { err = std::string("LBVH build: ") + cudaGetErrorString(e); return -1; }
+    const int B = 256, G = (n + B - 1) / B;
+    const int numTiles = (n + kSortTile - 1) / kSortTile;
+    kTriPrep<<<G, B, 0, st>>>(dTris, n, cen, bounds);
+    kMorton<<<G, B, 0, st>>>(cen, n, bounds, keysA, valsA);
+    unsigned long long *kin = keysA, *kout = keysB;
+    int *vin = valsA, *vout = valsB;
+    for (int shift = 0; shift < 64; shift += 4) {
+        kRadixHist<<<numTiles, kSortThreads, 0, st>>>(kin, n, shift, numTiles, hist);
+        kScanSingle<<<1, 1024, 0, st>>>(hist, kDigits * numTiles);
+        kRadixScatter<<<numTiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, numTiles, hist);
+        unsigned long long* tk = kin; kin = kout; kout = tk;
+        int* tv = vin; vin = vout; vout = tv;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { err = std::string("LBVH build: ") + cudaGetErrorString(e); return -1; }
+    *sortedKeys = kin; *spareKeys = kout; *sortedVals = vin; *spareVals = vout;
+    return 0;
+}
+
+// The Morton codes and sorted order the build produces for host triangles (a check of the integer steps).
+int lbvhMortonOrder(const TriangleData* hostTris, int n, unsigned long long* hostKeys, int* hostSorted,
+                    std::string& err)
+{
+    if (n <= 0 || !hostTris) { err = "bte_debug_lbvh_order: no triangles"; return -1; }
+    TriangleData* tris = nullptr;
+    float4* cen = nullptr;
+    unsigned int* bounds = nullptr;
+    unsigned long long *keysA = nullptr, *keysB = nullptr, *kin = nullptr, *kout = nullptr;
+    int *valsA = nullptr, *valsB = nullptr, *hist = nullptr, *vin = nullptr, *vout = nullptr;
+    const int numTiles = (n + kSortTile - 1) / kSortTile;
+    int rc = -1;
+    cudaStream_t st = nullptr;
+    auto okc = [&](cudaError_t e) {
+        if (e != cudaSuccess) err = std::string("bte_debug_lbvh_order: ") + cudaGetErrorString(e);
+        return e == cudaSuccess;
+    };
+    if (okc(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) &&
+        okc(cudaMalloc(&tris, sizeof(TriangleData) * n)) && okc(cudaMalloc(&cen, sizeof(float4) * n)) &&
+        okc(cudaMalloc(&bounds, sizeof(unsigned int) * 6)) && okc(cudaMalloc(&keysA, sizeof(unsigned long long) * n)) &&
+        okc(cudaMalloc(&keysB, sizeof(unsigned long long) * n)) && okc(cudaMalloc(&valsA, sizeof(int) * n)) &&
+        okc(cudaMalloc(&valsB, sizeof(int) * n)) && okc(cudaMalloc(&hist, sizeof(int) * kDigits * numTiles)) &&
+        okc(cudaMemcpyAsync(tris, hostTris, sizeof(TriangleData) * n, cudaMemcpyHostToDevice, st))) {
+        // the codes before sorting are kMorton's output: copy them out of keysA before the first pass moves them
+        const int B = 256, G = (n + B - 1) / B;
+        const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        if (okc(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st))) {
+            kTriPrep<<<G, B, 0, st>>>(tris, n, cen, bounds);
+            kMorton<<<G, B, 0, st>>>(cen, n, bounds, keysA, valsA);
+            if (okc(cudaGetLastError()) &&
+                okc(cudaMemcpyAsync(hostKeys, keysA, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, st)) &&
+                okc(cudaStreamSynchronize(st)) &&
+                launchMortonSort(tris, n, cen, bounds, keysA, keysB, valsA, valsB, hist, st, &kin, &kout, &vin, &vout,
+                                 err) == 0 &&
+                okc(cudaMemcpyAsync(hostSorted, vin, sizeof(int) * n, cudaMemcpyDeviceToHost, st)) &&
+                okc(cudaStreamSynchronize(st)))
+                rc = 0;
+        }
+    }
+    cudaFree(tris); cudaFree(cen); cudaFree(bounds); cudaFree(keysA); cudaFree(keysB); cudaFree(valsA); cudaFree(valsB);
+    cudaFree(hist);
+    if (st) cudaStreamDestroy(st);
+    return rc;
+}
+
 int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int builder, int radius, int wideCollapse,
               BvhBuildResult& out, cudaStream_t st, std::string& err)
 {
@@ -1059,23 +1135,13 @@ int buildLbvh(const TriangleData* dTris, int n, int maxLeaf, int width, int buil
         BVH_CK(cudaMalloc(&leafBox, sizeof(float) * 6 * n));
         BVH_CK(cudaMalloc(&sorted, sizeof(float4) * 3 * static_cast<size_t>(n)));
         if (width == 2) BVH_CK(cudaMalloc(&out.nodes, sizeof(BvhNode) * inner));
-        {
-            const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-            BVH_CK(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st));
-        }
         BVH_CK(cudaMemsetAsync(arrivals, 0, sizeof(int) * inner, st));
         const int B = 256, G = (n + B - 1) / B;
-        kTriPrep<<<G, B, 0, st>>>(dTris, n, cen, bounds);
-        kMorton<<<G, B, 0, st>>>(cen, n, bounds, keysA, valsA);
-        unsigned long long *kin = keysA, *kout = keysB;
-        int *vin = valsA, *vout = valsB;
-        for (int shift = 0; shift < 64; shift += 4) {
-            kRadixHist<<<numTiles, kSortThreads, 0, st>>>(kin, n, shift, numTiles, hist);
-            kScanSingle<<<1, 1024, 0, st>>>(hist, kDigits * numTiles);
-            kRadixScatter<<<numTiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, numTiles, hist);
-            unsigned long long* tk = kin; kin = kout; kout = tk;
-            int* tv = vin; vin = vout; vout = tv;
-        }
+        unsigned long long *kin = nullptr, *kout = nullptr;
+        int *vin = nullptr, *vout = nullptr;
+        if (launchMortonSort(dTris, n, cen, bounds, keysA, keysB, valsA, valsB, hist, st, &kin, &kout, &vin, &vout,
+                             err) != 0)
+            goto fail;
         out.builder = 0;
         if (n > 1 && builder == 1) {
             int depth = 0;

@@ -187,6 +187,14 @@ done:
 // one file-scope device array of fixed size, so maps are limited to
 // kNoAllocMaxTexels texels and kNoAllocMaxRows rows.
 //
+// The first use of the array on a device looks up its device address; under
+// CUDA's lazy module loading that lookup also loads this file's module, which
+// is when the array's memory is taken.  The renderer's device initialisation
+// (any bte_* call that sets up the renderer) does this lookup, and so does the
+// first call here: a caller that reserves the rest of device memory for its
+// own pool should make one of those calls first, and the first call here
+// should come before any stream capture.
+//
 // The array is shared by every call in the process: two calls whose kernels
 // overlap on the GPU (different streams, or different host threads on one
 // device) race on it and produce garbage; serialise them.  Nothing in it has
@@ -237,6 +245,15 @@ int scratchForCurrentDevice(unsigned char** out, std::string& err)
 
 }  // namespace
 
+// Looks up (and, under lazy module loading, loads) the scratch array on the current device.  The renderer's
+// device initialisation calls it, so a caller that initialises the renderer before reserving its memory pool
+// has the array in place before its first bte_env_build_alias_noalloc.
+int prepareEnvNoallocScratch(std::string& err)
+{
+    unsigned char* base = nullptr;
+    return scratchForCurrentDevice(&base, err);
+}
+
 }  // namespace bte
 
 extern "C" int bte_env_build_alias_noalloc(const float* dTexelsRGBA, int width, int height, float* dRowProb,
@@ -260,6 +277,12 @@ extern "C" int bte_env_build_alias_noalloc(const float* dTexelsRGBA, int width, 
     }
     if (reinterpret_cast<uintptr_t>(dTexelsRGBA) % 16 != 0) {
         setError("bte_env_build_alias_noalloc: texels must be 16-byte aligned (float4 per texel)");
+        return -1;
+    }
+    if (reinterpret_cast<uintptr_t>(dTotalPower) % 8 != 0 || reinterpret_cast<uintptr_t>(dRowProb) % 4 != 0 ||
+        reinterpret_cast<uintptr_t>(dRowAlias) % 4 != 0 || reinterpret_cast<uintptr_t>(dColProb) % 4 != 0 ||
+        reinterpret_cast<uintptr_t>(dColAlias) % 4 != 0 || reinterpret_cast<uintptr_t>(dPixelPdf) % 4 != 0) {
+        setError("bte_env_build_alias_noalloc: dTotalPower must be 8-byte aligned and the tables 4-byte aligned");
         return -1;
     }
     unsigned char* base = nullptr;

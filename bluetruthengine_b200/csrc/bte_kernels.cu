@@ -457,15 +457,28 @@ __global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams
     }
 }
 
+// Adds v to *counter with one atomic per group of lanes that arrive here together with the same key (the
+// counter is the same for equal keys); lanes of a warp may be at different bounces in the megakernel.
+BTE_DI void groupedAdd(int* counter, int key, int v)
+{
+    const unsigned active = __activemask();
+    const unsigned group = __match_any_sync(active, key);
+    const int total = __reduce_add_sync(group, v);
+    if (static_cast<unsigned>(__ffs(group) - 1) == (threadIdx.x & 31u) && total != 0) atomicAdd(counter, total);
+}
+
 // RenderMode::Megakernel, src/optix_programs.cu:54-108: one thread per pixel and one RNG stream per pixel and
 // frame, rngSeed(pixel, frameIndex) = makeRng(hashUint(pixel ^ frameIndex * 0x9e3779b9)), carried through f.spp
 // paths in turn, each drawing its jitter first.  Each path runs the tail kernel's bounce loop on the pixel's own
 // path slot (the stream returns through P.o.w); the paths' radiance is summed in sample order from zero, scaled
 // by div3, folded into the FP32 Welford mean once per frame (n = frames so far + 1) and into the FP64 sum, then
-// packed.
+// packed.  With features on (aovAccum), each path's first-hit albedo and normal (written by shadePath at bounce
+// 0 into the pixel's slot) are summed the same way and their per-frame mean folded into aovAccum, so the
+// denoiser sees the same features in both render modes.
 template <int Width>
 __global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, FrameParams f, float* accum,
-                                                   double* accumD, uint32_t* framebuffer, uint32_t* extFramebuffer)
+                                                   double* accumD, uint32_t* framebuffer, uint32_t* extFramebuffer,
+                                                   float* aovAccum)
 {
     const int pix = blockIdx.x * blockDim.x + threadIdx.x;
     const int wh = f.width * f.height;
@@ -474,6 +487,8 @@ __global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, Frame
     const int px = pix % f.width, py = pix / f.width;
     uint32_t rng = rngSeed(static_cast<uint32_t>(pix), frameIndex);
     V3 sum = v3(0.0f, 0.0f, 0.0f);
+    float feat[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const bool features = aovAccum && P.aovAlbedo;
     for (int k = 0; k < f.spp; ++k) {
         const float jx = rngNext(rng) - 0.5f;
         const float jy = rngNext(rng) - 0.5f;
@@ -485,7 +500,7 @@ __global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, Frame
         P.L[pix] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(1u << 16));
         P.shMask[pix] = 0u;
         for (int b = 0; b < P.maxDepth; ++b) {
-            atomicAdd(P.rayCount + b, 1);
+            groupedAdd(P.rayCount + b, b, 1);
             const float4 ro = P.o[pix];
             const float4 rd = P.d[pix];
             const RayPre r = rayPre(ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, s.sceneMaxAbs);
@@ -494,8 +509,8 @@ __global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, Frame
             P.hit[pix] = make_float4(t, u, v, __int_as_float(tri));
             const bool alive = shadePath(s, P, f, b, pix, false);
             uint32_t mask = P.shMask[pix];
+            groupedAdd(P.shadowCount + b, b, __popc(mask));
             if (mask) {
-                atomicAdd(P.shadowCount + b, __popc(mask));
                 const float4 so = P.shOrigin[pix];
                 const size_t base = static_cast<size_t>(pix) * P.slots;
                 for (uint32_t m = mask; m; m &= m - 1u) {
@@ -511,6 +526,20 @@ __global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, Frame
         const float4 L4 = P.L[pix];
         sum = add3(sum, resolveShadows(P, pix, v3(L4.x, L4.y, L4.z)));
         rng = __float_as_uint(P.o[pix].w);
+        if (features) {
+            const float4 a = P.aovAlbedo[pix], nn = P.aovNormal[pix];
+            feat[0] += a.x; feat[1] += a.y; feat[2] += a.z;
+            feat[3] += nn.x; feat[4] += nn.y; feat[5] += nn.z;
+        }
+    }
+    if (features) {
+        const float paths = static_cast<float>(f.spp);
+        const float n = static_cast<float>(frameIndex + 1u);
+        for (int c = 0; c < 6; ++c) {
+            float m = aovAccum[6 * static_cast<size_t>(pix) + c];
+            m = m + (feat[c] / paths - m) / n;
+            aovAccum[6 * static_cast<size_t>(pix) + c] = m;
+        }
     }
     const V3 c = div3(sum, static_cast<float>(f.spp));
     const float n = static_cast<float>(frameIndex + 1u);
@@ -780,11 +809,11 @@ void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cuda
     else kTail<2><<<blocks, 128, 0, st>>>(s, P, f);
 }
 void launchMegakernel(const DevScene& s, const DevPaths& P, const FrameParams& f, float* accum, double* accumD,
-                      uint32_t* fb, uint32_t* extFb, cudaStream_t st)
+                      uint32_t* fb, uint32_t* extFb, float* aovAccum, cudaStream_t st)
 {
     const int wh = f.width * f.height;
-    if (s.bvhWidth == 8) kMegakernel<8><<<(wh + 127) / 128, 128, 0, st>>>(s, P, f, accum, accumD, fb, extFb);
-    else kMegakernel<2><<<(wh + 127) / 128, 128, 0, st>>>(s, P, f, accum, accumD, fb, extFb);
+    if (s.bvhWidth == 8) kMegakernel<8><<<(wh + 127) / 128, 128, 0, st>>>(s, P, f, accum, accumD, fb, extFb, aovAccum);
+    else kMegakernel<2><<<(wh + 127) / 128, 128, 0, st>>>(s, P, f, accum, accumD, fb, extFb, aovAccum);
 }
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    float* aovAccum, cudaStream_t st)

@@ -15,7 +15,7 @@ void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
 void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cudaStream_t st);
 void launchMegakernel(const DevScene& s, const DevPaths& P, const FrameParams& f, float* accum, double* accumD,
-                      uint32_t* fb, uint32_t* extFb, cudaStream_t st);
+                      uint32_t* fb, uint32_t* extFb, float* aovAccum, cudaStream_t st);
 void launchPresentViews(const DevPaths& P, const FrameParams& f, int totalPixels, cudaStream_t st);
 void launchPresent(const DevPaths& P, const FrameParams& f, float* accum, double* accumD, uint32_t* fb, uint32_t* extFb,
                    float* aovAccum, cudaStream_t st);
@@ -54,10 +54,16 @@ struct BvhBuildResult {
 int buildLbvh(const TriangleData* dTris, int triCount, int maxLeaf, int width, int builder, int radius, int wideCollapse,
               BvhBuildResult& out, cudaStream_t st, std::string& err);
 
+// The LBVH's Morton codes (per triangle, before sorting) and its stable sorted order, for host triangles.
+int lbvhMortonOrder(const TriangleData* hostTris, int n, unsigned long long* hostKeys, int* hostSorted,
+                    std::string& err);
+
 // Env-map tables (bte_env.cu).
 int buildEnvCdf(const float4* dTexels, int w, int h, const float* hSinTheta, float* dMarginal, float* dConditional,
                 cudaStream_t st, std::string& err);
 int buildEnvAlias(const float4* dTexels, int w, int h, float* dRowProb, int* dRowAlias, float* dColProb, int* dColAlias,
                   float* dPixelPdf, double* hTotal, cudaStream_t st, std::string& err);
+// Device address lookup of bte_env_build_alias_noalloc's scratch array on the current device.
+int prepareEnvNoallocScratch(std::string& err);
 
 }  // namespace bte

@@ -35,6 +35,24 @@
 #define BTE_HDN inline
 #endif
 
+// Product build (BTE_FAST_MATH, compiled with fused multiply-adds allowed): on
+// the device the public float functions are CUDA's own single-precision
+// functions -- the ones the reference's device code calls (sinf, cosf, tanf,
+// expf, logf, powf, atan2f, acosf) -- and x^5, x^2 are float products, so
+// shading runs in FP32 only.  The host keeps the portable functions below.
+// The parity build (no BTE_FAST_MATH) evaluates every function as documented
+// above on both sides.
+#if defined(BTE_FAST_MATH) && defined(__CUDA_ARCH__)
+#define BTE_FAST_DEVICE_MATH 1
+#else
+#define BTE_FAST_DEVICE_MATH 0
+#endif
+#ifdef BTE_FAST_MATH
+#define BTE_MATHFN BTE_HD
+#else
+#define BTE_MATHFN BTE_HDN
+#endif
+
 namespace bte {
 namespace m {
 
@@ -206,41 +224,61 @@ BTE_HD double atan2D(double y, double x)
 }
 
 // ---- float entry points ----
-BTE_HDN float sinf_(float x)
+BTE_MATHFN float sinf_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::sinf(x);
+#else
     if (x == 0.0f || isnanf_(x)) return x + x * 0.0f;
     if (isinff_(x)) return NAN;
     return static_cast<float>(sinD(static_cast<double>(x)));
+#endif
 }
-BTE_HDN float cosf_(float x)
+BTE_MATHFN float cosf_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::cosf(x);
+#else
     if (isnanf_(x)) return x;
     if (isinff_(x)) return NAN;
     return static_cast<float>(cosD(static_cast<double>(x)));
+#endif
 }
-BTE_HDN float tanf_(float x)
+BTE_MATHFN float tanf_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::tanf(x);
+#else
     if (x == 0.0f || isnanf_(x)) return x + x * 0.0f;
     if (isinff_(x)) return NAN;
     int q;
     const double r = reducePio2(static_cast<double>(x), q);
     const double s = sinPoly(r), c = cosPoly(r);
     return static_cast<float>((q & 1) ? (-c / s) : (s / c));
+#endif
 }
-BTE_HDN float expf_(float x)
+BTE_MATHFN float expf_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::expf(x);
+#else
     if (isnanf_(x)) return x;
     if (x > 89.0f) return INFINITY;
     if (x < -104.0f) return 0.0f;
     return static_cast<float>(expD(static_cast<double>(x)));
+#endif
 }
-BTE_HDN float logf_(float x)
+BTE_MATHFN float logf_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::logf(x);
+#else
     if (isnanf_(x)) return x;
     if (x < 0.0f) return NAN;
     if (x == 0.0f) return -INFINITY;
     if (isinff_(x)) return x;
     return static_cast<float>(logD(static_cast<double>(x)));
+#endif
 }
 BTE_HD bool isIntF(float y) { return floorf(y) == y; }
 BTE_HD bool isOddIntF(float y)
@@ -248,8 +286,11 @@ BTE_HD bool isOddIntF(float y)
     if (!isIntF(y) || fabsf(y) >= 16777216.0f) return false;
     return (static_cast<int64_t>(y) & 1) != 0;
 }
-BTE_HDN float powf_(float x, float y)
+BTE_MATHFN float powf_(float x, float y)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::powf(x, y);
+#else
     if (y == 0.0f) return 1.0f;
     if (x == 1.0f) return 1.0f;
     if (isnanf_(x) || isnanf_(y)) return NAN;
@@ -281,28 +322,41 @@ BTE_HDN float powf_(float x, float y)
     if (l > 89.0) return sign * INFINITY;
     if (l < -104.0) return sign * 0.0f;
     return sign * static_cast<float>(expD(l));
+#endif
 }
 // x^5 and x^2 for the reference's powf(x, 5) / powf(x, 2) call sites: the
 // double products (x*x exact, then two rounded products) carry relative error
 // < 3e-16, so the single rounding to float gives the correctly rounded power
 // except in vanishingly rare near-halfway cases; special values follow C99
 // pow for odd/even integer exponents.
-BTE_HD float pow5f_(float x)
+BTE_MATHFN float pow5f_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    const float x2 = x * x;
+    return x2 * x2 * x;
+#else
     const double d = static_cast<double>(x);
     const double d2 = d * d;
     const double d4 = d2 * d2;
     return static_cast<float>(d4 * d);
+#endif
 }
-BTE_HD float pow2f_(float x)
+BTE_MATHFN float pow2f_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return x * x;
+#else
     const double d = static_cast<double>(x);
     return static_cast<float>(d * d);
+#endif
 }
 // sin and cos of one argument with a single reduction; bit-identical to
 // sinf_(x) and cosf_(x).
-BTE_HDN void sincosf_(float x, float& s, float& c)
+BTE_MATHFN void sincosf_(float x, float& s, float& c)
 {
+#if BTE_FAST_DEVICE_MATH
+    ::sincosf(x, &s, &c);
+#else
     if (isnanf_(x)) { s = x + x * 0.0f; c = x; return; }
     if (isinff_(x)) { s = NAN; c = NAN; return; }
     if (x == 0.0f) { s = x + x * 0.0f; c = static_cast<float>(cosD(static_cast<double>(x))); return; }
@@ -315,9 +369,13 @@ BTE_HDN void sincosf_(float x, float& s, float& c)
     case 2: s = static_cast<float>(-sp); c = static_cast<float>(-cp); break;
     default: s = static_cast<float>(-cp); c = static_cast<float>(sp); break;
     }
+#endif
 }
-BTE_HDN float atan2f_(float y, float x)
+BTE_MATHFN float atan2f_(float y, float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::atan2f(y, x);
+#else
     if (isnanf_(x) || isnanf_(y)) return NAN;
     if (y == 0.0f) {
         if (x > 0.0f || (x == 0.0f && !signbitf_(x))) return y;
@@ -332,9 +390,13 @@ BTE_HDN float atan2f_(float y, float x)
     }
     if (x == 0.0f) return (y > 0.0f) ? static_cast<float>(kPio2_1) : -static_cast<float>(kPio2_1);
     return static_cast<float>(atan2D(static_cast<double>(y), static_cast<double>(x)));
+#endif
 }
-BTE_HDN float acosf_(float x)
+BTE_MATHFN float acosf_(float x)
 {
+#if BTE_FAST_DEVICE_MATH
+    return ::acosf(x);
+#else
     if (isnanf_(x)) return x;
     if (x > 1.0f || x < -1.0f) return NAN;
     if (x == 1.0f) return 0.0f;
@@ -342,6 +404,7 @@ BTE_HDN float acosf_(float x)
     const double s = sqrt((1.0 - xd) * (1.0 + xd));
     if (xd == 0.0) return static_cast<float>(kPio2_1);
     return static_cast<float>(atan2D(s, xd));
+#endif
 }
 
 }  // namespace m

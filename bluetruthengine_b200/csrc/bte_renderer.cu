@@ -7,6 +7,7 @@
 // an LBVH instead of the OptiX GAS, and a frame that is a fixed,
 // host-synchronisation-free launch sequence.  Every entry point returns a
 // status and records a message for bte_last_error() instead of exiting.
+#include "../../include/bte/launch_params.h"
 #include "bte_denoise.h"
 #include "bte_internal.h"
 #include "bte_kernels.h"
@@ -200,6 +201,8 @@ void ensureInit()
     for (auto& e : g.stageEv) ck(cudaEventCreate(&e), "cudaEventCreate");
     ck(cudaHostAlloc(reinterpret_cast<void**>(&g.hFrameIndex), sizeof(uint32_t), cudaHostAllocDefault), "cudaHostAlloc");
     ensure(g.dFrameIndex, sizeof(uint32_t));
+    std::string err;
+    if (prepareEnvNoallocScratch(err) != 0) throw CudaError{err};
     g.init = true;
 }
 
@@ -428,8 +431,8 @@ void renderFrame(int w, int h)
     P.shContrib = g.shContrib.as<float4>();
     P.shMask = g.shMask.as<uint32_t>();
     P.hitLog = g.hitLogEnabled && !mega ? g.hitLog.as<int>() : nullptr;
-    P.aovAlbedo = g.aovEnabled && !mega ? g.aovAlbedo.as<float4>() : nullptr;
-    P.aovNormal = g.aovEnabled && !mega ? g.aovNormal.as<float4>() : nullptr;
+    P.aovAlbedo = g.aovEnabled ? g.aovAlbedo.as<float4>() : nullptr;
+    P.aovNormal = g.aovEnabled ? g.aovNormal.as<float4>() : nullptr;
     P.slots = slots;
     P.maxDepth = depth;
     P.count = paths;
@@ -462,7 +465,7 @@ void renderFrame(int w, int h)
     };
     auto frameLaunches = [&] {
         if (mega) {
-            launchMegakernel(s, P, f, accumF, accumDv, fb, g.extFramebuffer, st);
+            launchMegakernel(s, P, f, accumF, accumDv, fb, g.extFramebuffer, aovAcc, st);
             return;
         }
         launchGenerate(P, f, st);
@@ -1265,6 +1268,64 @@ int bte_toggle_denoiser(void)
     });
 }
 
+// include/optix_launch_params.h:34-86: the reference fills this block before every launch
+// (render_kernel.cu:58-143, wavefront_host.cu:122-148); here it is filled on request from the current state.
+int bte_get_launch_params(LaunchParams* out)
+{
+    return guarded([&] {
+        if (!out) throw CudaError{"bte_get_launch_params: null pointer"};
+        LaunchParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.framebuffer = g.framebuffer.as<uint32_t>();
+        p.accumBuffer = g.accum.as<Float3>();
+        p.width = g.accumW;
+        p.height = g.accumH;
+        p.launchOffsetY = 0;
+        p.frameIndex = g.frameIndex;
+        p.camera = g.camera;
+        const void* tree = g.builtWidth == 8 ? g.wideNodes.p : g.bvhNodes.p;
+        p.handle = g.accelReady ? static_cast<uint64_t>(reinterpret_cast<uintptr_t>(tree)) : 0u;
+        p.triangles = g.tris.as<TriangleData>();
+        p.triangleCount = g.triCount;
+        p.bsdfs = g.bsdfs.as<BsdfData>();
+        p.bsdfCount = g.bsdfCount;
+        p.triangleBsdfIds = g.triBsdfIds.as<int>();
+        p.triangleMaterialIds = g.triMatIds.as<int>();
+        p.triangleEmitterFlags = g.emitterFlags.as<uint8_t>();
+        p.triangleEmission = g.emission.as<Float3>();
+        p.emitters = g.emitters.as<EmitterData>();
+        p.emitterCount = g.emitterCount;
+        p.emitterTriIndices = g.emitterTriIndices.as<int>();
+        p.emitterTriCdf = g.emitterTriCdf.as<float>();
+        p.sceneEmitterCdf = g.sceneEmitterCdf.as<float>();
+        p.spotlights = g.spots.as<SpotlightData>();
+        p.spotlightCount = g.spotCount;
+        p.texObjects = nullptr;
+        p.texObjectsMr = nullptr;
+        p.textureCount = g.textureCount;
+        if (g.hasEnv) {
+            p.envMap.texObj = 0;
+            p.envMap.width = g.envW;
+            p.envMap.height = g.envH;
+            p.envMap.intensity = g.envIntensity;
+            p.envMap.rotationRadians = g.envRotation;
+            p.envMap.marginalCdf = g.envMarginal.as<float>();
+            p.envMap.conditionalCdf = g.envConditional.as<float>();
+            p.envMap.totalPower = g.envTotalPowerF;
+        }
+        p.hasEnvMap = g.hasEnv;
+        p.wf.rayQueue = g.q0.as<int>();
+        p.wf.rayQueueNext = g.q1.as<int>();
+        p.wf.rayCount = g.rayCount.as<int>();
+        p.wf.rayCountNext = g.rayCount.p ? g.rayCount.as<int>() + 1 : nullptr;
+        p.wf.shadowCount = g.shadowCount.as<int>();
+        p.wf.maxPaths = g.lastPaths;
+        p.wf.maxShadows = g.lastPaths * g.lastSlots;
+        *out = p;
+        return 0;
+    });
+}
+
 int bte_read_denoised(float* hostRGB)
 {
     return guarded([&] {
@@ -1544,6 +1605,18 @@ int bte_trace_occluded_lanes(const float* rays, const float* tmax, int n, int la
         ck(cudaStreamSynchronize(g.stream), "trace");
         ck(cudaMemcpyAsync(outOccluded, dout.p, n, cudaMemcpyDeviceToHost, g.stream), "cudaMemcpyAsync"); ck(cudaStreamSynchronize(g.stream), "sync");
         checkTraceFlags(de.p);
+        return 0;
+    });
+}
+
+int bte_debug_lbvh_order(const TriangleData* triangles, int n, uint64_t* mortonKeys, int* sortedOrder)
+{
+    return guarded([&] {
+        if (!triangles || !mortonKeys || !sortedOrder || n <= 0) throw CudaError{"bte_debug_lbvh_order: bad arguments"};
+        ensureInit();
+        std::string err;
+        if (lbvhMortonOrder(triangles, n, reinterpret_cast<unsigned long long*>(mortonKeys), sortedOrder, err) != 0)
+            throw CudaError{err};
         return 0;
     });
 }

@@ -64,7 +64,15 @@ BTE_DI RayPre rayPre(float ox, float oy, float oz, float dx, float dy, float dz,
     return r;
 }
 
-// Watertight test; returns true with t in [tmin, tmax].
+// Watertight test; returns true with t in [tmin, tmax].  Every product and difference is an explicitly rounded
+// operation (__fmul_rn / __fsub_rn / __fadd_rn, and __dmul_rn / __dsub_rn in the double fallback), so no build
+// contracts them into fused multiply-adds: hits are identical whether or not the library allows contraction.
+BTE_DI float mulSub(float a, float b, float c, float d) { return __fsub_rn(__fmul_rn(a, b), __fmul_rn(c, d)); }
+BTE_DI float mulSubD(float a, float b, float c, float d)
+{
+    return static_cast<float>(__dsub_rn(__dmul_rn(static_cast<double>(a), static_cast<double>(b)),
+                                        __dmul_rn(static_cast<double>(c), static_cast<double>(d))));
+}
 BTE_DI bool isectTri(const RayPre& r, float4 a, float4 b, float4 c, float tmin, float tmax, float& ot, float& ou,
                      float& ov)
 {
@@ -72,30 +80,30 @@ BTE_DI bool isectTri(const RayPre& r, float4 a, float4 b, float4 c, float tmin, 
     const float Bx0 = b.x - r.ox, By0 = b.y - r.oy, Bz0 = b.z - r.oz;
     const float Cx0 = c.x - r.ox, Cy0 = c.y - r.oy, Cz0 = c.z - r.oz;
     const float Akz = comp3(Ax0, Ay0, Az0, r.kz), Bkz = comp3(Bx0, By0, Bz0, r.kz), Ckz = comp3(Cx0, Cy0, Cz0, r.kz);
-    const float Ax = comp3(Ax0, Ay0, Az0, r.kx) - r.Sx * Akz;
-    const float Ay = comp3(Ax0, Ay0, Az0, r.ky) - r.Sy * Akz;
-    const float Bx = comp3(Bx0, By0, Bz0, r.kx) - r.Sx * Bkz;
-    const float By = comp3(Bx0, By0, Bz0, r.ky) - r.Sy * Bkz;
-    const float Cx = comp3(Cx0, Cy0, Cz0, r.kx) - r.Sx * Ckz;
-    const float Cy = comp3(Cx0, Cy0, Cz0, r.ky) - r.Sy * Ckz;
-    float U = Cx * By - Cy * Bx;
-    float V = Ax * Cy - Ay * Cx;
-    float W = Bx * Ay - By * Ax;
+    const float Ax = __fsub_rn(comp3(Ax0, Ay0, Az0, r.kx), __fmul_rn(r.Sx, Akz));
+    const float Ay = __fsub_rn(comp3(Ax0, Ay0, Az0, r.ky), __fmul_rn(r.Sy, Akz));
+    const float Bx = __fsub_rn(comp3(Bx0, By0, Bz0, r.kx), __fmul_rn(r.Sx, Bkz));
+    const float By = __fsub_rn(comp3(Bx0, By0, Bz0, r.ky), __fmul_rn(r.Sy, Bkz));
+    const float Cx = __fsub_rn(comp3(Cx0, Cy0, Cz0, r.kx), __fmul_rn(r.Sx, Ckz));
+    const float Cy = __fsub_rn(comp3(Cx0, Cy0, Cz0, r.ky), __fmul_rn(r.Sy, Ckz));
+    float U = mulSub(Cx, By, Cy, Bx);
+    float V = mulSub(Ax, Cy, Ay, Cx);
+    float W = mulSub(Bx, Ay, By, Ax);
     if (U == 0.0f || V == 0.0f || W == 0.0f) {
-        U = static_cast<float>(static_cast<double>(Cx) * static_cast<double>(By) - static_cast<double>(Cy) * static_cast<double>(Bx));
-        V = static_cast<float>(static_cast<double>(Ax) * static_cast<double>(Cy) - static_cast<double>(Ay) * static_cast<double>(Cx));
-        W = static_cast<float>(static_cast<double>(Bx) * static_cast<double>(Ay) - static_cast<double>(By) * static_cast<double>(Ax));
+        U = mulSubD(Cx, By, Cy, Bx);
+        V = mulSubD(Ax, Cy, Ay, Cx);
+        W = mulSubD(Bx, Ay, By, Ax);
     }
     if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
-    const float det = U + V + W;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
     if (det == 0.0f) return false;
-    const float Az = r.Sz * Akz, Bz = r.Sz * Bkz, Cz = r.Sz * Ckz;
-    const float T = U * Az + V * Bz + W * Cz;
-    const float t = T / det;
+    const float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+    const float t = __fdiv_rn(T, det);
     if (!(t >= tmin && t <= tmax)) return false;
     ot = t;
-    ou = V / det;
-    ov = W / det;
+    ou = __fdiv_rn(V, det);
+    ov = __fdiv_rn(W, det);
     return true;
 }
 

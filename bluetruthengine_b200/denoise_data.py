@@ -4,8 +4,9 @@
   albedo/normal features, and an independent long-run target (FP64 running sum / samples, from a
   disjoint range of sample indices).
 * `reference`: an FP64-accumulated high-spp image of a view.
-* `time_to_rel_mse`: device time plain accumulation needs to reach a relMSE bound against a reference,
-  and device time (render + denoise) the denoised low-spp form needs for the same bound.
+* `time_to_rel_mse`: wall time (host clock around the renderer calls and the readback, with the device
+  time beside it) that plain accumulation needs to reach a relMSE bound against a reference, and the
+  same for the denoised low-spp form (render + the renderer's denoise + readback).
 """
 from __future__ import annotations
 
@@ -79,38 +80,126 @@ def make_dataset(r, scene_paths, spp_in_choices=(2, 4, 8, 16, 32), spp_target=20
     return out
 
 
-def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, plain_spf=16, plain_max_spp=1 << 16,
-                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256)):
-    """Device time for plain accumulation and for denoised low-spp to reach relMSE <= bound."""
-    W, H = scene.width, scene.height
-    r.cleanup()
-    r.upload(scene)
-    # plain accumulation (progressive, the running FP32 mean the renderer keeps)
+def _sync():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+    except ImportError:
+        pass
+
+
+def plain_crossing(r, W, H, ref, bound, depth, step=4, max_spp=1 << 16, env=ENV_ALIAS):
+    """Smallest multiple of `step` samples at which progressive plain accumulation (the FP32 running mean
+    the renderer keeps, samples 0, 1, 2, ... of every pixel) reaches relMSE <= bound against `ref`.
+
+    The image is rendered `step` samples per frame.  relMSE is evaluated (outside any timing) on a schedule
+    that follows the 1/spp convergence of the error: after each evaluation the next one is placed half way
+    to the predicted crossing, and once that is within two steps, after every frame.  Returns
+    (spp or None, [(spp, relMSE), ...])."""
     r.reset_accumulation(W, H)
-    t_plain, spp, curve = 0.0, 0, []
-    plain = None
-    while spp < plain_max_spp:
-        r.set_config(samples_per_frame=plain_spf, max_depth=depth, rr_start=3, env_sampling=ENV_ALIAS, use_graph=1)
+    r.set_frame_index(0)
+    r.set_config(samples_per_frame=step, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
+    spp, nxt, curve = 0, step, []
+    while spp < max_spp:
         r.render(W, H)
-        t_plain += r.stats().msTotal
-        spp += plain_spf
+        spp += step
+        if spp < nxt:
+            continue
         e = rel_mse(r.read_accum(W, H).reshape(H, W, 3), ref)
-        curve.append((spp, t_plain, e))
+        curve.append((spp, e))
         if e <= bound:
-            plain = {"spp": spp, "ms": t_plain, "rel_mse": e}
-            break
-    # denoised: fresh low-spp renders of growing size
-    den = None
-    rows = []
-    for n in denoise_spps:
-        noisy, feat, ms_r = render_input(r, W, H, n, depth)
-        out = dn.denoise(noisy, feat)
-        ms_d = dn.last_ms()
-        e = rel_mse(out, ref)
-        e_noisy = rel_mse(noisy, ref)
-        rows.append({"spp": n, "ms_render": ms_r, "ms_denoise": ms_d, "rel_mse": e, "rel_mse_input": e_noisy})
-        if den is None and e <= bound:
-            den = {"spp": n, "ms": ms_r + ms_d, "ms_render": ms_r, "ms_denoise": ms_d, "rel_mse": e}
-            break
-    return {"bound": bound, "plain": plain, "denoised": den, "denoised_sweep": rows,
-            "plain_curve": curve[:: max(1, len(curve) // 24)]}
+            return spp, curve
+        predicted = spp * e / bound
+        gap = max(step, int((predicted - spp) * 0.5) // step * step)
+        nxt = spp + (step if predicted - spp <= 2 * step else gap)
+    return None, curve
+
+
+def plain_wall(r, W, H, spp, depth, spf=16, env=ENV_ALIAS):
+    """Host wall time (and summed device time) of plain accumulation to `spp` samples: reset, frames of
+    `spf` samples, then the FP32 mean read back to the host.  Returns (wall s, device ms, image)."""
+    r.set_config(samples_per_frame=min(spf, spp), max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
+    _sync()
+    t0 = time.perf_counter()
+    r.reset_accumulation(W, H)
+    r.set_frame_index(0)
+    done, ms = 0, 0.0
+    while done < spp:
+        k = min(spf, spp - done)
+        if k != min(spf, spp):
+            r.set_config(samples_per_frame=k, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
+        r.render(W, H)
+        ms += r.stats().msTotal
+        done += k
+    img = r.read_accum(W, H).reshape(H, W, 3)
+    return time.perf_counter() - t0, ms, img
+
+
+def denoised_wall(r, dn, W, H, spp, depth, env=ENV_ALIAS, max_spf=64):
+    """Host wall time of the denoised low-spp form through the renderer API: with the denoiser toggled on,
+    reset, frames of up to `max_spf` samples per pixel (one frame up to that size; the renderer denoises
+    its running mean with the first-hit albedo/normal features after every frame), and the denoised image
+    read back.  Returns (wall s, render ms, denoise ms, denoised image, noisy mean)."""
+    spf = min(spp, max_spf)
+    r.set_config(samples_per_frame=spf, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
+    _sync()
+    t0 = time.perf_counter()
+    r.reset_accumulation(W, H)
+    r.set_frame_index(0)
+    done, ms_render, ms_denoise = 0, 0.0, 0.0
+    while done < spp:
+        k = min(spf, spp - done)
+        if k != spf:
+            r.set_config(samples_per_frame=k, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
+        r.render(W, H)
+        ms_render += r.stats().msTotal
+        ms_denoise += dn.last_ms()
+        done += k
+    out = r.read_denoised(W, H)
+    wall = time.perf_counter() - t0
+    noisy = r.read_accum(W, H).reshape(H, W, 3)
+    return wall, ms_render, ms_denoise, out, noisy
+
+
+def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16, plain_max_spp=1 << 16,
+                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256)):
+    """Wall time (and device time) plain accumulation and the denoised low-spp form need to reach
+    relMSE <= bound against `ref`, on the uploaded scene's view.  The denoiser weights must be loaded.
+
+    plain: the crossing spp from `plain_crossing`, then that many samples rendered again and timed twice
+    (the first run captures the frame graphs; the second is reported as warm).
+    denoised: for growing spp, one frame plus the renderer's denoise and readback; each size is timed on
+    its first call (graph capture and buffers of a new size included) and again warm.  The first size
+    reaching the bound is the result."""
+    W, H = scene.width, scene.height
+    n_cross, curve = plain_crossing(r, W, H, ref, bound, depth, step=step, max_spp=plain_max_spp)
+    plain = None
+    if n_cross is not None:
+        cold = plain_wall(r, W, H, n_cross, depth, spf=plain_spf)
+        warm = plain_wall(r, W, H, n_cross, depth, spf=plain_spf)
+        plain = {"spp": n_cross, "wall_ms": warm[0] * 1e3, "wall_ms_first_run": cold[0] * 1e3,
+                 "device_ms": warm[1], "rel_mse": rel_mse(warm[2], ref)}
+    was_on = r.toggle_denoiser()
+    if not was_on:
+        raise RuntimeError("denoiser did not turn on")
+    rows, den = [], None
+    try:
+        for n in denoise_spps:
+            cold = denoised_wall(r, dn, W, H, n, depth)
+            warm = denoised_wall(r, dn, W, H, n, depth)
+            row = {"spp": n, "wall_ms": warm[0] * 1e3, "wall_ms_first_call": cold[0] * 1e3,
+                   "device_ms_render": warm[1], "device_ms_denoise": warm[2],
+                   "rel_mse": rel_mse(warm[3], ref), "rel_mse_input": rel_mse(warm[4], ref)}
+            rows.append(row)
+            if row["rel_mse"] <= bound:
+                den = dict(row)
+                break
+    finally:
+        r.toggle_denoiser()
+    res = {"bound": bound, "plain": plain, "denoised": den, "denoised_sweep": rows, "plain_curve": curve}
+    if plain and den:
+        res["speedup_wall"] = plain["wall_ms"] / den["wall_ms_first_call"]
+        res["speedup_wall_warm"] = plain["wall_ms"] / den["wall_ms"]
+        res["speedup_device"] = plain["device_ms"] / (den["device_ms_render"] + den["device_ms_denoise"])
+    return res

@@ -26,25 +26,31 @@ def _f32(a) -> np.ndarray:
 
 
 class Denoiser:
-    def __init__(self):
-        self.lib = load_library()
+    """The learned denoiser of one build of the library (default: the process default, see load_library);
+    the renderer of the same build presents its output when toggled on."""
+
+    def __init__(self, variant: str | None = None):
+        self.lib = load_library(variant=variant)
+
+    def _ck(self, rc: int) -> int:
+        return _check(rc, self.lib)
 
     def init(self, seed: int = 1):
-        _check(self.lib.bte_denoiser_init(C.c_uint64(seed)))
+        self._ck(self.lib.bte_denoiser_init(C.c_uint64(seed)))
 
     def param_count(self) -> int:
         n = C.c_longlong()
-        _check(self.lib.bte_denoiser_param_count(C.byref(n)))
+        self._ck(self.lib.bte_denoiser_param_count(C.byref(n)))
         return n.value
 
     def params(self) -> np.ndarray:
         out = np.empty(self.param_count(), dtype=np.float32)
-        _check(self.lib.bte_denoiser_get_params(out.ctypes.data_as(C.c_void_p), C.c_longlong(out.size)))
+        self._ck(self.lib.bte_denoiser_get_params(out.ctypes.data_as(C.c_void_p), C.c_longlong(out.size)))
         return out
 
     def set_params(self, p: np.ndarray):
         p = _f32(p)
-        _check(self.lib.bte_denoiser_set_params(p.ctypes.data_as(C.c_void_p), C.c_longlong(p.size)))
+        self._ck(self.lib.bte_denoiser_set_params(p.ctypes.data_as(C.c_void_p), C.c_longlong(p.size)))
 
     def save(self, path: str):
         np.savez_compressed(path, params=self.params().astype(np.float16))
@@ -60,12 +66,12 @@ class Denoiser:
         S, H, W, _ = noisy.shape
         assert features.shape == (S, H, W, 6) and target.shape == (S, H, W, 3)
         self._keep = (noisy, features, target)
-        _check(self.lib.bte_denoiser_set_dataset(noisy.ctypes.data_as(C.c_void_p), features.ctypes.data_as(C.c_void_p),
+        self._ck(self.lib.bte_denoiser_set_dataset(noisy.ctypes.data_as(C.c_void_p), features.ctypes.data_as(C.c_void_p),
                                                  target.ctypes.data_as(C.c_void_p), S, W, H))
 
     def train(self, steps: int, batch: int = 8, crop: int = 128, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
         loss = np.empty(steps, dtype=np.float32)
-        _check(self.lib.bte_denoiser_train(int(steps), int(batch), int(crop), C.c_float(lr), C.c_uint64(seed),
+        self._ck(self.lib.bte_denoiser_train(int(steps), int(batch), int(crop), C.c_float(lr), C.c_uint64(seed),
                                            loss.ctypes.data_as(C.c_void_p)))
         return loss
 
@@ -78,7 +84,7 @@ class Denoiser:
             features = _f32(features)
             assert features.shape == (H, W, 6)
             fp = features.ctypes.data_as(C.c_void_p)
-        _check(self.lib.bte_denoiser_denoise(radiance.ctypes.data_as(C.c_void_p), fp, W, H, out.ctypes.data_as(C.c_void_p)))
+        self._ck(self.lib.bte_denoiser_denoise(radiance.ctypes.data_as(C.c_void_p), fp, W, H, out.ctypes.data_as(C.c_void_p)))
         return out
 
     def set_tcgen05(self, mode):
@@ -86,11 +92,11 @@ class Denoiser:
         kernel for the full-resolution layers, 2 (the default) the tcgen05 row-tile kernel for every layer with
         enough 128-pixel row tiles (layers it does not take stay on the warp-level kernel), decoder inputs
         upsampled beforehand; 3 the same with the upsampling done inside the row-tile kernel."""
-        _check(self.lib.bte_denoiser_set_tcgen05(int(mode)))
+        self._ck(self.lib.bte_denoiser_set_tcgen05(int(mode)))
 
     def last_ms(self) -> float:
         ms = C.c_float()
-        _check(self.lib.bte_denoiser_last_ms(C.byref(ms)))
+        self._ck(self.lib.bte_denoiser_last_ms(C.byref(ms)))
         return ms.value
 
     def debug_conv(self, op: int, x=None, w=None, bias=None, dy=None, shape=(1, 16, 16, 16, 16), relu=True):
@@ -106,7 +112,7 @@ class Denoiser:
         else:
             out = np.empty(9 * cout * cin + cout, dtype=np.float32)
         ptrs = [None if a is None else a.ctypes.data_as(C.c_void_p) for a in keep]
-        _check(self.lib.bte_denoiser_debug_conv(op, ptrs[0], ptrs[1], ptrs[2], ptrs[3], n, h, wd, cin, cout,
+        self._ck(self.lib.bte_denoiser_debug_conv(op, ptrs[0], ptrs[1], ptrs[2], ptrs[3], n, h, wd, cin, cout,
                                                 1 if relu else 0, out.ctypes.data_as(C.c_void_p)))
         return out
 

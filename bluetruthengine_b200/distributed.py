@@ -19,7 +19,10 @@ def sample_base(rank: int, frames: int, samples_per_frame: int) -> int:
 
 def merge_accumulators(sum_f64, samples_this_rank: int, group=None):
     """All-reduce the per-pixel FP64 sums and sample counts; returns the mean image
-    (float64) identical on every rank.  `sum_f64` is a torch tensor or numpy array."""
+    (float64) identical on every rank.  `sum_f64` is a torch tensor or numpy array.
+
+    Wavefront mode: `samples_this_rank` is the rank's samples per pixel.  In megakernel mode the
+    accumulator is a sum of per-frame means, so pass the rank's frame count instead."""
     import torch
     import torch.distributed as dist
     t = sum_f64 if isinstance(sum_f64, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(sum_f64))

@@ -36,7 +36,10 @@ typedef struct { Float3 position, direction, radiance; float intensity, innerCon
 typedef struct { int type; Float4 p0, p1, p2, p3; } BsdfData;                                      /* 68 B */
 enum { BSDF_Diffuse = 1, BSDF_Dielectric = 2, BSDF_Mirror = 3, BSDF_Microfacet = 4, BSDF_Disney = 5 };
 
-/* render_kernel.h:199-202 (only Wavefront is implemented; Megakernel is accepted and runs the wavefront path) */
+/* render_kernel.h:199-202.  Wavefront: the staged path tracer.  Megakernel: the reference's megakernel
+ * (src/optix_programs.cu:54-108): one thread and one RNG stream per pixel through 5 paths, one Welford update
+ * per frame; bte_read_accum_f64 then holds a sum of per-frame means (divide by the frame count, which
+ * bte_get_frame_index reports in this mode). */
 enum { BTE_RENDER_MEGAKERNEL = 0, BTE_RENDER_WAVEFRONT = 1 };
 
 /* env-map importance sampling: the reference's marginal/conditional CDF
@@ -187,6 +190,11 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
                             int w_, int cin, int cout, int relu, float* out);
 
 /* ---- debug/parity entry points over device-resident state ---- */
+/* The LBVH's integer steps for n host triangles (the acceleration-structure build replacing
+ * src/host/optix_setup.cu:215-292): the 63-bit Morton code of each triangle's centroid (21 bits per axis
+ * over the centroid bounds, x in the highest interleaved bit) and the triangle order after the stable
+ * radix sort by code (ties in ascending index). */
+int bte_debug_lbvh_order(const TriangleData* triangles, int n, uint64_t* mortonKeys, int* sortedOrder);
 /* closest hit for n rays [origin, dir] (host arrays): triangle index (-1 miss) and t, u, v */
 int bte_trace_closest(const float* rays, int n, int* outTri, float* outTuv);
 int bte_trace_occluded(const float* rays, const float* tmax, int n, uint8_t* outOccluded);
@@ -216,9 +224,13 @@ int bte_tex_hw_vs_sw(const float* texels, int w, int h, int wrapV, const float* 
  * weight [1].  Work is queued on `stream` (0 = default stream) and nothing is
  * allocated: the intermediates live in one fixed device array, so maps are
  * limited to 131072 texels (e.g. 512x256) and 4096 rows; larger sizes return
- * an error.  The first call on a device looks up that array's address (make it
- * before any stream capture).  All calls share the array: calls whose kernels
- * overlap on the GPU race and must be serialised by the caller. */
+ * an error.  The array's device address is looked up once per device, by the
+ * renderer's device set-up (any renderer call) or else by the first call here;
+ * under lazy module loading that is also when the array's memory is taken, so
+ * make one of those calls before reserving the rest of device memory, and the
+ * first call here before any stream capture.  dTotalPower must be 8-byte
+ * aligned.  All calls share the array: calls whose kernels overlap on the GPU
+ * race and must be serialised by the caller. */
 int bte_env_build_alias_noalloc(const float* dTexelsRGBA, int width, int height, float* dRowProb, int* dRowAlias,
                                 float* dColProb, int* dColAlias, float* dPixelPdf, double* dTotalPower, void* stream);
 

@@ -24,6 +24,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 
+# The reference source tree the checker compiles from (read-only); override with BTE_REFERENCE_ROOT.
+REFERENCE_ROOT = os.environ.get("BTE_REFERENCE_ROOT", "/root/reference")
+
+
+def reference_present() -> bool:
+    return os.path.isdir(os.path.join(REFERENCE_ROOT, "include"))
+
+
 def build(ref: bool = True) -> None:
     """Build the oracle libraries (and the reference harness when the reference tree is present)."""
     targets = ["liboracle.so", "liboracle_libm.so"]
@@ -31,8 +39,8 @@ def build(ref: bool = True) -> None:
     env.pop("CC", None)
     env.pop("CXX", None)
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
-    if ref and os.path.isdir("/root/reference/include"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True, env=env)
+    if ref and reference_present():
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + REFERENCE_ROOT], check=True, env=env)
 
 
 class OCamera(C.Structure):
@@ -318,4 +326,92 @@ class Ref:
     @staticmethod
     def available(fast: bool = False) -> bool:
         return os.path.exists(os.path.join(REF_DIR, "libbteref_fast.so" if fast else "libbteref.so")) or \
-            os.path.isdir("/root/reference/include")
+            reference_present()
+
+
+# POD layouts of the reference's include/render_kernel.h:9-94 (the arrays the loader hands to the cudaInit* calls)
+_F3 = ("<f4", 3)
+REF_TRIANGLE_DTYPE = np.dtype([("v0",) + _F3, ("v1",) + _F3, ("v2",) + _F3, ("n0",) + _F3, ("n1",) + _F3,
+                               ("n2",) + _F3, ("uv0", "<f4", 2), ("uv1", "<f4", 2), ("uv2", "<f4", 2)])
+REF_BSDF_DTYPE = np.dtype([("type", "<i4"), ("p0", "<f4", 4), ("p1", "<f4", 4), ("p2", "<f4", 4), ("p3", "<f4", 4)])
+REF_EMITTER_DTYPE = np.dtype([("triIndexOffset", "<i4"), ("triCount", "<i4"), ("cdfOffset", "<i4"),
+                              ("radiance",) + _F3, ("areaSum", "<f4"), ("powerWeight", "<f4")])
+REF_SPOT_DTYPE = np.dtype([("position",) + _F3, ("direction",) + _F3, ("radiance",) + _F3, ("intensity", "<f4"),
+                           ("innerConeCosine", "<f4"), ("outerConeCosine", "<f4")])
+REF_CAMERA_DTYPE = np.dtype([("origin",) + _F3, ("forward",) + _F3, ("right",) + _F3, ("up",) + _F3,
+                             ("fovYRadians", "<f4"), ("aspect", "<f4")])
+
+
+class RefScene:
+    """A scene flattened by the reference's own loader (src/scene.cpp, tinyobjloader, mesh_transform.h,
+    gltf_loader.cpp and stb_image compiled from the reference tree: oracle/_ref/libbteref_loader.so) with the
+    glue of src/main.cpp:533-930.  Carries the attributes SceneView reads; no product library is involved."""
+
+    def __init__(self, path: str):
+        lib_path = os.path.join(REF_DIR, "libbteref_loader.so")
+        if not os.path.exists(lib_path):
+            build(ref=True)
+        lib = C.CDLL(lib_path)
+        if lib.refl_load(str(path).encode()) < 0:
+            raise RuntimeError("reference loader failed on %s" % path)
+        cnt = np.zeros(6, np.int32)
+        lib.refl_counts(_p(cnt))
+        T, B, E, EC, SC, NC = (int(x) for x in cnt)
+        self.triangles = np.empty(T, REF_TRIANGLE_DTYPE)
+        self.bsdfs = np.empty(B, REF_BSDF_DTYPE)
+        self.triangle_bsdf_ids, self.triangle_material_ids = np.empty(T, np.int32), np.empty(T, np.int32)
+        self.triangle_emitter_flags = np.empty(T, np.uint8)
+        self.emitter_tri_indices = np.empty(E, np.int32)
+        self.emitter_tri_cdf = np.empty(EC, np.float32)
+        self.scene_emitter_cdf = np.empty(SC, np.float32)
+        cam = np.empty(NC, np.float32)
+        lib.refl_copy(_p(self.triangles), _p(self.bsdfs), _p(self.triangle_bsdf_ids), _p(self.triangle_material_ids),
+                      _p(self.triangle_emitter_flags), _p(self.emitter_tri_indices), _p(self.emitter_tri_cdf),
+                      _p(self.scene_emitter_cdf), _p(cam))
+        ex = np.zeros(5, np.int32)
+        lib.refl_extras_counts(_p(ex))
+        NE, NT, NS, EW, EH = (int(x) for x in ex)
+        self.emitters = np.zeros(NE, REF_EMITTER_DTYPE)
+        self.triangle_emission = np.zeros((NT, 3), np.float32)
+        self.spotlights = np.zeros(NS, REF_SPOT_DTYPE)
+        env = np.zeros((EH, EW, 4), np.float32) if EW > 0 else np.zeros(4, np.float32)
+        self.camera = np.zeros(1, REF_CAMERA_DTYPE)
+        lib.refl_extras_copy(_p(self.emitters), _p(self.triangle_emission), _p(self.spotlights), _p(env),
+                             _p(self.camera))
+        self.camera = self.camera[0]
+        self.env_rgba = env if EW > 0 else None
+        self.width, self.height = int(cam[10]), int(cam[11])
+        self.env_intensity, self.env_rotation_deg = float(cam[12]), float(cam[13])
+        self.triangle_count = T
+
+
+def lbvh_morton_order(triangles):
+    """CPU restatement of the LBVH's integer steps (the product's acceleration-structure build; the reference
+    builds an OptiX GAS instead, src/host/optix_setup.cu:215-292, whose internals are closed): per triangle the
+    centroid 0.5*(min+max) of its vertex bounds in float32, the centroid bounds, per axis
+    q = min(trunc((c - lo) / (hi - lo) * 2^21), 2^21 - 1) (0 on a flat axis), the 63-bit code interleaving
+    qx, qy, qz (x highest), and the stable ascending order of the codes.  Returns (codes uint64, order int32)."""
+    v0, v1, v2 = (np.asarray(triangles[k], np.float32) for k in ("v0", "v1", "v2"))
+    lo = np.minimum(v0, np.minimum(v1, v2))
+    hi = np.maximum(v0, np.maximum(v1, v2))
+    c = (np.float32(0.5) * (lo + hi)).astype(np.float32)
+    clo, chi = c.min(axis=0), c.max(axis=0)
+    q = np.zeros_like(c, dtype=np.uint32)
+    for k in range(3):
+        ext = np.float32(chi[k] - clo[k])
+        if ext > 0:
+            f = ((c[:, k] - clo[k]) / ext).astype(np.float32)
+        else:
+            f = np.zeros(len(c), np.float32)
+        f = np.clip(f, np.float32(0.0), np.float32(1.0))
+        q[:, k] = np.minimum((f * np.float32(2097152.0)).astype(np.uint32), np.uint32(2097151))
+
+    def spread(x):
+        x = x.astype(np.uint64) & np.uint64(0x1fffff)
+        for shift, mask in ((32, 0x1f00000000ffff), (16, 0x1f0000ff0000ff), (8, 0x100f00f00f00f00f),
+                            (4, 0x10c30c30c30c30c3), (2, 0x1249249249249249)):
+            x = (x | (x << np.uint64(shift))) & np.uint64(mask)
+        return x
+
+    codes = (spread(q[:, 0]) << np.uint64(2)) | (spread(q[:, 1]) << np.uint64(1)) | spread(q[:, 2])
+    return codes, np.argsort(codes, kind="stable").astype(np.int32)

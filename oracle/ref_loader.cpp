@@ -40,6 +40,12 @@ std::vector<int> g_matW, g_matH;
 std::vector<std::vector<uint8_t>> g_matMr;      // metallic-roughness RGBA8 per material (empty: none)
 std::vector<int> g_mrW, g_mrH;
 int g_emitterCount = 0;
+std::vector<EmitterData> g_emitters;            // src/main.cpp:686-701 (finishEmitter)
+std::vector<Float3> g_emission;                 // per-triangle emission, src/main.cpp:735-750
+std::vector<SpotlightData> g_spots;             // src/main.cpp:883-905
+std::vector<float> g_env;                       // RGBA float texels, src/main.cpp:907-930
+int g_envW = 0, g_envH = 0;
+CameraData g_camera{};                          // src/main.cpp:533-564
 
 std::string resolve(const std::string& scenePath, const std::string& p)
 {
@@ -109,10 +115,29 @@ float area(const TriangleData& t)
 }
 }  // namespace
 
+// finishEmitter of src/main.cpp:686-701: one EmitterData per emitter whose triangles were just appended
+static void finishEmitter(int triIndexOffset, int cdfOffset, float areaSum, const Float3& radiance, float& wsum)
+{
+    const float lum = 0.2126f * radiance.x + 0.7152f * radiance.y + 0.0722f * radiance.z;
+    const float weight = areaSum * lum;
+    wsum += weight;
+    g_sceneCdf.push_back(wsum);
+    EmitterData e{};
+    e.triIndexOffset = triIndexOffset;
+    e.triCount = (int)g_emTri.size() - triIndexOffset;
+    e.cdfOffset = cdfOffset;
+    e.radiance = radiance;
+    e.areaSum = areaSum;
+    e.powerWeight = weight;
+    g_emitters.push_back(e);
+    ++g_emitterCount;
+}
+
 REF_API int refl_load(const char* scenePath)
 {
     g_tris.clear(); g_bsdfs.clear(); g_triBsdf.clear(); g_triMat.clear(); g_emTri.clear(); g_emCdf.clear();
     g_sceneCdf.clear(); g_flags.clear(); g_cam.clear();
+    g_emitters.clear(); g_emission.clear(); g_spots.clear(); g_env.clear(); g_envW = g_envH = 0;
     const SceneDescription d = loadSceneDescription(scenePath);   // src/scene.cpp:83
     g_matColour.clear(); g_matImage.clear(); g_matW.clear(); g_matH.clear();
     g_matMr.clear(); g_mrW.clear(); g_mrH.clear(); g_emitterCount = 0;
@@ -172,6 +197,8 @@ REF_API int refl_load(const char* scenePath)
         for (size_t i = 0; i < d.bsdfs.size(); ++i) if (d.bsdfs[i].name == d.materials[(size_t)matId].bsdfName) bsdfId = (int)i;
         std::vector<TriangleData> mt;
         loadObj(resolve(scenePath, m.filename), m.transform, mt);
+        const Float3 emitColor = {m.radianceR, m.radianceG, m.radianceB};
+        const int triIndexOffset = (int)g_emTri.size(), cdfOffset = (int)g_emCdf.size();
         if (m.isEmitter) g_emCdf.push_back(0.0f);
         float a = 0.0f;
         for (const auto& t : mt) {
@@ -179,18 +206,14 @@ REF_API int refl_load(const char* scenePath)
             g_triMat.push_back(matId);
             g_triBsdf.push_back(bsdfId);
             g_flags.push_back(m.isEmitter ? 1 : 0);
+            g_emission.push_back(m.isEmitter ? emitColor : Float3{0.0f, 0.0f, 0.0f});
             if (m.isEmitter) {
                 a += area(t);
                 g_emTri.push_back((int)g_tris.size() - 1);
                 g_emCdf.push_back(a);
             }
         }
-        if (m.isEmitter) {
-            const float lum = 0.2126f * m.radianceR + 0.7152f * m.radianceG + 0.0722f * m.radianceB;
-            wsum += a * lum;
-            g_sceneCdf.push_back(wsum);
-            ++g_emitterCount;
-        }
+        if (m.isEmitter) finishEmitter(triIndexOffset, cdfOffset, a, emitColor, wsum);
     }
     for (const auto& md : d.models) {   // src/main.cpp:760-817
         const GltfLoadResult gl = loadGltfModel(resolve(scenePath, md.filename), md.transform);
@@ -208,14 +231,17 @@ REF_API int refl_load(const char* scenePath)
         }
         for (size_t i = 0; i < gl.triangles.size(); ++i) {
             const int local = gl.materialIds[i];
+            const auto& slot = gl.materials[(size_t)local];
             g_tris.push_back(gl.triangles[i]);
             g_triMat.push_back(matOffset + local);
             g_triBsdf.push_back(bsdfOffset + local);
-            g_flags.push_back(gl.materials[(size_t)local].isEmitter ? 1 : 0);
+            g_flags.push_back(slot.isEmitter ? 1 : 0);
+            g_emission.push_back(slot.isEmitter ? slot.emission : Float3{0.0f, 0.0f, 0.0f});
         }
         for (size_t mi = 0; mi < gl.materials.size(); ++mi) {
             const auto& slot = gl.materials[mi];
             if (!slot.isEmitter) continue;
+            const int triIndexOffset = (int)g_emTri.size(), cdfOffset = (int)g_emCdf.size();
             g_emCdf.push_back(0.0f);
             float areaSum = 0.0f;
             const int matId = matOffset + (int)mi;
@@ -225,13 +251,51 @@ REF_API int refl_load(const char* scenePath)
                 g_emTri.push_back(ti);
                 g_emCdf.push_back(areaSum);
             }
-            if (areaSum > 0.0f) {
-                const float lum = 0.2126f * slot.emission.x + 0.7152f * slot.emission.y + 0.0722f * slot.emission.z;
-                wsum += areaSum * lum;
-                g_sceneCdf.push_back(wsum);
-                ++g_emitterCount;
-            }
+            if (areaSum > 0.0f) finishEmitter(triIndexOffset, cdfOffset, areaSum, slot.emission, wsum);
         }
+    }
+    for (const auto& sd : d.spotlights) {   // src/main.cpp:883-905
+        SpotlightData sp{};
+        sp.position = {sd.posX, sd.posY, sd.posZ};
+        float dx = sd.dirX, dy = sd.dirY, dz = sd.dirZ;
+        const float dlen = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (dlen > 1e-6f) { dx /= dlen; dy /= dlen; dz /= dlen; }
+        sp.direction = {dx, dy, dz};
+        sp.radiance = {sd.radianceR, sd.radianceG, sd.radianceB};
+        sp.intensity = sd.intensity;
+        const float kPi = 3.14159265358979323846f;
+        sp.innerConeCosine = cosf(sd.innerConeAngle * kPi / 180.0f);
+        sp.outerConeCosine = cosf(sd.outerConeAngle * kPi / 180.0f);
+        g_spots.push_back(sp);
+    }
+    if (!d.envMapPath.empty()) {   // src/main.cpp:907-930 (path taken relative to the scene file, as the OBJs)
+        int comp = 0;
+        float* rgb = stbi_loadf(resolve(scenePath, d.envMapPath).c_str(), &g_envW, &g_envH, &comp, 3);
+        if (!rgb) return -1;
+        g_env.assign((size_t)g_envW * g_envH * 4, 1.0f);
+        for (size_t i = 0; i < (size_t)g_envW * g_envH; ++i)
+            for (int c = 0; c < 3; ++c) g_env[4 * i + c] = rgb[3 * i + c];
+        stbi_image_free(rgb);
+    }
+    {   // src/main.cpp:533-564, with GLM's normalize (v * 1/sqrt(dot)), cross and radians
+        const CameraDesc& c = d.camera;
+        const Float3 eye = {c.eyeX, c.eyeY, c.eyeZ}, up = {c.upX, c.upY, c.upZ};
+        const Float3 tgt = {c.lookAtX, c.lookAtY, c.lookAtZ};
+        auto cross = [](Float3 x, Float3 y) {
+            return Float3{x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y};
+        };
+        auto normalize = [](Float3 v) {
+            const float inv = 1.0f / std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+            return Float3{v.x * inv, v.y * inv, v.z * inv};
+        };
+        const Float3 forward = normalize(Float3{tgt.x - eye.x, tgt.y - eye.y, tgt.z - eye.z});
+        const Float3 right = normalize(cross(forward, up));
+        g_camera.origin = eye;
+        g_camera.forward = forward;
+        g_camera.right = right;
+        g_camera.up = cross(right, forward);
+        g_camera.fovYRadians = c.fovYDegrees * 0.01745329251994329576923690768489f;
+        g_camera.aspect = (float)d.windowWidth / (float)d.windowHeight;
     }
     const CameraDesc& c = d.camera;
     g_cam = {c.eyeX, c.eyeY, c.eyeZ, c.lookAtX, c.lookAtY, c.lookAtZ, c.upX, c.upY, c.upZ, c.fovYDegrees,
@@ -282,4 +346,23 @@ REF_API void refl_copy(TriangleData* tris, BsdfData* bsdfs, int* triBsdf, int* t
     std::memcpy(emCdf, g_emCdf.data(), g_emCdf.size() * sizeof(float));
     std::memcpy(sceneCdf, g_sceneCdf.data(), g_sceneCdf.size() * sizeof(float));
     std::memcpy(cam, g_cam.data(), g_cam.size() * sizeof(float));
+}
+
+// The rest of what src/main.cpp:836-930 uploads: emitter table, per-triangle emission, spotlights, the env map
+// (RGBA float) and the camera.  Sizes first (null pointers), then copies.
+REF_API int refl_extras_counts(int* out)
+{
+    out[0] = (int)g_emitters.size(); out[1] = (int)g_emission.size(); out[2] = (int)g_spots.size();
+    out[3] = g_envW; out[4] = g_envH;
+    return 0;
+}
+
+REF_API void refl_extras_copy(EmitterData* emitters, Float3* emission, SpotlightData* spots, float* envRGBA,
+                              CameraData* camera)
+{
+    if (!g_emitters.empty()) std::memcpy(emitters, g_emitters.data(), g_emitters.size() * sizeof(EmitterData));
+    if (!g_emission.empty()) std::memcpy(emission, g_emission.data(), g_emission.size() * sizeof(Float3));
+    if (!g_spots.empty()) std::memcpy(spots, g_spots.data(), g_spots.size() * sizeof(SpotlightData));
+    if (!g_env.empty()) std::memcpy(envRGBA, g_env.data(), g_env.size() * sizeof(float));
+    std::memcpy(camera, &g_camera, sizeof(CameraData));
 }

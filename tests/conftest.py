@@ -1,4 +1,5 @@
-"""Shared fixtures.  GPU tests are marked `gpu`; everything else runs on CPU."""
+"""Shared fixtures.  GPU tests are marked `gpu`; everything else runs on CPU.  The default library of the
+test process is the parity build (BTE_LIBRARY=parity)."""
 import os
 import sys
 
@@ -7,6 +8,8 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
+# Bit-exact tests run on the parity build of the library; tests of the product build ask for variant="fast".
+os.environ.setdefault("BTE_LIBRARY", "parity")
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 

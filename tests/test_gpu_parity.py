@@ -573,6 +573,55 @@ def test_megakernel_mode_matches_oracle(renderer, oracle_mod, random_scene):
         renderer.set_render_mode(1)
 
 
+def test_megakernel_features_and_denoiser(renderer, bte, cornell_scene):
+    """Megakernel mode with features on: the radiance stays bit-identical to features off; the features are the
+    per-frame means of the first-hit albedo and normal (on the Cornell box, where every pixel sees a wall, they
+    agree with the wavefront's features of the same view wherever a pixel's samples all hit one surface); and
+    the renderer's toggled denoiser in this mode equals the stand-alone denoiser run on the read-back mean and
+    features, bit for bit."""
+    from bluetruthengine_b200.denoiser import Denoiser
+    sc = cornell_scene
+    W, H = sc.width, sc.height
+    weights = os.path.join(os.path.dirname(bte.__file__), "weights", "denoiser_c4.npz")
+    _upload(renderer, sc, env_mode=0, spp=16, depth=8)
+    renderer.set_aov(True)
+    renderer.reset_accumulation(W, H)
+    renderer.render(W, H)
+    wf_alb, wf_nrm = renderer.read_aov(W, H)
+    renderer.set_render_mode(0)
+    try:
+        out = {}
+        for aov in (False, True):
+            renderer.set_aov(aov)
+            renderer.reset_accumulation(W, H)
+            for _ in range(2):
+                renderer.render(W, H)
+            out[aov] = (renderer.read_accum(W, H).copy(), renderer.read_aov(W, H) if aov else None)
+        assert np.array_equal(bits(out[False][0]), bits(out[True][0]))
+        alb, nrm = out[True][1]
+        alb, nrm, wf_alb, wf_nrm = (a.reshape(-1, 3) for a in (alb, nrm, wf_alb, wf_nrm))
+        assert np.all(np.isfinite(alb)) and np.all((alb >= 0) & (alb <= 1.0 + 1e-6))
+        assert np.all(np.linalg.norm(nrm, axis=1) <= 1.0 + 1e-5)
+        same = np.all(np.abs(alb - wf_alb) <= 1e-6, axis=1) & np.all(np.abs(nrm - wf_nrm) <= 1e-5, axis=1)
+        assert same.mean() > 0.9, f"only {same.mean():.3f} of pixels agree with the wavefront features"
+        dn = Denoiser()
+        dn.load(weights)
+        assert renderer.toggle_denoiser()
+        try:
+            renderer.render(W, H)
+            den = renderer.read_denoised(W, H)
+            rad = renderer.read_accum(W, H).reshape(H, W, 3)
+            a2, n2 = renderer.read_aov(W, H)
+        finally:
+            renderer.toggle_denoiser()
+        ref = dn.denoise(rad, np.concatenate([a2.reshape(H, W, 3), n2.reshape(H, W, 3)], -1))
+        assert np.all(np.isfinite(den)) and float(den.mean()) > 0.0
+        assert np.array_equal(bits(den), bits(ref))
+    finally:
+        renderer.set_aov(False)
+        renderer.set_render_mode(1)
+
+
 def test_batched_views_match_single_view_frames(renderer, bte, random_scene):
     """Three views of uneven size and samples per frame rendered in one launch sequence, two frames: each
     view's FP32 mean and FP64 sum equal those of bte_render with that camera, bit for bit."""

@@ -12,9 +12,11 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, bits
+import oracle as _O  # the checker's reference-tree location (conftest puts oracle/ on the path)
 
 FIX = os.path.join(ROOT, "tests", "golden", "images", "fixtures.npz")
-REF_CHECKER = "/root/reference/assets/checkerboard.jpg"
+REF_ASSETS = os.path.join(_O.REFERENCE_ROOT, "assets")
+REF_CHECKER = os.path.join(REF_ASSETS, "checkerboard.jpg")
 
 
 @pytest.fixture(scope="module")
@@ -90,7 +92,7 @@ def test_corrupt_and_unsupported_inputs_fail_with_a_message(bte, fixtures):
             bte.decode_image(data)
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/assets/scene.xml"), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_ASSETS, "scene.xml")), reason="reference tree not present")
 def test_reference_scene_xml_materials(bte, monkeypatch, tmp_path):
     """The reference's own assets/scene.xml (its floor textured by assets/checkerboard.jpg), loaded from a
     working directory where assets/ is the reference's, as its application runs: material colours and texture
@@ -102,12 +104,12 @@ def test_reference_scene_xml_materials(bte, monkeypatch, tmp_path):
     if not os.path.exists(ref_path):
         import oracle as O
         O.build(ref=True)
-    os.symlink("/root/reference/assets", tmp_path / "assets")
-    xml = open("/root/reference/assets/scene.xml").read()
+    os.symlink(REF_ASSETS, tmp_path / "assets")
+    xml = open(os.path.join(REF_ASSETS, "scene.xml")).read()
     (tmp_path / "scene.xml").write_text(re.sub(r"<model\b[^>]*/>", "", xml, flags=re.S))
     monkeypatch.chdir(tmp_path)
     with pytest.raises(bte.BteError, match="sakutaro.glb"):
-        bte.load_scene("/root/reference/assets/scene.xml")
+        bte.load_scene(os.path.join(REF_ASSETS, "scene.xml"))
     sc = bte.load_scene("scene.xml")
     lib = C.CDLL(ref_path)
     lib.refl_load(b"scene.xml")
@@ -158,9 +160,9 @@ def test_textured_materials_match_reference_loader(bte, tmp_path, fixtures):
     sc = bte.load_scene(path)
     ref_path = os.path.join(ROOT, "oracle", "_ref", "libbteref_loader.so")
     if not os.path.exists(ref_path):
-        if not os.path.isdir("/root/reference/include"):
-            pytest.skip("reference loader harness not built")
         import oracle as O
+        if not O.reference_present():
+            pytest.skip("reference loader harness not built")
         O.build(ref=True)
     lib = C.CDLL(ref_path)
     lib.refl_load(path.encode())

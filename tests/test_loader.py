@@ -14,8 +14,8 @@ REF_LOADER = os.path.join(ROOT, "oracle", "_ref", "libbteref_loader.so")
 
 def _ref_flatten(bte, path):
     if not os.path.exists(REF_LOADER):
-        if os.path.isdir("/root/reference/include"):
-            import oracle as O
+        import oracle as O
+        if O.reference_present():
             O.build(ref=True)
         else:
             pytest.skip("reference loader harness not built")
@@ -53,6 +53,30 @@ def test_loader_matches_reference_parser(bte, which):
     assert np.float32(sc.env_intensity) == cam[12] and np.float32(sc.env_rotation_deg) == cam[13]
     assert len(sc.spotlights) == int(cam[14])
     assert np.array_equal(bits(sc.camera["origin"]), bits(cam[0:3]))
+
+
+@pytest.mark.parametrize("which", ["cornell", "random", "disney"])
+def test_reference_scene_matches_loader(bte, which):
+    """The whole upload set flattened by the reference's loader alone (oracle.RefScene: emitter table,
+    per-triangle emission, spotlights, the .hdr env map through the reference's stb_image, camera basis)
+    equals the product loader's, byte for byte.  The reference arm of the bench renders RefScene."""
+    import oracle as O
+    from bluetruthengine_b200 import scenes
+    if not (os.path.exists(REF_LOADER) or O.reference_present()):
+        pytest.skip("reference loader harness not built")
+    path = {"cornell": scenes.cornell, "random": lambda: scenes.random_scene(5), "disney": scenes.disney_spheres}[which]()
+    r = O.RefScene(path)
+    s = bte.load_scene(path)
+    same = lambda a, b: np.ascontiguousarray(a).tobytes() == np.ascontiguousarray(b).tobytes()  # noqa: E731
+    assert same(r.triangles, s.triangles) and same(r.bsdfs, s.bsdfs)
+    assert same(r.emitters, s.emitters) and same(r.spotlights, s.spotlights)
+    assert same(np.asarray(r.triangle_emission, np.float32), np.asarray(s.triangle_emission, np.float32))
+    assert (r.env_rgba is None) == (s.env_rgba is None)
+    if r.env_rgba is not None:
+        assert same(r.env_rgba, s.env_rgba)
+    assert same(r.camera, s.camera)
+    assert (r.width, r.height, r.env_intensity, r.env_rotation_deg) == \
+        (s.width, s.height, np.float32(s.env_intensity), np.float32(s.env_rotation_deg))
 
 
 def test_cornell_contents(cornell_scene):
