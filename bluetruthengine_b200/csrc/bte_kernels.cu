@@ -61,6 +61,35 @@ BTE_DI void sortAppend(const DevScene& s, const DevPaths& P, int bounce, int idx
 
 BTE_DI V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 
+// Whether bounce `bounce` walks its queue in ray-bin order (same answer in shade, kRayBins, kRayScatter, extend).
+BTE_DI bool raySorted(const DevPaths& P, int bounce, int count)
+{
+    return P.raySortBits > 0 && bounce >= 1 && bounce <= P.raySortBounces && count >= kRaySortMinRays;
+}
+BTE_DI int rayBinCount(const DevPaths& P) { return 8 << (3 * P.raySortBits); }
+BTE_DI uint32_t spreadBits3(uint32_t v)   // bit i of v -> bit 3i (v < 32)
+{
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) x |= ((v >> i) & 1u) << (3 * i);
+    return x;
+}
+// bin of a ray: direction octant in the high bits, then the Morton code of its origin cell
+BTE_DI int rayBinOf(const DevPaths& P, float sceneMaxAbs, float4 o, float4 d)
+{
+    const int bits = P.raySortBits;
+    const float m = sceneMaxAbs > 0.0f ? sceneMaxAbs : 1.0f;
+    const float scale = static_cast<float>(1 << bits) / (2.0f * m);
+    const int top = (1 << bits) - 1;
+    const int cx = min(max(static_cast<int>((o.x + m) * scale), 0), top);
+    const int cy = min(max(static_cast<int>((o.y + m) * scale), 0), top);
+    const int cz = min(max(static_cast<int>((o.z + m) * scale), 0), top);
+    const uint32_t cell = (spreadBits3(static_cast<uint32_t>(cx)) << 2) | (spreadBits3(static_cast<uint32_t>(cy)) << 1) |
+                          spreadBits3(static_cast<uint32_t>(cz));
+    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    return static_cast<int>((oct << (3 * bits)) | cell);
+}
+
 // The wavefront stops at the first bounce whose queue holds fewer than tailPaths paths; kTail then
 // finishes those paths one thread each (the few long paths no longer pay a launch per bounce).
 BTE_DI bool tailTakesOver(const DevPaths& P, int bounce)
@@ -134,7 +163,7 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
 {
     const int count = P.rayCount[bounce];
     if (tailTakesOver(P, bounce)) return;
-    const int* __restrict__ q = P.queue[bounce & 1];
+    const int* __restrict__ q = raySorted(P, bounce, count) ? P.sortedQueue : P.queue[bounce & 1];
     const int stride = gridDim.x * blockDim.x;
     for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += stride) {
         const int idx = q[slot];
@@ -274,8 +303,55 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
             idx = q[slot];
         }
         const bool alive = shadePath(s, P, f, bounce, idx, true);
-        if (alive && bounce + 1 < P.maxDepth) qn[appendCoalesced(P.rayCount + bounce + 1)] = idx;
+        if (alive && bounce + 1 < P.maxDepth) {
+            const int next = appendCoalesced(P.rayCount + bounce + 1);
+            qn[next] = idx;
+            if (P.raySortBits > 0 && bounce + 1 <= P.raySortBounces) {
+                const int bin = rayBinOf(P, s.sceneMaxAbs, P.o[idx], P.d[idx]);
+                P.rayBin[next] = bin;
+                appendKeyed(P.binCount + static_cast<size_t>(bounce + 1) * rayBinCount(P), bin);
+            }
+        }
     }
+}
+
+// Bin counts of a bounce -> bin starts (exclusive scan in place; one block, each thread a run of bins).
+__global__ void __launch_bounds__(1024) kRayBins(DevPaths P, int bounce)
+{
+    const int count = P.rayCount[bounce];
+    if (!raySorted(P, bounce, count)) return;
+    const int nb = rayBinCount(P);
+    int* c = P.binCount + static_cast<size_t>(bounce) * nb;
+    __shared__ int part[1024];
+    const int per = (nb + 1023) / 1024;
+    const int lo = min(static_cast<int>(threadIdx.x) * per, nb), hi = min(lo + per, nb);
+    int sum = 0;
+    for (int i = lo; i < hi; ++i) sum += c[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int v = static_cast<int>(threadIdx.x) >= off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
+    for (int i = lo; i < hi; ++i) {
+        const int v = c[i];
+        c[i] = run;
+        run += v;
+    }
+}
+
+// The bounce's queue in bin order (order inside a bin is arbitrary: results do not depend on queue order).
+__global__ void __launch_bounds__(256) kRayScatter(DevPaths P, int bounce)
+{
+    const int count = P.rayCount[bounce];
+    if (!raySorted(P, bounce, count)) return;
+    int* starts = P.binCount + static_cast<size_t>(bounce) * rayBinCount(P);
+    const int* __restrict__ q = P.queue[bounce & 1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        P.sortedQueue[appendKeyed(starts, P.rayBin[i])] = q[i];
 }
 
 // ---------------------------------------------------------------- connect
@@ -318,7 +394,7 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
     if (tailTakesOver(P, bounce)) return;
-    const int* __restrict__ q = P.queue[bounce & 1];
+    const int* __restrict__ q = raySorted(P, bounce, count) ? P.sortedQueue : P.queue[bounce & 1];
     uint2 stack[kWideStack];
     if (count <= static_cast<int>((gridDim.x * blockDim.x) >> 3)) {   // few rays: eight lanes per ray
         const int g = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
@@ -778,6 +854,11 @@ void launchGenerate(const DevPaths& P, const FrameParams& f, cudaStream_t st)
 {
     const int blocks = (P.count + 255) / 256;
     kGenerate<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, f);
+}
+void launchRaySort(const DevPaths& P, int bounce, int grid, cudaStream_t st)
+{
+    kRayBins<<<1, 1024, 0, st>>>(P, bounce);
+    kRayScatter<<<grid, 256, 0, st>>>(P, bounce);
 }
 void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
 {

@@ -103,6 +103,8 @@ struct Renderer {
     int plocRadius = 4;       // PLOC neighbour search radius (measured on the 1080p scene: 4 best of 4/6/8/12/16/32)
     int builtBuilder = 0;     // hierarchy in use
     int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
+    int raySortBits = 0;      // ray reordering before extend: origin cell bits per axis (0: off)
+    int raySortBounces = 4;   // bounces 1..raySortBounces are reordered
     bool sceneChanged = false;   // bte_mark_scene_changed: the next bte_render resets accumulation first
     int builtWidth = 2;       // tree in use
     int accelNodes = 0, accelDepth = 0;
@@ -120,7 +122,7 @@ struct Renderer {
     uint32_t* extFramebuffer = nullptr;
     // wavefront buffers
     DeviceBuffer pO, pD, pTp, pL, pHit, q0, q1, rayCount, shadowCount, fetch, shadowQueue, shOrigin, shDir, shContrib,
-        shMask, hitLog, errorFlags, sortQueue, sortCount;
+        shMask, hitLog, errorFlags, sortQueue, sortCount, rayBin, sortedQueue, binCount;
     int pathCap = 0, slotCap = 0, depthCap = 0;
     bool hitLogEnabled = false;
     bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
@@ -298,17 +300,34 @@ void releaseWavefront()
     releaseGraph();
     releaseViewGraph();
     for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch,
-                            &g.sortQueue, &g.sortCount, &g.shadowQueue,
+                            &g.sortQueue, &g.sortCount, &g.shadowQueue, &g.rayBin, &g.sortedQueue, &g.binCount,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
         b->release();
     g.aovAlbedo.release(); g.aovNormal.release();
     g.pathCap = g.slotCap = g.depthCap = 0;
 }
 
+// bin counts of the reordered bounces (0..raySortBounces) for the current ray-sort setting
+size_t rayBinBytes() { return sizeof(int) * static_cast<size_t>(g.raySortBounces + 1) * (8u << (3 * g.raySortBits)); }
+
+// ray-reordering fields of a frame's DevPaths (off in megakernel mode)
+void setRaySort(DevPaths& P, bool on)
+{
+    if (!on || g.raySortBits <= 0) return;
+    P.rayBin = g.rayBin.as<int>();
+    P.binCount = g.binCount.as<int>();
+    P.sortedQueue = g.sortedQueue.as<int>();
+    P.raySortBits = g.raySortBits;
+    P.raySortBounces = g.raySortBounces;
+}
+
 void ensureWavefront(int paths, int slots, int depth)
 {
     const bool grow = paths > g.pathCap || slots > g.slotCap || depth > g.depthCap;
-    if (!grow && (!g.hitLogEnabled || g.hitLog.p) && (!g.sortShading || g.sortQueue.p)) return;
+    const size_t binBytes = g.raySortBits > 0 ? rayBinBytes() : 0;
+    if (!grow && (!g.hitLogEnabled || g.hitLog.p) && (!g.sortShading || g.sortQueue.p) &&
+        (!g.raySortBits || (g.sortedQueue.p && g.binCount.bytes >= binBytes)))
+        return;
     if (grow) {
         releaseWavefront();
         const size_t P = static_cast<size_t>(paths), S = static_cast<size_t>(slots);
@@ -328,6 +347,11 @@ void ensureWavefront(int paths, int slots, int depth)
     }
     if (g.hitLogEnabled) ensure(g.hitLog, static_cast<size_t>(g.pathCap) * g.depthCap * 4);
     if (g.sortShading) ensure(g.sortQueue, static_cast<size_t>(g.pathCap) * kSortKeys * 4);
+    if (g.raySortBits > 0) {
+        ensure(g.rayBin, static_cast<size_t>(g.pathCap) * 4);
+        ensure(g.sortedQueue, static_cast<size_t>(g.pathCap) * 4);
+        ensure(g.binCount, binBytes);
+    }
 }
 
 void ensureAov(int paths)
@@ -376,6 +400,7 @@ int slotsFor() { return 1 + g.spotCount + 1; }
 void launchBounces(const DevScene& s, const DevPaths& P, const FrameParams& f, int depth, int block, cudaStream_t st)
 {
     for (int b = 0; b < depth; ++b) {
+        if (P.raySortBits > 0 && b >= 1 && b <= P.raySortBounces) launchRaySort(P, b, g.gridShade, st);
         launchExtend(s, P, b, g.gridExtend, block, st);
         if (g.overlapConnect && b > 0) ck(cudaStreamWaitEvent(st, g.evConnect, 0), "cudaStreamWaitEvent");
         launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
@@ -440,6 +465,7 @@ void renderFrame(int w, int h)
     P.sortQueue = g.sortShading ? g.sortQueue.as<int>() : nullptr;
     P.sortCount = g.sortCount.as<int>();
     P.tailPaths = mega ? 0 : g.tailPaths;
+    setRaySort(P, !mega);
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
     f.width = w; f.height = h; f.spp = spp;
@@ -460,6 +486,7 @@ void renderFrame(int w, int h)
         ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+        if (P.raySortBits > 0) ck(cudaMemsetAsync(g.binCount.p, 0, rayBinBytes(), st), "cudaMemsetAsync");
         if (g.hitLogEnabled) ck(cudaMemsetAsync(g.hitLog.p, 0xfe, static_cast<size_t>(paths) * depth * 4, st), "cudaMemsetAsync");
         ck(cudaMemcpyAsync(g.dFrameIndex.p, g.hFrameIndex, sizeof(uint32_t), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
     };
@@ -524,7 +551,10 @@ void renderFrame(int w, int h)
         };
         timed(0, [&] { launchGenerate(P, f, st); });
         for (int b = 0; b < depth; ++b) {
-            timed(1, [&] { launchExtend(s, P, b, g.gridExtend, block, st); });
+            timed(1, [&] {
+                if (P.raySortBits > 0 && b >= 1 && b <= P.raySortBounces) launchRaySort(P, b, g.gridShade, st);
+                launchExtend(s, P, b, g.gridExtend, block, st);
+            });
             timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st); });
             timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
         }
@@ -655,6 +685,7 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
     // Batched views have no megakernel counterpart in the reference; in that mode every path of the views runs
     // start to end in the tail kernel (the wavefront's per-sample streams, bit-identical images).
     P.tailPaths = g.renderMode == BTE_RENDER_MEGAKERNEL ? 0x7fffffff : g.tailPaths;
+    setRaySort(P, g.renderMode != BTE_RENDER_MEGAKERNEL);
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
     f.frameIndex = g.dFrameIndex.as<uint32_t>();
@@ -669,6 +700,7 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
         ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+        if (P.raySortBits > 0) ck(cudaMemsetAsync(g.binCount.p, 0, rayBinBytes(), st), "cudaMemsetAsync");
         launchGenerate(P, f, st);
         launchBounces(s, P, f, depth, block, st);
         launchTail(s, P, f, st);
@@ -1424,6 +1456,8 @@ int bte_set_tuning(const BteTuning* t)
         if (t->plocRadius < 1 || t->plocRadius > kPlocMaxRadius) throw CudaError{"bte_set_tuning: plocRadius in [1, 32]"};
         if (t->overlapConnect != 0 && t->overlapConnect != 1) throw CudaError{"bte_set_tuning: overlapConnect must be 0 or 1"};
         if (t->wideCollapse != 0 && t->wideCollapse != 1) throw CudaError{"bte_set_tuning: wideCollapse must be 0 or 1"};
+        if (t->raySortBits < 0 || t->raySortBits > 4) throw CudaError{"bte_set_tuning: raySortBits in [0, 4]"};
+        if (t->raySortBounces < 1 || t->raySortBounces > 64) throw CudaError{"bte_set_tuning: raySortBounces in [1, 64]"};
         g.bvhWidth = t->bvhWidth;
         g.maxLeaf = t->maxLeafTriangles;
         g.shadeMinBlocks = t->shadeMinBlocks;
@@ -1434,6 +1468,8 @@ int bte_set_tuning(const BteTuning* t)
         g.plocRadius = t->plocRadius;
         g.overlapConnect = t->overlapConnect;
         g.wideCollapse = t->wideCollapse;
+        g.raySortBits = t->raySortBits;
+        g.raySortBounces = t->raySortBounces;
         g.gridBlock = 0;   // recompute persistent grids
         return 0;
     });
@@ -1453,6 +1489,8 @@ int bte_get_tuning(BteTuning* t)
         t->plocRadius = g.plocRadius;
         t->overlapConnect = g.overlapConnect;
         t->wideCollapse = g.wideCollapse;
+        t->raySortBits = g.raySortBits;
+        t->raySortBounces = g.raySortBounces;
         return 0;
     });
 }

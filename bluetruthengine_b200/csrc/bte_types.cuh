@@ -125,7 +125,18 @@ struct DevPaths {
     int* sortCount;   // [(maxDepth + 1) * kSortKeys]
     int tailPaths;    // a bounce queue shorter than this is finished by kTail (0: wavefront to the end)
     unsigned int* errorFlags;   // bit 0: traversal stack overflow; bit 1: malformed tree (index out of range)
+    // ray reordering between bounces (raySortBits > 0): for bounces 1..raySortBounces with at least
+    // kRaySortMinRays rays, shade records each surviving path's bin -- its direction octant, then its origin
+    // cell (raySortBits bits per axis over the cube |x| <= sceneMaxAbs, Morton order) -- beside its queue entry
+    // and counts the bins; kRayBins turns the counts into bin starts and kRayScatter writes the queue in bin
+    // order, which extend walks, so a warp traces rays of one octant from one region.
+    int* rayBin;      // [count] bin of next-bounce queue slot i
+    int* binCount;    // [(raySortBounces + 1) << (3 + 3 * raySortBits)] counts per bounce, then bin positions
+    int* sortedQueue; // [count] the bounce's queue in bin order
+    int raySortBits;  // origin cell bits per axis, 0 (off) to 4
+    int raySortBounces;
 };
+constexpr int kRaySortMinRays = 32768;
 
 // One camera view of a batched frame (bte_render_views): its paths are
 // [pathOffset, pathOffset + width*height*spp) of the frame, sample-major as

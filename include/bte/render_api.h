@@ -160,6 +160,11 @@ typedef struct {
                             * rays (they share no data); 0: the stages run one after another */
     int wideCollapse;      /* children of each 8-wide node: 0 greedy (open the largest-area child first);
                             * 1 surface-area-optimal (dynamic program of Ylitie, Karras & Laine 2017) */
+    int raySortBits;       /* 0: off; 1-4: before the closest-hit rays of bounces 1..raySortBounces (queues of at
+                            * least 32768 rays), the queue is reordered by direction octant and origin cell
+                            * (raySortBits bits per axis of the scene's bounding cube), so a warp traces nearby
+                            * rays of one octant; results do not depend on it */
+    int raySortBounces;    /* last bounce reordered, 1-64 */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);

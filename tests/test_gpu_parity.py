@@ -52,9 +52,9 @@ def test_math_functions_bitexact(renderer, oracle_mod):
 
 
 def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0,
-            builder=1, radius=8, collapse=1):
+            builder=1, radius=8, collapse=1, ray_sort=0):
     renderer.cleanup()
-    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius, 1, collapse)
+    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius, 1, collapse, ray_sort)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
@@ -269,18 +269,20 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder",
-                         [(1, 8, 0, 0, 0), (0, 8, 0, 0, 0), (1, 2, 0, 0, 0), (1, 8, 1, 0, 0), (1, 8, 1, 200000, 0),
-                          (1, 8, 1, 0, 1), (0, 2, 0, 0, 1)])
+@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder,ray_sort",
+                         [(1, 8, 0, 0, 0, 0), (0, 8, 0, 0, 0, 0), (1, 2, 0, 0, 0, 0), (1, 8, 1, 0, 0, 0),
+                          (1, 8, 1, 200000, 0, 0), (1, 8, 1, 0, 1, 0), (0, 2, 0, 0, 1, 0), (1, 8, 1, 0, 1, 3),
+                          (1, 2, 0, 0, 1, 2)])
 def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading, tail_paths,
-                                     builder):
+                                     builder, ray_sort):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
-    pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit."""
+    pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit; with and without the rays of
+    bounces 1-4 reordered by direction octant and origin cell."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
     _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading,
-            tail_paths=tail_paths, max_leaf=1 if bvh_width == 2 else 2, builder=builder)
+            tail_paths=tail_paths, max_leaf=1 if bvh_width == 2 else 2, builder=builder, ray_sort=ray_sort)
     info = renderer.accel_info()
     print("accel", info)
     assert info["width"] == bvh_width and info["builder"] == builder
@@ -431,10 +433,11 @@ def test_tuning_roundtrip_and_validation(renderer):
     renderer.set_tuning(2, 2, 8, 35, 1, 4096, 1, 7)
     assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
                                  "sortShading": 1, "tailPaths": 4096, "bvhBuilder": 1, "plocRadius": 7,
-                                 "overlapConnect": 1, "wideCollapse": 1}
+                                 "overlapConnect": 1, "wideCollapse": 1, "raySortBits": 0, "raySortBounces": 4}
     for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2),
                 (1, 3, 8, 20, 1, -1), (1, 3, 8, 20, 1, 0, 2), (1, 3, 8, 20, 1, 0, 1, 0), (1, 3, 8, 20, 1, 0, 1, 33),
-                (1, 3, 8, 20, 1, 0, 1, 16, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 2)]:
+                (1, 3, 8, 20, 1, 0, 1, 16, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 5),
+                (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 2, 0)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
@@ -466,6 +469,30 @@ def test_overlapped_connect_matches_serial_stages(renderer, random_scene, use_gr
         assert np.array_equal(bits(o[0]), bits(out[0][0]))
         assert np.array_equal(o[1], out[0][1])
         assert np.array_equal(bits(o[2]), bits(out[0][2]))
+    renderer.set_tuning()
+
+
+@pytest.mark.parametrize("nbits,use_graph", [(1, 0), (3, 1), (4, 1)])
+def test_ray_sort_keeps_bits(renderer, cornell_scene, nbits, use_graph):
+    """Reordering the queues of bounces 1-4 by ray bin (direction octant, origin cell) before extend leaves
+    every per-sample radiance, the accumulation and the ray counts bit-identical (256x256 x 2 paths per
+    pixel: every reordered bounce holds more than the 32768 rays the reordering starts at)."""
+    sc = cornell_scene
+    W, H = sc.width, sc.height
+    out = {}
+    for key in (0, nbits):
+        _upload(renderer, sc, env_mode=0, spp=2, depth=8, sort_shading=1, ray_sort=key)
+        renderer.set_config(samples_per_frame=2, max_depth=8, rr_start=3, env_sampling=0, use_graph=use_graph)
+        renderer.reset_accumulation(W, H)
+        for _ in range(2):
+            renderer.render(W, H)
+        st = renderer.stats()
+        out[key] = (renderer.read_sample_radiance(W * H * 2).copy(), renderer.read_accum(W, H).copy(), st.extends,
+                    st.shadowRays)
+        assert renderer.tuning()["raySortBits"] == key
+    assert np.array_equal(bits(out[0][0]), bits(out[nbits][0]))
+    assert np.array_equal(bits(out[0][1]), bits(out[nbits][1]))
+    assert out[0][2:] == out[nbits][2:]
     renderer.set_tuning()
 
 
@@ -622,20 +649,24 @@ def test_megakernel_features_and_denoiser(renderer, bte, cornell_scene):
         renderer.set_render_mode(1)
 
 
-def test_batched_views_match_single_view_frames(renderer, bte, random_scene):
-    """Three views of uneven size and samples per frame rendered in one launch sequence, two frames: each
-    view's FP32 mean and FP64 sum equal those of bte_render with that camera, bit for bit."""
+@pytest.mark.parametrize("sizes,frames", [([(64, 48, 1), (40, 30, 2), (100, 20, 3)], 2),
+                                          ([(64, 48, 4), (40, 30, 24), (100, 20, 64)], 4)])
+def test_batched_views_match_single_view_frames(renderer, bte, random_scene, sizes, frames):
+    """Three views of uneven size and samples per frame rendered in one launch sequence: each view's FP32 mean
+    and FP64 sum equal those of bte_render with that camera, bit for bit.  The second case accumulates the views
+    to 16, 96 and 256 samples per pixel (4 frames of 4, 24 and 64), inside the 16-256 range the batched
+    configuration draws from."""
     sc = random_scene
     base = np.asarray(sc.camera, dtype=bte.CAMERA_DTYPE).copy()
     views = []
-    for k, (w, h, spp) in enumerate([(64, 48, 1), (40, 30, 2), (100, 20, 3)]):
+    for k, (w, h, spp) in enumerate(sizes):
         cam = base.copy()
         cam["origin"] = cam["origin"] + np.float32(0.4 * k) * cam["right"]
         cam["aspect"] = np.float32(w / h)
         views.append((cam, w, h, spp))
     _upload(renderer, sc, env_mode=1, spp=1, depth=10)
     renderer.reset_views()
-    for _ in range(2):
+    for _ in range(frames):
         renderer.render_views(views)
     batched = [renderer.read_view_accum(i, w, h) for i, (_, w, h, _) in enumerate(views)]
     st = renderer.stats()
@@ -644,7 +675,7 @@ def test_batched_views_match_single_view_frames(renderer, bte, random_scene):
         renderer.init_camera(cam)
         renderer.set_config(samples_per_frame=spp, max_depth=10, rr_start=3, env_sampling=1)
         renderer.reset_accumulation(w, h)
-        for _ in range(2):
+        for _ in range(frames):
             renderer.render(w, h)
         assert np.array_equal(bits(renderer.read_accum(w, h)), bits(bm))
         assert np.array_equal(renderer.read_accum_f64(w, h).view(np.uint64), bs.view(np.uint64))
