@@ -622,8 +622,8 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
     long long paths64 = 0, pixels64 = 0;
     for (int v = 0; v < count; ++v) {
         const BteView& in = views[v];
-        if (in.width <= 0 || in.height <= 0 || in.samplesPerFrame <= 0)
-            throw CudaError{"bte_render_views: view sizes and samplesPerFrame must be positive"};
+        if (in.width <= 0 || in.height <= 0 || in.samplesPerFrame < 0)
+            throw CudaError{"bte_render_views: view sizes must be positive and samplesPerFrame non-negative"};
         Renderer::ViewState& st = g.views[static_cast<size_t>(v)];
         const size_t n = static_cast<size_t>(in.width) * in.height;
         if (st.w != in.width || st.h != in.height || !st.accum.p) {   // new or resized view: fresh accumulation
@@ -647,6 +647,7 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
         pixels64 += static_cast<long long>(n);
         if (paths64 > (1LL << 30)) throw CudaError{"bte_render_views: too many paths per frame (sum W*H*spp > 2^30)"};
     }
+    if (paths64 == 0) throw CudaError{"bte_render_views: every view has samplesPerFrame 0"};
     const int paths = static_cast<int>(paths64);
     ensureWavefront(paths, slots, depth);
     const int block = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;

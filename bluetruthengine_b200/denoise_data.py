@@ -62,15 +62,17 @@ def render_pair(r, scene, spp_in, spp_target, depth=8):
 
 
 def make_dataset(r, scene_paths, spp_in_choices=(2, 4, 8, 16, 32), spp_target=2048, depth=8, seed=0, log=None):
+    """Pairs for every scene; `scene_paths` holds paths (rendered at `depth`) or (path, depth) pairs."""
     from . import load_scene
     rng = np.random.default_rng(seed)
     N = len(scene_paths)
     out = None
     t0 = time.perf_counter()
     for i, p in enumerate(scene_paths):
+        p, d = (p, depth) if isinstance(p, str) else p
         sc = load_scene(p)
         spp_in = int(rng.choice(spp_in_choices))
-        noisy, feat, target = render_pair(r, sc, spp_in, spp_target, depth)
+        noisy, feat, target = render_pair(r, sc, spp_in, spp_target, d)
         if out is None:
             H, W = noisy.shape[:2]
             out = (np.empty((N, H, W, 3), np.float32), np.empty((N, H, W, 6), np.float32), np.empty((N, H, W, 3), np.float32))

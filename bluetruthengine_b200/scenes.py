@@ -446,6 +446,85 @@ def c4_scene(seed: int, width: int = 256, height: int = 256) -> str:
     return path
 
 
+def _outdoor_assets() -> str:
+    """Shared assets of the outdoor denoiser training scenes: icospheres, a ground plane and four skies
+    (sun elevations 12, 30, 50 and 70 degrees, sun radius 0.5-1.5 degrees, 1024x512)."""
+    d = os.path.join(CACHE_ROOT, "outdoor_assets_v%d" % GENERATOR_VERSION)
+    os.makedirs(d, exist_ok=True)
+    if _done(d):
+        return d
+    for lvl in (2, 3, 4):
+        v, f = icosphere(lvl)
+        write_obj(os.path.join(d, "ico%d.obj" % lvl), v, f, normals=v)
+    gv, gf = grid_plane(24, 25.0)
+    write_obj(os.path.join(d, "ground.obj"), gv, gf)
+    for k, (el, rad) in enumerate([(12.0, 1.5), (30.0, 1.0), (50.0, 0.5), (70.0, 0.75)]):
+        write_hdr(os.path.join(d, "sky%d.hdr" % k), sky_env(1024, 512, sun_elev_deg=el, sun_radius_deg=rad))
+    _mark(d)
+    return d
+
+
+def outdoor_scene(seed: int, width: int = 256, height: int = 256) -> str:
+    """Denoiser training scene of the outdoor kind (the 1080p Disney/env-map view and the large scene's
+    materials): 6-20 spheres on a Disney ground under one of four procedural skies (random rotation and
+    intensity), each sphere Disney (baseColor U[0,1]^3, roughness U[0.05,1], metallic Bernoulli(0.3),
+    specular 0.5, clearcoat U[0,1]; 55%), microfacet (alpha U[0.01,0.5]; 15%), mirror (15%) or dielectric
+    (IOR U[1.3,1.8]; 15%); camera at a random azimuth, distance and height looking into the group.
+    Returns the XML path."""
+    d = _outdoor_assets()
+    path = os.path.join(d, "outdoor_%d_%dx%d.xml" % (seed, width, height))
+    if os.path.exists(path):
+        return path
+    rng = np.random.default_rng(2_000_029 * seed + 5)
+    g = rng.uniform(0.3, 0.7)
+    bs = ['<bsdf name="groundB" type="disney" base_colorR="%s" base_colorG="%s" base_colorB="%s" roughness="%s" '
+          'metallic="0" specular="0.5" clearcoat="0" />' % (_fmt(g), _fmt(g * rng.uniform(0.9, 1.1)),
+                                                            _fmt(g * rng.uniform(0.8, 1.1)), _fmt(rng.uniform(0.3, 0.9)))]
+    mats = ['<material name="groundM" bsdf="groundB" />']
+    meshes = ['<mesh filename="ground.obj" material="groundM" />']
+    for i in range(int(rng.integers(6, 21))):
+        r = rng.uniform(0.3, 2.5)
+        x, z = rng.uniform(-12.0, 12.0, size=2)
+        kind = rng.uniform()
+        if kind < 0.55:
+            bc = rng.uniform(0.0, 1.0, size=3)
+            bs.append('<bsdf name="s%dB" type="disney" base_colorR="%s" base_colorG="%s" base_colorB="%s" '
+                      'roughness="%s" metallic="%s" specular="0.5" clearcoat="%s" />'
+                      % (i, _fmt(bc[0]), _fmt(bc[1]), _fmt(bc[2]), _fmt(rng.uniform(0.05, 1.0)),
+                         _fmt(1.0 if rng.uniform() < 0.3 else 0.0), _fmt(rng.uniform(0.0, 1.0))))
+        elif kind < 0.70:
+            c = rng.uniform(0.05, 0.8, 3)
+            bs.append('<bsdf name="s%dB" type="microfacet" albedoR="%s" albedoG="%s" albedoB="%s" alpha="%s" '
+                      'intIOR="1.5" extIOR="1.0" />' % (i, _fmt(c[0]), _fmt(c[1]), _fmt(c[2]),
+                                                        _fmt(rng.uniform(0.01, 0.5))))
+        elif kind < 0.85:
+            c = rng.uniform(0.6, 0.95, 3)
+            bs.append('<bsdf name="s%dB" type="mirror" albedoR="%s" albedoG="%s" albedoB="%s" />'
+                      % (i, _fmt(c[0]), _fmt(c[1]), _fmt(c[2])))
+        else:
+            bs.append('<bsdf name="s%dB" type="dielectric" intIOR="%s" extIOR="1.0" />' % (i, _fmt(rng.uniform(1.3, 1.8))))
+        mats.append('<material name="s%dM" bsdf="s%dB" />' % (i, i))
+        meshes.append('<mesh filename="ico%d.obj" material="s%dM" scaleX="%s" scaleY="%s" scaleZ="%s" posX="%s" '
+                      'posY="%s" posZ="%s" />' % (int(rng.integers(2, 5)), i, _fmt(r), _fmt(r), _fmt(r), _fmt(x), _fmt(r),
+                                                  _fmt(z)))
+    az = rng.uniform(0, 2 * np.pi)
+    dist = rng.uniform(14.0, 34.0)
+    eye = (dist * np.cos(az), rng.uniform(1.5, 14.0), dist * np.sin(az))
+    tgt = (rng.uniform(-4, 4), rng.uniform(0.0, 2.0), rng.uniform(-4, 4))
+    xml = "<scene>\n    " + "\n    ".join(bs + mats + meshes) + "\n"
+    xml += '    <environment map="sky%d.hdr" intensity="%s" rotation="%s" />\n' % (
+        int(rng.integers(0, 4)), _fmt(rng.uniform(0.5, 2.0)), _fmt(rng.uniform(0.0, 360.0)))
+    xml += '    <window width="%d" height="%d" />\n' % (width, height)
+    xml += ('    <camera eyeX="%s" eyeY="%s" eyeZ="%s" lookAtX="%s" lookAtY="%s" lookAtZ="%s" upX="0" upY="1" upZ="0" '
+            'fovY="%s" />\n</scene>\n' % (_fmt(eye[0]), _fmt(eye[1]), _fmt(eye[2]), _fmt(tgt[0]), _fmt(tgt[1]),
+                                            _fmt(tgt[2]), _fmt(rng.uniform(30.0, 60.0))))
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        f.write(xml)
+    os.replace(tmp, path)
+    return path
+
+
 def blob_mesh(seed: int, nu: int = 125, nv: int = 100):
     """Seeded closed mesh of exactly 2*nu*nv triangles: a torus of random proportions whose surface is
     displaced along its normal by a few random low-frequency harmonics.  Returns (verts, faces, normals)."""

@@ -4,7 +4,9 @@
         --out bluetruthengine_b200/weights/denoiser_c4.npz
 
 Training scenes are the seeded Cornell-box variants of `scenes.c4_scene` (wall colours, light, boxes,
-1-3 dielectric spheres with IOR U[1.3, 1.8], an occasional mirror or microfacet sphere) at 256x256;
+1-3 dielectric spheres with IOR U[1.3, 1.8], an occasional mirror or microfacet sphere) and, with
+--outdoor, sky-lit sphere groups of `scenes.outdoor_scene` (Disney, microfacet, mirror and dielectric
+spheres under a procedural sky with a sun), all at 256x256;
 inputs mix 2-32 spp so that one network serves several noise levels; targets are independent
 FP64-accumulated long runs.  Weights are stored as float16 (`params`) with the training record.
 """
@@ -21,10 +23,12 @@ import numpy as np
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--scenes", type=int, default=512)
+    ap.add_argument("--scenes", type=int, default=512, help="Cornell-box scenes (scenes.c4_scene)")
+    ap.add_argument("--outdoor", type=int, default=0, help="outdoor sky-lit scenes (scenes.outdoor_scene)")
     ap.add_argument("--first-seed", type=int, default=1000)
     ap.add_argument("--spp-target", type=int, default=2048)
-    ap.add_argument("--depth", type=int, default=8)
+    ap.add_argument("--depth", type=int, default=8, help="max depth of the Cornell-box scenes")
+    ap.add_argument("--outdoor-depth", type=int, default=16)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--crop", type=int, default=128)
@@ -39,7 +43,10 @@ def main(argv=None):
     from bluetruthengine_b200.denoiser import Denoiser
     log = lambda m: print(m, flush=True)
     r = bte.Renderer()
-    paths = [scenes.c4_scene(args.first_seed + i) for i in range(args.scenes)]
+    paths = [(scenes.c4_scene(args.first_seed + i), args.depth) for i in range(args.scenes)]
+    paths += [(scenes.outdoor_scene(args.first_seed + i), args.outdoor_depth) for i in range(args.outdoor)]
+    order = np.random.default_rng(args.seed).permutation(len(paths))   # interleave the two kinds
+    paths = [paths[i] for i in order]
     t0 = time.perf_counter()
     noisy, feat, target = make_dataset(r, paths, spp_target=args.spp_target, depth=args.depth, seed=args.seed, log=log)
     t_data = time.perf_counter() - t0
@@ -58,7 +65,8 @@ def main(argv=None):
         log("step %d loss %.5f (%.1f ms / step)" % (s + k, float(np.mean(l[-50:])), dn.last_ms() / k))
     t_train = time.perf_counter() - t1
     p = dn.params()
-    rec = {"scenes": args.scenes, "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
+    rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth,
+           "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
            "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
            "seconds_data": t_data, "seconds_train": t_train, "loss_first": float(np.mean(losses[:50])),
            "loss_last": float(np.mean(losses[-50:]))}

@@ -101,7 +101,7 @@ int bte_render(int imageWidth, int imageHeight);                                
 typedef struct {
     CameraData camera;
     int width, height;
-    int samplesPerFrame;
+    int samplesPerFrame;   /* 0: the view is idle this frame (its accumulation is kept); not all views may be 0 */
 } BteView;
 int bte_render_views(const BteView* views, int count);            /* at most 64 views */
 int bte_read_view_accum(int view, float* hostRGB, double* hostRGBSum);   /* W*H*3 each; either may be NULL */

@@ -682,6 +682,42 @@ def test_batched_views_match_single_view_frames(renderer, bte, random_scene, siz
     renderer.reset_views()
 
 
+def test_batched_views_accumulate_to_their_own_spp(renderer, bte, random_scene):
+    """Views drawn to different sample counts (16, 40 and 24 per pixel) in one batch: each frame renders every
+    unfinished view with up to 8 samples per pixel and leaves finished views idle (samplesPerFrame 0); the
+    views' FP32 means and FP64 sums equal bte_render of the same camera over the same samples, bit for bit, and
+    the frame counters show the idle frames added nothing."""
+    sc = random_scene
+    views = _views_of(bte, sc, [(64, 48, 8), (40, 30, 8), (100, 20, 8)])
+    targets = [16, 40, 24]
+    _upload(renderer, sc, env_mode=1, spp=1, depth=10)
+    renderer.set_config(samples_per_frame=1, max_depth=10, rr_start=3, env_sampling=1, use_graph=1)
+    renderer.reset_views()
+    done = [0, 0, 0]
+    while any(d < t for d, t in zip(done, targets)):
+        frame = []
+        for k, (cam, w, h, _) in enumerate(views):
+            spf = min(8, targets[k] - done[k])
+            frame.append((cam, w, h, spf))
+            done[k] += spf
+        renderer.render_views(frame)
+        assert renderer.stats().samples == sum(w * h * spf for _, w, h, spf in frame)
+    batched = [renderer.read_view_accum(i, w, h) for i, (_, w, h, _) in enumerate(views)]
+    import bluetruthengine_b200 as B
+    with pytest.raises(B.BteError):
+        renderer.render_views([(cam, w, h, 0) for cam, w, h, _ in views])
+    renderer.reset_views()
+    renderer.set_config(samples_per_frame=8, max_depth=10, rr_start=3, env_sampling=1, use_graph=1)
+    for (cam, w, h, _), target, (bm, bs) in zip(views, targets, batched):
+        renderer.init_camera(cam)
+        renderer.reset_accumulation(w, h)
+        for _ in range(target // 8):
+            renderer.render(w, h)
+        assert renderer.frame_index() == target
+        assert np.array_equal(bits(renderer.read_accum(w, h)), bits(bm))
+        assert np.array_equal(renderer.read_accum_f64(w, h).view(np.uint64), bs.view(np.uint64))
+
+
 def _views_of(bte, scene, sizes):
     base = np.asarray(scene.camera, dtype=bte.CAMERA_DTYPE).copy()
     views = []
