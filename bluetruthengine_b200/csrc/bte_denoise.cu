@@ -607,6 +607,33 @@ int bte_denoiser_set_tcgen05(int mode)
     });
 }
 
+// The failure path of the tensor-core kernels' pipeline waits, exercised without a fault: a wait on a barrier
+// that nothing completes gives up after about two seconds; the status and duration come back to the host and
+// the context stays usable.
+int bte_denoiser_debug_wait_timeout(unsigned int* status, double* seconds)
+{
+    return guardedDn([&] {
+        ensureNet();
+        Buf b;
+        b.ensure(16);
+        ck(cudaMemsetAsync(b.p, 0, 16, net.stream), "cudaMemsetAsync");
+        waitTimeoutProbe(b.as<unsigned int>(), reinterpret_cast<unsigned long long*>(b.as<unsigned char>() + 8),
+                         net.stream);
+        ck(cudaGetLastError(), "probe launch");
+        unsigned char host[16];
+        ck(cudaMemcpyAsync(host, b.p, 16, cudaMemcpyDeviceToHost, net.stream), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(net.stream), "sync");
+        b.release();
+        unsigned int st = 0;
+        unsigned long long ns = 0;
+        std::memcpy(&st, host, 4);
+        std::memcpy(&ns, host + 8, 8);
+        if (status) *status = st;
+        if (seconds) *seconds = static_cast<double>(ns) * 1e-9;
+        return 0;
+    });
+}
+
 int bte_denoiser_last_ms(float* ms)
 {
     return guardedDn([&] {

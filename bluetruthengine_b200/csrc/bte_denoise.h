@@ -34,6 +34,9 @@ size_t convTcRowScratchBytes(int C1, int C2, bool up, int Cout, int N, int H, in
 bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,
                   const float* bias, int Cout, bool relu, void* Y, void* scratch, void* pool, unsigned int* errorFlag,
                   cudaStream_t st);
+// Runs the tcgen05 kernels' bounded pipeline wait on an mbarrier that nothing completes (one warp):
+// *dStatus 2 when the wait gave up, 1 if it returned as completed; *dNs its duration.
+void waitTimeoutProbe(unsigned int* dStatus, unsigned long long* dNs, cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);

@@ -50,8 +50,24 @@ constexpr int kTcMaxN = 256;
 constexpr int kStageABytes = kTcM * kTcKStage * 2;           // 16 KB
 constexpr int kStageBBytes = kTcMaxN * kTcKStage * 2;        // 32 KB
 constexpr unsigned kSpinLimit = 1u << 26;
+// A pipeline wait that lasts this long has failed (a stage waits microseconds): the waits below give up after
+// this much time, or after their iteration limit, whichever comes first, and the kernel reports an error.
+constexpr unsigned long long kWaitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ unsigned long long globalNs()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// true once kWaitNs have passed since the first call of a wait (t0 starts at 0)
+__device__ __forceinline__ bool waitExpired(unsigned long long& t0)
+{
+    const unsigned long long t = globalNs();
+    if (t0 == 0) { t0 = t; return false; }
+    return t - t0 > kWaitNs;
+}
 
 __device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, bool valid)
 {
@@ -69,6 +85,7 @@ __device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count)
 // bounded wait for the phase with the given parity; false on timeout
 __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity)
 {
+    unsigned long long t0 = 0;
     for (unsigned i = 0; i < kSpinLimit; ++i) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\t"
@@ -77,6 +94,7 @@ __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity)
                      : "=r"(done)
                      : "r"(bar), "r"(parity));
         if (done) return true;
+        if ((i & 1023u) == 1023u && waitExpired(t0)) return false;
     }
     return false;
 }
@@ -320,6 +338,7 @@ constexpr unsigned kRowSpin = 1u << 24;
 
 __device__ __forceinline__ bool mbarWaitRow(uint32_t bar, uint32_t parity, volatile int* abortFlag)
 {
+    unsigned long long t0 = 0;
     for (unsigned i = 0; i < kRowSpin; ++i) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\t"
@@ -328,9 +347,30 @@ __device__ __forceinline__ bool mbarWaitRow(uint32_t bar, uint32_t parity, volat
                      : "=r"(done)
                      : "r"(bar), "r"(parity));
         if (done) return true;
-        if ((i & 1023u) == 1023u && *abortFlag) return false;
+        if ((i & 1023u) == 1023u && (*abortFlag || waitExpired(t0))) return false;
     }
     return false;
+}
+
+// A wait that nothing completes: one warp initialises an mbarrier that no thread arrives at and waits on its
+// first phase with the row-tile kernel's bounded wait.  The wait must give up (status 2) in about kWaitNs
+// instead of hanging; status 1 would mean it returned as if completed.  Elapsed time in ns to *ns.
+__global__ void kWaitTimeoutProbe(unsigned int* status, unsigned long long* ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abortFlag;
+    if (threadIdx.x == 0) {
+        mbarInit(smemAddr(&bar), 1);
+        abortFlag = 0;
+    }
+    __syncthreads();
+    const unsigned long long t0 = globalNs();
+    const bool done = mbarWaitRow(smemAddr(&bar), 0u, &abortFlag);
+    const unsigned long long t1 = globalNs();
+    if (threadIdx.x == 0) {
+        *status = done ? 1u : 2u;
+        *ns = t1 - t0;
+    }
 }
 
 __device__ __forceinline__ void mbarArrive(uint32_t bar)
@@ -732,6 +772,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
             }
             // whatever happened, the last MMAs must be done before the tensor memory is freed
             if (issued && !mbarWaitRow(smemAddr(&accFull[lastA]), static_cast<uint32_t>(lastRound & 1), &abortFlag)) {
+                unsigned long long t0 = 0;
                 for (unsigned s = 0; s < kRowSpin; ++s) {   // on abort, wait on (bounded) without the abort exit
                     uint32_t done;
                     asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -739,6 +780,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
                                  : "=r"(done)
                                  : "r"(smemAddr(&accFull[lastA])), "r"(static_cast<uint32_t>(lastRound & 1)));
                     if (done) break;
+                    if ((s & 1023u) == 1023u && waitExpired(t0)) break;
                 }
             }
         }
@@ -1118,6 +1160,11 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
         }
     }
     return pooled;
+}
+
+void waitTimeoutProbe(unsigned int* dStatus, unsigned long long* dNs, cudaStream_t st)
+{
+    kWaitTimeoutProbe<<<1, 32, 0, st>>>(dStatus, dNs);
 }
 
 }  // namespace dn

@@ -94,6 +94,14 @@ class Denoiser:
         upsampled beforehand; 3 the same with the upsampling done inside the row-tile kernel."""
         self._ck(self.lib.bte_denoiser_set_tcgen05(int(mode)))
 
+    def debug_wait_timeout(self):
+        """Run the tensor-core kernels' bounded wait on a barrier nothing completes: (status, seconds), status 2
+        when the wait gave up as designed."""
+        st = C.c_uint()
+        sec = C.c_double()
+        self._ck(self.lib.bte_denoiser_debug_wait_timeout(C.byref(st), C.byref(sec)))
+        return st.value, sec.value
+
     def last_ms(self) -> float:
         ms = C.c_float()
         self._ck(self.lib.bte_denoiser_last_ms(C.byref(ms)))

@@ -190,6 +190,10 @@ int bte_denoiser_set_dataset(const float* noisy, const float* features, const fl
 int bte_denoiser_train(int steps, int batch, int crop, float learningRate, uint64_t seed, float* lossPerStep);
 int bte_denoiser_denoise(const float* radiance, const float* features, int width, int height, float* out);
 int bte_denoiser_last_ms(float* ms);                             /* device time of the last denoise / train call */
+/* The tensor-core kernels' bounded pipeline wait on a barrier that nothing completes: *status 2 when the wait
+ * gave up as designed (after about two seconds; the context stays usable), 1 if it returned as completed;
+ * *seconds its duration.  A check of the failure path without a fault. */
+int bte_denoiser_debug_wait_timeout(unsigned int* status, double* seconds);
 int bte_denoiser_set_tcgen05(int mode);   /* conv kernels: 0 warp-level MMA, 1 tcgen05 pixel tiles, 2 row tiles (default), 3 row tiles upsampling in-kernel */
 int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float* bias, const float* dy, int n, int h,
                             int w_, int cin, int cout, int relu, float* out);

@@ -260,3 +260,22 @@ def test_inference_replay_across_sizes(dn):
     back = dn.denoise(*a)           # first size again
     back2 = dn.denoise(*a)          # and replayed
     assert np.array_equal(first, again) and np.array_equal(first, back) and np.array_equal(first, back2)
+
+
+def test_pipeline_wait_gives_up_and_context_survives(dn):
+    """The failure path of the tensor-core kernels' pipeline waits, without a fault: a bounded wait on an mbarrier
+    that nothing completes gives up (status 2) after about two seconds instead of hanging, and the device is
+    still usable afterwards: the row-tile convolution then matches its result from before the probe bit for bit."""
+    rng = np.random.default_rng(9)
+    shape = (1, 16, 64, 16, 32)
+    n, h, w, cin, cout = shape
+    x = rng.normal(size=(n, h, w, cin)).astype(np.float32)
+    wt = (rng.normal(size=(9, cout, cin)) * 0.1).astype(np.float32)
+    b = rng.normal(size=cout).astype(np.float32)
+    before = dn.debug_conv(5, x=x, w=wt, bias=b, shape=shape)
+    status, seconds = dn.debug_wait_timeout()
+    print("wait gave up after", seconds, "s, status", status)
+    assert status == 2
+    assert 1.0 <= seconds < 30.0
+    after = dn.debug_conv(5, x=x, w=wt, bias=b, shape=shape)
+    assert np.array_equal(before.view(np.uint32), after.view(np.uint32))
