@@ -103,6 +103,7 @@ struct Renderer {
     int plocRadius = 4;       // PLOC neighbour search radius (measured on the 1080p scene: 4 best of 4/6/8/12/16/32)
     int builtBuilder = 0;     // hierarchy in use
     int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
+    int leafTestsPerStep = 0; // 8-wide walk: triangle tests per step (0: all of a node's leaves at once)
     int raySortBits = 0;      // ray reordering before extend: origin cell bits per axis (0: off)
     int raySortBounces = 4;   // bounces 1..raySortBounces are reordered
     bool sceneChanged = false;   // bte_mark_scene_changed: the next bte_render resets accumulation first
@@ -220,6 +221,7 @@ DevScene makeDevScene()
     s.bvhWidth = g.builtWidth;
     s.wideNodeCount = g.builtWidth == 8 ? g.accelNodes : 0;
     s.postponePct = g.postponePct;
+    s.leafTestsPerStep = g.leafTestsPerStep;
     s.rootIsLeaf = g.rootIsLeaf;
     s.rootCode = g.rootCode;
     s.sceneMaxAbs = g.sceneMaxAbs;
@@ -1459,6 +1461,8 @@ int bte_set_tuning(const BteTuning* t)
         if (t->wideCollapse != 0 && t->wideCollapse != 1) throw CudaError{"bte_set_tuning: wideCollapse must be 0 or 1"};
         if (t->raySortBits < 0 || t->raySortBits > 4) throw CudaError{"bte_set_tuning: raySortBits in [0, 4]"};
         if (t->raySortBounces < 1 || t->raySortBounces > 64) throw CudaError{"bte_set_tuning: raySortBounces in [1, 64]"};
+        if (t->leafTestsPerStep < 0 || t->leafTestsPerStep > 24)
+            throw CudaError{"bte_set_tuning: leafTestsPerStep in [0, 24]"};
         g.bvhWidth = t->bvhWidth;
         g.maxLeaf = t->maxLeafTriangles;
         g.shadeMinBlocks = t->shadeMinBlocks;
@@ -1471,6 +1475,7 @@ int bte_set_tuning(const BteTuning* t)
         g.wideCollapse = t->wideCollapse;
         g.raySortBits = t->raySortBits;
         g.raySortBounces = t->raySortBounces;
+        g.leafTestsPerStep = t->leafTestsPerStep;
         g.gridBlock = 0;   // recompute persistent grids
         return 0;
     });
@@ -1492,6 +1497,7 @@ int bte_get_tuning(BteTuning* t)
         t->wideCollapse = g.wideCollapse;
         t->raySortBits = g.raySortBits;
         t->raySortBounces = g.raySortBounces;
+        t->leafTestsPerStep = g.leafTestsPerStep;
         return 0;
     });
 }

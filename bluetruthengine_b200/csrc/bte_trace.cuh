@@ -278,7 +278,7 @@ struct WideWalk {
     // so that the scalar state stays in registers).
     BTE_DI bool step(const DevScene& s, uint2* stack, unsigned int* errorFlags)
     {
-        if (nBits >> 8) {
+        if (tHits == 0u && (nBits >> 8)) {
             const uint32_t hits = nBits >> 8;
             const uint32_t key = static_cast<uint32_t>(__ffs(hits) - 1);
             const uint32_t rest = hits & (hits - 1u);
@@ -358,6 +358,9 @@ struct WideWalk {
                 tHits = 0;
             }
         }
+        // leaf tests: all of them, or at most s.leafTestsPerStep per step (the rest wait for the next steps,
+        // which fetch no node until they are done), so that lanes with many triangles hold the warp less long
+        int budget = s.leafTestsPerStep;
         while (tHits) {
             const int k = __ffs(tHits) - 1;
             tHits &= tHits - 1u;
@@ -373,8 +376,9 @@ struct WideWalk {
                 const int idx = __float_as_int(a.w);
                 if (best < 0 || t < bt || (t == bt && idx < best)) { best = idx; bt = t; bu = u; bv = v; }
             }
+            if (--budget == 0) break;
         }
-        if ((nBits >> 8) == 0u) {
+        if (tHits == 0u && (nBits >> 8) == 0u) {
             if (sp == 0) return true;
             const uint2 e = stack[--sp];
             if (e.y & kTriGroup) {   // a deferred leaf group: test it next, with no node work pending

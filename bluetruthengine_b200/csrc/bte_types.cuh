@@ -76,6 +76,7 @@ struct DevScene {
     int bvhWidth;                     // 2 or 8
     int wideNodeCount;
     int postponePct;                  // leaf-test postponing threshold of the 8-wide walk (percent of lanes)
+    int leafTestsPerStep;             // 8-wide walk: triangle tests per walk step (0: all of the node's)
     int rootIsLeaf;                   // the whole scene is one leaf
     int rootCode;                     // its leaf code
     float sceneMaxAbs;                // max |coordinate| over all vertices (traversal error bound)

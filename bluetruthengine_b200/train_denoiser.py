@@ -29,6 +29,7 @@ def main(argv=None):
     ap.add_argument("--spp-target", type=int, default=2048)
     ap.add_argument("--depth", type=int, default=8, help="max depth of the Cornell-box scenes")
     ap.add_argument("--outdoor-depth", type=int, default=16)
+    ap.add_argument("--spp-in", default="2,4,8,16,32", help="input sample counts drawn per scene")
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--crop", type=int, default=128)
@@ -48,7 +49,9 @@ def main(argv=None):
     order = np.random.default_rng(args.seed).permutation(len(paths))   # interleave the two kinds
     paths = [paths[i] for i in order]
     t0 = time.perf_counter()
-    noisy, feat, target = make_dataset(r, paths, spp_target=args.spp_target, depth=args.depth, seed=args.seed, log=log)
+    spp_in = tuple(int(x) for x in args.spp_in.split(","))
+    noisy, feat, target = make_dataset(r, paths, spp_in_choices=spp_in, spp_target=args.spp_target, depth=args.depth,
+                                       seed=args.seed, log=log)
     t_data = time.perf_counter() - t0
     dn = Denoiser()
     dn.init(args.seed)
@@ -65,7 +68,7 @@ def main(argv=None):
         log("step %d loss %.5f (%.1f ms / step)" % (s + k, float(np.mean(l[-50:])), dn.last_ms() / k))
     t_train = time.perf_counter() - t1
     p = dn.params()
-    rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth,
+    rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth, "spp_in": list(spp_in),
            "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
            "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
            "seconds_data": t_data, "seconds_train": t_train, "loss_first": float(np.mean(losses[:50])),

@@ -165,6 +165,9 @@ typedef struct {
                             * (raySortBits bits per axis of the scene's bounding cube), so a warp traces nearby
                             * rays of one octant; results do not depend on it */
     int raySortBounces;    /* last bounce reordered, 1-64 */
+    int leafTestsPerStep;  /* 8-wide walk: 0 tests all triangles of a node's hit leaves in the step that fetched
+                            * the node; 1-24 tests at most that many per step and fetches the next node only
+                            * when they are done (lanes with many triangles hold their warp less long) */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);

@@ -52,9 +52,10 @@ def test_math_functions_bitexact(renderer, oracle_mod):
 
 
 def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0,
-            builder=1, radius=8, collapse=1, ray_sort=0):
+            builder=1, radius=8, collapse=1, ray_sort=0, leaf_tests=0):
     renderer.cleanup()
-    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius, 1, collapse, ray_sort)
+    renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius, 1, collapse, ray_sort, 4,
+                        leaf_tests)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
@@ -269,20 +270,22 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder,ray_sort",
-                         [(1, 8, 0, 0, 0, 0), (0, 8, 0, 0, 0, 0), (1, 2, 0, 0, 0, 0), (1, 8, 1, 0, 0, 0),
-                          (1, 8, 1, 200000, 0, 0), (1, 8, 1, 0, 1, 0), (0, 2, 0, 0, 1, 0), (1, 8, 1, 0, 1, 3),
-                          (1, 2, 0, 0, 1, 2)])
+@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder,ray_sort,leaf_tests",
+                         [(1, 8, 0, 0, 0, 0, 0), (0, 8, 0, 0, 0, 0, 0), (1, 2, 0, 0, 0, 0, 0), (1, 8, 1, 0, 0, 0, 0),
+                          (1, 8, 1, 200000, 0, 0, 0), (1, 8, 1, 0, 1, 0, 0), (0, 2, 0, 0, 1, 0, 0), (1, 8, 1, 0, 1, 3, 0),
+                          (1, 2, 0, 0, 1, 2, 0), (1, 8, 1, 0, 1, 3, 1), (0, 8, 1, 0, 1, 0, 2)])
 def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading, tail_paths,
-                                     builder, ray_sort):
+                                     builder, ray_sort, leaf_tests):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
     pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit; with and without the rays of
-    bounces 1-4 reordered by direction octant and origin cell."""
+    bounces 1-4 reordered by direction octant and origin cell, and with the 8-wide walk's triangle tests
+    spread over steps (1 or 2 per step)."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
     _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading,
-            tail_paths=tail_paths, max_leaf=1 if bvh_width == 2 else 2, builder=builder, ray_sort=ray_sort)
+            tail_paths=tail_paths, max_leaf=1 if bvh_width == 2 else 2, builder=builder, ray_sort=ray_sort,
+            leaf_tests=leaf_tests)
     info = renderer.accel_info()
     print("accel", info)
     assert info["width"] == bvh_width and info["builder"] == builder
@@ -433,11 +436,12 @@ def test_tuning_roundtrip_and_validation(renderer):
     renderer.set_tuning(2, 2, 8, 35, 1, 4096, 1, 7)
     assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
                                  "sortShading": 1, "tailPaths": 4096, "bvhBuilder": 1, "plocRadius": 7,
-                                 "overlapConnect": 1, "wideCollapse": 1, "raySortBits": 0, "raySortBounces": 4}
+                                 "overlapConnect": 1, "wideCollapse": 1, "raySortBits": 0, "raySortBounces": 4,
+                                 "leafTestsPerStep": 0}
     for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2),
                 (1, 3, 8, 20, 1, -1), (1, 3, 8, 20, 1, 0, 2), (1, 3, 8, 20, 1, 0, 1, 0), (1, 3, 8, 20, 1, 0, 1, 33),
                 (1, 3, 8, 20, 1, 0, 1, 16, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 5),
-                (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 2, 0)]:
+                (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 2, 0), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 0, 4, 25)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
