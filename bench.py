@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of replaying the frame graph")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised time-to-relMSE leg")
+    ap.add_argument("--no-large", action="store_true", help="skip the 10M-triangle 4K leg")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -540,6 +541,13 @@ def run_ours(args):
             out["denoise"] = denoise_leg()
         except Exception as e:
             out["denoise"] = {"unavailable": str(e)}
+    if rank == 0 and world == 1 and not args.no_large:
+        try:   # the large configuration: 10M triangles, 3840x2160, depth 24, 1 spp + denoise vs 1024-spp plain
+            from bluetruthengine_b200.large_eval import run as large_run
+            weights = os.path.join(ROOT, "bluetruthengine_b200", "weights", "denoiser_c4.npz")
+            out["large_scene"] = large_run(ref_spp=1024, depth=24, weights=weights, log=lambda m: None)
+        except Exception as e:
+            out["large_scene"] = {"unavailable": str(e)}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
