@@ -437,6 +437,15 @@ class Renderer:
         self._ck(self.lib.bte_get_selected_scene(C.byref(out)))
         return out.value
 
+    def set_batch_mode(self, mode: int):
+        """1: a scene batch renders in one launch sequence over every scene's paths (default); 0: per scene."""
+        self._ck(self.lib.bte_set_batch_mode(int(mode)))
+
+    def batch_mode(self) -> int:
+        out = C.c_int(0)
+        self._ck(self.lib.bte_get_batch_mode(C.byref(out)))
+        return out.value
+
     def render_scene_batch(self, batch):
         """One frame of several scene slots' views (sequence of (slot, views), views as for render_views): every
         scene's launch sequence is enqueued on its own streams before any wait, so the scenes run side by side."""

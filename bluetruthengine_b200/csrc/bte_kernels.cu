@@ -61,6 +61,15 @@ BTE_DI void sortAppend(const DevScene& s, const DevPaths& P, int bounce, int idx
 
 BTE_DI V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 
+// The scene of a path: the kernel's own scene, or -- in one launch sequence over several scenes' views
+// (DevPaths.scenes) -- the path's entry of the frame's scene table.
+template <bool Multi>
+BTE_DI const DevScene& sceneOf(const DevScene& s, const DevPaths& P, int path)
+{
+    if constexpr (Multi) return P.scenes[P.pathScene[path]];
+    else return s;
+}
+
 // Whether bounce `bounce` walks its queue in ray-bin order (same answer in shade, kRayBins, kRayScatter, extend).
 BTE_DI bool raySorted(const DevPaths& P, int bounce, int count)
 {
@@ -135,6 +144,7 @@ __global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
         frameIndex = vd.frameIndex;
         cam = &vd.cam;
         tanHalf = vd.tanHalf;
+        if (P.pathScene) P.pathScene[i] = static_cast<uint8_t>(vd.scene);
     } else {
         frameIndex = *f.frameIndex;
     }
@@ -277,7 +287,7 @@ BTE_DI bool shadePath(const DevScene& s, const DevPaths& P, const FrameParams& f
     return alive;
 }
 
-template <int MinBlocks>
+template <int MinBlocks, bool Multi>
 __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P, FrameParams f, int bounce)
 {
     const int count = P.rayCount[bounce];
@@ -302,12 +312,13 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
         } else {
             idx = q[slot];
         }
-        const bool alive = shadePath(s, P, f, bounce, idx, true);
+        const DevScene& ss = sceneOf<Multi>(s, P, idx);
+        const bool alive = shadePath(ss, P, f, bounce, idx, true);
         if (alive && bounce + 1 < P.maxDepth) {
             const int next = appendCoalesced(P.rayCount + bounce + 1);
             qn[next] = idx;
             if (P.raySortBits > 0 && bounce + 1 <= P.raySortBounces) {
-                const int bin = rayBinOf(P, s.sceneMaxAbs, P.o[idx], P.d[idx]);
+                const int bin = rayBinOf(P, ss.sceneMaxAbs, P.o[idx], P.d[idx]);
                 P.rayBin[next] = bin;
                 appendKeyed(P.binCount + static_cast<size_t>(bounce + 1) * rayBinCount(P), bin);
             }
@@ -390,6 +401,7 @@ BTE_DI bool warpNotNeeded(int count)
 // per-bounce counter) as soon as its current one ends, so that lanes do not
 // idle until the slowest ray of their warp finishes.
 // 72 registers keep 7 blocks of 128 threads resident per SM (74 would allow only 6)
+template <bool Multi>
 __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
@@ -400,16 +412,17 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
         const int g = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
         if (g >= count) return;
         const int idx = q[g];
+        const DevScene& ss = sceneOf<Multi>(s, P, idx);
         const float4 o = P.o[idx];
         const float4 d = P.d[idx];
-        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, ss.sceneMaxAbs);
         float t = 0.0f, u = 0.0f, v = 0.0f;
         int tri = -1;
-        if (r.valid && s.triCount > 0) tri = traceWideGroup<false>(s, r, kEps, 1e30f, stack, P.errorFlags, t, u, v);
+        if (r.valid && ss.triCount > 0) tri = traceWideGroup<false>(ss, r, kEps, 1e30f, stack, P.errorFlags, t, u, v);
         if ((threadIdx.x & 7u) == 0u) {
             P.hit[idx] = tri >= 0 ? make_float4(t, u, v, __int_as_float(tri)) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
             if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
-            if (P.sortQueue) sortAppend(s, P, bounce, idx, tri);
+            if (P.sortQueue) sortAppend(ss, P, bounce, idx, tri);
         }
         return;
     }
@@ -422,29 +435,32 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
             const int slot = appendCoalesced(fetch);
             if (slot >= count) break;
             idx = q[slot];
+            const DevScene& ss = sceneOf<Multi>(s, P, idx);
             const float4 o = P.o[idx];
             const float4 d = P.d[idx];
-            const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
-            if (!r.valid || s.triCount <= 0) {
+            const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, ss.sceneMaxAbs);
+            if (!r.valid || ss.triCount <= 0) {
                 P.hit[idx] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
                 if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = -1;
-                if (P.sortQueue) sortAppend(s, P, bounce, idx, -1);
+                if (P.sortQueue) sortAppend(ss, P, bounce, idx, -1);
                 idx = -1;
                 continue;
             }
             w.start(r, kEps, 1e30f);
         }
-        if (w.step(s, stack, P.errorFlags)) {
+        const DevScene& ss = sceneOf<Multi>(s, P, idx);
+        if (w.step(ss, stack, P.errorFlags)) {
             const int tri = w.best;
             P.hit[idx] = tri >= 0 ? make_float4(w.bt, w.bu, w.bv, __int_as_float(tri))
                                   : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
             if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
-            if (P.sortQueue) sortAppend(s, P, bounce, idx, tri);
+            if (P.sortQueue) sortAppend(ss, P, bounce, idx, tri);
             idx = -1;
         }
     }
 }
 
+template <bool Multi>
 __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.shadowCount[bounce];
@@ -455,12 +471,13 @@ __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int 
         if (g >= count) return;
         const int e = P.shadowQueue[g];
         const int path = e / P.slots;
+        const DevScene& ss = sceneOf<Multi>(s, P, path);
         const float4 o = P.shOrigin[path];
         const float4 d = P.shDir[e];
-        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
-        if (!r.valid || s.triCount <= 0) return;
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, ss.sceneMaxAbs);
+        if (!r.valid || ss.triCount <= 0) return;
         float t, u, v;
-        if (traceWideGroup<true>(s, r, kEps, d.w, stack, P.errorFlags, t, u, v) >= 0 && (threadIdx.x & 7u) == 0u)
+        if (traceWideGroup<true>(ss, r, kEps, d.w, stack, P.errorFlags, t, u, v) >= 0 && (threadIdx.x & 7u) == 0u)
             atomicAnd(P.shMask + path, ~(1u << (e - path * P.slots)));
         return;
     }
@@ -474,13 +491,14 @@ __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int 
             if (slot >= count) break;
             e = P.shadowQueue[slot];
             const int path = e / P.slots;
+            const DevScene& ss = sceneOf<Multi>(s, P, path);
             const float4 o = P.shOrigin[path];
             const float4 d = P.shDir[e];
-            const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
-            if (!r.valid || s.triCount <= 0) { e = -1; continue; }
+            const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, ss.sceneMaxAbs);
+            if (!r.valid || ss.triCount <= 0) { e = -1; continue; }
             w.start(r, kEps, d.w);
         }
-        if (w.step(s, stack, P.errorFlags)) {
+        if (w.step(sceneOf<Multi>(s, P, e / P.slots), stack, P.errorFlags)) {
             if (w.hit) {
                 const int path = e / P.slots;
                 atomicAnd(P.shMask + path, ~(1u << (e - path * P.slots)));
@@ -494,7 +512,7 @@ __global__ void __launch_bounds__(256) kConnectWide(DevScene s, DevPaths P, int 
 // Finishes the paths of the first bounce the wavefront left (tailTakesOver): per path, closest hit,
 // shading and its shadow rays, bounce after bounce, with the same per-path operations and counters
 // as the wavefront stages.
-template <int Width>
+template <int Width, bool Multi>
 __global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams f)
 {
     if (P.tailPaths <= 0) return;
@@ -506,16 +524,17 @@ __global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= count) return;
     const int idx = P.queue[b0 & 1][slot];
+    const DevScene& ss = sceneOf<Multi>(s, P, idx);
     for (int b = b0; b < P.maxDepth; ++b) {
         if (b > b0) atomicAdd(P.rayCount + b, 1);
         const float4 o = P.o[idx];
         const float4 d = P.d[idx];
-        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, s.sceneMaxAbs);
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, ss.sceneMaxAbs);
         float t = 0.0f, u = 0.0f, v = 0.0f;
-        const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
+        const int tri = traceClosestW<Width>(ss, r, kEps, 1e30f, t, u, v, P.errorFlags);
         P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
         if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + b] = tri;
-        const bool alive = shadePath(s, P, f, b, idx, false);
+        const bool alive = shadePath(ss, P, f, b, idx, false);
         uint32_t mask = P.shMask[idx];
         if (mask) {
             atomicAdd(P.shadowCount + b, __popc(mask));
@@ -524,8 +543,8 @@ __global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams
             for (uint32_t m = mask; m; m &= m - 1u) {
                 const int sl = __ffs(m) - 1;
                 const float4 sd = P.shDir[base + sl];
-                const RayPre sr = rayPre(so.x, so.y, so.z, sd.x, sd.y, sd.z, s.sceneMaxAbs);
-                if (traceOccludedW<Width>(s, sr, kEps, sd.w, P.errorFlags)) mask &= ~(1u << sl);
+                const RayPre sr = rayPre(so.x, so.y, so.z, sd.x, sd.y, sd.z, ss.sceneMaxAbs);
+                if (traceOccludedW<Width>(ss, sr, kEps, sd.w, P.errorFlags)) mask &= ~(1u << sl);
             }
             P.shMask[idx] = mask;
         }
@@ -860,21 +879,31 @@ void launchRaySort(const DevPaths& P, int bounce, int grid, cudaStream_t st)
     kRayBins<<<1, 1024, 0, st>>>(P, bounce);
     kRayScatter<<<grid, 256, 0, st>>>(P, bounce);
 }
+// Frames over several scenes (P.scenes) run the stage kernels' multi-scene instances; those scenes all use the
+// 8-wide tree (checked by the host).
 void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
 {
-    if (s.bvhWidth == 8) kExtendWide<<<grid, block, 0, st>>>(s, P, bounce);
+    if (P.scenes) kExtendWide<true><<<grid, block, 0, st>>>(s, P, bounce);
+    else if (s.bvhWidth == 8) kExtendWide<false><<<grid, block, 0, st>>>(s, P, bounce);
     else kExtend<2><<<grid, block, 0, st>>>(s, P, bounce);
 }
 void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block,
                  int minBlocks, cudaStream_t st)
 {
-    if (minBlocks == 4) kShade<4><<<grid, block, 0, st>>>(s, P, f, bounce);
-    else if (minBlocks == 3) kShade<3><<<grid, block, 0, st>>>(s, P, f, bounce);
-    else kShade<2><<<grid, block, 0, st>>>(s, P, f, bounce);
+    if (P.scenes) {
+        if (minBlocks == 4) kShade<4, true><<<grid, block, 0, st>>>(s, P, f, bounce);
+        else if (minBlocks == 3) kShade<3, true><<<grid, block, 0, st>>>(s, P, f, bounce);
+        else kShade<2, true><<<grid, block, 0, st>>>(s, P, f, bounce);
+        return;
+    }
+    if (minBlocks == 4) kShade<4, false><<<grid, block, 0, st>>>(s, P, f, bounce);
+    else if (minBlocks == 3) kShade<3, false><<<grid, block, 0, st>>>(s, P, f, bounce);
+    else kShade<2, false><<<grid, block, 0, st>>>(s, P, f, bounce);
 }
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st)
 {
-    if (s.bvhWidth == 8) kConnectWide<<<grid, block, 0, st>>>(s, P, bounce);
+    if (P.scenes) kConnectWide<true><<<grid, block, 0, st>>>(s, P, bounce);
+    else if (s.bvhWidth == 8) kConnectWide<false><<<grid, block, 0, st>>>(s, P, bounce);
     else kConnect<2><<<grid, block, 0, st>>>(s, P, bounce);
 }
 void launchPresentViews(const DevPaths& P, const FrameParams& f, int totalPixels, cudaStream_t st)
@@ -886,8 +915,9 @@ void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cuda
     if (P.tailPaths <= 0) return;
     const int n = P.tailPaths < P.count ? P.tailPaths : P.count;
     const int blocks = (n + 127) / 128;
-    if (s.bvhWidth == 8) kTail<8><<<blocks, 128, 0, st>>>(s, P, f);
-    else kTail<2><<<blocks, 128, 0, st>>>(s, P, f);
+    if (P.scenes) kTail<8, true><<<blocks, 128, 0, st>>>(s, P, f);
+    else if (s.bvhWidth == 8) kTail<8, false><<<blocks, 128, 0, st>>>(s, P, f);
+    else kTail<2, false><<<blocks, 128, 0, st>>>(s, P, f);
 }
 void launchMegakernel(const DevScene& s, const DevPaths& P, const FrameParams& f, float* accum, double* accumD,
                       uint32_t* fb, uint32_t* extFb, float* aovAccum, cudaStream_t st)
@@ -953,11 +983,11 @@ int occupancyGrid(int which, int block)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const void* fn = which == 0 ? reinterpret_cast<const void*>(kExtend<2>)
-                   : which == 1 ? reinterpret_cast<const void*>(kShade<2>)
-                   : which == 3 ? reinterpret_cast<const void*>(kShade<3>)
-                   : which == 6 ? reinterpret_cast<const void*>(kShade<4>)
-                   : which == 4 ? reinterpret_cast<const void*>(kExtendWide)
-                   : which == 5 ? reinterpret_cast<const void*>(kConnectWide)
+                   : which == 1 ? reinterpret_cast<const void*>(kShade<2, false>)
+                   : which == 3 ? reinterpret_cast<const void*>(kShade<3, false>)
+                   : which == 6 ? reinterpret_cast<const void*>(kShade<4, false>)
+                   : which == 4 ? reinterpret_cast<const void*>(kExtendWide<false>)
+                   : which == 5 ? reinterpret_cast<const void*>(kConnectWide<false>)
                                 : reinterpret_cast<const void*>(kConnect<2>);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0) != cudaSuccess || per < 1) per = 1;
     return sms * per;

@@ -13,6 +13,7 @@
 #include "bte_kernels.h"
 #include "bte_math.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -851,6 +852,248 @@ void renderSceneBatchGraph(const int* scenes, const int* viewCounts, const BteVi
     if (!firstError.empty()) throw CudaError{firstError};
 }
 
+// Several scenes' views as one launch sequence (the default batch mode): the scene table and the per-path scene
+// index, with the pinned staging of the scene and view tables and the captured frame.
+struct FusedBatch {
+    DeviceBuffer sceneTable, viewTable, pathScene;
+    DevScene* hScenes = nullptr;   // [kMaxScenes]
+    ViewDesc* hViews = nullptr;    // [kMaxScenes * kMaxViews]
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
+};
+FusedBatch g_fused;
+int g_batchMode = 1;   // 1: one launch sequence over every scene's paths when the scenes allow it; 0: per scene
+
+void releaseFusedGraph()
+{
+    if (g_fused.exec) cudaGraphExecDestroy(g_fused.exec);
+    if (g_fused.graph) cudaGraphDestroy(g_fused.graph);
+    g_fused.exec = nullptr;
+    g_fused.graph = nullptr;
+    g_fused.key.clear();
+}
+
+// One frame of several scenes' views in ONE launch sequence: the paths of every view of every scene are
+// concatenated (scene by scene, view by view), each path carries its scene's index (written by generate), and
+// the stage kernels take the path's geometry, tree, materials, lights and env map from the frame's scene table.
+// The first scene's slot provides the path-state buffers, the stream and the frame-level settings (max depth,
+// roulette start, block size, graph use, shading residency, material sorting, ray reordering, the shadow-ray
+// overlap and the tail threshold).  The scenes must all render in wavefront mode with the 8-wide tree and share
+// the first scene's max depth, roulette start, block size and graph use; otherwise nothing is done and false
+// comes back (the caller then runs each scene's own launch sequence).  Every scene's views accumulate exactly as
+// bte_render_views on that slot alone would leave them.
+bool renderSceneBatchFused(const int* scenes, const int* viewCounts, const BteView* views, int sceneCount,
+                           const std::vector<int>& offset, int home)
+{
+    if (g_batchMode == 0 || sceneCount < 2) return false;
+    int depth = 1, rr = 3, block = 128, useGraph = 0, slots = 1;
+    for (int i = 0; i < sceneCount; ++i) {   // eligibility first: nothing is changed unless the batch qualifies
+        selectScene(scenes[i]);
+        const int d = g.cfg.maxDepth > 0 ? g.cfg.maxDepth : 1;
+        const int b = g.cfg.blockSize > 0 ? g.cfg.blockSize : 128;
+        const bool ok = g.accelReady && g.builtWidth == 8 && g.renderMode == BTE_RENDER_WAVEFRONT &&
+                        (i == 0 || (d == depth && g.cfg.rrStart == rr && b == block && g.cfg.useGraph == useGraph));
+        if (!ok) {
+            selectScene(home);
+            return false;
+        }
+        if (i == 0) { depth = d; rr = g.cfg.rrStart; block = b; useGraph = g.cfg.useGraph; }
+    }
+    std::vector<ViewDesc> vd;
+    std::vector<long long> sceneSamples(static_cast<size_t>(sceneCount), 0);
+    DevScene table[kMaxScenes];
+    std::memset(table, 0, sizeof(table));
+    long long paths64 = 0, pixels64 = 0;
+    try {
+        for (int i = 0; i < sceneCount; ++i) {
+            selectScene(scenes[i]);
+            ensureInit();
+            if (!g.tris.p || g.triCount <= 0 || !g.bsdfs.p || !g.triBsdfIds.p || !g.emitterFlags.p)
+                throw CudaError{"bte_render_scene_batch: scene, acceleration structure, BSDFs and emitter flags must be uploaded"};
+            slots = std::max(slots, slotsFor());
+            if (slots > 32) throw CudaError{"bte_render_scene_batch: at most 30 spotlights are supported"};
+            table[i] = makeDevScene();
+            const BteView* sv = views + offset[static_cast<size_t>(i)];
+            const int count = viewCounts[i];
+            if (static_cast<int>(g.views.size()) != count) g.views.resize(static_cast<size_t>(count));
+            for (int v = 0; v < count; ++v) {
+                const BteView& in = sv[v];
+                if (in.width <= 0 || in.height <= 0 || in.samplesPerFrame < 0)
+                    throw CudaError{"bte_render_scene_batch: view sizes must be positive and samplesPerFrame non-negative"};
+                Renderer::ViewState& st = g.views[static_cast<size_t>(v)];
+                const size_t n = static_cast<size_t>(in.width) * in.height;
+                if (st.w != in.width || st.h != in.height || !st.accum.p) {   // new or resized view: fresh accumulation
+                    st.accum.release(); st.accumD.release(); st.fb.release();
+                    ensure(st.accum, n * 12); ensure(st.accumD, n * 24); ensure(st.fb, n * 4);
+                    ck(cudaMemsetAsync(st.accum.p, 0, n * 12, g.stream), "cudaMemsetAsync");
+                    ck(cudaMemsetAsync(st.accumD.p, 0, n * 24, g.stream), "cudaMemsetAsync");
+                    ck(cudaMemsetAsync(st.fb.p, 0, n * 4, g.stream), "cudaMemsetAsync");
+                    st.w = in.width; st.h = in.height; st.frameIndex = 0;
+                }
+                ViewDesc d;
+                std::memset(&d, 0, sizeof(d));
+                d.cam = in.camera;
+                d.tanHalf = m::tanf_(0.5f * in.camera.fovYRadians);
+                d.width = in.width; d.height = in.height; d.spp = in.samplesPerFrame;
+                d.frameIndex = st.frameIndex;
+                d.pathOffset = static_cast<int>(paths64);
+                d.pixelOffset = static_cast<int>(pixels64);
+                d.scene = i;
+                d.accum = st.accum.as<float>(); d.accumD = st.accumD.as<double>(); d.framebuffer = st.fb.as<uint32_t>();
+                vd.push_back(d);
+                paths64 += static_cast<long long>(n) * in.samplesPerFrame;
+                pixels64 += static_cast<long long>(n);
+                sceneSamples[static_cast<size_t>(i)] += static_cast<long long>(n) * in.samplesPerFrame;
+                if (paths64 > (1LL << 30))
+                    throw CudaError{"bte_render_scene_batch: too many paths per frame (sum W*H*spp > 2^30)"};
+            }
+            ck(cudaStreamSynchronize(g.stream), "cudaStreamSynchronize");   // new view buffers are cleared
+        }
+        if (paths64 == 0) throw CudaError{"bte_render_scene_batch: every view has samplesPerFrame 0"};
+    } catch (...) {
+        selectScene(home);
+        throw;
+    }
+    selectScene(scenes[0]);
+    const int paths = static_cast<int>(paths64), total = static_cast<int>(vd.size());
+    try {
+        ensureWavefront(paths, slots, depth);
+        if (g.gridBlock != block) {
+            g.gridExtend = occupancyGrid(4, block);
+            g.gridShade = occupancyGrid(g.shadeMinBlocks == 4 ? 6 : g.shadeMinBlocks == 3 ? 3 : 1, block);
+            g.gridConnect = occupancyGrid(5, block);
+            g.gridBlock = block;
+        }
+        ensure(g_fused.sceneTable, sizeof(DevScene) * kMaxScenes);
+        ensure(g_fused.viewTable, sizeof(ViewDesc) * kMaxScenes * kMaxViews);
+        ensure(g_fused.pathScene, static_cast<size_t>(g.pathCap));
+        if (!g_fused.hScenes)
+            ck(cudaHostAlloc(reinterpret_cast<void**>(&g_fused.hScenes), sizeof(DevScene) * kMaxScenes,
+                             cudaHostAllocDefault), "cudaHostAlloc");
+        if (!g_fused.hViews)
+            ck(cudaHostAlloc(reinterpret_cast<void**>(&g_fused.hViews), sizeof(ViewDesc) * kMaxScenes * kMaxViews,
+                             cudaHostAllocDefault), "cudaHostAlloc");
+        cudaStream_t st = g.stream;
+        std::memcpy(g_fused.hScenes, table, sizeof(DevScene) * kMaxScenes);   // the previous batch frame has finished
+        std::memcpy(g_fused.hViews, vd.data(), sizeof(ViewDesc) * vd.size());
+        ck(cudaMemcpyAsync(g_fused.sceneTable.p, g_fused.hScenes, sizeof(DevScene) * kMaxScenes, cudaMemcpyHostToDevice,
+                           st), "cudaMemcpyAsync");
+        ck(cudaMemcpyAsync(g_fused.viewTable.p, g_fused.hViews, sizeof(ViewDesc) * vd.size(), cudaMemcpyHostToDevice,
+                           st), "cudaMemcpyAsync");
+        DevPaths P;
+        std::memset(&P, 0, sizeof(P));
+        P.o = g.pO.as<float4>(); P.d = g.pD.as<float4>(); P.tp = g.pTp.as<float4>(); P.L = g.pL.as<float4>();
+        P.hit = g.pHit.as<float4>();
+        P.queue[0] = g.q0.as<int>(); P.queue[1] = g.q1.as<int>();
+        P.rayCount = g.rayCount.as<int>();
+        P.shadowCount = g.shadowCount.as<int>();
+        P.fetch = g.fetch.as<int>();
+        P.shadowQueue = g.shadowQueue.as<int>();
+        P.shOrigin = g.shOrigin.as<float4>();
+        P.shDir = g.shDir.as<float4>();
+        P.shContrib = g.shContrib.as<float4>();
+        P.shMask = g.shMask.as<uint32_t>();
+        P.slots = slots;
+        P.maxDepth = depth;
+        P.count = paths;
+        P.errorFlags = g.errorFlags.as<unsigned int>();
+        P.sortQueue = g.sortShading ? g.sortQueue.as<int>() : nullptr;
+        P.sortCount = g.sortCount.as<int>();
+        P.tailPaths = g.tailPaths;
+        setRaySort(P, true);
+        P.scenes = g_fused.sceneTable.as<DevScene>();
+        P.pathScene = g_fused.pathScene.as<uint8_t>();
+        P.sceneCount = sceneCount;
+        FrameParams f;
+        std::memset(&f, 0, sizeof(f));
+        f.frameIndex = g.dFrameIndex.as<uint32_t>();
+        f.rrStart = rr;
+        f.views = g_fused.viewTable.as<ViewDesc>();
+        f.viewCount = total;
+        const DevScene s = table[0];
+        auto body = [&] {
+            ck(cudaMemsetAsync(g.rayCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+            ck(cudaMemsetAsync(g.shadowCount.p, 0, sizeof(int) * (depth + 1), st), "cudaMemsetAsync");
+            ck(cudaMemsetAsync(g.fetch.p, 0, sizeof(int) * 2 * (depth + 1), st), "cudaMemsetAsync");
+            ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
+            ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
+            if (P.raySortBits > 0) ck(cudaMemsetAsync(g.binCount.p, 0, rayBinBytes(), st), "cudaMemsetAsync");
+            launchGenerate(P, f, st);
+            launchBounces(s, P, f, depth, block, st);
+            launchTail(s, P, f, st);
+            launchPresentViews(P, f, static_cast<int>(pixels64), st);
+        };
+        if (useGraph) {
+            // the scene and view tables travel through device memory; every baked launch argument keys the capture
+            std::vector<unsigned char> key;
+            auto put = [&](const void* p, size_t n) {
+                const unsigned char* c = static_cast<const unsigned char*>(p);
+                key.insert(key.end(), c, c + n);
+            };
+            const int ints[9] = {depth, block, g.gridExtend, g.gridShade, g.gridConnect, g.shadeMinBlocks,
+                                 static_cast<int>(pixels64), g.overlapConnect, g_scene};
+            put(&P, sizeof(P)); put(&f, sizeof(f)); put(&s, sizeof(s)); put(ints, sizeof(ints));
+            if (!g_fused.exec || key != g_fused.key) {
+                releaseFusedGraph();
+                ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+                try {
+                    body();
+                    ck(cudaGetLastError(), "kernel launch (capture)");
+                } catch (...) {
+                    cudaGraph_t broken = nullptr;
+                    cudaStreamEndCapture(st, &broken);
+                    if (broken) cudaGraphDestroy(broken);
+                    throw;
+                }
+                ck(cudaStreamEndCapture(st, &g_fused.graph), "cudaStreamEndCapture");
+                ck(cudaGraphInstantiate(&g_fused.exec, g_fused.graph, 0), "cudaGraphInstantiate");
+                g_fused.key = key;
+            }
+            ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+            ck(cudaGraphLaunch(g_fused.exec, st), "cudaGraphLaunch");
+        } else {
+            ck(cudaEventRecord(g.ev0, st), "cudaEventRecord");
+            body();
+        }
+        ck(cudaGetLastError(), "kernel launch");
+        ck(cudaEventRecord(g.ev1, st), "cudaEventRecord");
+        // the frame's counters, as finishViews reads them
+        g.pendDepth = depth; g.pendPaths = paths; g.pendCount = 0;
+        std::vector<int> rc(static_cast<size_t>(depth + 1)), sc(static_cast<size_t>(depth + 1));
+        unsigned int errFlags = 0;
+        ck(cudaMemcpyAsync(rc.data(), g.rayCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        ck(cudaMemcpyAsync(sc.data(), g.shadowCount.p, sizeof(int) * (depth + 1), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        ck(cudaMemcpyAsync(&errFlags, g.errorFlags.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(st), "frame");
+        BteFrameStats S{};
+        S.tailBounce = -1;
+        for (int b = 0; b < depth; ++b) {
+            S.extends += rc[static_cast<size_t>(b)];
+            S.shadowRays += sc[static_cast<size_t>(b)];
+            if (rc[static_cast<size_t>(b)] > 0) S.maxBounceReached = b;
+        }
+        ck(cudaEventElapsedTime(&S.msTotal, g.ev0, g.ev1), "cudaEventElapsedTime");
+        // every scene: its views advance, its stats are the batch's (samples: its own)
+        for (int i = 0; i < sceneCount; ++i) {
+            selectScene(scenes[i]);
+            g.stats = S;
+            g.stats.samples = sceneSamples[static_cast<size_t>(i)];
+            const BteView* sv = views + offset[static_cast<size_t>(i)];
+            for (int v = 0; v < viewCounts[i]; ++v)
+                g.views[static_cast<size_t>(v)].frameIndex += static_cast<uint32_t>(sv[v].samplesPerFrame);
+            g.lastPaths = 0;
+        }
+        selectScene(home);
+        if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
+        if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+    } catch (...) {
+        selectScene(home);
+        throw;
+    }
+    return true;
+}
+
 // One batch over several scene slots: every scene's view frame is enqueued on its own streams first, then
 // each is finished in turn, so the scenes' launch sequences run side by side on the GPU.  Each scene's
 // views accumulate exactly as bte_render_views would leave them; the selected slot is restored.
@@ -869,6 +1112,7 @@ void renderSceneBatch(const int* scenes, const int* viewCounts, const BteView* v
         offset[static_cast<size_t>(i) + 1] = offset[static_cast<size_t>(i)] + viewCounts[i];
     }
     const int home = g_scene;
+    if (renderSceneBatchFused(scenes, viewCounts, views, sceneCount, offset, home)) return;
     bool allGraph = true;
     for (int i = 0; i < sceneCount; ++i) {
         selectScene(scenes[i]);
@@ -1277,6 +1521,24 @@ int bte_get_selected_scene(int* scene)
     return guarded([&] {
         if (!scene) throw CudaError{"bte_get_selected_scene: null pointer"};
         *scene = g_scene;
+        return 0;
+    });
+}
+
+int bte_set_batch_mode(int mode)
+{
+    return guarded([&] {
+        if (mode != 0 && mode != 1) throw CudaError{"bte_set_batch_mode: mode must be 0 or 1"};
+        g_batchMode = mode;
+        return 0;
+    });
+}
+
+int bte_get_batch_mode(int* mode)
+{
+    return guarded([&] {
+        if (!mode) throw CudaError{"bte_get_batch_mode: null pointer"};
+        *mode = g_batchMode;
         return 0;
     });
 }

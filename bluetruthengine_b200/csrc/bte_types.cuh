@@ -136,6 +136,11 @@ struct DevPaths {
     int* sortedQueue; // [count] the bounce's queue in bin order
     int raySortBits;  // origin cell bits per axis, 0 (off) to 4
     int raySortBounces;
+    // one launch sequence over several scenes' views (bte_render_scene_batch): the frame's scene table and the
+    // scene of every path (its view's); null in single-scene frames
+    const DevScene* scenes;   // [sceneCount]
+    uint8_t* pathScene;       // [count]
+    int sceneCount;
 };
 constexpr int kRaySortMinRays = 32768;
 
@@ -149,6 +154,7 @@ struct ViewDesc {
     int width, height, spp;
     uint32_t frameIndex;          // samples of this view accumulated before this frame
     int pathOffset, pixelOffset;
+    int scene;                    // entry of the frame's scene table (several scenes in one launch sequence)
     float* accum;                 // [W*H*3] FP32 running mean
     double* accumD;               // [W*H*3] FP64 running sum
     uint32_t* framebuffer;        // [W*H] packed RGBA8

@@ -116,6 +116,15 @@ int bte_get_selected_scene(int* scene);
  * side on the GPU; each scene's views accumulate exactly as bte_render_views on that slot would leave them.
  * Slots must be distinct; the selected slot is unchanged afterwards. */
 int bte_render_scene_batch(const int* scenes, const int* viewCounts, const BteView* views, int sceneCount);
+/* How bte_render_scene_batch runs the scenes.  1 (the default): every view of every scene in ONE launch sequence
+ * (one generate, one extend / shade / connect per bounce, one present over all scenes' paths), each path looking
+ * its scene -- geometry, tree, materials, lights, env map -- up in a per-frame scene table; this needs every scene
+ * in wavefront mode with the 8-wide tree and the first scene's max depth, roulette start, block size and graph
+ * use, and the frame-level tuning is the first scene's; other batches fall back to mode 0.  0: each scene's own
+ * launch sequence, the scenes side by side on their own streams (one parent graph when all use graphs).  Frame
+ * stats of every scene in a one-sequence batch are the batch's, with each scene's own sample count. */
+int bte_set_batch_mode(int mode);
+int bte_get_batch_mode(int* mode);
 int bte_toggle_denoiser(void);                      /* :192; returns new state (0/1) or <0; needs denoiser weights */
 int bte_read_denoised(float* hostRGB);               /* W*H*3 denoised mean radiance of the last frame (denoiser on) */
 int bte_set_render_mode(int mode);                                              /* :205 */

@@ -733,16 +733,19 @@ def _views_of(bte, scene, sizes):
     return views
 
 
-@pytest.mark.parametrize("use_graph", [0, 1])
-def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene, use_graph):
-    """Two scene slots (the random scene with its env map, the Cornell box), each with views of uneven size and
-    samples per frame, rendered side by side in one batch for two frames (separate streams, or one launch of a
-    graph holding each scene's captured view frame): every view's FP32 mean and FP64 sum equal those of eager
-    bte_render_views on that slot alone, bit for bit, and so do captured single-slot view frames; the selected
-    slot is restored."""
-    scenes = [(random_scene, 1, 10, [(64, 48, 1), (40, 30, 2)]),
-              (cornell_scene, 0, 8, [(50, 50, 2), (32, 24, 1), (70, 20, 3)])]
+@pytest.mark.parametrize("use_graph,batch_mode", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene, use_graph, batch_mode):
+    """Two scene slots (the random scene with its env map and spotlight, the Cornell box), each with views of
+    uneven size and samples per frame, rendered in one batch for two frames: in batch mode 1 as one launch sequence
+    over both scenes' paths (each path looking up its scene), in mode 0 side by side (separate streams, or one
+    launch of a graph holding each scene's captured view frame).  Every view's FP32 mean and FP64 sum equal those
+    of eager bte_render_views on that slot alone, bit for bit, and so do captured single-slot view frames; the
+    selected slot is restored."""
+    depths = (10, 10) if batch_mode else (10, 8)   # one launch sequence needs one max depth
+    scenes = [(random_scene, 1, depths[0], [(64, 48, 1), (40, 30, 2)]),
+              (cornell_scene, 0, depths[1], [(50, 50, 2), (32, 24, 1), (70, 20, 3)])]
     batch = []
+    renderer.set_batch_mode(batch_mode)
     try:
         for slot, (sc, env_mode, depth, sizes) in enumerate(scenes):
             renderer.select_scene(slot)
@@ -755,12 +758,15 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
         for _ in range(2):
             renderer.render_scene_batch(batch)
         assert renderer.selected_scene() == 0
-        got = []
+        got, extends = [], []
         for slot, views in batch:
             renderer.select_scene(slot)
             got.append([renderer.read_view_accum(i, w, h) for i, (_, w, h, _) in enumerate(views)])
             st = renderer.stats()
             assert st.samples == sum(w * h * s for _, w, h, s in views)
+            extends.append(st.extends)
+        # one launch sequence: both slots report the batch's ray counts; per scene: each its own
+        assert (extends[0] == extends[1]) == bool(batch_mode)
         for (slot, views), (_, env_mode, depth, _) in zip(batch, scenes):   # the same views, one slot at a time
             renderer.select_scene(slot)
             for graph in sorted({0, use_graph}):
@@ -779,6 +785,7 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
         with pytest.raises(RuntimeError, match="out of range"):
             renderer.select_scene(8)
     finally:
+        renderer.set_batch_mode(1)
         renderer.select_scene(1)
         renderer.reset_views()
         renderer.cleanup()
