@@ -338,6 +338,20 @@ def denoise_leg():
     peak, kind = measured_bf16_tflops()
     out["inference_1080p"] = {"ms": t, "gflop": flops / 1e9, "tflops": flops / (t / 1e3) / 1e12,
                               "peak_tflops": peak, "peak_source": kind, "frac": flops / (t / 1e3) / 1e12 / peak}
+    # one training step (forward, L1 loss, data and weight gradients, Adam) at the training configuration's
+    # crop and batch, on a small seeded set of 256x256 images; the trained weights are loaded back afterwards
+    n_img, crop, batch, steps = 16, 256, 8, 40
+    dn.set_dataset(rng.exponential(0.5, size=(n_img, 256, 256, 3)).astype(np.float32),
+                   rng.uniform(0, 1, size=(n_img, 256, 256, 6)).astype(np.float32),
+                   rng.exponential(0.5, size=(n_img, 256, 256, 3)).astype(np.float32))
+    dn.train(5, batch=batch, crop=crop, lr=1e-4, seed=1)
+    dn.train(steps, batch=batch, crop=crop, lr=1e-4, seed=2)
+    ms_step = dn.last_ms() / steps
+    train_flops = 3 * DENOISER_FLOP_PER_PIXEL * batch * crop * crop   # forward + data + weight gradients
+    out["training_step"] = {"batch": batch, "crop": crop, "ms_per_step": ms_step,
+                            "tflops": train_flops / (ms_step / 1e3) / 1e12,
+                            "frac": train_flops / (ms_step / 1e3) / 1e12 / peak}
+    dn.load(weights)
     return out
 
 
