@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of replaying the frame graph")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised time-to-relMSE leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 10M-triangle 4K leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-views and multi-scene legs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -541,7 +542,7 @@ def run_ours(args):
             out["cpu_baseline"] = cpu_baseline(scene, args, seconds=args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never the product
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_batch:
         try:
             out["batched_views"] = batched_views_leg(scene, args)
         except Exception as e:
