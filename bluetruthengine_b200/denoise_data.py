@@ -44,12 +44,24 @@ def render_input(r, W, H, spp, depth, sample_base=0):
     return noisy, np.concatenate([alb, nrm], -1), ms
 
 
-def reference(r, W, H, spp, depth, sample_base=TARGET_SAMPLE_BASE, spf=256):
-    """FP64 running sum / spp over `spp` samples starting at `sample_base` -> [H,W,3] float64."""
+def reference(r, W, H, spp, depth, sample_base=TARGET_SAMPLE_BASE, spf=256, with_floor=False):
+    """FP64 running sum / spp over `spp` samples starting at `sample_base` -> [H,W,3] float64.
+
+    with_floor: also return the reference's own relMSE against the converged image, estimated from its two
+    halves A and B (disjoint samples): relMSE(A, B) is about twice the error of a half, four times the error
+    of the whole (errors of independent unbiased estimates add, and shrink as 1/spp)."""
     r.reset_accumulation(W, H)
     r.set_frame_index(sample_base)
-    _frames(r, W, H, spp, spf, depth)
-    return r.read_accum_f64(W, H).reshape(H, W, 3) / float(spp)
+    half = spp // 2
+    _frames(r, W, H, half, spf, depth)
+    first = r.read_accum_f64(W, H).reshape(H, W, 3).copy() if with_floor else None
+    _frames(r, W, H, spp - half, spf, depth)
+    total = r.read_accum_f64(W, H).reshape(H, W, 3)
+    ref = total / float(spp)
+    if not with_floor:
+        return ref
+    a, b = first / float(half), (total - first) / float(spp - half)
+    return ref, rel_mse(a, b) / 4.0
 
 
 def render_pair(r, scene, spp_in, spp_target, depth=8):
@@ -91,30 +103,36 @@ def _sync():
         pass
 
 
-def plain_crossing(r, W, H, ref, bound, depth, step=4, max_spp=1 << 16, env=ENV_ALIAS):
-    """Smallest multiple of `step` samples at which progressive plain accumulation (the FP32 running mean
-    the renderer keeps, samples 0, 1, 2, ... of every pixel) reaches relMSE <= bound against `ref`.
-
-    The image is rendered `step` samples per frame.  relMSE is evaluated (outside any timing) on a schedule
-    that follows the 1/spp convergence of the error: after each evaluation the next one is placed half way
-    to the predicted crossing, and once that is within two steps, after every frame.  Returns
-    (spp or None, [(spp, relMSE), ...])."""
+def plain_crossing(r, W, H, ref, bound, depth, step=4, max_spp=1 << 16, env=ENV_ALIAS, floor=0.0):
+    """Progressive plain accumulation (the FP32 running mean the renderer keeps, samples 0, 1, 2, ... of every
+    pixel, `step` samples per frame) against `ref`, until its relMSE less the reference's own error `floor`
+    reaches `bound`, or `max_spp`.  relMSE is evaluated outside the timing, on a schedule that follows the
+    1/spp convergence of the error: the next evaluation at most doubles the sample count and stops at 90% of the
+    predicted crossing; from there on, after every frame.  Host wall time is summed over the render
+    calls alone.  Returns (crossing spp or None, [(spp, wall ms, device ms, relMSE, relMSE - floor), ...])."""
+    r.set_config(samples_per_frame=step, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
     r.reset_accumulation(W, H)
     r.set_frame_index(0)
-    r.set_config(samples_per_frame=step, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
+    _sync()
     spp, nxt, curve = 0, step, []
+    wall, dev = 0.0, 0.0
     while spp < max_spp:
+        t0 = time.perf_counter()
         r.render(W, H)
+        wall += time.perf_counter() - t0
+        dev += r.stats().msTotal
         spp += step
-        if spp < nxt:
+        if spp < nxt and spp < max_spp:
             continue
         e = rel_mse(r.read_accum(W, H).reshape(H, W, 3), ref)
-        curve.append((spp, e))
-        if e <= bound:
+        curve.append((spp, wall * 1e3, dev, e, e - floor))
+        if e - floor <= bound:
             return spp, curve
-        predicted = spp * e / bound
-        gap = max(step, int((predicted - spp) * 0.5) // step * step)
-        nxt = spp + (step if predicted - spp <= 2 * step else gap)
+        predicted = spp * max(e - floor, 1e-12) / bound
+        if spp >= 0.9 * predicted:
+            nxt = spp + step
+        else:
+            nxt = max(spp + step, min(2 * spp, int(0.9 * predicted)) // step * step)
     return None, curve
 
 
@@ -165,23 +183,32 @@ def denoised_wall(r, dn, W, H, spp, depth, env=ENV_ALIAS, max_spf=64):
 
 
 def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16, plain_max_spp=1 << 16,
-                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256)):
-    """Wall time (and device time) plain accumulation and the denoised low-spp form need to reach
-    relMSE <= bound against `ref`, on the uploaded scene's view.  The denoiser weights must be loaded.
+                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256), floor=0.0):
+    """Wall time (and device time) that plain accumulation and the denoised low-spp form need to reach
+    relMSE <= bound against the converged image, on the uploaded scene's view.  The denoiser weights must be
+    loaded.  Every image's relMSE against `ref` is reported as measured and less `floor`, the reference's own
+    error (`reference(..., with_floor=True)`); the crossing uses the latter.
 
-    plain: the crossing spp from `plain_crossing`, then that many samples rendered again and timed twice
-    (the first run captures the frame graphs; the second is reported as warm).
-    denoised: for growing spp, one frame plus the renderer's denoise and readback; each size is timed on
-    its first call (graph capture and buffers of a new size included) and again warm.  The first size
-    reaching the bound is the result."""
+    plain: one progressive run (`plain_crossing`), its wall time summed over the render calls.  When it does not
+    cross within `plain_max_spp`, the spp it needs is extrapolated from the 1/spp law its error follows (the
+    median of spp x (relMSE - floor) over the curve's points from 64 spp) and its time from the measured time per
+    sample; the result says so.
+    denoised: for growing spp, one frame plus the renderer's denoise and readback; each size is timed on its
+    first call (graph capture and buffers of a new size included) and again warm.  The first size reaching the
+    bound is the result."""
     W, H = scene.width, scene.height
-    n_cross, curve = plain_crossing(r, W, H, ref, bound, depth, step=step, max_spp=plain_max_spp)
-    plain = None
+    n_cross, curve = plain_crossing(r, W, H, ref, bound, depth, step=step, max_spp=plain_max_spp, floor=floor)
+    last = curve[-1]
     if n_cross is not None:
-        cold = plain_wall(r, W, H, n_cross, depth, spf=plain_spf)
-        warm = plain_wall(r, W, H, n_cross, depth, spf=plain_spf)
-        plain = {"spp": n_cross, "wall_ms": warm[0] * 1e3, "wall_ms_first_run": cold[0] * 1e3,
-                 "device_ms": warm[1], "rel_mse": rel_mse(warm[2], ref)}
+        plain = {"spp": n_cross, "wall_ms": last[1], "device_ms": last[2], "rel_mse": last[3],
+                 "rel_mse_less_floor": last[4], "extrapolated": False}
+    else:
+        pts = [n * e for n, _, _, _, e in curve if n >= 64 and e > 0]
+        c = float(np.median(pts)) if pts else float(last[0] * last[4])
+        n_need = c / bound
+        plain = {"spp": n_need, "wall_ms": last[1] / last[0] * n_need, "device_ms": last[2] / last[0] * n_need,
+                 "extrapolated": True, "fit_spp_times_error": c, "measured_to_spp": last[0],
+                 "rel_mse_at_measured": last[3], "rel_mse_less_floor_at_measured": last[4]}
     was_on = r.toggle_denoiser()
     if not was_on:
         raise RuntimeError("denoiser did not turn on")
@@ -190,17 +217,20 @@ def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16
         for n in denoise_spps:
             cold = denoised_wall(r, dn, W, H, n, depth)
             warm = denoised_wall(r, dn, W, H, n, depth)
+            e, e_in = rel_mse(warm[3], ref), rel_mse(warm[4], ref)
             row = {"spp": n, "wall_ms": warm[0] * 1e3, "wall_ms_first_call": cold[0] * 1e3,
-                   "device_ms_render": warm[1], "device_ms_denoise": warm[2],
-                   "rel_mse": rel_mse(warm[3], ref), "rel_mse_input": rel_mse(warm[4], ref)}
+                   "device_ms_render": warm[1], "device_ms_denoise": warm[2], "rel_mse": e,
+                   "rel_mse_less_floor": e - floor, "rel_mse_input": e_in, "rel_mse_input_less_floor": e_in - floor}
             rows.append(row)
-            if row["rel_mse"] <= bound:
+            if row["rel_mse_less_floor"] <= bound:
                 den = dict(row)
                 break
     finally:
         r.toggle_denoiser()
-    res = {"bound": bound, "plain": plain, "denoised": den, "denoised_sweep": rows, "plain_curve": curve}
-    if plain and den:
+    res = {"bound": bound, "reference_floor": floor, "plain": plain, "denoised": den, "denoised_sweep": rows,
+           "plain_curve": [{"spp": n, "wall_ms": w, "device_ms": d, "rel_mse": e, "rel_mse_less_floor": ec}
+                           for n, w, d, e, ec in curve]}
+    if den:
         res["speedup_wall"] = plain["wall_ms"] / den["wall_ms_first_call"]
         res["speedup_wall_warm"] = plain["wall_ms"] / den["wall_ms"]
         res["speedup_device"] = plain["device_ms"] / (den["device_ms_render"] + den["device_ms_denoise"])

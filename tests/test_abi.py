@@ -212,7 +212,7 @@ def test_launch_params_filled_for_current_frame(bte, renderer, random_scene):
 
     def dev(ptr, nbytes):
         class A:
-            __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, True), "version": 3}
+            __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
         return torch.as_tensor(A(), device="cuda").cpu().numpy().tobytes()
 
     assert dev(u64(96), sc.triangle_count * 96) == np.ascontiguousarray(sc.triangles).tobytes()
