@@ -7,7 +7,8 @@ Reports the BVH build, plain throughput (Msamples/s), then 1 spp + denoise again
 `ref-spp` samples in the FP64 accumulator (from disjoint sample indices): host wall time (renderer calls and
 image readback; for the denoised form the first call at the size included, and a warm repeat) with the device
 time beside it, and the relMSE of every image against that accumulation -- the denoised 1-spp image, its noisy
-input, and plain accumulation at 4, 16, 64 and 256 samples.
+input, and plain accumulation at 4, 16, 64 and 256 samples -- as measured and less the accumulation's own
+error (estimated from its two halves).
 """
 from __future__ import annotations
 
@@ -52,13 +53,18 @@ def run(ref_spp=1024, depth=24, spf=8, weights=None, log=print, width=3840, heig
     t0 = time.perf_counter()
     r.reset_accumulation(W, H)
     r.set_frame_index(TARGET_SAMPLE_BASE)
-    done, dev_ref = 0, 0.0
+    done, dev_ref, first, half = 0, 0.0, None, 0
     while done < ref_spp:
         r.render(W, H)
         dev_ref += r.stats().msTotal
         done += spf
-    ref = r.read_accum_f64(W, H).reshape(H, W, 3) / float(done)
+        if first is None and done >= ref_spp // 2:   # the first half's sum, for the reference's own error
+            first, half = r.read_accum_f64(W, H).reshape(H, W, 3).copy(), done
+    total = r.read_accum_f64(W, H).reshape(H, W, 3)
+    ref = total / float(done)
     wall_ref = time.perf_counter() - t0
+    # the reference's own relMSE against the converged image: a quarter of its halves' relMSE to each other
+    floor = rel_mse(first / float(half), (total - first) / float(done - half)) / 4.0 if 0 < half < done else 0.0
     log("reference %d spp: %.1f s wall" % (done, wall_ref))
     # plain accumulation from sample 0, relMSE at a few sample counts
     curve = []
@@ -71,7 +77,8 @@ def run(ref_spp=1024, depth=24, spf=8, weights=None, log=print, width=3840, heig
             r.render(W, H)
             dev_plain += r.stats().msTotal
             n += 4
-        curve.append({"spp": n, "device_ms": dev_plain, "rel_mse": rel_mse(r.read_accum(W, H).reshape(H, W, 3), ref)})
+        e = rel_mse(r.read_accum(W, H).reshape(H, W, 3), ref)
+        curve.append({"spp": n, "device_ms": dev_plain, "rel_mse": e, "rel_mse_less_floor": e - floor})
     # 1 spp + denoise through the renderer
     dn = Denoiser()
     dn.load(weights)
@@ -86,10 +93,11 @@ def run(ref_spp=1024, depth=24, spf=8, weights=None, log=print, width=3840, heig
            "height": H, "depth": depth, "accel": accel, "seconds_load": t_load, "seconds_upload_build": t_upload,
            "ms_per_frame_1spp": t_frame, "msamples_per_s": W * H / t_frame / 1e3,
            "extends_per_sample": st.extends / st.samples, "shadow_rays_per_sample": st.shadowRays / st.samples,
-           "plain_reference": {"spp": done, "wall_ms": wall_ref * 1e3, "device_ms": dev_ref},
+           "plain_reference": {"spp": done, "wall_ms": wall_ref * 1e3, "device_ms": dev_ref, "own_rel_mse": floor},
            "denoised_1spp": {"wall_ms_first_call": cold[0] * 1e3, "wall_ms": warm[0] * 1e3,
                              "device_ms_render": warm[1], "device_ms_denoise": warm[2],
-                             "rel_mse": rel_mse(warm[3], ref), "rel_mse_input": rel_mse(warm[4], ref)},
+                             "rel_mse": rel_mse(warm[3], ref), "rel_mse_less_floor": rel_mse(warm[3], ref) - floor,
+                             "rel_mse_input": rel_mse(warm[4], ref)},
            "plain_curve": curve}
     res["wall_ratio_plain_reference_to_denoised"] = res["plain_reference"]["wall_ms"] / res["denoised_1spp"]["wall_ms"]
     return res
