@@ -104,6 +104,8 @@ struct Net {
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
     int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2/3 tcgen05 row tiles
+    int wgradKind = 0;   // weight gradients: 0 warp-level mma.sync, 1 tcgen05 (shapes it supports)
+    Buf wgScratch;       // channel-major copies for the tcgen05 weight gradient
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
     Buf upBuf;            // a decoder layer's upsampled input at full resolution (row-tile kernel)
@@ -315,7 +317,14 @@ void backward(int N, int Hp, int Wp)
             const Conv& c = kConvs[s.conv];
             const long long elems = static_cast<long long>(N) * H * W * c.cout;
             if (c.relu) reluMask(net.act[s.dst].p, net.gact[s.dst].p, net.gact[s.dst].p, elems, st);
-            convWgrad(net.act[s.src].p, net.gact[s.dst].p, N, H, W, c.cin, c.cout, net.grad.as<float>() + net.wOff[s.conv], st);
+            if (net.wgradKind == 1 && convWgradTcSupported(N, H, W, c.cin, c.cout)) {
+                net.wgScratch.ensure(convWgradTcScratchBytes(N, H, W, c.cin, c.cout));
+                convWgradTc(net.act[s.src].p, net.gact[s.dst].p, N, H, W, c.cin, c.cout,
+                            net.grad.as<float>() + net.wOff[s.conv], net.wgScratch.p, net.errFlag.as<unsigned int>(), st);
+            } else {
+                convWgrad(net.act[s.src].p, net.gact[s.dst].p, N, H, W, c.cin, c.cout,
+                          net.grad.as<float>() + net.wOff[s.conv], st);
+            }
             biasGrad(net.gact[s.dst].p, static_cast<long long>(N) * H * W, c.cout, net.grad.as<float>() + net.bOff[s.conv], st);
             if (s.src != 0)
                 convDispatch(net.gact[s.dst].p, c.cout, false, nullptr, 0, N, H, W,
@@ -634,6 +643,18 @@ int bte_denoiser_debug_wait_timeout(unsigned int* status, double* seconds)
     });
 }
 
+// weight-gradient kernel of training: 0 the warp-level mma.sync kernel; 1 the tcgen05 kernel for the layers whose
+// shapes it takes (image width a multiple of 8, pixels a multiple of 64), the warp-level one for the rest
+int bte_denoiser_set_wgrad(int kind)
+{
+    return guardedDn([&] {
+        if (kind != 0 && kind != 1) throw CudaErr{"bte_denoiser_set_wgrad: kind must be 0 or 1"};
+        ensureNet();
+        net.wgradKind = kind;
+        return 0;
+    });
+}
+
 int bte_denoiser_last_ms(float* ms)
 {
     return guardedDn([&] {
@@ -667,7 +688,13 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
             weightCopies(bf32.as<float>(), static_cast<int>(padded / 9), 1, dst.p, nullptr, st);
             ck(cudaStreamSynchronize(st), "sync");
         };
-        if (op < 0 || op > 6) throw CudaErr{"bte_denoiser_debug_conv: op must be 0 to 6"};
+        if (op < 0 || op > 7) throw CudaErr{"bte_denoiser_debug_conv: op must be 0 to 7"};
+        const bool wgradTc = op == 7;
+        if (wgradTc) {
+            if (!convWgradTcSupported(n, h, wd, cin, cout))
+                throw CudaErr{"bte_denoiser_debug_conv: shape not supported by the tcgen05 weight gradient"};
+            op = 2;
+        }
         // ops 3 and 4: ops 0 and 1 on the tcgen05 pixel-tile kernel; ops 5 and 6 on the row-tile kernel
         const int force = op >= 5 ? 2 : (op >= 3 ? 1 : 0);
         if (op >= 5) op -= 5;
@@ -706,12 +733,20 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
             Buf g;
             g.ensure((9ull * cin * cout + cout) * 4);
             ck(cudaMemsetAsync(g.p, 0, (9ull * cin * cout + cout) * 4, st), "cudaMemsetAsync");
-            convWgrad(bx.p, bdy.p, n, h, wd, cin, cout, g.as<float>(), st);
+            Buf scratch;
+            if (wgradTc) {
+                scratch.ensure(convWgradTcScratchBytes(n, h, wd, cin, cout));
+                convWgradTc(bx.p, bdy.p, n, h, wd, cin, cout, g.as<float>(), scratch.p, net.errFlag.as<unsigned int>(), st);
+            } else {
+                convWgrad(bx.p, bdy.p, n, h, wd, cin, cout, g.as<float>(), st);
+            }
             biasGrad(bdy.p, static_cast<long long>(px), cout, g.as<float>() + 9ull * cin * cout, st);
             ck(cudaGetLastError(), "wgrad launch");
             ck(cudaMemcpyAsync(out, g.p, (9ull * cin * cout + cout) * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
             ck(cudaStreamSynchronize(st), "sync");
+            if (wgradTc) checkTcFlag();
             g.release();
+            scratch.release();
         } else {
             throw CudaErr{"bte_denoiser_debug_conv: op must be 0 to 6"};
         }

@@ -37,6 +37,13 @@ bool conv3x3TcRow(const void* X1, int C1, bool up, const void* X2, int C2, int N
 // Runs the tcgen05 kernels' bounded pipeline wait on an mbarrier that nothing completes (one warp):
 // *dStatus 2 when the wait gave up, 1 if it returned as completed; *dNs its duration.
 void waitTimeoutProbe(unsigned int* dStatus, unsigned long long* dNs, cudaStream_t st);
+// The weight gradient on the tcgen05 tensor cores (pixels as the reduction axis, channel-major copies of dY and
+// of the column-shifted X made first in `scratch`, convWgradTcScratchBytes of it); same sums as convWgrad.
+// Needs W % 8 == 0, N*H*W % 64 == 0, 16 <= Cin <= 256, Cout <= 128; sets *errorFlag on an internal timeout.
+bool convWgradTcSupported(int N, int H, int W, int Cin, int Cout);
+size_t convWgradTcScratchBytes(int N, int H, int W, int Cin, int Cout);
+void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, void* scratch,
+                 unsigned int* errorFlag, cudaStream_t st);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);

@@ -919,6 +919,214 @@ __global__ void __launch_bounds__(kRowThreads, 1) kConvTcRow(const __grid_consta
 
 constexpr int kTcSmem = kTcStages * (kStageABytes + kStageBBytes);
 
+namespace {
+
+// ---------------------------------------------------------------- weight gradient on tcgen05
+// NHWC [P][C] -> channel-major [C][P], or the column-shifted channel-major copy (pixel (n, y, x) holds the value
+// of (n, y, x + dx), zero where x + dx leaves the row): 32 x 32 tiles through shared memory, both sides coalesced.
+__global__ void kPlanar(const bf16* __restrict__ in, int C, long long P, int W, int dx, bf16* __restrict__ out)
+{
+    __shared__ bf16 tile[32][34];
+    const long long pb = static_cast<long long>(blockIdx.x) * 32;
+    const int cb = static_cast<int>(blockIdx.y) * 32;
+    const int tx = static_cast<int>(threadIdx.x), ty = static_cast<int>(threadIdx.y);
+    for (int k = ty; k < 32; k += 8) {
+        const long long p = pb + k;
+        const int c = cb + tx;
+        bf16 v = __float2bfloat16(0.0f);
+        if (p < P && c < C) {
+            const int x = static_cast<int>(p % W);
+            if (x + dx >= 0 && x + dx < W) v = in[(p + dx) * C + c];
+        }
+        tile[k][tx] = v;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = cb + k;
+        const long long p = pb + tx;
+        if (c < C && p < P) out[static_cast<size_t>(c) * P + p] = tile[tx][k];
+    }
+}
+
+// dW[tap][co][ci] += sum over pixels p of dY[p][co] * X[p shifted by the tap][ci], as a GEMM with M = the output
+// channels (one 128-row tile; rows beyond Cout are zero), N = the input channels rounded up to 16 (at most 256)
+// and the pixels as K.  Both operands come from the channel-major copies made beforehand (dYt[co][p] and, per
+// column shift dx, Xs[dx + 1][ci][p]), so one K-major 16-byte chunk is 8 consecutive pixels of one channel; the
+// row shift dy is a whole-row offset (W % 8 == 0 keeps every chunk inside one image row, whose validity decides
+// the zero fill).  The pipeline is kConvTc's: 64-pixel stages through a 3-deep cp.async ring, one thread issues
+// four M128 x N x K16 MMAs per stage into one TMEM accumulator, every wait bounded.  The epilogue adds the CTA's
+// partial sums into dW with FP32 atomics.  Grid: (1, 9 taps, pixel splits of a multiple of 64 pixels).
+__global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt, const bf16* __restrict__ Xs, int H,
+                                                   int W, long long P, int Cin, int Cout, int nPad,
+                                                   long long pixPerSplit, float* __restrict__ dW,
+                                                   unsigned int* errorFlag)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t mbar[kTcStages];
+    __shared__ uint32_t tmemBase;
+    __shared__ volatile int abortFlag;
+    __shared__ volatile int lastCommit;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tap = static_cast<int>(blockIdx.y), dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const long long p0 = static_cast<long long>(blockIdx.z) * pixPerSplit;
+    const long long p1 = p0 + pixPerSplit < P ? p0 + pixPerSplit : P;
+    const int iters = p1 > p0 ? static_cast<int>((p1 - p0 + kTcKStage - 1) / kTcKStage) : 0;
+    const uint32_t sA = smemAddr(smem), sB = sA + kTcStages * kStageABytes;
+    const uint32_t tmemCols = nPad <= 32 ? 32 : (nPad <= 64 ? 64 : (nPad <= 128 ? 128 : 256));
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smemAddr(&tmemBase)),
+                     "r"(tmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int st = 0; st < kTcStages; ++st) mbarInit(smemAddr(&mbar[st]), 1);
+        abortFlag = 0;
+        lastCommit = -1;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t tmem = tmemBase;
+    const uint32_t lboA = (kTcM / 8) * 128;
+    const uint32_t lboB = static_cast<uint32_t>(nPad / 8) * 128;
+    const uint32_t idesc = instrDesc(nPad);
+    const bf16* Xd = Xs + static_cast<size_t>(dx + 1) * Cin * P;
+
+    auto issueCopies = [&](int it) {
+        const int stage = it % kTcStages;
+        const long long pc = p0 + static_cast<long long>(it) * kTcKStage;
+        const uint32_t aBase = sA + stage * kStageABytes;
+        for (int e = tid; e < kTcM * 8; e += 128) {   // A: 128 output channels x 8 chunks of 8 pixels
+            const int co = e & (kTcM - 1), j = e / kTcM;
+            const long long p = pc + 8 * j;
+            const bool ok = co < Cout && p < p1;
+            cpAsync16(aBase + j * lboA + (co >> 3) * 128 + (co & 7) * 16, ok ? dYt + static_cast<size_t>(co) * P + p : dYt,
+                      ok);
+        }
+        const uint32_t bBase = sB + stage * kStageBBytes;
+        for (int e = tid; e < nPad * 8; e += 128) {   // B: nPad input channels x 8 chunks, shifted by dy rows
+            const int ci = e % nPad, j = e / nPad;
+            const long long p = pc + 8 * j;
+            bool ok = ci < Cin && p < p1;
+            long long q = 0;
+            if (ok) {
+                const int y = static_cast<int>((p / W) % H);
+                ok = y + dy >= 0 && y + dy < H;
+                q = p + static_cast<long long>(dy) * W;
+            }
+            cpAsync16(bBase + j * lboB + (ci >> 3) * 128 + (ci & 7) * 16, ok ? Xd + static_cast<size_t>(ci) * P + q : Xd,
+                      ok);
+        }
+    };
+
+    // all threads run the same barriers; a timed-out wait only raises the abort flag (no further copy or MMA)
+    for (int it = 0; it < iters + kTcStages - 1; ++it) {
+        if (it < iters && !abortFlag) {
+            bool free = true;
+            if (it >= kTcStages) {
+                const int prev = it - kTcStages;
+                free = mbarWait(smemAddr(&mbar[prev % kTcStages]), static_cast<uint32_t>((prev / kTcStages) & 1));
+            }
+            if (free) issueCopies(it);
+            else abortFlag = 1;
+        }
+        cpAsyncCommit();
+        const int j = it - (kTcStages - 1);
+        if (j >= 0 && j < iters) {
+            cpAsyncWait<kTcStages - 1>();
+            asm volatile("fence.proxy.async.shared::cta;\n" ::);
+            __syncthreads();
+            if (tid == 0 && !abortFlag) {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+                const int stage = j % kTcStages;
+                for (int k = 0; k < kTcKStage / 16; ++k) {
+                    const uint64_t da = smemDesc(sA + stage * kStageABytes + 2 * k * lboA, lboA, 128);
+                    const uint64_t db = smemDesc(sB + stage * kStageBBytes + 2 * k * lboB, lboB, 128);
+                    umma(tmem, da, db, idesc, (j > 0 || k > 0) ? 1u : 0u);
+                }
+                ummaCommit(smemAddr(&mbar[stage]));
+                lastCommit = j;
+            }
+        }
+    }
+    cpAsyncWait<0>();
+    __syncthreads();
+    const int last = lastCommit;
+    if (last >= 0 && !mbarWait(smemAddr(&mbar[last % kTcStages]), static_cast<uint32_t>((last / kTcStages) & 1)))
+        abortFlag = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    __syncthreads();
+    if (iters == 0) {
+        // an empty split adds nothing
+    } else if (abortFlag || last != iters - 1) {
+        if (tid == 0 && errorFlag) atomicOr(errorFlag, 1u);
+    } else {
+        // warp w owns TMEM lanes 32w..32w+31 = output channels; columns = input channels
+        const int co = warp * 32 + (tid & 31);
+        float* dst = dW + (static_cast<size_t>(tap) * Cout + co) * Cin;
+        for (int c = 0; c < nPad; c += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                         "tcgen05.wait::ld.sync.aligned;\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                         : "r"(taddr));
+            if (co < Cout)
+                for (int k = 0; k < 16; ++k)
+                    if (c + k < Cin) atomicAdd(dst + c + k, __uint_as_float(v[k]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmemCols));
+}
+
+}  // namespace
+
+bool convWgradTcSupported(int N, int H, int W, int Cin, int Cout)
+{
+    const long long P = static_cast<long long>(N) * H * W;
+    return W % 8 == 0 && P % 64 == 0 && P > 0 && Cin >= 16 && Cin <= kTcMaxN && Cin % 8 == 0 && Cout >= 1 &&
+           Cout <= kTcM;
+}
+
+size_t convWgradTcScratchBytes(int N, int H, int W, int Cin, int Cout)
+{
+    return static_cast<size_t>(N) * H * W * (static_cast<size_t>(Cout) + 3 * static_cast<size_t>(Cin)) * sizeof(bf16);
+}
+
+void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, void* scratch,
+                 unsigned int* errorFlag, cudaStream_t st)
+{
+    const long long P = static_cast<long long>(N) * H * W;
+    bf16* dYt = static_cast<bf16*>(scratch);
+    bf16* Xs = dYt + static_cast<size_t>(Cout) * P;
+    const dim3 tb(32, 8);
+    const unsigned pb = static_cast<unsigned>((P + 31) / 32);
+    kPlanar<<<dim3(pb, static_cast<unsigned>((Cout + 31) / 32)), tb, 0, st>>>(static_cast<const bf16*>(dY), Cout, P, W,
+                                                                              0, dYt);
+    for (int dx = -1; dx <= 1; ++dx)
+        kPlanar<<<dim3(pb, static_cast<unsigned>((Cin + 31) / 32)), tb, 0, st>>>(
+            static_cast<const bf16*>(X), Cin, P, W, dx, Xs + static_cast<size_t>(dx + 1) * Cin * P);
+    static bool attrSet = false;
+    if (!attrSet) {
+        cudaFuncSetAttribute(kWgradTc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        attrSet = true;
+    }
+    const int nPad = (Cin + 15) / 16 * 16;
+    // about two CTAs per SM over the nine taps, each at least 512 pixels, splits a multiple of 64 pixels
+    long long splits = (2LL * 148 + 8) / 9;
+    long long per = (P + splits - 1) / splits;
+    if (per < 512) per = 512;
+    per = (per + kTcKStage - 1) / kTcKStage * kTcKStage;
+    splits = (P + per - 1) / per;
+    kWgradTc<<<dim3(1, 9, static_cast<unsigned>(splits)), 128, kTcSmem, st>>>(dYt, Xs, H, W, P, Cin, Cout, nPad, per, dW,
+                                                                               errorFlag);
+}
+
 bool convTcSupported(int Cin, int Cout) { return Cout % 16 == 0 && Cout >= 16 && Cout <= kTcMaxN && Cin % 16 == 0; }
 
 void conv3x3Tc(const void* X1, int C1, bool up, const void* X2, int C2, int N, int H, int W, const void* Wk,

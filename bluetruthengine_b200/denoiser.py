@@ -102,6 +102,10 @@ class Denoiser:
         self._ck(self.lib.bte_denoiser_debug_wait_timeout(C.byref(st), C.byref(sec)))
         return st.value, sec.value
 
+    def set_wgrad(self, kind: int):
+        """Weight-gradient kernel of training: 0 warp-level mma.sync, 1 tcgen05 (where the layer's shape allows)."""
+        self._ck(self.lib.bte_denoiser_set_wgrad(int(kind)))
+
     def last_ms(self) -> float:
         ms = C.c_float()
         self._ck(self.lib.bte_denoiser_last_ms(C.byref(ms)))
@@ -109,7 +113,8 @@ class Denoiser:
 
     def debug_conv(self, op: int, x=None, w=None, bias=None, dy=None, shape=(1, 16, 16, 16, 16), relu=True):
         """op 0: forward, 1: data gradient, 2: weight gradient (+ bias gradient) of one 3x3 conv layer;
-        ops 3 and 4: ops 0 and 1 on the tcgen05 pixel-tile kernel; ops 5 and 6 on the row-tile kernel.
+        ops 3 and 4: ops 0 and 1 on the tcgen05 pixel-tile kernel; ops 5 and 6 on the row-tile kernel;
+        op 7: op 2 on the tcgen05 weight-gradient kernel.
         shape = (N, H, W, Cin, Cout); x [N,H,W,Cin], w [9][Cout][Cin], dy [N,H,W,Cout]."""
         n, h, wd, cin, cout = shape
         keep = [None if a is None else _f32(a) for a in (x, w, bias, dy)]
