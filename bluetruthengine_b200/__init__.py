@@ -50,7 +50,7 @@ class Tuning(C.Structure):
                 ("postponePercent", C.c_int), ("sortShading", C.c_int), ("tailPaths", C.c_int),
                 ("bvhBuilder", C.c_int), ("plocRadius", C.c_int), ("overlapConnect", C.c_int),
                 ("wideCollapse", C.c_int), ("raySortBits", C.c_int), ("raySortBounces", C.c_int),
-                ("leafTestsPerStep", C.c_int)]
+                ("leafTestsPerStep", C.c_int), ("orderBounces", C.c_int)]
 
 
 class RenderConfig(C.Structure):
@@ -471,11 +471,11 @@ class Renderer:
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
                    postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 0, bvh_builder: int = 1,
                    ploc_radius: int = 4, overlap_connect: int = 1, wide_collapse: int = 1, ray_sort_bits: int = 0,
-                   ray_sort_bounces: int = 4, leaf_tests_per_step: int = 0):
+                   ray_sort_bounces: int = 4, leaf_tests_per_step: int = 0, order_bounces: int = 3):
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),
                    int(tail_paths), int(bvh_builder), int(ploc_radius),
                    int(overlap_connect), int(wide_collapse), int(ray_sort_bits), int(ray_sort_bounces),
-                   int(leaf_tests_per_step))
+                   int(leaf_tests_per_step), int(order_bounces))
         self._ck(self.lib.bte_set_tuning(C.byref(t)))
 
     def tuning(self) -> dict:

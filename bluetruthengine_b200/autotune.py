@@ -12,6 +12,8 @@ Sweeps the knobs that decide throughput on a given scene and GPU:
   * ray reordering before the closest-hit rays of bounces 1-4 (origin cell
     bits per axis; 0 = off) and the 8-wide walk's triangle tests per step
     (0 = all of a node's at once),
+  * the leading bounces whose material buckets and queues are rebuilt in
+    path order (0 = atomic appends in completion order throughout),
 timing whole frames on the device (CUDA events), and leaves the renderer in
 the fastest configuration.  Results are deterministic in value (every
 configuration renders the same bits); only speed differs.
@@ -34,6 +36,7 @@ class TuneResult:
     tail_paths: int
     ray_sort_bits: int
     leaf_tests_per_step: int
+    order_bounces: int
     ms_per_frame: float
     msamples_per_s: float
 
@@ -41,18 +44,19 @@ class TuneResult:
 def autotune(renderer, width: int, height: int, samples_per_frame: int, max_depth: int, env_sampling: int,
              trees=((8, 1), (8, 2), (8, 3), (2, 1)), blocks=(64, 128, 256), shade_min_blocks=(2, 3),
              postpone=(0, 20), sort_shading=(1,), tail_paths=(0, 1 << 14), ray_sort=(0,), leaf_tests=(0,),
-             frames: int = 3, verbose: bool = False):
+             order=(0, 3), frames: int = 3, verbose: bool = False):
     """Blocks run 64 to 256 threads: the stage kernels are compiled for at most 256 threads per block, which
     fixes their register budgets."""
     results = []
     for bvh_width, leaf in trees:
         renderer.set_tuning(leaf, 2, bvh_width)
         renderer.init_accel()
-        for blk, smb, pp, srt, tail, rs, lt in itertools.product(blocks, shade_min_blocks,
-                                                                 postpone if bvh_width == 8 else (0,), sort_shading,
-                                                                 tail_paths, ray_sort,
-                                                                 leaf_tests if bvh_width == 8 else (0,)):
-            renderer.set_tuning(leaf, smb, bvh_width, pp, srt, tail, ray_sort_bits=rs, leaf_tests_per_step=lt)
+        for blk, smb, pp, srt, tail, rs, lt, ob in itertools.product(blocks, shade_min_blocks,
+                                                                     postpone if bvh_width == 8 else (0,),
+                                                                     sort_shading, tail_paths, ray_sort,
+                                                                     leaf_tests if bvh_width == 8 else (0,), order):
+            renderer.set_tuning(leaf, smb, bvh_width, pp, srt, tail, ray_sort_bits=rs, leaf_tests_per_step=lt,
+                                order_bounces=ob)
             renderer.set_config(samples_per_frame=samples_per_frame, max_depth=max_depth, rr_start=3,
                                 env_sampling=env_sampling, block_size=blk)
             renderer.render(width, height)          # warm-up at this configuration
@@ -61,14 +65,15 @@ def autotune(renderer, width: int, height: int, samples_per_frame: int, max_dept
                 renderer.render(width, height)
                 ms += renderer.stats().msTotal
             ms /= frames
-            r = TuneResult(bvh_width, leaf, blk, smb, pp, srt, tail, rs, lt, ms,
+            r = TuneResult(bvh_width, leaf, blk, smb, pp, srt, tail, rs, lt, ob, ms,
                            width * height * samples_per_frame / ms / 1e3)
             results.append(r)
             if verbose:
                 print(json.dumps(asdict(r)), flush=True)
     best = min(results, key=lambda r: r.ms_per_frame)
     renderer.set_tuning(best.max_leaf, best.shade_min_blocks, best.bvh_width, best.postpone_percent, best.sort_shading,
-                        best.tail_paths, ray_sort_bits=best.ray_sort_bits, leaf_tests_per_step=best.leaf_tests_per_step)
+                        best.tail_paths, ray_sort_bits=best.ray_sort_bits, leaf_tests_per_step=best.leaf_tests_per_step,
+                        order_bounces=best.order_bounces)
     renderer.init_accel()
     renderer.set_config(samples_per_frame=samples_per_frame, max_depth=max_depth, rr_start=3,
                         env_sampling=env_sampling, block_size=best.block_size)

@@ -52,11 +52,23 @@ BTE_DI int appendKeyed(int* counters, int key)
 }
 
 // bucket of a path for material-sorted shading: 0 miss, else the BSDF type of the hit triangle
-BTE_DI void sortAppend(const DevScene& s, const DevPaths& P, int bounce, int idx, int tri)
+BTE_DI int sortKey(const DevScene& s, int tri)
 {
     const int key = tri < 0 ? 0 : s.bsdfs[s.triBsdfIds[tri]].type;
-    const int k = (key >= 0 && key < kSortKeys) ? key : 0;
+    return (key >= 0 && key < kSortKeys) ? key : 0;
+}
+BTE_DI void sortAppend(const DevScene& s, const DevPaths& P, int bounce, int idx, int tri)
+{
+    const int k = sortKey(s, tri);
     P.sortQueue[static_cast<size_t>(k) * P.count + appendKeyed(P.sortCount + bounce * kSortKeys, k)] = idx;
+}
+// extend's hand-over to shade: the bucket append, or -- on a path-ordered bounce -- the path's key, from which
+// the ordered compaction builds the buckets
+BTE_DI void bucketPath(const DevScene& s, const DevPaths& P, int bounce, int idx, int tri)
+{
+    if (!P.sortQueue) return;
+    if (bounce < P.orderBounces) P.pathKey[idx] = static_cast<uint8_t>(sortKey(s, tri));
+    else sortAppend(s, P, bounce, idx, tri);
 }
 
 BTE_DI V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
@@ -184,7 +196,7 @@ __global__ void __launch_bounds__(256) kExtend(DevScene s, DevPaths P, int bounc
         const int tri = traceClosestW<Width>(s, r, kEps, 1e30f, t, u, v, P.errorFlags);
         P.hit[idx] = make_float4(t, u, v, __int_as_float(tri));
         if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
-        if (P.sortQueue) sortAppend(s, P, bounce, idx, tri);
+        bucketPath(s, P, bounce, idx, tri);
     }
 }
 
@@ -314,7 +326,9 @@ __global__ void __launch_bounds__(256, MinBlocks) kShade(DevScene s, DevPaths P,
         }
         const DevScene& ss = sceneOf<Multi>(s, P, idx);
         const bool alive = shadePath(ss, P, f, bounce, idx, true);
-        if (alive && bounce + 1 < P.maxDepth) {
+        if (bounce + 1 < P.orderBounces) {   // the ordered compaction builds the next queue
+            P.pathKey[idx] = alive && bounce + 1 < P.maxDepth ? kKeyNext : kKeyDead;
+        } else if (alive && bounce + 1 < P.maxDepth) {
             const int next = appendCoalesced(P.rayCount + bounce + 1);
             qn[next] = idx;
             if (P.raySortBits > 0 && bounce + 1 <= P.raySortBounces) {
@@ -363,6 +377,121 @@ __global__ void __launch_bounds__(256) kRayScatter(DevPaths P, int bounce)
     const int* __restrict__ q = P.queue[bounce & 1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
         P.sortedQueue[appendKeyed(starts, P.rayBin[i])] = q[i];
+}
+
+// ---------------------------------------------------------------- path-ordered queues
+// A stable counting sort of the paths 0 .. count-1 by pathKey, for one bounce and one selection of keys lo ..
+// lo+n-1: the material buckets after extend (keys 0 .. kSortKeys-1 into sortQueue's bucket regions, totals into
+// sortCount) or the next bounce's queue after shade (key kKeyNext into queue[(bounce + 1) & 1], total into
+// rayCount[bounce + 1]).  A tile is kOrderTile consecutive paths, 16 per thread of a 256-thread block (one
+// 16-byte load of their keys; pathKey is padded to whole tiles).  Inside a key the paths keep index order.
+
+// keys of this thread's 16 paths; paths at or beyond count read as ended
+BTE_DI void orderKeys(const DevPaths& P, uint8_t (&k)[16], int& first)
+{
+    first = static_cast<int>(blockIdx.x) * kOrderTile + static_cast<int>(threadIdx.x) * 16;
+    const uint4 w = *reinterpret_cast<const uint4*>(P.pathKey + first);
+    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const uint8_t v = static_cast<uint8_t>(words[e >> 2] >> (8 * (e & 3)));
+        k[e] = first + e < P.count ? v : kKeyDead;
+    }
+}
+BTE_DI int orderCountKey(const uint8_t (&k)[16], int key)
+{
+    int c = 0;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) c += k[e] == key ? 1 : 0;
+    return c;
+}
+// exclusive prefix of v over the block's threads (in thread order) and the block's total; every thread calls it
+BTE_DI int blockExclusiveScan(int v, int* warpSum, int& total)
+{
+    const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
+    const int warps = static_cast<int>(blockDim.x >> 5);
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < warps ? warpSum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        warpSum[lane] = w;
+    }
+    __syncthreads();
+    total = warpSum[warps - 1];
+    const int excl = x - v + (warp > 0 ? warpSum[warp - 1] : 0);
+    __syncthreads();   // warpSum is reused by the next call
+    return excl;
+}
+
+// per-tile counts of keys lo .. lo+n-1 -> orderTiles[tile * 8 + j]
+__global__ void __launch_bounds__(256) kOrderCount(DevPaths P, int bounce, int lo, int n)
+{
+    if (tailTakesOver(P, bounce)) return;
+    __shared__ int warpSum[32];
+    uint8_t k[16];
+    int first;
+    orderKeys(P, k, first);
+    for (int j = 0; j < n; ++j) {
+        int total;
+        blockExclusiveScan(orderCountKey(k, lo + j), warpSum, total);
+        if (threadIdx.x == 0) P.orderTiles[blockIdx.x * 8 + j] = total;
+    }
+}
+
+// per-tile counts -> per-tile starts (exclusive over tiles, per key) and the totals; one block
+__global__ void __launch_bounds__(1024) kOrderScan(DevPaths P, int bounce, int lo, int n, int tiles)
+{
+    if (tailTakesOver(P, bounce)) return;
+    __shared__ int warpSum[32];
+    const int per = (tiles + static_cast<int>(blockDim.x) - 1) / static_cast<int>(blockDim.x);
+    const int t0 = static_cast<int>(threadIdx.x) * per;
+    const int t1 = min(t0 + per, tiles);
+    for (int j = 0; j < n; ++j) {
+        int sum = 0;
+        for (int t = t0; t < t1; ++t) sum += P.orderTiles[t * 8 + j];
+        int total;
+        int run = blockExclusiveScan(sum, warpSum, total);
+        for (int t = t0; t < t1; ++t) {
+            const int c = P.orderTiles[t * 8 + j];
+            P.orderTiles[t * 8 + j] = run;
+            run += c;
+        }
+        if (threadIdx.x == 0) {
+            if (lo == kKeyNext) P.rayCount[bounce + 1] = total;
+            else P.sortCount[bounce * kSortKeys + lo + j] = total;
+        }
+    }
+}
+
+// each path of a selected key to out[j * stride + its rank]
+__global__ void __launch_bounds__(256) kOrderScatter(DevPaths P, int bounce, int lo, int n, int* out, int stride)
+{
+    if (tailTakesOver(P, bounce)) return;
+    __shared__ int warpSum[32];
+    uint8_t k[16];
+    int first;
+    orderKeys(P, k, first);
+    for (int j = 0; j < n; ++j) {
+        const int c = orderCountKey(k, lo + j);
+        int total;
+        int pos = P.orderTiles[blockIdx.x * 8 + j] + blockExclusiveScan(c, warpSum, total);
+        if (c == 0) continue;
+        int* o = out + static_cast<size_t>(j) * stride;
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+            if (k[e] == lo + j) o[pos++] = first + e;
+    }
 }
 
 // ---------------------------------------------------------------- connect
@@ -422,7 +551,7 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
         if ((threadIdx.x & 7u) == 0u) {
             P.hit[idx] = tri >= 0 ? make_float4(t, u, v, __int_as_float(tri)) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
             if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
-            if (P.sortQueue) sortAppend(ss, P, bounce, idx, tri);
+            bucketPath(ss, P, bounce, idx, tri);
         }
         return;
     }
@@ -442,7 +571,7 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
             if (!r.valid || ss.triCount <= 0) {
                 P.hit[idx] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
                 if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = -1;
-                if (P.sortQueue) sortAppend(ss, P, bounce, idx, -1);
+                bucketPath(ss, P, bounce, idx, -1);
                 idx = -1;
                 continue;
             }
@@ -454,7 +583,7 @@ __global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
             P.hit[idx] = tri >= 0 ? make_float4(w.bt, w.bu, w.bv, __int_as_float(tri))
                                   : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
             if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + bounce] = tri;
-            if (P.sortQueue) sortAppend(ss, P, bounce, idx, tri);
+            bucketPath(ss, P, bounce, idx, tri);
             idx = -1;
         }
     }
@@ -878,6 +1007,17 @@ void launchRaySort(const DevPaths& P, int bounce, int grid, cudaStream_t st)
 {
     kRayBins<<<1, 1024, 0, st>>>(P, bounce);
     kRayScatter<<<grid, 256, 0, st>>>(P, bounce);
+}
+int orderTiles(int paths) { return (paths + kOrderTile - 1) / kOrderTile; }
+void launchOrder(const DevPaths& P, int bounce, bool nextQueue, cudaStream_t st)
+{
+    const int tiles = orderTiles(P.count);
+    const int lo = nextQueue ? kKeyNext : 0, n = nextQueue ? 1 : kSortKeys;
+    int* out = nextQueue ? P.queue[(bounce + 1) & 1] : P.sortQueue;
+    const int stride = nextQueue ? 0 : P.count;
+    kOrderCount<<<tiles, 256, 0, st>>>(P, bounce, lo, n);
+    kOrderScan<<<1, 1024, 0, st>>>(P, bounce, lo, n, tiles);
+    kOrderScatter<<<tiles, 256, 0, st>>>(P, bounce, lo, n, out, stride);
 }
 // Frames over several scenes (P.scenes) run the stage kernels' multi-scene instances; those scenes all use the
 // 8-wide tree (checked by the host).

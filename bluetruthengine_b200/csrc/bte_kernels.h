@@ -12,6 +12,9 @@ void launchGenerate(const DevPaths& P, const FrameParams& f, cudaStream_t st);
 void launchExtend(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);
 // bounce's queue into ray-bin order before its extend (no-op unless DevPaths.raySortBits and the bounce qualify)
 void launchRaySort(const DevPaths& P, int bounce, int grid, cudaStream_t st);
+// ordered compaction of a path-ordered bounce: the material buckets (after extend) or the next queue (after shade)
+int orderTiles(int paths);
+void launchOrder(const DevPaths& P, int bounce, bool nextQueue, cudaStream_t st);
 void launchShade(const DevScene& s, const DevPaths& P, const FrameParams& f, int bounce, int grid, int block,
                  int minBlocks, cudaStream_t st);
 void launchConnect(const DevScene& s, const DevPaths& P, int bounce, int grid, int block, cudaStream_t st);

@@ -105,6 +105,7 @@ struct Renderer {
     int builtBuilder = 0;     // hierarchy in use
     int overlapConnect = 1;   // bounce b's shadow rays run beside bounce b+1's closest-hit rays (11.1 -> 9.5 ms)
     int leafTestsPerStep = 0; // 8-wide walk: triangle tests per step (0: all of a node's leaves at once)
+    int orderBounces = 3;     // leading bounces whose buckets and queues are rebuilt in path order (0: off)
     int raySortBits = 0;      // ray reordering before extend: origin cell bits per axis (0: off)
     int raySortBounces = 4;   // bounces 1..raySortBounces are reordered
     bool sceneChanged = false;   // bte_mark_scene_changed: the next bte_render resets accumulation first
@@ -124,7 +125,7 @@ struct Renderer {
     uint32_t* extFramebuffer = nullptr;
     // wavefront buffers
     DeviceBuffer pO, pD, pTp, pL, pHit, q0, q1, rayCount, shadowCount, fetch, shadowQueue, shOrigin, shDir, shContrib,
-        shMask, hitLog, errorFlags, sortQueue, sortCount, rayBin, sortedQueue, binCount;
+        shMask, hitLog, errorFlags, sortQueue, sortCount, rayBin, sortedQueue, binCount, pathKey, orderTiles;
     int pathCap = 0, slotCap = 0, depthCap = 0;
     bool hitLogEnabled = false;
     bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
@@ -304,6 +305,7 @@ void releaseWavefront()
     releaseViewGraph();
     for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch,
                             &g.sortQueue, &g.sortCount, &g.shadowQueue, &g.rayBin, &g.sortedQueue, &g.binCount,
+                            &g.pathKey, &g.orderTiles,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
         b->release();
     g.aovAlbedo.release(); g.aovNormal.release();
@@ -324,12 +326,22 @@ void setRaySort(DevPaths& P, bool on)
     P.raySortBounces = g.raySortBounces;
 }
 
+// path-ordered queue fields of a frame's DevPaths (off in megakernel mode, without material-sorted shading and
+// with ray reordering, which appends the next queue in bin order)
+void setOrder(DevPaths& P, bool on)
+{
+    if (!on || g.orderBounces <= 0 || !P.sortQueue || P.raySortBits > 0) return;
+    P.pathKey = g.pathKey.as<uint8_t>();
+    P.orderTiles = g.orderTiles.as<int>();
+    P.orderBounces = g.orderBounces;
+}
+
 void ensureWavefront(int paths, int slots, int depth)
 {
     const bool grow = paths > g.pathCap || slots > g.slotCap || depth > g.depthCap;
     const size_t binBytes = g.raySortBits > 0 ? rayBinBytes() : 0;
     if (!grow && (!g.hitLogEnabled || g.hitLog.p) && (!g.sortShading || g.sortQueue.p) &&
-        (!g.raySortBits || (g.sortedQueue.p && g.binCount.bytes >= binBytes)))
+        (!g.raySortBits || (g.sortedQueue.p && g.binCount.bytes >= binBytes)) && (!g.orderBounces || g.pathKey.p))
         return;
     if (grow) {
         releaseWavefront();
@@ -350,6 +362,12 @@ void ensureWavefront(int paths, int slots, int depth)
     }
     if (g.hitLogEnabled) ensure(g.hitLog, static_cast<size_t>(g.pathCap) * g.depthCap * 4);
     if (g.sortShading) ensure(g.sortQueue, static_cast<size_t>(g.pathCap) * kSortKeys * 4);
+    if (g.orderBounces > 0 && !g.pathKey.p) {   // keys padded to whole tiles, padding never written
+        const int tiles = orderTiles(g.pathCap);
+        ensure(g.pathKey, static_cast<size_t>(tiles) * kOrderTile);
+        ck(cudaMemset(g.pathKey.p, kKeyDead, static_cast<size_t>(tiles) * kOrderTile), "cudaMemset");
+        ensure(g.orderTiles, static_cast<size_t>(tiles) * 8 * sizeof(int));
+    }
     if (g.raySortBits > 0) {
         ensure(g.rayBin, static_cast<size_t>(g.pathCap) * 4);
         ensure(g.sortedQueue, static_cast<size_t>(g.pathCap) * 4);
@@ -405,14 +423,18 @@ void launchBounces(const DevScene& s, const DevPaths& P, const FrameParams& f, i
     for (int b = 0; b < depth; ++b) {
         if (P.raySortBits > 0 && b >= 1 && b <= P.raySortBounces) launchRaySort(P, b, g.gridShade, st);
         launchExtend(s, P, b, g.gridExtend, block, st);
+        if (b < P.orderBounces) launchOrder(P, b, false, st);
         if (g.overlapConnect && b > 0) ck(cudaStreamWaitEvent(st, g.evConnect, 0), "cudaStreamWaitEvent");
         launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
+        const bool orderNext = b + 1 < P.orderBounces && b + 1 < depth;
         if (g.overlapConnect) {
             ck(cudaEventRecord(g.evShade, st), "cudaEventRecord");
             ck(cudaStreamWaitEvent(g.side, g.evShade, 0), "cudaStreamWaitEvent");
             launchConnect(s, P, b, g.gridConnect, block, g.side);
             ck(cudaEventRecord(g.evConnect, g.side), "cudaEventRecord");
+            if (orderNext) launchOrder(P, b, true, st);
         } else {
+            if (orderNext) launchOrder(P, b, true, st);
             launchConnect(s, P, b, g.gridConnect, block, st);
         }
     }
@@ -469,6 +491,7 @@ void renderFrame(int w, int h)
     P.sortCount = g.sortCount.as<int>();
     P.tailPaths = mega ? 0 : g.tailPaths;
     setRaySort(P, !mega);
+    setOrder(P, !mega);
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
     f.width = w; f.height = h; f.spp = spp;
@@ -557,8 +580,12 @@ void renderFrame(int w, int h)
             timed(1, [&] {
                 if (P.raySortBits > 0 && b >= 1 && b <= P.raySortBounces) launchRaySort(P, b, g.gridShade, st);
                 launchExtend(s, P, b, g.gridExtend, block, st);
+                if (b < P.orderBounces) launchOrder(P, b, false, st);
             });
-            timed(2, [&] { launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st); });
+            timed(2, [&] {
+                launchShade(s, P, f, b, g.gridShade, block, g.shadeMinBlocks, st);
+                if (b + 1 < P.orderBounces && b + 1 < depth) launchOrder(P, b, true, st);
+            });
             timed(3, [&] { launchConnect(s, P, b, g.gridConnect, block, st); });
         }
         timed(5, [&] { launchTail(s, P, f, st); });
@@ -690,6 +717,7 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
     // start to end in the tail kernel (the wavefront's per-sample streams, bit-identical images).
     P.tailPaths = g.renderMode == BTE_RENDER_MEGAKERNEL ? 0x7fffffff : g.tailPaths;
     setRaySort(P, g.renderMode != BTE_RENDER_MEGAKERNEL);
+    setOrder(P, g.renderMode != BTE_RENDER_MEGAKERNEL);
     FrameParams f;
     std::memset(&f, 0, sizeof(f));
     f.frameIndex = g.dFrameIndex.as<uint32_t>();
@@ -1002,6 +1030,7 @@ bool renderSceneBatchFused(const int* scenes, const int* viewCounts, const BteVi
         P.sortCount = g.sortCount.as<int>();
         P.tailPaths = g.tailPaths;
         setRaySort(P, true);
+        setOrder(P, true);
         P.scenes = g_fused.sceneTable.as<DevScene>();
         P.pathScene = g_fused.pathScene.as<uint8_t>();
         P.sceneCount = sceneCount;
@@ -1725,6 +1754,7 @@ int bte_set_tuning(const BteTuning* t)
         if (t->raySortBounces < 1 || t->raySortBounces > 64) throw CudaError{"bte_set_tuning: raySortBounces in [1, 64]"};
         if (t->leafTestsPerStep < 0 || t->leafTestsPerStep > 24)
             throw CudaError{"bte_set_tuning: leafTestsPerStep in [0, 24]"};
+        if (t->orderBounces < 0 || t->orderBounces > 64) throw CudaError{"bte_set_tuning: orderBounces in [0, 64]"};
         g.bvhWidth = t->bvhWidth;
         g.maxLeaf = t->maxLeafTriangles;
         g.shadeMinBlocks = t->shadeMinBlocks;
@@ -1738,6 +1768,7 @@ int bte_set_tuning(const BteTuning* t)
         g.raySortBits = t->raySortBits;
         g.raySortBounces = t->raySortBounces;
         g.leafTestsPerStep = t->leafTestsPerStep;
+        g.orderBounces = t->orderBounces;
         g.gridBlock = 0;   // recompute persistent grids
         return 0;
     });
@@ -1760,6 +1791,7 @@ int bte_get_tuning(BteTuning* t)
         t->raySortBits = g.raySortBits;
         t->raySortBounces = g.raySortBounces;
         t->leafTestsPerStep = g.leafTestsPerStep;
+        t->orderBounces = g.orderBounces;
         return 0;
     });
 }

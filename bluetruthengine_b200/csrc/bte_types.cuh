@@ -141,8 +141,20 @@ struct DevPaths {
     const DevScene* scenes;   // [sceneCount]
     uint8_t* pathScene;       // [count]
     int sceneCount;
+    // path-ordered queues for the first orderBounces bounces (material-sorted shading on, ray reordering off):
+    // extend records each path's bucket in pathKey instead of appending it, shade records kKeyNext or kKeyDead,
+    // and a stable compaction over path indices (kOrderCount, kOrderScan, kOrderScatter) writes the material
+    // buckets and the next bounce's queue in ascending path order, so that the 32 paths of a warp are
+    // neighbours in the path-state arrays (float4 entries share 32-byte sectors) instead of scattered
+    uint8_t* pathKey;         // [count rounded up to kOrderTile]
+    int* orderTiles;          // [tiles * 8] per-tile key counts, then per-tile starts
+    int orderBounces;
 };
 constexpr int kRaySortMinRays = 32768;
+constexpr int kOrderTile = 4096;            // paths per tile of the ordered compaction (256 threads x 16)
+constexpr uint8_t kKeyNext = 6;             // pathKey: the path continues to the next bounce
+constexpr uint8_t kKeyDead = 0xff;          // pathKey: the path has ended
+static_assert(kKeyNext >= kSortKeys, "next-bounce key distinct from the material buckets");
 
 // One camera view of a batched frame (bte_render_views): its paths are
 // [pathOffset, pathOffset + width*height*spp) of the frame, sample-major as

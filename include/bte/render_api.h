@@ -177,6 +177,11 @@ typedef struct {
     int leafTestsPerStep;  /* 8-wide walk: 0 tests all triangles of a node's hit leaves in the step that fetched
                             * the node; 1-24 tests at most that many per step and fetches the next node only
                             * when they are done (lanes with many triangles hold their warp less long) */
+    int orderBounces;      /* 0: off; 1-64: for bounces 0..orderBounces-1 the material buckets and the next
+                            * bounce's queue are rebuilt in ascending path order by a stable compaction over
+                            * path indices (instead of atomic appends in completion order), so a warp's paths
+                            * are neighbours in the path-state arrays (default 3); active only with
+                            * sortShading 1 and raySortBits 0; results do not depend on it */
 } BteTuning;
 int bte_set_tuning(const BteTuning* tuning);
 int bte_get_tuning(BteTuning* tuning);

@@ -52,10 +52,10 @@ def test_math_functions_bitexact(renderer, oracle_mod):
 
 
 def _upload(renderer, scene, env_mode=0, spp=1, depth=8, bvh_width=8, max_leaf=1, sort_shading=0, tail_paths=0,
-            builder=1, radius=8, collapse=1, ray_sort=0, leaf_tests=0):
+            builder=1, radius=8, collapse=1, ray_sort=0, leaf_tests=0, order=0):
     renderer.cleanup()
     renderer.set_tuning(max_leaf, 3, bvh_width, 20, sort_shading, tail_paths, builder, radius, 1, collapse, ray_sort, 4,
-                        leaf_tests)
+                        leaf_tests, order)
     renderer.upload(scene)
     renderer.set_config(samples_per_frame=spp, max_depth=depth, rr_start=3, env_sampling=env_mode)
 
@@ -270,22 +270,25 @@ def test_texture_filter_pin(renderer):
         assert rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder,ray_sort,leaf_tests",
-                         [(1, 8, 0, 0, 0, 0, 0), (0, 8, 0, 0, 0, 0, 0), (1, 2, 0, 0, 0, 0, 0), (1, 8, 1, 0, 0, 0, 0),
-                          (1, 8, 1, 200000, 0, 0, 0), (1, 8, 1, 0, 1, 0, 0), (0, 2, 0, 0, 1, 0, 0), (1, 8, 1, 0, 1, 3, 0),
-                          (1, 2, 0, 0, 1, 2, 0), (1, 8, 1, 0, 1, 3, 1), (0, 8, 1, 0, 1, 0, 2)])
+@pytest.mark.parametrize("env_mode,bvh_width,sort_shading,tail_paths,builder,ray_sort,leaf_tests,order",
+                         [(1, 8, 0, 0, 0, 0, 0, 0), (0, 8, 0, 0, 0, 0, 0, 0), (1, 2, 0, 0, 0, 0, 0, 0),
+                          (1, 8, 1, 0, 0, 0, 0, 0), (1, 8, 1, 200000, 0, 0, 0, 0), (1, 8, 1, 0, 1, 0, 0, 0),
+                          (0, 2, 0, 0, 1, 0, 0, 0), (1, 8, 1, 0, 1, 3, 0, 0), (1, 2, 0, 0, 1, 2, 0, 0),
+                          (1, 8, 1, 0, 1, 3, 1, 0), (0, 8, 1, 0, 1, 0, 2, 0), (1, 8, 1, 0, 1, 0, 0, 3),
+                          (0, 8, 1, 0, 1, 0, 0, 16), (1, 2, 1, 0, 1, 0, 0, 2), (1, 8, 1, 200000, 1, 0, 0, 4)])
 def test_bench_scene_subset_bitexact(renderer, oracle_mod, bte, env_mode, bvh_width, sort_shading, tail_paths,
-                                     builder, ray_sort, leaf_tests):
+                                     builder, ray_sort, leaf_tests, order):
     """The 1920x1080, ~1.04M-triangle Disney/env-map workload: a full frame on the GPU, 6000 random
     pixels re-traced by the oracle (its own CPU BVH), compared bit-for-bit; with and without the rays of
-    bounces 1-4 reordered by direction octant and origin cell, and with the 8-wide walk's triangle tests
-    spread over steps (1 or 2 per step)."""
+    bounces 1-4 reordered by direction octant and origin cell, with the 8-wide walk's triangle tests
+    spread over steps (1 or 2 per step), and with the first 2, 3, 4 or all bounces' queues rebuilt in path
+    order (also with the tail kernel taking over)."""
     from bluetruthengine_b200 import scenes
     scene = bte.load_scene(scenes.disney_spheres())
     W, H, depth = scene.width, scene.height, 16
     _upload(renderer, scene, env_mode=env_mode, spp=1, depth=depth, bvh_width=bvh_width, sort_shading=sort_shading,
             tail_paths=tail_paths, max_leaf=1 if bvh_width == 2 else 2, builder=builder, ray_sort=ray_sort,
-            leaf_tests=leaf_tests)
+            leaf_tests=leaf_tests, order=order)
     info = renderer.accel_info()
     print("accel", info)
     assert info["width"] == bvh_width and info["builder"] == builder
@@ -437,11 +440,12 @@ def test_tuning_roundtrip_and_validation(renderer):
     assert renderer.tuning() == {"bvhWidth": 8, "maxLeafTriangles": 2, "shadeMinBlocks": 2, "postponePercent": 35,
                                  "sortShading": 1, "tailPaths": 4096, "bvhBuilder": 1, "plocRadius": 7,
                                  "overlapConnect": 1, "wideCollapse": 1, "raySortBits": 0, "raySortBounces": 4,
-                                 "leafTestsPerStep": 0}
+                                 "leafTestsPerStep": 0, "orderBounces": 3}
     for bad in [(1, 3, 4, 20), (4, 3, 8, 20), (65, 3, 2, 20), (1, 1, 8, 20), (1, 3, 8, 101), (1, 3, 8, 20, 2),
                 (1, 3, 8, 20, 1, -1), (1, 3, 8, 20, 1, 0, 2), (1, 3, 8, 20, 1, 0, 1, 0), (1, 3, 8, 20, 1, 0, 1, 33),
                 (1, 3, 8, 20, 1, 0, 1, 16, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 2), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 5),
-                (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 2, 0), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 0, 4, 25)]:
+                (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 2, 0), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 0, 4, 25),
+                (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 0, 4, 0, 65), (1, 3, 8, 20, 1, 0, 1, 16, 1, 1, 0, 4, 0, -1)]:
         with pytest.raises(B.BteError):
             renderer.set_tuning(*bad)
     renderer.set_tuning()
@@ -653,9 +657,10 @@ def test_megakernel_features_and_denoiser(renderer, bte, cornell_scene):
         renderer.set_render_mode(1)
 
 
+@pytest.mark.parametrize("order", [0, 3])
 @pytest.mark.parametrize("sizes,frames", [([(64, 48, 1), (40, 30, 2), (100, 20, 3)], 2),
                                           ([(64, 48, 4), (40, 30, 24), (100, 20, 64)], 4)])
-def test_batched_views_match_single_view_frames(renderer, bte, random_scene, sizes, frames):
+def test_batched_views_match_single_view_frames(renderer, bte, random_scene, sizes, frames, order):
     """Three views of uneven size and samples per frame rendered in one launch sequence: each view's FP32 mean
     and FP64 sum equal those of bte_render with that camera, bit for bit.  The second case accumulates the views
     to 16, 96 and 256 samples per pixel (4 frames of 4, 24 and 64), inside the 16-256 range the batched
@@ -668,7 +673,7 @@ def test_batched_views_match_single_view_frames(renderer, bte, random_scene, siz
         cam["origin"] = cam["origin"] + np.float32(0.4 * k) * cam["right"]
         cam["aspect"] = np.float32(w / h)
         views.append((cam, w, h, spp))
-    _upload(renderer, sc, env_mode=1, spp=1, depth=10)
+    _upload(renderer, sc, env_mode=1, spp=1, depth=10, sort_shading=1, order=order)
     renderer.reset_views()
     for _ in range(frames):
         renderer.render_views(views)
@@ -733,14 +738,16 @@ def _views_of(bte, scene, sizes):
     return views
 
 
-@pytest.mark.parametrize("use_graph,batch_mode", [(0, 0), (1, 0), (0, 1), (1, 1)])
-def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene, use_graph, batch_mode):
+@pytest.mark.parametrize("use_graph,batch_mode,order", [(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0), (1, 1, 3),
+                                                        (0, 0, 3)])
+def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornell_scene, use_graph, batch_mode,
+                                             order):
     """Two scene slots (the random scene with its env map and spotlight, the Cornell box), each with views of
     uneven size and samples per frame, rendered in one batch for two frames: in batch mode 1 as one launch sequence
     over both scenes' paths (each path looking up its scene), in mode 0 side by side (separate streams, or one
     launch of a graph holding each scene's captured view frame).  Every view's FP32 mean and FP64 sum equal those
     of eager bte_render_views on that slot alone, bit for bit, and so do captured single-slot view frames; the
-    selected slot is restored."""
+    selected slot is restored.  With `order`, the first bounces' queues are rebuilt in path order."""
     depths = (10, 10) if batch_mode else (10, 8)   # one launch sequence needs one max depth
     scenes = [(random_scene, 1, depths[0], [(64, 48, 1), (40, 30, 2)]),
               (cornell_scene, 0, depths[1], [(50, 50, 2), (32, 24, 1), (70, 20, 3)])]
@@ -749,7 +756,7 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
     try:
         for slot, (sc, env_mode, depth, sizes) in enumerate(scenes):
             renderer.select_scene(slot)
-            _upload(renderer, sc, env_mode=env_mode, spp=1, depth=depth)
+            _upload(renderer, sc, env_mode=env_mode, spp=1, depth=depth, sort_shading=1, order=order)
             renderer.set_config(samples_per_frame=1, max_depth=depth, rr_start=3, env_sampling=env_mode,
                                 use_graph=use_graph)
             renderer.reset_views()
@@ -794,9 +801,9 @@ def test_scene_batch_matches_per_scene_views(renderer, bte, random_scene, cornel
 
 
 def test_autotune_picks_fastest_and_keeps_bits(renderer, random_scene):
-    """The autotuner over tree width, block size (64-256) and the compaction threshold (tail kernel below it) keeps
-    the fastest configuration it timed, leaves the renderer in it, and every configuration renders the same bits
-    as a fixed one."""
+    """The autotuner over tree width, block size (64-256), the compaction threshold (tail kernel below it) and the
+    path-ordered bounces keeps the fastest configuration it timed, leaves the renderer in it, and every
+    configuration renders the same bits as a fixed one."""
     from bluetruthengine_b200.autotune import autotune
     sc = random_scene
     W, H = 64, 48
@@ -806,10 +813,11 @@ def test_autotune_picks_fastest_and_keeps_bits(renderer, random_scene):
     renderer.render(W, H)
     fixed = renderer.read_accum(W, H).copy()
     best, results = autotune(renderer, W, H, 1, 8, 1, trees=((8, 1), (2, 1)), blocks=(64, 256),
-                             shade_min_blocks=(3,), postpone=(0,), tail_paths=(0, 1 << 12), frames=1)
-    assert len(results) == 2 * 2 * 2
+                             shade_min_blocks=(3,), postpone=(0,), tail_paths=(0, 1 << 12), order=(0, 3), frames=1)
+    assert len(results) == 2 * 2 * 2 * 2
     assert best.ms_per_frame == min(r.ms_per_frame for r in results)
     t = renderer.tuning()
-    assert (t["bvhWidth"], t["maxLeafTriangles"], t["tailPaths"]) == (best.bvh_width, best.max_leaf, best.tail_paths)
+    assert (t["bvhWidth"], t["maxLeafTriangles"], t["tailPaths"], t["orderBounces"]) == \
+        (best.bvh_width, best.max_leaf, best.tail_paths, best.order_bounces)
     renderer.render(W, H)
     assert np.array_equal(bits(renderer.read_accum(W, H)), bits(fixed))
