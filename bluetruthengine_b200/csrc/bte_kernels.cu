@@ -380,117 +380,172 @@ __global__ void __launch_bounds__(256) kRayScatter(DevPaths P, int bounce)
 }
 
 // ---------------------------------------------------------------- path-ordered queues
-// A stable counting sort of the paths 0 .. count-1 by pathKey, for one bounce and one selection of keys lo ..
-// lo+n-1: the material buckets after extend (keys 0 .. kSortKeys-1 into sortQueue's bucket regions, totals into
-// sortCount) or the next bounce's queue after shade (key kKeyNext into queue[(bounce + 1) & 1], total into
-// rayCount[bounce + 1]).  A tile is kOrderTile consecutive paths, 16 per thread of a 256-thread block (one
-// 16-byte load of their keys; pathKey is padded to whole tiles).  Inside a key the paths keep index order.
+// One launch per bounce and selection: a stable counting sort of the paths 0 .. count-1 by pathKey into the
+// material buckets after extend (keys 0 .. kSortKeys-1 into sortQueue's bucket regions, totals into sortCount)
+// or the next bounce's queue after shade (key kKeyNext into queue[(bounce + 1) & 1], total into
+// rayCount[bounce + 1]); inside a key the paths keep index order.  A tile is kOrderTile consecutive paths, 32 per
+// thread of a 256-thread block (two 16-byte loads of their keys; pathKey is padded to whole tiles).  Tiles are
+// taken in order from a ticket counter and find their output offsets by decoupled look-back (Merrill & Garland
+// 2016): each publishes its per-key counts, then sums its predecessors' published words back to the first
+// inclusive one.  A predecessor holds an earlier ticket, so it is running or done and its word arrives; the wait
+// is bounded all the same (error flag bit 2; the offsets stay in range).  One warp per key reads 128 predecessors'
+// words per round.  The tile's paths are staged in shared memory key by key and written out as contiguous runs.
+constexpr unsigned long long kOrderAggregate = 1ull << 32;   // status word: the tile's own count
+constexpr unsigned long long kOrderInclusive = 2ull << 32;   // status word: the count through this tile
+constexpr int kOrderWaitLimit = 1 << 22;
+constexpr int kOrderLookDepth = 4;   // look-back words per lane and round: 128 predecessors
 
-// keys of this thread's 16 paths; paths at or beyond count read as ended
-BTE_DI void orderKeys(const DevPaths& P, uint8_t (&k)[16], int& first)
-{
-    first = static_cast<int>(blockIdx.x) * kOrderTile + static_cast<int>(threadIdx.x) * 16;
-    const uint4 w = *reinterpret_cast<const uint4*>(P.pathKey + first);
-    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        const uint8_t v = static_cast<uint8_t>(words[e >> 2] >> (8 * (e & 3)));
-        k[e] = first + e < P.count ? v : kKeyDead;
-    }
-}
-BTE_DI int orderCountKey(const uint8_t (&k)[16], int key)
-{
-    int c = 0;
-#pragma unroll
-    for (int e = 0; e < 16; ++e) c += k[e] == key ? 1 : 0;
-    return c;
-}
 // exclusive prefix of v over the block's threads (in thread order) and the block's total; every thread calls it
-BTE_DI int blockExclusiveScan(int v, int* warpSum, int& total)
+template <class T>
+BTE_DI T blockExclusiveScan(T v, T* warpSum, T& total)
 {
     const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
     const int warps = static_cast<int>(blockDim.x >> 5);
-    int x = v;
+    T x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) warpSum[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        int w = lane < warps ? warpSum[lane] : 0;
+        T w = lane < warps ? warpSum[lane] : T(0);
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            const T y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += y;
         }
         warpSum[lane] = w;
     }
     __syncthreads();
     total = warpSum[warps - 1];
-    const int excl = x - v + (warp > 0 ? warpSum[warp - 1] : 0);
+    const T excl = x - v + (warp > 0 ? warpSum[warp - 1] : T(0));
     __syncthreads();   // warpSum is reused by the next call
     return excl;
 }
 
-// per-tile counts of keys lo .. lo+n-1 -> orderTiles[tile * 8 + j]
-__global__ void __launch_bounds__(256) kOrderCount(DevPaths P, int bounce, int lo, int n)
+__global__ void __launch_bounds__(256, 4) kOrderCompact(DevPaths P, int bounce, int lo, int n, int* out, int stride,
+                                                     int compaction)
 {
     if (tailTakesOver(P, bounce)) return;
-    __shared__ int warpSum[32];
-    uint8_t k[16];
-    int first;
-    orderKeys(P, k, first);
-    for (int j = 0; j < n; ++j) {
-        int total;
-        blockExclusiveScan(orderCountKey(k, lo + j), warpSum, total);
-        if (threadIdx.x == 0) P.orderTiles[blockIdx.x * 8 + j] = total;
-    }
-}
-
-// per-tile counts -> per-tile starts (exclusive over tiles, per key) and the totals; one block
-__global__ void __launch_bounds__(1024) kOrderScan(DevPaths P, int bounce, int lo, int n, int tiles)
-{
-    if (tailTakesOver(P, bounce)) return;
-    __shared__ int warpSum[32];
-    const int per = (tiles + static_cast<int>(blockDim.x) - 1) / static_cast<int>(blockDim.x);
-    const int t0 = static_cast<int>(threadIdx.x) * per;
-    const int t1 = min(t0 + per, tiles);
-    for (int j = 0; j < n; ++j) {
-        int sum = 0;
-        for (int t = t0; t < t1; ++t) sum += P.orderTiles[t * 8 + j];
-        int total;
-        int run = blockExclusiveScan(sum, warpSum, total);
-        for (int t = t0; t < t1; ++t) {
-            const int c = P.orderTiles[t * 8 + j];
-            P.orderTiles[t * 8 + j] = run;
-            run += c;
-        }
-        if (threadIdx.x == 0) {
-            if (lo == kKeyNext) P.rayCount[bounce + 1] = total;
-            else P.sortCount[bounce * kSortKeys + lo + j] = total;
-        }
-    }
-}
-
-// each path of a selected key to out[j * stride + its rank]
-__global__ void __launch_bounds__(256) kOrderScatter(DevPaths P, int bounce, int lo, int n, int* out, int stride)
-{
-    if (tailTakesOver(P, bounce)) return;
-    __shared__ int warpSum[32];
-    uint8_t k[16];
-    int first;
-    orderKeys(P, k, first);
-    for (int j = 0; j < n; ++j) {
-        const int c = orderCountKey(k, lo + j);
-        int total;
-        int pos = P.orderTiles[blockIdx.x * 8 + j] + blockExclusiveScan(c, warpSum, total);
-        if (c == 0) continue;
-        int* o = out + static_cast<size_t>(j) * stride;
+    __shared__ unsigned long long warpSum[32];
+    __shared__ int tileSh;
+    __shared__ int keyStart[kSortKeys], keyTotal[kSortKeys], keyBase[kSortKeys];
+    __shared__ int stage[kOrderTile];
+    const int tiles = (P.count + kOrderTile - 1) / kOrderTile;
+    unsigned long long* status = P.orderStatus + static_cast<size_t>(compaction) * tiles * kSortKeys;
+    if (threadIdx.x == 0) tileSh = atomicAdd(P.orderTicket + compaction, 1);
+    __syncthreads();
+    const int tile = tileSh;
+    // this thread's 32 keys (two 16-byte loads), key e in byte e & 3 of word e >> 2; paths at or beyond count
+    // read as ended
+    const int first = tile * kOrderTile + static_cast<int>(threadIdx.x) * 32;
+    const uint4 kw0 = *reinterpret_cast<const uint4*>(P.pathKey + first);
+    const uint4 kw1 = *reinterpret_cast<const uint4*>(P.pathKey + first + 16);
+    uint32_t words[8] = {kw0.x, kw0.y, kw0.z, kw0.w, kw1.x, kw1.y, kw1.z, kw1.w};
+    if (first + 32 > P.count) {
 #pragma unroll
-        for (int e = 0; e < 16; ++e)
-            if (k[e] == lo + j) o[pos++] = first + e;
+        for (int e = 0; e < 32; ++e)
+            if (first + e >= P.count) words[e >> 2] |= 0xffu << (8 * (e & 3));
+    }
+    // per-key counts of the thread, 16 bits per key: keys lo .. lo+3 in cA, lo+4 .. lo+5 in cB
+    unsigned long long cA = 0, cB = 0;
+#pragma unroll
+    for (int e = 0; e < 32; ++e) {
+        const unsigned int d = ((words[e >> 2] >> (8 * (e & 3))) & 0xffu) - static_cast<unsigned int>(lo);
+        if (d < static_cast<unsigned int>(n)) {
+            if (d < 4u) cA += 1ull << (16 * d);
+            else cB += 1ull << (16 * (d - 4u));
+        }
+    }
+    unsigned long long tA, tB = 0;
+    const unsigned long long xA = blockExclusiveScan(cA, warpSum, tA);
+    unsigned long long xB = 0;
+    if (n > 4) xB = blockExclusiveScan(cB, warpSum, tB);
+    // per key: this thread's first staging slot, the tile's count and its start in the staging array
+    int pos[kSortKeys];
+    int run = 0;
+#pragma unroll
+    for (int j = 0; j < kSortKeys; ++j) {
+        const unsigned long long x = j < 4 ? xA : xB, t = j < 4 ? tA : tB;
+        const int sh = 16 * (j & 3);
+        const int total = j < n ? static_cast<int>((t >> sh) & 0xffffu) : 0;
+        pos[j] = run + static_cast<int>((x >> sh) & 0xffffu);
+        if (threadIdx.x == 0 && j < n) { keyStart[j] = run; keyTotal[j] = total; }
+        run += total;
+    }
+    __syncthreads();   // keyStart / keyTotal (written by thread 0) before any warp reads them
+    // publish, look back, publish the inclusive count: warp j for key j, 128 predecessors per round
+    const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31u);
+    if (warp < n) {
+        const int j = warp;
+        volatile unsigned long long* st = status + static_cast<size_t>(tile) * kSortKeys + j;
+        const unsigned int own = static_cast<unsigned int>(keyTotal[j]);
+        if (lane == 0) *st = (tile == 0 ? kOrderInclusive : kOrderAggregate) | own;
+        unsigned int prefix = 0;
+        for (int base = tile - 1; base >= 0; base -= 32 * kOrderLookDepth) {
+            // predecessor base - (32 q + lane) in word q of this lane; before the first tile: inclusive 0
+            unsigned long long w[kOrderLookDepth];
+            const volatile unsigned long long* ps[kOrderLookDepth];
+            bool wait = false;
+#pragma unroll
+            for (int q = 0; q < kOrderLookDepth; ++q) {
+                const int p = base - 32 * q - lane;
+                ps[q] = status + static_cast<size_t>(p < 0 ? 0 : p) * kSortKeys + j;
+                w[q] = p >= 0 ? *ps[q] : kOrderInclusive;
+                wait |= (w[q] >> 32) == 0ull;
+            }
+            for (int spins = 0; __any_sync(0xffffffffu, wait); ++spins) {
+                if (spins > kOrderWaitLimit) {   // never for a running grid: give up with the error flag
+                    if (lane == 0) atomicOr(P.errorFlags, 4u);
+#pragma unroll
+                    for (int q = 0; q < kOrderLookDepth; ++q) w[q] = kOrderInclusive;
+                    break;
+                }
+                __nanosleep(64);
+                wait = false;
+#pragma unroll
+                for (int q = 0; q < kOrderLookDepth; ++q) {
+                    if ((w[q] >> 32) == 0ull) w[q] = *ps[q];
+                    wait |= (w[q] >> 32) == 0ull;
+                }
+            }
+            // the nearest inclusive word (smallest 32 q + lane) ends the sum
+            bool found = false;
+#pragma unroll
+            for (int q = 0; q < kOrderLookDepth; ++q) {
+                if (found) break;
+                const unsigned int inc = __ballot_sync(0xffffffffu, (w[q] >> 32) == 2ull);
+                const int stop = inc ? __ffs(inc) - 1 : 31;
+                prefix += __reduce_add_sync(0xffffffffu, lane <= stop ? static_cast<unsigned int>(w[q]) : 0u);
+                found = inc != 0u;
+            }
+            if (found) break;
+        }
+        if (lane == 0) {
+            if (tile > 0) *st = kOrderInclusive | (prefix + own);
+            keyBase[j] = static_cast<int>(prefix);
+            if (tile == tiles - 1) {
+                const int total = static_cast<int>(prefix + own);
+                if (lo == kKeyNext) P.rayCount[bounce + 1] = total;
+                else P.sortCount[bounce * kSortKeys + lo + j] = total;
+            }
+        }
+    }
+    // stage the tile's selected paths key by key, in index order
+#pragma unroll
+    for (int e = 0; e < 32; ++e) {
+        const unsigned int d = ((words[e >> 2] >> (8 * (e & 3))) & 0xffu) - static_cast<unsigned int>(lo);
+#pragma unroll
+        for (int jj = 0; jj < kSortKeys; ++jj)
+            if (d == static_cast<unsigned int>(jj) && jj < n) stage[pos[jj]++] = first + e;
+    }
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        int* o = out + static_cast<size_t>(j) * stride + keyBase[j];
+        const int* src = stage + keyStart[j];
+        for (int i = static_cast<int>(threadIdx.x); i < keyTotal[j]; i += static_cast<int>(blockDim.x)) o[i] = src[i];
     }
 }
 
@@ -1009,15 +1064,13 @@ void launchRaySort(const DevPaths& P, int bounce, int grid, cudaStream_t st)
     kRayScatter<<<grid, 256, 0, st>>>(P, bounce);
 }
 int orderTiles(int paths) { return (paths + kOrderTile - 1) / kOrderTile; }
+// compaction 2b builds bounce b's buckets, 2b+1 the queue of bounce b+1 (each has its own ticket and status words)
 void launchOrder(const DevPaths& P, int bounce, bool nextQueue, cudaStream_t st)
 {
-    const int tiles = orderTiles(P.count);
     const int lo = nextQueue ? kKeyNext : 0, n = nextQueue ? 1 : kSortKeys;
     int* out = nextQueue ? P.queue[(bounce + 1) & 1] : P.sortQueue;
     const int stride = nextQueue ? 0 : P.count;
-    kOrderCount<<<tiles, 256, 0, st>>>(P, bounce, lo, n);
-    kOrderScan<<<1, 1024, 0, st>>>(P, bounce, lo, n, tiles);
-    kOrderScatter<<<tiles, 256, 0, st>>>(P, bounce, lo, n, out, stride);
+    kOrderCompact<<<orderTiles(P.count), 256, 0, st>>>(P, bounce, lo, n, out, stride, 2 * bounce + (nextQueue ? 1 : 0));
 }
 // Frames over several scenes (P.scenes) run the stage kernels' multi-scene instances; those scenes all use the
 // 8-wide tree (checked by the host).

@@ -125,7 +125,8 @@ struct Renderer {
     uint32_t* extFramebuffer = nullptr;
     // wavefront buffers
     DeviceBuffer pO, pD, pTp, pL, pHit, q0, q1, rayCount, shadowCount, fetch, shadowQueue, shOrigin, shDir, shContrib,
-        shMask, hitLog, errorFlags, sortQueue, sortCount, rayBin, sortedQueue, binCount, pathKey, orderTiles;
+        shMask, hitLog, errorFlags, sortQueue, sortCount, rayBin, sortedQueue, binCount, pathKey, orderStatus,
+        orderTicket;
     int pathCap = 0, slotCap = 0, depthCap = 0;
     bool hitLogEnabled = false;
     bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
@@ -305,7 +306,7 @@ void releaseWavefront()
     releaseViewGraph();
     for (DeviceBuffer* b : {&g.pO, &g.pD, &g.pTp, &g.pL, &g.pHit, &g.q0, &g.q1, &g.rayCount, &g.shadowCount, &g.fetch,
                             &g.sortQueue, &g.sortCount, &g.shadowQueue, &g.rayBin, &g.sortedQueue, &g.binCount,
-                            &g.pathKey, &g.orderTiles,
+                            &g.pathKey, &g.orderStatus, &g.orderTicket,
                             &g.shOrigin, &g.shDir, &g.shContrib, &g.shMask, &g.hitLog, &g.errorFlags})
         b->release();
     g.aovAlbedo.release(); g.aovNormal.release();
@@ -326,14 +327,29 @@ void setRaySort(DevPaths& P, bool on)
     P.raySortBounces = g.raySortBounces;
 }
 
+// look-back words of a frame's ordered compactions (two per ordered bounce) over `paths` paths
+size_t orderStatusBytes(int paths)
+{
+    return static_cast<size_t>(2 * g.orderBounces) * orderTiles(paths) * kSortKeys * sizeof(unsigned long long);
+}
+
 // path-ordered queue fields of a frame's DevPaths (off in megakernel mode, without material-sorted shading and
 // with ray reordering, which appends the next queue in bin order)
 void setOrder(DevPaths& P, bool on)
 {
     if (!on || g.orderBounces <= 0 || !P.sortQueue || P.raySortBits > 0) return;
     P.pathKey = g.pathKey.as<uint8_t>();
-    P.orderTiles = g.orderTiles.as<int>();
+    P.orderStatus = g.orderStatus.as<unsigned long long>();
+    P.orderTicket = g.orderTicket.as<int>();
     P.orderBounces = g.orderBounces;
+}
+
+// frame prologue of the ordered compactions: clear their tickets and look-back words
+void clearOrder(const DevPaths& P, cudaStream_t st)
+{
+    if (P.orderBounces <= 0) return;
+    ck(cudaMemsetAsync(g.orderStatus.p, 0, orderStatusBytes(P.count), st), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(g.orderTicket.p, 0, sizeof(int) * 2 * P.orderBounces, st), "cudaMemsetAsync");
 }
 
 void ensureWavefront(int paths, int slots, int depth)
@@ -341,7 +357,8 @@ void ensureWavefront(int paths, int slots, int depth)
     const bool grow = paths > g.pathCap || slots > g.slotCap || depth > g.depthCap;
     const size_t binBytes = g.raySortBits > 0 ? rayBinBytes() : 0;
     if (!grow && (!g.hitLogEnabled || g.hitLog.p) && (!g.sortShading || g.sortQueue.p) &&
-        (!g.raySortBits || (g.sortedQueue.p && g.binCount.bytes >= binBytes)) && (!g.orderBounces || g.pathKey.p))
+        (!g.raySortBits || (g.sortedQueue.p && g.binCount.bytes >= binBytes)) &&
+        (!g.orderBounces || (g.pathKey.p && g.orderStatus.bytes >= orderStatusBytes(g.pathCap))))
         return;
     if (grow) {
         releaseWavefront();
@@ -362,11 +379,14 @@ void ensureWavefront(int paths, int slots, int depth)
     }
     if (g.hitLogEnabled) ensure(g.hitLog, static_cast<size_t>(g.pathCap) * g.depthCap * 4);
     if (g.sortShading) ensure(g.sortQueue, static_cast<size_t>(g.pathCap) * kSortKeys * 4);
-    if (g.orderBounces > 0 && !g.pathKey.p) {   // keys padded to whole tiles, padding never written
-        const int tiles = orderTiles(g.pathCap);
-        ensure(g.pathKey, static_cast<size_t>(tiles) * kOrderTile);
-        ck(cudaMemset(g.pathKey.p, kKeyDead, static_cast<size_t>(tiles) * kOrderTile), "cudaMemset");
-        ensure(g.orderTiles, static_cast<size_t>(tiles) * 8 * sizeof(int));
+    if (g.orderBounces > 0) {
+        if (!g.pathKey.p) {   // keys padded to whole tiles, padding never written
+            const size_t bytes = static_cast<size_t>(orderTiles(g.pathCap)) * kOrderTile;
+            ensure(g.pathKey, bytes);
+            ck(cudaMemset(g.pathKey.p, kKeyDead, bytes), "cudaMemset");
+        }
+        ensure(g.orderStatus, orderStatusBytes(g.pathCap));
+        ensure(g.orderTicket, sizeof(int) * 2 * 64);
     }
     if (g.raySortBits > 0) {
         ensure(g.rayBin, static_cast<size_t>(g.pathCap) * 4);
@@ -513,6 +533,7 @@ void renderFrame(int w, int h)
         ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
         if (P.raySortBits > 0) ck(cudaMemsetAsync(g.binCount.p, 0, rayBinBytes(), st), "cudaMemsetAsync");
+        clearOrder(P, st);
         if (g.hitLogEnabled) ck(cudaMemsetAsync(g.hitLog.p, 0xfe, static_cast<size_t>(paths) * depth * 4, st), "cudaMemsetAsync");
         ck(cudaMemcpyAsync(g.dFrameIndex.p, g.hFrameIndex, sizeof(uint32_t), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
     };
@@ -620,7 +641,7 @@ void renderFrame(int w, int h)
                 S.tailShadowRays += sc[static_cast<size_t>(b)];
             }
     }
-    if (g.denoiser && !(errFlags & 3u)) {
+    if (g.denoiser && !(errFlags & 7u)) {
         const size_t bytes = static_cast<size_t>(w) * h * 12;
         if (g.denoised.bytes != bytes) { g.denoised.release(); ensure(g.denoised, bytes); }
         dn::denoiseForRenderer(accumF, aovAcc, 1, h, w, g.denoised.as<float>(), st);
@@ -632,6 +653,7 @@ void renderFrame(int w, int h)
     g.lastPaths = mega ? 0 : paths; g.lastDepth = depth; g.lastSpp = spp; g.lastW = w; g.lastH = h; g.lastSlots = slots;
     if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
     if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+    if (errFlags & 4u) throw CudaError{"ordered queue compaction: a tile's wait for its predecessors gave up"};
 }
 
 // Several camera views of the scene in one frame: one launch sequence over the concatenated paths of all
@@ -733,6 +755,7 @@ void launchViews(const BteView* views, int count, bool deferToBatch = false)
         ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
         ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
         if (P.raySortBits > 0) ck(cudaMemsetAsync(g.binCount.p, 0, rayBinBytes(), st), "cudaMemsetAsync");
+        clearOrder(P, st);
         launchGenerate(P, f, st);
         launchBounces(s, P, f, depth, block, st);
         launchTail(s, P, f, st);
@@ -809,6 +832,7 @@ void finishViews(const BteView* views)
     g.lastPaths = 0;   // per-path debug readbacks refer to single-view frames
     if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
     if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+    if (errFlags & 4u) throw CudaError{"ordered queue compaction: a tile's wait for its predecessors gave up"};
 }
 
 void renderViews(const BteView* views, int count)
@@ -1048,6 +1072,7 @@ bool renderSceneBatchFused(const int* scenes, const int* viewCounts, const BteVi
             ck(cudaMemsetAsync(g.sortCount.p, 0, sizeof(int) * kSortKeys * (depth + 1), st), "cudaMemsetAsync");
             ck(cudaMemsetAsync(g.errorFlags.p, 0, 4, st), "cudaMemsetAsync");
             if (P.raySortBits > 0) ck(cudaMemsetAsync(g.binCount.p, 0, rayBinBytes(), st), "cudaMemsetAsync");
+            clearOrder(P, st);
             launchGenerate(P, f, st);
             launchBounces(s, P, f, depth, block, st);
             launchTail(s, P, f, st);
@@ -1116,6 +1141,7 @@ bool renderSceneBatchFused(const int* scenes, const int* viewCounts, const BteVi
         selectScene(home);
         if (errFlags & 1u) throw CudaError{"traversal stack overflow (BVH deeper than the traversal stack)"};
         if (errFlags & 2u) throw CudaError{"traversal met an out-of-range node or triangle index (malformed tree)"};
+        if (errFlags & 4u) throw CudaError{"ordered queue compaction: a tile's wait for its predecessors gave up"};
     } catch (...) {
         selectScene(home);
         throw;

@@ -143,15 +143,16 @@ struct DevPaths {
     int sceneCount;
     // path-ordered queues for the first orderBounces bounces (material-sorted shading on, ray reordering off):
     // extend records each path's bucket in pathKey instead of appending it, shade records kKeyNext or kKeyDead,
-    // and a stable compaction over path indices (kOrderCount, kOrderScan, kOrderScatter) writes the material
-    // buckets and the next bounce's queue in ascending path order, so that the 32 paths of a warp are
-    // neighbours in the path-state arrays (float4 entries share 32-byte sectors) instead of scattered
+    // and a stable compaction over path indices (kOrderCompact) writes the material buckets and the next
+    // bounce's queue in ascending path order, so that the 32 paths of a warp are neighbours in the path-state
+    // arrays (float4 entries share 32-byte sectors) instead of scattered
     uint8_t* pathKey;         // [count rounded up to kOrderTile]
-    int* orderTiles;          // [tiles * 8] per-tile key counts, then per-tile starts
+    unsigned long long* orderStatus;   // [2 * orderBounces][tiles][kSortKeys] look-back words, zeroed per frame
+    int* orderTicket;         // [2 * orderBounces] tile tickets, zeroed per frame
     int orderBounces;
 };
 constexpr int kRaySortMinRays = 32768;
-constexpr int kOrderTile = 4096;            // paths per tile of the ordered compaction (256 threads x 16)
+constexpr int kOrderTile = 8192;            // paths per tile of the ordered compaction (256 threads x 32)
 constexpr uint8_t kKeyNext = 6;             // pathKey: the path continues to the next bounce
 constexpr uint8_t kKeyDead = 0xff;          // pathKey: the path has ended
 static_assert(kKeyNext >= kSortKeys, "next-bounce key distinct from the material buckets");
