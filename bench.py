@@ -44,7 +44,7 @@ BYTES_PER_CONNECT_RAY = 68        # 44 R + 24 RMW
 # DRAM bytes per frame of each stage kernel on this workload (1920x1080, 2 paths per pixel, depth 16), summed
 # over the frame's launches of that kernel from one ncu capture of the current build
 # (dram__bytes_read.sum + dram__bytes_write.sum); reported per launch beside the algorithmic bytes.
-STAGE_DRAM_BYTES_PER_FRAME = {"extend": 756.0e6, "shade": 3794.5e6, "connect": 432.1e6}
+STAGE_DRAM_BYTES_PER_FRAME = {"extend": 726.4e6, "shade": 2915.0e6, "connect": 426.2e6}
 
 
 def parse():
@@ -345,13 +345,18 @@ def denoise_leg():
     dn.set_dataset(rng.exponential(0.5, size=(n_img, 256, 256, 3)).astype(np.float32),
                    rng.uniform(0, 1, size=(n_img, 256, 256, 6)).astype(np.float32),
                    rng.exponential(0.5, size=(n_img, 256, 256, 3)).astype(np.float32))
-    dn.train(5, batch=batch, crop=crop, lr=1e-4, seed=1)
-    dn.train(steps, batch=batch, crop=crop, lr=1e-4, seed=2)
-    ms_step = dn.last_ms() / steps
+    step_ms = {}
+    for kind in (1, 0):   # weight gradients on tcgen05, then the default warp-level kernel
+        dn.set_wgrad(kind)
+        dn.train(5, batch=batch, crop=crop, lr=1e-4, seed=1)
+        dn.train(steps, batch=batch, crop=crop, lr=1e-4, seed=2)
+        step_ms[kind] = dn.last_ms() / steps
+    ms_step = step_ms[0]
     train_flops = 3 * DENOISER_FLOP_PER_PIXEL * batch * crop * crop   # forward + data + weight gradients
     out["training_step"] = {"batch": batch, "crop": crop, "ms_per_step": ms_step,
                             "tflops": train_flops / (ms_step / 1e3) / 1e12,
-                            "frac": train_flops / (ms_step / 1e3) / 1e12 / peak}
+                            "frac": train_flops / (ms_step / 1e3) / 1e12 / peak,
+                            "ms_per_step_wgrad_tcgen05": step_ms[1]}
     dn.load(weights)
     return out
 
