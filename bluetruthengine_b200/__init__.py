@@ -469,7 +469,7 @@ class Renderer:
         return out[..., :3].copy(), out[..., 3:].copy()
 
     def set_tuning(self, max_leaf: int = 2, shade_min_blocks: int = 3, bvh_width: int = 8,
-                   postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 0, bvh_builder: int = 1,
+                   postpone_percent: int = 0, sort_shading: int = 1, tail_paths: int = 4096, bvh_builder: int = 1,
                    ploc_radius: int = 4, overlap_connect: int = 1, wide_collapse: int = 1, ray_sort_bits: int = 0,
                    ray_sort_bounces: int = 4, leaf_tests_per_step: int = 0, order_bounces: int = 3):
         t = Tuning(int(bvh_width), int(max_leaf), int(shade_min_blocks), int(postpone_percent), int(sort_shading),

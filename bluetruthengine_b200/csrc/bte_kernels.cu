@@ -736,6 +736,65 @@ __global__ void __launch_bounds__(128) kTail(DevScene s, DevPaths P, FrameParams
     }
 }
 
+// kTail over the 8-wide tree with eight lanes per path: a group of eight lanes walks the path's closest-hit and
+// shadow rays together (traceWideGroup: the same hits as one lane's walk), lane 0 of the group shades.  Each path
+// runs its bounces back to back, so the tail costs the longest remaining path rather than the sum over bounces of
+// each bounce's slowest ray (the wavefront's last launches, a few thousand rays each, are latency-bound).
+template <bool Multi>
+__global__ void __launch_bounds__(128) kTailGroup(DevScene s, DevPaths P, FrameParams f)
+{
+    if (P.tailPaths <= 0) return;
+    int b0 = -1;
+    for (int b = 0; b < P.maxDepth; ++b)
+        if (P.rayCount[b] < P.tailPaths) { b0 = b; break; }
+    if (b0 < 0) return;
+    const int count = P.rayCount[b0];
+    const int g = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+    if (g >= count) return;   // whole groups: 8 divides the block
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned gmask = 0xffu << (lane & ~7u);
+    const bool leader = (lane & 7u) == 0u;
+    const int idx = P.queue[b0 & 1][g];
+    const DevScene& ss = sceneOf<Multi>(s, P, idx);
+    uint2 stack[kWideStack];
+    for (int b = b0; b < P.maxDepth; ++b) {
+        if (b > b0 && leader) atomicAdd(P.rayCount + b, 1);
+        const float4 o = P.o[idx];
+        const float4 d = P.d[idx];
+        const RayPre r = rayPre(o.x, o.y, o.z, d.x, d.y, d.z, ss.sceneMaxAbs);
+        float t = 0.0f, u = 0.0f, v = 0.0f;
+        const int tri = (r.valid && ss.triCount > 0)
+                            ? traceWideGroup<false>(ss, r, kEps, 1e30f, stack, P.errorFlags, t, u, v) : -1;
+        int alive = 0;
+        if (leader) {
+            P.hit[idx] = tri >= 0 ? make_float4(t, u, v, __int_as_float(tri))
+                                  : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+            if (P.hitLog) P.hitLog[static_cast<size_t>(idx) * P.maxDepth + b] = tri;
+            alive = shadePath(ss, P, f, b, idx, false) ? 1 : 0;
+        }
+        __syncwarp(gmask);   // the leader's path state and shadow slots, before the group reads them
+        alive = __shfl_sync(gmask, alive, 0, 8);
+        uint32_t mask = P.shMask[idx];
+        if (mask) {
+            if (leader) atomicAdd(P.shadowCount + b, __popc(mask));
+            const float4 so = P.shOrigin[idx];
+            const size_t base = static_cast<size_t>(idx) * P.slots;
+            for (uint32_t m = mask; m; m &= m - 1u) {
+                const int sl = __ffs(m) - 1;
+                const float4 sd = P.shDir[base + sl];
+                const RayPre sr = rayPre(so.x, so.y, so.z, sd.x, sd.y, sd.z, ss.sceneMaxAbs);
+                float st, su, sv;
+                if (sr.valid && ss.triCount > 0 &&
+                    traceWideGroup<true>(ss, sr, kEps, sd.w, stack, P.errorFlags, st, su, sv) >= 0)
+                    mask &= ~(1u << sl);
+            }
+            if (leader) P.shMask[idx] = mask;
+        }
+        __syncwarp(gmask);
+        if (!alive || b + 1 >= P.maxDepth) break;
+    }
+}
+
 // Adds v to *counter with one atomic per group of lanes that arrive here together with the same key (the
 // counter is the same for equal keys); lanes of a warp may be at different bounces in the megakernel.
 BTE_DI void groupedAdd(int* counter, int key, int v)
@@ -1108,8 +1167,9 @@ void launchTail(const DevScene& s, const DevPaths& P, const FrameParams& f, cuda
     if (P.tailPaths <= 0) return;
     const int n = P.tailPaths < P.count ? P.tailPaths : P.count;
     const int blocks = (n + 127) / 128;
-    if (P.scenes) kTail<8, true><<<blocks, 128, 0, st>>>(s, P, f);
-    else if (s.bvhWidth == 8) kTail<8, false><<<blocks, 128, 0, st>>>(s, P, f);
+    const int groupBlocks = static_cast<int>((8LL * n + 127) / 128);   // eight lanes per path
+    if (P.scenes) kTailGroup<true><<<groupBlocks, 128, 0, st>>>(s, P, f);
+    else if (s.bvhWidth == 8) kTailGroup<false><<<groupBlocks, 128, 0, st>>>(s, P, f);
     else kTail<2, false><<<blocks, 128, 0, st>>>(s, P, f);
 }
 void launchMegakernel(const DevScene& s, const DevPaths& P, const FrameParams& f, float* accum, double* accumD,

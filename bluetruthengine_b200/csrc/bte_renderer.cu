@@ -97,7 +97,7 @@ struct Renderer {
     int bvhWidth = 8;         // tree built by the next bte_init_accel
     int postponePct = 0;      // 8-wide walk: leaf-test postponing threshold (0: never; neutral on the bench scene)
     int sortShading = 1;      // material-sorted shading (shade 5.9 -> 2.6 ms per frame on the 1080p bench scene)
-    int tailPaths = 0;        // bounce queues shorter than this finish in the tail kernel
+    int tailPaths = 4096;     // bounce queues shorter than this finish in the tail kernel (eight lanes per path)
     int bvhBuilder = 1;       // binary hierarchy of the next bte_init_accel: 0 Morton-prefix (Karras), 1 PLOC
                               // (PLOC: frame 10.96 -> 10.54 ms on the 1080p bench scene)
     int wideCollapse = 1;     // 8-wide node children: 0 greedy by surface area, 1 surface-area-optimal (DP)

@@ -159,9 +159,10 @@ typedef struct {
                             * percentage of the warp's lanes have leaf tests (0 = never, 0-100) */
     int sortShading;       /* 1: extend buckets paths by hit material (miss, BSDF type) and shade runs the
                             * buckets in order; 0: shade runs the extend queue as it is */
-    int tailPaths;         /* from the first bounce whose queue is shorter than this, one thread per path
-                            * finishes the path (extend + shade + shadow rays per bounce) in one kernel;
-                            * 0: the wavefront runs every bounce */
+    int tailPaths;         /* from the first bounce whose queue is shorter than this, one kernel finishes the
+                            * remaining paths (extend + shade + shadow rays per bounce, each path's bounces back
+                            * to back; eight lanes walk a path's rays over the 8-wide tree, one thread per path
+                            * over the binary tree); 0: the wavefront runs every bounce (default 4096) */
     int bvhBuilder;        /* binary hierarchy the trees are built from: 0 Morton-prefix splits (Karras 2012);
                             * 1 PLOC, locally-ordered clustering over the Morton order (Meister & Bittner 2018) */
     int plocRadius;        /* PLOC neighbour search radius in positions, 1-32 */
