@@ -4,7 +4,8 @@ Sweeps the knobs that decide throughput on a given scene and GPU:
   * tree width and leaf size (8-wide quantised tree with 1-3 triangles per
     leaf, or the binary LBVH with SAH-collapsed leaves),
   * threads per block of the persistent stage kernels,
-  * residency the shade kernel is compiled for (2 or 3 blocks per SM),
+  * the shade kernel's register budget (2 or 3 resident blocks of 256
+    threads per SM: 96 or 72 registers),
   * the leaf-test postponing threshold of the 8-wide walk,
   * material-sorted shading on or off,
   * the compaction threshold: bounce queues shorter than it finish in the

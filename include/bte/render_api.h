@@ -154,7 +154,8 @@ int bte_read_aov(float* hostAlbedoNormal);
 typedef struct {
     int bvhWidth;          /* 2: binary LBVH; 8: 8-wide tree with 8-bit quantised child boxes */
     int maxLeafTriangles;  /* 1-64 (binary tree), 1-3 (8-wide tree) */
-    int shadeMinBlocks;    /* resident blocks per SM the shade kernel is compiled for: 2, 3 or 4 */
+    int shadeMinBlocks;    /* register budget of the shade kernel: 2, 3 or 4 resident blocks of 256 threads per
+                            * SM (96, 72 or 64 registers per thread; 5, 7 or 8 blocks of 128 threads) */
     int postponePercent;   /* 8-wide walk: a lane defers its leaf tests while fewer than this
                             * percentage of the warp's lanes have leaf tests (0 = never, 0-100) */
     int sortShading;       /* 1: extend buckets paths by hit material (miss, BSDF type) and shade runs the
