@@ -183,7 +183,7 @@ def denoised_wall(r, dn, W, H, spp, depth, env=ENV_ALIAS, max_spf=64):
 
 
 def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16, plain_max_spp=1 << 16,
-                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256), floor=0.0):
+                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256), floor=0.0, denoise_max_spf=64):
     """Wall time (and device time) that plain accumulation and the denoised low-spp form need to reach
     relMSE <= bound against the converged image, on the uploaded scene's view.  The denoiser weights must be
     loaded.  Every image's relMSE against `ref` is reported as measured and less `floor`, the reference's own
@@ -194,8 +194,8 @@ def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16
     median of spp x (relMSE - floor) over the curve's points from 64 spp) and its time from the measured time per
     sample; the result says so.
     denoised: for growing spp, one frame plus the renderer's denoise and readback; each size is timed on its
-    first call (graph capture and buffers of a new size included) and again warm.  The first size reaching the
-    bound is the result."""
+    first call (graph capture and buffers of a new size included) and again warm, rendered in frames of at most
+    `denoise_max_spf` samples per pixel.  The first size reaching the bound is the result."""
     W, H = scene.width, scene.height
     n_cross, curve = plain_crossing(r, W, H, ref, bound, depth, step=step, max_spp=plain_max_spp, floor=floor)
     last = curve[-1]
@@ -215,8 +215,8 @@ def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16
     rows, den = [], None
     try:
         for n in denoise_spps:
-            cold = denoised_wall(r, dn, W, H, n, depth)
-            warm = denoised_wall(r, dn, W, H, n, depth)
+            cold = denoised_wall(r, dn, W, H, n, depth, max_spf=denoise_max_spf)
+            warm = denoised_wall(r, dn, W, H, n, depth, max_spf=denoise_max_spf)
             e, e_in = rel_mse(warm[3], ref), rel_mse(warm[4], ref)
             row = {"spp": n, "wall_ms": warm[0] * 1e3, "wall_ms_first_call": cold[0] * 1e3,
                    "device_ms_render": warm[1], "device_ms_denoise": warm[2], "rel_mse": e,

@@ -561,11 +561,15 @@ def blob_mesh(seed: int, nu: int = 125, nv: int = 100):
 
 
 def large_instanced(seed: int = 5, width: int = 3840, height: int = 2160, n_instances: int = 400, n_meshes: int = 8,
-                    env_w: int = 2048, env_h: int = 1024) -> str:
+                    env_w: int = 2048, env_h: int = 1024, sun_radius_deg: float = 6.0, sun_radiance: float = 20.0) -> str:
     """The large configuration: n_instances placements of n_meshes seed-generated 25,000-triangle meshes
     (10M triangles flattened), each instance mirror, dielectric or microfacet (alpha U[0.01, 0.5]), on a
-    diffuse ground under the procedural sky; returns the scene.xml path."""
-    d = _scene_dir("large_%dx%d_n%d_m%d" % (width, height, n_instances, n_meshes), seed)
+    diffuse ground under the procedural sky with a soft sun (a 6-degree disc of radiance 20: caustics through
+    the glass and mirror instances are found only by BSDF sampling, and under a 0.5-degree sun of radiance 1e4
+    their variance keeps even a 1024-spp accumulation at relMSE ~0.9 against the converged image); returns the
+    scene.xml path."""
+    d = _scene_dir("large_%dx%d_n%d_m%d_sun%g_%g" % (width, height, n_instances, n_meshes, sun_radius_deg,
+                                                     sun_radiance), seed)
     path = os.path.join(d, "scene.xml")
     if _done(d):
         return path
@@ -575,7 +579,7 @@ def large_instanced(seed: int = 5, width: int = 3840, height: int = 2160, n_inst
         write_obj(os.path.join(d, "blob%d.obj" % m), v, f, normals=n)
     gv, gf = quad((-200, 0, -200), (-200, 0, 200), (200, 0, 200), (200, 0, -200))
     write_obj(os.path.join(d, "ground.obj"), gv, gf)
-    write_hdr(os.path.join(d, "sky.hdr"), sky_env(env_w, env_h))
+    write_hdr(os.path.join(d, "sky.hdr"), sky_env(env_w, env_h, sun_radius_deg=sun_radius_deg, sun_radiance=sun_radiance))
     bs = ['<bsdf name="ground" type="diffuse" albedoR="0.45" albedoG="0.42" albedoB="0.38" />']
     mats = ['<material name="mGround" bsdf="ground" />']
     meshes = ['<mesh filename="ground.obj" material="mGround" />']

@@ -7,8 +7,11 @@ Training scenes are the seeded Cornell-box variants of `scenes.c4_scene` (wall c
 1-3 dielectric spheres with IOR U[1.3, 1.8], an occasional mirror or microfacet sphere) and, with
 --outdoor, sky-lit sphere groups of `scenes.outdoor_scene` (Disney, microfacet, mirror and dielectric
 spheres under a procedural sky with a sun), all at 256x256;
-inputs mix 2-32 spp so that one network serves several noise levels; targets are independent
-FP64-accumulated long runs.  Weights are stored as float16 (`params`) with the training record.
+inputs mix several sample counts (--spp-in, default 2-32 spp) so that one network serves several noise levels;
+targets are independent FP64-accumulated long runs.  Training runs in chunks of 250 steps; the weights of the
+chunk with the lowest mean loss are kept and saved, and a chunk whose mean loss exceeds 1.5 times the best
+(a blow-up: a few batches of bright caustics can throw Adam far off) returns to those weights with half the
+step size.  Weights are stored as float16 (`params`) with the training record.
 """
 from __future__ import annotations
 
@@ -60,19 +63,31 @@ def main(argv=None):
     t1 = time.perf_counter()
     chunk = 250
     lr = args.lr
+    best, best_p, best_step, rollbacks = float("inf"), None, 0, 0
     for s in range(0, args.steps, chunk):
         k = min(chunk, args.steps - s)
         lr_s = lr * (0.1 if s >= 0.8 * args.steps else 1.0)   # one step decay for the last fifth
         l = dn.train(k, batch=args.batch, crop=args.crop, lr=lr_s, seed=args.seed * 7919 + s)
         losses.extend(l.tolist())
+        m = float(np.mean(l))
         log("step %d loss %.5f (%.1f ms / step)" % (s + k, float(np.mean(l[-50:])), dn.last_ms() / k))
+        if best_p is not None and m > 1.5 * best:   # blow-up: back to the best weights, half the step size
+            dn.set_params(best_p)
+            lr *= 0.5
+            rollbacks += 1
+            log("step %d: chunk loss %.5f > 1.5 x best %.5f; back to the weights of step %d, lr %.3g"
+                % (s + k, m, best, best_step, lr))
+            continue
+        if m < best:
+            best, best_p, best_step = m, dn.params(), s + k
     t_train = time.perf_counter() - t1
-    p = dn.params()
+    p = best_p if best_p is not None else dn.params()
     rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth, "spp_in": list(spp_in),
            "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
            "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
            "seconds_data": t_data, "seconds_train": t_train, "loss_first": float(np.mean(losses[:50])),
-           "loss_last": float(np.mean(losses[-50:]))}
+           "loss_last": float(np.mean(losses[-50:])), "best_chunk_loss": best, "best_step": best_step,
+           "rollbacks": rollbacks}
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     np.savez_compressed(args.out, params=p.astype(np.float16), record=json.dumps(rec))
     log(json.dumps(rec))
