@@ -24,6 +24,32 @@ import time
 import numpy as np
 
 
+def train_chunks(dn, steps, batch, crop, lr, seed, log=lambda m: None, chunk=250, blowup=1.5):
+    """Trains `dn` for `steps` steps in chunks of `chunk`, the learning rate a tenth for the last fifth.  Keeps the
+    weights of the chunk with the lowest mean loss; a chunk whose mean loss exceeds `blowup` times that best returns
+    to those weights (which also clears Adam's moments) with half the learning rate.  Returns (best weights, all
+    step losses, best chunk loss, its step, rollbacks)."""
+    losses = []
+    best, best_p, best_step, rollbacks = float("inf"), None, 0, 0
+    for s in range(0, steps, chunk):
+        k = min(chunk, steps - s)
+        lr_s = lr * (0.1 if s >= 0.8 * steps else 1.0)   # one step decay for the last fifth
+        l = np.asarray(dn.train(k, batch=batch, crop=crop, lr=lr_s, seed=seed * 7919 + s))
+        losses.extend(l.tolist())
+        m = float(np.mean(l))
+        log("step %d loss %.5f (%.1f ms / step)" % (s + k, float(np.mean(l[-50:])), dn.last_ms() / k))
+        if best_p is not None and m > blowup * best:   # blow-up: back to the best weights, half the step size
+            dn.set_params(best_p)
+            lr *= 0.5
+            rollbacks += 1
+            log("step %d: chunk loss %.5f > %.1f x best %.5f; back to the weights of step %d, lr %.3g"
+                % (s + k, m, blowup, best, best_step, lr))
+            continue
+        if m < best:
+            best, best_p, best_step = m, dn.params(), s + k
+    return (best_p if best_p is not None else dn.params()), losses, best, best_step, rollbacks
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--scenes", type=int, default=512, help="Cornell-box scenes (scenes.c4_scene)")
@@ -59,29 +85,9 @@ def main(argv=None):
     dn = Denoiser()
     dn.init(args.seed)
     dn.set_dataset(noisy, feat, target)
-    losses = []
     t1 = time.perf_counter()
-    chunk = 250
-    lr = args.lr
-    best, best_p, best_step, rollbacks = float("inf"), None, 0, 0
-    for s in range(0, args.steps, chunk):
-        k = min(chunk, args.steps - s)
-        lr_s = lr * (0.1 if s >= 0.8 * args.steps else 1.0)   # one step decay for the last fifth
-        l = dn.train(k, batch=args.batch, crop=args.crop, lr=lr_s, seed=args.seed * 7919 + s)
-        losses.extend(l.tolist())
-        m = float(np.mean(l))
-        log("step %d loss %.5f (%.1f ms / step)" % (s + k, float(np.mean(l[-50:])), dn.last_ms() / k))
-        if best_p is not None and m > 1.5 * best:   # blow-up: back to the best weights, half the step size
-            dn.set_params(best_p)
-            lr *= 0.5
-            rollbacks += 1
-            log("step %d: chunk loss %.5f > 1.5 x best %.5f; back to the weights of step %d, lr %.3g"
-                % (s + k, m, best, best_step, lr))
-            continue
-        if m < best:
-            best, best_p, best_step = m, dn.params(), s + k
+    p, losses, best, best_step, rollbacks = train_chunks(dn, args.steps, args.batch, args.crop, args.lr, args.seed, log)
     t_train = time.perf_counter() - t1
-    p = best_p if best_p is not None else dn.params()
     rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth, "spp_in": list(spp_in),
            "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
            "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
