@@ -309,9 +309,9 @@ def denoise_leg():
     (256x256, depth 8); host wall clock around the renderer calls and the image readback (first call at a size
     included for the denoised form), device time beside it, the relMSE of every image; plus the denoiser's
     inference time at 1920x1080 against the measured BF16 tensor-core peak."""
-    weights = os.path.join(ROOT, "bluetruthengine_b200", "weights", "denoiser_c4.npz")
+    weights = os.path.join(ROOT, "bluetruthengine_b200", "weights", "denoiser_mixed.npz")
     if not os.path.exists(weights):
-        return {"unavailable": "no trained weights at bluetruthengine_b200/weights/denoiser_c4.npz"}
+        return {"unavailable": "no trained weights at bluetruthengine_b200/weights/denoiser_mixed.npz"}
     from bluetruthengine_b200.denoise_eval import evaluate
     from bluetruthengine_b200.denoiser import Denoiser
     out = {"metric": "wall ms to relMSE<=2e-3 vs FP64 16384-spp reference (device ms beside)"}
@@ -564,7 +564,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_large:
         try:   # the large configuration: 10M triangles, 3840x2160, depth 24, 1 spp + denoise vs 1024-spp plain
             from bluetruthengine_b200.large_eval import run as large_run
-            weights = os.path.join(ROOT, "bluetruthengine_b200", "weights", "denoiser_c4.npz")
+            weights = os.path.join(ROOT, "bluetruthengine_b200", "weights", "denoiser_mixed.npz")
             out["large_scene"] = large_run(ref_spp=1024, depth=24, weights=weights, log=lambda m: None)
         except Exception as e:
             out["large_scene"] = {"unavailable": str(e)}

@@ -64,7 +64,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--scene", default="disney_spheres_1080p", choices=sorted(VIEWS))
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
-                                                      "denoiser_c4.npz"))
+                                                      "denoiser_mixed.npz"))
     ap.add_argument("--ref-spp", type=int, default=16384)
     args = ap.parse_args(argv)
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))

@@ -142,7 +142,7 @@ def _main(argv=None):
     ap.add_argument("--kernels", type=int, default=2,
                     help="0 warp-level MMA only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles, 3 row tiles upsampling in-kernel")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
-                                                      "denoiser_c4.npz"))
+                                                      "denoiser_mixed.npz"))
     args = ap.parse_args(argv)
     dn = Denoiser()
     dn.load(args.weights)

@@ -70,7 +70,7 @@ def main(argv=None):
     ap.add_argument("--ref-spp", type=int, default=1024)
     ap.add_argument("--depth", type=int, default=24)
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
-                                                      "denoiser_c4.npz"))
+                                                      "denoiser_mixed.npz"))
     args = ap.parse_args(argv)
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     res = run(args.ref_spp, args.depth, weights=args.weights, log=lambda m: print(m, file=sys.stderr, flush=True))

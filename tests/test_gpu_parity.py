@@ -617,7 +617,7 @@ def test_megakernel_features_and_denoiser(renderer, bte, cornell_scene):
     from bluetruthengine_b200.denoiser import Denoiser
     sc = cornell_scene
     W, H = sc.width, sc.height
-    weights = os.path.join(os.path.dirname(bte.__file__), "weights", "denoiser_c4.npz")
+    weights = os.path.join(os.path.dirname(bte.__file__), "weights", "denoiser_mixed.npz")
     _upload(renderer, sc, env_mode=0, spp=16, depth=8)
     renderer.set_aov(True)
     renderer.reset_accumulation(W, H)
