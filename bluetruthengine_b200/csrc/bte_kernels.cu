@@ -139,23 +139,6 @@ BTE_DI V3 resolveShadows(const DevPaths& P, int idx, V3 L)
 // ---------------------------------------------------------------- generate
 // src/wavefront/ray_generate.cu:42-80.  Path i covers pixel i % (W*H) and
 // sample frameIndex + i / (W*H).
-#ifdef BTE_TILED_PRIMARY
-// Queue order of the primary rays: each 32 consecutive queue slots hold an 8x4 block of pixels of one sample
-// plane (single-view frames whose size allows it), so a warp traces a compact block instead of a pixel row.
-BTE_DI int primaryQueuePath(int i, const FrameParams& f)
-{
-    if (f.viewCount > 0 || (f.width & 7) || (f.height & 3)) return i;
-    const int wh = f.width * f.height;
-    const int smp = i / wh, j = i - smp * wh;
-    const int tile = j >> 5, k = j & 31;
-    const int tilesPerRow = f.width >> 3;
-    const int ty = tile / tilesPerRow, tx = tile - ty * tilesPerRow;
-    return smp * wh + (ty * 4 + (k >> 3)) * f.width + tx * 8 + (k & 7);
-}
-#else
-BTE_DI int primaryQueuePath(int i, const FrameParams&) { return i; }
-#endif
-
 __global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -190,7 +173,7 @@ __global__ void __launch_bounds__(256) kGenerate(DevPaths P, FrameParams f)
     P.d[i] = make_float4(d.x, d.y, d.z, 1.0f);
     P.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     P.L[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(1u << 16));
-    P.queue[0][i] = primaryQueuePath(i, f);
+    P.queue[0][i] = i;
     P.shMask[i] = 0u;
 }
 
