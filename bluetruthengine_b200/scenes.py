@@ -525,6 +525,80 @@ def outdoor_scene(seed: int, width: int = 256, height: int = 256) -> str:
     return path
 
 
+def _blob_assets() -> str:
+    """Shared assets of the blob denoiser training scenes: eight seeded 25,000-triangle blob meshes (seeds other
+    than the large scene's), a ground plane and four soft-sun skies (sun elevations 20, 35, 50 and 65 degrees,
+    radius 4-8 degrees, radiance 10-40; 1024x512)."""
+    d = os.path.join(CACHE_ROOT, "blob_assets_v%d" % GENERATOR_VERSION)
+    os.makedirs(d, exist_ok=True)
+    if _done(d):
+        return d
+    for m in range(8):
+        v, f, n = blob_mesh(9000 + m)
+        write_obj(os.path.join(d, "blob%d.obj" % m), v, f, normals=n)
+    gv, gf = quad((-60, 0, -60), (-60, 0, 60), (60, 0, 60), (60, 0, -60))
+    write_obj(os.path.join(d, "ground.obj"), gv, gf)
+    for k, (el, rad, lum) in enumerate([(20.0, 8.0, 10.0), (35.0, 6.0, 20.0), (50.0, 5.0, 30.0), (65.0, 4.0, 40.0)]):
+        write_hdr(os.path.join(d, "sky%d.hdr" % k),
+                  sky_env(1024, 512, sun_elev_deg=el, sun_radius_deg=rad, sun_radiance=lum))
+    _mark(d)
+    return d
+
+
+def blob_scene(seed: int, width: int = 256, height: int = 256) -> str:
+    """Denoiser training scene of the large configuration's kind: 6-16 instances of the blob meshes (scale
+    U[0.6, 1.4], rotations as in `large_instanced`), each mirror (tint U[0.6, 0.95]^3), dielectric (IOR
+    U[1.3, 1.8]) or microfacet (albedo U[0.05, 0.8]^3, alpha U[0.01, 0.5]) with equal odds, on a diffuse
+    ground under one of four soft-sun skies (random rotation and intensity); camera at a random azimuth,
+    distance and height looking into the group.  Returns the XML path."""
+    d = _blob_assets()
+    path = os.path.join(d, "blob_%d_%dx%d.xml" % (seed, width, height))
+    if os.path.exists(path):
+        return path
+    rng = np.random.default_rng(3_000_017 * seed + 11)
+    g = rng.uniform(0.3, 0.6)
+    bs = ['<bsdf name="groundB" type="diffuse" albedoR="%s" albedoG="%s" albedoB="%s" />'
+          % (_fmt(g), _fmt(g * rng.uniform(0.9, 1.05)), _fmt(g * rng.uniform(0.8, 1.0)))]
+    mats = ['<material name="groundM" bsdf="groundB" />']
+    meshes = ['<mesh filename="ground.obj" material="groundM" />']
+    for i in range(int(rng.integers(6, 17))):
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            c = rng.uniform(0.6, 0.95, 3)
+            bs.append('<bsdf name="b%dB" type="mirror" albedoR="%s" albedoG="%s" albedoB="%s" />'
+                      % (i, _fmt(c[0]), _fmt(c[1]), _fmt(c[2])))
+        elif kind == 1:
+            bs.append('<bsdf name="b%dB" type="dielectric" intIOR="%s" extIOR="1.0" />' % (i, _fmt(rng.uniform(1.3, 1.8))))
+        else:
+            c = rng.uniform(0.05, 0.8, 3)
+            bs.append('<bsdf name="b%dB" type="microfacet" albedoR="%s" albedoG="%s" albedoB="%s" alpha="%s" '
+                      'intIOR="1.5" extIOR="1.0" />' % (i, _fmt(c[0]), _fmt(c[1]), _fmt(c[2]),
+                                                        _fmt(rng.uniform(0.01, 0.5))))
+        mats.append('<material name="b%dM" bsdf="b%dB" />' % (i, i))
+        s = rng.uniform(0.6, 1.4)
+        x, z = rng.uniform(-7.0, 7.0, size=2)
+        meshes.append('<mesh filename="blob%d.obj" material="b%dM" scaleX="%s" scaleY="%s" scaleZ="%s" rotY="%s" '
+                      'rotX="%s" posX="%s" posY="%s" posZ="%s" />'
+                      % (int(rng.integers(0, 8)), i, _fmt(s), _fmt(s), _fmt(s), _fmt(rng.uniform(0, 360)),
+                         _fmt(rng.uniform(-30, 30)), _fmt(x), _fmt(s * 0.9), _fmt(z)))
+    az = rng.uniform(0, 2 * np.pi)
+    dist = rng.uniform(8.0, 22.0)
+    eye = (dist * np.cos(az), rng.uniform(2.0, 12.0), dist * np.sin(az))
+    tgt = (rng.uniform(-3, 3), rng.uniform(0.0, 1.5), rng.uniform(-3, 3))
+    xml = "<scene>\n    " + "\n    ".join(bs + mats + meshes) + "\n"
+    xml += '    <environment map="sky%d.hdr" intensity="%s" rotation="%s" />\n' % (
+        int(rng.integers(0, 4)), _fmt(rng.uniform(0.5, 2.0)), _fmt(rng.uniform(0.0, 360.0)))
+    xml += '    <window width="%d" height="%d" />\n' % (width, height)
+    xml += ('    <camera eyeX="%s" eyeY="%s" eyeZ="%s" lookAtX="%s" lookAtY="%s" lookAtZ="%s" upX="0" upY="1" upZ="0" '
+            'fovY="%s" />\n</scene>\n' % (_fmt(eye[0]), _fmt(eye[1]), _fmt(eye[2]), _fmt(tgt[0]), _fmt(tgt[1]),
+                                            _fmt(tgt[2]), _fmt(rng.uniform(30.0, 60.0))))
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        f.write(xml)
+    os.replace(tmp, path)
+    return path
+
+
 def blob_mesh(seed: int, nu: int = 125, nv: int = 100):
     """Seeded closed mesh of exactly 2*nu*nv triangles: a torus of random proportions whose surface is
     displaced along its normal by a few random low-frequency harmonics.  Returns (verts, faces, normals)."""

@@ -8,7 +8,8 @@
 Training scenes are the seeded Cornell-box variants of `scenes.c4_scene` (wall colours, light, boxes,
 1-3 dielectric spheres with IOR U[1.3, 1.8], an occasional mirror or microfacet sphere) and, with
 --outdoor, sky-lit sphere groups of `scenes.outdoor_scene` (Disney, microfacet, mirror and dielectric
-spheres under a procedural sky with a sun), all at 256x256;
+spheres under a procedural sky with a sun) and, with --blob, groups of mirror / dielectric / microfacet blob
+meshes under soft-sun skies (`scenes.blob_scene`, the large configuration's kind), all at 256x256;
 inputs mix several sample counts (--spp-in, default 2-32 spp) so that one network serves several noise levels;
 targets are independent FP64-accumulated long runs.  Training runs in chunks of 250 steps; the weights of the
 chunk with the lowest mean loss are kept and saved, and a chunk whose mean loss exceeds 1.5 times the best
@@ -60,6 +61,8 @@ def main(argv=None):
     ap.add_argument("--spp-target", type=int, default=2048)
     ap.add_argument("--depth", type=int, default=8, help="max depth of the Cornell-box scenes")
     ap.add_argument("--outdoor-depth", type=int, default=16)
+    ap.add_argument("--blob", type=int, default=0, help="blob-instance scenes (scenes.blob_scene)")
+    ap.add_argument("--blob-depth", type=int, default=24)
     ap.add_argument("--spp-in", default="2,4,8,16,32", help="input sample counts drawn per scene")
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
@@ -77,7 +80,8 @@ def main(argv=None):
     r = bte.Renderer()
     paths = [(scenes.c4_scene(args.first_seed + i), args.depth) for i in range(args.scenes)]
     paths += [(scenes.outdoor_scene(args.first_seed + i), args.outdoor_depth) for i in range(args.outdoor)]
-    order = np.random.default_rng(args.seed).permutation(len(paths))   # interleave the two kinds
+    paths += [(scenes.blob_scene(args.first_seed + i), args.blob_depth) for i in range(args.blob)]
+    order = np.random.default_rng(args.seed).permutation(len(paths))   # interleave the kinds
     paths = [paths[i] for i in order]
     t0 = time.perf_counter()
     spp_in = tuple(int(x) for x in args.spp_in.split(","))
@@ -90,7 +94,8 @@ def main(argv=None):
     t1 = time.perf_counter()
     p, losses, best, best_step, rollbacks = train_chunks(dn, args.steps, args.batch, args.crop, args.lr, args.seed, log)
     t_train = time.perf_counter() - t1
-    rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth, "spp_in": list(spp_in),
+    rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth, "blob": args.blob,
+           "blob_depth": args.blob_depth, "spp_in": list(spp_in),
            "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
            "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
            "seconds_data": t_data, "seconds_train": t_train, "loss_first": float(np.mean(losses[:50])),
