@@ -50,3 +50,27 @@ def test_bench_scene_size(bte):
     assert np.all(b["type"] == 5) and len(b) == 65
     metal = b["p1"][1:, 0]
     assert set(np.unique(metal)) <= {0.0, 1.0}
+
+
+def test_training_scene_generators(tmp_path, monkeypatch, bte):
+    """The denoiser's training scenes: the same seed writes the same scene description; blob scenes hold 6-16
+    mirror / dielectric / microfacet blob instances on a diffuse ground under a soft-sun sky."""
+    from bluetruthengine_b200 import scenes
+    monkeypatch.setattr(scenes, "CACHE_ROOT", str(tmp_path))
+    for gen in (scenes.outdoor_scene, scenes.blob_scene):
+        a = open(gen(7)).read()
+        os.remove(gen(7))
+        assert open(gen(7)).read() == a
+    sc = bte.load_scene(scenes.blob_scene(7))
+    types = sc.bsdfs["type"]
+    assert types[0] == 1 and 6 <= len(types) - 1 <= 16 and set(types[1:]) <= {2, 3, 4}
+    assert sc.triangle_count == 2 + 25_000 * (len(types) - 1)
+    assert 4.0 <= sc.env_rgba[..., :3].max() <= 40.0 + 1e-3
+
+
+def test_large_scene_soft_sun():
+    """The large configuration's sky: the sun disc at radiance 20 (the caustics of its glass and mirror instances
+    then leave a 1024-spp accumulation within 2e-3 relMSE of the converged image)."""
+    from bluetruthengine_b200 import scenes
+    env = scenes.sky_env(256, 128, sun_radius_deg=6.0, sun_radiance=20.0)
+    assert np.isclose(env.max(), 20.0, rtol=1e-6) and (env[..., 0] >= 19.0).sum() > 0
