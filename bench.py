@@ -162,6 +162,18 @@ DENOISER_CONVS = [(16, 32, 0), (32, 32, 0), (32, 48, 1), (48, 48, 1), (48, 64, 2
 DENOISER_FLOP_PER_PIXEL = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in DENOISER_CONVS)
 
 
+def denoiser_layer_bound_ms(W, H, tflops, gbs):
+    """Layer-by-layer roofline of one inference: each convolution takes at least the longer of its FLOPs at the
+    tensor peak and its compulsory HBM bytes (the bf16 input read once, the bf16 output written once) at the HBM
+    peak.  The full-resolution layers (16-80 channels) are HBM-bound under this bound, the deep ones tensor-bound."""
+    Hp = (H + 15) // 16 * 16
+    t = 0.0
+    for ci, co, lv in DENOISER_CONVS:
+        p = (W >> lv) * (Hp >> lv)
+        t += max(2 * 9 * ci * co * p / (tflops * 1e12), 2 * (ci + co) * p / (gbs * 1e9))
+    return t * 1e3
+
+
 def batched_views_leg(scene, args):
     """Several camera views of the bench scene in one launch sequence (bte_render_views): 8 seeded views with
     resolutions from {320x240, 640x480, 1280x720, 1920x1080} and 1, 2 or 4 samples per frame, against the
@@ -337,8 +349,11 @@ def denoise_leg():
     t = statistics.median(ms)
     flops = DENOISER_FLOP_PER_PIXEL * W * ((H + 15) // 16 * 16)
     peak, kind = measured_bf16_tflops()
+    hbm, _ = measured_peaks()
+    bound = denoiser_layer_bound_ms(W, H, peak, hbm)
     out["inference_1080p"] = {"ms": t, "gflop": flops / 1e9, "tflops": flops / (t / 1e3) / 1e12,
-                              "peak_tflops": peak, "peak_source": kind, "frac": flops / (t / 1e3) / 1e12 / peak}
+                              "peak_tflops": peak, "peak_source": kind, "frac": flops / (t / 1e3) / 1e12 / peak,
+                              "layer_roofline_ms": bound, "layer_roofline_frac": bound / t}
     # one training step (forward, L1 loss, data and weight gradients, Adam) at the training configuration's
     # crop and batch, on a small seeded set of 256x256 images; the trained weights are loaded back afterwards
     n_img, crop, batch, steps = 16, 256, 8, 40
