@@ -459,7 +459,8 @@ class Renderer:
         self._ck(self.lib.bte_render_scene_batch(_ptr(slots), _ptr(counts), _ptr(arr), len(batch)))
 
     def set_aov(self, enabled: bool):
-        """Accumulate first-hit albedo and shading normal per pixel (denoiser features)."""
+        """Accumulate the denoiser features per pixel: albedo and shading normal at each path's first hit that is not a
+        mirror or dielectric, seen through the ones in front of it (include/bte/render_api.h, bte_set_aov)."""
         self._ck(self.lib.bte_set_aov(1 if enabled else 0))
 
     def read_aov(self, width: int, height: int):

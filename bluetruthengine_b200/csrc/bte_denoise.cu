@@ -1,5 +1,5 @@
 // bte_denoise.cu -- the learned denoiser: a 5-level U-Net over the noisy
-// radiance and the first-hit albedo/normal features, trained on image pairs
+// radiance and the albedo/normal features, trained on image pairs
 // this renderer produces, replacing the reference's vendor denoiser stage
 // (src/host/denoiser.cu:72-109, cudaToggleDenoiser render_kernel.h:187).
 //

@@ -245,11 +245,17 @@ BTE_DI bool shadePath(const DevScene& s, const DevPaths& P, const FrameParams& f
         h.v = w0 * T.uv0.y + u * T.uv1.y + v * T.uv2.y;
     }
     const Bsdf b = loadBsdf(s, tri, h.u, h.v);
-    if (bounce == 0 && P.aovAlbedo) {   // denoiser features: the material colour and normal seen first
-        const float4 a = b.type == BSDF_Dielectric ? make_float4(1.0f, 1.0f, 1.0f, 0.0f)
-                                                   : make_float4(b.p0.x, b.p0.y, b.p0.z, 0.0f);
-        P.aovAlbedo[idx] = a;
+    bool featPending = false;
+    if (P.aovAlbedo && (bounce == 0 || ((bits >> 17) & 1u) != 0u)) {
+        // denoiser features: the material colour and shading normal of the first hit that is not a perfect
+        // mirror or dielectric, seen through the mirrors and dielectrics in front of it (their colours multiplied
+        // in: a mirror's tint, 1 for a dielectric).  While a path has met only such surfaces, the last one's
+        // normal and the product so far stand, and bit 17 of the packed bounce word marks the path as pending.
+        const float4 prev = bounce == 0 ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : P.aovAlbedo[idx];
+        const V3 c = b.type == BSDF_Dielectric ? v3(1.0f, 1.0f, 1.0f) : v3(b.p0.x, b.p0.y, b.p0.z);
+        P.aovAlbedo[idx] = make_float4(prev.x * c.x, prev.y * c.y, prev.z * c.z, 0.0f);
         P.aovNormal[idx] = make_float4(h.n.x, h.n.y, h.n.z, 0.0f);
+        featPending = !bsdfIsDiffuseClass(b.type);
     }
     if (s.emitterFlags[tri] != 0) accumulateEmitterHit(s, p, h);
 
@@ -295,7 +301,8 @@ BTE_DI bool shadePath(const DevScene& s, const DevPaths& P, const FrameParams& f
     P.d[idx] = make_float4(p.d.x, p.d.y, p.d.z, p.eta);
     P.tp[idx] = make_float4(p.tp.x, p.tp.y, p.tp.z, p.brdfPdf);
     P.L[idx] = make_float4(p.L.x, p.L.y, p.L.z,
-                           __uint_as_float(static_cast<uint32_t>(p.bounce) | (p.specular ? (1u << 16) : 0u)));
+                           __uint_as_float(static_cast<uint32_t>(p.bounce) | (p.specular ? (1u << 16) : 0u) |
+                                           (featPending ? (1u << 17) : 0u)));
     return alive;
 }
 
@@ -819,8 +826,8 @@ BTE_DI void groupedAdd(int* counter, int key, int v)
 // paths in turn, each drawing its jitter first.  Each path runs the tail kernel's bounce loop on the pixel's own
 // path slot (the stream returns through P.o.w); the paths' radiance is summed in sample order from zero, scaled
 // by div3, folded into the FP32 Welford mean once per frame (n = frames so far + 1) and into the FP64 sum, then
-// packed.  With features on (aovAccum), each path's first-hit albedo and normal (written by shadePath at bounce
-// 0 into the pixel's slot) are summed the same way and their per-frame mean folded into aovAccum, so the
+// packed.  With features on (aovAccum), each path's feature albedo and normal (written by shadePath into the
+// pixel's slot at the path's first hit that is not a mirror or dielectric) are summed the same way and their per-frame mean folded into aovAccum, so the
 // denoiser sees the same features in both render modes.
 template <int Width>
 __global__ void __launch_bounds__(128) kMegakernel(DevScene s, DevPaths P, FrameParams f, float* accum,
@@ -931,7 +938,7 @@ __global__ void __launch_bounds__(256) kPresent(DevPaths P, FrameParams f, float
     }
     accum[3 * pix] = ax; accum[3 * pix + 1] = ay; accum[3 * pix + 2] = az;
     accumD[3 * pix] = sx; accumD[3 * pix + 1] = sy; accumD[3 * pix + 2] = sz;
-    if (aovAccum && P.aovAlbedo) {   // running means of the first-hit albedo and normal, [W*H][6]
+    if (aovAccum && P.aovAlbedo) {   // running means of the feature albedo and normal, [W*H][6]
         float m[6];
         for (int c = 0; c < 6; ++c) m[c] = aovAccum[6 * static_cast<size_t>(pix) + c];
         for (int s = 0; s < f.spp; ++s) {

@@ -129,7 +129,7 @@ struct Renderer {
         orderTicket;
     int pathCap = 0, slotCap = 0, depthCap = 0;
     bool hitLogEnabled = false;
-    bool aovEnabled = false;          // first-hit albedo / normal features for the denoiser
+    bool aovEnabled = false;          // albedo / normal features for the denoiser
     DeviceBuffer aovAlbedo, aovNormal, aovAccum;
     DeviceBuffer denoised;            // [W*H*3] denoised mean radiance of the last frame (denoiser on)
     // batched views (bte_render_views): accumulation per view slot
@@ -1528,7 +1528,7 @@ int bte_get_framebuffer_size(int* width, int* height)
 
 // render_kernel.h:187 (cudaToggleDenoiser): returns the new state.  Turning
 // it on needs denoiser weights (bte_denoiser_set_params / bte_denoiser_init)
-// and switches the first-hit features on; each frame then presents the
+// and switches the albedo / normal features on; each frame then presents the
 // denoised accumulation.  Plain accumulation stays the buffer of record.
 int bte_render_views(const BteView* views, int count)
 {

@@ -115,8 +115,8 @@ struct DevPaths {
     float4* shContrib;// [paths*slots] contribution | unused
     uint32_t* shMask; // [paths] bit s: slot s visible and not yet added
     int* hitLog;      // optional [paths*maxDepth]
-    float4* aovAlbedo;// optional [paths] first-hit albedo (denoiser feature)
-    float4* aovNormal;// optional [paths] first-hit shading normal (denoiser feature)
+    float4* aovAlbedo;// optional [paths] feature albedo (denoiser feature)
+    float4* aovNormal;// optional [paths] feature shading normal (denoiser feature)
     int slots;        // 1 (area) + spotCount + 1 (env)
     int maxDepth;
     int count;        // paths in the frame

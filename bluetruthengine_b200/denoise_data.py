@@ -1,7 +1,7 @@
 """Training pairs and quality measurement for the learned denoiser, all rendered by this renderer.
 
-* `render_pair`: a low-spp input (FP32 running mean, as the renderer accumulates it) with its first-hit
-  albedo/normal features, and an independent long-run target (FP64 running sum / samples, from a
+* `render_pair`: a low-spp input (FP32 running mean, as the renderer accumulates it) with its albedo/normal
+  features, and an independent long-run target (FP64 running sum / samples, from a
   disjoint range of sample indices).
 * `reference`: an FP64-accumulated high-spp image of a view.
 * `time_to_rel_mse`: wall time (host clock around the renderer calls and the readback, with the device
@@ -159,7 +159,7 @@ def plain_wall(r, W, H, spp, depth, spf=16, env=ENV_ALIAS):
 def denoised_wall(r, dn, W, H, spp, depth, env=ENV_ALIAS, max_spf=64):
     """Host wall time of the denoised low-spp form through the renderer API: with the denoiser toggled on,
     reset, frames of up to `max_spf` samples per pixel (one frame up to that size; the renderer denoises
-    its running mean with the first-hit albedo/normal features after every frame), and the denoised image
+    its running mean with the albedo/normal features after every frame), and the denoised image
     read back.  Returns (wall s, render ms, denoise ms, denoised image, noisy mean)."""
     spf = min(spp, max_spf)
     r.set_config(samples_per_frame=spf, max_depth=depth, rr_start=3, env_sampling=env, use_graph=1)
@@ -183,7 +183,7 @@ def denoised_wall(r, dn, W, H, spp, depth, env=ENV_ALIAS, max_spf=64):
 
 
 def time_to_rel_mse(r, dn, scene, ref, bound=2e-3, depth=8, step=4, plain_spf=16, plain_max_spp=1 << 16,
-                    denoise_spps=(1, 2, 4, 8, 16, 32, 64, 128, 256), floor=0.0, denoise_max_spf=64):
+                    denoise_spps=(1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256), floor=0.0, denoise_max_spf=64):
     """Wall time (and device time) that plain accumulation and the denoised low-spp form need to reach
     relMSE <= bound against the converged image, on the uploaded scene's view.  The denoiser weights must be
     loaded.  Every image's relMSE against `ref` is reported as measured and less `floor`, the reference's own

@@ -2,7 +2,7 @@
 
 The network replaces the reference's vendor denoiser stage (src/host/denoiser.cu:72-109,
 cudaToggleDenoiser in include/render_kernel.h:187).  It is trained only on image pairs this
-renderer produces: low-spp radiance plus first-hit albedo/normal (bte_read_aov) as input, long-run
+renderer produces: low-spp radiance plus the albedo/normal features (bte_read_aov) as input, long-run
 FP64-accumulated radiance as target.
 """
 from __future__ import annotations

@@ -18,7 +18,7 @@ import os
 import sys
 import time
 
-DENOISE_SPPS = (1, 2, 4, 8, 16, 32, 64)
+DENOISE_SPPS = (1, 2, 4, 8, 16, 24, 32, 48, 64, 96, 128)
 
 
 def run(ref_spp=1024, depth=24, weights=None, log=print, width=3840, height=2160, bound=2e-3):

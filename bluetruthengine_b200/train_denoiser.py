@@ -53,6 +53,14 @@ def train_chunks(dn, steps, batch, crop, lr, seed, log=lambda m: None, chunk=250
     return (best_p if best_p is not None else dn.params()), losses, best, best_step, rollbacks
 
 
+def _record(path):
+    """The training record stored with a weights file (None when there is none)."""
+    if not path:
+        return None
+    with np.load(path) as z:
+        return json.loads(str(z["record"])) if "record" in z else None
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--scenes", type=int, default=512, help="Cornell-box scenes (scenes.c4_scene)")
@@ -69,6 +77,7 @@ def main(argv=None):
     ap.add_argument("--crop", type=int, default=128)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--init", default=None, help="start from these weights (a file written by this trainer)")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "denoiser_mixed.npz"))
     args = ap.parse_args(argv)
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -90,13 +99,16 @@ def main(argv=None):
     t_data = time.perf_counter() - t0
     dn = Denoiser()
     dn.init(args.seed)
+    if args.init:
+        dn.load(args.init)
     dn.set_dataset(noisy, feat, target)
     t1 = time.perf_counter()
     p, losses, best, best_step, rollbacks = train_chunks(dn, args.steps, args.batch, args.crop, args.lr, args.seed, log)
     t_train = time.perf_counter() - t1
     rec = {"scenes": args.scenes, "outdoor": args.outdoor, "outdoor_depth": args.outdoor_depth, "blob": args.blob,
            "blob_depth": args.blob_depth, "spp_in": list(spp_in),
-           "first_seed": args.first_seed, "spp_target": args.spp_target, "depth": args.depth,
+           "first_seed": args.first_seed, "init": os.path.basename(args.init) if args.init else None,
+           "init_record": _record(args.init), "spp_target": args.spp_target, "depth": args.depth,
            "steps": args.steps, "batch": args.batch, "crop": args.crop, "lr": args.lr, "seed": args.seed,
            "seconds_data": t_data, "seconds_train": t_train, "loss_first": float(np.mean(losses[:50])),
            "loss_last": float(np.mean(losses[-50:])), "best_chunk_loss": best, "best_step": best_step,

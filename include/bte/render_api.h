@@ -144,9 +144,13 @@ int bte_read_accum_f64(double* hostRGBSum);          /* FP64 running sum of samp
 int bte_read_sample_radiance(float* hostRGB, int count);  /* per-path radiance of the last frame [W*H*spp*3] */
 int bte_read_hit_log(int* hostTri, int count);       /* per-bounce closest-hit triangle of the last frame */
 int bte_set_hit_log(int enabled);                    /* record [path][bounce] hit triangles (debug/parity) */
-/* Denoiser features: per-pixel running means of the first-hit material colour
- * (BsdfData p0.xyz after textures; 1 for dielectrics; 0 on a miss) and shading
- * normal, accumulated with the radiance.  Read as [W*H][albedo.xyz, normal.xyz]. */
+/* Denoiser features: per-pixel running means of the material colour (BsdfData
+ * p0.xyz after textures) and shading normal at each path's first hit that is
+ * not a perfect mirror or dielectric, seen through the mirrors and dielectrics
+ * in front of it (colour times their tints: a mirror's p0.xyz, 1 for a
+ * dielectric; a path that meets only such surfaces keeps the last one's normal
+ * and the product so far; 0 when the first ray misses), accumulated with the
+ * radiance.  Read as [W*H][albedo.xyz, normal.xyz]. */
 int bte_set_aov(int enabled);
 int bte_read_aov(float* hostAlbedoNormal);
 /* Acceleration-structure and kernel tuning (what the autotuner sweeps).
@@ -196,7 +200,7 @@ int bte_get_accel_builder(int* builder);
 
 /* ---- learned denoiser (replaces the vendor denoiser stage, render_kernel.h:187 / src/host/denoiser.cu) ----
  * A 5-level U-Net (3x3 convolutions, 32-128 channels) over log(1 + radiance)
- * plus first-hit albedo and normal, BF16 tensor-core convolutions with FP32
+ * plus the feature albedo and normal (bte_set_aov), BF16 tensor-core convolutions with FP32
  * accumulation, FP32 master weights trained with Adam on L1 in log space.
  * Images are row-major [H][W][3] radiance and [H][W][6] features (albedo xyz,
  * normal xyz, as bte_read_aov returns them). */

@@ -529,9 +529,11 @@ def test_graph_frames_match_stream_frames(renderer, random_scene):
 
 
 def test_aov_features(renderer, random_scene):
-    """First-hit albedo/normal features: with one sample per pixel the albedo equals the hit triangle's
-    BSDF colour (1 for dielectrics, 0 for misses), the normal is unit length, and enabling the features
-    leaves the radiance bit-identical."""
+    """Albedo/normal features: with one sample per pixel the albedo is the BSDF colour of the path's first hit
+    that is not a mirror or dielectric, times the tints of the mirrors (their colour) and dielectrics (1) in
+    front of it -- worked out here from the hit log -- or that product alone when the path meets nothing else
+    (0 when the first ray misses); the normal is unit length; enabling the features leaves the radiance
+    bit-identical."""
     sc = random_scene
     W, H = sc.width, sc.height
     _upload(renderer, sc, env_mode=1, spp=1, depth=6)
@@ -544,17 +546,28 @@ def test_aov_features(renderer, random_scene):
     renderer.reset_accumulation(W, H)
     renderer.render(W, H)
     rad = renderer.read_sample_radiance(W * H)
-    hits = renderer.read_hit_log(W * H * 6).reshape(W * H, 6)[:, 0]
+    log = renderer.read_hit_log(W * H * 6).reshape(W * H, 6)
+    hits = log[:, 0]
     alb, nrm = renderer.read_aov(W, H)
     renderer.set_hit_log(False)
     renderer.set_aov(False)
     assert np.array_equal(bits(plain), bits(rad))
     alb = alb.reshape(-1, 3)
     nrm = nrm.reshape(-1, 3)
-    b = sc.bsdfs[sc.triangle_bsdf_ids[np.maximum(hits, 0)]]
-    expect = np.where((b["type"] == 2)[:, None], 1.0, b["p0"][:, :3]).astype(np.float32)   # 2 = dielectric
-    expect[hits < 0] = 0.0
+    expect = np.zeros((W * H, 3), np.float32)
+    tint = np.ones((W * H, 3), np.float32)
+    open_ = np.ones(W * H, bool)            # still looking through mirrors / dielectrics
+    for k in range(6):
+        tri = log[:, k]
+        on = open_ & (tri >= 0)             # a miss (-1) or a bounce not traced (0xfefefefe) ends the search
+        b = sc.bsdfs[sc.triangle_bsdf_ids[np.maximum(tri, 0)]]
+        c = np.where((b["type"] == 2)[:, None], np.float32(1.0), b["p0"][:, :3]).astype(np.float32)   # 2 = dielectric
+        tint = np.where(on[:, None], tint * c, tint)
+        expect[on] = tint[on]
+        open_ = on & np.isin(b["type"], (2, 3))   # 2 dielectric, 3 mirror
     assert np.array_equal(alb, expect)
+    first = sc.bsdfs[sc.triangle_bsdf_ids[np.maximum(hits, 0)]]["type"]
+    assert ((hits >= 0) & np.isin(first, (2, 3))).mean() > 0.02    # the scene has paths that look through
     ln = np.linalg.norm(nrm, axis=1)
     assert np.all(np.abs(ln[hits >= 0] - 1.0) < 1e-5) and np.all(ln[hits < 0] == 0.0)
     assert (hits >= 0).mean() > 0.3
@@ -610,7 +623,7 @@ def test_megakernel_mode_matches_oracle(renderer, oracle_mod, random_scene):
 
 def test_megakernel_features_and_denoiser(renderer, bte, cornell_scene):
     """Megakernel mode with features on: the radiance stays bit-identical to features off; the features are the
-    per-frame means of the first-hit albedo and normal (on the Cornell box, where every pixel sees a wall, they
+    per-frame means of the feature albedo and normal (on the Cornell box, where every pixel sees a wall, they
     agree with the wavefront's features of the same view wherever a pixel's samples all hit one surface); and
     the renderer's toggled denoiser in this mode equals the stand-alone denoiser run on the read-back mean and
     features, bit for bit."""
