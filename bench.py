@@ -330,8 +330,8 @@ def denoise_leg():
     for name in ("disney_spheres_1080p", "cornell"):
         res = evaluate(name, weights)
         keep = {k: res[k] for k in ("scene", "width", "height", "depth", "reference_spp", "reference_seconds", "bound",
-                                    "reference_floor", "plain", "denoised", "denoised_sweep", "speedup_wall",
-                                    "speedup_wall_warm", "speedup_device") if k in res}
+                                    "reference_floor", "plain", "denoised", "denoised_sweep", "one_time_ms_at_size",
+                                    "speedup_wall", "speedup_wall_first_call", "speedup_wall_warm", "speedup_device") if k in res}
         keep["plain_curve"] = res["plain_curve"][:: max(1, len(res["plain_curve"]) // 16)]
         out[name] = keep
     dn = Denoiser()

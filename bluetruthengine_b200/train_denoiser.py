@@ -1,9 +1,15 @@
 """Train the denoiser on pairs this renderer generates and save its weights.
 
-    python -m bluetruthengine_b200.train_denoiser --scenes 384 --outdoor 384 --spp-target 4096 \
-        --spp-in 1,2,4,8,16,32,64 --steps 20000 --lr 5e-4 --out bluetruthengine_b200/weights/denoiser_mixed.npz
+The shipped weights (bluetruthengine_b200/weights/denoiser_mixed.npz) came from two runs on one B200:
 
-(the recipe of the shipped weights: 6.7 min of pair rendering, 53 s of training on one B200).
+    python -m bluetruthengine_b200.train_denoiser --scenes 640 --outdoor 640 --blob 720 --spp-target 4096 \
+        --spp-in 1,2,4,8,16,32,64 --steps 40000 --lr 5e-4 --out base.npz
+    python -m bluetruthengine_b200.train_denoiser --init base.npz --scenes 200 --outdoor 200 --blob 400 \
+        --first-seed 5000 --spp-target 4096 --spp-in 1,2,4,8,16,32,48,64 --steps 60000 --lr 2e-4 \
+        --out bluetruthengine_b200/weights/denoiser_mixed.npz
+
+(2000 scenes, 22.4 min of pair rendering and 1.8 min of training; then 800 further scenes, 8.6 min and 2.7 min;
+the file's training record holds both runs' settings).
 
 Training scenes are the seeded Cornell-box variants of `scenes.c4_scene` (wall colours, light, boxes,
 1-3 dielectric spheres with IOR U[1.3, 1.8], an occasional mirror or microfacet sphere) and, with
