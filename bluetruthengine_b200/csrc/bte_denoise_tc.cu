@@ -994,31 +994,38 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
     const uint32_t idesc = instrDesc(nPad);
     const bf16* Xd = Xs + static_cast<size_t>(dx + 1) * Cin * P;
 
+    // The rows beyond Cout (A) and Cin (B) stay zero: written once here for every stage, never copied.
+    for (int st = 0; st < kTcStages; ++st) {
+        for (int e = tid; e < (kTcM - Cout) * 8; e += 128) {
+            const int co = Cout + e / 8, j = e & 7;
+            *reinterpret_cast<uint4*>(smem + st * kStageABytes + j * lboA + (co >> 3) * 128 + (co & 7) * 16) =
+                make_uint4(0u, 0u, 0u, 0u);
+        }
+        for (int e = tid; e < (nPad - Cin) * 8; e += 128) {
+            const int ci = Cin + e / 8, j = e & 7;
+            *reinterpret_cast<uint4*>(smem + kTcStages * kStageABytes + st * kStageBBytes + j * lboB + (ci >> 3) * 128 +
+                                      (ci & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
+        }
+    }
+    // Thread t copies chunk j = t % 8 (8 pixels) of channels t / 8, t / 8 + 16, ...: eight neighbouring threads
+    // read one channel's 128 contiguous bytes.  W % 8 == 0 keeps a chunk inside one image row, whose row index
+    // (32-bit: the pixel count is below 2^31) decides the zero fill of the dy-shifted operand.
+    const int cj = tid & 7, cr = tid >> 3;
     auto issueCopies = [&](int it) {
         const int stage = it % kTcStages;
-        const long long pc = p0 + static_cast<long long>(it) * kTcKStage;
-        const uint32_t aBase = sA + stage * kStageABytes;
-        for (int e = tid; e < kTcM * 8; e += 128) {   // A: 128 output channels x 8 chunks of 8 pixels
-            const int co = e & (kTcM - 1), j = e / kTcM;
-            const long long p = pc + 8 * j;
-            const bool ok = co < Cout && p < p1;
-            cpAsync16(aBase + j * lboA + (co >> 3) * 128 + (co & 7) * 16, ok ? dYt + static_cast<size_t>(co) * P + p : dYt,
-                      ok);
-        }
-        const uint32_t bBase = sB + stage * kStageBBytes;
-        for (int e = tid; e < nPad * 8; e += 128) {   // B: nPad input channels x 8 chunks, shifted by dy rows
-            const int ci = e % nPad, j = e / nPad;
-            const long long p = pc + 8 * j;
-            bool ok = ci < Cin && p < p1;
-            long long q = 0;
-            if (ok) {
-                const int y = static_cast<int>((p / W) % H);
-                ok = y + dy >= 0 && y + dy < H;
-                q = p + static_cast<long long>(dy) * W;
-            }
-            cpAsync16(bBase + j * lboB + (ci >> 3) * 128 + (ci & 7) * 16, ok ? Xd + static_cast<size_t>(ci) * P + q : Xd,
-                      ok);
-        }
+        const long long p = p0 + static_cast<long long>(it) * kTcKStage + 8 * cj;
+        const uint32_t aBase = sA + stage * kStageABytes + cj * lboA;
+        const uint32_t bBase = sB + stage * kStageBBytes + cj * lboB;
+        const bool inRange = p < p1;
+        const int y = static_cast<int>((static_cast<uint32_t>(p) / static_cast<uint32_t>(W)) % static_cast<uint32_t>(H));
+        const bool rowOk = inRange && y + dy >= 0 && y + dy < H;
+        const long long q = p + static_cast<long long>(dy) * W;
+        for (int co = cr; co < Cout; co += 16)   // A: dY^T, output channels x pixels
+            cpAsync16(aBase + (co >> 3) * 128 + (co & 7) * 16, inRange ? dYt + static_cast<size_t>(co) * P + p : dYt,
+                      inRange);
+        for (int ci = cr; ci < Cin; ci += 16)    // B: X shifted by the tap, input channels x pixels
+            cpAsync16(bBase + (ci >> 3) * 128 + (ci & 7) * 16, rowOk ? Xd + static_cast<size_t>(ci) * P + q : Xd,
+                      rowOk);
     };
 
     // all threads run the same barriers; a timed-out wait only raises the abort flag (no further copy or MMA)
@@ -1089,8 +1096,8 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
 bool convWgradTcSupported(int N, int H, int W, int Cin, int Cout)
 {
     const long long P = static_cast<long long>(N) * H * W;
-    return W % 8 == 0 && P % 64 == 0 && P > 0 && Cin >= 16 && Cin <= kTcMaxN && Cin % 8 == 0 && Cout >= 1 &&
-           Cout <= kTcM;
+    return W % 8 == 0 && P % 64 == 0 && P > 0 && P < (1LL << 31) && Cin >= 16 && Cin <= kTcMaxN && Cin % 8 == 0 &&
+           Cout >= 1 && Cout <= kTcM;
 }
 
 size_t convWgradTcScratchBytes(int N, int H, int W, int Cin, int Cout)
