@@ -972,6 +972,7 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
     const long long p1 = p0 + pixPerSplit < P ? p0 + pixPerSplit : P;
     const int iters = p1 > p0 ? static_cast<int>((p1 - p0 + kTcKStage - 1) / kTcKStage) : 0;
     const uint32_t sA = smemAddr(smem), sB = sA + kTcStages * kStageABytes;
+    const int stageB = nPad * kTcKStage * 2;   // B stage bytes: the launch's padded input channels
     const uint32_t tmemCols = nPad <= 32 ? 32 : (nPad <= 64 ? 64 : (nPad <= 128 ? 128 : 256));
 
     if (warp == 0) {
@@ -1003,7 +1004,7 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
         }
         for (int e = tid; e < (nPad - Cin) * 8; e += 128) {
             const int ci = Cin + e / 8, j = e & 7;
-            *reinterpret_cast<uint4*>(smem + kTcStages * kStageABytes + st * kStageBBytes + j * lboB + (ci >> 3) * 128 +
+            *reinterpret_cast<uint4*>(smem + kTcStages * kStageABytes + st * stageB + j * lboB + (ci >> 3) * 128 +
                                       (ci & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
         }
     }
@@ -1015,7 +1016,7 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
         const int stage = it % kTcStages;
         const long long p = p0 + static_cast<long long>(it) * kTcKStage + 8 * cj;
         const uint32_t aBase = sA + stage * kStageABytes + cj * lboA;
-        const uint32_t bBase = sB + stage * kStageBBytes + cj * lboB;
+        const uint32_t bBase = sB + stage * stageB + cj * lboB;
         const bool inRange = p < p1;
         const int y = static_cast<int>((static_cast<uint32_t>(p) / static_cast<uint32_t>(W)) % static_cast<uint32_t>(H));
         const bool rowOk = inRange && y + dy >= 0 && y + dy < H;
@@ -1050,7 +1051,7 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
                 const int stage = j % kTcStages;
                 for (int k = 0; k < kTcKStage / 16; ++k) {
                     const uint64_t da = smemDesc(sA + stage * kStageABytes + 2 * k * lboA, lboA, 128);
-                    const uint64_t db = smemDesc(sB + stage * kStageBBytes + 2 * k * lboB, lboB, 128);
+                    const uint64_t db = smemDesc(sB + stage * stageB + 2 * k * lboB, lboB, 128);
                     umma(tmem, da, db, idesc, (j > 0 || k > 0) ? 1u : 0u);
                 }
                 ummaCommit(smemAddr(&mbar[stage]));
@@ -1124,13 +1125,18 @@ void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, in
         attrSet = true;
     }
     const int nPad = (Cin + 15) / 16 * 16;
-    // about two CTAs per SM over the nine taps, each at least 512 pixels, splits a multiple of 64 pixels
-    long long splits = (2LL * 148 + 8) / 9;
+    // shared memory for this launch's channel count only (3 stages of A and of nPad-channel B): 54-78 KB up to 80
+    // input channels, so two to four CTAs share an SM (their TMEM columns, at most 2 x 256, fit its 512) and hide
+    // one another's copy and issue latency; a few CTAs per SM over the nine taps, each at least 512 pixels, splits
+    // a multiple of 64 pixels
+    const int smemBytes = kTcStages * (kStageABytes + nPad * kTcKStage * 2);
+    const int resident = (220 * 1024) / smemBytes < 1 ? 1 : (220 * 1024) / smemBytes;
+    long long splits = (static_cast<long long>(resident) * 2 * 148 + 8) / 9;
     long long per = (P + splits - 1) / splits;
     if (per < 512) per = 512;
     per = (per + kTcKStage - 1) / kTcKStage * kTcKStage;
     splits = (P + per - 1) / per;
-    kWgradTc<<<dim3(1, 9, static_cast<unsigned>(splits)), 128, kTcSmem, st>>>(dYt, Xs, H, W, P, Cin, Cout, nPad, per, dW,
+    kWgradTc<<<dim3(1, 9, static_cast<unsigned>(splits)), 128, smemBytes, st>>>(dYt, Xs, H, W, P, Cin, Cout, nPad, per, dW,
                                                                                errorFlag);
 }
 
