@@ -948,32 +948,37 @@ __global__ void kPlanar(const bf16* __restrict__ in, int C, long long P, int W, 
     }
 }
 
-// dW[tap][co][ci] += sum over pixels p of dY[p][co] * X[p shifted by the tap][ci], as a GEMM with M = the output
-// channels (one 128-row tile; rows beyond Cout are zero), N = the input channels rounded up to 16 (at most 256)
-// and the pixels as K.  Both operands come from the channel-major copies made beforehand (dYt[co][p] and, per
-// column shift dx, Xs[dx + 1][ci][p]), so one K-major 16-byte chunk is 8 consecutive pixels of one channel; the
-// row shift dy is a whole-row offset (W % 8 == 0 keeps every chunk inside one image row, whose validity decides
-// the zero fill).  The pipeline is kConvTc's: 64-pixel stages through a 3-deep cp.async ring, one thread issues
-// four M128 x N x K16 MMAs per stage into one TMEM accumulator, every wait bounded.  The epilogue adds the CTA's
-// partial sums into dW with FP32 atomics.  Grid: (1, 9 taps, pixel splits of a multiple of 64 pixels).
+// dW[tap][co][ci] += sum over pixels p of X[p shifted by the tap][ci] * dY[p][co], as one GEMM over all nine taps:
+// M = the taps' input channels (row r = tap * Cin + ci, 128-row tiles, rows beyond 9 * Cin zero), N = the output
+// channels (Cout, a multiple of 16) and K = the pixels.  A layer of few input channels thus fills the 128 rows with
+// several taps instead of padding its output channels to 128: for 16-32 input channels 3-4.5 times fewer MMAs
+// than one M = Cout GEMM per tap.  Both operands come from the channel-major copies made beforehand (dYt[co][p]
+// and, per column shift dx, Xs[dx + 1][ci][p]), so one K-major 16-byte chunk is 8 consecutive pixels of one
+// channel; a row's dy shift is a whole-row offset (W % 8 == 0 keeps every chunk inside one image row, whose
+// validity decides the zero fill).  The pipeline is kConvTc's: 64-pixel stages through a 3-deep cp.async ring,
+// one thread issues four M128 x N x K16 MMAs per stage into one TMEM accumulator, every wait bounded.  The
+// epilogue adds the CTA's partial sums into dW with FP32 atomics (neighbouring lanes hold neighbouring input
+// channels of one tap: neighbouring addresses).  Grid: (row tiles, 1, pixel splits of a multiple of 64 pixels).
 __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt, const bf16* __restrict__ Xs, int H,
-                                                   int W, long long P, int Cin, int Cout, int nPad,
-                                                   long long pixPerSplit, float* __restrict__ dW,
-                                                   unsigned int* errorFlag)
+                                                   int W, long long P, int Cin, int Cout, long long pixPerSplit,
+                                                   float* __restrict__ dW, unsigned int* errorFlag)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint64_t mbar[kTcStages];
     __shared__ uint32_t tmemBase;
     __shared__ volatile int abortFlag;
     __shared__ volatile int lastCommit;
+    __shared__ long long rowSrc[kTcM];   // row r: offset of its channel plane in Xs, plus its dy rows
+    __shared__ int rowDy[kTcM];
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int tap = static_cast<int>(blockIdx.y), dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const int row0 = static_cast<int>(blockIdx.x) * kTcM;
+    const int rows = 9 * Cin - row0 < kTcM ? 9 * Cin - row0 : kTcM;   // live rows of this tile
     const long long p0 = static_cast<long long>(blockIdx.z) * pixPerSplit;
     const long long p1 = p0 + pixPerSplit < P ? p0 + pixPerSplit : P;
     const int iters = p1 > p0 ? static_cast<int>((p1 - p0 + kTcKStage - 1) / kTcKStage) : 0;
+    const int stageB = Cout * kTcKStage * 2;
     const uint32_t sA = smemAddr(smem), sB = sA + kTcStages * kStageABytes;
-    const int stageB = nPad * kTcKStage * 2;   // B stage bytes: the launch's padded input channels
-    const uint32_t tmemCols = nPad <= 32 ? 32 : (nPad <= 64 ? 64 : (nPad <= 128 ? 128 : 256));
+    const uint32_t tmemCols = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : (Cout <= 128 ? 128 : 256));
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smemAddr(&tmemBase)),
@@ -986,31 +991,29 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
         lastCommit = -1;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
     }
+    if (tid < rows) {
+        const int r = row0 + tid, tap = r / Cin, ci = r - tap * Cin, dy = tap / 3 - 1, dx = tap % 3 - 1;
+        rowSrc[tid] = (static_cast<long long>(dx + 1) * Cin + ci) * P + static_cast<long long>(dy) * W;
+        rowDy[tid] = dy;
+    }
+    const uint32_t lboA = (kTcM / 8) * 128;
+    const uint32_t lboB = static_cast<uint32_t>(Cout / 8) * 128;
+    const uint32_t idesc = instrDesc(Cout);
+    // rows beyond the nine taps stay zero: written once here for every stage, never copied
+    for (int st = 0; st < kTcStages; ++st)
+        for (int e = tid; e < (kTcM - rows) * 8; e += 128) {
+            const int r = rows + e / 8, j = e & 7;
+            *reinterpret_cast<uint4*>(smem + st * kStageABytes + j * lboA + (r >> 3) * 128 + (r & 7) * 16) =
+                make_uint4(0u, 0u, 0u, 0u);
+        }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     const uint32_t tmem = tmemBase;
-    const uint32_t lboA = (kTcM / 8) * 128;
-    const uint32_t lboB = static_cast<uint32_t>(nPad / 8) * 128;
-    const uint32_t idesc = instrDesc(nPad);
-    const bf16* Xd = Xs + static_cast<size_t>(dx + 1) * Cin * P;
 
-    // The rows beyond Cout (A) and Cin (B) stay zero: written once here for every stage, never copied.
-    for (int st = 0; st < kTcStages; ++st) {
-        for (int e = tid; e < (kTcM - Cout) * 8; e += 128) {
-            const int co = Cout + e / 8, j = e & 7;
-            *reinterpret_cast<uint4*>(smem + st * kStageABytes + j * lboA + (co >> 3) * 128 + (co & 7) * 16) =
-                make_uint4(0u, 0u, 0u, 0u);
-        }
-        for (int e = tid; e < (nPad - Cin) * 8; e += 128) {
-            const int ci = Cin + e / 8, j = e & 7;
-            *reinterpret_cast<uint4*>(smem + kTcStages * kStageABytes + st * stageB + j * lboB + (ci >> 3) * 128 +
-                                      (ci & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
-        }
-    }
-    // Thread t copies chunk j = t % 8 (8 pixels) of channels t / 8, t / 8 + 16, ...: eight neighbouring threads
-    // read one channel's 128 contiguous bytes.  W % 8 == 0 keeps a chunk inside one image row, whose row index
-    // (32-bit: the pixel count is below 2^31) decides the zero fill of the dy-shifted operand.
+    // Thread t copies chunk j = t % 8 (8 pixels) of rows t / 8, t / 8 + 16, ...: eight neighbouring threads read one
+    // channel's 128 contiguous bytes.  The chunk's image row (32-bit: the pixel count is below 2^31) and each row's
+    // dy decide the zero fill.
     const int cj = tid & 7, cr = tid >> 3;
     auto issueCopies = [&](int it) {
         const int stage = it % kTcStages;
@@ -1019,14 +1022,14 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
         const uint32_t bBase = sB + stage * stageB + cj * lboB;
         const bool inRange = p < p1;
         const int y = static_cast<int>((static_cast<uint32_t>(p) / static_cast<uint32_t>(W)) % static_cast<uint32_t>(H));
-        const bool rowOk = inRange && y + dy >= 0 && y + dy < H;
-        const long long q = p + static_cast<long long>(dy) * W;
-        for (int co = cr; co < Cout; co += 16)   // A: dY^T, output channels x pixels
-            cpAsync16(aBase + (co >> 3) * 128 + (co & 7) * 16, inRange ? dYt + static_cast<size_t>(co) * P + p : dYt,
+        for (int r = cr; r < rows; r += 16) {   // A: the taps' shifted X, rows x pixels
+            const int yy = y + rowDy[r];
+            const bool ok = inRange && yy >= 0 && yy < H;
+            cpAsync16(aBase + (r >> 3) * 128 + (r & 7) * 16, ok ? Xs + rowSrc[r] + p : Xs, ok);
+        }
+        for (int co = cr; co < Cout; co += 16)   // B: dY^T, output channels x pixels
+            cpAsync16(bBase + (co >> 3) * 128 + (co & 7) * 16, inRange ? dYt + static_cast<size_t>(co) * P + p : dYt,
                       inRange);
-        for (int ci = cr; ci < Cin; ci += 16)    // B: X shifted by the tap, input channels x pixels
-            cpAsync16(bBase + (ci >> 3) * 128 + (ci & 7) * 16, rowOk ? Xd + static_cast<size_t>(ci) * P + q : Xd,
-                      rowOk);
     };
 
     // all threads run the same barriers; a timed-out wait only raises the abort flag (no further copy or MMA)
@@ -1071,10 +1074,11 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
     } else if (abortFlag || last != iters - 1) {
         if (tid == 0 && errorFlag) atomicOr(errorFlag, 1u);
     } else {
-        // warp w owns TMEM lanes 32w..32w+31 = output channels; columns = input channels
-        const int co = warp * 32 + (tid & 31);
-        float* dst = dW + (static_cast<size_t>(tap) * Cout + co) * Cin;
-        for (int c = 0; c < nPad; c += 16) {
+        // warp w owns TMEM lanes 32w..32w+31 = rows (tap, ci); columns = output channels
+        const int r = warp * 32 + (tid & 31), R = row0 + r;
+        const int tap = R / Cin, ci = R - tap * Cin;
+        float* dst = dW + static_cast<size_t>(tap) * Cout * Cin + ci;
+        for (int c = 0; c < Cout; c += 16) {
             uint32_t v[16];
             const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
@@ -1082,9 +1086,8 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
                            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                          : "r"(taddr));
-            if (co < Cout)
-                for (int k = 0; k < 16; ++k)
-                    if (c + k < Cin) atomicAdd(dst + c + k, __uint_as_float(v[k]));
+            if (r < rows)
+                for (int k = 0; k < 16; ++k) atomicAdd(dst + static_cast<size_t>(c + k) * Cin, __uint_as_float(v[k]));
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -1097,8 +1100,8 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
 bool convWgradTcSupported(int N, int H, int W, int Cin, int Cout)
 {
     const long long P = static_cast<long long>(N) * H * W;
-    return W % 8 == 0 && P % 64 == 0 && P > 0 && P < (1LL << 31) && Cin >= 16 && Cin <= kTcMaxN && Cin % 8 == 0 &&
-           Cout >= 1 && Cout <= kTcM;
+    return W % 8 == 0 && P % 64 == 0 && P > 0 && P < (1LL << 31) && Cin >= 1 && Cin % 8 == 0 && Cout >= 16 &&
+           Cout % 16 == 0 && Cout <= 128;
 }
 
 size_t convWgradTcScratchBytes(int N, int H, int W, int Cin, int Cout)
@@ -1124,20 +1127,20 @@ void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, in
         cudaFuncSetAttribute(kWgradTc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
         attrSet = true;
     }
-    const int nPad = (Cin + 15) / 16 * 16;
-    // shared memory for this launch's channel count only (3 stages of A and of nPad-channel B): 54-78 KB up to 80
-    // input channels, so two to four CTAs share an SM (their TMEM columns, at most 2 x 256, fit its 512) and hide
-    // one another's copy and issue latency; a few CTAs per SM over the nine taps, each at least 512 pixels, splits
-    // a multiple of 64 pixels
-    const int smemBytes = kTcStages * (kStageABytes + nPad * kTcKStage * 2);
-    const int resident = (220 * 1024) / smemBytes < 1 ? 1 : (220 * 1024) / smemBytes;
-    long long splits = (static_cast<long long>(resident) * 2 * 148 + 8) / 9;
+    // shared memory for this launch's output channels only (3 stages of the 128-row A and the Cout-row B: 54-96 KB),
+    // so two to four CTAs share an SM (their TMEM columns, at most 2 x 128, fit its 512) and hide one another's copy
+    // and issue latency; one wave of CTAs over the row tiles, each split at least 512 pixels, a multiple of 64
+    const int tiles = (9 * Cin + kTcM - 1) / kTcM;
+    const int smemBytes = kTcStages * (kStageABytes + Cout * kTcKStage * 2);
+    const int perSm = (227 * 1024) / (smemBytes + 3 * 1024);   // plus its static shared memory and the reserve
+    const int resident = perSm < 1 ? 1 : perSm;
+    long long splits = (static_cast<long long>(resident) * 148 + tiles - 1) / tiles;
     long long per = (P + splits - 1) / splits;
     if (per < 512) per = 512;
     per = (per + kTcKStage - 1) / kTcKStage * kTcKStage;
     splits = (P + per - 1) / per;
-    kWgradTc<<<dim3(1, 9, static_cast<unsigned>(splits)), 128, smemBytes, st>>>(dYt, Xs, H, W, P, Cin, Cout, nPad, per, dW,
-                                                                               errorFlag);
+    kWgradTc<<<dim3(static_cast<unsigned>(tiles), 1, static_cast<unsigned>(splits)), 128, smemBytes, st>>>(
+        dYt, Xs, H, W, P, Cin, Cout, per, dW, errorFlag);
 }
 
 bool convTcSupported(int Cin, int Cout) { return Cout % 16 == 0 && Cout >= 16 && Cout <= kTcMaxN && Cin % 16 == 0; }
