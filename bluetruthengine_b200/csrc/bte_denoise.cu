@@ -104,7 +104,7 @@ struct Net {
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
     int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2/3 tcgen05 row tiles
-    int wgradKind = 0;   // weight gradients: 0 warp-level mma.sync, 1 tcgen05 (shapes it supports)
+    int wgradKind = 1;   // weight gradients: 1 tcgen05 where the shape allows (default), 0 warp-level mma.sync
     Buf wgScratch;       // channel-major copies for the tcgen05 weight gradient
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
@@ -643,8 +643,8 @@ int bte_denoiser_debug_wait_timeout(unsigned int* status, double* seconds)
     });
 }
 
-// weight-gradient kernel of training: 0 the warp-level mma.sync kernel; 1 the tcgen05 kernel for the layers whose
-// shapes it takes (image width a multiple of 8, pixels a multiple of 64), the warp-level one for the rest
+// weight-gradient kernel of training: 1 (default) the tcgen05 kernel for the layers whose shapes it takes (image
+// width a multiple of 8, pixels a multiple of 64), the warp-level one for the rest; 0 the warp-level mma.sync kernel
 int bte_denoiser_set_wgrad(int kind)
 {
     return guardedDn([&] {

@@ -922,29 +922,42 @@ constexpr int kTcSmem = kTcStages * (kStageABytes + kStageBBytes);
 namespace {
 
 // ---------------------------------------------------------------- weight gradient on tcgen05
-// NHWC [P][C] -> channel-major [C][P], or the column-shifted channel-major copy (pixel (n, y, x) holds the value
-// of (n, y, x + dx), zero where x + dx leaves the row): 32 x 32 tiles through shared memory, both sides coalesced.
-__global__ void kPlanar(const bf16* __restrict__ in, int C, long long P, int W, int dx, bf16* __restrict__ out)
+// NHWC [P][C] -> kOut channel-major copies [kOut][C][P].  With kOut = 1 the plain transpose; with kOut = 3 the three
+// column-shifted copies s = 0, 1, 2 (dx = s - 1: pixel (n, y, x) holds the value of (n, y, x + dx), zero where
+// x + dx leaves the row), all made from one read of the input.  A block moves 64 pixels x 32 channels: 16-byte
+// loads of 8 channels of one pixel (plus one halo pixel each side for the shifts) into a padded shared tile, then
+// 16-byte stores of 8 pixels of one channel, a warp writing four whole 128-byte channel lines.  Needs C % 8 == 0,
+// W % 8 == 0 (a stored chunk's 8 pixels share one image row) and P % 8 == 0, P < 2^31.
+template <int kOut>
+__global__ void __launch_bounds__(256) kPlanar(const bf16* __restrict__ in, int C, int P, int W, bf16* __restrict__ out)
 {
-    __shared__ bf16 tile[32][34];
-    const long long pb = static_cast<long long>(blockIdx.x) * 32;
-    const int cb = static_cast<int>(blockIdx.y) * 32;
-    const int tx = static_cast<int>(threadIdx.x), ty = static_cast<int>(threadIdx.y);
-    for (int k = ty; k < 32; k += 8) {
-        const long long p = pb + k;
-        const int c = cb + tx;
-        bf16 v = __float2bfloat16(0.0f);
-        if (p < P && c < C) {
-            const int x = static_cast<int>(p % W);
-            if (x + dx >= 0 && x + dx < W) v = in[(p + dx) * C + c];
-        }
-        tile[k][tx] = v;
+    constexpr int kTP = 64, kTC = 32, kHalo = kOut == 3 ? 1 : 0, kRows = kTP + 2 * kHalo;
+    constexpr int kStride = kTC / 2 + 1;   // 32-bit words per tile row: 16 words of channels plus one of padding
+    __shared__ uint32_t tile[kRows * kStride];
+    const int pb = static_cast<int>(blockIdx.x) * kTP, cb = static_cast<int>(blockIdx.y) * kTC;
+    const int t = static_cast<int>(threadIdx.x);
+    for (int e = t; e < kRows * 4; e += 256) {   // tile row r = pixel pb - kHalo + r, chunk q = channels cb + 8q..
+        const int r = e >> 2, q = e & 3, p = pb - kHalo + r, c = cb + 8 * q;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (p >= 0 && p < P && c < C) v = *reinterpret_cast<const uint4*>(in + static_cast<size_t>(p) * C + c);
+        uint32_t* dst = tile + r * kStride + 4 * q;
+        dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; dst[3] = v.w;
     }
     __syncthreads();
-    for (int k = ty; k < 32; k += 8) {
-        const int c = cb + k;
-        const long long p = pb + tx;
-        if (c < C && p < P) out[static_cast<size_t>(c) * P + p] = tile[tx][k];
+    const unsigned short* tb = reinterpret_cast<const unsigned short*>(tile);
+    for (int u = t; u < kOut * kTC * 8; u += 256) {   // unit: copy s, channel cl, 8-pixel chunk j
+        const int j = u & 7, cl = (u >> 3) & (kTC - 1), s = u >> 8;
+        const int c = cb + cl, p0 = pb + 8 * j;
+        if (c >= C || p0 >= P) continue;
+        const int dx = s - kHalo, x0 = p0 % W;
+        uint32_t w[4];
+        for (int k = 0; k < 4; ++k) {
+            const int xa = x0 + 2 * k + dx, ra = 8 * j + 2 * k + dx + kHalo;   // source column, tile row
+            const uint32_t lo = xa >= 0 && xa < W ? tb[ra * (2 * kStride) + cl] : 0u;
+            const uint32_t hi = xa + 1 >= 0 && xa + 1 < W ? tb[(ra + 1) * (2 * kStride) + cl] : 0u;
+            w[k] = lo | (hi << 16);
+        }
+        *reinterpret_cast<uint4*>(out + (static_cast<size_t>(s) * C + c) * P + p0) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
@@ -1115,13 +1128,11 @@ void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, in
     const long long P = static_cast<long long>(N) * H * W;
     bf16* dYt = static_cast<bf16*>(scratch);
     bf16* Xs = dYt + static_cast<size_t>(Cout) * P;
-    const dim3 tb(32, 8);
-    const unsigned pb = static_cast<unsigned>((P + 31) / 32);
-    kPlanar<<<dim3(pb, static_cast<unsigned>((Cout + 31) / 32)), tb, 0, st>>>(static_cast<const bf16*>(dY), Cout, P, W,
-                                                                              0, dYt);
-    for (int dx = -1; dx <= 1; ++dx)
-        kPlanar<<<dim3(pb, static_cast<unsigned>((Cin + 31) / 32)), tb, 0, st>>>(
-            static_cast<const bf16*>(X), Cin, P, W, dx, Xs + static_cast<size_t>(dx + 1) * Cin * P);
+    const unsigned pt = static_cast<unsigned>((P + 63) / 64);
+    kPlanar<1><<<dim3(pt, static_cast<unsigned>((Cout + 31) / 32)), 256, 0, st>>>(static_cast<const bf16*>(dY), Cout,
+                                                                                  static_cast<int>(P), W, dYt);
+    kPlanar<3><<<dim3(pt, static_cast<unsigned>((Cin + 31) / 32)), 256, 0, st>>>(static_cast<const bf16*>(X), Cin,
+                                                                                 static_cast<int>(P), W, Xs);
     static bool attrSet = false;
     if (!attrSet) {
         cudaFuncSetAttribute(kWgradTc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);

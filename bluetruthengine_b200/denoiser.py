@@ -103,7 +103,7 @@ class Denoiser:
         return st.value, sec.value
 
     def set_wgrad(self, kind: int):
-        """Weight-gradient kernel of training: 0 warp-level mma.sync, 1 tcgen05 (where the layer's shape allows)."""
+        """Weight-gradient kernel of training: 1 tcgen05 where the layer's shape allows (default), 0 warp-level mma.sync."""
         self._ck(self.lib.bte_denoiser_set_wgrad(int(kind)))
 
     def last_ms(self) -> float:

@@ -59,7 +59,7 @@ def test_training_with_tcgen05_weight_gradient(dn):
             dn.set_dataset(noisy, feat, target)
             losses[kind] = dn.train(steps=60, batch=4, crop=48, lr=2e-3, seed=1)
     finally:
-        dn.set_wgrad(0)
+        dn.set_wgrad(1)   # the default
     for kind, loss in losses.items():
         print("wgrad kind", kind, "loss first/last", loss[:5].mean(), loss[-5:].mean())
         assert np.isfinite(loss).all() and loss[-5:].mean() < 0.7 * loss[:5].mean()
