@@ -271,7 +271,41 @@ __global__ void __launch_bounds__(128) kConvWgrad(const bf16* __restrict__ X, co
         }
 }
 
-// bias gradient: db[c] += sum_p dY[p][c]; one thread per channel pair, CTA over a pixel range
+// bias gradient: db[c] += sum_p dY[p][c].  A block of 256 threads sums a contiguous pixel range: thread t reads
+// the 16-byte chunk t % (C / 8) (8 channels) of every (256 / (C / 8))-th pixel, so a warp reads neighbouring
+// pixels' whole channel rows; the threads' sums are combined per channel in shared memory and added to db with one
+// atomic per channel and block.  C % 8 == 0, 8 <= C <= 256.
+__global__ void __launch_bounds__(256) kBiasGrad8(const bf16* __restrict__ dY, long long total, int C,
+                                                  long long pixPerCta, float* __restrict__ db)
+{
+    __shared__ float part[256 * 8];
+    const int chunks = C >> 3, lanes = 256 / chunks, t = static_cast<int>(threadIdx.x);
+    const int chunk = t % chunks, lane = t / chunks;
+    const long long p0 = static_cast<long long>(blockIdx.x) * pixPerCta;
+    const long long p1 = p0 + pixPerCta < total ? p0 + pixPerCta : total;
+    float s[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (lane < lanes) {
+#pragma unroll 4
+        for (long long p = p0 + lane; p < p1; p += lanes) {
+            const uint4 v = *reinterpret_cast<const uint4*>(dY + p * C + 8 * chunk);
+            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+            for (int k = 0; k < 4; ++k) {
+                s[2 * k] += __low2float(h[k]);
+                s[2 * k + 1] += __high2float(h[k]);
+            }
+        }
+    }
+    for (int k = 0; k < 8; ++k) part[t * 8 + k] = s[k];   // threads beyond lanes * chunks hold zeros
+    __syncthreads();
+    for (int c = t; c < C; c += 256) {
+        const int ch = c >> 3, k = c & 7;
+        float acc = 0.0f;
+        for (int l = 0; l < lanes; ++l) acc += part[(l * chunks + ch) * 8 + k];
+        atomicAdd(db + c, acc);
+    }
+}
+
+// bias gradient for channel counts that are not a multiple of 8: one thread per channel pair, CTA over a pixel range
 __global__ void kBiasGrad(const bf16* __restrict__ dY, long long total, int C, int pixPerCta, float* __restrict__ db)
 {
     const int c2 = threadIdx.x;   // blockDim = C / 2
@@ -285,6 +319,25 @@ __global__ void kBiasGrad(const bf16* __restrict__ dY, long long total, int C, i
     }
     atomicAdd(db + 2 * c2, s0);
     atomicAdd(db + 2 * c2 + 1, s1);
+}
+
+// dYm = dY where Y > 0 (ReLU derivative), elementwise over 16-byte groups of 8 bf16
+__global__ void kReluMask8(const uint4* __restrict__ Y, const uint4* dY, uint4* out, long long n8)   // out may be dY
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n8;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const uint4 y = Y[i];
+        uint4 d = dY[i];
+        const uint32_t* yw = reinterpret_cast<const uint32_t*>(&y);
+        uint32_t* dw = reinterpret_cast<uint32_t*>(&d);
+        for (int k = 0; k < 4; ++k) {
+            const __nv_bfloat162 yy = *reinterpret_cast<const __nv_bfloat162*>(&yw[k]);
+            const uint32_t keepLo = __low2float(yy) > 0.0f ? 0x0000ffffu : 0u;
+            const uint32_t keepHi = __high2float(yy) > 0.0f ? 0xffff0000u : 0u;
+            dw[k] &= keepLo | keepHi;
+        }
+        out[i] = d;
+    }
 }
 
 // dYm = dY where Y > 0 (ReLU derivative), elementwise over bf16 pairs
@@ -624,6 +677,16 @@ void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int 
 
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st)
 {
+    if (C % 8 == 0 && C >= 8 && C <= 256) {   // about eight blocks per SM, at least four pixels per thread
+        const long long lanes = 256 / (C / 8);
+        long long per = (pixels + 148LL * 8 - 1) / (148LL * 8);
+        if (per < 4 * lanes) per = 4 * lanes;
+        per = (per + lanes - 1) / lanes * lanes;
+        const long long ctas = (pixels + per - 1) / per;
+        if (ctas > 0)
+            kBiasGrad8<<<static_cast<unsigned>(ctas), 256, 0, st>>>(static_cast<const bf16*>(dY), pixels, C, per, db);
+        return;
+    }
     const int per = 1024;
     const long long ctas = (pixels + per - 1) / per;
     kBiasGrad<<<static_cast<unsigned>(ctas), C / 2, 0, st>>>(static_cast<const bf16*>(dY), pixels, C, per, db);
@@ -631,6 +694,12 @@ void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t s
 
 void reluMask(const void* Y, const void* dY, void* out, long long elems, cudaStream_t st)
 {
+    if (elems % 8 == 0 && reinterpret_cast<uintptr_t>(Y) % 16 == 0 && reinterpret_cast<uintptr_t>(dY) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(out) % 16 == 0) {
+        kReluMask8<<<gridFor(elems / 8), 256, 0, st>>>(static_cast<const uint4*>(Y), static_cast<const uint4*>(dY),
+                                                        static_cast<uint4*>(out), elems / 8);
+        return;
+    }
     kReluMask<<<gridFor(elems / 2), 256, 0, st>>>(static_cast<const bf16*>(Y), static_cast<const bf16*>(dY),
                                                   static_cast<bf16*>(out), elems / 2);
 }

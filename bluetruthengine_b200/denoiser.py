@@ -131,7 +131,9 @@ class Denoiser:
 
 
 def _main(argv=None):
-    """Time inference: python -m bluetruthengine_b200.denoiser --width 1920 --height 1080 --iters 5 [--kernels 0|1|2]"""
+    """Time inference: python -m bluetruthengine_b200.denoiser --width 1920 --height 1080 --iters 5 [--kernels 0|1|2]
+    Time training steps instead: python -m bluetruthengine_b200.denoiser --train-steps 10 [--wgrad 0|1] (batch 8 of
+    256x256 crops from 16 seeded synthetic images, after one untimed step)."""
     import argparse
     import json
     import os
@@ -143,8 +145,22 @@ def _main(argv=None):
                     help="0 warp-level MMA only, 1 tcgen05 pixel tiles, 2 tcgen05 row tiles, 3 row tiles upsampling in-kernel")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                       "denoiser_mixed.npz"))
+    ap.add_argument("--train-steps", type=int, default=0, help="time this many training steps instead of inference")
+    ap.add_argument("--wgrad", type=int, default=1, help="training weight gradients: 1 tcgen05, 0 warp-level")
     args = ap.parse_args(argv)
     dn = Denoiser()
+    if args.train_steps > 0:
+        dn.init(7)
+        rng = np.random.default_rng(0)
+        dn.set_dataset(rng.exponential(0.5, size=(16, 256, 256, 3)).astype(np.float32),
+                       rng.uniform(0, 1, size=(16, 256, 256, 6)).astype(np.float32),
+                       rng.exponential(0.5, size=(16, 256, 256, 3)).astype(np.float32))
+        dn.set_wgrad(args.wgrad)
+        dn.train(1, batch=8, crop=256, lr=1e-4, seed=1)
+        dn.train(args.train_steps, batch=8, crop=256, lr=1e-4, seed=2)
+        print(json.dumps({"train_steps": args.train_steps, "batch": 8, "crop": 256, "wgrad": args.wgrad,
+                          "ms_per_step": dn.last_ms() / args.train_steps}), flush=True)
+        return
     dn.load(args.weights)
     dn.set_tcgen05(args.kernels)
     rng = np.random.default_rng(0)
