@@ -104,7 +104,8 @@ struct Net {
     int dsCount = 0, dsW = 0, dsH = 0;
     float lastMs = 0.0f;
     int tcMode = 2;   // convolution kernels: 0 warp-level mma.sync only, 1 tcgen05 pixel tiles, 2/3 tcgen05 row tiles
-    int wgradKind = 1;   // weight gradients: 1 tcgen05 where the shape allows (default), 0 warp-level mma.sync
+    int wgradKind = 1;   // weight gradients: 1 tcgen05 where the shape allows (default), 0 warp-level mma.sync,
+                         // 2.. tcgen05 with pipeline shape wgradKind - 1 (convWgradTc's variants)
     Buf wgScratch;       // channel-major copies for the tcgen05 weight gradient
     Buf errFlag;          // set by a tcgen05 convolution that timed out
     Buf rowScratch;       // FP32 partial sums of a row-tile convolution that runs in passes
@@ -317,10 +318,11 @@ void backward(int N, int Hp, int Wp)
             const Conv& c = kConvs[s.conv];
             const long long elems = static_cast<long long>(N) * H * W * c.cout;
             if (c.relu) reluMask(net.act[s.dst].p, net.gact[s.dst].p, net.gact[s.dst].p, elems, st);
-            if (net.wgradKind == 1 && convWgradTcSupported(N, H, W, c.cin, c.cout)) {
+            if (net.wgradKind >= 1 && convWgradTcSupported(N, H, W, c.cin, c.cout)) {
                 net.wgScratch.ensure(convWgradTcScratchBytes(N, H, W, c.cin, c.cout));
                 convWgradTc(net.act[s.src].p, net.gact[s.dst].p, N, H, W, c.cin, c.cout,
-                            net.grad.as<float>() + net.wOff[s.conv], net.wgScratch.p, net.errFlag.as<unsigned int>(), st);
+                            net.grad.as<float>() + net.wOff[s.conv], net.wgScratch.p, net.errFlag.as<unsigned int>(), st,
+                            net.wgradKind - 1);
             } else {
                 convWgrad(net.act[s.src].p, net.gact[s.dst].p, N, H, W, c.cin, c.cout,
                           net.grad.as<float>() + net.wOff[s.conv], st);
@@ -644,11 +646,14 @@ int bte_denoiser_debug_wait_timeout(unsigned int* status, double* seconds)
 }
 
 // weight-gradient kernel of training: 1 (default) the tcgen05 kernel for the layers whose shapes it takes (image
-// width a multiple of 8, pixels a multiple of 64), the warp-level one for the rest; 0 the warp-level mma.sync kernel
+// width a multiple of 8, pixels a multiple of 64), the warp-level one for the rest; 0 the warp-level mma.sync kernel;
+// 2 to 1 + kWgradTcVariants: the tcgen05 kernel with pipeline shape kind - 1 (a tuning choice; the sums are the same)
 int bte_denoiser_set_wgrad(int kind)
 {
     return guardedDn([&] {
-        if (kind != 0 && kind != 1) throw CudaErr{"bte_denoiser_set_wgrad: kind must be 0 or 1"};
+        if (kind < 0 || kind > 1 + kWgradTcVariants)
+            throw CudaErr{"bte_denoiser_set_wgrad: kind must be 0 (warp-level), 1 (tcgen05) or 2 to " +
+                          std::to_string(1 + kWgradTcVariants) + " (tcgen05 pipeline shapes)"};
         ensureNet();
         net.wgradKind = kind;
         return 0;
@@ -736,7 +741,8 @@ int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float*
             Buf scratch;
             if (wgradTc) {
                 scratch.ensure(convWgradTcScratchBytes(n, h, wd, cin, cout));
-                convWgradTc(bx.p, bdy.p, n, h, wd, cin, cout, g.as<float>(), scratch.p, net.errFlag.as<unsigned int>(), st);
+                convWgradTc(bx.p, bdy.p, n, h, wd, cin, cout, g.as<float>(), scratch.p, net.errFlag.as<unsigned int>(), st,
+                            net.wgradKind >= 2 ? net.wgradKind - 1 : 0);
             } else {
                 convWgrad(bx.p, bdy.p, n, h, wd, cin, cout, g.as<float>(), st);
             }

@@ -42,8 +42,13 @@ void waitTimeoutProbe(unsigned int* dStatus, unsigned long long* dNs, cudaStream
 // Needs W % 8 == 0, N*H*W % 64 == 0, 16 <= Cin <= 256, Cout <= 128; sets *errorFlag on an internal timeout.
 bool convWgradTcSupported(int N, int H, int W, int Cin, int Cout);
 size_t convWgradTcScratchBytes(int N, int H, int W, int Cin, int Cout);
+// `variant` picks the pipeline shape (stages, copy lag, pixels per stage): 1 (3, 2, 64), 2 (4, 2, 64), 3 (6, 4, 32),
+// 4 (5, 3, 32) with zero-filling copies; 5 (3, 2, 64) and 6 (5, 3, 32) with plain copies of the in-range chunks and
+// shared-memory zero stores for the rest; 0 the default, kWgradTcDefaultVariant.
+constexpr int kWgradTcDefaultVariant = 1;
+constexpr int kWgradTcVariants = 6;
 void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, void* scratch,
-                 unsigned int* errorFlag, cudaStream_t st);
+                 unsigned int* errorFlag, cudaStream_t st, int variant = 0);
 // dW[9][Cout][Cin] += sum over pixels of dY x shifted X (FP32 atomics).
 void convWgrad(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, cudaStream_t st);
 void biasGrad(const void* dY, long long pixels, int C, float* db, cudaStream_t st);

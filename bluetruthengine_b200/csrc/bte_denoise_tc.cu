@@ -73,6 +73,15 @@ __device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, bool va
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0));
 }
+// the copy without the source-size operand (no zero fill): for chunks known to be in range
+__device__ __forceinline__ void cpAsync16Full(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+}
+__device__ __forceinline__ void stSharedZero16(uint32_t dst)
+{
+    asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};\n" ::"r"(dst), "r"(0u));
+}
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -968,29 +977,41 @@ __global__ void __launch_bounds__(256) kPlanar(const bf16* __restrict__ in, int 
 // than one M = Cout GEMM per tap.  Both operands come from the channel-major copies made beforehand (dYt[co][p]
 // and, per column shift dx, Xs[dx + 1][ci][p]), so one K-major 16-byte chunk is 8 consecutive pixels of one
 // channel; a row's dy shift is a whole-row offset (W % 8 == 0 keeps every chunk inside one image row, whose
-// validity decides the zero fill).  The pipeline is kConvTc's: 64-pixel stages through a 3-deep cp.async ring,
-// one thread issues four M128 x N x K16 MMAs per stage into one TMEM accumulator, every wait bounded.  The
-// epilogue adds the CTA's partial sums into dW with FP32 atomics (neighbouring lanes hold neighbouring input
-// channels of one tap: neighbouring addresses).  Grid: (row tiles, 1, pixel splits of a multiple of 64 pixels).
+// validity decides the zero fill).
+//
+// Pipeline: kKS-pixel stages in a kStages-deep ring filled by cp.async; the stage copied kLag iterations earlier is
+// handed to one thread, which issues kKS / 16 M128 x N x K16 MMAs into one TMEM accumulator and commits them to the
+// stage's barrier.  The buffer refilled at iteration it last held stage it - kStages, whose MMAs were issued at
+// iteration it - kStages + kLag: with kStages > kLag + 1 they had a whole iteration or more to finish, so the
+// threads seldom wait on them.  Each thread keeps its rows' source offsets, dy and shared-memory offsets in
+// registers and follows its chunk's image row by counting, so a stage costs its copies and little else.  Every
+// wait is bounded.  The epilogue adds the CTA's partial sums into dW with FP32 atomics (neighbouring lanes hold
+// neighbouring input channels of one tap: neighbouring addresses).  Grid: (row tiles, 1, pixel splits of a
+// multiple of kKS pixels).
+template <int kStages, int kLag, int kKS, bool kSplitFill>
 __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt, const bf16* __restrict__ Xs, int H,
                                                    int W, long long P, int Cin, int Cout, long long pixPerSplit,
                                                    float* __restrict__ dW, unsigned int* errorFlag)
 {
+    static_assert(kLag >= 1 && kLag < kStages && kKS % 16 == 0 && kKS >= 16 && kKS <= 64, "pipeline shape");
+    constexpr int kChunks = kKS / 8;               // 16-byte chunks (8 pixels) per row and stage
+    constexpr int kRowStep = 128 / kChunks;        // threads per chunk column
+    constexpr int kRowsPerThread = kTcM / kRowStep;
+    constexpr uint32_t kLboA = (kTcM / 8) * 128;   // distance between K-neighbouring core matrices of A
+    constexpr int kStageA = kTcM * kKS * 2;
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t mbar[kTcStages];
+    __shared__ uint64_t mbar[kStages];
     __shared__ uint32_t tmemBase;
     __shared__ volatile int abortFlag;
     __shared__ volatile int lastCommit;
-    __shared__ long long rowSrc[kTcM];   // row r: offset of its channel plane in Xs, plus its dy rows
-    __shared__ int rowDy[kTcM];
     const int tid = threadIdx.x, warp = tid >> 5;
     const int row0 = static_cast<int>(blockIdx.x) * kTcM;
     const int rows = 9 * Cin - row0 < kTcM ? 9 * Cin - row0 : kTcM;   // live rows of this tile
     const long long p0 = static_cast<long long>(blockIdx.z) * pixPerSplit;
     const long long p1 = p0 + pixPerSplit < P ? p0 + pixPerSplit : P;
-    const int iters = p1 > p0 ? static_cast<int>((p1 - p0 + kTcKStage - 1) / kTcKStage) : 0;
-    const int stageB = Cout * kTcKStage * 2;
-    const uint32_t sA = smemAddr(smem), sB = sA + kTcStages * kStageABytes;
+    const int iters = p1 > p0 ? static_cast<int>((p1 - p0 + kKS - 1) / kKS) : 0;
+    const int stageB = Cout * kKS * 2;
+    const uint32_t sA = smemAddr(smem), sB = sA + kStages * kStageA;
     const uint32_t tmemCols = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : (Cout <= 128 ? 128 : 256));
 
     if (warp == 0) {
@@ -999,86 +1020,111 @@ __global__ void __launch_bounds__(128, 1) kWgradTc(const bf16* __restrict__ dYt,
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 0) {
-        for (int st = 0; st < kTcStages; ++st) mbarInit(smemAddr(&mbar[st]), 1);
+        for (int st = 0; st < kStages; ++st) mbarInit(smemAddr(&mbar[st]), 1);
         abortFlag = 0;
         lastCommit = -1;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
     }
-    if (tid < rows) {
-        const int r = row0 + tid, tap = r / Cin, ci = r - tap * Cin, dy = tap / 3 - 1, dx = tap % 3 - 1;
-        rowSrc[tid] = (static_cast<long long>(dx + 1) * Cin + ci) * P + static_cast<long long>(dy) * W;
-        rowDy[tid] = dy;
-    }
-    const uint32_t lboA = (kTcM / 8) * 128;
     const uint32_t lboB = static_cast<uint32_t>(Cout / 8) * 128;
     const uint32_t idesc = instrDesc(Cout);
     // rows beyond the nine taps stay zero: written once here for every stage, never copied
-    for (int st = 0; st < kTcStages; ++st)
-        for (int e = tid; e < (kTcM - rows) * 8; e += 128) {
-            const int r = rows + e / 8, j = e & 7;
-            *reinterpret_cast<uint4*>(smem + st * kStageABytes + j * lboA + (r >> 3) * 128 + (r & 7) * 16) =
+    for (int st = 0; st < kStages; ++st)
+        for (int e = tid; e < (kTcM - rows) * kChunks; e += 128) {
+            const int r = rows + e / kChunks, j = e % kChunks;
+            *reinterpret_cast<uint4*>(smem + st * kStageA + j * kLboA + (r >> 3) * 128 + (r & 7) * 16) =
                 make_uint4(0u, 0u, 0u, 0u);
         }
+    // Thread t copies chunk cj = t % kChunks (8 pixels) of rows cr, cr + kRowStep, ...: neighbouring threads read
+    // one channel's contiguous pixels.  Per row: its source offset in Xs (channel plane plus dy rows), its dy and
+    // its offset in the stage buffer, fixed for the whole launch.
+    const int cj = tid % kChunks, cr = tid / kChunks;
+    long long rowSrc[kRowsPerThread];
+    int rowDy[kRowsPerThread];
+    uint32_t rowDst[kRowsPerThread];
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) {
+        const int r = cr + k * kRowStep;
+        const int R = row0 + (r < rows ? r : 0), tap = R / Cin, ci = R - tap * Cin, dy = tap / 3 - 1, dx = tap % 3 - 1;
+        rowSrc[k] = (static_cast<long long>(dx + 1) * Cin + ci) * P + static_cast<long long>(dy) * W;
+        rowDy[k] = r < rows ? dy : 1 << 20;   // a dead row never passes the row test below
+        rowDst[k] = cj * kLboA + (r >> 3) * 128 + (r & 7) * 16;
+    }
+    // the image row and column of this thread's first pixel, followed by counting from here on
+    long long pc = p0 + 8 * cj;
+    int x = static_cast<int>(pc % W);
+    int y = static_cast<int>((pc / W) % H);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     const uint32_t tmem = tmemBase;
 
-    // Thread t copies chunk j = t % 8 (8 pixels) of rows t / 8, t / 8 + 16, ...: eight neighbouring threads read one
-    // channel's 128 contiguous bytes.  The chunk's image row (32-bit: the pixel count is below 2^31) and each row's
-    // dy decide the zero fill.
-    const int cj = tid & 7, cr = tid >> 3;
-    auto issueCopies = [&](int it) {
-        const int stage = it % kTcStages;
-        const long long p = p0 + static_cast<long long>(it) * kTcKStage + 8 * cj;
-        const uint32_t aBase = sA + stage * kStageABytes + cj * lboA;
+    auto issueCopies = [&](int stage) {
+        const uint32_t aBase = sA + stage * kStageA;
         const uint32_t bBase = sB + stage * stageB + cj * lboB;
-        const bool inRange = p < p1;
-        const int y = static_cast<int>((static_cast<uint32_t>(p) / static_cast<uint32_t>(W)) % static_cast<uint32_t>(H));
-        for (int r = cr; r < rows; r += 16) {   // A: the taps' shifted X, rows x pixels
-            const int yy = y + rowDy[r];
+        const bool inRange = pc < p1;
+#pragma unroll
+        for (int k = 0; k < kRowsPerThread; ++k) {   // A: the taps' shifted X, rows x pixels
+            const int yy = y + rowDy[k];
             const bool ok = inRange && yy >= 0 && yy < H;
-            cpAsync16(aBase + (r >> 3) * 128 + (r & 7) * 16, ok ? Xs + rowSrc[r] + p : Xs, ok);
+            if (rowDy[k] == (1 << 20)) continue;
+            if (!kSplitFill) cpAsync16(aBase + rowDst[k], ok ? Xs + rowSrc[k] + pc : Xs, ok);
+            else if (ok) cpAsync16Full(aBase + rowDst[k], Xs + rowSrc[k] + pc);
+            else stSharedZero16(aBase + rowDst[k]);
         }
-        for (int co = cr; co < Cout; co += 16)   // B: dY^T, output channels x pixels
-            cpAsync16(bBase + (co >> 3) * 128 + (co & 7) * 16, inRange ? dYt + static_cast<size_t>(co) * P + p : dYt,
-                      inRange);
+        const bf16* b = dYt + static_cast<size_t>(cr) * P + pc;
+        for (int co = cr; co < Cout; co += kRowStep, b += static_cast<size_t>(kRowStep) * P) {   // B: dY^T
+            const uint32_t d = bBase + (co >> 3) * 128 + (co & 7) * 16;
+            if (!kSplitFill) cpAsync16(d, inRange ? b : dYt, inRange);
+            else if (inRange) cpAsync16Full(d, b);
+            else stSharedZero16(d);
+        }
     };
 
     // all threads run the same barriers; a timed-out wait only raises the abort flag (no further copy or MMA)
-    for (int it = 0; it < iters + kTcStages - 1; ++it) {
+    int fillStage = 0, mmaStage = 0;
+    for (int it = 0; it < iters + kLag; ++it) {
         if (it < iters && !abortFlag) {
             bool free = true;
-            if (it >= kTcStages) {
-                const int prev = it - kTcStages;
-                free = mbarWait(smemAddr(&mbar[prev % kTcStages]), static_cast<uint32_t>((prev / kTcStages) & 1));
+            if (it >= kStages) {
+                const int prev = it - kStages;
+                free = mbarWait(smemAddr(&mbar[fillStage]), static_cast<uint32_t>((prev / kStages) & 1));
             }
-            if (free) issueCopies(it);
+            if (free) issueCopies(fillStage);
             else abortFlag = 1;
         }
         cpAsyncCommit();
-        const int j = it - (kTcStages - 1);
+        if (it < iters) {   // the next stage's pixels: kKS columns on, into later image rows as they run out
+            pc += kKS;
+            x += kKS;
+            while (x >= W) {
+                x -= W;
+                if (++y == H) y = 0;
+            }
+            if (++fillStage == kStages) fillStage = 0;
+        }
+        const int j = it - kLag;
         if (j >= 0 && j < iters) {
-            cpAsyncWait<kTcStages - 1>();
+            cpAsyncWait<kLag>();
             asm volatile("fence.proxy.async.shared::cta;\n" ::);
             __syncthreads();
             if (tid == 0 && !abortFlag) {
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-                const int stage = j % kTcStages;
-                for (int k = 0; k < kTcKStage / 16; ++k) {
-                    const uint64_t da = smemDesc(sA + stage * kStageABytes + 2 * k * lboA, lboA, 128);
-                    const uint64_t db = smemDesc(sB + stage * stageB + 2 * k * lboB, lboB, 128);
+#pragma unroll
+                for (int k = 0; k < kKS / 16; ++k) {
+                    const uint64_t da = smemDesc(sA + mmaStage * kStageA + 2 * k * kLboA, kLboA, 128);
+                    const uint64_t db = smemDesc(sB + mmaStage * stageB + 2 * k * lboB, lboB, 128);
                     umma(tmem, da, db, idesc, (j > 0 || k > 0) ? 1u : 0u);
                 }
-                ummaCommit(smemAddr(&mbar[stage]));
+                ummaCommit(smemAddr(&mbar[mmaStage]));
                 lastCommit = j;
             }
+            if (++mmaStage == kStages) mmaStage = 0;
         }
     }
     cpAsyncWait<0>();
     __syncthreads();
     const int last = lastCommit;
-    if (last >= 0 && !mbarWait(smemAddr(&mbar[last % kTcStages]), static_cast<uint32_t>((last / kTcStages) & 1)))
+    if (last >= 0 && !mbarWait(smemAddr(&mbar[last % kStages]), static_cast<uint32_t>((last / kStages) & 1)))
         abortFlag = 1;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     __syncthreads();
@@ -1122,8 +1168,41 @@ size_t convWgradTcScratchBytes(int N, int H, int W, int Cin, int Cout)
     return static_cast<size_t>(N) * H * W * (static_cast<size_t>(Cout) + 3 * static_cast<size_t>(Cin)) * sizeof(bf16);
 }
 
+namespace {
+
+// one launch of kWgradTc<kStages, kLag, kKS>: shared memory for this launch's output channels only (kStages stages of
+// the 128-row A and the Cout-row B), as many CTAs per SM as shared memory and TMEM columns (512 per SM) allow, so
+// they hide one another's copy and issue latency; one wave of CTAs over the row tiles, each split at least 512
+// pixels and a multiple of kKS
+template <int kStages, int kLag, int kKS, bool kSplitFill>
+void launchWgradTc(const bf16* dYt, const bf16* Xs, int H, int W, long long P, int Cin, int Cout, float* dW,
+                   unsigned int* errorFlag, cudaStream_t st)
+{
+    static bool attrSet = false;
+    if (!attrSet) {
+        cudaFuncSetAttribute(kWgradTc<kStages, kLag, kKS, kSplitFill>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kStages * (kTcM + 128) * kKS * 2);
+        attrSet = true;
+    }
+    const int tiles = (9 * Cin + kTcM - 1) / kTcM;
+    const int smemBytes = kStages * (kTcM + Cout) * kKS * 2;
+    const int tmemCols = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : 128);
+    int perSm = (227 * 1024) / (smemBytes + 3 * 1024);   // plus its static shared memory and the reserve
+    if (perSm > 512 / tmemCols) perSm = 512 / tmemCols;
+    const int resident = perSm < 1 ? 1 : perSm;
+    long long splits = (static_cast<long long>(resident) * 148 + tiles - 1) / tiles;
+    long long per = (P + splits - 1) / splits;
+    if (per < 512) per = 512;
+    per = (per + kKS - 1) / kKS * kKS;
+    splits = (P + per - 1) / per;
+    kWgradTc<kStages, kLag, kKS, kSplitFill><<<dim3(static_cast<unsigned>(tiles), 1, static_cast<unsigned>(splits)), 128, smemBytes,
+                                   st>>>(dYt, Xs, H, W, P, Cin, Cout, per, dW, errorFlag);
+}
+
+}  // namespace
+
 void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, int Cout, float* dW, void* scratch,
-                 unsigned int* errorFlag, cudaStream_t st)
+                 unsigned int* errorFlag, cudaStream_t st, int variant)
 {
     const long long P = static_cast<long long>(N) * H * W;
     bf16* dYt = static_cast<bf16*>(scratch);
@@ -1133,25 +1212,15 @@ void convWgradTc(const void* X, const void* dY, int N, int H, int W, int Cin, in
                                                                                   static_cast<int>(P), W, dYt);
     kPlanar<3><<<dim3(pt, static_cast<unsigned>((Cin + 31) / 32)), 256, 0, st>>>(static_cast<const bf16*>(X), Cin,
                                                                                  static_cast<int>(P), W, Xs);
-    static bool attrSet = false;
-    if (!attrSet) {
-        cudaFuncSetAttribute(kWgradTc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-        attrSet = true;
+    // pipeline shapes (stages, copy lag, pixels per stage)
+    switch (variant == 0 ? kWgradTcDefaultVariant : variant) {
+    case 1: launchWgradTc<3, 2, 64, false>(dYt, Xs, H, W, P, Cin, Cout, dW, errorFlag, st); break;
+    case 2: launchWgradTc<4, 2, 64, false>(dYt, Xs, H, W, P, Cin, Cout, dW, errorFlag, st); break;
+    case 3: launchWgradTc<6, 4, 32, false>(dYt, Xs, H, W, P, Cin, Cout, dW, errorFlag, st); break;
+    case 4: launchWgradTc<5, 3, 32, false>(dYt, Xs, H, W, P, Cin, Cout, dW, errorFlag, st); break;
+    case 5: launchWgradTc<3, 2, 64, true>(dYt, Xs, H, W, P, Cin, Cout, dW, errorFlag, st); break;
+    default: launchWgradTc<5, 3, 32, true>(dYt, Xs, H, W, P, Cin, Cout, dW, errorFlag, st); break;
     }
-    // shared memory for this launch's output channels only (3 stages of the 128-row A and the Cout-row B: 54-96 KB),
-    // so two to four CTAs share an SM (their TMEM columns, at most 2 x 128, fit its 512) and hide one another's copy
-    // and issue latency; one wave of CTAs over the row tiles, each split at least 512 pixels, a multiple of 64
-    const int tiles = (9 * Cin + kTcM - 1) / kTcM;
-    const int smemBytes = kTcStages * (kStageABytes + Cout * kTcKStage * 2);
-    const int perSm = (227 * 1024) / (smemBytes + 3 * 1024);   // plus its static shared memory and the reserve
-    const int resident = perSm < 1 ? 1 : perSm;
-    long long splits = (static_cast<long long>(resident) * 148 + tiles - 1) / tiles;
-    long long per = (P + splits - 1) / splits;
-    if (per < 512) per = 512;
-    per = (per + kTcKStage - 1) / kTcKStage * kTcKStage;
-    splits = (P + per - 1) / per;
-    kWgradTc<<<dim3(static_cast<unsigned>(tiles), 1, static_cast<unsigned>(splits)), 128, smemBytes, st>>>(
-        dYt, Xs, H, W, P, Cin, Cout, per, dW, errorFlag);
 }
 
 bool convTcSupported(int Cin, int Cout) { return Cout % 16 == 0 && Cout >= 16 && Cout <= kTcMaxN && Cin % 16 == 0; }

@@ -103,7 +103,8 @@ class Denoiser:
         return st.value, sec.value
 
     def set_wgrad(self, kind: int):
-        """Weight-gradient kernel of training: 1 tcgen05 where the layer's shape allows (default), 0 warp-level mma.sync."""
+        """Weight-gradient kernel of training: 1 tcgen05 where the layer's shape allows (default), 0 warp-level mma.sync,
+        2-7 tcgen05 with one of its pipeline shapes (a tuning choice with the same sums)."""
         self._ck(self.lib.bte_denoiser_set_wgrad(int(kind)))
 
     def last_ms(self) -> float:
@@ -146,7 +147,7 @@ def _main(argv=None):
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                       "denoiser_mixed.npz"))
     ap.add_argument("--train-steps", type=int, default=0, help="time this many training steps instead of inference")
-    ap.add_argument("--wgrad", type=int, default=1, help="training weight gradients: 1 tcgen05, 0 warp-level")
+    ap.add_argument("--wgrad", type=int, default=1, help="training weight gradients: 1 tcgen05, 0 warp-level, 2-7 tcgen05 pipeline shapes")
     args = ap.parse_args(argv)
     dn = Denoiser()
     if args.train_steps > 0:

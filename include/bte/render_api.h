@@ -220,7 +220,10 @@ int bte_denoiser_debug_wait_timeout(unsigned int* status, double* seconds);
 int bte_denoiser_set_tcgen05(int mode);   /* conv kernels: 0 warp-level MMA, 1 tcgen05 pixel tiles, 2 row tiles (default), 3 row tiles upsampling in-kernel */
 /* Weight gradients of training: 1 (default) the tcgen05 kernel (pixels as the reduction axis over channel-major
  * copies) for layers whose image width is a multiple of 8 and pixel count a multiple of 64, the warp-level kernel
- * for the rest; 0 the warp-level mma.sync kernel for every layer. */
+ * for the rest; 0 the warp-level mma.sync kernel for every layer; 2-7 the tcgen05 kernel with one of its pipeline
+ * shapes (stages, copy lag, pixels per stage): 2 (3, 2, 64), 3 (4, 2, 64), 4 (6, 4, 32), 5 (5, 3, 32) with
+ * zero-filling copies, 6 (3, 2, 64) and 7 (5, 3, 32) with plain copies and shared-memory zero stores; a tuning
+ * choice with the same sums. */
 int bte_denoiser_set_wgrad(int kind);
 int bte_denoiser_debug_conv(int op, const float* x, const float* w, const float* bias, const float* dy, int n, int h,
                             int w_, int cin, int cout, int relu, float* out);

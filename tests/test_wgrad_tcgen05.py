@@ -41,6 +41,33 @@ def test_weight_gradient_tcgen05_matches_torch(dn, shape):
     assert np.abs(gw - warp_level).max() / np.abs(ref_w).max() < 1e-3
 
 
+@pytest.mark.parametrize("kind", [2, 3, 4, 5, 6, 7])
+def test_weight_gradient_tcgen05_pipeline_shapes(dn, kind):
+    """Every pipeline shape of the tcgen05 weight gradient (stages, copy lag, pixels per stage, copy form) gives the
+    same sums, on every test shape, two calls in a row."""
+    try:
+        dn.set_wgrad(kind)
+        for shape in SHAPES:
+            n, h, w, cin, cout = shape
+            rng = np.random.default_rng(cin * 7 + cout + kind)
+            x = _bf16(rng.normal(size=(n, h, w, cin)))
+            dy = _bf16(rng.normal(size=(n, h, w, cout)))
+            import torch
+            wt = np.zeros((9, cout, cin), np.float32)
+            _, wt_t, y = _torch_conv(x, wt, np.zeros(cout, np.float32))
+            y.backward(torch.from_numpy(dy).permute(0, 3, 1, 2))
+            ref_w = wt_t.grad.permute(2, 3, 0, 1).reshape(9, cout, cin).numpy()
+            ref_b = dy.reshape(-1, cout).sum(0)
+            for _ in range(2):
+                got = dn.debug_conv(7, x=x, dy=dy, shape=shape)
+                gw = got[:9 * cout * cin].reshape(9, cout, cin)
+                gb = got[9 * cout * cin:]
+                assert np.abs(gw - ref_w).max() / np.abs(ref_w).max() < 1e-3, (kind, shape)
+                assert np.abs(gb - ref_b).max() / max(np.abs(ref_b).max(), 1e-6) < 1e-3, (kind, shape)
+    finally:
+        dn.set_wgrad(1)   # the default
+
+
 def test_training_with_tcgen05_weight_gradient(dn):
     """The training loop with the tcgen05 weight gradient (the 48x48 crops and their 24x24 level take it; the
     smaller levels fall back) lowers the L1 loss as the warp-level kernel's run does."""
