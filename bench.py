@@ -162,6 +162,20 @@ DENOISER_CONVS = [(16, 32, 0), (32, 32, 0), (32, 48, 1), (48, 48, 1), (48, 64, 2
 DENOISER_FLOP_PER_PIXEL = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in DENOISER_CONVS)
 
 
+def frame_launches(depth: int, tuning: dict) -> int:
+    """Kernels one wavefront frame enqueues (bte_renderer.cu renderFrame / launchBounces): generate and present, an
+    extend, shade and connect per bounce, the tail kernel when it is on, one ordered compaction per hand-over of the
+    path-ordered bounces (buckets of bounces 0..K-1, queues of bounces 1..K-1; they need material sorting and no ray
+    reordering) and two launches (bin scan, scatter) per reordered bounce."""
+    n = 2 + 3 * depth + (1 if tuning.get("tailPaths", 0) > 0 else 0)
+    sort_bits = tuning.get("raySortBits", 0)
+    if sort_bits > 0:
+        n += 2 * max(0, min(tuning.get("raySortBounces", 0), depth - 1))
+    k = tuning.get("orderBounces", 0) if tuning.get("sortShading", 0) and sort_bits == 0 else 0
+    k = max(0, min(k, depth))
+    return n + k + max(k - 1, 0)
+
+
 def denoiser_layer_bound_ms(W, H, tflops, gbs):
     """Layer-by-layer roofline of one inference: each convolution takes at least the longer of its FLOPs at the
     tensor peak and its compulsory HBM bytes (the bf16 input read once, the bf16 output written once) at the HBM
@@ -519,7 +533,7 @@ def run_ours(args):
     stages = {"generate": st.msGenerate, "extend": st.msExtend, "shade": st.msShade, "connect": st.msConnect,
               "present": st.msPresent, "tail": st.msTail}
     dom = max((k for k in stages if k != "tail"), key=stages.get)
-    launches_per_frame = 2 + 3 * args.depth
+    launches_per_frame = frame_launches(args.depth, r.tuning())
     ext_f, sh_f = st.extends - st.tailExtends, st.shadowRays - st.tailShadowRays   # rays of the wavefront stages
     bytes_dom = {"extend": ext_f * BYTES_PER_EXTEND_RAY, "shade": ext_f * BYTES_PER_SHADE_SEGMENT,
                  "connect": sh_f * BYTES_PER_CONNECT_RAY, "tail": 0,

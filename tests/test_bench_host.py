@@ -6,6 +6,7 @@
   (include/wavefront/wavefront_buffers.h:40-90: path state 69 B, hit 36 B, queue entry 4 B, shadow record 44 B).
 * The layer-by-layer denoiser roofline is at least each bound it takes the larger of, and scales with the pixels.
 * Without a measured-peaks file the bench falls back to the stated fallback peaks and says so.
+* The kernel count it claims per frame follows the renderer's launch sequence for the tuning in force.
 """
 import importlib.util
 import os
@@ -83,3 +84,14 @@ def test_peaks_fall_back_without_measurements(bench, tmp_path, monkeypatch):
     (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 6550.7, "bf16_tflops": 1648.4}')
     assert bench.measured_peaks() == (6550.7, "measured")
     assert bench.measured_bf16_tflops()[0] == 1648.4
+
+
+def test_frame_launch_count(bench):
+    default = {"tailPaths": 4096, "sortShading": 1, "raySortBits": 0, "raySortBounces": 4, "orderBounces": 3}
+    # generate + present, 16 x (extend, shade, connect), tail, compactions: buckets of 0, 1, 2 and queues of 1, 2
+    assert bench.frame_launches(16, default) == 2 + 48 + 1 + 3 + 2
+    assert bench.frame_launches(16, dict(default, tailPaths=0)) == 55
+    assert bench.frame_launches(16, dict(default, sortShading=0)) == 51           # no path order without sorting
+    assert bench.frame_launches(16, dict(default, raySortBits=3)) == 51 + 2 * 4   # reordering replaces path order
+    assert bench.frame_launches(2, default) == 2 + 6 + 1 + 2 + 1                  # order capped at the depth
+    assert bench.frame_launches(1, dict(default, raySortBits=3)) == 2 + 3 + 1     # no bounce 1 to reorder
