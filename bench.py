@@ -176,6 +176,14 @@ def frame_launches(depth: int, tuning: dict) -> int:
     return n + k + max(k - 1, 0)
 
 
+def e2e_copy_bytes(W: int, H: int, depth: int) -> tuple:
+    """Host<->device bytes of one end-to-end step (bte_render + bte_read_framebuffer; bte_renderer.cu renderFrame):
+    to the device the frame's 4-byte sample-index base (the camera and scene stay resident; the frame parameters
+    travel as kernel arguments); back to the host the RGBA8 frame, the per-bounce extend and shadow-ray counters
+    ((depth + 1) 32-bit words each) and the 4-byte error word."""
+    return 4, W * H * 4 + 2 * (depth + 1) * 4 + 4
+
+
 def denoiser_layer_bound_ms(W, H, tflops, gbs):
     """Layer-by-layer roofline of one inference: each convolution takes at least the longer of its FLOPs at the
     tensor peak and its compulsory HBM bytes (the bf16 input read once, the bf16 output written once) at the HBM
@@ -554,8 +562,8 @@ def run_ours(args):
                       "l2": "inputs larger than L2 (path state %d MB per step)" % (spp_samples * 150 // (1 << 20)),
                       "parallelism": "replicas over sample ranges x%d" % world,
                       "frame_launch": "stream" if args.no_graph else "cuda graph", "tuning": r.tuning()},
-           "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": 56,
-                   "d2h_bytes_per_step": W * H * 4 + (3 * (args.depth + 1) * 4)},
+           "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": e2e_copy_bytes(W, H, args.depth)[0],
+                   "d2h_bytes_per_step": e2e_copy_bytes(W, H, args.depth)[1]},
            "gpu_launches": launches_per_frame * args.steps,
            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_source": peak_kind,

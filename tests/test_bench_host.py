@@ -6,7 +6,8 @@
   (include/wavefront/wavefront_buffers.h:40-90: path state 69 B, hit 36 B, queue entry 4 B, shadow record 44 B).
 * The layer-by-layer denoiser roofline is at least each bound it takes the larger of, and scales with the pixels.
 * Without a measured-peaks file the bench falls back to the stated fallback peaks and says so.
-* The kernel count it claims per frame follows the renderer's launch sequence for the tuning in force.
+* The kernel count it claims per frame follows the renderer's launch sequence for the tuning in force, and the
+  host<->device bytes it claims per end-to-end step are the copies the renderer's frame makes.
 """
 import importlib.util
 import os
@@ -95,3 +96,17 @@ def test_frame_launch_count(bench):
     assert bench.frame_launches(16, dict(default, raySortBits=3)) == 51 + 2 * 4   # reordering replaces path order
     assert bench.frame_launches(2, default) == 2 + 6 + 1 + 2 + 1                  # order capped at the depth
     assert bench.frame_launches(1, dict(default, raySortBits=3)) == 2 + 3 + 1     # no bounce 1 to reorder
+
+
+def test_e2e_copy_bytes_are_the_frames_copies(bench):
+    """The copies renderFrame makes (the frame-index upload, the counter and error-word readbacks) and the
+    framebuffer readback, counted from the renderer's source."""
+    src = open(os.path.join(ROOT, "bluetruthengine_b200", "csrc", "bte_renderer.cu")).read()
+    body = src[src.index("void renderFrame(int w, int h)"):]
+    body = body[:body.index("\n}\n")]
+    h2d = re.findall(r"cudaMemcpyAsync\(([^;]*?)cudaMemcpyHostToDevice", body)
+    d2h = re.findall(r"cudaMemcpyAsync\(([^;]*?)cudaMemcpyDeviceToHost", body)
+    assert len(h2d) == 1 and "sizeof(uint32_t)" in h2d[0]
+    assert len(d2h) == 3 and sum("(depth + 1)" in c for c in d2h) == 2 and sum(", 4," in c for c in d2h) == 1
+    W, H, depth = 1920, 1080, 16
+    assert bench.e2e_copy_bytes(W, H, depth) == (4, W * H * 4 + 2 * 17 * 4 + 4)
