@@ -109,21 +109,9 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.fh.close()
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
-            for line in open(self.path):
-                f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    sm.append(float(f[1]))
-                    mx = max(mx, float(f[2]))
-                except ValueError:
-                    continue
-                for k, name in enumerate(names):
-                    if f[5 + k].lower().startswith("active"):
-                        reasons.add(name)
+            with open(self.path) as f:
+                return parse_clock_lines(f)
         except Exception:
             return None
         finally:
@@ -131,9 +119,29 @@ class Clocks:
                 os.unlink(self.path)
             except OSError:
                 pass
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def parse_clock_lines(lines):
+    """Median SM clock, the highest max clock and the throttle reasons seen, from nvidia-smi's CSV lines (index,
+    clocks.sm, clocks.max.sm, power.draw, active-reasons mask, then hw_slowdown, hw_thermal_slowdown,
+    sw_thermal_slowdown and sw_power_cap as "Active" / "Not Active"); None without a sample."""
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in lines:
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = max(mx, float(f[2]))
+        except ValueError:
+            continue
+        for k, name in enumerate(names):
+            if f[5 + k].lower().startswith("active"):
+                reasons.add(name)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def measured_peaks():

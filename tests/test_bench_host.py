@@ -8,6 +8,7 @@
 * Without a measured-peaks file the bench falls back to the stated fallback peaks and says so.
 * The kernel count it claims per frame follows the renderer's launch sequence for the tuning in force, and the
   host<->device bytes it claims per end-to-end step are the copies the renderer's frame makes.
+* The clock record read from nvidia-smi's CSV: median SM clock, max clock and the throttle reasons seen.
 """
 import importlib.util
 import os
@@ -110,3 +111,16 @@ def test_e2e_copy_bytes_are_the_frames_copies(bench):
     assert len(d2h) == 3 and sum("(depth + 1)" in c for c in d2h) == 2 and sum(", 4," in c for c in d2h) == 1
     W, H, depth = 1920, 1080, 16
     assert bench.e2e_copy_bytes(W, H, depth) == (4, W * H * 4 + 2 * 17 * 4 + 4)
+
+
+def test_clock_lines(bench):
+    lines = ["0, 1965, 1965, 640.5, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active\n",
+             "0, 1950, 1965, 990.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n",
+             "0, 1800, 1965, 999.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n",
+             "0, [N/A], 1965, 10.0, 0x0, Not Active, Not Active, Not Active, Not Active\n",   # unreadable: skipped
+             "garbage\n"]
+    got = bench.parse_clock_lines(lines)
+    assert got == {"sm_mhz": 1950.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    hot = ["0, 1200, 1965, 700, 0x48, Not Active, Active, Not Active, Not Active\n"]
+    assert bench.parse_clock_lines(hot)["reasons"] == ["hw_thermal_slowdown"]
+    assert bench.parse_clock_lines([]) is None
