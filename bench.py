@@ -579,7 +579,9 @@ def run_ours(args):
                                     if dom in STAGE_DRAM_BYTES_PER_FRAME and W == 1920 and H == 1080 and args.spp == 2
                                     and args.depth == 16 else None),
                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on this "
-                                          "workload, per launch (one capture of the current build)",
+                                          "workload, per launch: a constant from one capture of the frame with "
+                                          "path-ordered queues (before the tail kernel and the register budgets); "
+                                          "null on other workloads",
                         "algorithmic_bytes_per_launch": bytes_dom / launches_dom,
                         "stage_ms": stages},
            "path_stats": {"extends_per_sample": s_mean, "shadow_rays_per_sample": r_mean,
