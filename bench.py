@@ -42,8 +42,9 @@ BYTES_PER_EXTEND_RAY = 64         # extend stage alone: queue 4 + ray 24 + hit 3
 BYTES_PER_SHADE_SEGMENT = 182
 BYTES_PER_CONNECT_RAY = 68        # 44 R + 24 RMW
 # DRAM bytes per frame of each stage kernel on this workload (1920x1080, 2 paths per pixel, depth 16), summed
-# over the frame's launches of that kernel from one ncu capture of the current build
-# (dram__bytes_read.sum + dram__bytes_write.sum); reported per launch beside the algorithmic bytes.
+# over the frame's launches of that kernel from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# frame with path-ordered queues, taken before the tail kernel and the register budgets; reported per launch beside
+# the algorithmic bytes.
 STAGE_DRAM_BYTES_PER_FRAME = {"extend": 726.4e6, "shade": 2915.0e6, "connect": 426.2e6}
 
 
