@@ -18,6 +18,12 @@ Sweeps the knobs that decide throughput on a given scene and GPU:
 timing whole frames on the device (CUDA events), and leaves the renderer in
 the fastest configuration.  Results are deterministic in value (every
 configuration renders the same bits); only speed differs.
+
+autotune_denoiser does the same for the learned denoiser: its convolution
+kernels (tcgen05 row tiles, row tiles upsampling in-kernel, pixel tiles) timed
+on inference at the caller's image size, and optionally the training weight
+gradient's kernel (tcgen05 pipeline shapes or the warp-level kernel) timed on
+training steps.
 """
 from __future__ import annotations
 
@@ -80,3 +86,60 @@ def autotune(renderer, width: int, height: int, samples_per_frame: int, max_dept
                         env_sampling=env_sampling, block_size=best.block_size)
     renderer.reset_accumulation(width, height)
     return best, results
+
+
+@dataclass
+class DenoiserTuneResult:
+    kernels: int            # convolution kernels (bte_denoiser_set_tcgen05 mode)
+    wgrad: int              # training weight-gradient kernel (bte_denoiser_set_wgrad kind); -1 when not timed
+    ms: float               # median device ms: one denoise, or one training step
+
+
+def autotune_denoiser(dn, width: int, height: int, kernels=(2, 3, 1), wgrad=(1, 2, 5, 7), train_steps: int = 0,
+                      batch: int = 8, crop: int = 128, iters: int = 3, seed: int = 0):
+    """Times the denoiser's kernel choices on this GPU and leaves the fastest in place.
+
+    Inference: with each convolution-kernel choice (`kernels`, bte_denoiser_set_tcgen05 modes) a seeded
+    width x height image is denoised once untimed (the first call at a size records its launch graph), then
+    `iters` times; the median device time decides.  Training, when `train_steps` > 0 and a data set is loaded:
+    with the chosen convolution kernels, each weight-gradient kernel (`wgrad`, bte_denoiser_set_wgrad kinds) runs
+    one untimed step and then `train_steps` timed ones, `iters` times.  Training moves the weights, so the weights
+    are put back afterwards through set_params, which also restarts Adam: tune before training.  Every choice
+    computes the same convolutions (to the tolerance of their tests), so only speed differs.
+
+    Returns (best kernels mode, best weight-gradient kind or None, every result)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    rad = rng.exponential(0.5, size=(height, width, 3)).astype(np.float32)
+    feat = rng.uniform(0, 1, size=(height, width, 6)).astype(np.float32)
+    results = []
+    for mode in kernels:
+        dn.set_tcgen05(mode)
+        dn.denoise(rad, feat)
+        ms = []
+        for _ in range(iters):
+            dn.denoise(rad, feat)
+            ms.append(dn.last_ms())
+        results.append(DenoiserTuneResult(mode, -1, float(np.median(ms))))
+    best_mode = min((r for r in results if r.wgrad < 0), key=lambda r: r.ms).kernels
+    dn.set_tcgen05(best_mode)
+    best_kind = None
+    if train_steps > 0 and wgrad:
+        saved = dn.params()
+        try:
+            timed = []
+            for kind in wgrad:
+                dn.set_wgrad(kind)
+                dn.train(1, batch=batch, crop=crop, lr=1e-4, seed=seed)
+                ms = []
+                for _ in range(iters):
+                    dn.train(train_steps, batch=batch, crop=crop, lr=1e-4, seed=seed + 1)
+                    ms.append(dn.last_ms() / train_steps)
+                timed.append(DenoiserTuneResult(best_mode, kind, float(np.median(ms))))
+            results += timed
+            best_kind = min(timed, key=lambda r: r.ms).wgrad
+            dn.set_wgrad(best_kind)
+        finally:
+            dn.set_params(saved)
+    return best_mode, best_kind, results
