@@ -95,14 +95,15 @@ class DenoiserTuneResult:
     ms: float               # median device ms: one denoise, or one training step
 
 
-def autotune_denoiser(dn, width: int, height: int, kernels=(2, 3, 1), wgrad=(1, 2, 5, 7), train_steps: int = 0,
+def autotune_denoiser(dn, width: int, height: int, kernels=(2, 3, 1), wgrad=(1, 3, 4, 5, 6, 7, 0), train_steps: int = 0,
                       batch: int = 8, crop: int = 128, iters: int = 3, seed: int = 0):
     """Times the denoiser's kernel choices on this GPU and leaves the fastest in place.
 
     Inference: with each convolution-kernel choice (`kernels`, bte_denoiser_set_tcgen05 modes) a seeded
     width x height image is denoised once untimed (the first call at a size records its launch graph), then
     `iters` times; the median device time decides.  Training, when `train_steps` > 0 and a data set is loaded:
-    with the chosen convolution kernels, each weight-gradient kernel (`wgrad`, bte_denoiser_set_wgrad kinds) runs
+    with the chosen convolution kernels, each weight-gradient kernel (`wgrad`, bte_denoiser_set_wgrad kinds: the
+    default list is every distinct one, kind 1 being the default pipeline shape of kind 2) runs
     one untimed step and then `train_steps` timed ones, `iters` times.  Training moves the weights, so the weights
     are put back afterwards through set_params, which also restarts Adam: tune before training.  Every choice
     computes the same convolutions (to the tolerance of their tests), so only speed differs.
